@@ -1,0 +1,119 @@
+"""Seeded synthetic inputs for the SIFT + guided-matching workloads.
+
+Nothing here is measured: these functions only build inputs with the shapes, sizes and value
+distributions of the benchmark workloads (no public dataset is involved).
+
+* ``synth_image``: sum of random Gaussian blobs (sigma 2-30 px, signed amplitudes up to 255) plus
+  1/f band-limited noise, rescaled to uint8 [0, 255].
+* ``random_homography`` / ``warp_pair``: image B = A warped by a random homography (rotation
+  +-10 deg, scale 0.9-1.1, translation +-200 px about the image centre) plus Gaussian noise
+  (sigma 3), clipped to uint8.
+* ``synth_descriptors``: SIFT-like 128-d uint8 descriptors (non-negative Gamma(0.6) draws,
+  L2-normalised, clipped at 0.2, renormalised, x512, rounded and saturated) with a fraction of
+  the B rows being copies of A rows with +-4 byte noise.
+"""
+import math
+
+import numpy as np
+
+
+def _blob_field(rng, h, w, n_blobs):
+    img = np.zeros((h, w), np.float32)
+    ys = rng.uniform(0, h, n_blobs)
+    xs = rng.uniform(0, w, n_blobs)
+    sig = rng.uniform(2.0, 30.0, n_blobs)
+    amp = rng.uniform(-255.0, 255.0, n_blobs)
+    for y, x, s, a in zip(ys, xs, sig, amp):
+        r = int(math.ceil(3.5 * s))
+        y0, y1 = max(0, int(y) - r), min(h, int(y) + r + 1)
+        x0, x1 = max(0, int(x) - r), min(w, int(x) + r + 1)
+        if y0 >= y1 or x0 >= x1:
+            continue
+        gy = np.exp(-((np.arange(y0, y1, dtype=np.float32) - y) ** 2) / (2 * s * s))
+        gx = np.exp(-((np.arange(x0, x1, dtype=np.float32) - x) ** 2) / (2 * s * s))
+        img[y0:y1, x0:x1] += np.float32(a) * gy[:, None] * gx[None, :]
+    return img
+
+
+def _pink_noise(rng, h, w, fmin=1.0 / 512, fmax=0.45):
+    white = rng.standard_normal((h, w)).astype(np.float32)
+    spec = np.fft.rfft2(white)
+    fy = np.fft.fftfreq(h)[:, None]
+    fx = np.fft.rfftfreq(w)[None, :]
+    f = np.sqrt(fx * fx + fy * fy)
+    band = (f >= fmin) & (f <= fmax)
+    scale = np.where(band, 1.0 / np.maximum(f, fmin), 0.0)
+    out = np.fft.irfft2(spec * scale, s=(h, w)).astype(np.float32)
+    return out / max(float(out.std()), 1e-6)
+
+
+def synth_image(h, w, seed, n_blobs=400, noise_weight=0.6):
+    """uint8 (h, w) image: Gaussian blobs + 1/f band-limited noise, min-max rescaled to 0..255."""
+    rng = np.random.default_rng(seed)
+    blobs = _blob_field(rng, h, w, n_blobs)
+    bs = float(blobs.std()) or 1.0
+    img = blobs / bs + np.float32(noise_weight) * _pink_noise(rng, h, w)
+    lo, hi = float(img.min()), float(img.max())
+    img = (img - lo) * (255.0 / max(hi - lo, 1e-6))
+    return np.clip(np.rint(img), 0, 255).astype(np.uint8)
+
+
+def random_homography(rng, h, w, rot_deg=10.0, scale=(0.9, 1.1), shift=200.0):
+    """3x3 float64 homography: rotation and scale about the image centre, then a translation."""
+    th = math.radians(rng.uniform(-rot_deg, rot_deg))
+    s = rng.uniform(*scale)
+    tx, ty = rng.uniform(-shift, shift, 2)
+    cx, cy = (w - 1) / 2.0, (h - 1) / 2.0
+    c, si = math.cos(th) * s, math.sin(th) * s
+    to_c = np.array([[1, 0, -cx], [0, 1, -cy], [0, 0, 1]], np.float64)
+    rs = np.array([[c, -si, 0], [si, c, 0], [0, 0, 1]], np.float64)
+    back = np.array([[1, 0, cx + tx], [0, 1, cy + ty], [0, 0, 1]], np.float64)
+    return back @ rs @ to_c
+
+
+def warp_pair(img, rng, noise_sigma=3.0, **hkw):
+    """Returns (B, H): B = img warped by a random homography H (A pixel -> B pixel) + noise."""
+    import cv2
+    h, w = img.shape
+    H = random_homography(rng, h, w, **hkw)
+    warped = cv2.warpPerspective(img, H, (w, h), flags=cv2.INTER_LINEAR, borderMode=cv2.BORDER_REFLECT_101)
+    noisy = warped.astype(np.float32) + rng.normal(0.0, noise_sigma, warped.shape).astype(np.float32)
+    return np.clip(np.rint(noisy), 0, 255).astype(np.uint8), H
+
+
+def synth_pair(h, w, seed):
+    """(A, B, H) image pair from one seed."""
+    a = synth_image(h, w, seed)
+    rng = np.random.default_rng(seed + 7919)
+    b, H = warp_pair(a, rng)
+    return a, b, H
+
+
+def apply_homography(H, xy):
+    """Project (n, 2) points by a 3x3 homography (float64)."""
+    xy = np.asarray(xy, np.float64)
+    p = np.c_[xy, np.ones(len(xy))] @ np.asarray(H, np.float64).T
+    return p[:, :2] / p[:, 2:3]
+
+
+def _sift_like(rng, n, d=128):
+    v = rng.gamma(0.6, 1.0, (n, d)).astype(np.float32)
+    v /= np.maximum(np.linalg.norm(v, axis=1, keepdims=True), 1e-12)
+    v = np.minimum(v, 0.2)
+    v /= np.maximum(np.linalg.norm(v, axis=1, keepdims=True), 1e-12)
+    return np.clip(np.rint(v * 512.0), 0, 255).astype(np.uint8)
+
+
+def synth_descriptors(na, nb, seed, true_frac=0.3, noise=4):
+    """(A u8 (na,128), B u8 (nb,128), truth) where truth[j] = A row copied into B row j, or -1."""
+    rng = np.random.default_rng(seed)
+    a = _sift_like(rng, na)
+    b = _sift_like(rng, nb)
+    n_true = int(round(true_frac * min(na, nb)))
+    rows_b = rng.choice(nb, n_true, replace=False)
+    rows_a = rng.choice(na, n_true, replace=False)
+    jitter = rng.integers(-noise, noise + 1, (n_true, a.shape[1]))
+    b[rows_b] = np.clip(a[rows_a].astype(np.int32) + jitter, 0, 255).astype(np.uint8)
+    truth = np.full(nb, -1, np.int64)
+    truth[rows_b] = rows_a
+    return a, b, truth
