@@ -1,0 +1,515 @@
+// C ABI of libfsb200: contexts, detect states, and the host-memory entry points declared in
+// include/fsb200.h.
+#include <time.h>
+
+#include <cmath>
+#include <cstring>
+#include <string>
+
+#include "fsb_internal.cuh"
+
+namespace fsb {
+
+static thread_local std::string g_err;
+
+void set_error(const char* fmt, ...) {
+    char buf[1024];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof(buf), fmt, ap);
+    va_end(ap);
+    g_err = buf;
+}
+
+int32_t DevBuf::ensure(size_t n) {
+    if (n <= bytes && p) return FSB_OK;
+    release();
+    size_t want = n < 256 ? 256 : n;
+    cudaError_t e = cudaMalloc(&p, want);
+    if (e != cudaSuccess) {
+        p = nullptr;
+        bytes = 0;
+        cudaGetLastError();
+        set_error("cudaMalloc(%zu) failed: %s", want, cudaGetErrorString(e));
+        return FSB_ERR_OOM;
+    }
+    bytes = want;
+    return FSB_OK;
+}
+
+void DevBuf::release() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    bytes = 0;
+}
+
+size_t Workspace::bytes() const {
+    size_t t = dog.bytes + mag.bytes + ang.bytes + img.bytes + cand.bytes + refined.bytes + oriented.bytes +
+               keys_a.bytes + keys_b.bytes + vals_a.bytes + vals_b.bytes + sort_tmp.bytes + counters.bytes +
+               kx.bytes + ky.bytes + ksize.bytes + kangle.bytes + kresp.bytes + koct.bytes + klayer.bytes;
+    for (const auto& b : plane) t += b.bytes;
+    return t;
+}
+
+void Workspace::release() {
+    DevBuf* all[] = {&dog, &mag, &ang, &img, &cand, &refined, &oriented, &keys_a, &keys_b, &vals_a, &vals_b,
+                     &sort_tmp, &counters, &kx, &ky, &ksize, &kangle, &kresp, &koct, &klayer,
+                     &plane[0], &plane[1], &plane[2]};
+    for (DevBuf* b : all) b->release();
+}
+
+// Sizes a workspace for an h x w image.
+static int32_t prepare_workspace(Workspace& ws, int h, int w) {
+    ws.g = make_geometry(h, w);
+    const Geometry& g = ws.g;
+    const size_t sum = (size_t)g.grad_off[g.n_oct] / 3;   // sum of octave pixels
+    const size_t p0 = (size_t)g.R[0] * g.C[0];
+    FSB_TRY(ws.dog.ensure(5 * sum * 4));
+    FSB_TRY(ws.mag.ensure(3 * sum * 4));
+    FSB_TRY(ws.ang.ensure(3 * sum * 4));
+    for (auto& b : ws.plane) FSB_TRY(b.ensure(p0 * 4));
+    FSB_TRY(ws.img.ensure((size_t)h * w));
+    if (ws.cap_cand < 65536) ws.cap_cand = 65536;
+    if (ws.cap_cand < sum / 64) ws.cap_cand = sum / 64;
+    FSB_TRY(ws.cand.ensure(ws.cap_cand * 4));
+    FSB_TRY(ws.counters.ensure(64));
+    return FSB_OK;
+}
+
+static Workspace* acquire(fsb_ctx* ctx) {
+    if (!ctx->pool.empty()) {
+        Workspace* w = ctx->pool.back();
+        ctx->pool.pop_back();
+        return w;
+    }
+    return new Workspace();
+}
+
+static void give_back(fsb_ctx* ctx, Workspace* w) {
+    if (ctx->pool.size() >= 2) {
+        w->release();
+        delete w;
+        return;
+    }
+    ctx->pool.push_back(w);
+}
+
+static int32_t use_device(fsb_ctx* ctx) {
+    FSB_CUDA(cudaSetDevice(ctx->device));
+    return FSB_OK;
+}
+
+template <class T>
+static int32_t to_dev(DevBuf& b, const T* h, size_t n, cudaStream_t s) {
+    FSB_TRY(b.ensure(n * sizeof(T) + 16));
+    if (n) FSB_CUDA(cudaMemcpyAsync(b.p, h, n * sizeof(T), cudaMemcpyHostToDevice, s));
+    return FSB_OK;
+}
+
+// detect into a workspace; the image is copied from host memory with its row stride
+static int32_t detect_into(fsb_ctx* ctx, Workspace& ws, const uint8_t* img, int h, int w, int stride,
+                           const fsb_sift_params* p, int max_kp) {
+    cudaStream_t s = ctx->stream;
+    FSB_TRY(prepare_workspace(ws, h, w));
+    FSB_CUDA(cudaMemcpy2DAsync(ws.img.p, (size_t)w, img, (size_t)stride, (size_t)w, (size_t)h,
+                               cudaMemcpyHostToDevice, s));
+    const bool exact = (p->flags & FSB_SIFT_EXACT_BLUR) != 0;
+    FSB_TRY(run_pyramid(ws, ws.img.as<uint8_t>(), w, exact, s));
+    FSB_TRY(run_detect(ws, p->contrast, p->edge, max_kp, s));
+    return FSB_OK;
+}
+
+__global__ void k_take(const int32_t* __restrict__ sel, int n, const float* x, const float* y, const float* sz,
+                       const float* an, const float* rs, const int32_t* oc, const int32_t* ly, float* ox, float* oy,
+                       float* osz, float* oan, float* ors, int32_t* ooc, int32_t* oly) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const int k = sel[i];
+    ox[i] = x[k]; oy[i] = y[k]; osz[i] = sz[k]; oan[i] = an[k]; ors[i] = rs[k]; ooc[i] = oc[k]; oly[i] = ly[k];
+}
+
+}  // namespace fsb
+
+using namespace fsb;
+
+extern "C" {
+
+int32_t fsb_version(void) { return 100; }
+
+const char* fsb_last_error(void) { return g_err.c_str(); }
+
+int32_t fsb_create(int32_t device, fsb_ctx** out) {
+    FSB_ARG(out != nullptr, "out is null");
+    *out = nullptr;
+    int n = 0;
+    FSB_CUDA(cudaGetDeviceCount(&n));
+    FSB_ARG(device >= 0 && device < n, "device index out of range");
+    cudaDeviceProp prop;
+    FSB_CUDA(cudaGetDeviceProperties(&prop, device));
+    if (prop.major != 10 || prop.minor != 0) {
+        set_error("device %d is sm_%d%d; this library is built for sm_100a (B200)", device, prop.major, prop.minor);
+        return FSB_ERR_UNSUPPORTED;
+    }
+    FSB_CUDA(cudaSetDevice(device));
+    fsb_ctx* ctx = new fsb_ctx();
+    ctx->device = device;
+    cudaError_t e = cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking);
+    if (e != cudaSuccess) {
+        delete ctx;
+        set_error("cudaStreamCreate failed: %s", cudaGetErrorString(e));
+        return FSB_ERR_CUDA;
+    }
+    int32_t st = upload_taps();
+    if (st != FSB_OK) {
+        cudaStreamDestroy(ctx->stream);
+        delete ctx;
+        return st;
+    }
+    *out = ctx;
+    return FSB_OK;
+}
+
+int32_t fsb_destroy(fsb_ctx* ctx) {
+    if (!ctx) return FSB_OK;
+    cudaSetDevice(ctx->device);
+    cudaStreamSynchronize(ctx->stream);
+    for (Workspace* w : ctx->pool) {
+        w->release();
+        delete w;
+    }
+    ctx->pool.clear();
+    DevBuf* all[] = {&ctx->s_u8a, &ctx->s_u8b, &ctx->s_f32a, &ctx->s_f32b, &ctx->s_i32, &ctx->s_i64,
+                     &ctx->s_u64, &ctx->s_misc, &ctx->s_misc2, &ctx->s_host_stage, &ctx->s_cub};
+    for (DevBuf* b : all) b->release();
+    if (ctx->pinned) cudaFreeHost(ctx->pinned);
+    cudaStreamDestroy(ctx->stream);
+    delete ctx;
+    return FSB_OK;
+}
+
+int32_t fsb_sync(fsb_ctx* ctx, int32_t timeout_ms) {
+    FSB_ARG(ctx, "ctx is null");
+    FSB_TRY(use_device(ctx));
+    cudaEvent_t ev;
+    FSB_CUDA(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+    cudaError_t e = cudaEventRecord(ev, ctx->stream);
+    if (e != cudaSuccess) {
+        cudaEventDestroy(ev);
+        set_error("cudaEventRecord failed: %s", cudaGetErrorString(e));
+        return FSB_ERR_CUDA;
+    }
+    // bounded poll: the host gives up after timeout_ms instead of blocking forever
+    const long long limit = timeout_ms <= 0 ? 0 : (long long)timeout_ms * 1000;
+    long long waited = 0;
+    while ((e = cudaEventQuery(ev)) == cudaErrorNotReady) {
+        if (waited >= limit) {
+            cudaEventDestroy(ev);
+            set_error("stream did not drain within %d ms", timeout_ms);
+            return FSB_ERR_TIMEOUT;
+        }
+        struct timespec ts = {0, 50000};
+        nanosleep(&ts, nullptr);
+        waited += 50;
+    }
+    cudaEventDestroy(ev);
+    if (e != cudaSuccess) {
+        set_error("stream error: %s", cudaGetErrorString(e));
+        return FSB_ERR_CUDA;
+    }
+    return FSB_OK;
+}
+
+void* fsb_stream(fsb_ctx* ctx) { return ctx ? (void*)ctx->stream : nullptr; }
+
+int64_t fsb_device_bytes(fsb_ctx* ctx) {
+    if (!ctx) return 0;
+    int64_t t = 0;
+    for (Workspace* w : ctx->pool) t += (int64_t)w->bytes();
+    const DevBuf* all[] = {&ctx->s_u8a, &ctx->s_u8b, &ctx->s_f32a, &ctx->s_f32b, &ctx->s_i32, &ctx->s_i64,
+                           &ctx->s_u64, &ctx->s_misc, &ctx->s_misc2, &ctx->s_host_stage, &ctx->s_cub};
+    for (const DevBuf* b : all) t += (int64_t)b->bytes;
+    return t;
+}
+
+int32_t fsb_detect(fsb_ctx* ctx, const uint8_t* img, int32_t h, int32_t w, int32_t stride,
+                   const fsb_sift_params* p, fsb_state** state, int32_t* n_kp) {
+    FSB_ARG(ctx && img && p && state && n_kp, "null pointer");
+    FSB_ARG(h > 0 && w > 0 && stride >= w, "bad image size or stride");
+    FSB_ARG(h <= 32768 && w <= 32768, "image larger than 32768 pixels on a side");
+    FSB_ARG(p->max_kp >= 0, "max_kp < 0");
+    *state = nullptr;
+    *n_kp = 0;
+    FSB_TRY(use_device(ctx));
+    Workspace* ws = acquire(ctx);
+    int32_t st = detect_into(ctx, *ws, img, h, w, stride, p, p->max_kp);
+    if (st == FSB_OK) {
+        cudaError_t e = cudaStreamSynchronize(ctx->stream);
+        if (e != cudaSuccess) {
+            set_error("detect: %s", cudaGetErrorString(e));
+            st = FSB_ERR_CUDA;
+        }
+    }
+    if (st != FSB_OK) {
+        give_back(ctx, ws);
+        return st;
+    }
+    ws->g.h = h;
+    fsb_state* s = new fsb_state();
+    s->ctx = ctx;
+    s->ws = ws;
+    s->magic = STATE_MAGIC;
+    s->exact = (p->flags & FSB_SIFT_EXACT_BLUR) != 0;
+    ctx->live_states++;
+    *state = s;
+    *n_kp = ws->n_kp;
+    return FSB_OK;
+}
+
+int32_t fsb_state_keypoints(fsb_state* st, float* x, float* y, float* size, float* angle, float* response,
+                            int32_t* octave, int32_t* layer) {
+    FSB_ARG(st && st->magic == STATE_MAGIC, "invalid state");
+    fsb_ctx* ctx = st->ctx;
+    FSB_TRY(use_device(ctx));
+    const Workspace& ws = *st->ws;
+    const size_t n = (size_t)ws.n_kp;
+    cudaStream_t s = ctx->stream;
+    struct { void* h; const DevBuf* d; } out[] = {{x, &ws.kx}, {y, &ws.ky}, {size, &ws.ksize}, {angle, &ws.kangle},
+                                                 {response, &ws.kresp}, {octave, &ws.koct}, {layer, &ws.klayer}};
+    for (auto& o : out)
+        if (o.h && n) FSB_CUDA(cudaMemcpyAsync(o.h, o.d->p, n * 4, cudaMemcpyDeviceToHost, s));
+    FSB_CUDA(cudaStreamSynchronize(s));
+    return FSB_OK;
+}
+
+int32_t fsb_describe(fsb_ctx* ctx, fsb_state* st, int32_t n, const float* x, const float* y, const float* size,
+                     const float* angle, const int32_t* octave, const int32_t* layer, float* desc,
+                     uint8_t* rootsift) {
+    FSB_ARG(ctx && st && st->magic == STATE_MAGIC, "invalid context or state");
+    if (st->ctx != ctx) {
+        set_error("state belongs to another context");
+        return FSB_ERR_STATE;
+    }
+    FSB_ARG(n >= 0, "n < 0");
+    if (n == 0) return FSB_OK;
+    FSB_ARG(x && y && size && angle && octave && layer, "null keypoint array");
+    const Workspace& ws = *st->ws;
+    for (int i = 0; i < n; ++i) {
+        if (octave[i] < 0 || octave[i] >= ws.g.n_oct || layer[i] < 1 || layer[i] > N_LAYERS) {
+            set_error("keypoint %d has octave %d / layer %d outside the detected pyramid", i, octave[i], layer[i]);
+            return FSB_ERR_ARG;
+        }
+    }
+    FSB_TRY(use_device(ctx));
+    cudaStream_t s = ctx->stream;
+    FSB_TRY(ctx->s_f32a.ensure((size_t)n * 4 * 6 + 256));
+    float* dx = ctx->s_f32a.as<float>();
+    float* dy = dx + n;
+    float* ds = dy + n;
+    float* da = ds + n;
+    int32_t* dout = reinterpret_cast<int32_t*>(da + n);
+    int32_t* dl = dout + n;
+    FSB_CUDA(cudaMemcpyAsync(dx, x, n * 4, cudaMemcpyHostToDevice, s));
+    FSB_CUDA(cudaMemcpyAsync(dy, y, n * 4, cudaMemcpyHostToDevice, s));
+    FSB_CUDA(cudaMemcpyAsync(ds, size, n * 4, cudaMemcpyHostToDevice, s));
+    FSB_CUDA(cudaMemcpyAsync(da, angle, n * 4, cudaMemcpyHostToDevice, s));
+    FSB_CUDA(cudaMemcpyAsync(dout, octave, n * 4, cudaMemcpyHostToDevice, s));
+    FSB_CUDA(cudaMemcpyAsync(dl, layer, n * 4, cudaMemcpyHostToDevice, s));
+    FSB_TRY(ctx->s_f32b.ensure((size_t)n * 128 * 4 + 256));
+    FSB_TRY(ctx->s_u8a.ensure((size_t)n * 128 + 256));
+    float* dd = desc ? ctx->s_f32b.as<float>() : nullptr;
+    uint8_t* du = rootsift ? ctx->s_u8a.as<uint8_t>() : nullptr;
+    FSB_TRY(run_describe_mode(ws, n, dx, dy, ds, da, dout, dl, dd, du, st->exact, s));
+    if (desc) FSB_CUDA(cudaMemcpyAsync(desc, dd, (size_t)n * 128 * 4, cudaMemcpyDeviceToHost, s));
+    if (rootsift) FSB_CUDA(cudaMemcpyAsync(rootsift, du, (size_t)n * 128, cudaMemcpyDeviceToHost, s));
+    FSB_CUDA(cudaStreamSynchronize(s));
+    return FSB_OK;
+}
+
+int32_t fsb_state_free(fsb_state* st) {
+    if (!st) return FSB_OK;
+    FSB_ARG(st->magic == STATE_MAGIC, "invalid state (double free?)");
+    fsb_ctx* ctx = st->ctx;
+    st->magic = 0;
+    cudaSetDevice(ctx->device);
+    give_back(ctx, st->ws);
+    ctx->live_states--;
+    delete st;
+    return FSB_OK;
+}
+
+int32_t fsb_sift_features(fsb_ctx* ctx, const uint8_t* img, int32_t h, int32_t w, int32_t stride,
+                          const fsb_sift_params* p, int32_t nfeat, float* xy, float* resp, float* desc,
+                          uint8_t* rootsift, int32_t* n_out) {
+    FSB_ARG(ctx && img && p && n_out, "null pointer");
+    FSB_ARG(h > 0 && w > 0 && stride >= w, "bad image size or stride");
+    FSB_ARG(nfeat >= 0, "nfeat < 0");
+    *n_out = 0;
+    FSB_TRY(use_device(ctx));
+    cudaStream_t s = ctx->stream;
+    Workspace* ws = acquire(ctx);
+    struct Guard {
+        fsb_ctx* c;
+        Workspace* w;
+        ~Guard() { give_back(c, w); }
+    } guard{ctx, ws};
+    const int max_kp = (int)((double)nfeat * 2.2);
+    FSB_TRY(detect_into(ctx, *ws, img, h, w, stride, p, max_kp));
+    if (ws->n_kp < 10) {
+        FSB_CUDA(cudaStreamSynchronize(s));
+        return FSB_OK;
+    }
+    FSB_TRY(ctx->s_i64.ensure((size_t)ws->n_kp * 4 + 256));
+    int32_t* sel = ctx->s_i64.as<int32_t>();
+    int n_sel = 0;
+    FSB_TRY(run_spread(*ws, nfeat, sel, &n_sel, ctx, s));
+    if (n_sel == 0) return FSB_OK;
+    FSB_TRY(ctx->s_f32a.ensure((size_t)n_sel * 4 * 7 + 256));
+    float* tx = ctx->s_f32a.as<float>();
+    float* ty = tx + n_sel;
+    float* tsz = ty + n_sel;
+    float* tan_ = tsz + n_sel;
+    float* trs = tan_ + n_sel;
+    int32_t* toc = reinterpret_cast<int32_t*>(trs + n_sel);
+    int32_t* tly = toc + n_sel;
+    k_take<<<(n_sel + 255) / 256, 256, 0, s>>>(sel, n_sel, ws->kx.as<float>(), ws->ky.as<float>(),
+                                               ws->ksize.as<float>(), ws->kangle.as<float>(), ws->kresp.as<float>(),
+                                               ws->koct.as<int32_t>(), ws->klayer.as<int32_t>(), tx, ty, tsz, tan_,
+                                               trs, toc, tly);
+    FSB_CUDA(cudaGetLastError());
+    FSB_TRY(ctx->s_f32b.ensure((size_t)n_sel * 128 * 4 + 256));
+    FSB_TRY(ctx->s_u8a.ensure((size_t)n_sel * 128 + 256));
+    float* dd = desc ? ctx->s_f32b.as<float>() : nullptr;
+    uint8_t* du = rootsift ? ctx->s_u8a.as<uint8_t>() : nullptr;
+    const bool exact = (p->flags & FSB_SIFT_EXACT_BLUR) != 0;
+    FSB_TRY(run_describe_mode(*ws, n_sel, tx, ty, tsz, tan_, toc, tly, dd, du, exact, s));
+    if (xy) {
+        FSB_CUDA(cudaMemcpy2DAsync(xy, 8, tx, 4, 4, n_sel, cudaMemcpyDeviceToHost, s));
+        FSB_CUDA(cudaMemcpy2DAsync(xy + 1, 8, ty, 4, 4, n_sel, cudaMemcpyDeviceToHost, s));
+    }
+    if (resp) FSB_CUDA(cudaMemcpyAsync(resp, trs, (size_t)n_sel * 4, cudaMemcpyDeviceToHost, s));
+    if (desc) FSB_CUDA(cudaMemcpyAsync(desc, dd, (size_t)n_sel * 512, cudaMemcpyDeviceToHost, s));
+    if (rootsift) FSB_CUDA(cudaMemcpyAsync(rootsift, du, (size_t)n_sel * 128, cudaMemcpyDeviceToHost, s));
+    FSB_CUDA(cudaStreamSynchronize(s));
+    *n_out = n_sel;
+    return FSB_OK;
+}
+
+int32_t fsb_match_bf(fsb_ctx* ctx, const uint8_t* a, int32_t na, const uint8_t* b, int32_t nb, float ratio,
+                     int32_t precision, int64_t* q, int64_t* t, int32_t* n_out) {
+    FSB_ARG(ctx && n_out, "null pointer");
+    FSB_ARG(na >= 0 && nb >= 0, "negative size");
+    FSB_ARG((na == 0 || a) && (nb == 0 || b), "null descriptor array");
+    FSB_ARG(na == 0 || (q && t), "null output array");
+    FSB_ARG(precision >= FSB_PREC_FP32 && precision <= FSB_PREC_FP8, "unknown precision");
+    *n_out = 0;
+    if (na < 2 || nb < 2) return FSB_OK;
+    FSB_TRY(use_device(ctx));
+    cudaStream_t s = ctx->stream;
+    FSB_TRY(to_dev(ctx->s_u8a, a, (size_t)na * 128, s));
+    FSB_TRY(to_dev(ctx->s_u8b, b, (size_t)nb * 128, s));
+    FSB_TRY(ctx->s_i64.ensure((size_t)na * 16 + 64));
+    int64_t* dq = ctx->s_i64.as<int64_t>();
+    int64_t* dt = dq + na;
+    int* dn = reinterpret_cast<int*>(dt + na);
+    FSB_TRY(run_match_bf(ctx, ctx->s_u8a.as<uint8_t>(), na, ctx->s_u8b.as<uint8_t>(), nb, ratio, precision, dq, dt,
+                         dn, s));
+    int n = 0;
+    FSB_CUDA(cudaMemcpyAsync(&n, dn, sizeof(int), cudaMemcpyDeviceToHost, s));
+    FSB_CUDA(cudaStreamSynchronize(s));
+    if (n) {
+        FSB_CUDA(cudaMemcpyAsync(q, dq, (size_t)n * 8, cudaMemcpyDeviceToHost, s));
+        FSB_CUDA(cudaMemcpyAsync(t, dt, (size_t)n * 8, cudaMemcpyDeviceToHost, s));
+        FSB_CUDA(cudaStreamSynchronize(s));
+    }
+    *n_out = n;
+    return FSB_OK;
+}
+
+int32_t fsb_match_guided(fsb_ctx* ctx, const double* pred_xy, const uint8_t* a, int32_t na, const double* b_xy,
+                         const uint8_t* b, int32_t nb, double w_b, double h_b, double radius, int32_t kc,
+                         float ratio, int64_t* q, int64_t* t, int32_t* n_out) {
+    FSB_ARG(ctx && n_out, "null pointer");
+    FSB_ARG(na >= 0 && nb >= 0, "negative size");
+    FSB_ARG((na == 0 || (a && pred_xy && q && t)) && (nb == 0 || (b && b_xy)), "null array");
+    FSB_ARG(std::isfinite(radius) && std::isfinite(w_b) && std::isfinite(h_b), "non-finite frame or radius");
+    *n_out = 0;
+    if (na == 0 || nb == 0 || !(radius > 0.0)) return FSB_OK;
+    FSB_TRY(use_device(ctx));
+    cudaStream_t s = ctx->stream;
+    FSB_TRY(to_dev(ctx->s_u8a, a, (size_t)na * 128, s));
+    FSB_TRY(to_dev(ctx->s_u8b, b, (size_t)nb * 128, s));
+    FSB_TRY(ctx->s_f32a.ensure((size_t)(na + nb) * 16 + 256));
+    double* dp = ctx->s_f32a.as<double>();
+    double* dbx = dp + 2 * (size_t)na;
+    FSB_CUDA(cudaMemcpyAsync(dp, pred_xy, (size_t)na * 16, cudaMemcpyHostToDevice, s));
+    FSB_CUDA(cudaMemcpyAsync(dbx, b_xy, (size_t)nb * 16, cudaMemcpyHostToDevice, s));
+    FSB_TRY(ctx->s_i64.ensure((size_t)na * 16 + 64));
+    int64_t* dq = ctx->s_i64.as<int64_t>();
+    int64_t* dt = dq + na;
+    int* dn = reinterpret_cast<int*>(dt + na);
+    FSB_TRY(run_match_guided(ctx, dp, ctx->s_u8a.as<uint8_t>(), na, dbx, ctx->s_u8b.as<uint8_t>(), nb, w_b, h_b, radius,
+                             kc, ratio, dq, dt, dn, s));
+    int n = 0;
+    FSB_CUDA(cudaMemcpyAsync(&n, dn, sizeof(int), cudaMemcpyDeviceToHost, s));
+    FSB_CUDA(cudaStreamSynchronize(s));
+    if (n) {
+        FSB_CUDA(cudaMemcpyAsync(q, dq, (size_t)n * 8, cudaMemcpyDeviceToHost, s));
+        FSB_CUDA(cudaMemcpyAsync(t, dt, (size_t)n * 8, cudaMemcpyDeviceToHost, s));
+        FSB_CUDA(cudaStreamSynchronize(s));
+    }
+    *n_out = n;
+    return FSB_OK;
+}
+
+int32_t fsb_unique(fsb_ctx* ctx, const int64_t* q, const int64_t* t, const float* dd, int32_t n, int64_t* q_out,
+                   int64_t* t_out, int32_t* n_out) {
+    FSB_ARG(ctx && n_out, "null pointer");
+    FSB_ARG(n >= 0 && (n == 0 || (q && t && dd && q_out && t_out)), "bad arrays");
+    *n_out = 0;
+    if (n == 0) return FSB_OK;
+    FSB_TRY(use_device(ctx));
+    cudaStream_t s = ctx->stream;
+    FSB_TRY(ctx->s_i64.ensure((size_t)n * 8 * 4 + (size_t)n * 4 + 64));
+    int64_t* dq = ctx->s_i64.as<int64_t>();
+    int64_t* dt = dq + n;
+    int64_t* dqo = dt + n;
+    int64_t* dto = dqo + n;
+    float* ddd = reinterpret_cast<float*>(dto + n);
+    FSB_TRY(ctx->s_i32.ensure(64));
+    int* dn = ctx->s_i32.as<int>();
+    FSB_CUDA(cudaMemcpyAsync(dq, q, (size_t)n * 8, cudaMemcpyHostToDevice, s));
+    FSB_CUDA(cudaMemcpyAsync(dt, t, (size_t)n * 8, cudaMemcpyHostToDevice, s));
+    FSB_CUDA(cudaMemcpyAsync(ddd, dd, (size_t)n * 4, cudaMemcpyHostToDevice, s));
+    FSB_TRY(run_unique_general(ctx, dq, dt, ddd, n, dqo, dto, dn, s));
+    int m = 0;
+    FSB_CUDA(cudaMemcpyAsync(&m, dn, sizeof(int), cudaMemcpyDeviceToHost, s));
+    FSB_CUDA(cudaStreamSynchronize(s));
+    if (m) {
+        FSB_CUDA(cudaMemcpyAsync(q_out, dqo, (size_t)m * 8, cudaMemcpyDeviceToHost, s));
+        FSB_CUDA(cudaMemcpyAsync(t_out, dto, (size_t)m * 8, cudaMemcpyDeviceToHost, s));
+        FSB_CUDA(cudaStreamSynchronize(s));
+    }
+    *n_out = m;
+    return FSB_OK;
+}
+
+int32_t fsb_perspective(fsb_ctx* ctx, const double* xy, int32_t n, const double* hm9, double* out) {
+    FSB_ARG(ctx && hm9, "null pointer");
+    FSB_ARG(n >= 0 && (n == 0 || (xy && out)), "bad points");
+    if (n == 0) return FSB_OK;
+    FSB_TRY(use_device(ctx));
+    cudaStream_t s = ctx->stream;
+    FSB_TRY(ctx->s_f32a.ensure((size_t)n * 32 + 256));
+    double* dx = ctx->s_f32a.as<double>();
+    double* dout = dx + 2 * (size_t)n;
+    FSB_TRY(ctx->s_misc.ensure(128));
+    double* dh = ctx->s_misc.as<double>();
+    FSB_CUDA(cudaMemcpyAsync(dx, xy, (size_t)n * 16, cudaMemcpyHostToDevice, s));
+    FSB_CUDA(cudaMemcpyAsync(dh, hm9, 72, cudaMemcpyHostToDevice, s));
+    FSB_TRY(run_perspective(dx, n, dh, dout, s));
+    FSB_CUDA(cudaMemcpyAsync(out, dout, (size_t)n * 16, cudaMemcpyDeviceToHost, s));
+    FSB_CUDA(cudaStreamSynchronize(s));
+    return FSB_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,157 @@
+// Internal declarations shared by the CUDA translation units of libfsb200.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <cstdarg>
+#include <cstdio>
+#include <string>
+#include <vector>
+
+#include "../../include/fsb200.h"
+
+namespace fsb {
+
+// ---------------------------------------------------------------------------------- errors
+void set_error(const char* fmt, ...);
+
+#define FSB_CUDA(call)                                                                      \
+    do {                                                                                    \
+        cudaError_t e_ = (call);                                                            \
+        if (e_ != cudaSuccess) {                                                            \
+            ::fsb::set_error("%s failed: %s (%s:%d)", #call, cudaGetErrorString(e_),        \
+                             __FILE__, __LINE__);                                           \
+            return e_ == cudaErrorMemoryAllocation ? FSB_ERR_OOM : FSB_ERR_CUDA;           \
+        }                                                                                   \
+    } while (0)
+
+#define FSB_TRY(expr)                   \
+    do {                                \
+        int32_t s_ = (expr);            \
+        if (s_ != FSB_OK) return s_;    \
+    } while (0)
+
+#define FSB_ARG(cond, msg)                                  \
+    do {                                                    \
+        if (!(cond)) {                                      \
+            ::fsb::set_error("invalid argument: %s", msg);  \
+            return FSB_ERR_ARG;                             \
+        }                                                   \
+    } while (0)
+
+// ------------------------------------------------------------------------ SIFT constants
+// app/planesite/gsift.py:13-25, 224
+constexpr int N_LAYERS = 3;
+constexpr float SIGMA = 1.6f;
+constexpr int BORDER = 5;
+constexpr int MAX_INTERP = 5;
+constexpr int ORI_BINS = 36;
+constexpr float ORI_RADIUS = 4.5f;
+constexpr float ORI_SIG = 1.5f;
+constexpr int ORI_R_MAX = 16;
+constexpr int D_WIDTH = 4;
+constexpr int D_BINS = 8;
+constexpr int MAXO = 16;
+
+// Octave geometry of one image: octave o is R[o] x C[o]; DoG layers 0..4 of octave o start at
+// dog_off[o] in the DoG atlas, gradient layers 1..3 (magnitude and angle) at grad_off[o].
+struct Geometry {
+    int h, w, n_oct;
+    int R[MAXO], C[MAXO];
+    long long dog_off[MAXO + 1];
+    long long grad_off[MAXO + 1];
+};
+Geometry make_geometry(int h, int w);
+
+// A refined extremum (one per surviving candidate).
+struct Refined {
+    uint32_t f;     // flat DoG-atlas index of the originating extremum (sort tie-break)
+    int16_t o, l;   // octave, layer 1..3 (after refinement)
+    int32_t r, c;   // integer position after refinement
+    float x0, x1, x2;  // sub-pixel offset (column, row, layer)
+    float resp;     // |contrast| at the fitted position
+};
+
+// One orientation peak of a refined extremum.
+struct Oriented {
+    uint32_t ri;    // index into the Refined array
+    int32_t j;      // histogram bin of the peak (0..35)
+    float angle;    // degrees
+};
+
+// ------------------------------------------------------------------- device buffers
+struct DevBuf {
+    void* p = nullptr;
+    size_t bytes = 0;
+    int32_t ensure(size_t n);   // grows (never shrinks); contents are not preserved
+    void release();
+    template <class T> T* as() const { return reinterpret_cast<T*>(p); }
+};
+
+// Pyramid + detection workspace sized for one image geometry.
+struct Workspace {
+    Geometry g{};
+    DevBuf dog, mag, ang;        // atlases
+    DevBuf plane[3];             // gauss-layer scratch planes (octave-0 size)
+    DevBuf img;                  // uploaded uint8 image
+    DevBuf cand, refined, oriented;
+    DevBuf keys_a, keys_b, vals_a, vals_b, sort_tmp;
+    DevBuf counters;             // [0] candidates, [1] refined, [2] oriented
+    size_t cap_cand = 0, cap_ref = 0, cap_ori = 0;
+    // sorted, capped keypoints (structure of arrays)
+    DevBuf kx, ky, ksize, kangle, kresp, koct, klayer;
+    int n_kp = 0;
+    size_t bytes() const;
+    void release();
+};
+
+}  // namespace fsb
+
+struct fsb_ctx {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    std::vector<fsb::Workspace*> pool;   // idle workspaces
+    int live_states = 0;
+    // scratch for description and matching (grown on demand)
+    fsb::DevBuf s_u8a, s_u8b, s_f32a, s_f32b, s_i32, s_i64, s_u64, s_misc, s_misc2, s_host_stage;
+    fsb::DevBuf s_cub;   // CUB temporary storage (one primitive at a time)
+    void* pinned = nullptr;
+    size_t pinned_bytes = 0;
+};
+
+struct fsb_state {
+    fsb_ctx* ctx = nullptr;
+    fsb::Workspace* ws = nullptr;
+    uint32_t magic = 0;
+    bool exact = false;   // detect ran with FSB_SIFT_EXACT_BLUR; describe uses float64 sample math
+};
+
+namespace fsb {
+constexpr uint32_t STATE_MAGIC = 0x51f7b200u;
+
+// ---------------------------------------------------------------- pyramid.cu
+int32_t upload_taps();
+int32_t run_pyramid(Workspace& ws, const uint8_t* d_img, int img_stride, bool exact, cudaStream_t s);
+
+// ---------------------------------------------------------------- detect.cu
+int32_t run_detect(Workspace& ws, double contrast, double edge, int max_kp, cudaStream_t s);
+int32_t run_describe_mode(const Workspace& ws, int n, const float* d_x, const float* d_y, const float* d_size,
+                          const float* d_angle, const int32_t* d_oct, const int32_t* d_layer, float* d_desc,
+                          uint8_t* d_u8, bool exact, cudaStream_t s);
+int32_t run_describe(const Workspace& ws, int n, const float* d_x, const float* d_y, const float* d_size,
+                     const float* d_angle, const int32_t* d_oct, const int32_t* d_layer, float* d_desc,
+                     uint8_t* d_u8, cudaStream_t s);
+int32_t run_spread(const Workspace& ws, int nfeat, int32_t* d_sel, int* n_sel, fsb_ctx* ctx, cudaStream_t s);
+
+// ---------------------------------------------------------------- match.cu
+int32_t run_match_bf(fsb_ctx* ctx, const uint8_t* d_a, int na, const uint8_t* d_b, int nb, float ratio,
+                     int precision, int64_t* d_q, int64_t* d_t, int* d_n, cudaStream_t s);
+int32_t run_match_guided(fsb_ctx* ctx, const double* d_pred, const uint8_t* d_a, int na, const double* d_bxy,
+                         const uint8_t* d_b, int nb, double wb, double hb, double radius, int kc, float ratio,
+                         int64_t* d_q, int64_t* d_t, int* d_n, cudaStream_t s);
+int32_t run_perspective(const double* d_xy, int n, const double* hm9, double* d_out, cudaStream_t s);
+int32_t run_unique_general(fsb_ctx* ctx, const int64_t* d_q, const int64_t* d_t, const float* d_dd, int n,
+                           int64_t* d_qo, int64_t* d_to, int* d_n, cudaStream_t s);
+
+}  // namespace fsb

@@ -1,0 +1,550 @@
+// Descriptor matching on uint8 RootSIFT descriptors.
+//
+//   k_bf_fp32     exhaustive nearest / second-nearest squared distance, CUDA-core FP32 tiles
+//                 (the plain path of matching._ratio_match_bf, app/planesite/matching.py:86-100)
+//   k_bf_merge    merge of the per-split top-2, float32 ratio test
+//   k_guided      prior-guided candidates within a radius on a uniform grid, exact integer
+//                 distances (matching._guided, app/planesite/matching.py:113-152)
+//   k_unique      one match per target: atomicMin on (distance << 32 | query) keys
+//                 (matching._unique, app/planesite/matching.py:103-110), then target-ordered
+//                 compaction
+//
+// Exactness: descriptors are uint8 and every squared distance na + nb - 2 a.b is an integer below
+// 2^24, so FP32 FMA accumulation in any order, integer dp4a, and BF16 x BF16 -> FP32 tensor-core
+// products all give the same values as the reference's float32 BLAS. Results therefore depend only
+// on the values and the tie rules, which follow the reference.
+#include <cub/cub.cuh>
+
+#include "fsb_internal.cuh"
+
+namespace fsb {
+namespace {
+
+inline unsigned blocks(long long n, int t) { return (unsigned)((n + t - 1) / t); }
+
+// squared L2 norm of each uint8 row (exact integer)
+__global__ void k_norms(const uint8_t* __restrict__ d, int n, int32_t* __restrict__ out) {
+    const int row = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    const int lane = threadIdx.x & 31;
+    if (row >= n) return;
+    const uint32_t w = reinterpret_cast<const uint32_t*>(d + (size_t)row * 128)[lane];
+    int s = (int)__dp4a(w, w, 0u);
+    for (int sh = 16; sh; sh >>= 1) s += __shfl_xor_sync(0xffffffffu, s, sh);
+    if (lane == 0) out[row] = s;
+}
+
+// ------------------------------------------------------------------------- FP32 dense tiles
+constexpr int BM = 128, BN = 128, BK = 32, TM = 8, TN = 8, BF_THREADS = 256;
+
+struct Top2 {
+    float b1, b2;
+    int i1;
+};
+
+__device__ __forceinline__ void top2_push(Top2& t, float d, int j) {
+    if (d < t.b1) {
+        t.b2 = t.b1;
+        t.b1 = d;
+        t.i1 = j;
+    } else if (d < t.b2) {
+        t.b2 = d;
+    }
+}
+
+__device__ __forceinline__ Top2 top2_merge(Top2 a, Top2 b) {
+    Top2 r;
+    if (a.b1 < b.b1 || (a.b1 == b.b1 && a.i1 <= b.i1)) {
+        r.b1 = a.b1; r.i1 = a.i1; r.b2 = fminf(a.b2, b.b1);
+    } else {
+        r.b1 = b.b1; r.i1 = b.i1; r.b2 = fminf(b.b2, a.b1);
+    }
+    return r;
+}
+
+// grid: (row blocks, splits of B). Each CTA sweeps B rows [n0, n1) for 128 A rows and writes the
+// per-row top-2 of its split.
+__global__ void __launch_bounds__(BF_THREADS) k_bf_fp32(const uint8_t* __restrict__ A, int na,
+                                                        const uint8_t* __restrict__ B, int nb,
+                                                        const int32_t* __restrict__ nA, const int32_t* __restrict__ nB,
+                                                        int split_len, Top2* __restrict__ part) {
+    // operand tiles during the sweep; the same bytes hold the row merge afterwards
+    constexpr size_t kTileBytes = 2 * sizeof(float) * BK * (BM + 4);
+    constexpr size_t kRedBytes = sizeof(Top2) * 16 * BM;
+    __shared__ __align__(16) unsigned char smem[kTileBytes > kRedBytes ? kTileBytes : kRedBytes];
+    float (*As)[BM + 4] = reinterpret_cast<float (*)[BM + 4]>(smem);
+    float (*Bs)[BN + 4] = reinterpret_cast<float (*)[BN + 4]>(smem + sizeof(float) * BK * (BM + 4));
+    const int tid = threadIdx.x;
+    const int tx = tid & 15, ty = tid >> 4;
+    const int m0 = blockIdx.x * BM;
+    const int n_begin = blockIdx.y * split_len;
+    const int n_end = min(nb, n_begin + split_len);
+    Top2 best[TM];
+#pragma unroll
+    for (int i = 0; i < TM; ++i) best[i] = Top2{INFINITY, INFINITY, -1};
+    float rn[TM];
+#pragma unroll
+    for (int i = 0; i < TM; ++i) {
+        const int r = m0 + ty + 16 * i;
+        rn[i] = r < na ? (float)nA[r] : 0.f;
+    }
+    for (int n0 = n_begin; n0 < n_end; n0 += BN) {
+        float acc[TM][TN];
+#pragma unroll
+        for (int i = 0; i < TM; ++i)
+#pragma unroll
+            for (int j = 0; j < TN; ++j) acc[i][j] = 0.f;
+        for (int k0 = 0; k0 < 128; k0 += BK) {
+            // stage 128 x 32 bytes of A and B as float, transposed (k-major)
+            for (int e = tid; e < BM * (BK / 4); e += BF_THREADS) {
+                const int r = e / (BK / 4), q = e - r * (BK / 4);
+                uint32_t wa = 0, wb = 0;
+                if (m0 + r < na) wa = reinterpret_cast<const uint32_t*>(A + (size_t)(m0 + r) * 128 + k0)[q];
+                if (n0 + r < n_end) wb = reinterpret_cast<const uint32_t*>(B + (size_t)(n0 + r) * 128 + k0)[q];
+#pragma unroll
+                for (int b = 0; b < 4; ++b) {
+                    As[q * 4 + b][r] = (float)((wa >> (8 * b)) & 255u);
+                    Bs[q * 4 + b][r] = (float)((wb >> (8 * b)) & 255u);
+                }
+            }
+            __syncthreads();
+#pragma unroll 4
+            for (int kk = 0; kk < BK; ++kk) {
+                float a[TM], b[TN];
+#pragma unroll
+                for (int i = 0; i < TM; ++i) a[i] = As[kk][ty + 16 * i];
+#pragma unroll
+                for (int j = 0; j < TN; ++j) b[j] = Bs[kk][tx + 16 * j];
+#pragma unroll
+                for (int i = 0; i < TM; ++i)
+#pragma unroll
+                    for (int j = 0; j < TN; ++j) acc[i][j] = fmaf(a[i], b[j], acc[i][j]);
+            }
+            __syncthreads();
+        }
+#pragma unroll
+        for (int j = 0; j < TN; ++j) {
+            const int c = n0 + tx + 16 * j;
+            if (c >= n_end) continue;
+            const float cn = (float)nB[c];
+#pragma unroll
+            for (int i = 0; i < TM; ++i) top2_push(best[i], (rn[i] + cn) - 2.f * acc[i][j], c);
+        }
+    }
+    // merge the 16 column groups of each row through shared memory
+    Top2 (*red)[BM] = reinterpret_cast<Top2 (*)[BM]>(smem);
+#pragma unroll
+    for (int i = 0; i < TM; ++i) red[tx][ty + 16 * i] = best[i];
+    __syncthreads();
+    if (tid < BM) {
+        Top2 t = red[0][tid];
+        for (int g = 1; g < 16; ++g) t = top2_merge(t, red[g][tid]);
+        const int r = m0 + tid;
+        if (r < na) part[(size_t)blockIdx.y * na + r] = t;
+    }
+}
+
+// merge the splits, ratio test (float32, app/planesite/matching.py:96-99)
+__global__ void k_bf_merge(const Top2* __restrict__ part, int na, int splits, float ratio,
+                           int32_t* __restrict__ t_row, uint32_t* __restrict__ d_row) {
+    const int r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= na) return;
+    Top2 t = part[r];
+    for (int s = 1; s < splits; ++s) t = top2_merge(t, part[(size_t)s * na + r]);
+    const float b1 = fmaxf(t.b1, 0.f), b2 = fmaxf(t.b2, 0.f);
+    const bool ok = __fsqrt_rn(b1) < __fmul_rn(ratio, __fsqrt_rn(b2));
+    t_row[r] = ok ? t.i1 : -1;
+    d_row[r] = (uint32_t)b1;
+}
+
+// ------------------------------------------------------------------------------ one-to-one
+__global__ void k_fill_u64(unsigned long long* p, int n, unsigned long long v) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) p[i] = v;
+}
+
+__global__ void k_unique_keys(const int32_t* __restrict__ t_row, const uint32_t* __restrict__ d_row, int na,
+                              unsigned long long* __restrict__ key) {
+    const int r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= na) return;
+    const int t = t_row[r];
+    if (t >= 0) atomicMin(key + t, ((unsigned long long)d_row[r] << 32) | (unsigned)r);
+}
+
+__global__ void k_unique_flags(const unsigned long long* __restrict__ key, int nb, uint8_t* __restrict__ flag,
+                               int32_t* __restrict__ iota) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= nb) return;
+    flag[t] = key[t] != ~0ull;
+    iota[t] = t;
+}
+
+__global__ void k_unique_emit(const unsigned long long* __restrict__ key, const int32_t* __restrict__ tsel,
+                              const int* __restrict__ n, int64_t* __restrict__ q, int64_t* __restrict__ t) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= *n) return;
+    const int tt = tsel[i];
+    q[i] = (int64_t)(key[tt] & 0xffffffffull);
+    t[i] = tt;
+}
+
+// ------------------------------------------------------------------------------ guided
+struct GridSpec {
+    double x0, y0, cs;   // origin and cell size
+    int gw, gh;
+};
+
+__device__ __forceinline__ int cell_of(double v, double o, double cs, int n) {
+    const double f = floor((v - o) / cs);
+    return f < 0.0 ? 0 : (f >= (double)(n - 1) ? n - 1 : (int)f);
+}
+
+__global__ void k_grid_count(const double* __restrict__ bxy, int nb, GridSpec gs, int32_t* __restrict__ cell,
+                             int32_t* __restrict__ count) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nb) return;
+    const int cx = cell_of(bxy[2 * i], gs.x0, gs.cs, gs.gw), cy = cell_of(bxy[2 * i + 1], gs.y0, gs.cs, gs.gh);
+    const int c = cy * gs.gw + cx;
+    cell[i] = c;
+    atomicAdd(count + c, 1);
+}
+
+__global__ void k_grid_fill(const int32_t* __restrict__ cell, int nb, const int32_t* __restrict__ start,
+                            int32_t* __restrict__ cursor, int32_t* __restrict__ items) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nb) return;
+    const int c = cell[i];
+    items[start[c] + atomicAdd(cursor + c, 1)] = i;
+}
+
+constexpr int G_WARPS = 4, G_CAND = 512;
+
+__device__ __forceinline__ int exact_d2(const uint32_t* __restrict__ qa, const uint8_t* __restrict__ B, int j,
+                                        int qn, const int32_t* __restrict__ nB) {
+    const uint4* pb = reinterpret_cast<const uint4*>(B + (size_t)j * 128);
+    unsigned dot = 0;
+#pragma unroll
+    for (int v = 0; v < 8; ++v) {
+        const uint4 w = __ldg(pb + v);
+        dot = __dp4a(qa[4 * v + 0], w.x, dot);
+        dot = __dp4a(qa[4 * v + 1], w.y, dot);
+        dot = __dp4a(qa[4 * v + 2], w.z, dot);
+        dot = __dp4a(qa[4 * v + 3], w.w, dot);
+    }
+    return (qn + nB[j]) - 2 * (int)dot;
+}
+
+__global__ void __launch_bounds__(G_WARPS * 32) k_guided(const double* __restrict__ pred, const uint8_t* __restrict__ A,
+                                                         int na, const double* __restrict__ bxy,
+                                                         const uint8_t* __restrict__ B, int nb,
+                                                         const int32_t* __restrict__ nA, const int32_t* __restrict__ nB,
+                                                         GridSpec gs, const int32_t* __restrict__ start,
+                                                         const int32_t* __restrict__ items, double wb, double hb,
+                                                         double radius, int kc, float ratio,
+                                                         int32_t* __restrict__ t_row, uint32_t* __restrict__ d_row,
+                                                         int* __restrict__ overflow) {
+    __shared__ uint32_t s_q[G_WARPS][32];
+    __shared__ double s_cd[G_WARPS][G_CAND];
+    __shared__ int32_t s_ci[G_WARPS][G_CAND];
+    const int wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int q = blockIdx.x * G_WARPS + wid;
+    if (q >= na) return;
+    const double px = pred[2 * q], py = pred[2 * q + 1];
+    int32_t res_t = -1;
+    uint32_t res_d = 0;
+    const bool inside = px > -radius && px < wb + radius && py > -radius && py < hb + radius;
+    if (inside) {
+        s_q[wid][lane] = reinterpret_cast<const uint32_t*>(A + (size_t)q * 128)[lane];
+        __syncwarp();
+        uint32_t qa[32];
+#pragma unroll
+        for (int v = 0; v < 32; ++v) qa[v] = s_q[wid][v];
+        const int qn = nA[q];
+        const double r2 = radius * radius;
+        const int cx = cell_of(px, gs.x0, gs.cs, gs.gw), cy = cell_of(py, gs.y0, gs.cs, gs.gh);
+        Top2 best{INFINITY, INFINITY, -1};
+        if (kc <= 0) {
+            // every B keypoint strictly within the radius is a candidate
+            for (int yy = max(cy - 1, 0); yy <= min(cy + 1, gs.gh - 1); ++yy)
+                for (int xx = max(cx - 1, 0); xx <= min(cx + 1, gs.gw - 1); ++xx) {
+                    const int c = yy * gs.gw + xx;
+                    const int s0 = start[c], s1 = start[c + 1];
+                    for (int p = s0 + lane; p < s1; p += 32) {
+                        const int j = items[p];
+                        const double dx = __dsub_rn(bxy[2 * j], px), dy = __dsub_rn(bxy[2 * j + 1], py);
+                        const double d2 = __dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy));
+                        if (d2 < r2) top2_push(best, (float)exact_d2(qa, B, j, qn, nB), j);
+                    }
+                }
+        } else {
+            // collect candidates (spatial distance, index) in shared memory
+            int cnt = 0;
+            for (int yy = max(cy - 1, 0); yy <= min(cy + 1, gs.gh - 1); ++yy)
+                for (int xx = max(cx - 1, 0); xx <= min(cx + 1, gs.gw - 1); ++xx) {
+                    const int c = yy * gs.gw + xx;
+                    const int s0 = start[c], s1 = start[c + 1];
+                    for (int p0 = s0; p0 < s1; p0 += 32) {
+                        const int p = p0 + lane;
+                        bool hit = false;
+                        double d2 = 0.0;
+                        int j = 0;
+                        if (p < s1) {
+                            j = items[p];
+                            const double dx = __dsub_rn(bxy[2 * j], px), dy = __dsub_rn(bxy[2 * j + 1], py);
+                            d2 = __dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy));
+                            hit = d2 < r2;
+                        }
+                        const unsigned m = __ballot_sync(0xffffffffu, hit);
+                        if (hit) {
+                            const int pos = cnt + __popc(m & ((1u << lane) - 1u));
+                            if (pos < G_CAND) {
+                                s_cd[wid][pos] = d2;
+                                s_ci[wid][pos] = j;
+                            }
+                        }
+                        cnt += __popc(m);
+                    }
+                }
+            __syncwarp();
+            if (cnt > G_CAND) {
+                if (lane == 0) atomicExch(overflow, 1);
+                cnt = G_CAND;
+            }
+            // keep the kc nearest (ties: smaller B index)
+            for (int e = lane; e < cnt; e += 32) {
+                const double de = s_cd[wid][e];
+                const int ie = s_ci[wid][e];
+                int rank = 0;
+                if (cnt > kc)
+                    for (int f = 0; f < cnt; ++f) {
+                        const double df = s_cd[wid][f];
+                        rank += (df < de || (df == de && s_ci[wid][f] < ie)) ? 1 : 0;
+                    }
+                if (rank < kc) top2_push(best, (float)exact_d2(qa, B, ie, qn, nB), ie);
+            }
+        }
+        // warp merge of the per-lane top-2
+#pragma unroll
+        for (int sh = 16; sh; sh >>= 1) {
+            Top2 o;
+            o.b1 = __shfl_xor_sync(0xffffffffu, best.b1, sh);
+            o.b2 = __shfl_xor_sync(0xffffffffu, best.b2, sh);
+            o.i1 = __shfl_xor_sync(0xffffffffu, best.i1, sh);
+            best = top2_merge(best, o);
+        }
+        if (best.i1 >= 0) {
+            // single candidate: b2 = inf passes (app/planesite/matching.py:142-146)
+            const bool ok = __fsqrt_rn(best.b1) < __fmul_rn(ratio, __fsqrt_rn(best.b2));
+            if (ok) {
+                res_t = best.i1;
+                res_d = (uint32_t)best.b1;
+            }
+        }
+    }
+    if (lane == 0) {
+        t_row[q] = res_t;
+        d_row[q] = res_d;
+    }
+}
+
+__global__ void k_perspective(const double* __restrict__ xy, int n, const double* __restrict__ hm,
+                              double* __restrict__ out) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const double x = xy[2 * i], y = xy[2 * i + 1];
+    double w = __dadd_rn(__dadd_rn(__dmul_rn(hm[6], x), __dmul_rn(hm[7], y)), hm[8]);
+    double u = 0.0, v = 0.0;
+    if (fabs(w) > 1.1920928955078125e-07) {
+        w = 1.0 / w;
+        u = __dmul_rn(__dadd_rn(__dadd_rn(__dmul_rn(hm[0], x), __dmul_rn(hm[1], y)), hm[2]), w);
+        v = __dmul_rn(__dadd_rn(__dadd_rn(__dmul_rn(hm[3], x), __dmul_rn(hm[4], y)), hm[5]), w);
+    }
+    out[2 * i] = u;
+    out[2 * i + 1] = v;
+}
+
+// one-to-one filter + compaction ordered by target: q[i], t[i], *d_n
+int32_t run_unique(fsb_ctx* ctx, const int32_t* t_row, const uint32_t* d_row, int na, int nb, int64_t* d_q,
+                   int64_t* d_t, int* d_n, cudaStream_t s) {
+    FSB_TRY(ctx->s_u64.ensure((size_t)nb * 8 + 64));
+    FSB_TRY(ctx->s_misc2.ensure((size_t)nb * 9 + 1024));
+    unsigned long long* key = ctx->s_u64.as<unsigned long long>();
+    uint8_t* flag = ctx->s_misc2.as<uint8_t>();
+    int32_t* iota = reinterpret_cast<int32_t*>(flag + ((nb + 255) / 256) * 256);
+    int32_t* tsel = iota + nb;
+    k_fill_u64<<<blocks(nb, 256), 256, 0, s>>>(key, nb, ~0ull);
+    k_unique_keys<<<blocks(na, 256), 256, 0, s>>>(t_row, d_row, na, key);
+    k_unique_flags<<<blocks(nb, 256), 256, 0, s>>>(key, nb, flag, iota);
+    size_t tb = 0;
+    cub::DeviceSelect::Flagged(nullptr, tb, iota, flag, tsel, d_n, nb, s);
+    FSB_TRY(ctx->s_cub.ensure(tb + 16));
+    FSB_CUDA(cub::DeviceSelect::Flagged(ctx->s_cub.p, tb, iota, flag, tsel, d_n, nb, s));
+    k_unique_emit<<<blocks(nb, 256), 256, 0, s>>>(key, tsel, d_n, d_q, d_t);
+    FSB_CUDA(cudaGetLastError());
+    return FSB_OK;
+}
+
+__device__ __forceinline__ uint32_t orderable(float f) {
+    const uint32_t b = __float_as_uint(f);
+    return (b & 0x80000000u) ? ~b : (b | 0x80000000u);
+}
+
+__global__ void k_uq_keys1(const float* __restrict__ dd, int n, uint32_t* __restrict__ key, uint32_t* __restrict__ val) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    key[i] = orderable(dd[i]);
+    val[i] = (uint32_t)i;
+}
+
+__global__ void k_uq_keys2(const int64_t* __restrict__ t, const uint32_t* __restrict__ perm, int n,
+                           unsigned long long* __restrict__ key) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    key[i] = (unsigned long long)t[perm[i]] ^ 0x8000000000000000ull;
+}
+
+__global__ void k_uq_first(const unsigned long long* __restrict__ key, int n, uint8_t* __restrict__ flag) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    flag[i] = (i == 0 || key[i] != key[i - 1]) ? 1 : 0;
+}
+
+__global__ void k_uq_emit(const uint32_t* __restrict__ pos, const int* __restrict__ n, const int64_t* __restrict__ q,
+                          const int64_t* __restrict__ t, int64_t* __restrict__ qo, int64_t* __restrict__ to) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= *n) return;
+    qo[i] = q[pos[i]];
+    to[i] = t[pos[i]];
+}
+
+}  // namespace
+
+// General one-to-one filter (matching._unique) for arbitrary int64 targets and float distances:
+// stable sorts by distance then by target give (t, dd, position) order; the first of each target
+// run is kept.
+int32_t run_unique_general(fsb_ctx* ctx, const int64_t* d_q, const int64_t* d_t, const float* d_dd, int n,
+                           int64_t* d_qo, int64_t* d_to, int* d_n, cudaStream_t s) {
+    const size_t N = (size_t)n;
+    FSB_TRY(ctx->s_misc.ensure(N * (4 * 4 + 8 * 2 + 1 + 4) + 256));
+    uint32_t* k1 = ctx->s_misc.as<uint32_t>();
+    uint32_t* k1o = k1 + N;
+    uint32_t* v1 = k1o + N;
+    uint32_t* v1o = v1 + N;
+    unsigned long long* k2 = reinterpret_cast<unsigned long long*>(v1o + N);
+    unsigned long long* k2o = k2 + N;
+    uint32_t* v2o = reinterpret_cast<uint32_t*>(k2o + N);
+    uint8_t* flag = reinterpret_cast<uint8_t*>(v2o + N);
+    uint32_t* sel = v1;   // reused after the second sort
+    size_t t1 = 0, t2 = 0, t3 = 0;
+    cub::DeviceRadixSort::SortPairs(nullptr, t1, k1, k1o, v1, v1o, n, 0, 32, s);
+    cub::DeviceRadixSort::SortPairs(nullptr, t2, k2, k2o, v1o, v2o, n, 0, 64, s);
+    cub::DeviceSelect::Flagged(nullptr, t3, v2o, flag, sel, d_n, n, s);
+    size_t tmax = t1 > t2 ? t1 : t2;
+    tmax = tmax > t3 ? tmax : t3;
+    FSB_TRY(ctx->s_cub.ensure(tmax + 16));
+    k_uq_keys1<<<blocks(n, 256), 256, 0, s>>>(d_dd, n, k1, v1);
+    size_t tb = tmax;
+    FSB_CUDA(cub::DeviceRadixSort::SortPairs(ctx->s_cub.p, tb, k1, k1o, v1, v1o, n, 0, 32, s));
+    k_uq_keys2<<<blocks(n, 256), 256, 0, s>>>(d_t, v1o, n, k2);
+    tb = tmax;
+    FSB_CUDA(cub::DeviceRadixSort::SortPairs(ctx->s_cub.p, tb, k2, k2o, v1o, v2o, n, 0, 64, s));
+    k_uq_first<<<blocks(n, 256), 256, 0, s>>>(k2o, n, flag);
+    tb = tmax;
+    FSB_CUDA(cub::DeviceSelect::Flagged(ctx->s_cub.p, tb, v2o, flag, sel, d_n, n, s));
+    k_uq_emit<<<blocks(n, 256), 256, 0, s>>>(sel, d_n, d_q, d_t, d_qo, d_to);
+    FSB_CUDA(cudaGetLastError());
+    return FSB_OK;
+}
+
+int32_t run_perspective(const double* d_xy, int n, const double* d_hm9, double* d_out, cudaStream_t s) {
+    if (n <= 0) return FSB_OK;
+    k_perspective<<<blocks(n, 256), 256, 0, s>>>(d_xy, n, d_hm9, d_out);
+    FSB_CUDA(cudaGetLastError());
+    return FSB_OK;
+}
+
+int32_t run_match_bf(fsb_ctx* ctx, const uint8_t* d_a, int na, const uint8_t* d_b, int nb, float ratio,
+                     int precision, int64_t* d_q, int64_t* d_t, int* d_n, cudaStream_t s) {
+    if (na < 2 || nb < 2) {
+        FSB_CUDA(cudaMemsetAsync(d_n, 0, sizeof(int), s));
+        return FSB_OK;
+    }
+    if (precision != FSB_PREC_FP32) {
+        set_error("precision %d is not built into this library", precision);
+        return FSB_ERR_UNSUPPORTED;
+    }
+    const int row_blocks = (na + BM - 1) / BM;
+    int splits = 1;
+    while (row_blocks * splits < 2 * 148 && (nb + splits * 2 - 1) / (splits * 2) >= BN) splits *= 2;
+    int split_len = (nb + splits - 1) / splits;
+    split_len = ((split_len + BN - 1) / BN) * BN;
+    splits = (nb + split_len - 1) / split_len;
+    FSB_TRY(ctx->s_i32.ensure((size_t)(na + nb) * 4 + (size_t)na * 8 + 64));
+    int32_t* nA = ctx->s_i32.as<int32_t>();
+    int32_t* nB = nA + na;
+    int32_t* t_row = nB + nb;
+    uint32_t* d_row = reinterpret_cast<uint32_t*>(t_row + na);
+    FSB_TRY(ctx->s_misc.ensure((size_t)splits * na * sizeof(Top2) + 64));
+    Top2* part = ctx->s_misc.as<Top2>();
+    k_norms<<<blocks(na, 8), 256, 0, s>>>(d_a, na, nA);
+    k_norms<<<blocks(nb, 8), 256, 0, s>>>(d_b, nb, nB);
+    k_bf_fp32<<<dim3(row_blocks, splits), BF_THREADS, 0, s>>>(d_a, na, d_b, nb, nA, nB, split_len, part);
+    k_bf_merge<<<blocks(na, 256), 256, 0, s>>>(part, na, splits, ratio, t_row, d_row);
+    FSB_CUDA(cudaGetLastError());
+    return run_unique(ctx, t_row, d_row, na, nb, d_q, d_t, d_n, s);
+}
+
+int32_t run_match_guided(fsb_ctx* ctx, const double* d_pred, const uint8_t* d_a, int na, const double* d_bxy,
+                         const uint8_t* d_b, int nb, double wb, double hb, double radius, int kc, float ratio,
+                         int64_t* d_q, int64_t* d_t, int* d_n, cudaStream_t s) {
+    if (na < 1 || nb < 1 || !(radius > 0.0)) {
+        FSB_CUDA(cudaMemsetAsync(d_n, 0, sizeof(int), s));
+        return FSB_OK;
+    }
+    GridSpec gs;
+    gs.x0 = 0.0;
+    gs.y0 = 0.0;
+    gs.cs = radius;
+    double gwd = (wb > 0 ? wb : 1.0) / radius + 1.0, ghd = (hb > 0 ? hb : 1.0) / radius + 1.0;
+    while (gwd * ghd > 4.0e6) {
+        gs.cs *= 2.0;
+        gwd = (wb > 0 ? wb : 1.0) / gs.cs + 1.0;
+        ghd = (hb > 0 ? hb : 1.0) / gs.cs + 1.0;
+    }
+    gs.gw = (int)gwd;
+    gs.gh = (int)ghd;
+    const int ncell = gs.gw * gs.gh;
+    FSB_TRY(ctx->s_i32.ensure((size_t)(na + nb) * 4 + (size_t)na * 8 + (size_t)nb * 8 + (size_t)ncell * 12 + 256));
+    int32_t* nA = ctx->s_i32.as<int32_t>();
+    int32_t* nB = nA + na;
+    int32_t* t_row = nB + nb;
+    uint32_t* d_row = reinterpret_cast<uint32_t*>(t_row + na);
+    int32_t* cell = reinterpret_cast<int32_t*>(d_row + na);
+    int32_t* items = cell + nb;
+    int32_t* count = items + nb;      // ncell + 1
+    int32_t* start = count + ncell + 1;
+    int32_t* cursor = start + ncell + 1;
+    int* overflow = cursor + ncell;
+    FSB_CUDA(cudaMemsetAsync(count, 0, (size_t)(ncell + 1) * 4, s));
+    FSB_CUDA(cudaMemsetAsync(cursor, 0, (size_t)ncell * 4 + 4, s));
+    k_norms<<<blocks(na, 8), 256, 0, s>>>(d_a, na, nA);
+    k_norms<<<blocks(nb, 8), 256, 0, s>>>(d_b, nb, nB);
+    k_grid_count<<<blocks(nb, 256), 256, 0, s>>>(d_bxy, nb, gs, cell, count);
+    size_t tb = 0;
+    cub::DeviceScan::ExclusiveSum(nullptr, tb, count, start, ncell + 1, s);
+    FSB_TRY(ctx->s_cub.ensure(tb + 16));
+    FSB_CUDA(cub::DeviceScan::ExclusiveSum(ctx->s_cub.p, tb, count, start, ncell + 1, s));
+    k_grid_fill<<<blocks(nb, 256), 256, 0, s>>>(cell, nb, start, cursor, items);
+    k_guided<<<blocks(na, G_WARPS), G_WARPS * 32, 0, s>>>(d_pred, d_a, na, d_bxy, d_b, nb, nA, nB, gs, start, items,
+                                                          wb, hb, radius, kc, ratio, t_row, d_row, overflow);
+    FSB_CUDA(cudaGetLastError());
+    int h_over = 0;
+    FSB_CUDA(cudaMemcpyAsync(&h_over, overflow, sizeof(int), cudaMemcpyDeviceToHost, s));
+    FSB_CUDA(cudaStreamSynchronize(s));
+    if (h_over) {
+        set_error("more than %d B keypoints within the radius of one prediction (kc mode)", G_CAND);
+        return FSB_ERR_OVERFLOW;
+    }
+    return run_unique(ctx, t_row, d_row, na, nb, d_q, d_t, d_n, s);
+}
+
+}  // namespace fsb

@@ -1,0 +1,248 @@
+// Gaussian / DoG pyramid with fused DoG, gradient and downsample epilogues.
+//
+// Reference: app/planesite/gsift.py:52-72 (taps), 85-102 (blur, 2x upsample), 158-179 (pyramid),
+// 227-267 (DoG atlas, gradient magnitude / angle of gauss layers 1..3).
+//
+// Layout in HBM (per image):
+//   DoG atlas   float32 [octave][layer 0..4][R][C], octave o at Geometry::dog_off[o]
+//   MAG / ANG   float32 [octave][layer 1..3][R][C], octave o at Geometry::grad_off[o]
+//   planes      three octave-0-sized float32 scratch planes for gauss layers in flight
+//
+// One launch per (octave, layer): a 64x32 output tile is staged through shared memory with its
+// mirrored halo, blurred vertically then horizontally (the reference's axis order, with the
+// intermediate rounded to float32), and the epilogue writes L_i, the DoG L_i - L_{i-1}, the
+// gradient of L_{i-1} (layers 1..3) and the [::2, ::2] downsample of L_3 (next octave's base)
+// from the tile already in shared memory, so none of those needs a separate pass over HBM.
+#include <cmath>
+
+#include "fsb_internal.cuh"
+
+namespace fsb {
+
+// Normalised Gaussian taps of gsift._gauss_kernel for the base sigma sqrt(1.6^2 - 1) and the five
+// layer increments (float32 values, written as hex literals so they are exact).
+// Tap set 0: base (11 taps); 1..5: layers 1..5 (11, 13, 17, 21, 27 taps).
+static const int kTapCount[6] = {11, 11, 13, 17, 21, 27};
+static const float kTaps[6][27] = {
+    {0x1.bbb27cp-14f, 0x1.f04b54p-10f, 0x1.2469f0p-6f, 0x1.6b036ep-4f, 0x1.dac530p-3f, 0x1.4713cep-2f,
+     0x1.dac530p-3f, 0x1.6b036ep-4f, 0x1.2469f0p-6f, 0x1.f04b54p-10f, 0x1.bbb27cp-14f},
+    {0x1.4edfacp-14f, 0x1.a1407ap-10f, 0x1.0b5ddep-6f, 0x1.606d0ep-4f, 0x1.ddcdfcp-3f, 0x1.4d2364p-2f,
+     0x1.ddcdfcp-3f, 0x1.606d0ep-4f, 0x1.0b5ddep-6f, 0x1.a1407ap-10f, 0x1.4edfacp-14f},
+    {0x1.1f90cap-13f, 0x1.680080p-10f, 0x1.287054p-7f, 0x1.411cd4p-5f, 0x1.c995cap-4f, 0x1.ace486p-3f,
+     0x1.086a76p-2f, 0x1.ace486p-3f, 0x1.c995cap-4f, 0x1.411cd4p-5f, 0x1.287054p-7f, 0x1.680080p-10f,
+     0x1.1f90cap-13f},
+    {0x1.719152p-15f, 0x1.4e5a92p-12f, 0x1.d0a8dcp-10f, 0x1.eff6b8p-8f, 0x1.9695c0p-6f, 0x1.ffffbap-5f,
+     0x1.ef3104p-4f, 0x1.6fd80cp-3f, 0x1.a3bafcp-3f, 0x1.6fd80cp-3f, 0x1.ef3104p-4f, 0x1.ffffbap-5f,
+     0x1.9695c0p-6f, 0x1.eff6b8p-8f, 0x1.d0a8dcp-10f, 0x1.4e5a92p-12f, 0x1.719152p-15f},
+    {0x1.4ee0b6p-15f, 0x1.9634a6p-13f, 0x1.a141c6p-11f, 0x1.6af5d4p-9f, 0x1.0b5eb2p-7f, 0x1.4d9348p-6f,
+     0x1.606e26p-5f, 0x1.3b51b8p-4f, 0x1.ddcf78p-4f, 0x1.3291c0p-3f, 0x1.4d246cp-3f, 0x1.3291c0p-3f,
+     0x1.ddcf78p-4f, 0x1.3b51b8p-4f, 0x1.606e26p-5f, 0x1.4d9348p-6f, 0x1.0b5eb2p-7f, 0x1.6af5d4p-9f,
+     0x1.a141c6p-11f, 0x1.9634a6p-13f, 0x1.4ee0b6p-15f},
+    {0x1.36a04cp-16f, 0x1.1f903ep-14f, 0x1.df7c20p-13f, 0x1.67ffd2p-11f, 0x1.e6d384p-10f, 0x1.286fc4p-8f,
+     0x1.451d18p-7f, 0x1.411c3ap-6f, 0x1.1d9ebap-5f, 0x1.c994eep-5f, 0x1.4a176ap-4f, 0x1.ace3b6p-4f,
+     0x1.f5d90ep-4f, 0x1.0869f6p-3f, 0x1.f5d90ep-4f, 0x1.ace3b6p-4f, 0x1.4a176ap-4f, 0x1.c994eep-5f,
+     0x1.1d9ebap-5f, 0x1.411c3ap-6f, 0x1.451d18p-7f, 0x1.286fc4p-8f, 0x1.e6d384p-10f, 0x1.67ffd2p-11f,
+     0x1.df7c20p-13f, 0x1.1f903ep-14f, 0x1.36a04cp-16f},
+};
+
+__constant__ float c_taps[6][28];
+__constant__ double c_taps_d[6][28];
+
+int32_t upload_taps() {
+    float f[6][28] = {};
+    double d[6][28] = {};
+    for (int s = 0; s < 6; ++s)
+        for (int j = 0; j < kTapCount[s]; ++j) {
+            f[s][j] = kTaps[s][j];
+            d[s][j] = (double)kTaps[s][j];
+        }
+    FSB_CUDA(cudaMemcpyToSymbol(c_taps, f, sizeof(f)));
+    FSB_CUDA(cudaMemcpyToSymbol(c_taps_d, d, sizeof(d)));
+    return FSB_OK;
+}
+
+Geometry make_geometry(int h, int w) {
+    Geometry g{};
+    g.h = h;
+    g.w = w;
+    int mn = h < w ? h : w;
+    int budget = (int)std::nearbyint(std::log2((double)mn) - 2.0) + 1;   // gsift.py:167
+    if (budget < 1) budget = 1;
+    int R = 2 * h, C = 2 * w;
+    long long dog = 0, grad = 0;
+    g.n_oct = 0;
+    for (int o = 0; o < budget && o < MAXO; ++o) {
+        if ((R < C ? R : C) < 2 * BORDER + 4) break;                         // gsift.py:171
+        g.R[o] = R;
+        g.C[o] = C;
+        g.dog_off[o] = dog;
+        g.grad_off[o] = grad;
+        dog += 5LL * R * C;
+        grad += 3LL * R * C;
+        g.n_oct = o + 1;
+        R = (R + 1) / 2;   // layers[3][::2, ::2]
+        C = (C + 1) / 2;
+    }
+    g.dog_off[g.n_oct] = dog;
+    g.grad_off[g.n_oct] = grad;
+    return g;
+}
+
+namespace {
+
+constexpr int TX = 64, TY = 32, NT = 256;
+// degrees per radian as NumPy's float32 rad2deg computes it: float(180) / float(pi)
+constexpr float kRad2Deg = 0x1.ca5dc0p+5f;
+
+__device__ __forceinline__ int mirror(int p, int n) {
+    if (n == 1) return 0;
+    while (p < 0 || p >= n) p = p < 0 ? -p : 2 * n - 2 - p;
+    return p;
+}
+
+struct BlurArgs {
+    const float* src;          // previous gauss layer (layer launches)
+    const uint8_t* img;        // uint8 input (base launch)
+    int img_stride, ih, iw;
+    int rows, cols;
+    float* dst;                // this layer, or null
+    float* dog;                // DoG plane (this - previous), or null
+    float* mag;                // gradient magnitude of the previous layer, or null
+    float* ang;                // gradient angle of the previous layer (degrees), or null
+    float* down;               // previous layer [::2, ::2], or null
+    int down_cols;
+};
+
+// Bilinear 2x upsample sample of the uint8 image at (Y, X) of the 2h x 2w grid, float32 with the
+// reference's rounding: a = u8 * float(1/255); t = 0.75 a[iy] + 0.25 a[ny] (rows first), then the
+// same along columns (gsift.py:90-102, 160).
+__device__ __forceinline__ float up2_sample(const BlurArgs& a, int Y, int X) {
+    const float s = (float)(1.0 / 255.0);
+    const int iy = Y >> 1, ix = X >> 1;
+    const int ny = (Y & 1) ? min(iy + 1, a.ih - 1) : max(iy - 1, 0);
+    const int nx = (X & 1) ? min(ix + 1, a.iw - 1) : max(ix - 1, 0);
+    const uint8_t* r0 = a.img + (size_t)iy * a.img_stride;
+    const uint8_t* r1 = a.img + (size_t)ny * a.img_stride;
+    const float p00 = __fmul_rn((float)r0[ix], s), p10 = __fmul_rn((float)r1[ix], s);
+    const float p01 = __fmul_rn((float)r0[nx], s), p11 = __fmul_rn((float)r1[nx], s);
+    const float vc = __fadd_rn(__fmul_rn(0.75f, p00), __fmul_rn(0.25f, p10));
+    const float vn = __fadd_rn(__fmul_rn(0.75f, p01), __fmul_rn(0.25f, p11));
+    return __fadd_rn(__fmul_rn(0.75f, vc), __fmul_rn(0.25f, vn));
+}
+
+// Correlation of 2*RAD+1 samples p[0], p[stride], ... with tap set TS.
+// EXACT: float64, centre term first, then symmetric pairs from the outside in, each product and
+// sum rounded separately, one final rounding to float32 (scipy.ndimage.correlate1d's order).
+template <int TS, int RAD, bool EXACT>
+__device__ __forceinline__ float conv(const float* p, int stride) {
+    if (EXACT) {
+        double s = __dmul_rn((double)p[RAD * stride], c_taps_d[TS][RAD]);
+#pragma unroll
+        for (int j = RAD; j >= 1; --j)
+            s = __dadd_rn(s, __dmul_rn(__dadd_rn((double)p[(RAD - j) * stride], (double)p[(RAD + j) * stride]),
+                                       c_taps_d[TS][RAD - j]));
+        return (float)s;
+    } else {
+        float s = 0.f;
+#pragma unroll
+        for (int j = 0; j <= 2 * RAD; ++j) s = fmaf(c_taps[TS][j], p[j * stride], s);
+        return s;
+    }
+}
+
+template <int TS, int RAD, bool EXACT, bool BASE>
+__global__ void __launch_bounds__(NT) k_blur(BlurArgs a) {
+    constexpr int IW = TX + 2 * RAD, IH = TY + 2 * RAD, SW = IW + 1;
+    __shared__ float s_in[IH * SW];
+    __shared__ float s_mid[TY * SW];
+    const int x0 = blockIdx.x * TX, y0 = blockIdx.y * TY;
+    for (int i = threadIdx.x; i < IH * IW; i += NT) {
+        const int yy = i / IW, xx = i - yy * IW;
+        const int gy = mirror(y0 + yy - RAD, a.rows), gx = mirror(x0 + xx - RAD, a.cols);
+        s_in[yy * SW + xx] = BASE ? up2_sample(a, gy, gx) : __ldg(a.src + (size_t)gy * a.cols + gx);
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < TY * IW; i += NT) {
+        const int yy = i / IW, xx = i - yy * IW;
+        s_mid[yy * SW + xx] = conv<TS, RAD, EXACT>(&s_in[yy * SW + xx], SW);
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < TY * TX; i += NT) {
+        const int yy = i / TX, xx = i - yy * TX;
+        const int gy = y0 + yy, gx = x0 + xx;
+        if (gy >= a.rows || gx >= a.cols) continue;
+        const float v = conv<TS, RAD, EXACT>(&s_mid[yy * SW + xx], 1);
+        const size_t at = (size_t)gy * a.cols + gx;
+        if (a.dst) a.dst[at] = v;
+        const float* c = &s_in[(yy + RAD) * SW + xx + RAD];   // previous layer at (gy, gx)
+        if (a.dog) a.dog[at] = __fsub_rn(v, c[0]);
+        if (a.mag) {
+            float dx = 0.f, dy = 0.f;
+            if (gy > 0 && gy < a.rows - 1 && gx > 0 && gx < a.cols - 1) {
+                dx = __fsub_rn(c[1], c[-1]);
+                dy = __fsub_rn(c[-SW], c[SW]);
+            }
+            a.mag[at] = __fsqrt_rn(__fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dy, dy)));
+            float an = __fmul_rn(atan2f(dy, dx), kRad2Deg);
+            a.ang[at] = an < 0.f ? __fadd_rn(an, 360.f) : an;
+        }
+        if (a.down && !(gy & 1) && !(gx & 1)) a.down[(size_t)(gy >> 1) * a.down_cols + (gx >> 1)] = c[0];
+    }
+}
+
+template <int TS, int RAD, bool BASE>
+void launch(bool exact, const BlurArgs& a, cudaStream_t s) {
+    dim3 grid((a.cols + TX - 1) / TX, (a.rows + TY - 1) / TY);
+    if (exact)
+        k_blur<TS, RAD, true, BASE><<<grid, NT, 0, s>>>(a);
+    else
+        k_blur<TS, RAD, false, BASE><<<grid, NT, 0, s>>>(a);
+}
+
+}  // namespace
+
+int32_t run_pyramid(Workspace& ws, const uint8_t* d_img, int img_stride, bool exact, cudaStream_t s) {
+    const Geometry& g = ws.g;
+    float* P[3] = {ws.plane[0].as<float>(), ws.plane[1].as<float>(), ws.plane[2].as<float>()};
+    float* DF = ws.dog.as<float>();
+    float* MAG = ws.mag.as<float>();
+    float* ANG = ws.ang.as<float>();
+    BlurArgs a{};
+    a.img = d_img;
+    a.img_stride = img_stride;
+    a.ih = g.h;
+    a.iw = g.w;
+    a.rows = g.R[0];
+    a.cols = g.C[0];
+    a.dst = P[0];
+    launch<0, 5, true>(exact, a, s);
+    for (int o = 0; o < g.n_oct; ++o) {
+        const long long RC = (long long)g.R[o] * g.C[o];
+        float* dog = DF + g.dog_off[o];
+        float* mag = MAG + g.grad_off[o];
+        float* ang = ANG + g.grad_off[o];
+        BlurArgs b{};
+        b.rows = g.R[o];
+        b.cols = g.C[o];
+        // layer 1: L0 (P0) -> P1, DoG 0
+        b.src = P[0]; b.dst = P[1]; b.dog = dog;
+        launch<1, 5, false>(exact, b, s);
+        // layer 2: L1 (P1) -> P2, DoG 1, gradient of L1
+        b.src = P[1]; b.dst = P[2]; b.dog = dog + RC; b.mag = mag; b.ang = ang;
+        launch<2, 6, false>(exact, b, s);
+        // layer 3: L2 (P2) -> P1, DoG 2, gradient of L2
+        b.src = P[2]; b.dst = P[1]; b.dog = dog + 2 * RC; b.mag = mag + RC; b.ang = ang + RC;
+        launch<3, 8, false>(exact, b, s);
+        // layer 4: L3 (P1) -> P2, DoG 3, gradient of L3, L3[::2, ::2] -> P0 (next octave base)
+        b.src = P[1]; b.dst = P[2]; b.dog = dog + 3 * RC; b.mag = mag + 2 * RC; b.ang = ang + 2 * RC;
+        if (o + 1 < g.n_oct) { b.down = P[0]; b.down_cols = g.C[o + 1]; }
+        launch<4, 10, false>(exact, b, s);
+        // layer 5: L4 (P2) -> DoG 4 only
+        b.src = P[2]; b.dst = nullptr; b.dog = dog + 4 * RC; b.mag = nullptr; b.ang = nullptr; b.down = nullptr;
+        launch<5, 13, false>(exact, b, s);
+    }
+    FSB_CUDA(cudaGetLastError());
+    return FSB_OK;
+}
+
+}  // namespace fsb

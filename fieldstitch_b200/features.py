@@ -1,0 +1,65 @@
+"""Drop-in for PlaneSite's per-photo GPU feature step (app/planesite/features.py:74-129).
+
+``sift_gpu(g2, nfeat)`` keeps the reference's signature and return value (xy float32 (n,2), desc
+float32 (n,128) or None, resp float32 (n,), seconds spent describing) but runs detect -> grid
+spread -> stable response sort -> describe -> RootSIFT in one device pass (fsb_sift_features).
+``sift_gpu_u8`` also returns the RootSIFT uint8 bytes of the feature file, computed on the device,
+and ``save_features`` writes the reference's .npz feature-file format.
+"""
+import ctypes
+import time
+
+import numpy as np
+
+from . import _lib
+from .gsift import _gray, _params
+
+
+def _extract(g2, nfeat, contrast, edge, exact, want_desc, want_u8, device):
+    g = _gray(g2)
+    ctx = _lib.context(device)
+    nf = int(nfeat)
+    xy = np.empty((max(nf, 0), 2), np.float32)
+    resp = np.empty(max(nf, 0), np.float32)
+    desc = np.empty((max(nf, 0), 128), np.float32) if want_desc else None
+    u8 = np.empty((max(nf, 0), 128), np.uint8) if want_u8 else None
+    n = ctypes.c_int32()
+    p = _params(contrast, edge, 0, exact)
+    _lib.check(ctx.lib.fsb_sift_features(ctx.handle, _lib.ptr(g), g.shape[0], g.shape[1], g.strides[0],
+                                         ctypes.byref(p), nf, _lib.ptr(xy), _lib.ptr(resp), _lib.ptr(desc),
+                                         _lib.ptr(u8), ctypes.byref(n)), "fsb_sift_features")
+    n = n.value
+    return xy[:n], (desc[:n] if desc is not None else None), resp[:n], (u8[:n] if u8 is not None else None)
+
+
+def sift_gpu(g2, nfeat, gpu=True, contrast=0.015, edge=12.0, exact=False, device=0):
+    """features.sift_gpu (app/planesite/features.py:115-129): (xy, desc, resp, t_desc); returns
+    zeros and None when fewer than 10 keypoints are found."""
+    if not gpu:
+        raise NotImplementedError("fieldstitch_b200 runs SIFT on the GPU only (no CPU fallback)")
+    t = time.perf_counter()
+    xy, desc, resp, _ = _extract(g2, nfeat, contrast, edge, exact, True, False, device)
+    if len(xy) == 0:
+        return np.zeros((0, 2), np.float32), None, np.zeros(0, np.float32), 0.0
+    return xy, desc, resp, time.perf_counter() - t
+
+
+def sift_gpu_u8(g2, nfeat, contrast=0.015, edge=12.0, exact=False, device=0):
+    """(xy, rootsift uint8 (n,128), resp): the feature-file content of features._save
+    (app/planesite/features.py:74-86) with the RootSIFT encoding done on the device."""
+    xy, _, resp, u8 = _extract(g2, nfeat, contrast, edge, exact, False, True, device)
+    if len(xy) < 10:
+        return np.zeros((0, 2), np.float32), np.zeros((0, 128), np.uint8), np.zeros(0, np.float32)
+    return xy, u8, resp
+
+
+def save_features(out_npz, xy, desc_u8, resp, w, h):
+    """Writes the feature file in the reference's format (keys xy, desc, resp, red_wh;
+    app/planesite/features.py:74-86). Returns the number of features written."""
+    if desc_u8 is None or len(xy) < 10:
+        np.savez(out_npz, xy=np.zeros((0, 2), np.float32), desc=np.zeros((0, 128), np.uint8),
+                 resp=np.zeros(0, np.float32), red_wh=np.array([w, h], np.int32))
+        return 0
+    np.savez(out_npz, xy=np.asarray(xy, np.float32), desc=np.asarray(desc_u8, np.uint8),
+             resp=np.asarray(resp, np.float32), red_wh=np.array([w, h], np.int32))
+    return len(xy)

@@ -1,0 +1,96 @@
+"""Drop-in for PlaneSite's descriptor matching (app/planesite/matching.py:86-152) on the B200.
+
+* ``_ratio_match_bf(da, db, ratio, na=None, nb=None, precision="fp32")`` - exhaustive ratio test
+  (matching.py:86-100) + ``_unique``. ``precision`` picks the distance engine; every engine
+  returns the same pairs.
+* ``_guided(A, B, Hm, radius, kc, ratio)`` - prior-guided matching (matching.py:113-152).
+  ``guided_from_pred`` takes predicted positions directly (the ground-plane prior of
+  matching.py:155-172, or any other prior); ``kc=None`` takes every B keypoint within radius.
+* ``_unique(q, t, dd)`` - one-to-one filter on the target (matching.py:103-110).
+
+Descriptors are the feature file's uint8 RootSIFT vectors (uint8 arrays, or float arrays holding
+uint8 values as the reference does). ``na``/``nb`` must be the squared norms when given (the
+reference callers pass exactly those); the device recomputes them.
+"""
+import ctypes
+
+import numpy as np
+
+from . import _lib
+
+
+def _out(n):
+    return np.empty(max(n, 1), np.int64), np.empty(max(n, 1), np.int64)
+
+
+def _ratio_match_bf(da, db, ratio, na=None, nb=None, precision="fp32", device=0):
+    if len(da) < 2 or len(db) < 2:
+        return np.zeros(0, np.int64), np.zeros(0, np.int64)
+    a = _lib.as_u8_desc(da, "da")
+    b = _lib.as_u8_desc(db, "db")
+    ctx = _lib.context(device)
+    q, t = _out(len(a))
+    n = ctypes.c_int32()
+    _lib.check(ctx.lib.fsb_match_bf(ctx.handle, _lib.ptr(a), len(a), _lib.ptr(b), len(b), float(ratio),
+                                    _lib.PREC[precision], _lib.ptr(q), _lib.ptr(t), ctypes.byref(n)), "fsb_match_bf")
+    return q[:n.value].copy(), t[:n.value].copy()
+
+
+def perspective(xy, Hm, device=0):
+    """cv2.perspectiveTransform of (n,2) float64 points on the device (matching.py:115)."""
+    xy = np.ascontiguousarray(np.asarray(xy, np.float64).reshape(-1, 2))
+    h = np.ascontiguousarray(np.asarray(Hm, np.float64).reshape(9))
+    out = np.empty_like(xy)
+    if len(xy):
+        ctx = _lib.context(device)
+        _lib.check(ctx.lib.fsb_perspective(ctx.handle, _lib.ptr(xy), len(xy), _lib.ptr(h), _lib.ptr(out)),
+                   "fsb_perspective")
+    return out
+
+
+def guided_from_pred(pred, a_desc, b_xy, b_desc, wh_b, radius, kc, ratio, device=0):
+    """Guided matching given predicted positions of A's keypoints in B's frame."""
+    a = _lib.as_u8_desc(a_desc, "A desc")
+    b = _lib.as_u8_desc(b_desc, "B desc")
+    pred = np.ascontiguousarray(np.asarray(pred, np.float64).reshape(-1, 2))
+    bxy = np.ascontiguousarray(np.asarray(b_xy, np.float64).reshape(-1, 2))
+    if len(pred) != len(a) or len(bxy) != len(b):
+        raise ValueError("positions and descriptors differ in length")
+    if len(a) == 0 or len(b) == 0:
+        return np.zeros(0, np.int64), np.zeros(0, np.int64)
+    ctx = _lib.context(device)
+    q, t = _out(len(a))
+    n = ctypes.c_int32()
+    k = 0 if kc is None else int(min(kc, len(b)))
+    if kc is not None and k < 1:
+        raise ValueError("kc must be >= 1 or None")
+    wb, hb = wh_b
+    _lib.check(ctx.lib.fsb_match_guided(ctx.handle, _lib.ptr(pred), _lib.ptr(a), len(a), _lib.ptr(bxy), _lib.ptr(b),
+                                        len(b), float(wb), float(hb), float(radius), k, float(ratio), _lib.ptr(q),
+                                        _lib.ptr(t), ctypes.byref(n)), "fsb_match_guided")
+    return q[:n.value].copy(), t[:n.value].copy()
+
+
+def _guided(A, B, Hm, radius, kc, ratio, device=0):
+    """matching._guided (app/planesite/matching.py:113-152) on feature dicts with keys und (n,2),
+    desc (n,128) and wh (W, H)."""
+    pred = perspective(A["und"], Hm, device)
+    return guided_from_pred(pred, A["desc"], B["und"], B["desc"], B["wh"], radius, kc, ratio, device)
+
+
+def _unique(q, t, dd, device=0):
+    """matching._unique (app/planesite/matching.py:103-110): per target t keep the entry with the
+    smallest dd (ties: earlier position); output ordered by t."""
+    q = np.ascontiguousarray(np.asarray(q, np.int64))
+    t = np.ascontiguousarray(np.asarray(t, np.int64))
+    dd = np.ascontiguousarray(np.asarray(dd, np.float32))
+    if len(q) == 0:
+        return q, t
+    if not (len(q) == len(t) == len(dd)):
+        raise ValueError("q, t and dd differ in length")
+    ctx = _lib.context(device)
+    qo, to = _out(len(q))
+    n = ctypes.c_int32()
+    _lib.check(ctx.lib.fsb_unique(ctx.handle, _lib.ptr(q), _lib.ptr(t), _lib.ptr(dd), len(q), _lib.ptr(qo),
+                                  _lib.ptr(to), ctypes.byref(n)), "fsb_unique")
+    return qo[:n.value].copy(), to[:n.value].copy()

@@ -48,12 +48,13 @@ def _pink_noise(rng, h, w, fmin=1.0 / 512, fmax=0.45):
 
 
 def synth_image(h, w, seed, n_blobs=400, noise_weight=0.6):
-    """uint8 (h, w) image: Gaussian blobs + 1/f band-limited noise, min-max rescaled to 0..255."""
+    """uint8 (h, w) image: Gaussian blobs + 1/f band-limited noise, rescaled so that the 0.5 and
+    99.5 percentiles map to 0 and 255 (clipped)."""
     rng = np.random.default_rng(seed)
     blobs = _blob_field(rng, h, w, n_blobs)
     bs = float(blobs.std()) or 1.0
     img = blobs / bs + np.float32(noise_weight) * _pink_noise(rng, h, w)
-    lo, hi = float(img.min()), float(img.max())
+    lo, hi = (float(v) for v in np.percentile(img[::4, ::4], [0.5, 99.5]))
     img = (img - lo) * (255.0 / max(hi - lo, 1e-6))
     return np.clip(np.rint(img), 0, 255).astype(np.uint8)
 

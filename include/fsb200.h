@@ -1,0 +1,128 @@
+/*
+ * fsb200.h - C ABI of the B200 (sm_100a) SIFT + guided-matching front end.
+ *
+ * Plain C types only (pointers, sizes, status codes). Every function returns FSB_OK (0) or a
+ * non-zero status; fsb_last_error() returns a message for the calling thread. Unless a
+ * function's comment says "device pointers", array arguments are HOST memory and the call
+ * returns once its results are in host memory.
+ *
+ * Each entry point replaces a function of PlaneSite (Edko01/FieldStitch); the citation names the
+ * reference file:line whose behaviour it reproduces. A context (fsb_ctx) owns one CUDA stream on
+ * one device and is not thread-safe: use one context per thread, or guard it.
+ */
+#ifndef FSB200_H
+#define FSB200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* status codes */
+#define FSB_OK 0
+#define FSB_ERR_ARG 1         /* invalid argument (null pointer, bad size, unknown mode) */
+#define FSB_ERR_OOM 2         /* device allocation failed */
+#define FSB_ERR_CUDA 3        /* a CUDA runtime call failed */
+#define FSB_ERR_TIMEOUT 4     /* a bounded device wait gave up */
+#define FSB_ERR_STATE 5       /* a detect state was used with another context or after free */
+#define FSB_ERR_UNSUPPORTED 6 /* the device is not sm_100 or the mode is not built */
+#define FSB_ERR_OVERFLOW 7    /* an internal capacity was exceeded and could not be grown */
+
+/* dense matcher precision (fsb_match_bf) */
+#define FSB_PREC_FP32 0 /* CUDA-core FP32 distances: the plain path */
+#define FSB_PREC_BF16 1 /* tcgen05 BF16 x BF16 -> FP32 distances, exact re-rank of the top 4 */
+#define FSB_PREC_FP8 2  /* tcgen05 E4M3 (per-descriptor scale) -> FP32, exact re-rank of the top 4 */
+
+typedef struct fsb_ctx fsb_ctx;
+typedef struct fsb_state fsb_state;
+
+/* SIFT parameters (gsift.detect keyword arguments, app/planesite/gsift.py:435). */
+typedef struct {
+    double contrast; /* contrast threshold (default 0.015; OpenCV default 0.04) */
+    double edge;     /* edge threshold (default 12; OpenCV default 10) */
+    int32_t max_kp;  /* keep at most this many keypoints, strongest first (default 12000) */
+    int32_t flags;   /* FSB_SIFT_* bits */
+} fsb_sift_params;
+
+/* blur accumulates in float64 and rounds once to float32 per pass, as scipy.ndimage does in the
+   reference's CPU path: the pyramid is then bit-identical to it (slower). Default: float32 FMA. */
+#define FSB_SIFT_EXACT_BLUR 1
+
+/* ---- library / context ------------------------------------------------------------------- */
+int32_t fsb_version(void);
+const char* fsb_last_error(void);
+/* Creates a context on CUDA device `device` (the CuPy device/stream the reference's GPU worker
+   uses, app/planesite/features.py:258-267). Fails with FSB_ERR_UNSUPPORTED unless sm_100. */
+int32_t fsb_create(int32_t device, fsb_ctx** out);
+int32_t fsb_destroy(fsb_ctx* ctx);
+/* Waits, for at most timeout_ms, for the context's stream; FSB_ERR_TIMEOUT if it did not drain. */
+int32_t fsb_sync(fsb_ctx* ctx, int32_t timeout_ms);
+/* The context's cudaStream_t, as an opaque pointer (for callers that share the stream). */
+void* fsb_stream(fsb_ctx* ctx);
+/* Bytes of device memory the context holds (workspaces and scratch). */
+int64_t fsb_device_bytes(fsb_ctx* ctx);
+
+/* ---- SIFT detection / description ---------------------------------------------------------- */
+/* gsift.detect (app/planesite/gsift.py:435-477): 2x upsample, Gaussian/DoG pyramid, 3x3x3
+   extrema, sub-pixel refinement with contrast and edge tests, 36-bin orientations, strongest
+   first (ties: octave, layer, row, column of the extremum, then orientation bin), at most
+   p->max_kp. `img` is a uint8 grey image with `stride` bytes per row. On success *state holds
+   the gradient atlas for fsb_describe and *n_kp the keypoint count. */
+int32_t fsb_detect(fsb_ctx* ctx, const uint8_t* img, int32_t h, int32_t w, int32_t stride,
+                   const fsb_sift_params* p, fsb_state** state, int32_t* n_kp);
+/* Copies the detected keypoints (n_kp entries each) into host arrays: x, y in input-image
+   pixels, size, angle (degrees), response, 0-based octave of the upsampled image, layer 1..3
+   (the dict returned by gsift.detect, app/planesite/gsift.py:473-474). Null outputs are skipped. */
+int32_t fsb_state_keypoints(fsb_state* st, float* x, float* y, float* size, float* angle,
+                            float* response, int32_t* octave, int32_t* layer);
+/* gsift.describe (app/planesite/gsift.py:480-525): 128-d descriptors of n keypoints given by
+   their x, y, size, angle, octave, layer (usually kps[sel] of fsb_detect). desc (n*128 float32,
+   L2 norm 512, unrounded) and/or rootsift (n*128 uint8, the feature-file encoding of
+   app/planesite/features.py:80-82) may be null. */
+int32_t fsb_describe(fsb_ctx* ctx, fsb_state* st, int32_t n, const float* x, const float* y,
+                     const float* size, const float* angle, const int32_t* octave,
+                     const int32_t* layer, float* desc, uint8_t* rootsift);
+int32_t fsb_state_free(fsb_state* st);
+
+/* features.sift_gpu (app/planesite/features.py:115-129) in one device pass: detect with
+   max_kp = int(2.2 nfeat) (p->max_kp is ignored), grid-spread selection of nfeat keypoints
+   (features.py:38-57, ties by index), stable sort by response, describe, RootSIFT. Outputs hold
+   up to nfeat rows: xy (n*2 float32), resp (n float32), desc (n*128 float32, nullable),
+   rootsift (n*128 uint8, nullable). *n_out = 0 when fewer than 10 keypoints were found
+   (features.py:121-122). */
+int32_t fsb_sift_features(fsb_ctx* ctx, const uint8_t* img, int32_t h, int32_t w, int32_t stride,
+                          const fsb_sift_params* p, int32_t nfeat, float* xy, float* resp,
+                          float* desc, uint8_t* rootsift, int32_t* n_out);
+
+/* ---- matching ------------------------------------------------------------------------------- */
+/* matching._ratio_match_bf + _unique (app/planesite/matching.py:86-110) on uint8 descriptors
+   (na x 128, nb x 128, row-major): nearest and second-nearest squared L2 distance over all of B,
+   ratio test sqrt(b1) < ratio * sqrt(b2) in float32, then one match per target keeping the
+   smallest distance (ties: smaller query index). Writes *n_out pairs ordered by target into
+   q, t (capacity na each). precision: FSB_PREC_*; every precision returns the same pairs. */
+int32_t fsb_match_bf(fsb_ctx* ctx, const uint8_t* a, int32_t na, const uint8_t* b, int32_t nb,
+                     float ratio, int32_t precision, int64_t* q, int64_t* t, int32_t* n_out);
+/* matching._guided + _unique (app/planesite/matching.py:113-152) given predicted positions
+   pred_xy (na x 2 float64) of A's keypoints in B: predictions outside B's w_b x h_b frame
+   widened by radius are skipped; candidates are B keypoints (b_xy, nb x 2 float64) strictly
+   within radius; kc > 0 keeps only the kc nearest (ties: smaller B index), kc <= 0 keeps all;
+   exact squared descriptor distances; top-2 ratio test (a single candidate passes); one match
+   per target. Writes *n_out pairs ordered by target. */
+int32_t fsb_match_guided(fsb_ctx* ctx, const double* pred_xy, const uint8_t* a, int32_t na,
+                         const double* b_xy, const uint8_t* b, int32_t nb, double w_b, double h_b,
+                         double radius, int32_t kc, float ratio, int64_t* q, int64_t* t,
+                         int32_t* n_out);
+/* matching._unique (app/planesite/matching.py:103-110) for n candidate pairs (q, t, dd): per
+   target t keeps the entry with the smallest dd (ties: earlier position), output ordered by t
+   (q_out, t_out capacity n; *n_out entries written). */
+int32_t fsb_unique(fsb_ctx* ctx, const int64_t* q, const int64_t* t, const float* dd, int32_t n,
+                   int64_t* q_out, int64_t* t_out, int32_t* n_out);
+/* cv2.perspectiveTransform of app/planesite/matching.py:115 on the device (float64):
+   out = (H [x y 1]^T)_{xy} / (H [x y 1]^T)_z. */
+int32_t fsb_perspective(fsb_ctx* ctx, const double* xy, int32_t n, const double* hm9, double* out);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* FSB200_H */

@@ -74,10 +74,16 @@ def guided_from_pred(pred, a_desc, b_und, b_desc, wh_b, radius, kc, ratio, a_nor
     valid = idx < nb
     has = valid.any(1)
     inside, idx, valid = inside[has], idx[has], valid[has]
+    if len(inside) == 0:
+        # the reference reaches np.concatenate([]) here and raises ValueError (caught by
+        # match_pair's handler); the drop-in returns no matches instead
+        return np.zeros(0, np.int64), np.zeros(0, np.int64)
     idx = np.where(valid, idx, 0)
     qs, ts, ds = [], [], []
-    for s0 in range(0, len(inside), 1024):
-        sl = slice(s0, s0 + 1024)
+    # the reference uses 1024-query chunks; smaller chunks for large k only bound memory
+    chunk = max(1, min(1024, (1 << 21) // max(k, 1)))
+    for s0 in range(0, len(inside), chunk):
+        sl = slice(s0, s0 + chunk)
         da = a_desc[inside[sl]]
         cand = b_desc[idx[sl]]
         d2 = a_norm[inside[sl], None] + b_norm[idx[sl]] - 2 * np.matmul(cand, da[:, :, None])[:, :, 0]

@@ -1,0 +1,141 @@
+"""Parity of the CUDA SIFT path (through the C ABI) with the oracle, the reference fixtures and
+OpenCV. Tolerances are the north-star ones: position <= 0.01 px, angle <= 0.1 deg, descriptor
+bytes within +-1."""
+import numpy as np
+import pytest
+
+from sift_compare import angle_diff, paired_fraction
+
+pytestmark = pytest.mark.gpu
+
+CASES = ["s240x320_c04", "s200x264_c015", "s97x131_c04"]
+
+
+@pytest.fixture(scope="module")
+def fsb():
+    import fieldstitch_b200 as f
+    f.context(0)
+    return f
+
+
+def _ref(golden, case):
+    g = golden["sift_ref"]
+    kps = {k: g[case + "/kp_" + k] for k in ("x", "y", "size", "angle", "response", "octave", "layer")}
+    contrast, edge, max_kp, nfeat = g[case + "/params"]
+    return g[case + "/img"], kps, float(contrast), float(edge), int(max_kp), int(nfeat)
+
+
+@pytest.mark.parametrize("case", CASES)
+def test_detect_exact_blur_matches_reference(fsb, golden, case):
+    """float64 blur: positions, responses, octaves and layers identical to the reference's CPU
+    path for >= 99 % of keypoints; angles within 0.1 deg."""
+    img, ref, contrast, edge, max_kp, _ = _ref(golden, case)
+    got, _ = fsb.gsift.detect(img, max_kp=max_kp, contrast=contrast, edge=edge, exact=True)
+    assert abs(len(got["x"]) - len(ref["x"])) <= 0.01 * len(ref["x"]) + 2
+    frac, p = paired_fraction(ref, got, pos_tol=1e-6, ang_tol=0.1)
+    assert frac >= 0.99, frac
+    m = p >= 0
+    np.testing.assert_array_equal(got["response"][p[m]], ref["response"][m])
+    np.testing.assert_array_equal(got["octave"][p[m]], ref["octave"][m])
+    np.testing.assert_array_equal(got["layer"][p[m]], ref["layer"][m])
+    np.testing.assert_allclose(got["size"][p[m]], ref["size"][m], rtol=1e-6)
+
+
+@pytest.mark.parametrize("case", CASES)
+def test_detect_fast_matches_reference(fsb, golden, case):
+    """float32 FMA blur: >= 97 % of the reference's keypoints within 0.01 px and 0.1 deg."""
+    img, ref, contrast, edge, max_kp, _ = _ref(golden, case)
+    got, _ = fsb.gsift.detect(img, max_kp=max_kp, contrast=contrast, edge=edge)
+    frac, _ = paired_fraction(ref, got)
+    assert frac >= 0.97, frac
+    back, _ = paired_fraction(got, ref)
+    assert back >= 0.97, back
+
+
+@pytest.mark.parametrize("case", CASES[:2])
+def test_detect_agrees_with_opencv(fsb, golden, case):
+    """OpenCV SIFT (the reference CPU extractor) on the same image: >= 90 % of OpenCV's keypoints
+    have a GPU keypoint within 0.01 px and 0.1 deg (the reference's own CPU path reaches ~98 %)."""
+    img, _, contrast, edge, max_kp, _ = _ref(golden, case)
+    c = golden["sift_cv2"]
+    cv = {"x": c[case + "/xy"][:, 0], "y": c[case + "/xy"][:, 1], "angle": c[case + "/angle"]}
+    got, _ = fsb.gsift.detect(img, max_kp=max_kp, contrast=contrast, edge=edge)
+    frac, p = paired_fraction(cv, got)
+    assert frac >= 0.90, frac
+    # descriptors of paired keypoints: OpenCV rounds to integers; compare bytes
+    m = np.nonzero(p >= 0)[0]
+    _, st = fsb.gsift.detect(img, max_kp=max_kp, contrast=contrast, edge=edge)
+    d = fsb.gsift.describe(st, got, p[m])
+    diff = np.abs(np.rint(d) - c[case + "/desc"][m].astype(np.float64))
+    assert (diff <= 1).mean() >= 0.99, (diff <= 1).mean()
+
+
+@pytest.mark.parametrize("exact", [True, False])
+@pytest.mark.parametrize("case", CASES)
+def test_describe_matches_reference(fsb, golden, case, exact):
+    """Descriptors of the reference's own keypoints: float values within 0.02 (of 512 norm) for
+    >= 99.9 % of entries and RootSIFT bytes within +-1."""
+    from oracle import features_ref
+    img, ref, contrast, edge, max_kp, _ = _ref(golden, case)
+    _, st = fsb.gsift.detect(img, max_kp=max_kp, contrast=contrast, edge=edge, exact=exact)
+    sel = np.arange(len(ref["x"]))
+    d, u8 = fsb.gsift.describe(st, ref, sel, rootsift=True)
+    want = golden["sift_ref"][case + "/desc"]
+    err = np.abs(d - want)
+    assert (err <= 0.02).mean() >= 0.999, (err <= 0.02).mean()
+    assert err.max() < (5.0 if exact else 20.0), err.max()
+    du = np.abs(u8.astype(np.int32) - features_ref.rootsift_u8(want).astype(np.int32))
+    assert (du <= 1).mean() >= 0.9999, (du <= 1).mean()
+    # the device RootSIFT encoding is the reference's exactly, on the device's own floats
+    np.testing.assert_array_equal(u8, features_ref.rootsift_u8(d))
+
+
+@pytest.mark.parametrize("case", CASES)
+def test_sift_gpu_sequence(fsb, golden, case):
+    """features.sift_gpu: selection, order and RootSIFT bytes vs the reference's worker output."""
+    img, _, _, _, _, nfeat = _ref(golden, case)
+    g = golden["sift_ref"]
+    xy, u8, resp = fsb.features.sift_gpu_u8(img, nfeat, exact=True)
+    want_xy, want_u8 = g[case + "/sg_xy"], g[case + "/sg_u8"]
+    assert len(xy) == len(want_xy)
+    same = np.all(xy == want_xy, axis=1)
+    assert same.mean() >= 0.97, same.mean()
+    du = np.abs(u8[same].astype(np.int32) - want_u8[same].astype(np.int32))
+    assert (du <= 1).mean() >= 0.999
+    xy2, desc, resp2, _ = fsb.features.sift_gpu(img, nfeat, exact=True)
+    np.testing.assert_array_equal(xy2, xy)
+    np.testing.assert_array_equal(resp2, resp)
+
+
+def test_flat_image_and_tiny_image(fsb):
+    kps, st = fsb.gsift.detect(np.full((64, 80), 128, np.uint8))
+    assert len(kps["x"]) == 0 and kps["x"].dtype == np.float32
+    assert fsb.gsift.describe(st, kps, np.zeros(0, np.int64)).shape == (0, 128)
+    xy, desc, resp, _ = fsb.features.sift_gpu(np.full((40, 40), 3, np.uint8), 100)
+    assert xy.shape == (0, 2) and desc is None
+    kps, _ = fsb.gsift.detect(np.zeros((7, 9), np.uint8))   # smaller than one octave: no pyramid
+    assert len(kps["x"]) == 0
+
+
+def test_strided_input_and_determinism(fsb, golden):
+    img = golden["sift_ref"]["s240x320_c04/img"]
+    big = np.zeros((240, 400), np.uint8)
+    big[:, 30:350] = img
+    a, _ = fsb.gsift.detect(big[:, 30:350], contrast=0.04, edge=10)
+    b, _ = fsb.gsift.detect(np.ascontiguousarray(img), contrast=0.04, edge=10)
+    c, _ = fsb.gsift.detect(img, contrast=0.04, edge=10)
+    for k in a:
+        np.testing.assert_array_equal(a[k], b[k])
+        np.testing.assert_array_equal(b[k], c[k])
+
+
+def test_large_image_against_oracle(fsb):
+    """660 x 495 synthetic image (about 3.5 M octave pixels): oracle agreement at a larger size."""
+    from fieldstitch_b200 import synth
+    from oracle import gsift_ref
+    img = synth.synth_image(495, 660, 77)
+    ref, _ = gsift_ref.detect(img, max_kp=100000, contrast=0.04, edge=10)
+    got, _ = fsb.gsift.detect(img, max_kp=100000, contrast=0.04, edge=10, exact=True)
+    frac, p = paired_fraction(ref, got, pos_tol=1e-6)
+    assert frac >= 0.99, frac
+    assert np.all(angle_diff(ref["angle"][p >= 0], got["angle"][p[p >= 0]]) <= 0.1)
