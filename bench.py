@@ -1,0 +1,373 @@
+#!/usr/bin/env python
+"""Benchmark: pairs/s of SIFT extraction + prior-guided matching at 2640x1978.
+
+Workload (one step): 64 synthetic image pairs at 2640x1978 (uint8; seeded blobs + 1/f noise; B =
+A warped by a random homography + noise), per-image keypoint caps drawn from U[2000, 16000];
+every image goes through the features.sift_gpu sequence (detect with max_kp = 2.2 nfeat, grid
+spread, describe, RootSIFT); each pair is then matched by prior-guided matching: predicted
+position = true homography + N(0, 15 px), candidates = the 16 nearest keypoints within 40 px
+(the pipeline's guided_k), exact squared distances, ratio 0.85, one-to-one filter. A "pair" is
+extraction of both images + the match.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl fsb|reference]
+
+value  : pairs/s with the images resident in HBM (device-pointer C ABI, fsb_*_d).
+e2e    : the same pairs through the public host API (features.sift_gpu_u8 + matching
+         guided_from_pred) with host buffers, copies included.
+roofline: the pyramid (dominant stage) from CUDA events on the library stream over the timed
+         steps; algorithmic bytes per image = H*W + 44 * (sum of octave pixels).
+--impl reference: the reference's CPU implementation of the path (OpenCV SIFT as
+         features.sift_cpu calls it + the NumPy/cKDTree guided matcher), oracle port, on the host
+         cores; one pair per step.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+if ROOT not in sys.path:
+    sys.path.insert(0, ROOT)
+
+METRIC = "pairs/s SIFT+guided match @2640x1978: BF16/FP8+rerank vs FP32, same matches"
+H_IMG, W_IMG = 1978, 2640
+RADIUS, RATIO, KC = 40.0, 0.85, 16
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=5)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", default="fsb", choices=["fsb", "reference"])
+    p.add_argument("--pairs", type=int, default=64)
+    p.add_argument("--seed", type=int, default=1000)
+    p.add_argument("--no-e2e", action="store_true")
+    p.add_argument("--no-cpu", action="store_true")
+    return p.parse_args()
+
+
+def config(args, extra=None):
+    c = {"workload": "SIFT (sift_gpu sequence) + prior-guided match of %d pairs at %dx%d per GPU per step; "
+                     "nfeat U[2000,16000] per image; prior = true homography + N(0,15 px); the %d nearest "
+                     "keypoints within %g px, ratio %g" % (args.pairs, W_IMG, H_IMG, KC, RADIUS, RATIO),
+         "pairs_per_step_per_gpu": args.pairs, "image": [W_IMG, H_IMG], "radius_px": RADIUS, "kc": KC, "ratio": RATIO,
+         "contrast": 0.015, "edge": 12.0, "distances": "exact (uint8 RootSIFT, integer dp4a)",
+         "l2": "inputs larger than L2: %d images x %.1f MB per step" % (2 * args.pairs, H_IMG * W_IMG / 1e6),
+         "parallelism": "replicas: independent pairs per GPU (weak scaling)"}
+    if extra:
+        c.update(extra)
+    return c
+
+
+def gen_pairs(n, seed):
+    import multiprocessing as mp
+    jobs = [(H_IMG, W_IMG, seed + i) for i in range(n)]
+    from fieldstitch_b200 import synth
+    workers = max(1, min(len(jobs), (os.cpu_count() or 2) - 1, 32))
+    if workers == 1:
+        return [synth.flight_pair(j) for j in jobs]
+    with mp.get_context("spawn").Pool(workers) as pool:
+        return pool.map(synth.flight_pair, jobs)
+
+
+# ------------------------------------------------------------------------------------- clocks
+class Clocks:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_id):
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", "-i", str(gpu_id), "--query-gpu=" + self.FIELDS,
+                                       "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.f,
+                                      stderr=subprocess.DEVNULL)
+        except OSError:
+            self.p = None
+
+    def stop(self):
+        if self.p is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.p.terminate()
+        try:
+            self.p.wait(5)
+        except subprocess.TimeoutExpired:
+            self.p.kill()
+        self.f.flush()
+        rows = [r.split(",") for r in open(self.f.name).read().strip().splitlines() if r.count(",") >= 8]
+        os.unlink(self.f.name)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        sm = [float(r[1]) for r in rows if r[1].strip().replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].strip().replace(".", "").isdigit()]
+        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+        reasons = [n for i, n in enumerate(names) if any(r[5 + i].strip() == "Active" for r in rows)]
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def gpu_smi_id(torch, dev):
+    try:
+        return "GPU-" + str(torch.cuda.get_device_properties(dev).uuid)
+    except Exception:  # noqa: BLE001
+        return str(dev)
+
+
+def peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        d = json.load(open(path))
+        return float(d["hbm_gbs"]), "measured (MEASURED_PEAKS.json hbm_gbs)"
+    return 6650.0, "fallback (6.65 TB/s)"
+
+
+def pyramid_bytes(h, w):
+    """Algorithmic bytes of one image's pyramid: H*W input + 44 B per octave pixel (DoG 5 x 4 B +
+    gradient magnitude and angle 3 x 8 B)."""
+    import math
+    R, C = 2 * h, 2 * w
+    budget = max(1, int(round(math.log2(min(h, w)) - 2)) + 1)
+    tot = 0
+    for _ in range(budget):
+        if min(R, C) < 14:
+            break
+        tot += R * C
+        R, C = (R + 1) // 2, (C + 1) // 2
+    return h * w + 44 * tot
+
+
+def traffic_per_pyramid():
+    path = os.path.join(ROOT, "profiles", "pyramid_traffic.json")
+    if os.path.exists(path):
+        try:
+            return json.load(open(path)).get("dram_bytes_per_image_2640x1978")
+        except (ValueError, OSError):
+            return None
+    return None
+
+
+# ------------------------------------------------------------------------------ CPU reference
+def cpu_pair(pair, pidx, seed, cores):
+    """One pair through the reference's CPU path (oracle port): features.sift_cpu (OpenCV SIFT) ->
+    RootSIFT bytes -> prior-guided matching (NumPy + cKDTree). Returns (matches, seconds)."""
+    import cv2
+
+    from fieldstitch_b200 import synth
+    from oracle import features_ref, matching_ref
+    cv2.setNumThreads(cores)
+    a, b, H, na, nb = pair
+    t0 = time.perf_counter()
+    xa, da, _, _ = features_ref.sift_cpu(a, na)
+    xb, db, _, _ = features_ref.sift_cpu(b, nb)
+    if da is None or db is None:
+        return 0, time.perf_counter() - t0
+    ua, ub = features_ref.rootsift_u8(da), features_ref.rootsift_u8(db)
+    pred = synth.apply_homography(H, xa) + synth.prior_noise(len(xa), seed + pidx).astype(np.float64)
+    q, _ = matching_ref.guided_from_pred(pred, ua, xb.astype(np.float64), ub, (W_IMG, H_IMG), RADIUS, KC, RATIO)
+    return len(q), time.perf_counter() - t0
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    cores = os.cpu_count() or 1
+    pairs = gen_pairs(args.warmup + args.steps, args.seed)
+    for i in range(args.warmup):
+        cpu_pair(pairs[i], i, args.seed, cores)
+    times = []
+    for i in range(args.warmup, args.warmup + args.steps):
+        times.append(cpu_pair(pairs[i], i, args.seed, cores)[1])
+    per_pair = sum(times) / len(times)
+    v = 1.0 / per_pair
+    line = {"metric": METRIC, "value": v, "unit": "pairs/s", "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": per_pair * 1000.0, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded)",
+            "config": config(args, {"pairs_per_step_per_gpu": 1}), "impl": "reference",
+            "cpu_baseline": {"value": v, "unit": "pairs/s", "cores": cores, "kind": "port",
+                             "sample": "1 pair per step (2 images 2640x1978 + guided match), %d steps" % args.steps},
+            "e2e": {"value": v, "unit": "pairs/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# ---------------------------------------------------------------------------------- GPU arm
+def run_fsb(args):
+    import ctypes
+
+    import torch
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    pairs = gen_pairs(args.pairs, args.seed + 100000 * rank)   # before any CUDA work
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300), device_id=torch.device("cuda", local))
+
+    import fieldstitch_b200 as F
+    from fieldstitch_b200 import _lib, synth
+    ctx = F.context(local)
+    L = ctx.lib
+    stream = torch.cuda.ExternalStream(ctx.stream())
+    dev = torch.device("cuda", local)
+    h, w = H_IMG, W_IMG
+    nmax = 16000
+    # device-resident inputs and per-pair prior errors
+    d_img = [(torch.from_numpy(a).to(dev), torch.from_numpy(b).to(dev)) for a, b, _, _, _ in pairs]
+    d_noise = [torch.from_numpy(synth.prior_noise(nmax, args.seed + 7 * i)).to(dev) for i in range(len(pairs))]
+    xy = [torch.empty((nmax, 2), dtype=torch.float32, device=dev) for _ in range(2)]
+    rs = [torch.empty(nmax, dtype=torch.float32, device=dev) for _ in range(2)]
+    u8 = [torch.empty((nmax, 128), dtype=torch.uint8, device=dev) for _ in range(2)]
+    pred = torch.empty((nmax, 2), dtype=torch.float64, device=dev)
+    bxy = torch.empty((nmax, 2), dtype=torch.float64, device=dev)
+    dq = torch.empty(nmax, dtype=torch.int64, device=dev)
+    dt = torch.empty(nmax, dtype=torch.int64, device=dev)
+    eye = np.eye(3).reshape(9).copy()
+    Hs = [np.ascontiguousarray(p[2].reshape(9)) for p in pairs]
+    prm = _lib.SiftParams(0.015, 12.0, 0, 0)
+    n_out = ctypes.c_int32()
+    torch.cuda.synchronize()
+
+    def P(t):
+        return ctypes.c_void_p(t.data_ptr())
+
+    def one_step():
+        matches = 0
+        for i, (ia, ib) in enumerate(d_img):
+            n = []
+            for k, (img, nf) in enumerate(((ia, pairs[i][3]), (ib, pairs[i][4]))):
+                _lib.check(L.fsb_sift_features_d(ctx.handle, P(img), h, w, w, ctypes.byref(prm), nf, P(xy[k]),
+                                                 P(rs[k]), None, P(u8[k]), ctypes.byref(n_out)), "sift")
+                n.append(n_out.value)
+            _lib.check(L.fsb_project_d(ctx.handle, P(xy[0]), n[0], _lib.ptr(Hs[i]), P(d_noise[i]), P(pred)), "proj")
+            _lib.check(L.fsb_project_d(ctx.handle, P(xy[1]), n[1], _lib.ptr(eye), None, P(bxy)), "proj")
+            _lib.check(L.fsb_match_guided_d(ctx.handle, P(pred), P(u8[0]), n[0], P(bxy), P(u8[1]), n[1], float(w),
+                                            float(h), RADIUS, KC, RATIO, P(dq), P(dt), ctypes.byref(n_out)), "guided")
+            matches += n_out.value
+        return matches
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+
+    for _ in range(args.warmup):
+        one_step()
+    torch.cuda.synchronize()
+    barrier()
+    ctx.timing(True)
+    ctx.stage_times()
+    clocks = Clocks(gpu_smi_id(torch, local))
+    launches0 = _lib.launch_count()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    matches = 0
+    for _ in range(args.steps):
+        matches += one_step()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    launches = _lib.launch_count() - launches0
+    stages = ctx.stage_times()
+    ctx.timing(False)
+    ms_step = e0.elapsed_time(e1) / args.steps
+    if dist is not None:
+        t = torch.tensor([ms_step], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms_step = float(t.item())
+        barrier()
+    value = world * args.pairs / (ms_step / 1000.0)
+
+    # ---- e2e through the public host API (host buffers, copies inside the timed region)
+    e2e = None
+    if not args.no_e2e:
+        host = [(np.ascontiguousarray(a), np.ascontiguousarray(b)) for a, b, _, _, _ in pairs]
+
+        def e2e_step():
+            h2d = d2h = 0
+            for i, (a, b) in enumerate(host):
+                xa, ua, _ = F.features.sift_gpu_u8(a, pairs[i][3])
+                xb, ub, _ = F.features.sift_gpu_u8(b, pairs[i][4])
+                pr = synth.apply_homography(pairs[i][2], xa) + \
+                    synth.prior_noise(nmax, args.seed + 7 * i)[:len(xa)].astype(np.float64)
+                q, _ = F.matching.guided_from_pred(pr, ua, xb.astype(np.float64), ub, (w, h), RADIUS, KC, RATIO)
+                h2d += a.nbytes + b.nbytes + pr.nbytes + ua.nbytes + 16 * len(xb) + ub.nbytes
+                d2h += (len(xa) + len(xb)) * (8 + 4 + 128) + 16 * len(q) + 16
+            return h2d, d2h
+
+        e2e_step()
+        torch.cuda.synchronize()
+        barrier()
+        f0 = torch.cuda.Event(enable_timing=True)
+        f1 = torch.cuda.Event(enable_timing=True)
+        f0.record(stream)
+        h2d = d2h = 0
+        ksteps = max(1, args.steps // 2)
+        for _ in range(ksteps):
+            a_, b_ = e2e_step()
+            h2d, d2h = a_, b_
+        f1.record(stream)
+        torch.cuda.synchronize()
+        ms_e2e = f0.elapsed_time(f1) / ksteps
+        if dist is not None:
+            t = torch.tensor([ms_e2e], device=dev)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            ms_e2e = float(t.item())
+        e2e = {"value": world * args.pairs / (ms_e2e / 1000.0), "unit": "pairs/s", "h2d_bytes_per_step": int(h2d),
+               "d2h_bytes_per_step": int(d2h), "ms_per_step": ms_e2e, "steps": ksteps}
+
+    # ---- roofline of the dominant stage (pyramid), from the events of the timed steps
+    pk, pk_src = peaks()
+    pyr_ms, pyr_n = stages["pyramid"]
+    per_img_ms = pyr_ms / max(pyr_n, 1)
+    alg = pyramid_bytes(h, w)
+    achieved = alg / (per_img_ms / 1000.0) / 1e9 if per_img_ms > 0 else None
+    roof = {"bound": "hbm", "kernel": "pyramid (k_blur launches of one image)", "achieved": achieved, "peak": pk,
+            "peak_source": pk_src, "unit": "GB/s", "frac": (achieved / pk) if achieved else None,
+            "traffic": traffic_per_pyramid(), "algorithmic_bytes": alg, "ms_per_launch_group": per_img_ms}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        cores = os.cpu_count() or 1
+        n_cpu = 2
+        ts = [cpu_pair(pairs[i], i, args.seed, cores)[1] for i in range(n_cpu)]
+        cpu = {"value": n_cpu / sum(ts), "unit": "pairs/s", "cores": cores, "kind": "port",
+               "sample": "%d pairs of the same workload (OpenCV SIFT as features.sift_cpu + NumPy/cKDTree "
+                         "guided match)" % n_cpu}
+
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": "pairs/s", "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded)", "config": config(args),
+                "clocks": clk, "e2e": e2e, "gpu_launches": int(launches), "roofline": roof, "cpu_baseline": cpu,
+                "matches_per_step": matches / args.steps,
+                "stages_ms_per_step": {k: v[0] / args.steps for k, v in stages.items()}}
+        print(json.dumps(line), flush=True)
+    if dist is not None:
+        barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_fsb(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

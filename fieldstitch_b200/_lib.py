@@ -45,7 +45,17 @@ SIGNATURES = [
                                  c_vp, c_vp, c_vp]),
     ("fsb_unique", c_i32, [c_vp, c_vp, c_vp, c_vp, c_i32, c_vp, c_vp, c_vp]),
     ("fsb_perspective", c_i32, [c_vp, c_vp, c_i32, c_vp, c_vp]),
+    ("fsb_launch_count", c_i64, []),
+    ("fsb_timing", c_i32, [c_vp, c_i32]),
+    ("fsb_stage_times", c_i32, [c_vp, c_vp, c_vp, c_i32]),
+    ("fsb_sift_features_d", c_i32, [c_vp, c_vp, c_i32, c_i32, c_i32, c_vp, c_i32, c_vp, c_vp, c_vp, c_vp, c_vp]),
+    ("fsb_project_d", c_i32, [c_vp, c_vp, c_i32, c_vp, c_vp, c_vp]),
+    ("fsb_match_guided_d", c_i32, [c_vp, c_vp, c_vp, c_i32, c_vp, c_vp, c_i32, c_f64, c_f64, c_f64, c_i32, c_f32,
+                                   c_vp, c_vp, c_vp]),
+    ("fsb_match_bf_d", c_i32, [c_vp, c_vp, c_i32, c_vp, c_i32, c_f32, c_i32, c_vp, c_vp, c_vp]),
 ]
+
+STAGES = ("upload", "pyramid", "extrema", "refine", "orientation", "sort", "spread", "describe", "match")
 
 _lib = None
 _lock = threading.Lock()
@@ -105,6 +115,25 @@ class Context:
 
     def device_bytes(self):
         return int(self.lib.fsb_device_bytes(self.handle))
+
+    def stream(self):
+        """The context's cudaStream_t as an integer handle."""
+        return int(self.lib.fsb_stream(self.handle) or 0)
+
+    def timing(self, on=True):
+        check(self.lib.fsb_timing(self.handle, 1 if on else 0), "fsb_timing")
+
+    def stage_times(self):
+        """{stage: (milliseconds, calls)} accumulated since the last call (then reset)."""
+        ms = np.zeros(len(STAGES), np.float64)
+        n = np.zeros(len(STAGES), np.int64)
+        check(self.lib.fsb_stage_times(self.handle, ptr(ms), ptr(n), len(STAGES)), "fsb_stage_times")
+        return {s: (float(ms[i]), int(n[i])) for i, s in enumerate(STAGES)}
+
+
+def launch_count():
+    """Kernel launches issued by libfsb200 in this process."""
+    return int(load().fsb_launch_count())
 
 
 _tls = threading.local()

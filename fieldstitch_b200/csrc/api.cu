@@ -4,6 +4,7 @@
 
 #include <cmath>
 #include <cstring>
+#include <atomic>
 #include <string>
 
 #include "fsb_internal.cuh"
@@ -106,29 +107,99 @@ static int32_t to_dev(DevBuf& b, const T* h, size_t n, cudaStream_t s) {
     return FSB_OK;
 }
 
+// detect on an image already in device memory (the workspace must be prepared for h x w)
+static int32_t detect_dev(fsb_ctx* ctx, Workspace& ws, const uint8_t* d_img, int stride, const fsb_sift_params* p,
+                          int max_kp) {
+    const bool exact = (p->flags & FSB_SIFT_EXACT_BLUR) != 0;
+    ctx->stage_begin(ST_PYRAMID);
+    FSB_TRY(run_pyramid(ws, d_img, stride, exact, ctx->stream));
+    ctx->stage_end(ST_PYRAMID);
+    FSB_TRY(run_detect(ctx, ws, p->contrast, p->edge, max_kp));
+    return FSB_OK;
+}
+
 // detect into a workspace; the image is copied from host memory with its row stride
 static int32_t detect_into(fsb_ctx* ctx, Workspace& ws, const uint8_t* img, int h, int w, int stride,
                            const fsb_sift_params* p, int max_kp) {
     cudaStream_t s = ctx->stream;
     FSB_TRY(prepare_workspace(ws, h, w));
+    ctx->stage_begin(ST_UPLOAD);
     FSB_CUDA(cudaMemcpy2DAsync(ws.img.p, (size_t)w, img, (size_t)stride, (size_t)w, (size_t)h,
                                cudaMemcpyHostToDevice, s));
-    const bool exact = (p->flags & FSB_SIFT_EXACT_BLUR) != 0;
-    FSB_TRY(run_pyramid(ws, ws.img.as<uint8_t>(), w, exact, s));
-    FSB_TRY(run_detect(ws, p->contrast, p->edge, max_kp, s));
-    return FSB_OK;
+    ctx->stage_end(ST_UPLOAD);
+    return detect_dev(ctx, ws, ws.img.as<uint8_t>(), w, p, max_kp);
 }
 
+// selected keypoints -> describe inputs (tx..tly) and optional interleaved xy / response outputs
 __global__ void k_take(const int32_t* __restrict__ sel, int n, const float* x, const float* y, const float* sz,
                        const float* an, const float* rs, const int32_t* oc, const int32_t* ly, float* ox, float* oy,
-                       float* osz, float* oan, float* ors, int32_t* ooc, int32_t* oly) {
+                       float* osz, float* oan, float* ors, int32_t* ooc, int32_t* oly, float* oxy, float* oresp) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     const int k = sel[i];
     ox[i] = x[k]; oy[i] = y[k]; osz[i] = sz[k]; oan[i] = an[k]; ors[i] = rs[k]; ooc[i] = oc[k]; oly[i] = ly[k];
+    if (oxy) { oxy[2 * i] = x[k]; oxy[2 * i + 1] = y[k]; }
+    if (oresp) oresp[i] = rs[k];
 }
 
+// features.sift_gpu after detection: spread, stable response order, describe; device outputs
+// (d_xy n*2 interleaved, d_resp, d_desc, d_u8; each nullable). *n_out = 0 below 10 keypoints.
+static int32_t features_dev(fsb_ctx* ctx, Workspace& ws, int nfeat, bool exact, float* d_xy, float* d_resp,
+                            float* d_desc, uint8_t* d_u8, int* n_out) {
+    cudaStream_t s = ctx->stream;
+    *n_out = 0;
+    if (ws.n_kp < 10) return FSB_OK;
+    FSB_TRY(ctx->s_i64.ensure((size_t)ws.n_kp * 4 + 256));
+    int32_t* sel = ctx->s_i64.as<int32_t>();
+    int n_sel = 0;
+    ctx->stage_begin(ST_SPREAD);
+    FSB_TRY(run_spread(ws, nfeat, sel, &n_sel, ctx, s));
+    if (n_sel == 0) return FSB_OK;
+    FSB_TRY(ctx->s_f32a.ensure((size_t)n_sel * 4 * 7 + 256));
+    float* tx = ctx->s_f32a.as<float>();
+    float* ty = tx + n_sel;
+    float* tsz = ty + n_sel;
+    float* tan_ = tsz + n_sel;
+    float* trs = tan_ + n_sel;
+    int32_t* toc = reinterpret_cast<int32_t*>(trs + n_sel);
+    int32_t* tly = toc + n_sel;
+    k_take<<<(n_sel + 255) / 256, 256, 0, s>>>(sel, n_sel, ws.kx.as<float>(), ws.ky.as<float>(),
+                                               ws.ksize.as<float>(), ws.kangle.as<float>(), ws.kresp.as<float>(),
+                                               ws.koct.as<int32_t>(), ws.klayer.as<int32_t>(), tx, ty, tsz, tan_,
+                                               trs, toc, tly, d_xy, d_resp);
+    note_launch();
+    FSB_CUDA(cudaGetLastError());
+    ctx->stage_end(ST_SPREAD);
+    ctx->stage_begin(ST_DESCRIBE);
+    FSB_TRY(run_describe_mode(ws, n_sel, tx, ty, tsz, tan_, toc, tly, d_desc, d_u8, exact, s));
+    ctx->stage_end(ST_DESCRIBE);
+    *n_out = n_sel;
+    return FSB_OK;
+}
+
+static std::atomic<long long> g_launches{0};
+
 }  // namespace fsb
+
+void fsb::note_launch(int n) { fsb::g_launches.fetch_add(n, std::memory_order_relaxed); }
+
+void fsb_ctx::stage_begin(int st) {
+    if (!timing) return;
+    cudaEventRecord(ev[2 * st], stream);
+    ev_open[st] = true;
+}
+
+void fsb_ctx::stage_end(int st) {
+    if (!timing || !ev_open[st]) return;
+    cudaEventRecord(ev[2 * st + 1], stream);
+    cudaEventSynchronize(ev[2 * st + 1]);
+    float ms = 0.f;
+    if (cudaEventElapsedTime(&ms, ev[2 * st], ev[2 * st + 1]) == cudaSuccess) {
+        stage_ms[st] += ms;
+        stage_n[st] += 1;
+    }
+    ev_open[st] = false;
+}
 
 using namespace fsb;
 
@@ -182,6 +253,8 @@ int32_t fsb_destroy(fsb_ctx* ctx) {
                      &ctx->s_u64, &ctx->s_misc, &ctx->s_misc2, &ctx->s_host_stage, &ctx->s_cub};
     for (DevBuf* b : all) b->release();
     if (ctx->pinned) cudaFreeHost(ctx->pinned);
+    for (auto& e : ctx->ev)
+        if (e) cudaEventDestroy(e);
     cudaStreamDestroy(ctx->stream);
     delete ctx;
     return FSB_OK;
@@ -342,6 +415,7 @@ int32_t fsb_sift_features(fsb_ctx* ctx, const uint8_t* img, int32_t h, int32_t w
                           uint8_t* rootsift, int32_t* n_out) {
     FSB_ARG(ctx && img && p && n_out, "null pointer");
     FSB_ARG(h > 0 && w > 0 && stride >= w, "bad image size or stride");
+    FSB_ARG(h <= 32768 && w <= 32768, "image larger than 32768 pixels on a side");
     FSB_ARG(nfeat >= 0, "nfeat < 0");
     *n_out = 0;
     FSB_TRY(use_device(ctx));
@@ -354,43 +428,128 @@ int32_t fsb_sift_features(fsb_ctx* ctx, const uint8_t* img, int32_t h, int32_t w
     } guard{ctx, ws};
     const int max_kp = (int)((double)nfeat * 2.2);
     FSB_TRY(detect_into(ctx, *ws, img, h, w, stride, p, max_kp));
-    if (ws->n_kp < 10) {
-        FSB_CUDA(cudaStreamSynchronize(s));
-        return FSB_OK;
+    const size_t cap = (size_t)(nfeat > 0 ? nfeat : 1);
+    FSB_TRY(ctx->s_f32b.ensure(cap * (128 * 4 + 12) + 1024));
+    FSB_TRY(ctx->s_u8a.ensure(cap * 128 + 256));
+    float* dd = ctx->s_f32b.as<float>();
+    float* dxy = dd + cap * 128;
+    float* drs = dxy + cap * 2;
+    int n = 0;
+    FSB_TRY(features_dev(ctx, *ws, nfeat, (p->flags & FSB_SIFT_EXACT_BLUR) != 0, dxy, drs, desc ? dd : nullptr,
+                         rootsift ? ctx->s_u8a.as<uint8_t>() : nullptr, &n));
+    if (n) {
+        if (xy) FSB_CUDA(cudaMemcpyAsync(xy, dxy, (size_t)n * 8, cudaMemcpyDeviceToHost, s));
+        if (resp) FSB_CUDA(cudaMemcpyAsync(resp, drs, (size_t)n * 4, cudaMemcpyDeviceToHost, s));
+        if (desc) FSB_CUDA(cudaMemcpyAsync(desc, dd, (size_t)n * 512, cudaMemcpyDeviceToHost, s));
+        if (rootsift) FSB_CUDA(cudaMemcpyAsync(rootsift, ctx->s_u8a.p, (size_t)n * 128, cudaMemcpyDeviceToHost, s));
     }
-    FSB_TRY(ctx->s_i64.ensure((size_t)ws->n_kp * 4 + 256));
-    int32_t* sel = ctx->s_i64.as<int32_t>();
-    int n_sel = 0;
-    FSB_TRY(run_spread(*ws, nfeat, sel, &n_sel, ctx, s));
-    if (n_sel == 0) return FSB_OK;
-    FSB_TRY(ctx->s_f32a.ensure((size_t)n_sel * 4 * 7 + 256));
-    float* tx = ctx->s_f32a.as<float>();
-    float* ty = tx + n_sel;
-    float* tsz = ty + n_sel;
-    float* tan_ = tsz + n_sel;
-    float* trs = tan_ + n_sel;
-    int32_t* toc = reinterpret_cast<int32_t*>(trs + n_sel);
-    int32_t* tly = toc + n_sel;
-    k_take<<<(n_sel + 255) / 256, 256, 0, s>>>(sel, n_sel, ws->kx.as<float>(), ws->ky.as<float>(),
-                                               ws->ksize.as<float>(), ws->kangle.as<float>(), ws->kresp.as<float>(),
-                                               ws->koct.as<int32_t>(), ws->klayer.as<int32_t>(), tx, ty, tsz, tan_,
-                                               trs, toc, tly);
-    FSB_CUDA(cudaGetLastError());
-    FSB_TRY(ctx->s_f32b.ensure((size_t)n_sel * 128 * 4 + 256));
-    FSB_TRY(ctx->s_u8a.ensure((size_t)n_sel * 128 + 256));
-    float* dd = desc ? ctx->s_f32b.as<float>() : nullptr;
-    uint8_t* du = rootsift ? ctx->s_u8a.as<uint8_t>() : nullptr;
-    const bool exact = (p->flags & FSB_SIFT_EXACT_BLUR) != 0;
-    FSB_TRY(run_describe_mode(*ws, n_sel, tx, ty, tsz, tan_, toc, tly, dd, du, exact, s));
-    if (xy) {
-        FSB_CUDA(cudaMemcpy2DAsync(xy, 8, tx, 4, 4, n_sel, cudaMemcpyDeviceToHost, s));
-        FSB_CUDA(cudaMemcpy2DAsync(xy + 1, 8, ty, 4, 4, n_sel, cudaMemcpyDeviceToHost, s));
-    }
-    if (resp) FSB_CUDA(cudaMemcpyAsync(resp, trs, (size_t)n_sel * 4, cudaMemcpyDeviceToHost, s));
-    if (desc) FSB_CUDA(cudaMemcpyAsync(desc, dd, (size_t)n_sel * 512, cudaMemcpyDeviceToHost, s));
-    if (rootsift) FSB_CUDA(cudaMemcpyAsync(rootsift, du, (size_t)n_sel * 128, cudaMemcpyDeviceToHost, s));
     FSB_CUDA(cudaStreamSynchronize(s));
-    *n_out = n_sel;
+    *n_out = n;
+    return FSB_OK;
+}
+
+int32_t fsb_sift_features_d(fsb_ctx* ctx, const uint8_t* d_img, int32_t h, int32_t w, int32_t stride,
+                            const fsb_sift_params* p, int32_t nfeat, float* d_xy, float* d_resp, float* d_desc,
+                            uint8_t* d_rootsift, int32_t* n_out) {
+    FSB_ARG(ctx && d_img && p && n_out, "null pointer");
+    FSB_ARG(h > 0 && w > 0 && stride >= w, "bad image size or stride");
+    FSB_ARG(h <= 32768 && w <= 32768, "image larger than 32768 pixels on a side");
+    FSB_ARG(nfeat >= 0, "nfeat < 0");
+    *n_out = 0;
+    FSB_TRY(use_device(ctx));
+    Workspace* ws = acquire(ctx);
+    struct Guard {
+        fsb_ctx* c;
+        Workspace* w;
+        ~Guard() { give_back(c, w); }
+    } guard{ctx, ws};
+    FSB_TRY(prepare_workspace(*ws, h, w));
+    FSB_TRY(detect_dev(ctx, *ws, d_img, stride, p, (int)((double)nfeat * 2.2)));
+    int n = 0;
+    FSB_TRY(features_dev(ctx, *ws, nfeat, (p->flags & FSB_SIFT_EXACT_BLUR) != 0, d_xy, d_resp, d_desc, d_rootsift,
+                         &n));
+    FSB_CUDA(cudaStreamSynchronize(ctx->stream));
+    *n_out = n;
+    return FSB_OK;
+}
+
+int32_t fsb_project_d(fsb_ctx* ctx, const float* d_xy, int32_t n, const double* hm9, const float* d_offset,
+                      double* d_out) {
+    FSB_ARG(ctx && hm9, "null pointer");
+    FSB_ARG(n >= 0 && (n == 0 || (d_xy && d_out)), "bad points");
+    if (n == 0) return FSB_OK;
+    FSB_TRY(use_device(ctx));
+    FSB_TRY(run_project(d_xy, n, hm9, d_offset, d_out, ctx->stream));
+    FSB_CUDA(cudaStreamSynchronize(ctx->stream));
+    return FSB_OK;
+}
+
+int32_t fsb_match_guided_d(fsb_ctx* ctx, const double* d_pred, const uint8_t* d_a, int32_t na, const double* d_bxy,
+                           const uint8_t* d_b, int32_t nb, double w_b, double h_b, double radius, int32_t kc,
+                           float ratio, int64_t* d_q, int64_t* d_t, int32_t* n_out) {
+    FSB_ARG(ctx && n_out, "null pointer");
+    FSB_ARG(na >= 0 && nb >= 0, "negative size");
+    FSB_ARG((na == 0 || (d_a && d_pred && d_q && d_t)) && (nb == 0 || (d_b && d_bxy)), "null array");
+    FSB_ARG(std::isfinite(radius) && std::isfinite(w_b) && std::isfinite(h_b), "non-finite frame or radius");
+    *n_out = 0;
+    if (na == 0 || nb == 0 || !(radius > 0.0)) return FSB_OK;
+    FSB_TRY(use_device(ctx));
+    cudaStream_t s = ctx->stream;
+    FSB_TRY(ctx->s_misc2.ensure(64));
+    int* dn = ctx->s_misc2.as<int>();
+    ctx->stage_begin(ST_MATCH);
+    FSB_TRY(run_match_guided(ctx, d_pred, d_a, na, d_bxy, d_b, nb, w_b, h_b, radius, kc, ratio, d_q, d_t, dn, s));
+    int n = 0;
+    FSB_CUDA(cudaMemcpyAsync(&n, dn, sizeof(int), cudaMemcpyDeviceToHost, s));
+    FSB_CUDA(cudaStreamSynchronize(s));
+    ctx->stage_end(ST_MATCH);
+    *n_out = n;
+    return FSB_OK;
+}
+
+int32_t fsb_match_bf_d(fsb_ctx* ctx, const uint8_t* d_a, int32_t na, const uint8_t* d_b, int32_t nb, float ratio,
+                       int32_t precision, int64_t* d_q, int64_t* d_t, int32_t* n_out) {
+    FSB_ARG(ctx && n_out, "null pointer");
+    FSB_ARG(na >= 0 && nb >= 0, "negative size");
+    FSB_ARG((na == 0 || (d_a && d_q && d_t)) && (nb == 0 || d_b), "null array");
+    FSB_ARG(precision >= FSB_PREC_FP32 && precision <= FSB_PREC_FP8, "unknown precision");
+    *n_out = 0;
+    if (na < 2 || nb < 2) return FSB_OK;
+    FSB_TRY(use_device(ctx));
+    cudaStream_t s = ctx->stream;
+    FSB_TRY(ctx->s_misc2.ensure(64));
+    int* dn = ctx->s_misc2.as<int>();
+    ctx->stage_begin(ST_MATCH);
+    FSB_TRY(run_match_bf(ctx, d_a, na, d_b, nb, ratio, precision, d_q, d_t, dn, s));
+    int n = 0;
+    FSB_CUDA(cudaMemcpyAsync(&n, dn, sizeof(int), cudaMemcpyDeviceToHost, s));
+    FSB_CUDA(cudaStreamSynchronize(s));
+    ctx->stage_end(ST_MATCH);
+    *n_out = n;
+    return FSB_OK;
+}
+
+int64_t fsb_launch_count(void) { return fsb::g_launches.load(); }
+
+int32_t fsb_timing(fsb_ctx* ctx, int32_t on) {
+    FSB_ARG(ctx, "ctx is null");
+    FSB_TRY(use_device(ctx));
+    if (on && !ctx->ev[0])
+        for (auto& e : ctx->ev) FSB_CUDA(cudaEventCreate(&e));
+    ctx->timing = on != 0;
+    return FSB_OK;
+}
+
+int32_t fsb_stage_times(fsb_ctx* ctx, double* ms, int64_t* calls, int32_t n) {
+    FSB_ARG(ctx && n >= 0, "bad arguments");
+    for (int i = 0; i < n && i < ST_COUNT; ++i) {
+        if (ms) ms[i] = ctx->stage_ms[i];
+        if (calls) calls[i] = ctx->stage_n[i];
+    }
+    for (int i = 0; i < ST_COUNT; ++i) {
+        ctx->stage_ms[i] = 0.0;
+        ctx->stage_n[i] = 0;
+    }
     return FSB_OK;
 }
 

@@ -514,17 +514,21 @@ DetectConsts make_consts(const Geometry& g, double contrast, double edge) {
 }  // namespace
 
 // Full detection pipeline; contrast/edge in double as the reference's Python floats.
-int32_t run_detect(Workspace& ws, double contrast, double edge, int max_kp, cudaStream_t s) {
+int32_t run_detect(fsb_ctx* ctx, Workspace& ws, double contrast, double edge, int max_kp) {
+    cudaStream_t s = ctx->stream;
     const Geometry& g = ws.g;
     const DetectConsts k = make_consts(g, contrast, edge);
     uint32_t* cnt = ws.counters.as<uint32_t>();
     const float* DF = ws.dog.as<float>();
     uint32_t h_cnt[3];
+    ctx->stage_begin(ST_EXTREMA);
     for (int attempt = 0; attempt < 3; ++attempt) {
         FSB_CUDA(cudaMemsetAsync(cnt, 0, 3 * sizeof(uint32_t), s));
         const long long nvox = k.vox_off[g.n_oct];
-        if (nvox > 0)
+        if (nvox > 0) {
             k_extrema<<<blocks(nvox, 256), 256, 0, s>>>(DF, k, ws.cand.as<uint32_t>(), cnt, (uint32_t)ws.cap_cand);
+            note_launch();
+        }
         FSB_CUDA(cudaGetLastError());
         FSB_CUDA(cudaMemcpyAsync(h_cnt, cnt, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
         FSB_CUDA(cudaStreamSynchronize(s));
@@ -532,20 +536,25 @@ int32_t run_detect(Workspace& ws, double contrast, double edge, int max_kp, cuda
         ws.cap_cand = (size_t)h_cnt[0] + (h_cnt[0] >> 3) + 1024;
         FSB_TRY(ws.cand.ensure(ws.cap_cand * sizeof(uint32_t)));
     }
+    ctx->stage_end(ST_EXTREMA);
     const uint32_t n_cand = h_cnt[0];
     if (n_cand == 0) { ws.n_kp = 0; return FSB_OK; }
     if (ws.cap_ref < n_cand) {
         ws.cap_ref = n_cand;
         FSB_TRY(ws.refined.ensure(ws.cap_ref * sizeof(Refined)));
     }
+    ctx->stage_begin(ST_REFINE);
     k_refine<<<blocks(n_cand, 128), 128, 0, s>>>(DF, k, ws.cand.as<uint32_t>(), cnt, (uint32_t)ws.cap_cand,
                                                  ws.refined.as<Refined>(), cnt + 1, (uint32_t)ws.cap_ref);
+    note_launch();
     FSB_CUDA(cudaGetLastError());
     FSB_CUDA(cudaMemcpyAsync(h_cnt + 1, cnt + 1, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
     FSB_CUDA(cudaStreamSynchronize(s));
+    ctx->stage_end(ST_REFINE);
     const uint32_t n_ref = h_cnt[1];
     if (n_ref == 0) { ws.n_kp = 0; return FSB_OK; }
     uint32_t n_ori = 0;
+    ctx->stage_begin(ST_ORIENT);
     for (int attempt = 0; attempt < 3; ++attempt) {
         if (ws.cap_ori < (size_t)n_ref * 2 + 1024) ws.cap_ori = (size_t)n_ref * 2 + 1024;
         FSB_TRY(ws.oriented.ensure(ws.cap_ori * sizeof(Oriented)));
@@ -554,6 +563,7 @@ int32_t run_detect(Workspace& ws, double contrast, double edge, int max_kp, cuda
         k_orient<<<ob < 148 * 16 ? ob : 148 * 16, ORI_WARPS * 32, 0, s>>>(
             ws.mag.as<float>(), ws.ang.as<float>(), k, ws.refined.as<Refined>(), cnt + 1, (uint32_t)ws.cap_ref,
             ws.oriented.as<Oriented>(), cnt + 2, (uint32_t)ws.cap_ori);
+        note_launch();
         FSB_CUDA(cudaGetLastError());
         FSB_CUDA(cudaMemcpyAsync(h_cnt + 2, cnt + 2, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
         FSB_CUDA(cudaStreamSynchronize(s));
@@ -561,8 +571,10 @@ int32_t run_detect(Workspace& ws, double contrast, double edge, int max_kp, cuda
         if (n_ori <= ws.cap_ori) break;
         ws.cap_ori = (size_t)n_ori + 1024;
     }
+    ctx->stage_end(ST_ORIENT);
     if (n_ori > ws.cap_ori) { set_error("orientation list overflow"); return FSB_ERR_OVERFLOW; }
     if (n_ori == 0) { ws.n_kp = 0; return FSB_OK; }
+    ctx->stage_begin(ST_SORT);
     // stable two-key sort: (extremum index, bin) ascending, then response descending
     FSB_TRY(ws.keys_a.ensure((size_t)n_ori * 8 * 2));
     FSB_TRY(ws.vals_a.ensure((size_t)n_ori * 4 * 2));
@@ -600,7 +612,9 @@ int32_t run_detect(Workspace& ws, double contrast, double edge, int max_kp, cuda
                                                      ws.kx.as<float>(), ws.ky.as<float>(), ws.ksize.as<float>(),
                                                      ws.kangle.as<float>(), ws.kresp.as<float>(), ws.koct.as<int32_t>(),
                                                      ws.klayer.as<int32_t>());
+    note_launch(n_keep ? 3 : 2);
     FSB_CUDA(cudaGetLastError());
+    ctx->stage_end(ST_SORT);
     ws.n_kp = (int)n_keep;
     return FSB_OK;
 }
@@ -617,6 +631,7 @@ int32_t run_describe_mode(const Workspace& ws, int n, const float* d_x, const fl
     else
         k_describe<false><<<grid, DESC_WARPS * 32, 0, s>>>(ws.mag.as<float>(), ws.ang.as<float>(), ws.g, n, d_x, d_y,
                                                            d_size, d_angle, d_oct, d_layer, d_desc, d_u8);
+    note_launch();
     FSB_CUDA(cudaGetLastError());
     return FSB_OK;
 }
@@ -685,6 +700,7 @@ int32_t run_spread(const Workspace& ws, int nfeat, int32_t* d_sel_out, int* n_se
     }
     // stable sort of the selection by response, descending (features.py:126)
     k_resp_keys<<<blocks(nfeat, 256), 256, 0, s>>>(sel2, nfeat, ws.kresp.as<float>(), keyb);
+    note_launch(n1 < nfeat ? 5 : 3);
     tb = tmax;
     FSB_CUDA(cub::DeviceRadixSort::SortPairs(tmp, tb, keyb, keyb + N, sel2, sel, nfeat, 0, 32, s));
     FSB_CUDA(cudaGetLastError());

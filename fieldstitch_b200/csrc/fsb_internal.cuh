@@ -16,6 +16,13 @@ namespace fsb {
 // ---------------------------------------------------------------------------------- errors
 void set_error(const char* fmt, ...);
 
+// Count of kernel launches issued by this library (observability; read by fsb_launch_count).
+void note_launch(int n = 1);
+
+// Per-stage device timers (CUDA events on the context stream), enabled by fsb_timing().
+enum Stage { ST_UPLOAD = 0, ST_PYRAMID, ST_EXTREMA, ST_REFINE, ST_ORIENT, ST_SORT, ST_SPREAD, ST_DESCRIBE,
+             ST_MATCH, ST_COUNT };
+
 #define FSB_CUDA(call)                                                                      \
     do {                                                                                    \
         cudaError_t e_ = (call);                                                            \
@@ -118,6 +125,14 @@ struct fsb_ctx {
     fsb::DevBuf s_cub;   // CUB temporary storage (one primitive at a time)
     void* pinned = nullptr;
     size_t pinned_bytes = 0;
+    // stage timers: events recorded at stage boundaries while timing is on
+    bool timing = false;
+    cudaEvent_t ev[2 * fsb::ST_COUNT] = {};
+    bool ev_open[fsb::ST_COUNT] = {};
+    double stage_ms[fsb::ST_COUNT] = {};
+    long long stage_n[fsb::ST_COUNT] = {};
+    void stage_begin(int st);
+    void stage_end(int st);    // synchronises on the end event and accumulates
 };
 
 struct fsb_state {
@@ -135,7 +150,7 @@ int32_t upload_taps();
 int32_t run_pyramid(Workspace& ws, const uint8_t* d_img, int img_stride, bool exact, cudaStream_t s);
 
 // ---------------------------------------------------------------- detect.cu
-int32_t run_detect(Workspace& ws, double contrast, double edge, int max_kp, cudaStream_t s);
+int32_t run_detect(fsb_ctx* ctx, Workspace& ws, double contrast, double edge, int max_kp);
 int32_t run_describe_mode(const Workspace& ws, int n, const float* d_x, const float* d_y, const float* d_size,
                           const float* d_angle, const int32_t* d_oct, const int32_t* d_layer, float* d_desc,
                           uint8_t* d_u8, bool exact, cudaStream_t s);
@@ -151,6 +166,8 @@ int32_t run_match_guided(fsb_ctx* ctx, const double* d_pred, const uint8_t* d_a,
                          const uint8_t* d_b, int nb, double wb, double hb, double radius, int kc, float ratio,
                          int64_t* d_q, int64_t* d_t, int* d_n, cudaStream_t s);
 int32_t run_perspective(const double* d_xy, int n, const double* hm9, double* d_out, cudaStream_t s);
+int32_t run_project(const float* d_xy, int n, const double* hm9_host, const float* d_off, double* d_out,
+                    cudaStream_t s);
 int32_t run_unique_general(fsb_ctx* ctx, const int64_t* d_q, const int64_t* d_t, const float* d_dd, int n,
                            int64_t* d_qo, int64_t* d_to, int* d_n, cudaStream_t s);
 

@@ -379,6 +379,7 @@ int32_t run_unique(fsb_ctx* ctx, const int32_t* t_row, const uint32_t* d_row, in
     FSB_TRY(ctx->s_cub.ensure(tb + 16));
     FSB_CUDA(cub::DeviceSelect::Flagged(ctx->s_cub.p, tb, iota, flag, tsel, d_n, nb, s));
     k_unique_emit<<<blocks(nb, 256), 256, 0, s>>>(key, tsel, d_n, d_q, d_t);
+    note_launch(4);
     FSB_CUDA(cudaGetLastError());
     return FSB_OK;
 }
@@ -451,6 +452,43 @@ int32_t run_unique_general(fsb_ctx* ctx, const int64_t* d_q, const int64_t* d_t,
     tb = tmax;
     FSB_CUDA(cub::DeviceSelect::Flagged(ctx->s_cub.p, tb, v2o, flag, sel, d_n, n, s));
     k_uq_emit<<<blocks(n, 256), 256, 0, s>>>(sel, d_n, d_q, d_t, d_qo, d_to);
+    note_launch(4);
+    FSB_CUDA(cudaGetLastError());
+    return FSB_OK;
+}
+
+struct H9 {
+    double h[9];
+};
+
+// float32 points -> float64 positions through a homography, plus optional float32 offsets
+__global__ void k_project(const float* __restrict__ xy, int n, H9 H, const float* __restrict__ off,
+                          double* __restrict__ out) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const double x = (double)xy[2 * i], y = (double)xy[2 * i + 1];
+    const double* hm = H.h;
+    double w = __dadd_rn(__dadd_rn(__dmul_rn(hm[6], x), __dmul_rn(hm[7], y)), hm[8]);
+    double u = 0.0, v = 0.0;
+    if (fabs(w) > 1.1920928955078125e-07) {
+        w = 1.0 / w;
+        u = __dmul_rn(__dadd_rn(__dadd_rn(__dmul_rn(hm[0], x), __dmul_rn(hm[1], y)), hm[2]), w);
+        v = __dmul_rn(__dadd_rn(__dadd_rn(__dmul_rn(hm[3], x), __dmul_rn(hm[4], y)), hm[5]), w);
+    }
+    if (off) {
+        u += (double)off[2 * i];
+        v += (double)off[2 * i + 1];
+    }
+    out[2 * i] = u;
+    out[2 * i + 1] = v;
+}
+
+int32_t run_project(const float* d_xy, int n, const double* hm9, const float* d_off, double* d_out, cudaStream_t s) {
+    if (n <= 0) return FSB_OK;
+    H9 H;
+    for (int i = 0; i < 9; ++i) H.h[i] = hm9[i];
+    k_project<<<blocks(n, 256), 256, 0, s>>>(d_xy, n, H, d_off, d_out);
+    note_launch();
     FSB_CUDA(cudaGetLastError());
     return FSB_OK;
 }
@@ -458,6 +496,7 @@ int32_t run_unique_general(fsb_ctx* ctx, const int64_t* d_q, const int64_t* d_t,
 int32_t run_perspective(const double* d_xy, int n, const double* d_hm9, double* d_out, cudaStream_t s) {
     if (n <= 0) return FSB_OK;
     k_perspective<<<blocks(n, 256), 256, 0, s>>>(d_xy, n, d_hm9, d_out);
+    note_launch();
     FSB_CUDA(cudaGetLastError());
     return FSB_OK;
 }
@@ -489,6 +528,7 @@ int32_t run_match_bf(fsb_ctx* ctx, const uint8_t* d_a, int na, const uint8_t* d_
     k_norms<<<blocks(nb, 8), 256, 0, s>>>(d_b, nb, nB);
     k_bf_fp32<<<dim3(row_blocks, splits), BF_THREADS, 0, s>>>(d_a, na, d_b, nb, nA, nB, split_len, part);
     k_bf_merge<<<blocks(na, 256), 256, 0, s>>>(part, na, splits, ratio, t_row, d_row);
+    note_launch(4);
     FSB_CUDA(cudaGetLastError());
     return run_unique(ctx, t_row, d_row, na, nb, d_q, d_t, d_n, s);
 }
@@ -534,6 +574,7 @@ int32_t run_match_guided(fsb_ctx* ctx, const double* d_pred, const uint8_t* d_a,
     FSB_TRY(ctx->s_cub.ensure(tb + 16));
     FSB_CUDA(cub::DeviceScan::ExclusiveSum(ctx->s_cub.p, tb, count, start, ncell + 1, s));
     k_grid_fill<<<blocks(nb, 256), 256, 0, s>>>(cell, nb, start, cursor, items);
+    note_launch(5);
     k_guided<<<blocks(na, G_WARPS), G_WARPS * 32, 0, s>>>(d_pred, d_a, na, d_bxy, d_b, nb, nA, nB, gs, start, items,
                                                           wb, hb, radius, kc, ratio, t_row, d_row, overflow);
     FSB_CUDA(cudaGetLastError());

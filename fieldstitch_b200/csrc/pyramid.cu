@@ -197,6 +197,7 @@ void launch(bool exact, const BlurArgs& a, cudaStream_t s) {
         k_blur<TS, RAD, true, BASE><<<grid, NT, 0, s>>>(a);
     else
         k_blur<TS, RAD, false, BASE><<<grid, NT, 0, s>>>(a);
+    note_launch();
 }
 
 }  // namespace

@@ -90,6 +90,21 @@ def synth_pair(h, w, seed):
     return a, b, H
 
 
+def flight_pair(args):
+    """One pair of the batched guided-matching workload: (A, B, H, nfeat_A, nfeat_B) for
+    (h, w, seed). Keypoint caps are drawn uniformly from [2000, 16000]."""
+    h, w, seed = args
+    a, b, H = synth_pair(h, w, seed)
+    rng = np.random.default_rng(seed + 104729)
+    na, nb = (int(v) for v in rng.integers(2000, 16001, 2))
+    return a, b, H, na, nb
+
+
+def prior_noise(n, seed, sigma=15.0):
+    """Gaussian prior error (n, 2) float32 in pixels (GNSS/gimbal prior sigma)."""
+    return np.random.default_rng(seed + 1299709).normal(0.0, sigma, (n, 2)).astype(np.float32)
+
+
 def apply_homography(H, xy):
     """Project (n, 2) points by a 3x3 homography (float64)."""
     xy = np.asarray(xy, np.float64)

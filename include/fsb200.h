@@ -62,6 +62,24 @@ int32_t fsb_sync(fsb_ctx* ctx, int32_t timeout_ms);
 void* fsb_stream(fsb_ctx* ctx);
 /* Bytes of device memory the context holds (workspaces and scratch). */
 int64_t fsb_device_bytes(fsb_ctx* ctx);
+/* Number of kernel launches this library has issued in the process (all contexts). */
+int64_t fsb_launch_count(void);
+/* Per-stage device timing, the counterpart of gsift.detect(timings=dict)
+   (app/planesite/gsift.py:441-446): while on, CUDA events bracket each stage on the context
+   stream. fsb_stage_times copies the accumulated milliseconds and call counts of the FSB_STAGE_*
+   stages (n entries each, nullable) and resets them. */
+int32_t fsb_timing(fsb_ctx* ctx, int32_t on);
+int32_t fsb_stage_times(fsb_ctx* ctx, double* ms, int64_t* calls, int32_t n);
+#define FSB_STAGE_UPLOAD 0
+#define FSB_STAGE_PYRAMID 1
+#define FSB_STAGE_EXTREMA 2
+#define FSB_STAGE_REFINE 3
+#define FSB_STAGE_ORIENT 4
+#define FSB_STAGE_SORT 5
+#define FSB_STAGE_SPREAD 6
+#define FSB_STAGE_DESCRIBE 7
+#define FSB_STAGE_MATCH 8
+#define FSB_STAGE_COUNT 9
 
 /* ---- SIFT detection / description ---------------------------------------------------------- */
 /* gsift.detect (app/planesite/gsift.py:435-477): 2x upsample, Gaussian/DoG pyramid, 3x3x3
@@ -94,6 +112,29 @@ int32_t fsb_state_free(fsb_state* st);
 int32_t fsb_sift_features(fsb_ctx* ctx, const uint8_t* img, int32_t h, int32_t w, int32_t stride,
                           const fsb_sift_params* p, int32_t nfeat, float* xy, float* resp,
                           float* desc, uint8_t* rootsift, int32_t* n_out);
+
+/* ---- device-pointer variants ---------------------------------------------------------------
+   Same computations with inputs and outputs in device memory of the context's device (the
+   caller keeps them resident across calls); counts are returned to the host and the call returns
+   once its outputs are written. */
+/* fsb_sift_features on an image in device memory. d_xy (nfeat*2), d_resp (nfeat),
+   d_desc (nfeat*128 float32) and d_rootsift (nfeat*128 uint8) are device pointers (nullable). */
+int32_t fsb_sift_features_d(fsb_ctx* ctx, const uint8_t* d_img, int32_t h, int32_t w, int32_t stride,
+                            const fsb_sift_params* p, int32_t nfeat, float* d_xy, float* d_resp,
+                            float* d_desc, uint8_t* d_rootsift, int32_t* n_out);
+/* Prior prediction: projects n float32 points (d_xy, n*2) through the homography hm9 (host,
+   row-major 3x3) into float64 positions d_out (n*2), adding the float32 offsets d_offset (n*2,
+   nullable) - e.g. a GNSS/gimbal prior and its error. Identity hm9 converts to float64. */
+int32_t fsb_project_d(fsb_ctx* ctx, const float* d_xy, int32_t n, const double* hm9,
+                      const float* d_offset, double* d_out);
+/* fsb_match_guided with every array in device memory; d_q, d_t capacity na. */
+int32_t fsb_match_guided_d(fsb_ctx* ctx, const double* d_pred, const uint8_t* d_a, int32_t na,
+                           const double* d_bxy, const uint8_t* d_b, int32_t nb, double w_b, double h_b,
+                           double radius, int32_t kc, float ratio, int64_t* d_q, int64_t* d_t,
+                           int32_t* n_out);
+/* fsb_match_bf with every array in device memory; d_q, d_t capacity na. */
+int32_t fsb_match_bf_d(fsb_ctx* ctx, const uint8_t* d_a, int32_t na, const uint8_t* d_b, int32_t nb,
+                       float ratio, int32_t precision, int64_t* d_q, int64_t* d_t, int32_t* n_out);
 
 /* ---- matching ------------------------------------------------------------------------------- */
 /* matching._ratio_match_bf + _unique (app/planesite/matching.py:86-110) on uint8 descriptors
