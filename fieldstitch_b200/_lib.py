@@ -53,6 +53,7 @@ SIGNATURES = [
     ("fsb_match_guided_d", c_i32, [c_vp, c_vp, c_vp, c_i32, c_vp, c_vp, c_i32, c_f64, c_f64, c_f64, c_i32, c_f32,
                                    c_vp, c_vp, c_vp]),
     ("fsb_match_bf_d", c_i32, [c_vp, c_vp, c_i32, c_vp, c_i32, c_f32, c_i32, c_vp, c_vp, c_vp]),
+    ("fsb_match_bf_noalloc", c_i32, [c_vp, c_i32, c_vp, c_i32, c_f32, c_vp, c_vp, c_vp, c_vp]),
 ]
 
 STAGES = ("upload", "pyramid", "extrema", "refine", "orientation", "sort", "spread", "describe", "match")

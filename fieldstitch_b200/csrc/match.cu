@@ -15,6 +15,8 @@
 // on the values and the tie rules, which follow the reference.
 #include <cub/cub.cuh>
 
+#include <mutex>
+
 #include "fsb_internal.cuh"
 
 namespace fsb {
@@ -589,3 +591,131 @@ int32_t run_match_guided(fsb_ctx* ctx, const double* d_pred, const uint8_t* d_a,
 }
 
 }  // namespace fsb
+
+// ---------------------------------------------------------------------------------------------
+// Allocation-free dense ratio matcher (fsb_match_bf_noalloc).
+//
+// Some callers cannot call cudaMalloc: services that reserve their whole device-memory budget
+// when they start (a fixed pool handed to them by a host application, as in multi-tenant
+// serving), host frameworks that own the CUDA allocator and forbid allocations behind their back,
+// and real-time loops where an allocation may block or fail in the middle of a frame. For them
+// this entry point runs the FP32 dense matcher with all of its scratch in one file-scope device
+// array of fixed size (kNoAllocScratchBytes, about 1.9 MiB), so a call allocates nothing: the
+// caller passes device inputs and outputs and a stream.
+//
+// The array lives in every GPU that loads this library until the process exits. Host code may
+// not use its name as an address (on the host it is only a stand-in symbol), so its device
+// address is looked up once per device with cudaGetSymbolAddress, with that device current, by
+// the first call made on the device; that first call should come before any stream capture.
+// Every call shares the array and it keeps the last call's contents: the per-target key table is
+// re-filled at the start of each call, everything else is fully overwritten. Calls whose work
+// overlaps on the GPU (different streams, or host threads using the same device) race on the
+// array and must be serialised by the caller.
+namespace fsb {
+namespace {
+
+constexpr int kNoAllocMaxRows = 16384;
+constexpr int kNoAllocSplitRows = 8 * kNoAllocMaxRows;   // capacity of the per-split top-2 table
+constexpr size_t kNoAllocScratchBytes =
+    4 * sizeof(int32_t) * kNoAllocMaxRows +                // norms of A and B, best target, distance
+    sizeof(unsigned long long) * kNoAllocMaxRows +         // one-to-one keys per target
+    sizeof(Top2) * (size_t)kNoAllocSplitRows;              // per-split top-2 of every A row
+
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
+
+std::mutex g_noalloc_mu;
+void* g_noalloc_addr[256] = {};
+
+// device address of g_noalloc_scratch on the current device (looked up on first use)
+int32_t noalloc_scratch(void** out) {
+    int dev = 0;
+    FSB_CUDA(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= 256) {
+        set_error("device ordinal %d out of range", dev);
+        return FSB_ERR_ARG;
+    }
+    std::lock_guard<std::mutex> lk(g_noalloc_mu);
+    if (!g_noalloc_addr[dev]) {
+        void* p = nullptr;
+        const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+        if (e != cudaSuccess || p == nullptr) {
+            set_error("cudaGetSymbolAddress(scratch) failed on device %d: %s", dev, cudaGetErrorString(e));
+            return FSB_ERR_CUDA;
+        }
+        g_noalloc_addr[dev] = p;
+    }
+    *out = g_noalloc_addr[dev];
+    return FSB_OK;
+}
+
+// single-CTA, target-ordered compaction of the one-to-one keys (nb <= kNoAllocMaxRows)
+constexpr int kCompactThreads = 1024;
+__global__ void __launch_bounds__(kCompactThreads) k_noalloc_compact(const unsigned long long* __restrict__ key, int nb,
+                                                                      int64_t* __restrict__ q, int64_t* __restrict__ t,
+                                                                      int32_t* __restrict__ n_out) {
+    typedef cub::BlockScan<int, kCompactThreads> Scan;
+    __shared__ typename Scan::TempStorage tmp;
+    const int per = (nb + kCompactThreads - 1) / kCompactThreads;
+    const int t0 = threadIdx.x * per, t1 = min(nb, t0 + per);
+    int cnt = 0;
+    for (int i = t0; i < t1; ++i) cnt += key[i] != ~0ull;
+    int off = 0, total = 0;
+    Scan(tmp).ExclusiveSum(cnt, off, total);
+    for (int i = t0; i < t1; ++i) {
+        const unsigned long long k = key[i];
+        if (k != ~0ull) {
+            q[off] = (int64_t)(k & 0xffffffffull);
+            t[off] = i;
+            ++off;
+        }
+    }
+    if (threadIdx.x == 0) *n_out = total;
+}
+
+}  // namespace
+}  // namespace fsb
+
+extern "C" int32_t fsb_match_bf_noalloc(const uint8_t* d_a, int32_t na, const uint8_t* d_b, int32_t nb,
+                                        float ratio, int64_t* d_q, int64_t* d_t, int32_t* d_n, void* stream) {
+    using namespace fsb;
+    FSB_ARG(d_n != nullptr, "n_out is null");
+    FSB_ARG(na >= 0 && nb >= 0, "negative size");
+    if (na > kNoAllocMaxRows || nb > kNoAllocMaxRows) {
+        set_error("invalid argument: na=%d, nb=%d exceeds the %d-row limit of the allocation-free matcher "
+                  "(use fsb_match_bf_d)", na, nb, kNoAllocMaxRows);
+        return FSB_ERR_ARG;
+    }
+    FSB_ARG((na == 0 || (d_a && d_q && d_t)) && (nb == 0 || d_b), "null device array");
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    if (na < 2 || nb < 2) {
+        FSB_CUDA(cudaMemsetAsync(d_n, 0, sizeof(int32_t), s));
+        return FSB_OK;
+    }
+    void* base = nullptr;
+    FSB_TRY(noalloc_scratch(&base));
+    int32_t* nA = static_cast<int32_t*>(base);
+    int32_t* nB = nA + kNoAllocMaxRows;
+    int32_t* t_row = nB + kNoAllocMaxRows;
+    uint32_t* d_row = reinterpret_cast<uint32_t*>(t_row + kNoAllocMaxRows);
+    unsigned long long* key = reinterpret_cast<unsigned long long*>(d_row + kNoAllocMaxRows);
+    Top2* part = reinterpret_cast<Top2*>(key + kNoAllocMaxRows);
+    // same split rule as the allocating matcher, bounded by the top-2 table's capacity
+    const int row_blocks = (na + BM - 1) / BM;
+    const int max_splits = kNoAllocSplitRows / na;
+    int splits = 1;
+    while (row_blocks * splits < 2 * 148 && (nb + splits * 2 - 1) / (splits * 2) >= BN && splits * 2 <= max_splits)
+        splits *= 2;
+    int split_len = (nb + splits - 1) / splits;
+    split_len = ((split_len + BN - 1) / BN) * BN;
+    splits = (nb + split_len - 1) / split_len;
+    k_norms<<<blocks(na, 8), 256, 0, s>>>(d_a, na, nA);
+    k_norms<<<blocks(nb, 8), 256, 0, s>>>(d_b, nb, nB);
+    k_bf_fp32<<<dim3(row_blocks, splits), BF_THREADS, 0, s>>>(d_a, na, d_b, nb, nA, nB, split_len, part);
+    k_bf_merge<<<blocks(na, 256), 256, 0, s>>>(part, na, splits, ratio, t_row, d_row);
+    k_fill_u64<<<blocks(nb, 256), 256, 0, s>>>(key, nb, ~0ull);
+    k_unique_keys<<<blocks(na, 256), 256, 0, s>>>(t_row, d_row, na, key);
+    k_noalloc_compact<<<1, kCompactThreads, 0, s>>>(key, nb, d_q, d_t, d_n);
+    note_launch(7);
+    FSB_CUDA(cudaGetLastError());
+    return FSB_OK;
+}

@@ -136,6 +136,21 @@ int32_t fsb_match_guided_d(fsb_ctx* ctx, const double* d_pred, const uint8_t* d_
 int32_t fsb_match_bf_d(fsb_ctx* ctx, const uint8_t* d_a, int32_t na, const uint8_t* d_b, int32_t nb,
                        float ratio, int32_t precision, int64_t* d_q, int64_t* d_t, int32_t* n_out);
 
+/* Allocation-free variant of fsb_match_bf_d (FP32 distances), for callers that cannot call
+   cudaMalloc: processes that reserve their whole device-memory budget up front, host frameworks
+   that own the CUDA allocator, real-time loops that must not block or fail in an allocation.
+   No counterpart in the reference (PlaneSite allocates through CuPy/NumPy). All scratch lives in
+   one fixed device array inside the library (about 1.9 MiB, held on every GPU that loads the
+   library until exit); na and nb must be <= 16384, larger sizes are rejected with FSB_ERR_ARG.
+   Inputs d_a (na x 128), d_b (nb x 128) and outputs d_q, d_t (capacity na, int64) and d_n (one
+   int32, the number of pairs, ordered by target) are device pointers; the work is queued on
+   `stream` (a cudaStream_t; null = the legacy default stream) and the call does not wait for it.
+   The first call on a device looks up the array's device address (cudaGetSymbolAddress) with
+   that device current; make that first call before any stream capture. Calls share the array:
+   calls whose work can overlap on the GPU race and must be serialised by the caller. */
+int32_t fsb_match_bf_noalloc(const uint8_t* d_a, int32_t na, const uint8_t* d_b, int32_t nb, float ratio,
+                             int64_t* d_q, int64_t* d_t, int32_t* d_n, void* stream);
+
 /* ---- matching ------------------------------------------------------------------------------- */
 /* matching._ratio_match_bf + _unique (app/planesite/matching.py:86-110) on uint8 descriptors
    (na x 128, nb x 128, row-major): nearest and second-nearest squared L2 distance over all of B,
