@@ -39,6 +39,8 @@ SIGNATURES = [
     ("fsb_state_keypoints", c_i32, [c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp]),
     ("fsb_describe", c_i32, [c_vp, c_vp, c_i32, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp]),
     ("fsb_state_free", c_i32, [c_vp]),
+    ("fsb_state_geometry", c_i32, [c_vp, c_vp, c_vp, c_vp]),
+    ("fsb_state_atlas", c_i32, [c_vp, c_i32, c_vp, c_i64]),
     ("fsb_sift_features", c_i32, [c_vp, c_vp, c_i32, c_i32, c_i32, c_vp, c_i32, c_vp, c_vp, c_vp, c_vp, c_vp]),
     ("fsb_match_bf", c_i32, [c_vp, c_vp, c_i32, c_vp, c_i32, c_f32, c_i32, c_vp, c_vp, c_vp]),
     ("fsb_match_guided", c_i32, [c_vp, c_vp, c_vp, c_i32, c_vp, c_vp, c_i32, c_f64, c_f64, c_f64, c_i32, c_f32,

@@ -114,7 +114,7 @@ static int32_t detect_dev(fsb_ctx* ctx, Workspace& ws, const uint8_t* d_img, int
     ctx->stage_begin(ST_PYRAMID);
     FSB_TRY(run_pyramid(ws, d_img, stride, exact, ctx->stream));
     ctx->stage_end(ST_PYRAMID);
-    FSB_TRY(run_detect(ctx, ws, p->contrast, p->edge, max_kp));
+    FSB_TRY(run_detect(ctx, ws, p->contrast, p->edge, max_kp, exact));
     return FSB_OK;
 }
 
@@ -395,6 +395,34 @@ int32_t fsb_describe(fsb_ctx* ctx, fsb_state* st, int32_t n, const float* x, con
     if (desc) FSB_CUDA(cudaMemcpyAsync(desc, dd, (size_t)n * 128 * 4, cudaMemcpyDeviceToHost, s));
     if (rootsift) FSB_CUDA(cudaMemcpyAsync(rootsift, du, (size_t)n * 128, cudaMemcpyDeviceToHost, s));
     FSB_CUDA(cudaStreamSynchronize(s));
+    return FSB_OK;
+}
+
+int32_t fsb_state_geometry(fsb_state* st, int32_t* n_oct, int32_t* rows, int32_t* cols) {
+    FSB_ARG(st && st->magic == STATE_MAGIC, "invalid state");
+    const Geometry& g = st->ws->g;
+    if (n_oct) *n_oct = g.n_oct;
+    for (int o = 0; o < g.n_oct; ++o) {
+        if (rows) rows[o] = g.R[o];
+        if (cols) cols[o] = g.C[o];
+    }
+    return FSB_OK;
+}
+
+int32_t fsb_state_atlas(fsb_state* st, int32_t which, float* out, int64_t n_floats) {
+    FSB_ARG(st && st->magic == STATE_MAGIC, "invalid state");
+    FSB_ARG(out && which >= 0 && which <= 2, "bad atlas request");
+    const Geometry& g = st->ws->g;
+    const int64_t want = which == 0 ? g.dog_off[g.n_oct] : g.grad_off[g.n_oct];
+    if (n_floats != want) {
+        set_error("invalid argument: atlas %d holds %lld floats, %lld requested", which, (long long)want,
+                  (long long)n_floats);
+        return FSB_ERR_ARG;
+    }
+    FSB_TRY(use_device(st->ctx));
+    const DevBuf& b = which == 0 ? st->ws->dog : which == 1 ? st->ws->mag : st->ws->ang;
+    if (want) FSB_CUDA(cudaMemcpyAsync(out, b.p, (size_t)want * 4, cudaMemcpyDeviceToHost, st->ctx->stream));
+    FSB_CUDA(cudaStreamSynchronize(st->ctx->stream));
     return FSB_OK;
 }
 

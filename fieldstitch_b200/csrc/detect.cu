@@ -6,12 +6,9 @@
 //
 //   k_extrema   3x3x3 extrema of DoG layers 1..3 (gsift.py:293-319), warp-aggregated append
 //   k_refine    sub-pixel fit, contrast and edge tests (gsift.py:322-369), thread per candidate
-//   k_orient    36-bin orientation histogram + smoothing + peaks (gsift.py:372-432), warp per
-//               keypoint, exact fixed-point accumulation (order-independent, deterministic)
+//   orientation peaks come from describe.cu (run_orient)
 //   sort        stable radix sorts: (extremum index, bin) then response descending (gsift.py:471)
 //   k_gather    keypoint fields in input-image pixels (gsift.py:462-474)
-//   k_describe  rotated 4x4x8 trilinear histogram, L2 clip/renormalise (gsift.py:480-525,
-//               800-871) and RootSIFT bytes (features.py:80-82), warp per keypoint
 //   spread      grid-spread selection of features.py:38-57
 #include <cub/cub.cuh>
 
@@ -28,10 +25,6 @@ struct DetectConsts {
     long long vox_off[MAXO + 1];
 };
 
-constexpr double kHistScale = 1125899906842624.0;        // 2^50, orientation histogram fixed point
-constexpr double kHistInv = 1.0 / 1125899906842624.0;
-constexpr double kDescScale = 281474976710656.0;         // 2^48, descriptor histogram fixed point
-constexpr double kDescInv = 1.0 / 281474976710656.0;
 
 __device__ __forceinline__ int find_octave(const Geometry& g, long long f) {
     int o = 0;
@@ -54,42 +47,124 @@ __device__ __forceinline__ void warp_append(bool flag, const T& v, T* out, uint3
     }
 }
 
-__global__ void __launch_bounds__(256) k_extrema(const float* __restrict__ DF, DetectConsts k,
-                                                 uint32_t* __restrict__ cand, uint32_t* counter,
-                                                 uint32_t cap) {
-    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    bool ext = false;
-    uint32_t fidx = 0;
-    if (t < k.vox_off[k.g.n_oct]) {
-        int o = 0;
-        while (t >= k.vox_off[o + 1]) ++o;
-        const int R = k.g.R[o], C = k.g.C[o];
-        const int iw = C - 2 * BORDER, ih = R - 2 * BORDER;
-        const long long loc = t - k.vox_off[o], per = (long long)iw * ih;
-        const int l = (int)(loc / per) + 1;
-        const long long rem = loc - (long long)(l - 1) * per;
-        const int r = (int)(rem / iw) + BORDER;
-        const int c = (int)(rem - (long long)(r - BORDER) * iw) + BORDER;
-        const long long RC = (long long)R * C;
-        const long long kk = k.g.dog_off[o] + l * RC + (long long)r * C + c;
-        const float v = DF[kk];
-        bool mx = v > k.pthr, mn = v < -k.pthr;
-        if (mx || mn) {
-#pragma unroll
-            for (int dl = -1; dl <= 1; ++dl)
-#pragma unroll
-                for (int dr = -1; dr <= 1; ++dr)
-#pragma unroll
-                    for (int dc = -1; dc <= 1; ++dc) {
-                        const float u = DF[kk + dl * RC + dr * C + dc];
-                        mx = mx && !(u > v);
-                        mn = mn && !(u < v);
-                    }
+// One CTA per (octave, 4 interior rows, 256 columns): DoG layers 0..4, rows r-1 .. r+4, columns
+// c0-4 .. c0+259 are staged in shared memory with 16-byte loads (each DoG value comes from DRAM
+// about 1.5 times: the row halo), then every thread tests its column for 4 rows x layers 1..3.
+constexpr int EX_T = 256, EX_ROWS = 4, EX_W = 264;
+
+struct ExTiles {
+    int n_oct;
+    int col_tiles[MAXO], row_tiles[MAXO];
+    int first[MAXO + 1];     // first block of each octave
+};
+
+__global__ void __launch_bounds__(EX_T) k_extrema(const float* __restrict__ DF, DetectConsts k, ExTiles tl,
+                                                  uint32_t* __restrict__ cand, uint32_t* counter, uint32_t cap) {
+    __shared__ __align__(16) float tile[5][EX_ROWS + 2][EX_W];
+    int o = 0;
+    while (o + 1 < tl.n_oct && (int)blockIdx.x >= tl.first[o + 1]) ++o;
+    const int b = blockIdx.x - tl.first[o];
+    const int ry = b / tl.col_tiles[o], cx = b - ry * tl.col_tiles[o];
+    const int R = k.g.R[o], C = k.g.C[o];
+    const int r0 = BORDER + ry * EX_ROWS, c0 = cx * 256;
+    const long long RC = (long long)R * C;
+    const float* base = DF + k.g.dog_off[o];
+    const bool vec = (C & 3) == 0 && (k.g.dog_off[o] & 3) == 0;
+    // stage layers 0..4, rows r0-1 .. r0+EX_ROWS, columns c0-4 .. c0+259
+    for (int e = threadIdx.x; e < 5 * (EX_ROWS + 2) * (EX_W / 4); e += EX_T) {
+        const int q = e % (EX_W / 4), t = e / (EX_W / 4);
+        const int rr = t % (EX_ROWS + 2), l = t / (EX_ROWS + 2);
+        const int y = r0 - 1 + rr, x = c0 - 4 + 4 * q;
+        float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
+        if (y < R) {
+            const float* p = base + l * RC + (long long)y * C;
+            if (vec && x >= 0 && x + 4 <= C) {
+                v = *reinterpret_cast<const float4*>(p + x);
+            } else {
+                if (x >= 0 && x < C) v.x = p[x];
+                if (x + 1 >= 0 && x + 1 < C) v.y = p[x + 1];
+                if (x + 2 >= 0 && x + 2 < C) v.z = p[x + 2];
+                if (x + 3 >= 0 && x + 3 < C) v.w = p[x + 3];
+            }
         }
-        ext = mx || mn;
-        fidx = (uint32_t)kk;
+        *reinterpret_cast<float4*>(&tile[l][rr][4 * q]) = v;
     }
-    warp_append(ext, fidx, cand, counter, cap);
+    __syncthreads();
+    const int c = c0 + threadIdx.x, tc = threadIdx.x + 4;
+    const bool col_ok = c >= BORDER && c < C - BORDER;
+    // bit (3 s + l - 1): voxel (layer l, row r0 + s) of this column is an extremum. Separable 3x3x3
+    // maximum / minimum (columns, then rows, then layers) in registers; the voxel is an extremum
+    // when it equals the maximum (minimum) of its 27-neighbourhood - ties count - and is beyond
+    // the threshold, as scipy's maximum_filter / minimum_filter test in the reference.
+    unsigned mask = 0;
+    if (col_ok) {
+        float hmx[5][EX_ROWS + 2], hmn[5][EX_ROWS + 2];
+#pragma unroll
+        for (int l = 0; l < 5; ++l)
+#pragma unroll
+            for (int rr = 0; rr < EX_ROWS + 2; ++rr) {
+                const float a = tile[l][rr][tc - 1], b = tile[l][rr][tc], cc = tile[l][rr][tc + 1];
+                hmx[l][rr] = fmaxf(fmaxf(a, b), cc);
+                hmn[l][rr] = fminf(fminf(a, b), cc);
+            }
+        float vmx[5][EX_ROWS], vmn[5][EX_ROWS];
+#pragma unroll
+        for (int l = 0; l < 5; ++l)
+#pragma unroll
+            for (int s = 0; s < EX_ROWS; ++s) {
+                vmx[l][s] = fmaxf(fmaxf(hmx[l][s], hmx[l][s + 1]), hmx[l][s + 2]);
+                vmn[l][s] = fminf(fminf(hmn[l][s], hmn[l][s + 1]), hmn[l][s + 2]);
+            }
+#pragma unroll
+        for (int s = 0; s < EX_ROWS; ++s) {
+            const bool row_ok = r0 + s < R - BORDER;
+#pragma unroll
+            for (int l = 1; l <= N_LAYERS; ++l) {
+                const float v = tile[l][s + 1][tc];
+                const float mx = fmaxf(fmaxf(vmx[l - 1][s], vmx[l][s]), vmx[l + 1][s]);
+                const float mn = fminf(fminf(vmn[l - 1][s], vmn[l][s]), vmn[l + 1][s]);
+                const bool e = (v >= mx && v > k.pthr) || (v <= mn && v < -k.pthr);
+                if (row_ok && e) mask |= 1u << (3 * s + l - 1);
+            }
+        }
+    }
+    // one warp-aggregated append of all candidates of the warp
+    const int lane = threadIdx.x & 31;
+    const int cntv = __popc(mask);
+    int incl = cntv;
+#pragma unroll
+    for (int sh = 1; sh < 32; sh <<= 1) {
+        const int t = __shfl_up_sync(0xffffffffu, incl, sh);
+        if (lane >= sh) incl += t;
+    }
+    const int total = __shfl_sync(0xffffffffu, incl, 31);
+    if (total == 0) return;
+    uint32_t basepos = 0;
+    if (lane == 31) basepos = atomicAdd(counter, (uint32_t)total);
+    basepos = __shfl_sync(0xffffffffu, basepos, 31);
+    uint32_t pos = basepos + (uint32_t)(incl - cntv);
+    while (mask) {
+        const int bit = __ffs(mask) - 1;
+        mask &= mask - 1;
+        const int s = bit / 3, l = bit - 3 * s + 1;
+        if (pos < cap) cand[pos] = (uint32_t)(k.g.dog_off[o] + l * RC + (long long)(r0 + s) * C + c);
+        ++pos;
+    }
+}
+
+ExTiles make_tiles(const Geometry& g, int* total) {
+    ExTiles t{};
+    t.n_oct = g.n_oct;
+    int acc = 0;
+    for (int o = 0; o < g.n_oct; ++o) {
+        t.first[o] = acc;
+        t.col_tiles[o] = (g.C[o] + 255) / 256;
+        t.row_tiles[o] = (g.R[o] - 2 * BORDER + EX_ROWS - 1) / EX_ROWS;
+        acc += t.col_tiles[o] * t.row_tiles[o];
+    }
+    t.first[g.n_oct] = acc;
+    *total = acc;
+    return t;
 }
 
 struct Fit {
@@ -184,84 +259,6 @@ __device__ __forceinline__ float kp_scale(int l, float x2) {
     return 1.6f * exp2f(t);
 }
 
-constexpr int ORI_WARPS = 8;
-
-__global__ void __launch_bounds__(ORI_WARPS * 32) k_orient(const float* __restrict__ MAG, const float* __restrict__ ANG,
-                                                           DetectConsts k, const Refined* __restrict__ ref,
-                                                           const uint32_t* n_ref, uint32_t cap_ref,
-                                                           Oriented* __restrict__ out, uint32_t* counter,
-                                                           uint32_t cap) {
-    __shared__ unsigned long long s_hist[ORI_WARPS][ORI_BINS];
-    __shared__ float s_raw[ORI_WARPS][ORI_BINS];
-    __shared__ float s_sm[ORI_WARPS][ORI_BINS];
-    const int wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const uint32_t n = min(*n_ref, cap_ref);
-    const uint32_t nw = gridDim.x * ORI_WARPS;
-    for (uint32_t i = blockIdx.x * ORI_WARPS + wid; i < n; i += nw) {
-        const Refined e = ref[i];
-        const int o = e.o, R = k.g.R[o], C = k.g.C[o];
-        const float scl = kp_scale(e.l, e.x2);
-        const int rad = min((int)rintf(4.5f * scl), ORI_R_MAX);
-        const float sw = 1.5f * scl;
-        const float den = 2.f * (sw * sw);
-        const int W = 2 * rad + 1;
-        const long long gb = k.g.grad_off[o] + (long long)(e.l - 1) * R * C;
-        for (int b = lane; b < ORI_BINS; b += 32) s_hist[wid][b] = 0ull;
-        __syncwarp();
-        for (int s = lane; s < W * W; s += 32) {
-            const int ii = s / W - rad, jj = s - (s / W) * W - rad;
-            const int y = e.r + ii, x = e.c + jj;
-            if (y > 0 && y < R - 1 && x > 0 && x < C - 1) {
-                const long long gi = gb + (long long)y * C + x;
-                const float d2 = (float)(ii * ii + jj * jj);
-                const float w = expf(-d2 / den);
-                const float m = MAG[gi] * w;
-                int b = (int)rintf(ANG[gi] * 0.1f);
-                b = ((b % ORI_BINS) + ORI_BINS) % ORI_BINS;
-                atomicAdd(&s_hist[wid][b], (unsigned long long)llrint((double)m * kHistScale));
-            }
-        }
-        __syncwarp();
-        for (int b = lane; b < ORI_BINS; b += 32) s_raw[wid][b] = (float)((double)s_hist[wid][b] * kHistInv);
-        __syncwarp();
-        float hmax = 0.f;
-        for (int b = lane; b < ORI_BINS; b += 32) {
-            const float* h = s_raw[wid];
-            const float v = ((h[(b + 34) % 36] + h[(b + 2) % 36]) * 0.0625f + (h[(b + 35) % 36] + h[(b + 1) % 36]) * 0.25f) +
-                            h[b] * 0.375f;
-            s_sm[wid][b] = v;
-            hmax = fmaxf(hmax, v);
-        }
-#pragma unroll
-        for (int sh = 16; sh; sh >>= 1) hmax = fmaxf(hmax, __shfl_xor_sync(0xffffffffu, hmax, sh));
-        __syncwarp();
-        const float thr = 0.8f * hmax;
-        for (int b0 = 0; b0 < 64; b0 += 32) {
-            const int b = b0 + lane;
-            bool pk = false;
-            Oriented ent{};
-            if (b < ORI_BINS) {
-                const float* h = s_sm[wid];
-                const float hl = h[(b + 35) % 36], hc = h[b], hr = h[(b + 1) % 36];
-                pk = hc > hl && hc > hr && hc >= thr && hmax > 0.f;
-                if (pk) {
-                    float dn = (hl - 2.f * hc) + hr;
-                    if (fabsf(dn) < 1e-12f) dn = -1e-12f;
-                    const float off = (0.5f * (hl - hr)) / dn;
-                    double pos = (double)b + (double)off;
-                    if (pos < 0.0) pos += 36.0;
-                    if (pos >= 36.0) pos -= 36.0;
-                    double ang = 360.0 - 10.0 * pos;
-                    if (fabs(ang - 360.0) < 1e-4) ang = 0.0;
-                    ent.ri = i; ent.j = b; ent.angle = (float)ang;
-                }
-            }
-            warp_append(pk, ent, out, counter, cap);
-        }
-        __syncwarp();
-    }
-}
-
 __global__ void k_sort_keys_a(const Oriented* __restrict__ ori, const Refined* __restrict__ ref, uint32_t n,
                               unsigned long long* __restrict__ key, uint32_t* __restrict__ val) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -294,161 +291,6 @@ __global__ void k_gather(const Oriented* __restrict__ ori, const Refined* __rest
     kresp[i] = r.resp;
     koct[i] = r.o;
     klayer[i] = r.l;
-}
-
-// ------------------------------------------------------------------------------ descriptor
-constexpr int DESC_WARPS = 4;
-constexpr int DH = (D_WIDTH + 2) * (D_WIDTH + 2) * (D_BINS + 2);   // 360
-
-// NumPy's float32 sum of 128 contiguous values: eight strided partial sums, then a fixed tree.
-__device__ __forceinline__ float np_sum128(const float* v, int lane) {
-    float r = 0.f;
-    if (lane < 8) {
-        r = v[lane];
-        for (int i = 8 + lane; i < 128; i += 8) r = r + v[i];
-    }
-    const float r1 = __shfl_down_sync(0xffffffffu, r, 1);
-    const float p = r + r1;                                // lanes 0,2,4,6: (r0+r1),(r2+r3),...
-    const float p2 = __shfl_down_sync(0xffffffffu, p, 2);
-    const float q = p + p2;                                // lanes 0,4: ((r0+r1)+(r2+r3)), ((r4+r5)+(r6+r7))
-    const float q4 = __shfl_down_sync(0xffffffffu, q, 4);
-    return __shfl_sync(0xffffffffu, q + q4, 0);
-}
-
-template <bool EXACT>
-__global__ void __launch_bounds__(DESC_WARPS * 32) k_describe(const float* __restrict__ MAG, const float* __restrict__ ANG,
-                                                              Geometry g, int n, const float* __restrict__ kx,
-                                                              const float* __restrict__ ky, const float* __restrict__ ks,
-                                                              const float* __restrict__ ka, const int32_t* __restrict__ ko,
-                                                              const int32_t* __restrict__ kl, float* __restrict__ desc,
-                                                              uint8_t* __restrict__ u8) {
-    __shared__ unsigned long long s_hist[DESC_WARPS][DH];
-    __shared__ float s_d[DESC_WARPS][128];
-    __shared__ float s_t[DESC_WARPS][128];
-    const int wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int nw = gridDim.x * DESC_WARPS;
-    for (int k = blockIdx.x * DESC_WARPS + wid; k < n; k += nw) {
-        // keypoint geometry in float64 as the reference's host code computes it (gsift.py:490-501)
-        const int o = ko[k], li = kl[k];
-        const double f = 1.0 / (exp2((double)o) * 0.5);
-        const double px = (double)kx[k] * f, py = (double)ky[k] * f;
-        const double scl = (double)ks[k] * f * 0.5;
-        double ori = 360.0 - (double)ka[k];
-        if (fabs(ori - 360.0) < 1e-4) ori = 0.0;
-        const int rows = g.R[o], cols = g.C[o];
-        long long rad = llrint(3.0 * scl * 1.4142135623730951 * 5.0 * 0.5);
-        const long long rmax = (long long)sqrt((double)rows * rows + (double)cols * cols);
-        if (rad > rmax) rad = rmax;
-        const int R = (int)rad, W = 2 * R + 1;
-        const long long gb = g.grad_off[o] + (long long)(li - 1) * rows * cols;
-        const int pr = (int)rint(py), pc = (int)rint(px);
-        const double hw = 3.0 * scl;
-        const double t = ori * 0.017453292519943295;   // np.radians
-        const double cos_d = cos(t) / hw, sin_d = sin(t) / hw;
-        const float cos_f = (float)cos_d, sin_f = (float)sin_d, ori_f = (float)ori;
-        for (int b = lane; b < DH; b += 32) s_hist[wid][b] = 0ull;
-        __syncwarp();
-        for (int s = lane; s < W * W; s += 32) {
-            const int ii = s / W - R, jj = s - (s / W) * W - R;
-            const int y = pr + ii, x = pc + jj;
-            if (!(y > 0 && y < rows - 1 && x > 0 && x < cols - 1)) continue;
-            int r0, c0, o0;
-            double vv[8];
-            if (EXACT) {
-                const double c_rot = (double)jj * cos_d - (double)ii * sin_d;
-                const double r_rot = (double)jj * sin_d + (double)ii * cos_d;
-                const double rbin = (r_rot + 2.0) - 0.5, cbin = (c_rot + 2.0) - 0.5;
-                if (!(rbin > -1.0 && rbin < 4.0 && cbin > -1.0 && cbin < 4.0)) continue;
-                const long long gi = gb + (long long)y * cols + x;
-                const double w = exp((c_rot * c_rot + r_rot * r_rot) * (-1.0 / 8.0));
-                const double m = (double)MAG[gi] * w;
-                const double obin = ((double)ANG[gi] - ori) * (8.0 / 360.0);
-                const double fr = floor(rbin), fc = floor(cbin), fo = floor(obin);
-                const double rb = rbin - fr, cb = cbin - fc, ob = obin - fo;
-                r0 = (int)fr; c0 = (int)fc; o0 = (int)fo;
-                const double v_r1 = m * rb, v_r0 = m - v_r1;
-                const double v_rc11 = v_r1 * cb, v_rc10 = v_r1 - v_rc11;
-                const double v_rc01 = v_r0 * cb, v_rc00 = v_r0 - v_rc01;
-                vv[1] = v_rc00 * ob; vv[0] = v_rc00 - vv[1];
-                vv[3] = v_rc01 * ob; vv[2] = v_rc01 - vv[3];
-                vv[5] = v_rc10 * ob; vv[4] = v_rc10 - vv[5];
-                vv[7] = v_rc11 * ob; vv[6] = v_rc11 - vv[7];
-            } else {
-                const float c_rot = (float)jj * cos_f - (float)ii * sin_f;
-                const float r_rot = (float)jj * sin_f + (float)ii * cos_f;
-                const float rbin = r_rot + 1.5f, cbin = c_rot + 1.5f;
-                if (!(rbin > -1.f && rbin < 4.f && cbin > -1.f && cbin < 4.f)) continue;
-                const long long gi = gb + (long long)y * cols + x;
-                const float w = expf((c_rot * c_rot + r_rot * r_rot) * (-1.f / 8.f));
-                const float m = MAG[gi] * w;
-                const float obin = (ANG[gi] - ori_f) * (8.f / 360.f);
-                const float fr = floorf(rbin), fc = floorf(cbin), fo = floorf(obin);
-                const float rb = rbin - fr, cb = cbin - fc, ob = obin - fo;
-                r0 = (int)fr; c0 = (int)fc; o0 = (int)fo;
-                const float v_r1 = m * rb, v_r0 = m - v_r1;
-                const float v_rc11 = v_r1 * cb, v_rc10 = v_r1 - v_rc11;
-                const float v_rc01 = v_r0 * cb, v_rc00 = v_r0 - v_rc01;
-                float t1;
-                t1 = v_rc00 * ob; vv[1] = t1; vv[0] = v_rc00 - t1;
-                t1 = v_rc01 * ob; vv[3] = t1; vv[2] = v_rc01 - t1;
-                t1 = v_rc10 * ob; vv[5] = t1; vv[4] = v_rc10 - t1;
-                t1 = v_rc11 * ob; vv[7] = t1; vv[6] = v_rc11 - t1;
-            }
-            if (o0 < 0) o0 += D_BINS;
-            if (o0 >= D_BINS) o0 -= D_BINS;
-            const int idx = ((r0 + 1) * (D_WIDTH + 2) + c0 + 1) * (D_BINS + 2) + o0;
-            unsigned long long* h = s_hist[wid];
-            // (r, c, o) corners: 000 001 010 011 100 101 110 111
-            atomicAdd(h + idx, (unsigned long long)llrint(vv[0] * kDescScale));
-            atomicAdd(h + idx + 1, (unsigned long long)llrint(vv[1] * kDescScale));
-            atomicAdd(h + idx + 10, (unsigned long long)llrint(vv[2] * kDescScale));
-            atomicAdd(h + idx + 11, (unsigned long long)llrint(vv[3] * kDescScale));
-            atomicAdd(h + idx + 60, (unsigned long long)llrint(vv[4] * kDescScale));
-            atomicAdd(h + idx + 61, (unsigned long long)llrint(vv[5] * kDescScale));
-            atomicAdd(h + idx + 70, (unsigned long long)llrint(vv[6] * kDescScale));
-            atomicAdd(h + idx + 71, (unsigned long long)llrint(vv[7] * kDescScale));
-        }
-        __syncwarp();
-        // float32 histogram, fold the angle wrap bins, keep the 4x4x8 interior (gsift.py:789-793)
-        float* d = s_d[wid];
-        for (int q = lane; q < 128; q += 32) {
-            const int rc = q >> 3, ob = q & 7;
-            const int r = (rc >> 2) + 1, c = (rc & 3) + 1;
-            const unsigned long long* h = s_hist[wid] + (r * (D_WIDTH + 2) + c) * (D_BINS + 2);
-            float v = (float)((double)h[ob] * kDescInv);
-            if (ob < 2) v = v + (float)((double)h[ob + D_BINS] * kDescInv);
-            d[q] = v;
-        }
-        __syncwarp();
-        float sq[4];
-        for (int u = 0; u < 4; ++u) sq[u] = d[lane + 32 * u];
-        float* tmp = s_t[wid];
-        for (int u = 0; u < 4; ++u) tmp[lane + 32 * u] = sq[u] * sq[u];
-        __syncwarp();
-        const float n1 = sqrtf(np_sum128(tmp, lane));
-        const float clip = n1 * 0.2f;
-        for (int u = 0; u < 4; ++u) sq[u] = fminf(sq[u], clip);
-        __syncwarp();
-        for (int u = 0; u < 4; ++u) tmp[lane + 32 * u] = sq[u] * sq[u];
-        __syncwarp();
-        const float n2 = sqrtf(np_sum128(tmp, lane));
-        const float sc = 512.f / fmaxf(n2, 1e-7f);
-        for (int u = 0; u < 4; ++u) sq[u] = sq[u] * sc;
-        if (desc)
-            for (int u = 0; u < 4; ++u) desc[(size_t)k * 128 + lane + 32 * u] = sq[u];
-        if (u8) {
-            __syncwarp();
-            for (int u = 0; u < 4; ++u) tmp[lane + 32 * u] = fabsf(sq[u]);
-            __syncwarp();
-            const float l1 = np_sum128(tmp, lane) + 1e-7f;
-            for (int u = 0; u < 4; ++u) {
-                float v = sqrtf(sq[u] / l1) * 512.f;
-                v = fminf(fmaxf(v, 0.f), 255.f);
-                u8[(size_t)k * 128 + lane + 32 * u] = (uint8_t)v;
-            }
-        }
-        __syncwarp();
-    }
 }
 
 // ------------------------------------------------------------------------------------ spread
@@ -514,7 +356,7 @@ DetectConsts make_consts(const Geometry& g, double contrast, double edge) {
 }  // namespace
 
 // Full detection pipeline; contrast/edge in double as the reference's Python floats.
-int32_t run_detect(fsb_ctx* ctx, Workspace& ws, double contrast, double edge, int max_kp) {
+int32_t run_detect(fsb_ctx* ctx, Workspace& ws, double contrast, double edge, int max_kp, bool exact) {
     cudaStream_t s = ctx->stream;
     const Geometry& g = ws.g;
     const DetectConsts k = make_consts(g, contrast, edge);
@@ -524,9 +366,10 @@ int32_t run_detect(fsb_ctx* ctx, Workspace& ws, double contrast, double edge, in
     ctx->stage_begin(ST_EXTREMA);
     for (int attempt = 0; attempt < 3; ++attempt) {
         FSB_CUDA(cudaMemsetAsync(cnt, 0, 3 * sizeof(uint32_t), s));
-        const long long nvox = k.vox_off[g.n_oct];
-        if (nvox > 0) {
-            k_extrema<<<blocks(nvox, 256), 256, 0, s>>>(DF, k, ws.cand.as<uint32_t>(), cnt, (uint32_t)ws.cap_cand);
+        int nblk = 0;
+        const ExTiles tl = make_tiles(g, &nblk);
+        if (nblk > 0) {
+            k_extrema<<<nblk, EX_T, 0, s>>>(DF, k, tl, ws.cand.as<uint32_t>(), cnt, (uint32_t)ws.cap_cand);
             note_launch();
         }
         FSB_CUDA(cudaGetLastError());
@@ -559,12 +402,8 @@ int32_t run_detect(fsb_ctx* ctx, Workspace& ws, double contrast, double edge, in
         if (ws.cap_ori < (size_t)n_ref * 2 + 1024) ws.cap_ori = (size_t)n_ref * 2 + 1024;
         FSB_TRY(ws.oriented.ensure(ws.cap_ori * sizeof(Oriented)));
         FSB_CUDA(cudaMemsetAsync(cnt + 2, 0, sizeof(uint32_t), s));
-        const unsigned ob = blocks(n_ref, ORI_WARPS);
-        k_orient<<<ob < 148 * 16 ? ob : 148 * 16, ORI_WARPS * 32, 0, s>>>(
-            ws.mag.as<float>(), ws.ang.as<float>(), k, ws.refined.as<Refined>(), cnt + 1, (uint32_t)ws.cap_ref,
-            ws.oriented.as<Oriented>(), cnt + 2, (uint32_t)ws.cap_ori);
-        note_launch();
-        FSB_CUDA(cudaGetLastError());
+        FSB_TRY(run_orient(ws, ws.refined.as<Refined>(), cnt + 1, n_ref, (uint32_t)ws.cap_ref,
+                           ws.oriented.as<Oriented>(), cnt + 2, (uint32_t)ws.cap_ori, exact, s));
         FSB_CUDA(cudaMemcpyAsync(h_cnt + 2, cnt + 2, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
         FSB_CUDA(cudaStreamSynchronize(s));
         n_ori = h_cnt[2];
@@ -617,29 +456,6 @@ int32_t run_detect(fsb_ctx* ctx, Workspace& ws, double contrast, double edge, in
     ctx->stage_end(ST_SORT);
     ws.n_kp = (int)n_keep;
     return FSB_OK;
-}
-
-int32_t run_describe_mode(const Workspace& ws, int n, const float* d_x, const float* d_y, const float* d_size,
-                          const float* d_angle, const int32_t* d_oct, const int32_t* d_layer, float* d_desc,
-                          uint8_t* d_u8, bool exact, cudaStream_t s) {
-    if (n <= 0) return FSB_OK;
-    const unsigned nb = blocks(n, DESC_WARPS);
-    const unsigned grid = nb < 148u * 32u ? nb : 148u * 32u;
-    if (exact)
-        k_describe<true><<<grid, DESC_WARPS * 32, 0, s>>>(ws.mag.as<float>(), ws.ang.as<float>(), ws.g, n, d_x, d_y,
-                                                          d_size, d_angle, d_oct, d_layer, d_desc, d_u8);
-    else
-        k_describe<false><<<grid, DESC_WARPS * 32, 0, s>>>(ws.mag.as<float>(), ws.ang.as<float>(), ws.g, n, d_x, d_y,
-                                                           d_size, d_angle, d_oct, d_layer, d_desc, d_u8);
-    note_launch();
-    FSB_CUDA(cudaGetLastError());
-    return FSB_OK;
-}
-
-int32_t run_describe(const Workspace& ws, int n, const float* d_x, const float* d_y, const float* d_size,
-                     const float* d_angle, const int32_t* d_oct, const int32_t* d_layer, float* d_desc,
-                     uint8_t* d_u8, cudaStream_t s) {
-    return run_describe_mode(ws, n, d_x, d_y, d_size, d_angle, d_oct, d_layer, d_desc, d_u8, false, s);
 }
 
 // grid-spread selection of nfeat keypoints out of the detected (response-sorted) ones,

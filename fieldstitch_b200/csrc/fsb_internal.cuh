@@ -148,9 +148,15 @@ constexpr uint32_t STATE_MAGIC = 0x51f7b200u;
 // ---------------------------------------------------------------- pyramid.cu
 int32_t upload_taps();
 int32_t run_pyramid(Workspace& ws, const uint8_t* d_img, int img_stride, bool exact, cudaStream_t s);
+// octave.cu
+int32_t upload_octave_taps(const float* taps, int stride, const int* counts);
+int32_t launch_octave_fused(const float* L0, int R, int C, float* dog, float* mag, float* ang, float* down,
+                            int down_cols, cudaStream_t s);
 
-// ---------------------------------------------------------------- detect.cu
-int32_t run_detect(fsb_ctx* ctx, Workspace& ws, double contrast, double edge, int max_kp);
+// ---------------------------------------------------------------- detect.cu / describe.cu
+int32_t run_orient(const Workspace& ws, const Refined* ref, const uint32_t* d_nref, uint32_t n_ref_host,
+                   uint32_t cap_ref, Oriented* out, uint32_t* d_counter, uint32_t cap, bool exact, cudaStream_t s);
+int32_t run_detect(fsb_ctx* ctx, Workspace& ws, double contrast, double edge, int max_kp, bool exact);
 int32_t run_describe_mode(const Workspace& ws, int n, const float* d_x, const float* d_y, const float* d_size,
                           const float* d_angle, const int32_t* d_oct, const int32_t* d_layer, float* d_desc,
                           uint8_t* d_u8, bool exact, cudaStream_t s);

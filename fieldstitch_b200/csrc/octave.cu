@@ -1,0 +1,312 @@
+// Fused octave kernel: the five layer blurs of one octave in one pass over HBM.
+//
+// Reference: app/planesite/gsift.py:85-87 (separable mirror blur), 158-179 (layers, DoG,
+// downsample), 244-267 (gradient magnitude / angle of gauss layers 1..3).
+//
+// A CTA owns a 168-column strip and a range of output rows and streams down the rows, S = 4 rows
+// per step. Stage i (1..5) keeps the rows of L_{i-1} it still needs in a shared-memory ring
+// (2 r_i + S rows; L0's ring has S more rows so the next step's rows load with cp.async while
+// this step computes) and produces S new rows of L_i per step:
+//   vertical pass   thread = (column pair, row pair): float2 loads of 2 r + 2 ring rows, two
+//                   output rows, stored row-pair-interleaved;
+//   horizontal pass thread = (row pair, column pair): r + 1 16-byte loads, two output columns
+//                   of two rows, stored into the next ring.
+// Arithmetic is packed FP32x2 (__ffma2_rn / __fadd2_rn) with symmetric tap pairing
+// w_0 x_0 + sum_j w_j (x_-j + x_j): a mirrored input gives a bit-identical mirrored output, so
+// mirroring L0 once when it is loaded reproduces the reference's per-layer reflect-101 borders.
+// After each stage the epilogue writes, for the strip's output rows, the DoG L_i - L_{i-1}, the
+// gradient of L_{i-1} (layers 1..3) and L_3[::2, ::2] (the next octave's base), with 16-byte
+// stores where the row pitch allows. HBM traffic per octave pixel: L0 read once (plus the column
+// halo) and 44 B written; no intermediate layer ever leaves the SM.
+#include "fsb_internal.cuh"
+
+namespace fsb {
+
+__constant__ float2 c_tap2[6][14];   // (w_j, w_j) at distance j = 0..r of layer i's taps
+
+int32_t upload_octave_taps(const float* taps, int stride, const int* counts) {
+    float2 t[6][14] = {};
+    for (int i = 0; i < 6; ++i) {
+        const int r = counts[i] / 2;
+        for (int j = 0; j <= r; ++j) t[i][j] = make_float2(taps[i * stride + r + j], taps[i * stride + r + j]);
+    }
+    FSB_CUDA(cudaMemcpyToSymbol(c_tap2, t, sizeof(t)));
+    return FSB_OK;
+}
+
+namespace {
+
+constexpr int NT = 256;      // threads per CTA
+constexpr int SW = 168;      // output columns per strip
+constexpr int S = 4;         // rows per step
+constexpr int X0 = 44;       // L0 columns held left of the strip (keeps the load origin 16-byte aligned)
+constexpr int HALO = 42;     // rows above / below a chunk that feed its outputs (5+6+8+10+13)
+
+// radius of layer i's blur; first held column of layer i relative to the strip (x0 - H(i));
+// held width of layer i (padded to 4); ring pitch and rows
+__host__ __device__ constexpr int RAD(int i) { return i == 1 ? 5 : i == 2 ? 6 : i == 3 ? 8 : i == 4 ? 10 : i == 5 ? 13 : 0; }
+__host__ __device__ constexpr int H(int i) { return i == 0 ? 44 : i == 1 ? 39 : i == 2 ? 33 : i == 3 ? 25 : i == 4 ? 15 : 2; }
+__host__ __device__ constexpr int WIN(int i) { return i == 0 ? 256 : i == 1 ? 248 : i == 2 ? 236 : i == 3 ? 220 : i == 4 ? 200 : 172; }
+__host__ __device__ constexpr int PITCH(int i) { return i == 0 ? 260 : WIN(i); }
+__host__ __device__ constexpr int ROWS(int i) { return i == 0 ? 2 * 5 + 2 * S : i == 5 ? S : 2 * RAD(i + 1) + S; }
+__host__ __device__ constexpr int LAG(int i) { return i == 1 ? 5 : i == 2 ? 11 : i == 3 ? 19 : i == 4 ? 29 : i == 5 ? 42 : 0; }
+__host__ __device__ constexpr int off_of(int i) { return i == 0 ? 0 : off_of(i - 1) + ROWS(i - 1) * PITCH(i - 1); }
+constexpr int T2_OFF = off_of(6);     // row-pair interleaved vertical outputs (float2 per column)
+constexpr int T2_PITCH = 260;         // float2 per row pair
+constexpr int SMEM_BYTES = (T2_OFF + 2 * T2_PITCH * 2) * 4;
+
+struct Args {
+    const float* L0;              // octave base, pitch C
+    int R, C, rows_per_cta;
+    float* dog[5];                // DoG planes R x C
+    float* mag[3];                // gradient magnitude of layers 1..3
+    float* ang[3];                // gradient angle of layers 1..3
+    float* down;                  // next octave base or null
+    int down_cols;
+};
+
+__device__ __forceinline__ int mir(int p, int n) {
+    if (n == 1) return 0;
+    while (p < 0 || p >= n) p = p < 0 ? -p : 2 * n - 2 - p;
+    return p;
+}
+
+// slot of `row` in a ring of N rows, with row - base >= 0
+template <int N>
+__device__ __forceinline__ int slot_of(int row, int base) { return (row - base) % N; }
+
+template <int N>
+__device__ __forceinline__ int wrap(int s) { return s >= N ? s - N : s; }
+
+__device__ __forceinline__ void cp_async4(float* dst, const float* src) {
+    const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(d), "l"(src));
+}
+__device__ __forceinline__ void cp_async16(float* dst, const float* src) {
+    const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(d), "l"(src));
+}
+__device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+__device__ __forceinline__ void cp_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::); }
+
+// rows [g, g + S) of L0 (mirrored) into ring 0: one 16-byte group per thread
+__device__ __forceinline__ void load_rows(float* ring0, const Args& a, int x0, int g, int ybase, bool aligned) {
+    const int s = threadIdx.x >> 6, q = threadIdx.x & 63;
+    const int y = g + s;
+    float* dst = ring0 + slot_of<ROWS(0)>(y, ybase) * PITCH(0) + 4 * q;
+    const float* row = a.L0 + (size_t)mir(y, a.R) * a.C;
+    const int x = x0 - X0 + 4 * q;
+    if (aligned) {
+        cp_async16(dst, row + x);
+    } else {
+#pragma unroll
+        for (int k = 0; k < 4; ++k) cp_async4(dst + k, row + mir(x + k, a.C));
+    }
+}
+
+// rows yb, yb+1 (row pair rp) .. of L_I from L_{I-1} rows in `ring`; thread = (column pair, row pair)
+template <int I>
+__device__ __forceinline__ void vpass(const float* ring, float2* t2, int yb, int ybase) {
+    constexpr int r = RAD(I), NR = ROWS(I - 1), P = PITCH(I - 1);
+    constexpr int NP = WIN(I - 1) / 2 + 1;   // column pairs the horizontal pass reads
+    const int cp = threadIdx.x & 127, rp = threadIdx.x >> 7;
+    if (cp >= NP) return;
+    const int s0 = slot_of<NR>(yb + 2 * rp - r, ybase);
+    float2 x[2 * r + 2];
+#pragma unroll
+    for (int k = 0; k < 2 * r + 2; ++k)
+        x[k] = *reinterpret_cast<const float2*>(ring + wrap<NR>(s0 + k) * P + 2 * cp);
+    float2 o[2];
+#pragma unroll
+    for (int s = 0; s < 2; ++s) {
+        float2 acc = __fmul2_rn(x[s + r], c_tap2[I][0]);
+#pragma unroll
+        for (int j = r; j >= 1; --j) acc = __ffma2_rn(__fadd2_rn(x[s + r - j], x[s + r + j]), c_tap2[I][j], acc);
+        o[s] = acc;
+    }
+    *reinterpret_cast<float4*>(t2 + rp * T2_PITCH + 2 * cp) = make_float4(o[0].x, o[1].x, o[0].y, o[1].y);
+}
+
+// L_I rows yb .. yb+3 from the interleaved vertical outputs; thread = (row pair, column pair)
+template <int I>
+__device__ __forceinline__ void hpass(const float2* t2, float* out, int yb, int ybase) {
+    constexpr int r = RAD(I), NO = ROWS(I), P = PITCH(I);
+    constexpr int NG = WIN(I) / 2;
+    const int p = threadIdx.x >> 7, g = threadIdx.x & 127;
+    if (g >= NG) return;
+    const float4* src = reinterpret_cast<const float4*>(t2 + p * T2_PITCH + 2 * g);
+    float2 y[2 * r + 2];
+#pragma unroll
+    for (int k = 0; k < r + 1; ++k) {
+        const float4 v = src[k];
+        y[2 * k] = make_float2(v.x, v.y);
+        y[2 * k + 1] = make_float2(v.z, v.w);
+    }
+    float2 o[2];
+#pragma unroll
+    for (int c = 0; c < 2; ++c) {
+        float2 acc = __fmul2_rn(y[c + r], c_tap2[I][0]);
+#pragma unroll
+        for (int j = r; j >= 1; --j) acc = __ffma2_rn(__fadd2_rn(y[c + r - j], y[c + r + j]), c_tap2[I][j], acc);
+        o[c] = acc;
+    }
+    const int s0 = slot_of<NO>(yb + 2 * p, ybase), s1 = wrap<NO>(s0 + 1);
+    *reinterpret_cast<float2*>(out + s0 * P + 2 * g) = make_float2(o[0].x, o[1].x);
+    *reinterpret_cast<float2*>(out + s1 * P + 2 * g) = make_float2(o[0].y, o[1].y);
+}
+
+// degrees per radian as NumPy's float32 rad2deg computes it: float(180) / float(pi)
+constexpr float kRad2Deg = 0x1.ca5dc0p+5f;
+
+// DoG of stage I (L_I - L_{I-1}), gradient of L_{I-1} (I = 2..4), L_3[::2, ::2] (I = 4)
+template <int I>
+__device__ __forceinline__ void epilogue(const float* prev, const float* cur, const Args& a, int x0, int yb, int ybase,
+                                         int ya, int yz) {
+    constexpr int PP = PITCH(I - 1), PR = ROWS(I - 1), CP = PITCH(I), CR = ROWS(I);
+    constexpr int hp = H(I - 1), hc = H(I);
+    const int e = threadIdx.x;
+    if (e >= S * (SW / 4)) return;
+    const int s = e / (SW / 4), q = e - s * (SW / 4);
+    const int y = yb + s;
+    const int xg = x0 + 4 * q;
+    if (y < ya || y >= yz || xg >= a.C) return;
+    const int ps = slot_of<PR>(y, ybase);
+    const float* pr = prev + ps * PP + 4 * q + hp;
+    const float* cr = cur + slot_of<CR>(y, ybase) * CP + 4 * q + hc;
+    float d[4];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) d[k] = cr[k] - pr[k];
+    const int at = y * a.C + xg;
+    const bool vec = (a.C & 3) == 0 && xg + 4 <= a.C;
+    float* dg = a.dog[I - 1] + at;
+    if (vec) {
+        *reinterpret_cast<float4*>(dg) = make_float4(d[0], d[1], d[2], d[3]);
+    } else {
+        for (int k = 0; k < 4 && xg + k < a.C; ++k) dg[k] = d[k];
+    }
+    if (I >= 2 && I <= 4) {
+        const float* up = prev + wrap<PR>(ps + PR - 1) * PP + 4 * q + hp;
+        const float* dn = prev + wrap<PR>(ps + 1) * PP + 4 * q + hp;
+        float mg[4], an[4];
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            const int x = xg + k;
+            float dx = 0.f, dy = 0.f;
+            if (y > 0 && y < a.R - 1 && x > 0 && x < a.C - 1) {
+                dx = __fsub_rn(pr[k + 1], pr[k - 1]);
+                dy = __fsub_rn(up[k], dn[k]);
+            }
+            mg[k] = __fsqrt_rn(__fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dy, dy)));
+            const float t = __fmul_rn(atan2f(dy, dx), kRad2Deg);
+            an[k] = t < 0.f ? __fadd_rn(t, 360.f) : t;
+        }
+        float* m = a.mag[I - 2] + at;
+        float* n = a.ang[I - 2] + at;
+        if (vec) {
+            *reinterpret_cast<float4*>(m) = make_float4(mg[0], mg[1], mg[2], mg[3]);
+            *reinterpret_cast<float4*>(n) = make_float4(an[0], an[1], an[2], an[3]);
+        } else {
+            for (int k = 0; k < 4 && xg + k < a.C; ++k) {
+                m[k] = mg[k];
+                n[k] = an[k];
+            }
+        }
+    }
+    if (I == 4 && a.down && !(y & 1)) {
+        float* o = a.down + (y >> 1) * a.down_cols + (xg >> 1);
+        o[0] = pr[0];
+        if (xg + 2 < a.C) o[1] = pr[2];
+    }
+}
+
+__global__ void __launch_bounds__(NT, 2) k_octave(Args a) {
+    extern __shared__ __align__(16) float sm[];
+    float* ring0 = sm + off_of(0);
+    float* ring1 = sm + off_of(1);
+    float* ring2 = sm + off_of(2);
+    float* ring3 = sm + off_of(3);
+    float* ring4 = sm + off_of(4);
+    float* ring5 = sm + off_of(5);
+    float2* t2 = reinterpret_cast<float2*>(sm + T2_OFF);
+    const int x0 = blockIdx.x * SW;
+    const int ya = blockIdx.y * a.rows_per_cta;
+    const int yz = min(a.R, ya + a.rows_per_cta);
+    const int ybase = ya - 128;                             // keeps every (row - ybase) positive
+    const int g0 = ya - HALO;
+    const int steps = (yz - ya + 2 * HALO + S - 1) / S;
+    const bool aligned = (a.C & 3) == 0 && x0 - X0 >= 0 && x0 - X0 + WIN(0) <= a.C;
+    load_rows(ring0, a, x0, g0, ybase, aligned);
+    cp_commit();
+    for (int t = 0; t < steps; ++t) {
+        cp_wait_all();
+        __syncthreads();
+        const int g = g0 + t * S;                            // L0 rows g .. g+3 are in ring 0
+        if (t + 1 < steps) load_rows(ring0, a, x0, g + S, ybase, aligned);
+        cp_commit();
+        // stage i produces rows g - LAG(i) .. g - LAG(i) + 3
+        vpass<1>(ring0, t2, g - LAG(1), ybase);
+        __syncthreads();
+        hpass<1>(t2, ring1, g - LAG(1), ybase);
+        __syncthreads();
+        epilogue<1>(ring0, ring1, a, x0, g - LAG(1), ybase, ya, yz);
+        vpass<2>(ring1, t2, g - LAG(2), ybase);
+        __syncthreads();
+        hpass<2>(t2, ring2, g - LAG(2), ybase);
+        __syncthreads();
+        epilogue<2>(ring1, ring2, a, x0, g - LAG(2), ybase, ya, yz);
+        vpass<3>(ring2, t2, g - LAG(3), ybase);
+        __syncthreads();
+        hpass<3>(t2, ring3, g - LAG(3), ybase);
+        __syncthreads();
+        epilogue<3>(ring2, ring3, a, x0, g - LAG(3), ybase, ya, yz);
+        vpass<4>(ring3, t2, g - LAG(4), ybase);
+        __syncthreads();
+        hpass<4>(t2, ring4, g - LAG(4), ybase);
+        __syncthreads();
+        epilogue<4>(ring3, ring4, a, x0, g - LAG(4), ybase, ya, yz);
+        vpass<5>(ring4, t2, g - LAG(5), ybase);
+        __syncthreads();
+        hpass<5>(t2, ring5, g - LAG(5), ybase);
+        __syncthreads();
+        epilogue<5>(ring4, ring5, a, x0, g - LAG(5), ybase, ya, yz);
+    }
+    cp_wait_all();
+}
+
+}  // namespace
+
+int32_t launch_octave_fused(const float* L0, int R, int C, float* dog, float* mag, float* ang, float* down,
+                            int down_cols, cudaStream_t s) {
+    static bool attr = false;
+    if (!attr) {
+        FSB_CUDA(cudaFuncSetAttribute(k_octave, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES));
+        FSB_CUDA(cudaFuncSetAttribute(k_octave, cudaFuncAttributePreferredSharedMemoryCarveout, 100));
+        attr = true;
+    }
+    Args a;
+    a.L0 = L0;
+    a.R = R;
+    a.C = C;
+    const long long RC = (long long)R * C;
+    for (int i = 0; i < 5; ++i) a.dog[i] = dog + i * RC;
+    for (int i = 0; i < 3; ++i) {
+        a.mag[i] = mag + i * RC;
+        a.ang[i] = ang + i * RC;
+    }
+    a.down = down;
+    a.down_cols = down_cols;
+    // about two CTAs per SM over the whole octave
+    const int strips = (C + SW - 1) / SW;
+    int chunks = (2 * 148 + strips / 2) / strips;
+    if (chunks < 1) chunks = 1;
+    int rows = (R + chunks - 1) / chunks;
+    if (rows < 32) rows = 32;
+    a.rows_per_cta = rows;
+    dim3 grid(strips, (R + rows - 1) / rows);
+    k_octave<<<grid, NT, SMEM_BYTES, s>>>(a);
+    note_launch();
+    FSB_CUDA(cudaGetLastError());
+    return FSB_OK;
+}
+
+}  // namespace fsb

@@ -58,7 +58,7 @@ int32_t upload_taps() {
         }
     FSB_CUDA(cudaMemcpyToSymbol(c_taps, f, sizeof(f)));
     FSB_CUDA(cudaMemcpyToSymbol(c_taps_d, d, sizeof(d)));
-    return FSB_OK;
+    return upload_octave_taps(&kTaps[0][0], 27, kTapCount);
 }
 
 Geometry make_geometry(int h, int w) {
@@ -202,6 +202,10 @@ void launch(bool exact, const BlurArgs& a, cudaStream_t s) {
 
 }  // namespace
 
+// octaves at least this wide go through the fused kernel (octave.cu); narrower ones have too
+// little work per row to amortise its 84-row pipeline fill and use the per-layer kernels
+static const int kFusedMinCols = 2000;
+
 int32_t run_pyramid(Workspace& ws, const uint8_t* d_img, int img_stride, bool exact, cudaStream_t s) {
     const Geometry& g = ws.g;
     float* P[3] = {ws.plane[0].as<float>(), ws.plane[1].as<float>(), ws.plane[2].as<float>()};
@@ -217,29 +221,40 @@ int32_t run_pyramid(Workspace& ws, const uint8_t* d_img, int img_stride, bool ex
     a.cols = g.C[0];
     a.dst = P[0];
     launch<0, 5, true>(exact, a, s);
+    float* cur = P[0];   // base of the current octave
     for (int o = 0; o < g.n_oct; ++o) {
         const long long RC = (long long)g.R[o] * g.C[o];
         float* dog = DF + g.dog_off[o];
         float* mag = MAG + g.grad_off[o];
         float* ang = ANG + g.grad_off[o];
+        float* other[2];
+        for (int k = 0, n = 0; k < 3; ++k)
+            if (P[k] != cur) other[n++] = P[k];
+        if (!exact && g.C[o] >= kFusedMinCols) {
+            // fused octave: reads cur, writes the next base into another plane
+            float* down = o + 1 < g.n_oct ? other[0] : nullptr;
+            FSB_TRY(launch_octave_fused(cur, g.R[o], g.C[o], dog, mag, ang, down, o + 1 < g.n_oct ? g.C[o + 1] : 0, s));
+            cur = other[0];
+            continue;
+        }
         BlurArgs b{};
         b.rows = g.R[o];
         b.cols = g.C[o];
-        // layer 1: L0 (P0) -> P1, DoG 0
-        b.src = P[0]; b.dst = P[1]; b.dog = dog;
+        // layer 1: L0 -> X, DoG 0
+        b.src = cur; b.dst = other[0]; b.dog = dog;
         launch<1, 5, false>(exact, b, s);
-        // layer 2: L1 (P1) -> P2, DoG 1, gradient of L1
-        b.src = P[1]; b.dst = P[2]; b.dog = dog + RC; b.mag = mag; b.ang = ang;
+        // layer 2: L1 (X) -> Y, DoG 1, gradient of L1
+        b.src = other[0]; b.dst = other[1]; b.dog = dog + RC; b.mag = mag; b.ang = ang;
         launch<2, 6, false>(exact, b, s);
-        // layer 3: L2 (P2) -> P1, DoG 2, gradient of L2
-        b.src = P[2]; b.dst = P[1]; b.dog = dog + 2 * RC; b.mag = mag + RC; b.ang = ang + RC;
+        // layer 3: L2 (Y) -> X, DoG 2, gradient of L2
+        b.src = other[1]; b.dst = other[0]; b.dog = dog + 2 * RC; b.mag = mag + RC; b.ang = ang + RC;
         launch<3, 8, false>(exact, b, s);
-        // layer 4: L3 (P1) -> P2, DoG 3, gradient of L3, L3[::2, ::2] -> P0 (next octave base)
-        b.src = P[1]; b.dst = P[2]; b.dog = dog + 3 * RC; b.mag = mag + 2 * RC; b.ang = ang + 2 * RC;
-        if (o + 1 < g.n_oct) { b.down = P[0]; b.down_cols = g.C[o + 1]; }
+        // layer 4: L3 (X) -> Y, DoG 3, gradient of L3, L3[::2, ::2] -> the (dead) base plane
+        b.src = other[0]; b.dst = other[1]; b.dog = dog + 3 * RC; b.mag = mag + 2 * RC; b.ang = ang + 2 * RC;
+        if (o + 1 < g.n_oct) { b.down = cur; b.down_cols = g.C[o + 1]; }
         launch<4, 10, false>(exact, b, s);
-        // layer 5: L4 (P2) -> DoG 4 only
-        b.src = P[2]; b.dst = nullptr; b.dog = dog + 4 * RC; b.mag = nullptr; b.ang = nullptr; b.down = nullptr;
+        // layer 5: L4 (Y) -> DoG 4 only
+        b.src = other[1]; b.dst = nullptr; b.dog = dog + 4 * RC; b.mag = nullptr; b.ang = nullptr; b.down = nullptr;
         launch<5, 13, false>(exact, b, s);
     }
     FSB_CUDA(cudaGetLastError());

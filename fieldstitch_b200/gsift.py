@@ -33,6 +33,27 @@ class State:
             _lib.load().fsb_state_free(self.handle)
             self.handle = None
 
+    def atlas(self):
+        """(shapes [(R, C)], DoG list of (5,R,C), magnitude list of (3,R,C), angle list of (3,R,C))
+        copied to host - the reference state's `_Atlas` content per octave."""
+        lib = _lib.load()
+        n = ctypes.c_int32()
+        rows = np.zeros(16, np.int32)
+        cols = np.zeros(16, np.int32)
+        _lib.check(lib.fsb_state_geometry(self.handle, ctypes.byref(n), _lib.ptr(rows), _lib.ptr(cols)), "geometry")
+        shapes = [(int(rows[o]), int(cols[o])) for o in range(n.value)]
+        out = []
+        for which, layers in ((0, 5), (1, 3), (2, 3)):
+            tot = sum(layers * r * c for r, c in shapes)
+            buf = np.empty(tot, np.float32)
+            _lib.check(lib.fsb_state_atlas(self.handle, which, _lib.ptr(buf), tot), "fsb_state_atlas")
+            per, at = [], 0
+            for r, c in shapes:
+                per.append(buf[at:at + layers * r * c].reshape(layers, r, c))
+                at += layers * r * c
+            out.append(per)
+        return shapes, out[0], out[1], out[2]
+
     def __del__(self):
         try:
             self.close()

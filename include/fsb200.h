@@ -102,6 +102,12 @@ int32_t fsb_describe(fsb_ctx* ctx, fsb_state* st, int32_t n, const float* x, con
                      const float* size, const float* angle, const int32_t* octave,
                      const int32_t* layer, float* desc, uint8_t* rootsift);
 int32_t fsb_state_free(fsb_state* st);
+/* The detect state's atlases (gsift's `_Atlas`, app/planesite/gsift.py:227-267): octave count and
+   per-octave rows/cols (capacity 16 each), then a copy of one atlas into host memory:
+   which = 0 DoG [octave][layer 0..4][R][C], 1 gradient magnitude, 2 gradient angle (degrees)
+   [octave][layer 1..3][R][C]; n_floats must equal the atlas size. */
+int32_t fsb_state_geometry(fsb_state* st, int32_t* n_oct, int32_t* rows, int32_t* cols);
+int32_t fsb_state_atlas(fsb_state* st, int32_t which, float* out, int64_t n_floats);
 
 /* features.sift_gpu (app/planesite/features.py:115-129) in one device pass: detect with
    max_kp = int(2.2 nfeat) (p->max_kp is ignored), grid-spread selection of nfeat keypoints

@@ -1,0 +1,73 @@
+"""The device pyramid (DoG, gradient magnitude and angle atlases) against the oracle's, octave by
+octave. With FSB_SIFT_EXACT_BLUR the DoG and magnitude atlases are bit-identical to the
+reference's NumPy/SciPy path; the float32 FMA path (fused streaming kernel for wide octaves,
+per-layer kernels for narrow ones) stays within a few float32 ulps."""
+import numpy as np
+import pytest
+
+from sift_compare import paired_fraction
+
+pytestmark = pytest.mark.gpu
+
+SIZES = [(240, 320, 11), (495, 660, 77), (989, 1320, 5)]
+
+
+@pytest.fixture(scope="module")
+def oracle_pyr():
+    from fieldstitch_b200 import synth
+    from oracle import gsift_ref
+    out = {}
+    for h, w, seed in SIZES:
+        img = synth.synth_image(h, w, seed)
+        octs = gsift_ref.build_pyramid(img)
+        out[(h, w)] = (img, [o["dog"] for o in octs], [gsift_ref.gradients(o) for o in octs])
+    return out
+
+
+def _ang_diff(a, b):
+    d = np.abs(a.astype(np.float64) - b.astype(np.float64)) % 360.0
+    return np.minimum(d, 360.0 - d)
+
+
+@pytest.mark.parametrize("hw", [(h, w) for h, w, _ in SIZES])
+def test_atlas_exact_is_bit_identical(oracle_pyr, hw):
+    import fieldstitch_b200 as f
+    img, dogs, grads = oracle_pyr[hw]
+    _, st = f.gsift.detect(img, exact=True)
+    shapes, dog, mag, ang = st.atlas()
+    assert shapes == [d.shape[1:] for d in dogs]
+    for o in range(len(shapes)):
+        np.testing.assert_array_equal(dog[o], dogs[o], err_msg="DoG octave %d" % o)
+        np.testing.assert_array_equal(mag[o], grads[o][0], err_msg="magnitude octave %d" % o)
+        assert _ang_diff(ang[o], grads[o][1]).max() < 1e-3
+
+
+@pytest.mark.parametrize("hw", [(h, w) for h, w, _ in SIZES])
+def test_atlas_fast_within_ulps(oracle_pyr, hw):
+    import fieldstitch_b200 as f
+    img, dogs, grads = oracle_pyr[hw]
+    _, st = f.gsift.detect(img)
+    shapes, dog, mag, ang = st.atlas()
+    for o in range(len(shapes)):
+        ddog = np.abs(dog[o] - dogs[o])
+        assert ddog.max() < 2e-6, (o, ddog.max())
+        assert ddog.mean() < 5e-8, (o, ddog.mean())
+        assert np.abs(mag[o] - grads[o][0]).max() < 4e-6
+        # the angle error scales like (float32 error of dx, dy) / magnitude
+        for floor, tol in ((1e-3, 0.05), (1e-2, 0.01)):
+            strong = grads[o][0] > floor
+            assert _ang_diff(ang[o][strong], grads[o][1][strong]).max() < tol, (o, floor)
+
+
+def test_detect_fast_wide_image_matches_oracle():
+    """1320 x 989 (config-1 size; octave 0 is 2640 wide and takes the fused kernel)."""
+    import fieldstitch_b200 as f
+    from fieldstitch_b200 import synth
+    from oracle import gsift_ref
+    img = synth.synth_image(989, 1320, 5)
+    ref, _ = gsift_ref.detect(img, max_kp=100000, contrast=0.04, edge=10.0)
+    got, _ = f.gsift.detect(img, max_kp=100000, contrast=0.04, edge=10.0)
+    frac, _ = paired_fraction(ref, got)
+    assert frac >= 0.97, frac
+    back, _ = paired_fraction(got, ref)
+    assert back >= 0.97, back
