@@ -50,6 +50,7 @@ def parse():
     p.add_argument("--seed", type=int, default=1000)
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-cpu", action="store_true")
+    p.add_argument("--streams", type=int, default=4, help="host threads, each with its own context/stream")
     return p.parse_args()
 
 
@@ -201,6 +202,7 @@ def run_reference(args):
 # ---------------------------------------------------------------------------------- GPU arm
 def run_fsb(args):
     import ctypes
+    from concurrent.futures import ThreadPoolExecutor
 
     import torch
 
@@ -218,72 +220,104 @@ def run_fsb(args):
 
     import fieldstitch_b200 as F
     from fieldstitch_b200 import _lib, synth
-    ctx = F.context(local)
-    L = ctx.lib
-    stream = torch.cuda.ExternalStream(ctx.stream())
     dev = torch.device("cuda", local)
     h, w = H_IMG, W_IMG
     nmax = 16000
     # device-resident inputs and per-pair prior errors
     d_img = [(torch.from_numpy(a).to(dev), torch.from_numpy(b).to(dev)) for a, b, _, _, _ in pairs]
     d_noise = [torch.from_numpy(synth.prior_noise(nmax, args.seed + 7 * i)).to(dev) for i in range(len(pairs))]
-    xy = [torch.empty((nmax, 2), dtype=torch.float32, device=dev) for _ in range(2)]
-    rs = [torch.empty(nmax, dtype=torch.float32, device=dev) for _ in range(2)]
-    u8 = [torch.empty((nmax, 128), dtype=torch.uint8, device=dev) for _ in range(2)]
-    pred = torch.empty((nmax, 2), dtype=torch.float64, device=dev)
-    bxy = torch.empty((nmax, 2), dtype=torch.float64, device=dev)
-    dq = torch.empty(nmax, dtype=torch.int64, device=dev)
-    dt = torch.empty(nmax, dtype=torch.int64, device=dev)
     eye = np.eye(3).reshape(9).copy()
     Hs = [np.ascontiguousarray(p[2].reshape(9)) for p in pairs]
     prm = _lib.SiftParams(0.015, 12.0, 0, 0)
-    n_out = ctypes.c_int32()
-    torch.cuda.synchronize()
 
     def P(t):
         return ctypes.c_void_p(t.data_ptr())
 
+    class Worker:
+        """One context (stream + workspaces) and its output buffers; runs the pairs i = idx mod n."""
+
+        def __init__(self, idx, n):
+            self.items = list(range(idx, len(pairs), n))
+            self.ctx = _lib.Context(local)
+            self.L = self.ctx.lib
+            self.stream = torch.cuda.ExternalStream(self.ctx.stream())
+            self.xy = [torch.empty((nmax, 2), dtype=torch.float32, device=dev) for _ in range(2)]
+            self.rs = [torch.empty(nmax, dtype=torch.float32, device=dev) for _ in range(2)]
+            self.u8 = [torch.empty((nmax, 128), dtype=torch.uint8, device=dev) for _ in range(2)]
+            self.pred = torch.empty((nmax, 2), dtype=torch.float64, device=dev)
+            self.bxy = torch.empty((nmax, 2), dtype=torch.float64, device=dev)
+            self.dq = torch.empty(nmax, dtype=torch.int64, device=dev)
+            self.dt = torch.empty(nmax, dtype=torch.int64, device=dev)
+            self.n_out = ctypes.c_int32()
+
+        def run(self, items=None):
+            L, c, n_out = self.L, self.ctx.handle, self.n_out
+            matches = 0
+            for i in (self.items if items is None else items):
+                ia, ib = d_img[i]
+                n = []
+                for k, (img, nf) in enumerate(((ia, pairs[i][3]), (ib, pairs[i][4]))):
+                    _lib.check(L.fsb_sift_features_d(c, P(img), h, w, w, ctypes.byref(prm), nf, P(self.xy[k]),
+                                                     P(self.rs[k]), None, P(self.u8[k]), ctypes.byref(n_out)), "sift")
+                    n.append(n_out.value)
+                _lib.check(L.fsb_project_d(c, P(self.xy[0]), n[0], _lib.ptr(Hs[i]), P(d_noise[i]), P(self.pred)),
+                           "proj")
+                _lib.check(L.fsb_project_d(c, P(self.xy[1]), n[1], _lib.ptr(eye), None, P(self.bxy)), "proj")
+                _lib.check(L.fsb_match_guided_d(c, P(self.pred), P(self.u8[0]), n[0], P(self.bxy), P(self.u8[1]), n[1],
+                                                float(w), float(h), RADIUS, KC, RATIO, P(self.dq), P(self.dt),
+                                                ctypes.byref(n_out)), "guided")
+                matches += n_out.value
+            return matches
+
+    workers = [Worker(i, args.streams) for i in range(args.streams)]
+    pool = ThreadPoolExecutor(max_workers=args.streams)
+
     def one_step():
-        matches = 0
-        for i, (ia, ib) in enumerate(d_img):
-            n = []
-            for k, (img, nf) in enumerate(((ia, pairs[i][3]), (ib, pairs[i][4]))):
-                _lib.check(L.fsb_sift_features_d(ctx.handle, P(img), h, w, w, ctypes.byref(prm), nf, P(xy[k]),
-                                                 P(rs[k]), None, P(u8[k]), ctypes.byref(n_out)), "sift")
-                n.append(n_out.value)
-            _lib.check(L.fsb_project_d(ctx.handle, P(xy[0]), n[0], _lib.ptr(Hs[i]), P(d_noise[i]), P(pred)), "proj")
-            _lib.check(L.fsb_project_d(ctx.handle, P(xy[1]), n[1], _lib.ptr(eye), None, P(bxy)), "proj")
-            _lib.check(L.fsb_match_guided_d(ctx.handle, P(pred), P(u8[0]), n[0], P(bxy), P(u8[1]), n[1], float(w),
-                                            float(h), RADIUS, KC, RATIO, P(dq), P(dt), ctypes.byref(n_out)), "guided")
-            matches += n_out.value
-        return matches
+        return sum(f.result() for f in [pool.submit(wk.run) for wk in workers])
 
     def barrier():
         if dist is not None:
             dist.barrier()
 
+    def timed(fn, steps):
+        """Device time of `steps` calls of fn: start event on the current stream, every worker
+        stream waits on it; every worker stream records its end, the current stream waits on all."""
+        main = torch.cuda.current_stream(dev)
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record(main)
+        for wk in workers:
+            wk.stream.wait_event(e0)
+        out = 0
+        for _ in range(steps):
+            out += fn()
+        for wk in workers:
+            ev = torch.cuda.Event()
+            ev.record(wk.stream)
+            main.wait_event(ev)
+        e1.record(main)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / steps, out
+
     for _ in range(args.warmup):
         one_step()
     torch.cuda.synchronize()
     barrier()
-    ctx.timing(True)
-    ctx.stage_times()
+    for wk in workers:
+        wk.ctx.timing(True)
+        wk.ctx.stage_times()
     clocks = Clocks(gpu_smi_id(torch, local))
     launches0 = _lib.launch_count()
-    e0 = torch.cuda.Event(enable_timing=True)
-    e1 = torch.cuda.Event(enable_timing=True)
-    torch.cuda.synchronize()
-    e0.record(stream)
-    matches = 0
-    for _ in range(args.steps):
-        matches += one_step()
-    e1.record(stream)
-    torch.cuda.synchronize()
+    ms_step, matches = timed(one_step, args.steps)
     clk = clocks.stop()
     launches = _lib.launch_count() - launches0
-    stages = ctx.stage_times()
-    ctx.timing(False)
-    ms_step = e0.elapsed_time(e1) / args.steps
+    stages = {}
+    for wk in workers:
+        for k_, (ms_, n_) in wk.ctx.stage_times().items():
+            a_, b_ = stages.get(k_, (0.0, 0))
+            stages[k_] = (a_ + ms_, b_ + n_)
+        wk.ctx.timing(False)
     if dist is not None:
         t = torch.tensor([ms_step], device=dev)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
@@ -296,48 +330,68 @@ def run_fsb(args):
     if not args.no_e2e:
         host = [(np.ascontiguousarray(a), np.ascontiguousarray(b)) for a, b, _, _, _ in pairs]
 
-        def e2e_step():
-            h2d = d2h = 0
-            for i, (a, b) in enumerate(host):
-                xa, ua, _ = F.features.sift_gpu_u8(a, pairs[i][3])
-                xb, ub, _ = F.features.sift_gpu_u8(b, pairs[i][4])
-                pr = synth.apply_homography(pairs[i][2], xa) + \
-                    synth.prior_noise(nmax, args.seed + 7 * i)[:len(xa)].astype(np.float64)
-                q, _ = F.matching.guided_from_pred(pr, ua, xb.astype(np.float64), ub, (w, h), RADIUS, KC, RATIO)
-                h2d += a.nbytes + b.nbytes + pr.nbytes + ua.nbytes + 16 * len(xb) + ub.nbytes
-                d2h += (len(xa) + len(xb)) * (8 + 4 + 128) + 16 * len(q) + 16
+        def e2e_pair(i):
+            a, b = host[i]
+            xa, ua, _ = F.features.sift_gpu_u8(a, pairs[i][3], device=local)
+            xb, ub, _ = F.features.sift_gpu_u8(b, pairs[i][4], device=local)
+            pr = synth.apply_homography(pairs[i][2], xa) + \
+                synth.prior_noise(nmax, args.seed + 7 * i)[:len(xa)].astype(np.float64)
+            q, _ = F.matching.guided_from_pred(pr, ua, xb.astype(np.float64), ub, (w, h), RADIUS, KC, RATIO,
+                                               device=local)
+            h2d = a.nbytes + b.nbytes + pr.nbytes + ua.nbytes + 16 * len(xb) + ub.nbytes
+            d2h = (len(xa) + len(xb)) * (8 + 4 + 128) + 16 * len(q) + 16
             return h2d, d2h
+
+        def e2e_step():
+            res = list(pool.map(e2e_pair, range(len(pairs))))
+            return sum(r[0] for r in res), sum(r[1] for r in res)
 
         e2e_step()
         torch.cuda.synchronize()
         barrier()
-        f0 = torch.cuda.Event(enable_timing=True)
-        f1 = torch.cuda.Event(enable_timing=True)
-        f0.record(stream)
-        h2d = d2h = 0
         ksteps = max(1, args.steps // 2)
+        f0 = time.perf_counter()
+        main = torch.cuda.current_stream(dev)
+        g0 = torch.cuda.Event(enable_timing=True)
+        g1 = torch.cuda.Event(enable_timing=True)
+        g0.record(main)
+        h2d = d2h = 0
         for _ in range(ksteps):
-            a_, b_ = e2e_step()
-            h2d, d2h = a_, b_
-        f1.record(stream)
+            h2d, d2h = e2e_step()
+        # the host API returns only after its results are in host memory, so the device is idle
+        # here; the device-side events bracket the whole region on the synchronised device
         torch.cuda.synchronize()
-        ms_e2e = f0.elapsed_time(f1) / ksteps
+        g1.record(main)
+        torch.cuda.synchronize()
+        ms_e2e = max(g0.elapsed_time(g1), (time.perf_counter() - f0) * 1000.0) / ksteps
         if dist is not None:
             t = torch.tensor([ms_e2e], device=dev)
             dist.all_reduce(t, op=dist.ReduceOp.MAX)
             ms_e2e = float(t.item())
         e2e = {"value": world * args.pairs / (ms_e2e / 1000.0), "unit": "pairs/s", "h2d_bytes_per_step": int(h2d),
-               "d2h_bytes_per_step": int(d2h), "ms_per_step": ms_e2e, "steps": ksteps}
+               "d2h_bytes_per_step": int(d2h), "ms_per_step": ms_e2e, "steps": ksteps,
+               "api": "features.sift_gpu_u8 + matching.guided_from_pred, %d host threads" % args.streams}
 
-    # ---- roofline of the dominant stage (pyramid), from the events of the timed steps
+    # ---- roofline of the dominant stage (pyramid): CUDA events on the library stream, one stream
+    # alone (8 images), so the per-image time is not inflated by the other streams' kernels
+    iso = workers[0]
+    iso.ctx.timing(True)
+    iso.ctx.stage_times()
+    iso.run(items=list(range(min(4, len(pairs)))))
+    iso_st = iso.ctx.stage_times()
+    iso.ctx.timing(False)
     pk, pk_src = peaks()
-    pyr_ms, pyr_n = stages["pyramid"]
+    pyr_ms, pyr_n = iso_st["pyramid"]
     per_img_ms = pyr_ms / max(pyr_n, 1)
     alg = pyramid_bytes(h, w)
     achieved = alg / (per_img_ms / 1000.0) / 1e9 if per_img_ms > 0 else None
-    roof = {"bound": "hbm", "kernel": "pyramid (k_blur launches of one image)", "achieved": achieved, "peak": pk,
-            "peak_source": pk_src, "unit": "GB/s", "frac": (achieved / pk) if achieved else None,
-            "traffic": traffic_per_pyramid(), "algorithmic_bytes": alg, "ms_per_launch_group": per_img_ms}
+    c_ms, c_n = stages["pyramid"]
+    roof = {"bound": "hbm", "kernel": "pyramid (fused octave kernels + per-layer kernels of one image)",
+            "achieved": achieved, "peak": pk, "peak_source": pk_src, "unit": "GB/s",
+            "frac": (achieved / pk) if achieved else None, "traffic": traffic_per_pyramid(),
+            "algorithmic_bytes": alg, "ms_per_launch_group": per_img_ms,
+            "measured": "CUDA events on the library stream, one stream alone, %d images" % pyr_n,
+            "ms_per_launch_group_in_timed_region": c_ms / max(c_n, 1)}
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
@@ -351,11 +405,15 @@ def run_fsb(args):
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": "pairs/s", "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
-                "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded)", "config": config(args),
+                "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded)",
+                "config": config(args, {"host_streams": args.streams}),
                 "clocks": clk, "e2e": e2e, "gpu_launches": int(launches), "roofline": roof, "cpu_baseline": cpu,
                 "matches_per_step": matches / args.steps,
-                "stages_ms_per_step": {k: v[0] / args.steps for k, v in stages.items()}}
+                "stages_ms_per_step_summed_over_streams": {k: v[0] / args.steps for k, v in stages.items()}}
         print(json.dumps(line), flush=True)
+    pool.shutdown()
+    for wk in workers:
+        wk.ctx.close()
     if dist is not None:
         barrier()
         dist.destroy_process_group()
