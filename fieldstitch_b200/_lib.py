@@ -56,6 +56,8 @@ SIGNATURES = [
                                    c_vp, c_vp, c_vp]),
     ("fsb_match_bf_d", c_i32, [c_vp, c_vp, c_i32, c_vp, c_i32, c_f32, c_i32, c_vp, c_vp, c_vp]),
     ("fsb_match_bf_noalloc", c_i32, [c_vp, c_i32, c_vp, c_i32, c_f32, c_vp, c_vp, c_vp, c_vp]),
+    ("fsb_match_bf_batch_d", c_i32, [c_vp, c_i32, c_vp, c_vp, c_vp, c_vp, c_f32, c_i32, c_vp, c_vp, c_vp]),
+    ("fsb_match_tc_stats", c_i32, [c_vp, c_vp, c_vp, c_vp, c_vp]),
 ]
 
 STAGES = ("upload", "pyramid", "extrema", "refine", "orientation", "sort", "spread", "describe", "match")

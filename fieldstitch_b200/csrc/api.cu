@@ -250,7 +250,8 @@ int32_t fsb_destroy(fsb_ctx* ctx) {
     }
     ctx->pool.clear();
     DevBuf* all[] = {&ctx->s_u8a, &ctx->s_u8b, &ctx->s_f32a, &ctx->s_f32b, &ctx->s_i32, &ctx->s_i64,
-                     &ctx->s_u64, &ctx->s_misc, &ctx->s_misc2, &ctx->s_host_stage, &ctx->s_cub};
+                     &ctx->s_u64, &ctx->s_misc, &ctx->s_misc2, &ctx->s_host_stage, &ctx->s_cub,
+                     &ctx->s_tc_pack, &ctx->s_tc_part, &ctx->s_tc_aux};
     for (DevBuf* b : all) b->release();
     if (ctx->pinned) cudaFreeHost(ctx->pinned);
     for (auto& e : ctx->ev)
@@ -299,7 +300,8 @@ int64_t fsb_device_bytes(fsb_ctx* ctx) {
     int64_t t = 0;
     for (Workspace* w : ctx->pool) t += (int64_t)w->bytes();
     const DevBuf* all[] = {&ctx->s_u8a, &ctx->s_u8b, &ctx->s_f32a, &ctx->s_f32b, &ctx->s_i32, &ctx->s_i64,
-                           &ctx->s_u64, &ctx->s_misc, &ctx->s_misc2, &ctx->s_host_stage, &ctx->s_cub};
+                           &ctx->s_u64, &ctx->s_misc, &ctx->s_misc2, &ctx->s_host_stage, &ctx->s_cub,
+                     &ctx->s_tc_pack, &ctx->s_tc_part, &ctx->s_tc_aux};
     for (const DevBuf* b : all) t += (int64_t)b->bytes;
     return t;
 }
@@ -554,6 +556,73 @@ int32_t fsb_match_bf_d(fsb_ctx* ctx, const uint8_t* d_a, int32_t na, const uint8
     FSB_CUDA(cudaStreamSynchronize(s));
     ctx->stage_end(ST_MATCH);
     *n_out = n;
+    return FSB_OK;
+}
+
+int32_t fsb_match_bf_batch_d(fsb_ctx* ctx, int32_t n_pairs, const uint8_t* const* d_a, const int32_t* na,
+                             const uint8_t* const* d_b, const int32_t* nb, float ratio, int32_t precision,
+                             int64_t* const* d_q, int64_t* const* d_t, int32_t* n_out) {
+    FSB_ARG(ctx && n_out && n_pairs >= 0, "bad arguments");
+    FSB_ARG(n_pairs == 0 || (d_a && na && d_b && nb && d_q && d_t), "null array");
+    FSB_ARG(precision >= FSB_PREC_FP32 && precision <= FSB_PREC_FP8, "unknown precision");
+    for (int p = 0; p < n_pairs; ++p) {
+        FSB_ARG(na[p] >= 0 && nb[p] >= 0, "negative size");
+        FSB_ARG((na[p] == 0 || (d_a[p] && d_q[p] && d_t[p])) && (nb[p] == 0 || d_b[p]), "null array");
+        n_out[p] = 0;
+    }
+    if (n_pairs == 0) return FSB_OK;
+    FSB_TRY(use_device(ctx));
+    cudaStream_t s = ctx->stream;
+    FSB_TRY(ctx->s_misc2.ensure(64));
+    std::vector<int> live;
+    for (int p = 0; p < n_pairs; ++p)
+        if (na[p] >= 2 && nb[p] >= 2) live.push_back(p);
+    if (live.empty()) return FSB_OK;
+    ctx->stage_begin(ST_MATCH);
+    std::vector<int> cnt(n_pairs, 0);
+    FSB_TRY(ctx->s_host_stage.ensure((size_t)n_pairs * 4 + 64));
+    int* dn_all = ctx->s_host_stage.as<int>();
+    FSB_CUDA(cudaMemsetAsync(dn_all, 0, (size_t)n_pairs * 4, s));
+    if (precision == FSB_PREC_FP32) {
+        for (int p : live)
+            FSB_TRY(run_match_bf(ctx, d_a[p], na[p], d_b[p], nb[p], ratio, precision, d_q[p], d_t[p], dn_all + p, s));
+    } else {
+        std::vector<const uint8_t*> pa, pb;
+        std::vector<int> ra, rb, row0;
+        int rows = 0;
+        for (int p : live) {
+            pa.push_back(d_a[p]);
+            pb.push_back(d_b[p]);
+            ra.push_back(na[p]);
+            rb.push_back(nb[p]);
+            row0.push_back(rows);
+            rows += na[p];
+        }
+        FSB_TRY(ctx->s_i32.ensure((size_t)rows * 8 + 64));
+        int32_t* t_row = ctx->s_i32.as<int32_t>();
+        uint32_t* d_row = reinterpret_cast<uint32_t*>(t_row + rows);
+        FSB_TRY(run_match_bf_tc_rows(ctx, (int)live.size(), pa.data(), ra.data(), pb.data(), rb.data(), ratio,
+                                     precision, t_row, d_row, row0.data(), &ctx->tc_stats, s));
+        for (size_t i = 0; i < live.size(); ++i) {
+            const int p = live[i];
+            FSB_TRY(run_unique_rows(ctx, t_row + row0[i], d_row + row0[i], na[p], nb[p], d_q[p], d_t[p], dn_all + p,
+                                    s));
+        }
+    }
+    FSB_CUDA(cudaMemcpyAsync(cnt.data(), dn_all, (size_t)n_pairs * 4, cudaMemcpyDeviceToHost, s));
+    FSB_CUDA(cudaStreamSynchronize(s));
+    ctx->stage_end(ST_MATCH);
+    for (int p = 0; p < n_pairs; ++p) n_out[p] = cnt[p];
+    return FSB_OK;
+}
+
+int32_t fsb_match_tc_stats(fsb_ctx* ctx, int64_t* rows, int64_t* fallback_rows, double* max_abs_err,
+                           double* mean_abs_err) {
+    FSB_ARG(ctx, "ctx is null");
+    if (rows) *rows = ctx->tc_stats.rows;
+    if (fallback_rows) *fallback_rows = ctx->tc_stats.fallback_rows;
+    if (max_abs_err) *max_abs_err = ctx->tc_stats.max_abs_err;
+    if (mean_abs_err) *mean_abs_err = ctx->tc_stats.mean_abs_err;
     return FSB_OK;
 }
 

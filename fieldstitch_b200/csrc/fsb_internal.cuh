@@ -96,6 +96,14 @@ struct DevBuf {
     template <class T> T* as() const { return reinterpret_cast<T*>(p); }
 };
 
+// Outcome of one tensor-core dense match (all pairs of the call).
+struct TcStats {
+    long long rows = 0;            // query rows
+    long long fallback_rows = 0;   // rows recomputed exactly because the certificate did not hold
+    float max_abs_err = 0.f;       // |approximate - exact| best distance, largest over rows
+    float mean_abs_err = 0.f;      // and its mean
+};
+
 // Pyramid + detection workspace sized for one image geometry.
 struct Workspace {
     Geometry g{};
@@ -123,6 +131,8 @@ struct fsb_ctx {
     // scratch for description and matching (grown on demand)
     fsb::DevBuf s_u8a, s_u8b, s_f32a, s_f32b, s_i32, s_i64, s_u64, s_misc, s_misc2, s_host_stage;
     fsb::DevBuf s_cub;   // CUB temporary storage (one primitive at a time)
+    fsb::DevBuf s_tc_pack, s_tc_part, s_tc_aux;   // tensor-core matcher: packed operands, candidates, tables
+    fsb::TcStats tc_stats{};                      // of the last tensor-core dense match
     void* pinned = nullptr;
     size_t pinned_bytes = 0;
     // stage timers: events recorded at stage boundaries while timing is on
@@ -171,6 +181,12 @@ int32_t run_match_bf(fsb_ctx* ctx, const uint8_t* d_a, int na, const uint8_t* d_
 int32_t run_match_guided(fsb_ctx* ctx, const double* d_pred, const uint8_t* d_a, int na, const double* d_bxy,
                          const uint8_t* d_b, int nb, double wb, double hb, double radius, int kc, float ratio,
                          int64_t* d_q, int64_t* d_t, int* d_n, cudaStream_t s);
+int32_t run_unique_rows(fsb_ctx* ctx, const int32_t* t_row, const uint32_t* d_row, int na, int nb, int64_t* d_q,
+                        int64_t* d_t, int* d_n, cudaStream_t s);
+// tc_match.cu
+int32_t run_match_bf_tc_rows(fsb_ctx* ctx, int n_pairs, const uint8_t* const* d_a, const int* na,
+                             const uint8_t* const* d_b, const int* nb, float ratio, int precision, int32_t* t_row,
+                             uint32_t* d_row, const int* row0, TcStats* stats, cudaStream_t s);
 int32_t run_perspective(const double* d_xy, int n, const double* hm9, double* d_out, cudaStream_t s);
 int32_t run_project(const float* d_xy, int n, const double* hm9_host, const float* d_off, double* d_out,
                     cudaStream_t s);

@@ -1,0 +1,897 @@
+// Dense descriptor matching on the tcgen05 tensor cores (sm_100a).
+//
+// matching._ratio_match_bf (app/planesite/matching.py:86-100) needs, for every query row a_q, the
+// smallest and second-smallest d2(q, j) = |a_q|^2 + |b_j|^2 - 2 a_q.b_j over all target rows b_j
+// and the index of the smallest. Here that contraction runs as one K-major GEMM per pair:
+//
+//   k_tc_pack    uint8 rows -> operand rows in the canonical no-swizzle core-matrix layout
+//                (8 rows x 16 bytes per core matrix, one contiguous block per 128 rows):
+//                BF16: 128 descriptor values + 16 extra slots that carry the norm term, so that
+//                      a'.b' = a.b - |b|^2 / 2 (query slots -32768, -128, -0.5; target slots the
+//                      three bytes of |b|^2). For uint8 data every product and partial sum is an
+//                      integer or half-integer below 2^23, so the FP32 accumulation is exact.
+//                E4M3: per-row power-of-two scale s with max(row) * s <= 448, round to nearest;
+//                      the norm term and the column scale are applied in the epilogue.
+//   k_tc_dense   persistent warp-specialised kernel. Warp 0 streams 128-row target tiles into a
+//                shared-memory ring with bulk asynchronous copies (no tensor map, no multicast);
+//                warp 1 issues tcgen05.mma (M=128, N=128) for the two 128-row halves of a 256-row
+//                query block into double-buffered FP32 accumulators (4 x 128 of the 512 TMEM
+//                columns); warps 2-9 read the accumulators with tcgen05.ld and keep, per query row,
+//                the K largest values of a'.b' over 32-column chunks and the chunks they came from.
+//   k_tc_finish  per query row: the K best chunks of all column splits, exact integer distances
+//                of their columns (dp4a), top-2, the float32 ratio test of the reference, and a
+//                certificate that no column outside those chunks can change the decision. With
+//                BF16 the certificate always holds; with E4M3 it uses a bound on the rounding
+//                error, and rows it cannot settle are recomputed by k_tc_exact_rows.
+//
+// Results (the best target, the exact best distance, the accept decision) are therefore the
+// same as those of the CUDA-core FP32 path and of the reference for every precision.
+#include <cuda_fp8.h>
+
+#include <cfloat>
+#include <cmath>
+#include <vector>
+
+#include "fsb_internal.cuh"
+
+namespace fsb {
+namespace {
+
+inline unsigned nblk(long long n, int t) { return (unsigned)((n + t - 1) / t); }
+
+constexpr int TC_THREADS = 320;      // producer warp, MMA warp, 8 epilogue warps
+constexpr int TC_ROWS = 256;         // query rows per work item (two M=128 halves)
+constexpr int TC_N = 128;            // target rows per tile (MMA N)
+constexpr int TC_CHUNK = 32;         // columns per tcgen05.ld and per candidate chunk
+constexpr int TC_MAX_SPLITS = 8;
+constexpr long long TC_TIMEOUT_CYCLES = 4000000000ll;   // about two seconds at full clock
+
+template <int PREC> struct TcTraits;
+template <> struct TcTraits<FSB_PREC_BF16> {
+    static constexpr int ROW_BYTES = 288;   // 144 BF16 values
+    static constexpr int KSTEPS = 9;        // K = 16 per MMA (32 bytes)
+    static constexpr int STAGES = 4;
+    static constexpr int TOPK = 2;
+    // kind::f16: F32 accumulator (bit 4), A and B BF16 (bits 7, 10), K-major, N>>3 at 17, M>>4 at 24
+    static constexpr uint32_t IDESC = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(TC_N >> 3) << 17) |
+                                      ((uint32_t)(128 >> 4) << 24);
+};
+template <> struct TcTraits<FSB_PREC_FP8> {
+    static constexpr int ROW_BYTES = 128;   // 128 E4M3 values
+    static constexpr int KSTEPS = 4;        // K = 32 per MMA (32 bytes)
+    static constexpr int STAGES = 8;
+    static constexpr int TOPK = 4;
+    // kind::f8f6f4: F32 accumulator, A and B E4M3 (format 0), K-major
+    static constexpr uint32_t IDESC = (1u << 4) | ((uint32_t)(TC_N >> 3) << 17) | ((uint32_t)(128 >> 4) << 24);
+};
+
+template <int PREC> constexpr int tile_bytes() { return 128 * TcTraits<PREC>::ROW_BYTES; }
+template <int PREC> constexpr int smem_bytes() {
+    return 2 * tile_bytes<PREC>() + TcTraits<PREC>::STAGES * tile_bytes<PREC>() + 2048;
+}
+
+// Byte offset of (row, k-byte) inside a 128-row block: core matrix (row / 8, kb / 16) at
+// (row / 8) * SBO + (kb / 16) * 128, with SBO = ROW_BYTES * 8 (LBO = 128).
+__host__ __device__ constexpr int core_off(int row, int kb, int row_bytes) {
+    return (row >> 3) * (row_bytes * 8) + (kb >> 4) * 128 + (row & 7) * 16 + (kb & 15);
+}
+
+// ------------------------------------------------------------------------ per-pair tables
+struct TcPair {
+    const uint8_t* a;      // uint8 query rows (na x 128)
+    const uint8_t* b;      // uint8 target rows (nb x 128)
+    const uint8_t* pa;     // packed query blocks (rb x 256 rows)
+    const uint8_t* pb;     // packed target tiles (ntiles x 128 rows)
+    const float2* colsc;   // E4M3: per target (1 / s_b, |b|^2 / 2)
+    const float* rowsc;    // E4M3: per query (-s_a, 1 / s_a, |a|, |alpha|)
+    const float* bmax;     // E4M3: (max |b|, max |beta|) over the targets
+    const int32_t* nA;     // |a|^2
+    const int32_t* nB;     // |b|^2
+    int na, nb, nrb, ntiles, splits, tps;   // tps: tiles per split
+    int item0;             // first work item
+    int row0;              // first row in the concatenated row outputs
+    long long part0;       // first candidate record
+};
+
+struct Cand {
+    float v;   // a'.b' (BF16: exact; E4M3: s_a-scaled approximation until the end of the row)
+    int c;     // chunk index (column / 32), -1 when empty
+};
+
+__device__ __forceinline__ int find_pair(const TcPair* __restrict__ pairs, int np, int item) {
+    int lo = 0, hi = np - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (pairs[mid].item0 <= item) lo = mid; else hi = mid - 1;
+    }
+    return lo;
+}
+
+__device__ __forceinline__ int find_pair_row(const TcPair* __restrict__ pairs, int np, int row) {
+    int lo = 0, hi = np - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (pairs[mid].row0 <= row) lo = mid; else hi = mid - 1;
+    }
+    return lo;
+}
+
+// ------------------------------------------------------------------------ packing
+__device__ __forceinline__ uint16_t bf16_bits(float x) {
+    return (uint16_t)(__float_as_uint(x) >> 16);   // exact for the integers 0..255 and powers of two
+}
+
+// One warp per packed row (padding rows are written as zeros). role 0: query, 1: target.
+template <int PREC>
+__global__ void k_tc_pack(const uint8_t* __restrict__ src, int n, int n_pad, int role, uint8_t* __restrict__ dst,
+                          int32_t* __restrict__ norms, float2* __restrict__ colsc, float* __restrict__ rowsc,
+                          float* __restrict__ bmax) {
+    constexpr int RB = TcTraits<PREC>::ROW_BYTES;
+    const int row = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    const int lane = threadIdx.x & 31;
+    if (row >= n_pad) return;
+    uint8_t* blk = dst + (size_t)(row >> 7) * (128 * RB);
+    const int r = row & 127;
+    const uint32_t w = row < n ? reinterpret_cast<const uint32_t*>(src + (size_t)row * 128)[lane] : 0u;
+    int nrm = (int)__dp4a(w, w, 0u);
+    for (int sh = 16; sh; sh >>= 1) nrm += __shfl_xor_sync(0xffffffffu, nrm, sh);
+    if (lane == 0 && row < n) norms[row] = nrm;
+    if constexpr (PREC == FSB_PREC_BF16) {
+        uint2 v;
+        v.x = (uint32_t)bf16_bits((float)(w & 255u)) | ((uint32_t)bf16_bits((float)((w >> 8) & 255u)) << 16);
+        v.y = (uint32_t)bf16_bits((float)((w >> 16) & 255u)) | ((uint32_t)bf16_bits((float)(w >> 24)) << 16);
+        *reinterpret_cast<uint2*>(blk + core_off(r, lane * 8, RB)) = v;
+        if (lane < 4) {   // the 16 norm slots (32 bytes), 8 bytes per lane
+            uint16_t e[4] = {0, 0, 0, 0};
+            if (lane == 0 && row < n) {
+                if (role == 0) {
+                    e[0] = bf16_bits(-32768.f);
+                    e[1] = bf16_bits(-128.f);
+                    e[2] = bf16_bits(-0.5f);
+                } else {
+                    e[0] = bf16_bits((float)((nrm >> 16) & 255));
+                    e[1] = bf16_bits((float)((nrm >> 8) & 255));
+                    e[2] = bf16_bits((float)(nrm & 255));
+                }
+            }
+            uint2 x;
+            x.x = (uint32_t)e[0] | ((uint32_t)e[1] << 16);
+            x.y = (uint32_t)e[2] | ((uint32_t)e[3] << 16);
+            *reinterpret_cast<uint2*>(blk + core_off(r, 256 + lane * 8, RB)) = x;
+        }
+    } else {
+        // per-row power-of-two scale: the largest e <= 8 with max * 2^e <= 448
+        uint32_t mx = max(max(w & 255u, (w >> 8) & 255u), max((w >> 16) & 255u, w >> 24));
+        for (int sh = 16; sh; sh >>= 1) mx = max(mx, __shfl_xor_sync(0xffffffffu, mx, sh));
+        int e = 8;
+        while (e > 0 && (mx << e) > 448u) --e;
+        const float s = (float)(1 << e);
+        uint32_t packed = 0;
+        float err2 = 0.f;
+#pragma unroll
+        for (int b = 0; b < 4; ++b) {
+            const float x = (float)((w >> (8 * b)) & 255u);
+            const __nv_fp8_storage_t q = __nv_cvt_float_to_fp8(x * s, __NV_SATFINITE, __NV_E4M3);
+            const __half_raw hr = __nv_cvt_fp8_to_halfraw(q, __NV_E4M3);
+            const float back = __half2float(__half(hr)) / s;
+            err2 = fmaf(back - x, back - x, err2);
+            packed |= (uint32_t)q << (8 * b);
+        }
+        for (int sh = 16; sh; sh >>= 1) err2 += __shfl_xor_sync(0xffffffffu, err2, sh);
+        *reinterpret_cast<uint32_t*>(blk + core_off(r, lane * 4, RB)) = packed;
+        if (lane == 0 && row < n) {
+            const float len = sqrtf((float)nrm) * (1.f + 1e-6f), elen = sqrtf(err2) * (1.f + 1e-6f);
+            if (role == 0) {
+                reinterpret_cast<float4*>(rowsc)[row] = make_float4(-s, 1.f / s, len, elen);
+            } else {
+                colsc[row] = make_float2(1.f / s, 0.5f * (float)nrm);
+                atomicMax(reinterpret_cast<int*>(bmax), __float_as_int(len));
+                atomicMax(reinterpret_cast<int*>(bmax) + 1, __float_as_int(elen));
+            }
+        }
+    }
+}
+
+// ------------------------------------------------------------------------ PTX wrappers
+__device__ __forceinline__ uint32_t saddr(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void mbar_init(uint64_t* b, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(saddr(b)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* b, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(saddr(b)), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ void mbar_arrive(uint64_t* b) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(saddr(b)) : "memory");
+}
+__device__ __forceinline__ bool mbar_test(uint64_t* b, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(saddr(b)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+// Bounded wait: false (and the CTA-wide abort flag set) when the phase does not complete in time
+// or another role already gave up.
+__device__ __noinline__ bool mbar_wait(uint64_t* b, uint32_t parity, volatile int* abort_flag) {
+    if (mbar_test(b, parity)) return true;
+    const long long t0 = clock64();
+    while (!mbar_test(b, parity)) {
+        if (*abort_flag) return false;
+        if (clock64() - t0 > TC_TIMEOUT_CYCLES) {
+            *abort_flag = 1;
+            return false;
+        }
+    }
+    return true;
+}
+__device__ __forceinline__ void bulk_load(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(saddr(dst)),
+        "l"(src), "r"(bytes), "r"(saddr(bar))
+        : "memory");
+}
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+
+__device__ __forceinline__ uint64_t smem_desc(uint32_t addr, uint32_t sbo) {
+    // start >> 4 at [0,14), LBO = 128 >> 4 at [16,30), SBO >> 4 at [32,46), version 1 at [46,48),
+    // base offset 0, no swizzle (layout type 0 at [61,64))
+    return (uint64_t)((addr & 0x3FFFFu) >> 4) | ((uint64_t)(128u >> 4) << 16) | ((uint64_t)(sbo >> 4) << 32) |
+           (1ull << 46);
+}
+
+template <int PREC>
+__device__ __forceinline__ void mma(uint32_t tmem_d, uint64_t da, uint64_t db, uint32_t accumulate) {
+    if constexpr (PREC == FSB_PREC_BF16) {
+        asm volatile(
+            "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+            "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem_d),
+            "l"(da), "l"(db), "r"(TcTraits<PREC>::IDESC), "r"(accumulate)
+            : "memory");
+    } else {
+        asm volatile(
+            "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+            "tcgen05.mma.cta_group::1.kind::f8f6f4 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem_d),
+            "l"(da), "l"(db), "r"(TcTraits<PREC>::IDESC), "r"(accumulate)
+            : "memory");
+    }
+}
+__device__ __forceinline__ void mma_commit(uint64_t* bar) {
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(saddr(bar))
+                 : "memory");
+}
+
+__device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&r)[32]) {
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x32.b32 "
+        "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+        "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]),
+          "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]),
+          "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+        : "r"(taddr));
+}
+__device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
+
+__device__ __forceinline__ float max3(float a, float b, float c) {
+    float r;
+    asm("max.f32 %0, %1, %2, %3;" : "=f"(r) : "f"(a), "f"(b), "f"(c));
+    return r;
+}
+
+template <int K>
+__device__ __forceinline__ void cand_insert(float (&m)[K], int (&c)[K], float v, int id) {
+    // v > m[K-1]; keep m descending, earlier chunks first among equal values
+#pragma unroll
+    for (int i = K - 1; i >= 0; --i) {
+        if (v > m[i]) {
+            if (i > 0 && v > m[i - 1]) {
+                m[i] = m[i - 1];
+                c[i] = c[i - 1];
+            } else {
+                m[i] = v;
+                c[i] = id;
+            }
+        }
+    }
+}
+
+// ------------------------------------------------------------------------ the dense kernel
+template <int PREC>
+__global__ void __launch_bounds__(TC_THREADS, 1)
+    k_tc_dense(const TcPair* __restrict__ pairs, int n_pairs, int n_items, Cand* __restrict__ part,
+               int* __restrict__ err) {
+    using T = TcTraits<PREC>;
+    constexpr int TB = tile_bytes<PREC>();
+    constexpr int NST = T::STAGES;
+    constexpr int K = T::TOPK;
+    constexpr uint32_t SBO = T::ROW_BYTES * 8;
+    extern __shared__ __align__(1024) unsigned char smem_raw[];
+    unsigned char* smem = reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+    unsigned char* sA = smem;                  // 2 x TB
+    unsigned char* sB = smem + 2 * TB;         // NST x TB
+    uint64_t* bars = reinterpret_cast<uint64_t*>(sB + NST * TB);
+    uint64_t* b_full = bars;                   // NST
+    uint64_t* b_empty = bars + NST;            // NST
+    uint64_t* a_full = bars + 2 * NST;
+    uint64_t* a_empty = a_full + 1;
+    uint64_t* acc_full = a_full + 2;           // 2
+    uint64_t* acc_empty = a_full + 4;          // 2
+    uint64_t* done_bar = a_full + 6;
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(a_full + 8);
+    volatile int* abort_flag = reinterpret_cast<volatile int*>(tmem_slot + 1);
+
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (threadIdx.x == 0) {
+        for (int i = 0; i < NST; ++i) {
+            mbar_init(b_full + i, 1);
+            mbar_init(b_empty + i, 1);
+        }
+        mbar_init(a_full, 1);
+        mbar_init(a_empty, 1);
+        for (int i = 0; i < 2; ++i) {
+            mbar_init(acc_full + i, 1);
+            mbar_init(acc_empty + i, 8);
+        }
+        mbar_init(done_bar, 1);
+        *abort_flag = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    }
+    if (warp == 1) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], 512;" ::"r"(saddr(tmem_slot))
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = *tmem_slot;
+
+    if (warp == 0) {
+        // ---------------------------------------------------------------- producer
+        if (lane == 0) {
+            uint32_t bit = 0;   // B tiles issued so far
+            int wi = 0;
+            bool ok = true;
+            int pend[NST];
+            for (int i = 0; i < NST; ++i) pend[i] = -1;
+            int a_pend = -1;
+            for (int item = blockIdx.x; item < n_items && ok; item += gridDim.x, ++wi) {
+                const TcPair& P = pairs[find_pair(pairs, n_pairs, item)];
+                const int local = item - P.item0;
+                const int rb = local / P.splits, sp = local - rb * P.splits;
+                const int t0 = sp * P.tps, t1 = min(P.ntiles, t0 + P.tps);
+                const int pre = min(t1 - t0, NST);
+                // the first target tiles of this item do not depend on the query block
+                for (int t = t0; t < t0 + pre && ok; ++t, ++bit) {
+                    const int st = bit % NST;
+                    ok = mbar_wait(b_empty + st, ((bit / NST) & 1) ^ 1, abort_flag);
+                    if (!ok) break;
+                    mbar_expect_tx(b_full + st, TB);
+                    bulk_load(sB + st * TB, P.pb + (size_t)t * TB, TB, b_full + st);
+                    pend[st] = (int)((bit / NST) & 1);
+                }
+                if (!ok) break;
+                ok = mbar_wait(a_empty, (wi & 1) ^ 1, abort_flag);
+                if (!ok) break;
+                mbar_expect_tx(a_full, 2 * TB);
+                bulk_load(sA, P.pa + (size_t)rb * 2 * TB, TB, a_full);
+                bulk_load(sA + TB, P.pa + (size_t)rb * 2 * TB + TB, TB, a_full);
+                a_pend = wi & 1;
+                for (int t = t0 + pre; t < t1 && ok; ++t, ++bit) {
+                    const int st = bit % NST;
+                    ok = mbar_wait(b_empty + st, ((bit / NST) & 1) ^ 1, abort_flag);
+                    if (!ok) break;
+                    mbar_expect_tx(b_full + st, TB);
+                    bulk_load(sB + st * TB, P.pb + (size_t)t * TB, TB, b_full + st);
+                    pend[st] = (int)((bit / NST) & 1);
+                }
+            }
+            if (!ok) {
+                // let every copy already issued land before the CTA leaves (bounded)
+                const long long t0 = clock64();
+                for (int st = 0; st < NST; ++st)
+                    if (pend[st] >= 0)
+                        while (!mbar_test(b_full + st, (uint32_t)pend[st]) && clock64() - t0 < TC_TIMEOUT_CYCLES) {
+                        }
+                if (a_pend >= 0)
+                    while (!mbar_test(a_full, (uint32_t)a_pend) && clock64() - t0 < TC_TIMEOUT_CYCLES) {
+                    }
+            }
+        }
+        __syncwarp();
+    } else if (warp == 1) {
+        // ---------------------------------------------------------------- MMA issuer
+        if (lane == 0) {
+            uint32_t bit = 0, tit = 0;
+            int wi = 0;
+            bool ok = true;
+            bool issued = false;
+            const uint32_t a0 = saddr(sA), b0 = saddr(sB);
+            for (int item = blockIdx.x; item < n_items && ok; item += gridDim.x, ++wi) {
+                const TcPair& P = pairs[find_pair(pairs, n_pairs, item)];
+                const int local = item - P.item0;
+                const int rb = local / P.splits, sp = local - rb * P.splits;
+                const int t0 = sp * P.tps, t1 = min(P.ntiles, t0 + P.tps);
+                (void)rb;
+                ok = mbar_wait(a_full, wi & 1, abort_flag);
+                if (!ok) break;
+                tc_fence_after();
+                for (int t = t0; t < t1; ++t, ++bit, ++tit) {
+                    const int st = bit % NST;
+                    const int ac = tit & 1;
+                    ok = mbar_wait(b_full + st, (bit / NST) & 1, abort_flag);
+                    if (!ok) break;
+                    ok = mbar_wait(acc_empty + ac, ((tit >> 1) & 1) ^ 1, abort_flag);
+                    if (!ok) break;
+                    tc_fence_after();
+#pragma unroll
+                    for (int h = 0; h < 2; ++h) {
+                        const uint32_t d = tmem + (uint32_t)(ac * 256 + h * 128);
+#pragma unroll
+                        for (int k = 0; k < T::KSTEPS; ++k) {
+                            const uint64_t da = smem_desc(a0 + h * TB + k * 256, SBO);
+                            const uint64_t db = smem_desc(b0 + st * TB + k * 256, SBO);
+                            mma<PREC>(d, da, db, k > 0 ? 1u : 0u);
+                        }
+                    }
+                    issued = true;
+                    mma_commit(b_empty + st);
+                    mma_commit(acc_full + ac);
+                }
+                if (!ok) break;
+                mma_commit(a_empty);
+            }
+            // every MMA issued by this thread has completed before TMEM is released
+            if (issued) {
+                mma_commit(done_bar);
+                const long long c0 = clock64();
+                while (!mbar_test(done_bar, 0) && clock64() - c0 < TC_TIMEOUT_CYCLES) {
+                }
+            }
+        }
+        __syncwarp();
+    } else {
+        // ---------------------------------------------------------------- epilogue
+        const int ew = warp - 2;
+        const int lq = warp & 3;          // TMEM lane quarter this warp may access
+        const int h = ew >> 2;            // query half
+        const int rloc = h * 128 + lq * 32 + lane;
+        uint32_t tit = 0;
+        bool ok = true;
+        for (int item = blockIdx.x; item < n_items && ok; item += gridDim.x) {
+            const TcPair& P = pairs[find_pair(pairs, n_pairs, item)];
+            const int local = item - P.item0;
+            const int rb = local / P.splits, sp = local - rb * P.splits;
+            const int t0 = sp * P.tps, t1 = min(P.ntiles, t0 + P.tps);
+            const int q = rb * TC_ROWS + rloc;
+            float m[K];
+            int c[K];
+#pragma unroll
+            for (int i = 0; i < K; ++i) {
+                m[i] = -INFINITY;
+                c[i] = -1;
+            }
+            float neg_sa = -1.f;
+            if constexpr (PREC == FSB_PREC_FP8) neg_sa = q < P.na ? P.rowsc[4 * q] : -1.f;
+            for (int t = t0; t < t1; ++t, ++tit) {
+                const int ac = tit & 1;
+                ok = mbar_wait(acc_full + ac, (tit >> 1) & 1, abort_flag);
+                if (!ok) break;
+                tc_fence_after();
+                const uint32_t base = tmem + ((uint32_t)(lq * 32) << 16) + (uint32_t)(ac * 256 + h * 128);
+#pragma unroll 1
+                for (int ch = 0; ch < TC_N / TC_CHUNK; ++ch) {
+                    uint32_t r[32];
+                    tmem_ld32(base + ch * TC_CHUNK, r);
+                    tmem_wait_ld();
+                    if (ch == TC_N / TC_CHUNK - 1) {
+                        tc_fence_before();
+                        __syncwarp();
+                        if (lane == 0) mbar_arrive(acc_empty + ac);
+                    }
+                    const int j0 = t * TC_N + ch * TC_CHUNK;
+                    float v[32];
+                    if constexpr (PREC == FSB_PREC_FP8) {
+                        const float4* cs = reinterpret_cast<const float4*>(P.colsc + j0);
+#pragma unroll
+                        for (int i = 0; i < 16; ++i) {
+                            const float4 s4 = __ldg(cs + i);   // targets j0+2i, j0+2i+1 (padded table)
+                            v[2 * i] = fmaf(neg_sa, s4.y, __uint_as_float(r[2 * i]) * s4.x);
+                            v[2 * i + 1] = fmaf(neg_sa, s4.w, __uint_as_float(r[2 * i + 1]) * s4.z);
+                        }
+                    } else {
+#pragma unroll
+                        for (int i = 0; i < 32; ++i) v[i] = __uint_as_float(r[i]);
+                    }
+                    if (j0 + TC_CHUNK > P.nb) {
+#pragma unroll
+                        for (int i = 0; i < 32; ++i)
+                            if (j0 + i >= P.nb) v[i] = -INFINITY;
+                    }
+                    float a0 = max3(v[0], v[1], v[2]), a1 = max3(v[3], v[4], v[5]), a2 = max3(v[6], v[7], v[8]);
+                    float a3 = max3(v[9], v[10], v[11]), a4 = max3(v[12], v[13], v[14]);
+                    float a5 = max3(v[15], v[16], v[17]), a6 = max3(v[18], v[19], v[20]);
+                    float a7 = max3(v[21], v[22], v[23]), a8 = max3(v[24], v[25], v[26]);
+                    float a9 = max3(v[27], v[28], v[29]), a10 = fmaxf(v[30], v[31]);
+                    a0 = max3(a0, a1, a2);
+                    a3 = max3(a3, a4, a5);
+                    a6 = max3(a6, a7, a8);
+                    a9 = fmaxf(a9, a10);
+                    const float mx = fmaxf(max3(a0, a3, a6), a9);
+                    if (mx > m[K - 1]) cand_insert<K>(m, c, mx, j0 / TC_CHUNK);
+                }
+            }
+            if (!ok) break;
+            if (q < P.na) {
+                Cand* out = part + P.part0 + ((size_t)q * P.splits + sp) * K;
+#pragma unroll
+                for (int i = 0; i < K; ++i) out[i] = Cand{m[i], c[i]};
+            }
+        }
+    }
+    __syncthreads();
+    if (threadIdx.x == 0 && *abort_flag) atomicExch(err, 1);
+    if (warp == 1) {
+        tc_fence_after();
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, 512;" ::"r"(tmem) : "memory");
+    }
+}
+
+// ------------------------------------------------------------------------ finishing
+__device__ __forceinline__ bool ratio_ok(float b1, float b2, float ratio) {
+    // app/planesite/matching.py:96-99 on float32 values: sqrt(b1) < ratio * sqrt(b2)
+    return __fsqrt_rn(fmaxf(b1, 0.f)) < __fmul_rn(ratio, __fsqrt_rn(fmaxf(b2, 0.f)));
+}
+
+__device__ __forceinline__ int exact_dot(const uint4 (&a)[8], const uint8_t* __restrict__ brow) {
+    const uint4* b4 = reinterpret_cast<const uint4*>(brow);
+    uint32_t s = 0;
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+        const uint4 b = __ldg(b4 + i);
+        s = __dp4a(a[i].x, b.x, s);
+        s = __dp4a(a[i].y, b.y, s);
+        s = __dp4a(a[i].z, b.z, s);
+        s = __dp4a(a[i].w, b.w, s);
+    }
+    return (int)s;
+}
+
+// warp-wide merge of per-lane (d1, j1, d2): smallest d first, smaller index among equal d
+__device__ __forceinline__ void warp_top2(long long& k1, long long& d2) {
+    for (int sh = 16; sh; sh >>= 1) {
+        const long long ok1 = __shfl_xor_sync(0xffffffffu, k1, sh);
+        const long long od2 = __shfl_xor_sync(0xffffffffu, d2, sh);
+        const long long hi = max(k1, ok1);
+        d2 = min(min(d2, od2), hi >> 32);
+        k1 = min(k1, ok1);
+    }
+}
+
+template <int K>
+__global__ void k_tc_finish(const TcPair* __restrict__ pairs, int n_pairs, int n_rows, const Cand* __restrict__ part,
+                            float ratio, int prec, int32_t* __restrict__ t_row, uint32_t* __restrict__ d_row,
+                            int32_t* __restrict__ flagged, int* __restrict__ n_flagged, float* __restrict__ err_stat) {
+    const int g = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    const int lane = threadIdx.x & 31;
+    if (g >= n_rows) return;
+    const TcPair& P = pairs[find_pair_row(pairs, n_pairs, g)];
+    const int q = g - P.row0;
+    if (q >= P.na) return;
+    const int ne = P.splits * K;   // <= 32
+    Cand e = lane < ne ? part[P.part0 + (size_t)q * ne + lane] : Cand{-INFINITY, -1};
+    // the K best chunks over all splits (value descending, chunk ascending)
+    float sv[K];
+    int sc[K];
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+        float bv = e.v;
+        int bc = e.c < 0 ? INT_MAX : e.c;
+        for (int sh = 16; sh; sh >>= 1) {
+            const float ov = __shfl_xor_sync(0xffffffffu, bv, sh);
+            const int oc = __shfl_xor_sync(0xffffffffu, bc, sh);
+            if (ov > bv || (ov == bv && oc < bc)) {
+                bv = ov;
+                bc = oc;
+            }
+        }
+        sv[k] = bv;
+        sc[k] = bc == INT_MAX ? -1 : bc;
+        if (e.c == bc && e.c >= 0) e = Cand{-INFINITY, -1};
+    }
+    // exact distances of the candidate columns
+    const uint4* ar = reinterpret_cast<const uint4*>(P.a + (size_t)q * 128);
+    uint4 a[8];
+#pragma unroll
+    for (int i = 0; i < 8; ++i) a[i] = __ldg(ar + i);
+    const long long na = P.nA[q];
+    long long k1 = LLONG_MAX, d2 = LLONG_MAX >> 32;
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+        if (sc[k] < 0) continue;
+        const int j = sc[k] * 32 + lane;
+        if (j >= P.nb) continue;
+        const long long d = na + P.nB[j] - 2ll * exact_dot(a, P.b + (size_t)j * 128);
+        const long long key = (d << 32) | (unsigned)j;
+        if (key < k1) {
+            d2 = min(d2, k1 >> 32);
+            k1 = key;
+        } else {
+            d2 = min(d2, d);
+        }
+    }
+    warp_top2(k1, d2);
+    if (lane != 0) return;
+    const long long e1 = k1 >> 32, e2 = d2;
+    const int j1 = (int)(k1 & 0xffffffffll);
+    // lower bound on the exact distance of every column outside the candidate chunks
+    double L = INFINITY;
+    if (sv[K - 1] > -INFINITY) {
+        double vk = sv[K - 1], eps = 0.0;
+        if (prec == FSB_PREC_FP8) {
+            const float4 rs = reinterpret_cast<const float4*>(P.rowsc)[q];
+            const double bl = P.bmax[0], be = P.bmax[1];
+            vk *= (double)rs.y;   // s_a-scaled -> a'.b' units
+            eps = (double)rs.z * be + (double)rs.w * bl + (double)rs.w * be + (double)rs.z * bl * (1.0 / 512.0) + 4.0;
+        }
+        L = ceil((double)na - 2.0 * (vk + eps));
+        if (L < 0.0) L = 0.0;
+    }
+    const float fL = L > 16777216.0 ? 16777216.f : (float)L;
+    const float f1 = e1 > (1ll << 24) ? 16777216.f : (float)e1;
+    const float f2 = e2 > (1ll << 24) ? 16777216.f : (float)e2;
+    const bool has1 = k1 != LLONG_MAX;
+    const bool accept = has1 && (double)e1 < L && ratio_ok(f1, fminf(f2, fL), ratio);
+    const bool reject = !has1 || !ratio_ok(fminf(f1, fL), f2, ratio);
+    if (err_stat && has1 && sv[0] > -INFINITY) {
+        // distance error of the best candidate: approximate (from the chunk maximum) vs exact
+        double v1 = sv[0];
+        if (prec == FSB_PREC_FP8) v1 *= (double)reinterpret_cast<const float4*>(P.rowsc)[q].y;
+        const float de = (float)fabs(((double)na - 2.0 * v1) - (double)e1);
+        atomicMax(reinterpret_cast<int*>(err_stat), __float_as_int(de));
+        atomicAdd(err_stat + 1, de);
+    }
+    if (accept) {
+        t_row[g] = j1;
+        d_row[g] = (uint32_t)e1;
+    } else if (reject) {
+        t_row[g] = -1;
+        d_row[g] = has1 ? (uint32_t)e1 : 0u;
+    } else {
+        t_row[g] = -1;
+        d_row[g] = 0u;
+        flagged[atomicAdd(n_flagged, 1)] = g;
+    }
+}
+
+// Exact fallback for rows the certificate could not settle: one CTA per row, every target.
+__global__ void __launch_bounds__(256) k_tc_exact_rows(const TcPair* __restrict__ pairs, int n_pairs,
+                                                       const int32_t* __restrict__ rows, const int* __restrict__ n_rows,
+                                                       float ratio, int32_t* __restrict__ t_row,
+                                                       uint32_t* __restrict__ d_row) {
+    __shared__ long long s_k1[8], s_d2[8];
+    const int nr = *n_rows;
+    for (int ri = blockIdx.x; ri < nr; ri += gridDim.x) {
+        const int g = rows[ri];
+        const TcPair& P = pairs[find_pair_row(pairs, n_pairs, g)];
+        const int q = g - P.row0;
+        const uint4* ar = reinterpret_cast<const uint4*>(P.a + (size_t)q * 128);
+        uint4 a[8];
+#pragma unroll
+        for (int i = 0; i < 8; ++i) a[i] = __ldg(ar + i);
+        const long long na = P.nA[q];
+        long long k1 = LLONG_MAX, d2 = LLONG_MAX >> 32;
+        for (int j = threadIdx.x; j < P.nb; j += blockDim.x) {
+            const long long d = na + P.nB[j] - 2ll * exact_dot(a, P.b + (size_t)j * 128);
+            const long long key = (d << 32) | (unsigned)j;
+            if (key < k1) {
+                d2 = min(d2, k1 >> 32);
+                k1 = key;
+            } else {
+                d2 = min(d2, d);
+            }
+        }
+        warp_top2(k1, d2);
+        const int w = threadIdx.x >> 5;
+        if ((threadIdx.x & 31) == 0) {
+            s_k1[w] = k1;
+            s_d2[w] = d2;
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            long long b1 = s_k1[0], b2 = s_d2[0];
+            for (int i = 1; i < 8; ++i) {
+                const long long hi = max(b1, s_k1[i]);
+                b2 = min(min(b2, s_d2[i]), hi >> 32);
+                b1 = min(b1, s_k1[i]);
+            }
+            const long long e1 = b1 >> 32;
+            const float f1 = (float)e1, f2 = b2 > (1ll << 24) ? 16777216.f : (float)b2;
+            const bool ok = b1 != LLONG_MAX && ratio_ok(f1, f2, ratio);
+            t_row[g] = ok ? (int32_t)(b1 & 0xffffffffll) : -1;
+            d_row[g] = b1 != LLONG_MAX ? (uint32_t)e1 : 0u;
+        }
+        __syncthreads();
+    }
+}
+
+template <int PREC>
+int32_t tc_launch_dense(const TcPair* d_pairs, int n_pairs, int n_items, Cand* part, int* err, int grid,
+                        cudaStream_t s) {
+    static bool configured[64] = {};
+    int dev = 0;
+    FSB_CUDA(cudaGetDevice(&dev));
+    if (dev < 64 && !configured[dev]) {
+        FSB_CUDA(cudaFuncSetAttribute(k_tc_dense<PREC>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_bytes<PREC>()));
+        configured[dev] = true;
+    }
+    k_tc_dense<PREC><<<grid, TC_THREADS, smem_bytes<PREC>(), s>>>(d_pairs, n_pairs, n_items, part, err);
+    FSB_CUDA(cudaGetLastError());
+    return FSB_OK;
+}
+
+}  // namespace
+
+// Tensor-core dense top-2 for a batch of pairs. Per pair p, rows [row0_p, row0_p + na_p) of t_row and
+// d_row receive the accepted target (or -1) and the exact best distance. Buffers come from ctx.
+int32_t run_match_bf_tc_rows(fsb_ctx* ctx, int n_pairs, const uint8_t* const* d_a, const int* na,
+                             const uint8_t* const* d_b, const int* nb, float ratio, int precision, int32_t* t_row,
+                             uint32_t* d_row, const int* row0, TcStats* stats, cudaStream_t s) {
+    if (precision != FSB_PREC_BF16 && precision != FSB_PREC_FP8) {
+        set_error("precision %d has no tensor-core path", precision);
+        return FSB_ERR_UNSUPPORTED;
+    }
+    const bool fp8 = precision == FSB_PREC_FP8;
+    const int RB = fp8 ? TcTraits<FSB_PREC_FP8>::ROW_BYTES : TcTraits<FSB_PREC_BF16>::ROW_BYTES;
+    const int K = fp8 ? TcTraits<FSB_PREC_FP8>::TOPK : TcTraits<FSB_PREC_BF16>::TOPK;
+    int num_sms = 148;
+    {
+        int dev = 0;
+        FSB_CUDA(cudaGetDevice(&dev));
+        FSB_CUDA(cudaDeviceGetAttribute(&num_sms, cudaDevAttrMultiProcessorCount, dev));
+    }
+    // layout of the scratch: packed operands, norms, scales, candidates, row lists
+    std::vector<TcPair> hp(n_pairs);
+    size_t off_pa = 0, off_pb = 0, n_norm = 0, n_rows = 0, n_parts = 0, n_colsc = 0, n_rowsc = 0;
+    int items = 0, rows_total = 0;
+    long long rb_total = 0;
+    for (int p = 0; p < n_pairs; ++p) rb_total += (na[p] + TC_ROWS - 1) / TC_ROWS;
+    for (int p = 0; p < n_pairs; ++p) {
+        TcPair& P = hp[p];
+        P.a = d_a[p];
+        P.b = d_b[p];
+        P.na = na[p];
+        P.nb = nb[p];
+        P.nrb = (na[p] + TC_ROWS - 1) / TC_ROWS;
+        P.ntiles = (nb[p] + TC_N - 1) / TC_N;
+        int splits = 1;
+        if (rb_total < 2 * num_sms) {
+            splits = (int)((2 * num_sms + rb_total - 1) / rb_total);
+            splits = std::min(std::min(splits, TC_MAX_SPLITS), std::max(1, 32 / K));
+            splits = std::min(splits, P.ntiles);
+            splits = std::max(splits, 1);
+        }
+        P.tps = (P.ntiles + splits - 1) / splits;
+        P.splits = (P.ntiles + P.tps - 1) / P.tps;
+        P.item0 = items;
+        P.row0 = row0 ? row0[p] : rows_total;
+        P.part0 = (long long)n_parts;
+        items += P.nrb * P.splits;
+        rows_total = std::max(rows_total, P.row0 + P.na);
+        off_pa += (size_t)P.nrb * TC_ROWS * RB;
+        off_pb += (size_t)P.ntiles * TC_N * RB;
+        n_norm += (size_t)P.na + P.nb;
+        n_parts += (size_t)P.na * P.splits * K;
+        n_colsc += (size_t)P.ntiles * TC_N;
+        n_rowsc += (size_t)P.na;
+    }
+    n_rows = (size_t)rows_total;
+    auto al = [](size_t x) { return (x + 255) & ~size_t(255); };
+    const size_t bytes_pack = al(off_pa) + al(off_pb);
+    const size_t bytes_aux = al(n_norm * 4) + al(n_colsc * 8) + al(n_rowsc * 16) + al((size_t)n_pairs * 8) +
+                             al(n_rows * 4) + al((size_t)n_pairs * sizeof(TcPair)) + 256;
+    FSB_TRY(ctx->s_tc_pack.ensure(bytes_pack));
+    FSB_TRY(ctx->s_tc_part.ensure(al(n_parts * sizeof(Cand)) + 256));
+    FSB_TRY(ctx->s_tc_aux.ensure(bytes_aux));
+    uint8_t* pack = ctx->s_tc_pack.as<uint8_t>();
+    uint8_t* aux = ctx->s_tc_aux.as<uint8_t>();
+    int32_t* norms = reinterpret_cast<int32_t*>(aux);
+    float2* colsc = reinterpret_cast<float2*>(aux + al(n_norm * 4));
+    float* rowsc = reinterpret_cast<float*>(reinterpret_cast<uint8_t*>(colsc) + al(n_colsc * 8));
+    float* bmax = reinterpret_cast<float*>(reinterpret_cast<uint8_t*>(rowsc) + al(n_rowsc * 16));
+    int32_t* flagged = reinterpret_cast<int32_t*>(reinterpret_cast<uint8_t*>(bmax) + al((size_t)n_pairs * 8));
+    TcPair* d_pairs = reinterpret_cast<TcPair*>(reinterpret_cast<uint8_t*>(flagged) + al(n_rows * 4));
+    int* small = reinterpret_cast<int*>(reinterpret_cast<uint8_t*>(d_pairs) + al((size_t)n_pairs * sizeof(TcPair)));
+    // small: [0] abort flag, [1] flagged rows, [2..3] error statistics (max, sum)
+    FSB_CUDA(cudaMemsetAsync(small, 0, 64, s));
+    FSB_CUDA(cudaMemsetAsync(bmax, 0, (size_t)n_pairs * 8, s));
+    size_t pa = 0, pb = 0, nn = 0, cs = 0, rs = 0;
+    for (int p = 0; p < n_pairs; ++p) {
+        TcPair& P = hp[p];
+        P.pa = pack + pa;
+        P.pb = pack + al(off_pa) + pb;
+        P.nA = norms + nn;
+        P.nB = norms + nn + P.na;
+        P.colsc = colsc + cs;
+        P.rowsc = rowsc + rs * 4;
+        P.bmax = bmax + 2 * p;
+        pa += (size_t)P.nrb * TC_ROWS * RB;
+        pb += (size_t)P.ntiles * TC_N * RB;
+        nn += (size_t)P.na + P.nb;
+        cs += (size_t)P.ntiles * TC_N;
+        rs += (size_t)P.na;
+        const int pad_a = P.nrb * TC_ROWS, pad_b = P.ntiles * TC_N;
+        if (fp8) {
+            FSB_CUDA(cudaMemsetAsync(const_cast<float2*>(P.colsc), 0, (size_t)pad_b * 8, s));
+            k_tc_pack<FSB_PREC_FP8><<<nblk(pad_a, 8), 256, 0, s>>>(P.a, P.na, pad_a, 0, const_cast<uint8_t*>(P.pa),
+                                                                  const_cast<int32_t*>(P.nA), nullptr,
+                                                                  const_cast<float*>(P.rowsc), nullptr);
+            k_tc_pack<FSB_PREC_FP8><<<nblk(pad_b, 8), 256, 0, s>>>(P.b, P.nb, pad_b, 1, const_cast<uint8_t*>(P.pb),
+                                                                  const_cast<int32_t*>(P.nB),
+                                                                  const_cast<float2*>(P.colsc), nullptr,
+                                                                  const_cast<float*>(P.bmax));
+        } else {
+            k_tc_pack<FSB_PREC_BF16><<<nblk(pad_a, 8), 256, 0, s>>>(P.a, P.na, pad_a, 0, const_cast<uint8_t*>(P.pa),
+                                                                   const_cast<int32_t*>(P.nA), nullptr, nullptr,
+                                                                   nullptr);
+            k_tc_pack<FSB_PREC_BF16><<<nblk(pad_b, 8), 256, 0, s>>>(P.b, P.nb, pad_b, 1, const_cast<uint8_t*>(P.pb),
+                                                                   const_cast<int32_t*>(P.nB), nullptr, nullptr,
+                                                                   nullptr);
+        }
+        note_launch(2);
+    }
+    FSB_CUDA(cudaGetLastError());
+    FSB_CUDA(cudaMemcpyAsync(d_pairs, hp.data(), (size_t)n_pairs * sizeof(TcPair), cudaMemcpyHostToDevice, s));
+    Cand* part = ctx->s_tc_part.as<Cand>();
+    const int grid = std::min(items, num_sms);
+    if (items > 0) {
+        if (fp8) FSB_TRY(tc_launch_dense<FSB_PREC_FP8>(d_pairs, n_pairs, items, part, small, grid, s));
+        else FSB_TRY(tc_launch_dense<FSB_PREC_BF16>(d_pairs, n_pairs, items, part, small, grid, s));
+        note_launch(1);
+    }
+    if (rows_total > 0) {
+        if (fp8)
+            k_tc_finish<TcTraits<FSB_PREC_FP8>::TOPK><<<nblk(rows_total, 8), 256, 0, s>>>(
+                d_pairs, n_pairs, rows_total, part, ratio, precision, t_row, d_row, flagged, small + 1,
+                stats ? reinterpret_cast<float*>(small + 2) : nullptr);
+        else
+            k_tc_finish<TcTraits<FSB_PREC_BF16>::TOPK><<<nblk(rows_total, 8), 256, 0, s>>>(
+                d_pairs, n_pairs, rows_total, part, ratio, precision, t_row, d_row, flagged, small + 1,
+                stats ? reinterpret_cast<float*>(small + 2) : nullptr);
+        note_launch(1);
+        FSB_CUDA(cudaGetLastError());
+    }
+    int host_small[4] = {0, 0, 0, 0};
+    FSB_CUDA(cudaMemcpyAsync(host_small, small, sizeof(host_small), cudaMemcpyDeviceToHost, s));
+    FSB_CUDA(cudaStreamSynchronize(s));
+    if (host_small[0]) {
+        set_error("tensor-core matcher: a pipeline wait timed out");
+        return FSB_ERR_CUDA;
+    }
+    if (host_small[1] > 0) {
+        k_tc_exact_rows<<<std::min(host_small[1], 8 * num_sms), 256, 0, s>>>(d_pairs, n_pairs, flagged, small + 1,
+                                                                            ratio, t_row, d_row);
+        note_launch(1);
+        FSB_CUDA(cudaGetLastError());
+    }
+    if (stats) {
+        float mx, sum;
+        memcpy(&mx, &host_small[2], 4);
+        memcpy(&sum, &host_small[3], 4);
+        stats->rows = rows_total;
+        stats->fallback_rows = host_small[1];
+        stats->max_abs_err = mx;
+        stats->mean_abs_err = rows_total ? sum / (float)rows_total : 0.f;
+    }
+    return FSB_OK;
+}
+
+}  // namespace fsb

@@ -36,6 +36,50 @@ def _ratio_match_bf(da, db, ratio, na=None, nb=None, precision="fp32", device=0)
     return q[:n.value].copy(), t[:n.value].copy()
 
 
+def ratio_match_bf_batch_d(a_list, b_list, ratio, precision="bf16", device=0):
+    """Many independent ``_ratio_match_bf`` problems in one call on device-resident descriptors.
+
+    ``a_list[p]``, ``b_list[p]`` are CUDA tensors (uint8, n x 128, contiguous) on ``device``.
+    Returns a list of (q, t) int64 CUDA tensors, ordered by target like ``_ratio_match_bf``.
+    With ``precision`` "bf16" or "fp8" every pair goes through one persistent tensor-core launch.
+    """
+    import torch
+    if len(a_list) != len(b_list):
+        raise ValueError("a_list and b_list differ in length")
+    n = len(a_list)
+    for x in list(a_list) + list(b_list):
+        if x.dtype != torch.uint8 or x.dim() != 2 or x.shape[1] != 128 or not x.is_contiguous() or not x.is_cuda:
+            raise ValueError("descriptors must be contiguous CUDA uint8 tensors of shape (n, 128)")
+    ctx = _lib.context(device)
+    outs = [(torch.empty(max(len(a), 1), dtype=torch.int64, device=a.device),
+             torch.empty(max(len(a), 1), dtype=torch.int64, device=a.device)) for a in a_list]
+    P = ctypes.c_void_p * max(n, 1)
+    I = ctypes.c_int32 * max(n, 1)
+    pa = P(*[a.data_ptr() for a in a_list])
+    pb = P(*[b.data_ptr() for b in b_list])
+    na = I(*[len(a) for a in a_list])
+    nb = I(*[len(b) for b in b_list])
+    pq = P(*[o[0].data_ptr() for o in outs])
+    pt = P(*[o[1].data_ptr() for o in outs])
+    cnt = I()
+    torch.cuda.current_stream(device).synchronize()
+    _lib.check(ctx.lib.fsb_match_bf_batch_d(ctx.handle, n, pa, na, pb, nb, float(ratio), _lib.PREC[precision],
+                                            pq, pt, cnt), "fsb_match_bf_batch_d")
+    return [(o[0][:cnt[i]], o[1][:cnt[i]]) for i, o in enumerate(outs)]
+
+
+def tc_stats(device=0):
+    """Statistics of the last tensor-core dense match on this thread's context for ``device``:
+    rows, rows recomputed exactly (certificate not settled), largest / mean absolute error of the
+    approximate best squared distance against the exact one."""
+    ctx = _lib.context(device)
+    r, f = ctypes.c_int64(), ctypes.c_int64()
+    mx, mean = ctypes.c_double(), ctypes.c_double()
+    _lib.check(ctx.lib.fsb_match_tc_stats(ctx.handle, ctypes.byref(r), ctypes.byref(f), ctypes.byref(mx),
+                                          ctypes.byref(mean)), "fsb_match_tc_stats")
+    return {"rows": r.value, "fallback_rows": f.value, "max_abs_err": mx.value, "mean_abs_err": mean.value}
+
+
 def perspective(xy, Hm, device=0):
     """cv2.perspectiveTransform of (n,2) float64 points on the device (matching.py:115)."""
     xy = np.ascontiguousarray(np.asarray(xy, np.float64).reshape(-1, 2))

@@ -31,8 +31,9 @@ extern "C" {
 
 /* dense matcher precision (fsb_match_bf) */
 #define FSB_PREC_FP32 0 /* CUDA-core FP32 distances: the plain path */
-#define FSB_PREC_BF16 1 /* tcgen05 BF16 x BF16 -> FP32 distances, exact re-rank of the top 4 */
-#define FSB_PREC_FP8 2  /* tcgen05 E4M3 (per-descriptor scale) -> FP32, exact re-rank of the top 4 */
+#define FSB_PREC_BF16 1 /* tcgen05 BF16 x BF16 -> FP32 (exact for uint8 rows), exact integer re-rank */
+#define FSB_PREC_FP8 2  /* tcgen05 E4M3 (per-row power-of-two scale) -> FP32, exact integer re-rank of
+                           the best 4 x 32 columns, certified ratio test, exact fallback rows */
 
 typedef struct fsb_ctx fsb_ctx;
 typedef struct fsb_state fsb_state;
@@ -141,6 +142,23 @@ int32_t fsb_match_guided_d(fsb_ctx* ctx, const double* d_pred, const uint8_t* d_
 /* fsb_match_bf with every array in device memory; d_q, d_t capacity na. */
 int32_t fsb_match_bf_d(fsb_ctx* ctx, const uint8_t* d_a, int32_t na, const uint8_t* d_b, int32_t nb,
                        float ratio, int32_t precision, int64_t* d_q, int64_t* d_t, int32_t* n_out);
+
+/* A batch of independent fsb_match_bf_d problems in one call: pair p matches d_a[p] (na[p] x 128)
+   against d_b[p] (nb[p] x 128) and writes n_out[p] pairs into d_q[p], d_t[p] (device, capacity
+   na[p]). The pointer and size arrays are host arrays; the descriptors and outputs are device
+   memory. With FSB_PREC_BF16 / FSB_PREC_FP8 all pairs share one persistent tensor-core launch
+   (work items of 256 query rows, uneven sizes allowed); FSB_PREC_FP32 runs the pairs one after
+   another. Replaces a Python loop over matching._ratio_match_bf (app/planesite/matching.py:86-100);
+   every precision returns the same pairs. */
+int32_t fsb_match_bf_batch_d(fsb_ctx* ctx, int32_t n_pairs, const uint8_t* const* d_a, const int32_t* na,
+                             const uint8_t* const* d_b, const int32_t* nb, float ratio, int32_t precision,
+                             int64_t* const* d_q, int64_t* const* d_t, int32_t* n_out);
+/* Statistics of the last tensor-core dense match on ctx (fsb_match_bf* with FSB_PREC_BF16 or
+   FSB_PREC_FP8): query rows, rows whose ratio-test decision the rounding-error certificate could
+   not settle and that were recomputed exactly, and the largest and mean absolute difference
+   between the approximate and the exact best squared distance of a row. Any pointer may be null. */
+int32_t fsb_match_tc_stats(fsb_ctx* ctx, int64_t* rows, int64_t* fallback_rows, double* max_abs_err,
+                           double* mean_abs_err);
 
 /* Allocation-free variant of fsb_match_bf_d (FP32 distances), for callers that cannot call
    cudaMalloc: processes that reserve their whole device-memory budget up front, host frameworks
