@@ -51,6 +51,8 @@ def parse():
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-cpu", action="store_true")
     p.add_argument("--streams", type=int, default=4, help="host threads, each with its own context/stream")
+    p.add_argument("--sweep-pairs", type=int, default=256, help="dense precision sweep: pairs per batch (0: skip)")
+    p.add_argument("--sweep-n", type=int, default=16384, help="dense precision sweep: descriptors per image")
     return p.parse_args()
 
 
@@ -200,6 +202,83 @@ def run_reference(args):
 
 
 # ---------------------------------------------------------------------------------- GPU arm
+def dense_sweep(args, local):
+    """Precision sweep of the exhaustive matcher (_ratio_match_bf + _unique): one batch of
+    args.sweep_pairs pairs of args.sweep_n x args.sweep_n SIFT-like uint8 descriptors (30% true
+    correspondences with +-4 byte noise), ratio 0.8, per precision FP32 (CUDA cores), BF16 and
+    E4M3 (tcgen05). Reports pairs/s of the whole batch call, the tensor-core kernel's own time and
+    TFLOP/s, the approximate-vs-exact best-distance error, the rows the certificate sent to the
+    exact fallback, and whether every pair's match list equals the FP32 one."""
+    import torch
+
+    from fieldstitch_b200 import _lib, matching, synth
+    dev = torch.device("cuda", local)
+    n, npairs = args.sweep_n, args.sweep_pairs
+    A, B = [], []
+    for p in range(npairs):
+        a, b, _ = synth.synth_descriptors_device(n, n, args.seed + 31 * p, device=local)
+        A.append(a)
+        B.append(b)
+    outs = [(torch.empty(n, dtype=torch.int64, device=dev), torch.empty(n, dtype=torch.int64, device=dev))
+            for _ in range(npairs)]
+    ref_outs = [(torch.empty(n, dtype=torch.int64, device=dev), torch.empty(n, dtype=torch.int64, device=dev))
+                for _ in range(npairs)]
+    torch.cuda.synchronize()
+    ctx = _lib.context(local)
+    ctx.timing(True)
+    flops = 2.0 * 128 * n * n * npairs
+    peak_bf16 = None
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            peak_bf16 = float(json.load(f)["bf16_tflops"])
+        peak_src = "measured (MEASURED_PEAKS.json bf16_tflops, burst)"
+    except (OSError, KeyError, ValueError):
+        peak_bf16, peak_src = 1590.0, "fallback 1.59 PFLOP/s"
+    out, ref = {}, None
+    for prec in ("fp32", "bf16", "fp8"):
+        o = ref_outs if prec == "fp32" else outs
+        res = matching.ratio_match_bf_batch_d(A, B, 0.8, precision=prec, out=o)   # warm-up
+        torch.cuda.synchronize()
+        ctx.stage_times()
+        steps = 2
+        main = torch.cuda.current_stream(dev)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(main)
+        for _ in range(steps):
+            res = matching.ratio_match_bf_batch_d(A, B, 0.8, precision=prec, out=o)
+        torch.cuda.synchronize()
+        e1.record(main)
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / steps
+        st = ctx.stage_times()
+        r = {"pairs_per_s": npairs / (ms / 1000.0), "ms_per_batch": ms,
+             "matches": int(sum(len(q) for q, _ in res))}
+        if prec == "fp32":
+            ref = res
+            r["distance_error_vs_fp64"] = {"max_abs": 0.0, "note": "integers < 2^24, exact in FP32"}
+        else:
+            ts = matching.tc_stats(local)
+            kms, kn = st["tc_dense"]
+            kms = kms / max(kn, 1)
+            tfl = flops / (kms / 1000.0) / 1e12 if kms > 0 else None
+            pk_t = peak_bf16 if prec == "bf16" else 2.0 * peak_bf16
+            r.update({"tc_dense_ms": kms, "tc_dense_tflops": tfl, "peak_tflops": pk_t,
+                      "peak_source": peak_src + ("" if prec == "bf16" else " x2 (E4M3 rate)"),
+                      "frac": tfl / pk_t if tfl else None,
+                      "distance_error_vs_fp64": {"max_abs": ts["max_abs_err"], "mean_abs": ts["mean_abs_err"],
+                                                 "of": "best squared distance per query row, approximate vs exact"},
+                      "fallback_rows": ts["fallback_rows"], "rows": ts["rows"],
+                      "identical_to_fp32": all(torch.equal(q, q2) and torch.equal(t, t2)
+                                               for (q, t), (q2, t2) in zip(res, ref))})
+        out[prec] = r
+    ctx.timing(False)
+    return {"workload": "%d pairs of %dx%d 128-d uint8 SIFT-like descriptors (30%% true correspondences, +-4 "
+                        "byte noise), ratio 0.8, _ratio_match_bf + _unique, one batch call per step" % (npairs, n, n),
+            "flops_per_batch_algorithmic": flops, **out,
+            "speedup_bf16_vs_fp32": out["fp32"]["ms_per_batch"] / out["bf16"]["ms_per_batch"],
+            "speedup_fp8_vs_fp32": out["fp32"]["ms_per_batch"] / out["fp8"]["ms_per_batch"]}
+
+
 def run_fsb(args):
     import ctypes
     from concurrent.futures import ThreadPoolExecutor
@@ -402,13 +481,17 @@ def run_fsb(args):
                "sample": "%d pairs of the same workload (OpenCV SIFT as features.sift_cpu + NumPy/cKDTree "
                          "guided match)" % n_cpu}
 
+    sweep = None
+    if rank == 0 and args.sweep_pairs > 0:
+        sweep = dense_sweep(args, local)
+
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": "pairs/s", "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
                 "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded)",
                 "config": config(args, {"host_streams": args.streams}),
                 "clocks": clk, "e2e": e2e, "gpu_launches": int(launches), "roofline": roof, "cpu_baseline": cpu,
-                "matches_per_step": matches / args.steps,
+                "matches_per_step": matches / args.steps, "dense_precision_sweep": sweep,
                 "stages_ms_per_step_summed_over_streams": {k: v[0] / args.steps for k, v in stages.items()}}
         print(json.dumps(line), flush=True)
     pool.shutdown()

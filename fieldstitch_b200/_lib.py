@@ -60,7 +60,7 @@ SIGNATURES = [
     ("fsb_match_tc_stats", c_i32, [c_vp, c_vp, c_vp, c_vp, c_vp]),
 ]
 
-STAGES = ("upload", "pyramid", "extrema", "refine", "orientation", "sort", "spread", "describe", "match")
+STAGES = ("upload", "pyramid", "extrema", "refine", "orientation", "sort", "spread", "describe", "match", "tc_dense")
 
 _lib = None
 _lock = threading.Lock()

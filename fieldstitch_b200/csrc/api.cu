@@ -251,7 +251,7 @@ int32_t fsb_destroy(fsb_ctx* ctx) {
     ctx->pool.clear();
     DevBuf* all[] = {&ctx->s_u8a, &ctx->s_u8b, &ctx->s_f32a, &ctx->s_f32b, &ctx->s_i32, &ctx->s_i64,
                      &ctx->s_u64, &ctx->s_misc, &ctx->s_misc2, &ctx->s_host_stage, &ctx->s_cub,
-                     &ctx->s_tc_pack, &ctx->s_tc_part, &ctx->s_tc_aux};
+                     &ctx->s_tc_pack, &ctx->s_tc_part, &ctx->s_tc_aux, &ctx->s_count};
     for (DevBuf* b : all) b->release();
     if (ctx->pinned) cudaFreeHost(ctx->pinned);
     for (auto& e : ctx->ev)
@@ -301,7 +301,7 @@ int64_t fsb_device_bytes(fsb_ctx* ctx) {
     for (Workspace* w : ctx->pool) t += (int64_t)w->bytes();
     const DevBuf* all[] = {&ctx->s_u8a, &ctx->s_u8b, &ctx->s_f32a, &ctx->s_f32b, &ctx->s_i32, &ctx->s_i64,
                            &ctx->s_u64, &ctx->s_misc, &ctx->s_misc2, &ctx->s_host_stage, &ctx->s_cub,
-                     &ctx->s_tc_pack, &ctx->s_tc_part, &ctx->s_tc_aux};
+                     &ctx->s_tc_pack, &ctx->s_tc_part, &ctx->s_tc_aux, &ctx->s_count};
     for (const DevBuf* b : all) t += (int64_t)b->bytes;
     return t;
 }
@@ -525,8 +525,8 @@ int32_t fsb_match_guided_d(fsb_ctx* ctx, const double* d_pred, const uint8_t* d_
     if (na == 0 || nb == 0 || !(radius > 0.0)) return FSB_OK;
     FSB_TRY(use_device(ctx));
     cudaStream_t s = ctx->stream;
-    FSB_TRY(ctx->s_misc2.ensure(64));
-    int* dn = ctx->s_misc2.as<int>();
+    FSB_TRY(ctx->s_count.ensure(64));
+    int* dn = ctx->s_count.as<int>();
     ctx->stage_begin(ST_MATCH);
     FSB_TRY(run_match_guided(ctx, d_pred, d_a, na, d_bxy, d_b, nb, w_b, h_b, radius, kc, ratio, d_q, d_t, dn, s));
     int n = 0;
@@ -547,8 +547,8 @@ int32_t fsb_match_bf_d(fsb_ctx* ctx, const uint8_t* d_a, int32_t na, const uint8
     if (na < 2 || nb < 2) return FSB_OK;
     FSB_TRY(use_device(ctx));
     cudaStream_t s = ctx->stream;
-    FSB_TRY(ctx->s_misc2.ensure(64));
-    int* dn = ctx->s_misc2.as<int>();
+    FSB_TRY(ctx->s_count.ensure(64));
+    int* dn = ctx->s_count.as<int>();
     ctx->stage_begin(ST_MATCH);
     FSB_TRY(run_match_bf(ctx, d_a, na, d_b, nb, ratio, precision, d_q, d_t, dn, s));
     int n = 0;
@@ -573,41 +573,40 @@ int32_t fsb_match_bf_batch_d(fsb_ctx* ctx, int32_t n_pairs, const uint8_t* const
     if (n_pairs == 0) return FSB_OK;
     FSB_TRY(use_device(ctx));
     cudaStream_t s = ctx->stream;
-    FSB_TRY(ctx->s_misc2.ensure(64));
     std::vector<int> live;
     for (int p = 0; p < n_pairs; ++p)
         if (na[p] >= 2 && nb[p] >= 2) live.push_back(p);
     if (live.empty()) return FSB_OK;
     ctx->stage_begin(ST_MATCH);
     std::vector<int> cnt(n_pairs, 0);
-    FSB_TRY(ctx->s_host_stage.ensure((size_t)n_pairs * 4 + 64));
-    int* dn_all = ctx->s_host_stage.as<int>();
+    FSB_TRY(ctx->s_count.ensure((size_t)n_pairs * 4 + 64));
+    int* dn_all = ctx->s_count.as<int>();
     FSB_CUDA(cudaMemsetAsync(dn_all, 0, (size_t)n_pairs * 4, s));
     if (precision == FSB_PREC_FP32) {
         for (int p : live)
             FSB_TRY(run_match_bf(ctx, d_a[p], na[p], d_b[p], nb[p], ratio, precision, d_q[p], d_t[p], dn_all + p, s));
     } else {
         std::vector<const uint8_t*> pa, pb;
-        std::vector<int> ra, rb, row0;
-        int rows = 0;
+        std::vector<int64_t*> pq, pt;
+        std::vector<int> ra, rb;
         for (int p : live) {
             pa.push_back(d_a[p]);
             pb.push_back(d_b[p]);
+            pq.push_back(d_q[p]);
+            pt.push_back(d_t[p]);
             ra.push_back(na[p]);
             rb.push_back(nb[p]);
-            row0.push_back(rows);
-            rows += na[p];
         }
-        FSB_TRY(ctx->s_i32.ensure((size_t)rows * 8 + 64));
-        int32_t* t_row = ctx->s_i32.as<int32_t>();
-        uint32_t* d_row = reinterpret_cast<uint32_t*>(t_row + rows);
-        FSB_TRY(run_match_bf_tc_rows(ctx, (int)live.size(), pa.data(), ra.data(), pb.data(), rb.data(), ratio,
-                                     precision, t_row, d_row, row0.data(), &ctx->tc_stats, s));
-        for (size_t i = 0; i < live.size(); ++i) {
-            const int p = live[i];
-            FSB_TRY(run_unique_rows(ctx, t_row + row0[i], d_row + row0[i], na[p], nb[p], d_q[p], d_t[p], dn_all + p,
-                                    s));
-        }
+        int32_t* dn_live = dn_all;
+        FSB_TRY(run_match_bf_tc(ctx, (int)live.size(), pa.data(), ra.data(), pb.data(), rb.data(), ratio, precision,
+                                pq.data(), pt.data(), dn_live, &ctx->tc_stats, s));
+        std::vector<int> cl(live.size(), 0);
+        FSB_CUDA(cudaMemcpyAsync(cl.data(), dn_live, cl.size() * 4, cudaMemcpyDeviceToHost, s));
+        FSB_CUDA(cudaStreamSynchronize(s));
+        for (size_t i = 0; i < live.size(); ++i) cnt[live[i]] = cl[i];
+        ctx->stage_end(ST_MATCH);
+        for (int p = 0; p < n_pairs; ++p) n_out[p] = cnt[p];
+        return FSB_OK;
     }
     FSB_CUDA(cudaMemcpyAsync(cnt.data(), dn_all, (size_t)n_pairs * 4, cudaMemcpyDeviceToHost, s));
     FSB_CUDA(cudaStreamSynchronize(s));
@@ -666,7 +665,8 @@ int32_t fsb_match_bf(fsb_ctx* ctx, const uint8_t* a, int32_t na, const uint8_t* 
     FSB_TRY(ctx->s_i64.ensure((size_t)na * 16 + 64));
     int64_t* dq = ctx->s_i64.as<int64_t>();
     int64_t* dt = dq + na;
-    int* dn = reinterpret_cast<int*>(dt + na);
+    FSB_TRY(ctx->s_count.ensure(64));
+    int* dn = ctx->s_count.as<int>();
     FSB_TRY(run_match_bf(ctx, ctx->s_u8a.as<uint8_t>(), na, ctx->s_u8b.as<uint8_t>(), nb, ratio, precision, dq, dt,
                          dn, s));
     int n = 0;
@@ -702,7 +702,8 @@ int32_t fsb_match_guided(fsb_ctx* ctx, const double* pred_xy, const uint8_t* a, 
     FSB_TRY(ctx->s_i64.ensure((size_t)na * 16 + 64));
     int64_t* dq = ctx->s_i64.as<int64_t>();
     int64_t* dt = dq + na;
-    int* dn = reinterpret_cast<int*>(dt + na);
+    FSB_TRY(ctx->s_count.ensure(64));
+    int* dn = ctx->s_count.as<int>();
     FSB_TRY(run_match_guided(ctx, dp, ctx->s_u8a.as<uint8_t>(), na, dbx, ctx->s_u8b.as<uint8_t>(), nb, w_b, h_b, radius,
                              kc, ratio, dq, dt, dn, s));
     int n = 0;
@@ -731,8 +732,8 @@ int32_t fsb_unique(fsb_ctx* ctx, const int64_t* q, const int64_t* t, const float
     int64_t* dqo = dt + n;
     int64_t* dto = dqo + n;
     float* ddd = reinterpret_cast<float*>(dto + n);
-    FSB_TRY(ctx->s_i32.ensure(64));
-    int* dn = ctx->s_i32.as<int>();
+    FSB_TRY(ctx->s_count.ensure(64));
+    int* dn = ctx->s_count.as<int>();
     FSB_CUDA(cudaMemcpyAsync(dq, q, (size_t)n * 8, cudaMemcpyHostToDevice, s));
     FSB_CUDA(cudaMemcpyAsync(dt, t, (size_t)n * 8, cudaMemcpyHostToDevice, s));
     FSB_CUDA(cudaMemcpyAsync(ddd, dd, (size_t)n * 4, cudaMemcpyHostToDevice, s));

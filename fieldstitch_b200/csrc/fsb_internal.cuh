@@ -21,7 +21,7 @@ void note_launch(int n = 1);
 
 // Per-stage device timers (CUDA events on the context stream), enabled by fsb_timing().
 enum Stage { ST_UPLOAD = 0, ST_PYRAMID, ST_EXTREMA, ST_REFINE, ST_ORIENT, ST_SORT, ST_SPREAD, ST_DESCRIBE,
-             ST_MATCH, ST_COUNT };
+             ST_MATCH, ST_TC_DENSE, ST_COUNT };
 
 #define FSB_CUDA(call)                                                                      \
     do {                                                                                    \
@@ -132,6 +132,7 @@ struct fsb_ctx {
     fsb::DevBuf s_u8a, s_u8b, s_f32a, s_f32b, s_i32, s_i64, s_u64, s_misc, s_misc2, s_host_stage;
     fsb::DevBuf s_cub;   // CUB temporary storage (one primitive at a time)
     fsb::DevBuf s_tc_pack, s_tc_part, s_tc_aux;   // tensor-core matcher: packed operands, candidates, tables
+    fsb::DevBuf s_count;   // result counts of the API calls; never grown by the internal stages
     fsb::TcStats tc_stats{};                      // of the last tensor-core dense match
     void* pinned = nullptr;
     size_t pinned_bytes = 0;
@@ -181,12 +182,11 @@ int32_t run_match_bf(fsb_ctx* ctx, const uint8_t* d_a, int na, const uint8_t* d_
 int32_t run_match_guided(fsb_ctx* ctx, const double* d_pred, const uint8_t* d_a, int na, const double* d_bxy,
                          const uint8_t* d_b, int nb, double wb, double hb, double radius, int kc, float ratio,
                          int64_t* d_q, int64_t* d_t, int* d_n, cudaStream_t s);
-int32_t run_unique_rows(fsb_ctx* ctx, const int32_t* t_row, const uint32_t* d_row, int na, int nb, int64_t* d_q,
-                        int64_t* d_t, int* d_n, cudaStream_t s);
-// tc_match.cu
-int32_t run_match_bf_tc_rows(fsb_ctx* ctx, int n_pairs, const uint8_t* const* d_a, const int* na,
-                             const uint8_t* const* d_b, const int* nb, float ratio, int precision, int32_t* t_row,
-                             uint32_t* d_row, const int* row0, TcStats* stats, cudaStream_t s);
+// tc_match.cu: tensor-core dense matching of a batch of pairs (na, nb >= 1), _unique included;
+// counts (device, one per pair), q_out/t_out device arrays of capacity na[p]
+int32_t run_match_bf_tc(fsb_ctx* ctx, int n_pairs, const uint8_t* const* d_a, const int* na,
+                        const uint8_t* const* d_b, const int* nb, float ratio, int precision, int64_t* const* q_out,
+                        int64_t* const* t_out, int32_t* counts, TcStats* stats, cudaStream_t s);
 int32_t run_perspective(const double* d_xy, int n, const double* hm9, double* d_out, cudaStream_t s);
 int32_t run_project(const float* d_xy, int n, const double* hm9_host, const float* d_off, double* d_out,
                     cudaStream_t s);

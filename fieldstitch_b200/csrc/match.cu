@@ -509,14 +509,8 @@ int32_t run_match_bf(fsb_ctx* ctx, const uint8_t* d_a, int na, const uint8_t* d_
         FSB_CUDA(cudaMemsetAsync(d_n, 0, sizeof(int), s));
         return FSB_OK;
     }
-    if (precision != FSB_PREC_FP32) {
-        FSB_TRY(ctx->s_i32.ensure((size_t)na * 8 + 64));
-        int32_t* t_row = ctx->s_i32.as<int32_t>();
-        uint32_t* d_row = reinterpret_cast<uint32_t*>(t_row + na);
-        FSB_TRY(run_match_bf_tc_rows(ctx, 1, &d_a, &na, &d_b, &nb, ratio, precision, t_row, d_row, nullptr,
-                                     &ctx->tc_stats, s));
-        return run_unique(ctx, t_row, d_row, na, nb, d_q, d_t, d_n, s);
-    }
+    if (precision != FSB_PREC_FP32)
+        return run_match_bf_tc(ctx, 1, &d_a, &na, &d_b, &nb, ratio, precision, &d_q, &d_t, d_n, &ctx->tc_stats, s);
     const int row_blocks = (na + BM - 1) / BM;
     int splits = 1;
     while (row_blocks * splits < 2 * 148 && (nb + splits * 2 - 1) / (splits * 2) >= BN) splits *= 2;
@@ -536,11 +530,6 @@ int32_t run_match_bf(fsb_ctx* ctx, const uint8_t* d_a, int na, const uint8_t* d_
     k_bf_merge<<<blocks(na, 256), 256, 0, s>>>(part, na, splits, ratio, t_row, d_row);
     note_launch(4);
     FSB_CUDA(cudaGetLastError());
-    return run_unique(ctx, t_row, d_row, na, nb, d_q, d_t, d_n, s);
-}
-
-int32_t run_unique_rows(fsb_ctx* ctx, const int32_t* t_row, const uint32_t* d_row, int na, int nb, int64_t* d_q,
-                        int64_t* d_t, int* d_n, cudaStream_t s) {
     return run_unique(ctx, t_row, d_row, na, nb, d_q, d_t, d_n, s);
 }
 

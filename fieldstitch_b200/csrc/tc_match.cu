@@ -2,34 +2,46 @@
 //
 // matching._ratio_match_bf (app/planesite/matching.py:86-100) needs, for every query row a_q, the
 // smallest and second-smallest d2(q, j) = |a_q|^2 + |b_j|^2 - 2 a_q.b_j over all target rows b_j
-// and the index of the smallest. Here that contraction runs as one K-major GEMM per pair:
+// and the index of the smallest; _unique (matching.py:103-110) then keeps one query per target.
+// Here the contraction runs as K-major GEMMs with the accumulators in tensor memory:
 //
-//   k_tc_pack    uint8 rows -> operand rows in the canonical no-swizzle core-matrix layout
-//                (8 rows x 16 bytes per core matrix, one contiguous block per 128 rows):
-//                BF16: 128 descriptor values + 16 extra slots that carry the norm term, so that
-//                      a'.b' = a.b - |b|^2 / 2 (query slots -32768, -128, -0.5; target slots the
-//                      three bytes of |b|^2). For uint8 data every product and partial sum is an
-//                      integer or half-integer below 2^23, so the FP32 accumulation is exact.
-//                E4M3: per-row power-of-two scale s with max(row) * s <= 448, round to nearest;
-//                      the norm term and the column scale are applied in the epilogue.
+//   k_tc_pack    uint8 rows of every pair (one launch) -> operand rows in the canonical no-swizzle
+//                core-matrix layout (8 rows x 16 bytes per core matrix, one block per 128 rows).
+//                Each row ends with 16 BF16 "norm slots": query slots -s*32768, -s*128, -s*0.5,
+//                target slots the three bytes of |b|^2, so one extra K=16 MMA step adds
+//                -s*|b|^2/2 and the accumulator holds s * (a.b - |b|^2/2): its largest value over
+//                j is the smallest d2 of the row.
+//                BF16: the 128 values are exact (uint8 fits the 8-bit significand) and every partial
+//                      sum is a multiple of 1/2 below 2^23, so the FP32 accumulation is exact; s = 1.
+//                E4M3: round to nearest with a per-query power-of-two scale s (max * s <= 448);
+//                      targets are not scaled (uint8 never exceeds the E4M3 range). A power-of-two
+//                      scale moves only the exponent, so for uint8 values it changes no rounded
+//                      value; it is kept for inputs whose range needs it.
 //   k_tc_dense   persistent warp-specialised kernel. Warp 0 streams 128-row target tiles into a
 //                shared-memory ring with bulk asynchronous copies (no tensor map, no multicast);
-//                warp 1 issues tcgen05.mma (M=128, N=128) for the two 128-row halves of a 256-row
+//                warp 1 issues the MMAs (M=128, N=128) for the two 128-row halves of a 256-row
 //                query block into double-buffered FP32 accumulators (4 x 128 of the 512 TMEM
-//                columns); warps 2-9 read the accumulators with tcgen05.ld and keep, per query row,
-//                the K largest values of a'.b' over 32-column chunks and the chunks they came from.
-//   k_tc_finish  per query row: the K best chunks of all column splits, exact integer distances
-//                of their columns (dp4a), top-2, the float32 ratio test of the reference, and a
-//                certificate that no column outside those chunks can change the decision. With
-//                BF16 the certificate always holds; with E4M3 it uses a bound on the rounding
-//                error, and rows it cannot settle are recomputed by k_tc_exact_rows.
+//                columns); warps 2-9 read the accumulators with tcgen05.ld (32 columns at a time)
+//                and keep, per query row, the two largest 32-column maxima and their chunks.
+//   k_tc_finish  per query row: the two best chunks over all column splits and the exact integer
+//                distances (dp4a) of their columns (BF16: the best chunk only; the second chunk's
+//                maximum is already exact), top-2, the float32 ratio test of the reference, and a
+//                certificate that no other column can change the decision. BF16: the best chunk's
+//                tensor-core maximum must equal the exact best (otherwise the row is recomputed).
+//                E4M3: the bound on the rounding error decides; unsettled rows are recomputed by
+//                k_tc_exact_rows over every target.
+//   k_tcu_*      _unique for every pair of the batch at once (one key per target, atomicMin on
+//                (distance << 32 | query), target-ordered compaction by a prefix sum).
 //
-// Results (the best target, the exact best distance, the accept decision) are therefore the
-// same as those of the CUDA-core FP32 path and of the reference for every precision.
+// The best target, the exact best distance and the accept decision are therefore the same as
+// those of the CUDA-core FP32 path and of the reference, for every precision.
+#include <cub/cub.cuh>
 #include <cuda_fp8.h>
 
 #include <cfloat>
+#include <climits>
 #include <cmath>
+#include <cstring>
 #include <vector>
 
 #include "fsb_internal.cuh"
@@ -42,27 +54,28 @@ inline unsigned nblk(long long n, int t) { return (unsigned)((n + t - 1) / t); }
 constexpr int TC_THREADS = 320;      // producer warp, MMA warp, 8 epilogue warps
 constexpr int TC_ROWS = 256;         // query rows per work item (two M=128 halves)
 constexpr int TC_N = 128;            // target rows per tile (MMA N)
-constexpr int TC_CHUNK = 32;         // columns per tcgen05.ld and per candidate chunk
+constexpr int TC_CHUNK = 32;         // columns per tcgen05.ld
 constexpr int TC_MAX_SPLITS = 8;
 constexpr long long TC_TIMEOUT_CYCLES = 4000000000ll;   // about two seconds at full clock
 
+// kind::f16 descriptor: F32 accumulator (bit 4), A and B BF16 (bits 7, 10), K-major, N>>3 at 17, M>>4 at 24
+constexpr uint32_t IDESC_BF16 = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(TC_N >> 3) << 17) |
+                                ((uint32_t)(128 >> 4) << 24);
+// kind::f8f6f4 descriptor: F32 accumulator, A and B E4M3 (format 0), K-major
+constexpr uint32_t IDESC_E4M3 = (1u << 4) | ((uint32_t)(TC_N >> 3) << 17) | ((uint32_t)(128 >> 4) << 24);
+
 template <int PREC> struct TcTraits;
 template <> struct TcTraits<FSB_PREC_BF16> {
-    static constexpr int ROW_BYTES = 288;   // 144 BF16 values
-    static constexpr int KSTEPS = 9;        // K = 16 per MMA (32 bytes)
+    static constexpr int ROW_BYTES = 288;   // 128 + 16 BF16 values
+    static constexpr int MAIN_STEPS = 8;    // K = 16 BF16 per MMA (32 bytes)
     static constexpr int STAGES = 4;
     static constexpr int TOPK = 2;
-    // kind::f16: F32 accumulator (bit 4), A and B BF16 (bits 7, 10), K-major, N>>3 at 17, M>>4 at 24
-    static constexpr uint32_t IDESC = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(TC_N >> 3) << 17) |
-                                      ((uint32_t)(128 >> 4) << 24);
 };
 template <> struct TcTraits<FSB_PREC_FP8> {
-    static constexpr int ROW_BYTES = 128;   // 128 E4M3 values
-    static constexpr int KSTEPS = 4;        // K = 32 per MMA (32 bytes)
+    static constexpr int ROW_BYTES = 160;   // 128 E4M3 + 16 BF16 values
+    static constexpr int MAIN_STEPS = 4;    // K = 32 E4M3 per MMA (32 bytes)
     static constexpr int STAGES = 8;
-    static constexpr int TOPK = 4;
-    // kind::f8f6f4: F32 accumulator, A and B E4M3 (format 0), K-major
-    static constexpr uint32_t IDESC = (1u << 4) | ((uint32_t)(TC_N >> 3) << 17) | ((uint32_t)(128 >> 4) << 24);
+    static constexpr int TOPK = 2;
 };
 
 template <int PREC> constexpr int tile_bytes() { return 128 * TcTraits<PREC>::ROW_BYTES; }
@@ -71,7 +84,7 @@ template <int PREC> constexpr int smem_bytes() {
 }
 
 // Byte offset of (row, k-byte) inside a 128-row block: core matrix (row / 8, kb / 16) at
-// (row / 8) * SBO + (kb / 16) * 128, with SBO = ROW_BYTES * 8 (LBO = 128).
+// (row / 8) * SBO + (kb / 16) * 128 with SBO = ROW_BYTES * 8; the descriptor's LBO is 128.
 __host__ __device__ constexpr int core_off(int row, int kb, int row_bytes) {
     return (row >> 3) * (row_bytes * 8) + (kb >> 4) * 128 + (row & 7) * 16 + (kb & 15);
 }
@@ -80,38 +93,43 @@ __host__ __device__ constexpr int core_off(int row, int kb, int row_bytes) {
 struct TcPair {
     const uint8_t* a;      // uint8 query rows (na x 128)
     const uint8_t* b;      // uint8 target rows (nb x 128)
-    const uint8_t* pa;     // packed query blocks (rb x 256 rows)
+    const uint8_t* pa;     // packed query blocks (nrb x 256 rows)
     const uint8_t* pb;     // packed target tiles (ntiles x 128 rows)
-    const float2* colsc;   // E4M3: per target (1 / s_b, |b|^2 / 2)
-    const float* rowsc;    // E4M3: per query (-s_a, 1 / s_a, |a|, |alpha|)
+    const float* rowsc;    // E4M3: per query (s, 1 / s, |a|, |alpha|)
     const float* bmax;     // E4M3: (max |b|, max |beta|) over the targets
     const int32_t* nA;     // |a|^2
     const int32_t* nB;     // |b|^2
+    int64_t* q_out;        // _unique output (capacity na)
+    int64_t* t_out;
     int na, nb, nrb, ntiles, splits, tps;   // tps: tiles per split
     int item0;             // first work item
-    int row0;              // first row in the concatenated row outputs
+    int row0;              // first row in the concatenated row arrays
     long long part0;       // first candidate record
+    long long key0;        // first target in the concatenated key array
 };
 
 struct Cand {
-    float v;   // a'.b' (BF16: exact; E4M3: s_a-scaled approximation until the end of the row)
-    int c;     // chunk index (column / 32), -1 when empty
+    float v;   // largest s * (a.b - |b|^2 / 2) of a 32-column chunk, as computed by the tensor cores
+    int j;     // the chunk (column / 32), -1 when empty
 };
 
-__device__ __forceinline__ int find_pair(const TcPair* __restrict__ pairs, int np, int item) {
-    int lo = 0, hi = np - 1;
-    while (lo < hi) {
-        const int mid = (lo + hi + 1) >> 1;
-        if (pairs[mid].item0 <= item) lo = mid; else hi = mid - 1;
-    }
-    return lo;
-}
+// Packing job: `n` rows of `src` (padded with zero rows to n_pad) into `dst`.
+struct PackSeg {
+    const uint8_t* src;
+    uint8_t* dst;
+    int32_t* norms;
+    float* rowsc;   // E4M3 queries
+    float* bmax;    // E4M3 targets
+    int n, n_pad, role;   // role 0: query, 1: target
+    long long first;      // first packed row of this job in the launch
+};
 
-__device__ __forceinline__ int find_pair_row(const TcPair* __restrict__ pairs, int np, int row) {
-    int lo = 0, hi = np - 1;
+template <class T, class F>
+__device__ __forceinline__ int upper_index(const T* __restrict__ arr, int n, long long key, F field) {
+    int lo = 0, hi = n - 1;   // last element with field <= key
     while (lo < hi) {
         const int mid = (lo + hi + 1) >> 1;
-        if (pairs[mid].row0 <= row) lo = mid; else hi = mid - 1;
+        if (field(arr[mid]) <= key) lo = mid; else hi = mid - 1;
     }
     return lo;
 }
@@ -121,74 +139,76 @@ __device__ __forceinline__ uint16_t bf16_bits(float x) {
     return (uint16_t)(__float_as_uint(x) >> 16);   // exact for the integers 0..255 and powers of two
 }
 
-// One warp per packed row (padding rows are written as zeros). role 0: query, 1: target.
+// One warp per packed row of every job.
 template <int PREC>
-__global__ void k_tc_pack(const uint8_t* __restrict__ src, int n, int n_pad, int role, uint8_t* __restrict__ dst,
-                          int32_t* __restrict__ norms, float2* __restrict__ colsc, float* __restrict__ rowsc,
-                          float* __restrict__ bmax) {
+__global__ void k_tc_pack(const PackSeg* __restrict__ segs, int nseg, long long total) {
     constexpr int RB = TcTraits<PREC>::ROW_BYTES;
-    const int row = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    constexpr int XB = RB - 32;   // byte offset of the norm slots
+    const long long gw = (long long)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
     const int lane = threadIdx.x & 31;
-    if (row >= n_pad) return;
-    uint8_t* blk = dst + (size_t)(row >> 7) * (128 * RB);
+    if (gw >= total) return;
+    const PackSeg& S = segs[upper_index(segs, nseg, gw, [](const PackSeg& x) { return x.first; })];
+    const int row = (int)(gw - S.first);
+    uint8_t* blk = S.dst + (size_t)(row >> 7) * (128 * RB);
     const int r = row & 127;
-    const uint32_t w = row < n ? reinterpret_cast<const uint32_t*>(src + (size_t)row * 128)[lane] : 0u;
+    const bool live = row < S.n;
+    const uint32_t w = live ? reinterpret_cast<const uint32_t*>(S.src + (size_t)row * 128)[lane] : 0u;
     int nrm = (int)__dp4a(w, w, 0u);
     for (int sh = 16; sh; sh >>= 1) nrm += __shfl_xor_sync(0xffffffffu, nrm, sh);
-    if (lane == 0 && row < n) norms[row] = nrm;
+    if (lane == 0 && live) S.norms[row] = nrm;
+    float s = 1.f;
     if constexpr (PREC == FSB_PREC_BF16) {
         uint2 v;
         v.x = (uint32_t)bf16_bits((float)(w & 255u)) | ((uint32_t)bf16_bits((float)((w >> 8) & 255u)) << 16);
         v.y = (uint32_t)bf16_bits((float)((w >> 16) & 255u)) | ((uint32_t)bf16_bits((float)(w >> 24)) << 16);
         *reinterpret_cast<uint2*>(blk + core_off(r, lane * 8, RB)) = v;
-        if (lane < 4) {   // the 16 norm slots (32 bytes), 8 bytes per lane
-            uint16_t e[4] = {0, 0, 0, 0};
-            if (lane == 0 && row < n) {
-                if (role == 0) {
-                    e[0] = bf16_bits(-32768.f);
-                    e[1] = bf16_bits(-128.f);
-                    e[2] = bf16_bits(-0.5f);
-                } else {
-                    e[0] = bf16_bits((float)((nrm >> 16) & 255));
-                    e[1] = bf16_bits((float)((nrm >> 8) & 255));
-                    e[2] = bf16_bits((float)(nrm & 255));
-                }
-            }
-            uint2 x;
-            x.x = (uint32_t)e[0] | ((uint32_t)e[1] << 16);
-            x.y = (uint32_t)e[2] | ((uint32_t)e[3] << 16);
-            *reinterpret_cast<uint2*>(blk + core_off(r, 256 + lane * 8, RB)) = x;
-        }
     } else {
-        // per-row power-of-two scale: the largest e <= 8 with max * 2^e <= 448
-        uint32_t mx = max(max(w & 255u, (w >> 8) & 255u), max((w >> 16) & 255u, w >> 24));
-        for (int sh = 16; sh; sh >>= 1) mx = max(mx, __shfl_xor_sync(0xffffffffu, mx, sh));
-        int e = 8;
-        while (e > 0 && (mx << e) > 448u) --e;
-        const float s = (float)(1 << e);
+        if (S.role == 0) {   // per-query power-of-two scale: the largest e <= 8 with max * 2^e <= 448
+            uint32_t mx = max(max(w & 255u, (w >> 8) & 255u), max((w >> 16) & 255u, w >> 24));
+            for (int sh = 16; sh; sh >>= 1) mx = max(mx, __shfl_xor_sync(0xffffffffu, mx, sh));
+            int e = 8;
+            while (e > 0 && (mx << e) > 448u) --e;
+            s = (float)(1 << e);
+        }
         uint32_t packed = 0;
         float err2 = 0.f;
 #pragma unroll
         for (int b = 0; b < 4; ++b) {
             const float x = (float)((w >> (8 * b)) & 255u);
             const __nv_fp8_storage_t q = __nv_cvt_float_to_fp8(x * s, __NV_SATFINITE, __NV_E4M3);
-            const __half_raw hr = __nv_cvt_fp8_to_halfraw(q, __NV_E4M3);
-            const float back = __half2float(__half(hr)) / s;
+            const float back = __half2float(__half(__nv_cvt_fp8_to_halfraw(q, __NV_E4M3))) / s;
             err2 = fmaf(back - x, back - x, err2);
             packed |= (uint32_t)q << (8 * b);
         }
         for (int sh = 16; sh; sh >>= 1) err2 += __shfl_xor_sync(0xffffffffu, err2, sh);
         *reinterpret_cast<uint32_t*>(blk + core_off(r, lane * 4, RB)) = packed;
-        if (lane == 0 && row < n) {
+        if (lane == 0 && live) {
             const float len = sqrtf((float)nrm) * (1.f + 1e-6f), elen = sqrtf(err2) * (1.f + 1e-6f);
-            if (role == 0) {
-                reinterpret_cast<float4*>(rowsc)[row] = make_float4(-s, 1.f / s, len, elen);
+            if (S.role == 0) {
+                reinterpret_cast<float4*>(S.rowsc)[row] = make_float4(s, 1.f / s, len, elen);
             } else {
-                colsc[row] = make_float2(1.f / s, 0.5f * (float)nrm);
-                atomicMax(reinterpret_cast<int*>(bmax), __float_as_int(len));
-                atomicMax(reinterpret_cast<int*>(bmax) + 1, __float_as_int(elen));
+                atomicMax(reinterpret_cast<int*>(S.bmax), __float_as_int(len));
+                atomicMax(reinterpret_cast<int*>(S.bmax) + 1, __float_as_int(elen));
             }
         }
+    }
+    if (lane < 4) {   // the 16 norm slots (32 bytes), 8 bytes per lane
+        uint16_t e[4] = {0, 0, 0, 0};
+        if (lane == 0 && live) {
+            if (S.role == 0) {
+                e[0] = bf16_bits(-32768.f * s);
+                e[1] = bf16_bits(-128.f * s);
+                e[2] = bf16_bits(-0.5f * s);
+            } else {
+                e[0] = bf16_bits((float)((nrm >> 16) & 255));
+                e[1] = bf16_bits((float)((nrm >> 8) & 255));
+                e[2] = bf16_bits((float)(nrm & 255));
+            }
+        }
+        uint2 x;
+        x.x = (uint32_t)e[0] | ((uint32_t)e[1] << 16);
+        x.y = (uint32_t)e[2] | ((uint32_t)e[3] << 16);
+        *reinterpret_cast<uint2*>(blk + core_off(r, XB + lane * 8, RB)) = x;
     }
 }
 
@@ -245,21 +265,19 @@ __device__ __forceinline__ uint64_t smem_desc(uint32_t addr, uint32_t sbo) {
            (1ull << 46);
 }
 
-template <int PREC>
-__device__ __forceinline__ void mma(uint32_t tmem_d, uint64_t da, uint64_t db, uint32_t accumulate) {
-    if constexpr (PREC == FSB_PREC_BF16) {
-        asm volatile(
-            "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
-            "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem_d),
-            "l"(da), "l"(db), "r"(TcTraits<PREC>::IDESC), "r"(accumulate)
-            : "memory");
-    } else {
-        asm volatile(
-            "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
-            "tcgen05.mma.cta_group::1.kind::f8f6f4 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem_d),
-            "l"(da), "l"(db), "r"(TcTraits<PREC>::IDESC), "r"(accumulate)
-            : "memory");
-    }
+__device__ __forceinline__ void mma_bf16(uint32_t tmem_d, uint64_t da, uint64_t db, uint32_t accumulate) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem_d),
+        "l"(da), "l"(db), "r"(IDESC_BF16), "r"(accumulate)
+        : "memory");
+}
+__device__ __forceinline__ void mma_e4m3(uint32_t tmem_d, uint64_t da, uint64_t db, uint32_t accumulate) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::f8f6f4 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem_d),
+        "l"(da), "l"(db), "r"(IDESC_E4M3), "r"(accumulate)
+        : "memory");
 }
 __device__ __forceinline__ void mma_commit(uint64_t* bar) {
     asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(saddr(bar))
@@ -285,18 +303,18 @@ __device__ __forceinline__ float max3(float a, float b, float c) {
     return r;
 }
 
+// v > t[K-1]: insert keeping t descending; among equal values the earlier chunk stays first
 template <int K>
-__device__ __forceinline__ void cand_insert(float (&m)[K], int (&c)[K], float v, int id) {
-    // v > m[K-1]; keep m descending, earlier chunks first among equal values
+__device__ __forceinline__ void top_insert(float (&t)[K], int (&j)[K], float v, int col) {
 #pragma unroll
     for (int i = K - 1; i >= 0; --i) {
-        if (v > m[i]) {
-            if (i > 0 && v > m[i - 1]) {
-                m[i] = m[i - 1];
-                c[i] = c[i - 1];
+        if (v > t[i]) {
+            if (i > 0 && v > t[i - 1]) {
+                t[i] = t[i - 1];
+                j[i] = j[i - 1];
             } else {
-                m[i] = v;
-                c[i] = id;
+                t[i] = v;
+                j[i] = col;
             }
         }
     }
@@ -313,21 +331,23 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
     constexpr int K = T::TOPK;
     constexpr uint32_t SBO = T::ROW_BYTES * 8;
     extern __shared__ __align__(1024) unsigned char smem_raw[];
-    unsigned char* smem = reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
-    unsigned char* sA = smem;                  // 2 x TB
-    unsigned char* sB = smem + 2 * TB;         // NST x TB
+    unsigned char* smem =
+        reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+    unsigned char* sA = smem;            // 2 x TB
+    unsigned char* sB = smem + 2 * TB;   // NST x TB
     uint64_t* bars = reinterpret_cast<uint64_t*>(sB + NST * TB);
-    uint64_t* b_full = bars;                   // NST
-    uint64_t* b_empty = bars + NST;            // NST
+    uint64_t* b_full = bars;             // NST
+    uint64_t* b_empty = bars + NST;      // NST
     uint64_t* a_full = bars + 2 * NST;
     uint64_t* a_empty = a_full + 1;
-    uint64_t* acc_full = a_full + 2;           // 2
-    uint64_t* acc_empty = a_full + 4;          // 2
+    uint64_t* acc_full = a_full + 2;     // 2
+    uint64_t* acc_empty = a_full + 4;    // 2
     uint64_t* done_bar = a_full + 6;
     uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(a_full + 8);
     volatile int* abort_flag = reinterpret_cast<volatile int*>(tmem_slot + 1);
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    auto item0_of = [](const TcPair& x) { return (long long)x.item0; };
     if (threadIdx.x == 0) {
         for (int i = 0; i < NST; ++i) {
             mbar_init(b_full + i, 1);
@@ -357,14 +377,14 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
     if (warp == 0) {
         // ---------------------------------------------------------------- producer
         if (lane == 0) {
-            uint32_t bit = 0;   // B tiles issued so far
+            uint32_t bit = 0;   // target tiles issued so far
             int wi = 0;
             bool ok = true;
             int pend[NST];
             for (int i = 0; i < NST; ++i) pend[i] = -1;
             int a_pend = -1;
             for (int item = blockIdx.x; item < n_items && ok; item += gridDim.x, ++wi) {
-                const TcPair& P = pairs[find_pair(pairs, n_pairs, item)];
+                const TcPair& P = pairs[upper_index(pairs, n_pairs, item, item0_of)];
                 const int local = item - P.item0;
                 const int rb = local / P.splits, sp = local - rb * P.splits;
                 const int t0 = sp * P.tps, t1 = min(P.ntiles, t0 + P.tps);
@@ -396,13 +416,13 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
             }
             if (!ok) {
                 // let every copy already issued land before the CTA leaves (bounded)
-                const long long t0 = clock64();
+                const long long c0 = clock64();
                 for (int st = 0; st < NST; ++st)
                     if (pend[st] >= 0)
-                        while (!mbar_test(b_full + st, (uint32_t)pend[st]) && clock64() - t0 < TC_TIMEOUT_CYCLES) {
+                        while (!mbar_test(b_full + st, (uint32_t)pend[st]) && clock64() - c0 < TC_TIMEOUT_CYCLES) {
                         }
                 if (a_pend >= 0)
-                    while (!mbar_test(a_full, (uint32_t)a_pend) && clock64() - t0 < TC_TIMEOUT_CYCLES) {
+                    while (!mbar_test(a_full, (uint32_t)a_pend) && clock64() - c0 < TC_TIMEOUT_CYCLES) {
                     }
             }
         }
@@ -412,15 +432,13 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
         if (lane == 0) {
             uint32_t bit = 0, tit = 0;
             int wi = 0;
-            bool ok = true;
-            bool issued = false;
+            bool ok = true, issued = false;
             const uint32_t a0 = saddr(sA), b0 = saddr(sB);
             for (int item = blockIdx.x; item < n_items && ok; item += gridDim.x, ++wi) {
-                const TcPair& P = pairs[find_pair(pairs, n_pairs, item)];
+                const TcPair& P = pairs[upper_index(pairs, n_pairs, item, item0_of)];
                 const int local = item - P.item0;
-                const int rb = local / P.splits, sp = local - rb * P.splits;
+                const int sp = local % P.splits;
                 const int t0 = sp * P.tps, t1 = min(P.ntiles, t0 + P.tps);
-                (void)rb;
                 ok = mbar_wait(a_full, wi & 1, abort_flag);
                 if (!ok) break;
                 tc_fence_after();
@@ -435,12 +453,16 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
 #pragma unroll
                     for (int h = 0; h < 2; ++h) {
                         const uint32_t d = tmem + (uint32_t)(ac * 256 + h * 128);
+                        const uint32_t ra = a0 + h * TB, rb = b0 + st * TB;
 #pragma unroll
-                        for (int k = 0; k < T::KSTEPS; ++k) {
-                            const uint64_t da = smem_desc(a0 + h * TB + k * 256, SBO);
-                            const uint64_t db = smem_desc(b0 + st * TB + k * 256, SBO);
-                            mma<PREC>(d, da, db, k > 0 ? 1u : 0u);
+                        for (int k = 0; k < T::MAIN_STEPS; ++k) {
+                            if constexpr (PREC == FSB_PREC_BF16)
+                                mma_bf16(d, smem_desc(ra + k * 256, SBO), smem_desc(rb + k * 256, SBO), k > 0);
+                            else
+                                mma_e4m3(d, smem_desc(ra + k * 256, SBO), smem_desc(rb + k * 256, SBO), k > 0);
                         }
+                        mma_bf16(d, smem_desc(ra + T::MAIN_STEPS * 256, SBO), smem_desc(rb + T::MAIN_STEPS * 256, SBO),
+                                 1u);
                     }
                     issued = true;
                     mma_commit(b_empty + st);
@@ -461,26 +483,24 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
     } else {
         // ---------------------------------------------------------------- epilogue
         const int ew = warp - 2;
-        const int lq = warp & 3;          // TMEM lane quarter this warp may access
-        const int h = ew >> 2;            // query half
+        const int lq = warp & 3;   // TMEM lane quarter this warp may access
+        const int h = ew >> 2;     // query half
         const int rloc = h * 128 + lq * 32 + lane;
         uint32_t tit = 0;
         bool ok = true;
         for (int item = blockIdx.x; item < n_items && ok; item += gridDim.x) {
-            const TcPair& P = pairs[find_pair(pairs, n_pairs, item)];
+            const TcPair& P = pairs[upper_index(pairs, n_pairs, item, item0_of)];
             const int local = item - P.item0;
             const int rb = local / P.splits, sp = local - rb * P.splits;
             const int t0 = sp * P.tps, t1 = min(P.ntiles, t0 + P.tps);
             const int q = rb * TC_ROWS + rloc;
-            float m[K];
-            int c[K];
+            float tv[K];
+            int tj[K];
 #pragma unroll
             for (int i = 0; i < K; ++i) {
-                m[i] = -INFINITY;
-                c[i] = -1;
+                tv[i] = -INFINITY;
+                tj[i] = -1;
             }
-            float neg_sa = -1.f;
-            if constexpr (PREC == FSB_PREC_FP8) neg_sa = q < P.na ? P.rowsc[4 * q] : -1.f;
             for (int t = t0; t < t1; ++t, ++tit) {
                 const int ac = tit & 1;
                 ok = mbar_wait(acc_full + ac, (tit >> 1) & 1, abort_flag);
@@ -499,18 +519,8 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
                     }
                     const int j0 = t * TC_N + ch * TC_CHUNK;
                     float v[32];
-                    if constexpr (PREC == FSB_PREC_FP8) {
-                        const float4* cs = reinterpret_cast<const float4*>(P.colsc + j0);
 #pragma unroll
-                        for (int i = 0; i < 16; ++i) {
-                            const float4 s4 = __ldg(cs + i);   // targets j0+2i, j0+2i+1 (padded table)
-                            v[2 * i] = fmaf(neg_sa, s4.y, __uint_as_float(r[2 * i]) * s4.x);
-                            v[2 * i + 1] = fmaf(neg_sa, s4.w, __uint_as_float(r[2 * i + 1]) * s4.z);
-                        }
-                    } else {
-#pragma unroll
-                        for (int i = 0; i < 32; ++i) v[i] = __uint_as_float(r[i]);
-                    }
+                    for (int i = 0; i < 32; ++i) v[i] = __uint_as_float(r[i]);
                     if (j0 + TC_CHUNK > P.nb) {
 #pragma unroll
                         for (int i = 0; i < 32; ++i)
@@ -526,14 +536,14 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
                     a6 = max3(a6, a7, a8);
                     a9 = fmaxf(a9, a10);
                     const float mx = fmaxf(max3(a0, a3, a6), a9);
-                    if (mx > m[K - 1]) cand_insert<K>(m, c, mx, j0 / TC_CHUNK);
+                    if (mx > tv[K - 1]) top_insert<K>(tv, tj, mx, j0 / TC_CHUNK);
                 }
             }
             if (!ok) break;
             if (q < P.na) {
                 Cand* out = part + P.part0 + ((size_t)q * P.splits + sp) * K;
 #pragma unroll
-                for (int i = 0; i < K; ++i) out[i] = Cand{m[i], c[i]};
+                for (int i = 0; i < K; ++i) out[i] = Cand{tv[i], tj[i]};
             }
         }
     }
@@ -565,7 +575,7 @@ __device__ __forceinline__ int exact_dot(const uint4 (&a)[8], const uint8_t* __r
     return (int)s;
 }
 
-// warp-wide merge of per-lane (d1, j1, d2): smallest d first, smaller index among equal d
+// warp-wide merge of per-lane (key1 = d << 32 | j, d2): smallest d first, smaller index among equal d
 __device__ __forceinline__ void warp_top2(long long& k1, long long& d2) {
     for (int sh = 16; sh; sh >>= 1) {
         const long long ok1 = __shfl_xor_sync(0xffffffffu, k1, sh);
@@ -576,6 +586,8 @@ __device__ __forceinline__ void warp_top2(long long& k1, long long& d2) {
     }
 }
 
+constexpr long long NO_D = LLONG_MAX >> 32;   // "no distance" (above every uint8 distance)
+
 template <int K>
 __global__ void k_tc_finish(const TcPair* __restrict__ pairs, int n_pairs, int n_rows, const Cand* __restrict__ part,
                             float ratio, int prec, int32_t* __restrict__ t_row, uint32_t* __restrict__ d_row,
@@ -583,7 +595,7 @@ __global__ void k_tc_finish(const TcPair* __restrict__ pairs, int n_pairs, int n
     const int g = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
     const int lane = threadIdx.x & 31;
     if (g >= n_rows) return;
-    const TcPair& P = pairs[find_pair_row(pairs, n_pairs, g)];
+    const TcPair& P = pairs[upper_index(pairs, n_pairs, g, [](const TcPair& x) { return (long long)x.row0; })];
     const int q = g - P.row0;
     if (q >= P.na) return;
     const int ne = P.splits * K;   // <= 32
@@ -594,7 +606,7 @@ __global__ void k_tc_finish(const TcPair* __restrict__ pairs, int n_pairs, int n
 #pragma unroll
     for (int k = 0; k < K; ++k) {
         float bv = e.v;
-        int bc = e.c < 0 ? INT_MAX : e.c;
+        int bc = e.j < 0 ? INT_MAX : e.j;
         for (int sh = 16; sh; sh >>= 1) {
             const float ov = __shfl_xor_sync(0xffffffffu, bv, sh);
             const int oc = __shfl_xor_sync(0xffffffffu, bc, sh);
@@ -605,19 +617,27 @@ __global__ void k_tc_finish(const TcPair* __restrict__ pairs, int n_pairs, int n
         }
         sv[k] = bv;
         sc[k] = bc == INT_MAX ? -1 : bc;
-        if (e.c == bc && e.c >= 0) e = Cand{-INFINITY, -1};
+        if (e.j == bc && e.j >= 0) e = Cand{-INFINITY, -1};
     }
-    // exact distances of the candidate columns
+    const long long na = P.nA[q];
+    double inv_s = 1.0, eps = 0.0;
+    if (prec == FSB_PREC_FP8) {
+        const float4 rs = reinterpret_cast<const float4*>(P.rowsc)[q];
+        const double bl = P.bmax[0], be = P.bmax[1];
+        inv_s = rs.y;
+        eps = (double)rs.z * be + (double)rs.w * bl + (double)rs.w * be + (double)rs.z * bl * (1.0 / 512.0) + 4.0;
+    }
+    // exact distances of the re-ranked chunks: one column per lane
+    const int nre = prec == FSB_PREC_BF16 ? 1 : K;
     const uint4* ar = reinterpret_cast<const uint4*>(P.a + (size_t)q * 128);
     uint4 a[8];
 #pragma unroll
     for (int i = 0; i < 8; ++i) a[i] = __ldg(ar + i);
-    const long long na = P.nA[q];
-    long long k1 = LLONG_MAX, d2 = LLONG_MAX >> 32;
+    long long k1 = LLONG_MAX, d2 = NO_D;
 #pragma unroll
     for (int k = 0; k < K; ++k) {
-        if (sc[k] < 0) continue;
-        const int j = sc[k] * 32 + lane;
+        if (k >= nre || sc[k] < 0) continue;
+        const int j = sc[k] * TC_CHUNK + lane;
         if (j >= P.nb) continue;
         const long long d = na + P.nB[j] - 2ll * exact_dot(a, P.b + (size_t)j * 128);
         const long long key = (d << 32) | (unsigned)j;
@@ -630,39 +650,42 @@ __global__ void k_tc_finish(const TcPair* __restrict__ pairs, int n_pairs, int n
     }
     warp_top2(k1, d2);
     if (lane != 0) return;
-    const long long e1 = k1 >> 32, e2 = d2;
+    const bool has1 = k1 != LLONG_MAX;
+    const long long e1 = has1 ? (k1 >> 32) : NO_D;
     const int j1 = (int)(k1 & 0xffffffffll);
-    // lower bound on the exact distance of every column outside the candidate chunks
-    double L = INFINITY;
-    if (sv[K - 1] > -INFINITY) {
-        double vk = sv[K - 1], eps = 0.0;
-        if (prec == FSB_PREC_FP8) {
-            const float4 rs = reinterpret_cast<const float4*>(P.rowsc)[q];
-            const double bl = P.bmax[0], be = P.bmax[1];
-            vk *= (double)rs.y;   // s_a-scaled -> a'.b' units
-            eps = (double)rs.z * be + (double)rs.w * bl + (double)rs.w * be + (double)rs.z * bl * (1.0 / 512.0) + 4.0;
+    long long e2 = d2;
+    bool mismatch = false;
+    float err = 0.f;
+    if (has1) {
+        const double approx = (double)na - 2.0 * (double)sv[0] * inv_s;   // the best chunk's maximum
+        err = (float)fabs(approx - (double)e1);
+        if (prec == FSB_PREC_BF16) {
+            mismatch = err != 0.f;
+            // BF16 values are exact: the best column outside the first chunk is the second chunk's maximum
+            if (sv[1] > -INFINITY) e2 = min(e2, na - (long long)(2.0 * (double)sv[1]));
         }
-        L = ceil((double)na - 2.0 * (vk + eps));
+    }
+    // lower bound on the exact distance of every column outside the re-ranked chunks
+    double L = INFINITY;
+    const float vb = sv[nre < K ? nre : K - 1];
+    if (vb > -INFINITY) {
+        L = ceil((double)na - 2.0 * ((double)vb * inv_s + eps));
         if (L < 0.0) L = 0.0;
     }
     const float fL = L > 16777216.0 ? 16777216.f : (float)L;
     const float f1 = e1 > (1ll << 24) ? 16777216.f : (float)e1;
     const float f2 = e2 > (1ll << 24) ? 16777216.f : (float)e2;
-    const bool has1 = k1 != LLONG_MAX;
     const bool accept = has1 && (double)e1 < L && ratio_ok(f1, fminf(f2, fL), ratio);
     const bool reject = !has1 || !ratio_ok(fminf(f1, fL), f2, ratio);
-    if (err_stat && has1 && sv[0] > -INFINITY) {
-        // distance error of the best candidate: approximate (from the chunk maximum) vs exact
-        double v1 = sv[0];
-        if (prec == FSB_PREC_FP8) v1 *= (double)reinterpret_cast<const float4*>(P.rowsc)[q].y;
-        const float de = (float)fabs(((double)na - 2.0 * v1) - (double)e1);
-        atomicMax(reinterpret_cast<int*>(err_stat), __float_as_int(de));
-        atomicAdd(err_stat + 1, de);
+    if (err_stat && has1) {
+        atomicMax(reinterpret_cast<int*>(err_stat), __float_as_int(err));
+        atomicAdd(err_stat + 1, err);
+        atomicAdd(reinterpret_cast<int*>(err_stat) + 2, 1);
     }
-    if (accept) {
+    if (!mismatch && accept) {
         t_row[g] = j1;
         d_row[g] = (uint32_t)e1;
-    } else if (reject) {
+    } else if (!mismatch && reject) {
         t_row[g] = -1;
         d_row[g] = has1 ? (uint32_t)e1 : 0u;
     } else {
@@ -681,14 +704,14 @@ __global__ void __launch_bounds__(256) k_tc_exact_rows(const TcPair* __restrict_
     const int nr = *n_rows;
     for (int ri = blockIdx.x; ri < nr; ri += gridDim.x) {
         const int g = rows[ri];
-        const TcPair& P = pairs[find_pair_row(pairs, n_pairs, g)];
+        const TcPair& P = pairs[upper_index(pairs, n_pairs, g, [](const TcPair& x) { return (long long)x.row0; })];
         const int q = g - P.row0;
         const uint4* ar = reinterpret_cast<const uint4*>(P.a + (size_t)q * 128);
         uint4 a[8];
 #pragma unroll
         for (int i = 0; i < 8; ++i) a[i] = __ldg(ar + i);
         const long long na = P.nA[q];
-        long long k1 = LLONG_MAX, d2 = LLONG_MAX >> 32;
+        long long k1 = LLONG_MAX, d2 = NO_D;
         for (int j = threadIdx.x; j < P.nb; j += blockDim.x) {
             const long long d = na + P.nB[j] - 2ll * exact_dot(a, P.b + (size_t)j * 128);
             const long long key = (d << 32) | (unsigned)j;
@@ -723,6 +746,45 @@ __global__ void __launch_bounds__(256) k_tc_exact_rows(const TcPair* __restrict_
     }
 }
 
+// ------------------------------------------------------------------------ batched _unique
+__global__ void k_tcu_fill(unsigned long long* __restrict__ key, long long n) {
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) key[i] = ~0ull;
+}
+
+__global__ void k_tcu_keys(const TcPair* __restrict__ pairs, int n_pairs, int n_rows, const int32_t* __restrict__ t_row,
+                           const uint32_t* __restrict__ d_row, unsigned long long* __restrict__ key) {
+    const int g = blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= n_rows) return;
+    const int t = t_row[g];
+    if (t < 0) return;
+    const TcPair& P = pairs[upper_index(pairs, n_pairs, g, [](const TcPair& x) { return (long long)x.row0; })];
+    const int q = g - P.row0;
+    if (q >= P.na) return;
+    atomicMin(key + P.key0 + t, ((unsigned long long)d_row[g] << 32) | (unsigned)q);
+}
+
+__global__ void k_tcu_flags(const unsigned long long* __restrict__ key, long long n, int32_t* __restrict__ flag) {
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i <= n) flag[i] = i < n && key[i] != ~0ull;
+}
+
+__global__ void k_tcu_emit(const TcPair* __restrict__ pairs, int n_pairs, long long n,
+                           const unsigned long long* __restrict__ key, const int32_t* __restrict__ pos,
+                           int32_t* __restrict__ counts) {
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const int p = upper_index(pairs, n_pairs, i, [](const TcPair& x) { return x.key0; });
+    const TcPair& P = pairs[p];
+    const long long local = i - P.key0;
+    if (local == P.nb - 1) counts[p] = pos[P.key0 + P.nb] - pos[P.key0];
+    const unsigned long long k = key[i];
+    if (k == ~0ull) return;
+    const int o = pos[i] - pos[P.key0];
+    P.q_out[o] = (int64_t)(k & 0xffffffffull);
+    P.t_out[o] = local;
+}
+
 template <int PREC>
 int32_t tc_launch_dense(const TcPair* d_pairs, int n_pairs, int n_items, Cand* part, int* err, int grid,
                         cudaStream_t s) {
@@ -740,15 +802,17 @@ int32_t tc_launch_dense(const TcPair* d_pairs, int n_pairs, int n_items, Cand* p
 
 }  // namespace
 
-// Tensor-core dense top-2 for a batch of pairs. Per pair p, rows [row0_p, row0_p + na_p) of t_row and
-// d_row receive the accepted target (or -1) and the exact best distance. Buffers come from ctx.
-int32_t run_match_bf_tc_rows(fsb_ctx* ctx, int n_pairs, const uint8_t* const* d_a, const int* na,
-                             const uint8_t* const* d_b, const int* nb, float ratio, int precision, int32_t* t_row,
-                             uint32_t* d_row, const int* row0, TcStats* stats, cudaStream_t s) {
+// Tensor-core dense matching of a batch of pairs, _unique included: pair p writes counts[p]
+// (device) matches into q_out[p], t_out[p] (device, capacity na[p]). Pairs need na, nb >= 1.
+// Scratch comes from ctx; stats (nullable) receives the certificate and error statistics.
+int32_t run_match_bf_tc(fsb_ctx* ctx, int n_pairs, const uint8_t* const* d_a, const int* na,
+                        const uint8_t* const* d_b, const int* nb, float ratio, int precision, int64_t* const* q_out,
+                        int64_t* const* t_out, int32_t* counts, TcStats* stats, cudaStream_t s) {
     if (precision != FSB_PREC_BF16 && precision != FSB_PREC_FP8) {
         set_error("precision %d has no tensor-core path", precision);
         return FSB_ERR_UNSUPPORTED;
     }
+    if (n_pairs <= 0) return FSB_OK;
     const bool fp8 = precision == FSB_PREC_FP8;
     const int RB = fp8 ? TcTraits<FSB_PREC_FP8>::ROW_BYTES : TcTraits<FSB_PREC_BF16>::ROW_BYTES;
     const int K = fp8 ? TcTraits<FSB_PREC_FP8>::TOPK : TcTraits<FSB_PREC_BF16>::TOPK;
@@ -758,11 +822,11 @@ int32_t run_match_bf_tc_rows(fsb_ctx* ctx, int n_pairs, const uint8_t* const* d_
         FSB_CUDA(cudaGetDevice(&dev));
         FSB_CUDA(cudaDeviceGetAttribute(&num_sms, cudaDevAttrMultiProcessorCount, dev));
     }
-    // layout of the scratch: packed operands, norms, scales, candidates, row lists
+    auto al = [](size_t x) { return (x + 255) & ~size_t(255); };
     std::vector<TcPair> hp(n_pairs);
-    size_t off_pa = 0, off_pb = 0, n_norm = 0, n_rows = 0, n_parts = 0, n_colsc = 0, n_rowsc = 0;
-    int items = 0, rows_total = 0;
-    long long rb_total = 0;
+    size_t off_pa = 0, off_pb = 0, n_norm = 0, n_parts = 0;
+    long long n_keys = 0, rb_total = 0;
+    int items = 0, rows = 0;
     for (int p = 0; p < n_pairs; ++p) rb_total += (na[p] + TC_ROWS - 1) / TC_ROWS;
     for (int p = 0; p < n_pairs; ++p) {
         TcPair& P = hp[p];
@@ -770,106 +834,110 @@ int32_t run_match_bf_tc_rows(fsb_ctx* ctx, int n_pairs, const uint8_t* const* d_
         P.b = d_b[p];
         P.na = na[p];
         P.nb = nb[p];
+        P.q_out = q_out[p];
+        P.t_out = t_out[p];
         P.nrb = (na[p] + TC_ROWS - 1) / TC_ROWS;
         P.ntiles = (nb[p] + TC_N - 1) / TC_N;
         int splits = 1;
-        if (rb_total < 2 * num_sms) {
+        if (rb_total < 2 * num_sms) {   // too few query blocks to fill the GPU: split the targets too
             splits = (int)((2 * num_sms + rb_total - 1) / rb_total);
-            splits = std::min(std::min(splits, TC_MAX_SPLITS), std::max(1, 32 / K));
-            splits = std::min(splits, P.ntiles);
-            splits = std::max(splits, 1);
+            splits = std::max(1, std::min(std::min(splits, TC_MAX_SPLITS), std::min(32 / K, P.ntiles)));
         }
         P.tps = (P.ntiles + splits - 1) / splits;
         P.splits = (P.ntiles + P.tps - 1) / P.tps;
         P.item0 = items;
-        P.row0 = row0 ? row0[p] : rows_total;
+        P.row0 = rows;
         P.part0 = (long long)n_parts;
+        P.key0 = n_keys;
         items += P.nrb * P.splits;
-        rows_total = std::max(rows_total, P.row0 + P.na);
+        rows += P.na;
+        n_keys += P.nb;
         off_pa += (size_t)P.nrb * TC_ROWS * RB;
         off_pb += (size_t)P.ntiles * TC_N * RB;
         n_norm += (size_t)P.na + P.nb;
         n_parts += (size_t)P.na * P.splits * K;
-        n_colsc += (size_t)P.ntiles * TC_N;
-        n_rowsc += (size_t)P.na;
     }
-    n_rows = (size_t)rows_total;
-    auto al = [](size_t x) { return (x + 255) & ~size_t(255); };
-    const size_t bytes_pack = al(off_pa) + al(off_pb);
-    const size_t bytes_aux = al(n_norm * 4) + al(n_colsc * 8) + al(n_rowsc * 16) + al((size_t)n_pairs * 8) +
-                             al(n_rows * 4) + al((size_t)n_pairs * sizeof(TcPair)) + 256;
-    FSB_TRY(ctx->s_tc_pack.ensure(bytes_pack));
+    size_t tb_scan = 0;
+    cub::DeviceScan::ExclusiveSum(nullptr, tb_scan, (int32_t*)nullptr, (int32_t*)nullptr, (int)(n_keys + 1), s);
+    // scratch layout
+    const size_t b_pairs = al((size_t)n_pairs * sizeof(TcPair)), b_segs = al((size_t)2 * n_pairs * sizeof(PackSeg));
+    const size_t b_norm = al(n_norm * 4), b_rowsc = fp8 ? al((size_t)rows * 16) : 0, b_bmax = al((size_t)n_pairs * 8);
+    const size_t b_rowi = al((size_t)rows * 4), b_keys = al((size_t)n_keys * 8), b_flag = al((size_t)(n_keys + 1) * 4);
+    FSB_TRY(ctx->s_tc_pack.ensure(al(off_pa) + al(off_pb)));
     FSB_TRY(ctx->s_tc_part.ensure(al(n_parts * sizeof(Cand)) + 256));
-    FSB_TRY(ctx->s_tc_aux.ensure(bytes_aux));
+    FSB_TRY(ctx->s_tc_aux.ensure(b_pairs + b_segs + b_norm + b_rowsc + b_bmax + 4 * b_rowi + b_keys + 2 * b_flag +
+                                 al(tb_scan) + 512));
     uint8_t* pack = ctx->s_tc_pack.as<uint8_t>();
-    uint8_t* aux = ctx->s_tc_aux.as<uint8_t>();
-    int32_t* norms = reinterpret_cast<int32_t*>(aux);
-    float2* colsc = reinterpret_cast<float2*>(aux + al(n_norm * 4));
-    float* rowsc = reinterpret_cast<float*>(reinterpret_cast<uint8_t*>(colsc) + al(n_colsc * 8));
-    float* bmax = reinterpret_cast<float*>(reinterpret_cast<uint8_t*>(rowsc) + al(n_rowsc * 16));
-    int32_t* flagged = reinterpret_cast<int32_t*>(reinterpret_cast<uint8_t*>(bmax) + al((size_t)n_pairs * 8));
-    TcPair* d_pairs = reinterpret_cast<TcPair*>(reinterpret_cast<uint8_t*>(flagged) + al(n_rows * 4));
-    int* small = reinterpret_cast<int*>(reinterpret_cast<uint8_t*>(d_pairs) + al((size_t)n_pairs * sizeof(TcPair)));
-    // small: [0] abort flag, [1] flagged rows, [2..3] error statistics (max, sum)
+    uint8_t* cur = ctx->s_tc_aux.as<uint8_t>();
+    auto take = [&](size_t bytes) {
+        uint8_t* p = cur;
+        cur += bytes;
+        return p;
+    };
+    TcPair* d_pairs = reinterpret_cast<TcPair*>(take(b_pairs));
+    PackSeg* d_segs = reinterpret_cast<PackSeg*>(take(b_segs));
+    int32_t* norms = reinterpret_cast<int32_t*>(take(b_norm));
+    float* rowsc = reinterpret_cast<float*>(take(b_rowsc));
+    float* bmax = reinterpret_cast<float*>(take(b_bmax));
+    int32_t* t_row = reinterpret_cast<int32_t*>(take(b_rowi));
+    uint32_t* d_row = reinterpret_cast<uint32_t*>(take(b_rowi));
+    int32_t* flagged = reinterpret_cast<int32_t*>(take(b_rowi));
+    take(b_rowi);
+    unsigned long long* keys = reinterpret_cast<unsigned long long*>(take(b_keys));
+    int32_t* flag = reinterpret_cast<int32_t*>(take(b_flag));
+    int32_t* pos = reinterpret_cast<int32_t*>(take(b_flag));
+    void* scan_tmp = take(al(tb_scan));
+    int* small = reinterpret_cast<int*>(take(256));   // [0] abort, [1] flagged rows, [2..4] error statistics
     FSB_CUDA(cudaMemsetAsync(small, 0, 64, s));
-    FSB_CUDA(cudaMemsetAsync(bmax, 0, (size_t)n_pairs * 8, s));
-    size_t pa = 0, pb = 0, nn = 0, cs = 0, rs = 0;
+    if (fp8) FSB_CUDA(cudaMemsetAsync(bmax, 0, (size_t)n_pairs * 8, s));
+    std::vector<PackSeg> segs;
+    segs.reserve(2 * n_pairs);
+    size_t pa = 0, pb = 0, nn = 0, rr = 0;
+    long long first = 0;
     for (int p = 0; p < n_pairs; ++p) {
         TcPair& P = hp[p];
         P.pa = pack + pa;
         P.pb = pack + al(off_pa) + pb;
         P.nA = norms + nn;
         P.nB = norms + nn + P.na;
-        P.colsc = colsc + cs;
-        P.rowsc = rowsc + rs * 4;
+        P.rowsc = fp8 ? rowsc + 4 * rr : nullptr;
         P.bmax = bmax + 2 * p;
-        pa += (size_t)P.nrb * TC_ROWS * RB;
-        pb += (size_t)P.ntiles * TC_N * RB;
-        nn += (size_t)P.na + P.nb;
-        cs += (size_t)P.ntiles * TC_N;
-        rs += (size_t)P.na;
         const int pad_a = P.nrb * TC_ROWS, pad_b = P.ntiles * TC_N;
-        if (fp8) {
-            FSB_CUDA(cudaMemsetAsync(const_cast<float2*>(P.colsc), 0, (size_t)pad_b * 8, s));
-            k_tc_pack<FSB_PREC_FP8><<<nblk(pad_a, 8), 256, 0, s>>>(P.a, P.na, pad_a, 0, const_cast<uint8_t*>(P.pa),
-                                                                  const_cast<int32_t*>(P.nA), nullptr,
-                                                                  const_cast<float*>(P.rowsc), nullptr);
-            k_tc_pack<FSB_PREC_FP8><<<nblk(pad_b, 8), 256, 0, s>>>(P.b, P.nb, pad_b, 1, const_cast<uint8_t*>(P.pb),
-                                                                  const_cast<int32_t*>(P.nB),
-                                                                  const_cast<float2*>(P.colsc), nullptr,
-                                                                  const_cast<float*>(P.bmax));
-        } else {
-            k_tc_pack<FSB_PREC_BF16><<<nblk(pad_a, 8), 256, 0, s>>>(P.a, P.na, pad_a, 0, const_cast<uint8_t*>(P.pa),
-                                                                   const_cast<int32_t*>(P.nA), nullptr, nullptr,
-                                                                   nullptr);
-            k_tc_pack<FSB_PREC_BF16><<<nblk(pad_b, 8), 256, 0, s>>>(P.b, P.nb, pad_b, 1, const_cast<uint8_t*>(P.pb),
-                                                                   const_cast<int32_t*>(P.nB), nullptr, nullptr,
-                                                                   nullptr);
-        }
-        note_launch(2);
+        segs.push_back(PackSeg{P.a, const_cast<uint8_t*>(P.pa), const_cast<int32_t*>(P.nA), const_cast<float*>(P.rowsc),
+                               nullptr, P.na, pad_a, 0, first});
+        first += pad_a;
+        segs.push_back(PackSeg{P.b, const_cast<uint8_t*>(P.pb), const_cast<int32_t*>(P.nB), nullptr,
+                               const_cast<float*>(P.bmax), P.nb, pad_b, 1, first});
+        first += pad_b;
+        pa += (size_t)pad_a * RB;
+        pb += (size_t)pad_b * RB;
+        nn += (size_t)P.na + P.nb;
+        rr += (size_t)P.na;
     }
-    FSB_CUDA(cudaGetLastError());
     FSB_CUDA(cudaMemcpyAsync(d_pairs, hp.data(), (size_t)n_pairs * sizeof(TcPair), cudaMemcpyHostToDevice, s));
+    FSB_CUDA(cudaMemcpyAsync(d_segs, segs.data(), segs.size() * sizeof(PackSeg), cudaMemcpyHostToDevice, s));
+    if (fp8)
+        k_tc_pack<FSB_PREC_FP8><<<nblk(first, 8), 256, 0, s>>>(d_segs, (int)segs.size(), first);
+    else
+        k_tc_pack<FSB_PREC_BF16><<<nblk(first, 8), 256, 0, s>>>(d_segs, (int)segs.size(), first);
+    note_launch(1);
+    FSB_CUDA(cudaGetLastError());
     Cand* part = ctx->s_tc_part.as<Cand>();
-    const int grid = std::min(items, num_sms);
-    if (items > 0) {
-        if (fp8) FSB_TRY(tc_launch_dense<FSB_PREC_FP8>(d_pairs, n_pairs, items, part, small, grid, s));
-        else FSB_TRY(tc_launch_dense<FSB_PREC_BF16>(d_pairs, n_pairs, items, part, small, grid, s));
-        note_launch(1);
-    }
-    if (rows_total > 0) {
-        if (fp8)
-            k_tc_finish<TcTraits<FSB_PREC_FP8>::TOPK><<<nblk(rows_total, 8), 256, 0, s>>>(
-                d_pairs, n_pairs, rows_total, part, ratio, precision, t_row, d_row, flagged, small + 1,
-                stats ? reinterpret_cast<float*>(small + 2) : nullptr);
-        else
-            k_tc_finish<TcTraits<FSB_PREC_BF16>::TOPK><<<nblk(rows_total, 8), 256, 0, s>>>(
-                d_pairs, n_pairs, rows_total, part, ratio, precision, t_row, d_row, flagged, small + 1,
-                stats ? reinterpret_cast<float*>(small + 2) : nullptr);
-        note_launch(1);
-        FSB_CUDA(cudaGetLastError());
-    }
-    int host_small[4] = {0, 0, 0, 0};
+    ctx->stage_begin(ST_TC_DENSE);
+    if (fp8) FSB_TRY(tc_launch_dense<FSB_PREC_FP8>(d_pairs, n_pairs, items, part, small, std::min(items, num_sms), s));
+    else FSB_TRY(tc_launch_dense<FSB_PREC_BF16>(d_pairs, n_pairs, items, part, small, std::min(items, num_sms), s));
+    note_launch(1);
+    ctx->stage_end(ST_TC_DENSE);
+    float* err_stat = stats ? reinterpret_cast<float*>(small + 2) : nullptr;
+    if (fp8)
+        k_tc_finish<TcTraits<FSB_PREC_FP8>::TOPK><<<nblk(rows, 8), 256, 0, s>>>(
+            d_pairs, n_pairs, rows, part, ratio, precision, t_row, d_row, flagged, small + 1, err_stat);
+    else
+        k_tc_finish<TcTraits<FSB_PREC_BF16>::TOPK><<<nblk(rows, 8), 256, 0, s>>>(
+            d_pairs, n_pairs, rows, part, ratio, precision, t_row, d_row, flagged, small + 1, err_stat);
+    note_launch(1);
+    FSB_CUDA(cudaGetLastError());
+    int host_small[5] = {0, 0, 0, 0, 0};
     FSB_CUDA(cudaMemcpyAsync(host_small, small, sizeof(host_small), cudaMemcpyDeviceToHost, s));
     FSB_CUDA(cudaStreamSynchronize(s));
     if (host_small[0]) {
@@ -882,14 +950,22 @@ int32_t run_match_bf_tc_rows(fsb_ctx* ctx, int n_pairs, const uint8_t* const* d_
         note_launch(1);
         FSB_CUDA(cudaGetLastError());
     }
+    // _unique of every pair
+    k_tcu_fill<<<nblk(n_keys, 256), 256, 0, s>>>(keys, n_keys);
+    k_tcu_keys<<<nblk(rows, 256), 256, 0, s>>>(d_pairs, n_pairs, rows, t_row, d_row, keys);
+    k_tcu_flags<<<nblk(n_keys + 1, 256), 256, 0, s>>>(keys, n_keys, flag);
+    FSB_CUDA(cub::DeviceScan::ExclusiveSum(scan_tmp, tb_scan, flag, pos, (int)(n_keys + 1), s));
+    k_tcu_emit<<<nblk(n_keys, 256), 256, 0, s>>>(d_pairs, n_pairs, n_keys, keys, pos, counts);
+    note_launch(5);
+    FSB_CUDA(cudaGetLastError());
     if (stats) {
         float mx, sum;
         memcpy(&mx, &host_small[2], 4);
         memcpy(&sum, &host_small[3], 4);
-        stats->rows = rows_total;
+        stats->rows = rows;
         stats->fallback_rows = host_small[1];
         stats->max_abs_err = mx;
-        stats->mean_abs_err = rows_total ? sum / (float)rows_total : 0.f;
+        stats->mean_abs_err = host_small[4] ? sum / (float)host_small[4] : 0.f;
     }
     return FSB_OK;
 }

@@ -36,12 +36,14 @@ def _ratio_match_bf(da, db, ratio, na=None, nb=None, precision="fp32", device=0)
     return q[:n.value].copy(), t[:n.value].copy()
 
 
-def ratio_match_bf_batch_d(a_list, b_list, ratio, precision="bf16", device=0):
+def ratio_match_bf_batch_d(a_list, b_list, ratio, precision="bf16", device=0, out=None):
     """Many independent ``_ratio_match_bf`` problems in one call on device-resident descriptors.
 
     ``a_list[p]``, ``b_list[p]`` are CUDA tensors (uint8, n x 128, contiguous) on ``device``.
-    Returns a list of (q, t) int64 CUDA tensors, ordered by target like ``_ratio_match_bf``.
-    With ``precision`` "bf16" or "fp8" every pair goes through one persistent tensor-core launch.
+    Returns a list of (q, t) int64 CUDA tensors, ordered by target like ``_ratio_match_bf``
+    (views into ``out[p]`` when given: pairs of int64 CUDA tensors with at least len(a_list[p])
+    elements each, reused across calls). With ``precision`` "bf16" or "fp8" every pair goes
+    through one persistent tensor-core launch.
     """
     import torch
     if len(a_list) != len(b_list):
@@ -51,8 +53,14 @@ def ratio_match_bf_batch_d(a_list, b_list, ratio, precision="bf16", device=0):
         if x.dtype != torch.uint8 or x.dim() != 2 or x.shape[1] != 128 or not x.is_contiguous() or not x.is_cuda:
             raise ValueError("descriptors must be contiguous CUDA uint8 tensors of shape (n, 128)")
     ctx = _lib.context(device)
-    outs = [(torch.empty(max(len(a), 1), dtype=torch.int64, device=a.device),
-             torch.empty(max(len(a), 1), dtype=torch.int64, device=a.device)) for a in a_list]
+    if out is None:
+        outs = [(torch.empty(max(len(a), 1), dtype=torch.int64, device=a.device),
+                 torch.empty(max(len(a), 1), dtype=torch.int64, device=a.device)) for a in a_list]
+    else:
+        outs = list(out)
+        if len(outs) != n or any(len(q) < len(a) or len(t) < len(a) or q.dtype != torch.int64 or t.dtype != torch.int64
+                                 for (q, t), a in zip(outs, a_list)):
+            raise ValueError("out must hold one (q, t) pair of int64 tensors of length >= na per pair")
     P = ctypes.c_void_p * max(n, 1)
     I = ctypes.c_int32 * max(n, 1)
     pa = P(*[a.data_ptr() for a in a_list])

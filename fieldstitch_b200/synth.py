@@ -133,3 +133,32 @@ def synth_descriptors(na, nb, seed, true_frac=0.3, noise=4):
     truth = np.full(nb, -1, np.int64)
     truth[rows_b] = rows_a
     return a, b, truth
+
+
+def synth_descriptors_device(na, nb, seed, device=0, true_frac=0.3, noise=4):
+    """``synth_descriptors`` drawn on the GPU with torch (same distribution: gamma(0.6) magnitudes,
+    L2-normalised, clipped at 0.2, renormalised, x512 rounded to uint8; a ``true_frac`` share of B
+    rows are copies of A rows with uniform +-noise byte jitter). Returns (A, B, truth) CUDA tensors;
+    for benchmark batches too large to draw on the host."""
+    import torch
+    dev = torch.device("cuda", device)
+    with torch.random.fork_rng(devices=[dev]):
+        torch.manual_seed(seed)
+
+        def sift_like(n):
+            v = torch._standard_gamma(torch.full((n, 128), 0.6, device=dev))
+            v = v / v.norm(dim=1, keepdim=True).clamp_min(1e-12)
+            v = v.clamp_max(0.2)
+            v = v / v.norm(dim=1, keepdim=True).clamp_min(1e-12)
+            return torch.round(v * 512.0).clamp(0, 255).to(torch.uint8)
+
+        a = sift_like(na)
+        b = sift_like(nb)
+        n_true = int(round(true_frac * min(na, nb)))
+        rows_b = torch.randperm(nb, device=dev)[:n_true]
+        rows_a = torch.randperm(na, device=dev)[:n_true]
+        jitter = torch.randint(-noise, noise + 1, (n_true, 128), device=dev, dtype=torch.int32)
+        b[rows_b] = (a[rows_a].to(torch.int32) + jitter).clamp(0, 255).to(torch.uint8)
+        truth = torch.full((nb,), -1, dtype=torch.int64, device=dev)
+        truth[rows_b] = rows_a
+    return a.contiguous(), b.contiguous(), truth

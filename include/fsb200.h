@@ -80,7 +80,8 @@ int32_t fsb_stage_times(fsb_ctx* ctx, double* ms, int64_t* calls, int32_t n);
 #define FSB_STAGE_SPREAD 6
 #define FSB_STAGE_DESCRIBE 7
 #define FSB_STAGE_MATCH 8
-#define FSB_STAGE_COUNT 9
+#define FSB_STAGE_TC_DENSE 9 /* the tensor-core contraction kernel alone (inside FSB_STAGE_MATCH) */
+#define FSB_STAGE_COUNT 10
 
 /* ---- SIFT detection / description ---------------------------------------------------------- */
 /* gsift.detect (app/planesite/gsift.py:435-477): 2x upsample, Gaussian/DoG pyramid, 3x3x3
