@@ -58,6 +58,19 @@ SIGNATURES = [
     ("fsb_match_bf_noalloc", c_i32, [c_vp, c_i32, c_vp, c_i32, c_f32, c_vp, c_vp, c_vp, c_vp]),
     ("fsb_match_bf_batch_d", c_i32, [c_vp, c_i32, c_vp, c_vp, c_vp, c_vp, c_f32, c_i32, c_vp, c_vp, c_vp]),
     ("fsb_match_tc_stats", c_i32, [c_vp, c_vp, c_vp, c_vp, c_vp]),
+    ("fsb_sift_features_ex_d", c_i32, [c_vp, c_vp, c_i32, c_i32, c_i32, c_vp, c_i32, c_vp, c_vp, c_vp, c_vp, c_vp,
+                                       c_vp, c_vp, c_vp]),
+    ("fsb_match_guided_cand_d", c_i32, [c_vp, c_vp, c_vp, c_i32, c_vp, c_vp, c_i32, c_f64, c_f64, c_f64, c_i32,
+                                        c_vp, c_vp]),
+    ("fsb_mlp_param_count", c_i32, []),
+    ("fsb_mlp_trainable_count", c_i32, []),
+    ("fsb_mlp_features_d", c_i32, [c_vp, c_i32, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp,
+                                   c_f32, c_vp]),
+    ("fsb_mlp_grad_d", c_i32, [c_vp, c_vp, c_i32, c_vp, c_vp, c_vp, c_vp]),
+    ("fsb_mlp_train_d", c_i32, [c_vp, c_vp, c_vp, c_vp, c_i32, c_vp, c_vp, c_i32, c_i32, c_f32, ctypes.c_uint32,
+                                c_vp]),
+    ("fsb_mlp_infer_d", c_i32, [c_vp, c_vp, c_i32, c_vp, c_i32, c_vp]),
+    ("fsb_mlp_filter_d", c_i32, [c_vp, c_i32, c_vp, c_vp, c_vp, c_f32, c_f32, c_i32, c_vp, c_vp, c_vp]),
 ]
 
 STAGES = ("upload", "pyramid", "extrema", "refine", "orientation", "sort", "spread", "describe", "match", "tc_dense")

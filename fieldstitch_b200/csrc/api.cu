@@ -145,7 +145,8 @@ __global__ void k_take(const int32_t* __restrict__ sel, int n, const float* x, c
 // features.sift_gpu after detection: spread, stable response order, describe; device outputs
 // (d_xy n*2 interleaved, d_resp, d_desc, d_u8; each nullable). *n_out = 0 below 10 keypoints.
 static int32_t features_dev(fsb_ctx* ctx, Workspace& ws, int nfeat, bool exact, float* d_xy, float* d_resp,
-                            float* d_desc, uint8_t* d_u8, int* n_out) {
+                            float* d_desc, uint8_t* d_u8, int* n_out, float* d_size = nullptr,
+                            float* d_angle = nullptr, int32_t* d_oct = nullptr) {
     cudaStream_t s = ctx->stream;
     *n_out = 0;
     if (ws.n_kp < 10) return FSB_OK;
@@ -173,6 +174,9 @@ static int32_t features_dev(fsb_ctx* ctx, Workspace& ws, int nfeat, bool exact, 
     ctx->stage_begin(ST_DESCRIBE);
     FSB_TRY(run_describe_mode(ws, n_sel, tx, ty, tsz, tan_, toc, tly, d_desc, d_u8, exact, s));
     ctx->stage_end(ST_DESCRIBE);
+    if (d_size) FSB_CUDA(cudaMemcpyAsync(d_size, tsz, (size_t)n_sel * 4, cudaMemcpyDeviceToDevice, s));
+    if (d_angle) FSB_CUDA(cudaMemcpyAsync(d_angle, tan_, (size_t)n_sel * 4, cudaMemcpyDeviceToDevice, s));
+    if (d_oct) FSB_CUDA(cudaMemcpyAsync(d_oct, toc, (size_t)n_sel * 4, cudaMemcpyDeviceToDevice, s));
     *n_out = n_sel;
     return FSB_OK;
 }
@@ -503,6 +507,32 @@ int32_t fsb_sift_features_d(fsb_ctx* ctx, const uint8_t* d_img, int32_t h, int32
     return FSB_OK;
 }
 
+int32_t fsb_sift_features_ex_d(fsb_ctx* ctx, const uint8_t* d_img, int32_t h, int32_t w, int32_t stride,
+                               const fsb_sift_params* p, int32_t nfeat, float* d_xy, float* d_resp, float* d_desc,
+                               uint8_t* d_rootsift, float* d_size, float* d_angle, int32_t* d_octave,
+                               int32_t* n_out) {
+    FSB_ARG(ctx && d_img && p && n_out, "null pointer");
+    FSB_ARG(h > 0 && w > 0 && stride >= w, "bad image size or stride");
+    FSB_ARG(h <= 32768 && w <= 32768, "image larger than 32768 pixels on a side");
+    FSB_ARG(nfeat >= 0, "nfeat < 0");
+    *n_out = 0;
+    FSB_TRY(use_device(ctx));
+    Workspace* ws = acquire(ctx);
+    struct Guard {
+        fsb_ctx* c;
+        Workspace* w;
+        ~Guard() { give_back(c, w); }
+    } guard{ctx, ws};
+    FSB_TRY(prepare_workspace(*ws, h, w));
+    FSB_TRY(detect_dev(ctx, *ws, d_img, stride, p, (int)((double)nfeat * 2.2)));
+    int n = 0;
+    FSB_TRY(features_dev(ctx, *ws, nfeat, (p->flags & FSB_SIFT_EXACT_BLUR) != 0, d_xy, d_resp, d_desc, d_rootsift,
+                         &n, d_size, d_angle, d_octave));
+    FSB_CUDA(cudaStreamSynchronize(ctx->stream));
+    *n_out = n;
+    return FSB_OK;
+}
+
 int32_t fsb_project_d(fsb_ctx* ctx, const float* d_xy, int32_t n, const double* hm9, const float* d_offset,
                       double* d_out) {
     FSB_ARG(ctx && hm9, "null pointer");
@@ -622,6 +652,90 @@ int32_t fsb_match_tc_stats(fsb_ctx* ctx, int64_t* rows, int64_t* fallback_rows, 
     if (fallback_rows) *fallback_rows = ctx->tc_stats.fallback_rows;
     if (max_abs_err) *max_abs_err = ctx->tc_stats.max_abs_err;
     if (mean_abs_err) *mean_abs_err = ctx->tc_stats.mean_abs_err;
+    return FSB_OK;
+}
+
+int32_t fsb_match_guided_cand_d(fsb_ctx* ctx, const double* d_pred, const uint8_t* d_a, int32_t na,
+                                const double* d_bxy, const uint8_t* d_b, int32_t nb, double w_b, double h_b,
+                                double radius, int32_t kc, int32_t* d_t1, float* d_b12) {
+    FSB_ARG(ctx, "null pointer");
+    FSB_ARG(na >= 0 && nb >= 0, "negative size");
+    FSB_ARG((na == 0 || (d_a && d_pred && d_t1 && d_b12)) && (nb == 0 || (d_b && d_bxy)), "null array");
+    FSB_ARG(std::isfinite(radius) && std::isfinite(w_b) && std::isfinite(h_b), "non-finite frame or radius");
+    if (na == 0) return FSB_OK;
+    FSB_TRY(use_device(ctx));
+    cudaStream_t s = ctx->stream;
+    ctx->stage_begin(ST_MATCH);
+    FSB_TRY(run_match_guided(ctx, d_pred, d_a, na, d_bxy, d_b, nb, w_b, h_b, radius, kc, 1.f, nullptr, nullptr,
+                             nullptr, s, d_t1, d_b12));
+    FSB_CUDA(cudaStreamSynchronize(s));
+    ctx->stage_end(ST_MATCH);
+    return FSB_OK;
+}
+
+int32_t fsb_mlp_param_count(void) { return mlp_param_count(); }
+int32_t fsb_mlp_trainable_count(void) { return mlp_trainable_count(); }
+
+int32_t fsb_mlp_features_d(fsb_ctx* ctx, int32_t n, const int32_t* d_t1, const float* d_b12, const double* d_pred,
+                           const float* d_xy_b, const float* d_size_a, const float* d_angle_a, const float* d_resp_a,
+                           const int32_t* d_oct_a, const float* d_size_b, const float* d_angle_b,
+                           const float* d_resp_b, float radius, float* d_feat) {
+    FSB_ARG(ctx && n >= 0, "bad arguments");
+    FSB_ARG(n == 0 || (d_t1 && d_b12 && d_pred && d_xy_b && d_size_a && d_angle_a && d_resp_a && d_oct_a && d_size_b &&
+                       d_angle_b && d_resp_b && d_feat), "null array");
+    FSB_ARG(radius > 0.f, "radius must be positive");
+    if (n == 0) return FSB_OK;
+    FSB_TRY(use_device(ctx));
+    FSB_TRY(run_mlp_features(n, d_t1, d_b12, d_pred, d_xy_b, d_size_a, d_angle_a, d_resp_a, d_oct_a, d_size_b,
+                             d_angle_b, d_resp_b, radius, d_feat, ctx->stream));
+    FSB_CUDA(cudaStreamSynchronize(ctx->stream));
+    return FSB_OK;
+}
+
+int32_t fsb_mlp_grad_d(fsb_ctx* ctx, const float* d_params, int32_t n, const float* d_feat, const float* d_label,
+                       float* d_grad, double* loss) {
+    FSB_ARG(ctx && d_params && d_grad && n > 0 && d_feat && d_label, "bad arguments");
+    FSB_TRY(use_device(ctx));
+    return run_mlp_grad(ctx, d_params, n, d_feat, d_label, d_grad, loss, ctx->stream);
+}
+
+int32_t fsb_mlp_train_d(fsb_ctx* ctx, float* d_params, float* d_m, float* d_v, int32_t n, const float* d_feat,
+                        const float* d_label, int32_t epochs, int32_t batch, float lr, uint32_t seed, double* losses) {
+    FSB_ARG(ctx && d_params && d_m && d_v && d_feat && d_label, "null pointer");
+    FSB_ARG(n > 0 && epochs >= 0 && batch > 0 && lr > 0.f, "bad training arguments");
+    FSB_TRY(use_device(ctx));
+    return run_mlp_train(ctx, d_params, d_m, d_v, n, d_feat, d_label, epochs, batch, lr, seed, losses, ctx->stream);
+}
+
+int32_t fsb_mlp_infer_d(fsb_ctx* ctx, const float* d_params, int32_t n, const float* d_feat, int32_t bf16,
+                        float* d_prob) {
+    FSB_ARG(ctx && d_params && n >= 0 && (n == 0 || (d_feat && d_prob)), "bad arguments");
+    if (n == 0) return FSB_OK;
+    FSB_TRY(use_device(ctx));
+    FSB_TRY(run_mlp_infer(d_params, n, d_feat, bf16 != 0, d_prob, ctx->stream));
+    FSB_CUDA(cudaStreamSynchronize(ctx->stream));
+    return FSB_OK;
+}
+
+int32_t fsb_mlp_filter_d(fsb_ctx* ctx, int32_t na, const int32_t* d_t1, const float* d_b12, const float* d_prob,
+                         float threshold, float ratio, int32_t nb, int64_t* d_q, int64_t* d_t, int32_t* n_out) {
+    FSB_ARG(ctx && n_out && na >= 0 && nb >= 0, "bad arguments");
+    FSB_ARG(na == 0 || (d_t1 && d_b12 && d_q && d_t), "null array");
+    *n_out = 0;
+    if (na == 0 || nb == 0) return FSB_OK;
+    FSB_TRY(use_device(ctx));
+    cudaStream_t s = ctx->stream;
+    FSB_TRY(ctx->s_i32.ensure((size_t)na * 8 + 64));
+    int32_t* t_row = ctx->s_i32.as<int32_t>();
+    uint32_t* d_row = reinterpret_cast<uint32_t*>(t_row + na);
+    FSB_TRY(ctx->s_count.ensure(64));
+    int* dn = ctx->s_count.as<int>();
+    FSB_TRY(run_mlp_accept(na, d_t1, d_b12, d_prob, threshold, ratio, t_row, d_row, s));
+    FSB_TRY(run_unique_rows(ctx, t_row, d_row, na, nb, d_q, d_t, dn, s));
+    int n = 0;
+    FSB_CUDA(cudaMemcpyAsync(&n, dn, sizeof(int), cudaMemcpyDeviceToHost, s));
+    FSB_CUDA(cudaStreamSynchronize(s));
+    *n_out = n;
     return FSB_OK;
 }
 

@@ -179,9 +179,27 @@ int32_t run_spread(const Workspace& ws, int nfeat, int32_t* d_sel, int* n_sel, f
 // ---------------------------------------------------------------- match.cu
 int32_t run_match_bf(fsb_ctx* ctx, const uint8_t* d_a, int na, const uint8_t* d_b, int nb, float ratio,
                      int precision, int64_t* d_q, int64_t* d_t, int* d_n, cudaStream_t s);
+// d_n null: candidates only (c_t, c_b12: best target or -1, b1, b2 per query; no ratio test, no _unique)
 int32_t run_match_guided(fsb_ctx* ctx, const double* d_pred, const uint8_t* d_a, int na, const double* d_bxy,
                          const uint8_t* d_b, int nb, double wb, double hb, double radius, int kc, float ratio,
-                         int64_t* d_q, int64_t* d_t, int* d_n, cudaStream_t s);
+                         int64_t* d_q, int64_t* d_t, int* d_n, cudaStream_t s, int32_t* c_t = nullptr,
+                         float* c_b12 = nullptr);
+int32_t run_unique_rows(fsb_ctx* ctx, const int32_t* t_row, const uint32_t* d_row, int na, int nb, int64_t* d_q,
+                        int64_t* d_t, int* d_n, cudaStream_t s);
+// mlp.cu
+int mlp_param_count();
+int mlp_trainable_count();
+int32_t run_mlp_features(int n, const int32_t* t1, const float* b12, const double* pred, const float* xy_b,
+                         const float* size_a, const float* angle_a, const float* resp_a, const int32_t* oct_a,
+                         const float* size_b, const float* angle_b, const float* resp_b, float radius, float* feat,
+                         cudaStream_t s);
+int32_t run_mlp_infer(const float* prm, int n, const float* feat, bool bf16, float* prob, cudaStream_t s);
+int32_t run_mlp_accept(int n, const int32_t* t1, const float* b12, const float* prob, float thr, float ratio,
+                       int32_t* t_row, uint32_t* d_row, cudaStream_t s);
+int32_t run_mlp_grad(fsb_ctx* ctx, const float* prm, int n, const float* feat, const float* label, float* grad,
+                     double* loss, cudaStream_t s);
+int32_t run_mlp_train(fsb_ctx* ctx, float* prm, float* m, float* v, int n, const float* feat, const float* label,
+                      int epochs, int batch, float lr, uint32_t seed, double* losses, cudaStream_t s);
 // tc_match.cu: tensor-core dense matching of a batch of pairs (na, nb >= 1), _unique included;
 // counts (device, one per pair), q_out/t_out device arrays of capacity na[p]
 int32_t run_match_bf_tc(fsb_ctx* ctx, int n_pairs, const uint8_t* const* d_a, const int* na,

@@ -243,6 +243,7 @@ __global__ void __launch_bounds__(G_WARPS * 32) k_guided(const double* __restric
                                                          const int32_t* __restrict__ items, double wb, double hb,
                                                          double radius, int kc, float ratio,
                                                          int32_t* __restrict__ t_row, uint32_t* __restrict__ d_row,
+                                                         int32_t* __restrict__ c_t, float* __restrict__ c_b12,
                                                          int* __restrict__ overflow) {
     __shared__ uint32_t s_q[G_WARPS][32];
     __shared__ double s_cd[G_WARPS][G_CAND];
@@ -253,6 +254,8 @@ __global__ void __launch_bounds__(G_WARPS * 32) k_guided(const double* __restric
     const double px = pred[2 * q], py = pred[2 * q + 1];
     int32_t res_t = -1;
     uint32_t res_d = 0;
+    int32_t cand_t = -1;
+    float cand_b1 = INFINITY, cand_b2 = INFINITY;
     const bool inside = px > -radius && px < wb + radius && py > -radius && py < hb + radius;
     if (inside) {
         s_q[wid][lane] = reinterpret_cast<const uint32_t*>(A + (size_t)q * 128)[lane];
@@ -333,6 +336,9 @@ __global__ void __launch_bounds__(G_WARPS * 32) k_guided(const double* __restric
             o.i1 = __shfl_xor_sync(0xffffffffu, best.i1, sh);
             best = top2_merge(best, o);
         }
+        cand_t = best.i1;
+        cand_b1 = best.b1;
+        cand_b2 = best.b2;
         if (best.i1 >= 0) {
             // single candidate: b2 = inf passes (app/planesite/matching.py:142-146)
             const bool ok = __fsqrt_rn(best.b1) < __fmul_rn(ratio, __fsqrt_rn(best.b2));
@@ -343,8 +349,15 @@ __global__ void __launch_bounds__(G_WARPS * 32) k_guided(const double* __restric
         }
     }
     if (lane == 0) {
-        t_row[q] = res_t;
-        d_row[q] = res_d;
+        if (t_row) {
+            t_row[q] = res_t;
+            d_row[q] = res_d;
+        }
+        if (c_t) {   // the best candidate before the ratio test (learned filter input)
+            c_t[q] = cand_t;
+            c_b12[2 * q] = cand_b1;
+            c_b12[2 * q + 1] = cand_b2;
+        }
     }
 }
 
@@ -533,11 +546,17 @@ int32_t run_match_bf(fsb_ctx* ctx, const uint8_t* d_a, int na, const uint8_t* d_
     return run_unique(ctx, t_row, d_row, na, nb, d_q, d_t, d_n, s);
 }
 
+int32_t run_unique_rows(fsb_ctx* ctx, const int32_t* t_row, const uint32_t* d_row, int na, int nb, int64_t* d_q,
+                        int64_t* d_t, int* d_n, cudaStream_t s) {
+    return run_unique(ctx, t_row, d_row, na, nb, d_q, d_t, d_n, s);
+}
+
 int32_t run_match_guided(fsb_ctx* ctx, const double* d_pred, const uint8_t* d_a, int na, const double* d_bxy,
                          const uint8_t* d_b, int nb, double wb, double hb, double radius, int kc, float ratio,
-                         int64_t* d_q, int64_t* d_t, int* d_n, cudaStream_t s) {
+                         int64_t* d_q, int64_t* d_t, int* d_n, cudaStream_t s, int32_t* c_t, float* c_b12) {
     if (na < 1 || nb < 1 || !(radius > 0.0)) {
-        FSB_CUDA(cudaMemsetAsync(d_n, 0, sizeof(int), s));
+        if (d_n) FSB_CUDA(cudaMemsetAsync(d_n, 0, sizeof(int), s));
+        if (c_t && na > 0) FSB_CUDA(cudaMemsetAsync(c_t, 0xff, (size_t)na * 4, s));
         return FSB_OK;
     }
     GridSpec gs;
@@ -576,7 +595,8 @@ int32_t run_match_guided(fsb_ctx* ctx, const double* d_pred, const uint8_t* d_a,
     k_grid_fill<<<blocks(nb, 256), 256, 0, s>>>(cell, nb, start, cursor, items);
     note_launch(5);
     k_guided<<<blocks(na, G_WARPS), G_WARPS * 32, 0, s>>>(d_pred, d_a, na, d_bxy, d_b, nb, nA, nB, gs, start, items,
-                                                          wb, hb, radius, kc, ratio, t_row, d_row, overflow);
+                                                          wb, hb, radius, kc, ratio, d_n ? t_row : nullptr,
+                                                          d_row, c_t, c_b12, overflow);
     FSB_CUDA(cudaGetLastError());
     int h_over = 0;
     FSB_CUDA(cudaMemcpyAsync(&h_over, overflow, sizeof(int), cudaMemcpyDeviceToHost, s));
@@ -585,6 +605,7 @@ int32_t run_match_guided(fsb_ctx* ctx, const double* d_pred, const uint8_t* d_a,
         set_error("more than %d B keypoints within the radius of one prediction (kc mode)", G_CAND);
         return FSB_ERR_OVERFLOW;
     }
+    if (!d_n) return FSB_OK;   // candidates only
     return run_unique(ctx, t_row, d_row, na, nb, d_q, d_t, d_n, s);
 }
 

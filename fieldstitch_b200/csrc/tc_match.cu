@@ -121,7 +121,6 @@ struct PackSeg {
     float* rowsc;   // E4M3 queries
     float* bmax;    // E4M3 targets
     int n, n_pad, role;   // role 0: query, 1: target
-    long long first;      // first packed row of this job in the launch
 };
 
 template <class T, class F>
@@ -139,16 +138,15 @@ __device__ __forceinline__ uint16_t bf16_bits(float x) {
     return (uint16_t)(__float_as_uint(x) >> 16);   // exact for the integers 0..255 and powers of two
 }
 
-// One warp per packed row of every job.
+// One warp per packed row; blockIdx.y is the job.
 template <int PREC>
-__global__ void k_tc_pack(const PackSeg* __restrict__ segs, int nseg, long long total) {
+__global__ void k_tc_pack(const PackSeg* __restrict__ segs) {
     constexpr int RB = TcTraits<PREC>::ROW_BYTES;
     constexpr int XB = RB - 32;   // byte offset of the norm slots
-    const long long gw = (long long)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    const PackSeg& S = segs[blockIdx.y];
+    const int row = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
     const int lane = threadIdx.x & 31;
-    if (gw >= total) return;
-    const PackSeg& S = segs[upper_index(segs, nseg, gw, [](const PackSeg& x) { return x.first; })];
-    const int row = (int)(gw - S.first);
+    if (row >= S.n_pad) return;
     uint8_t* blk = S.dst + (size_t)(row >> 7) * (128 * RB);
     const int r = row & 127;
     const bool live = row < S.n;
@@ -182,14 +180,16 @@ __global__ void k_tc_pack(const PackSeg* __restrict__ segs, int nseg, long long 
         }
         for (int sh = 16; sh; sh >>= 1) err2 += __shfl_xor_sync(0xffffffffu, err2, sh);
         *reinterpret_cast<uint32_t*>(blk + core_off(r, lane * 4, RB)) = packed;
-        if (lane == 0 && live) {
-            const float len = sqrtf((float)nrm) * (1.f + 1e-6f), elen = sqrtf(err2) * (1.f + 1e-6f);
-            if (S.role == 0) {
-                reinterpret_cast<float4*>(S.rowsc)[row] = make_float4(s, 1.f / s, len, elen);
-            } else {
-                atomicMax(reinterpret_cast<int*>(S.bmax), __float_as_int(len));
-                atomicMax(reinterpret_cast<int*>(S.bmax) + 1, __float_as_int(elen));
-            }
+        const float len = live ? sqrtf((float)nrm) * (1.f + 1e-6f) : 0.f;
+        const float elen = live ? sqrtf(err2) * (1.f + 1e-6f) : 0.f;
+        if (lane == 0 && live && S.role == 0)
+            reinterpret_cast<float4*>(S.rowsc)[row] = make_float4(s, 1.f / s, len, elen);
+        if (lane == 0 && live && S.role == 1) {
+            // the largest |b| and |beta| of the job (non-negative floats order like their bit
+            // patterns); the atomic is skipped once the running maximum is already larger
+            int* bm = reinterpret_cast<int*>(S.bmax);
+            if (__float_as_int(len) > *reinterpret_cast<volatile int*>(bm)) atomicMax(bm, __float_as_int(len));
+            if (__float_as_int(elen) > *reinterpret_cast<volatile int*>(bm + 1)) atomicMax(bm + 1, __float_as_int(elen));
         }
     }
     if (lane < 4) {   // the 16 norm slots (32 bytes), 8 bytes per lane
@@ -589,15 +589,14 @@ __device__ __forceinline__ void warp_top2(long long& k1, long long& d2) {
 constexpr long long NO_D = LLONG_MAX >> 32;   // "no distance" (above every uint8 distance)
 
 template <int K>
-__global__ void k_tc_finish(const TcPair* __restrict__ pairs, int n_pairs, int n_rows, const Cand* __restrict__ part,
+__global__ void k_tc_finish(const TcPair* __restrict__ pairs, const Cand* __restrict__ part,
                             float ratio, int prec, int32_t* __restrict__ t_row, uint32_t* __restrict__ d_row,
                             int32_t* __restrict__ flagged, int* __restrict__ n_flagged, float* __restrict__ err_stat) {
-    const int g = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    const TcPair& P = pairs[blockIdx.y];
+    const int q = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
     const int lane = threadIdx.x & 31;
-    if (g >= n_rows) return;
-    const TcPair& P = pairs[upper_index(pairs, n_pairs, g, [](const TcPair& x) { return (long long)x.row0; })];
-    const int q = g - P.row0;
     if (q >= P.na) return;
+    const int g = P.row0 + q;
     const int ne = P.splits * K;   // <= 32
     Cand e = lane < ne ? part[P.part0 + (size_t)q * ne + lane] : Cand{-INFINITY, -1};
     // the K best chunks over all splits (value descending, chunk ascending)
@@ -627,25 +626,39 @@ __global__ void k_tc_finish(const TcPair* __restrict__ pairs, int n_pairs, int n
         inv_s = rs.y;
         eps = (double)rs.z * be + (double)rs.w * bl + (double)rs.w * be + (double)rs.z * bl * (1.0 / 512.0) + 4.0;
     }
-    // exact distances of the re-ranked chunks: one column per lane
+    // exact distances of the re-ranked chunks: 8 lanes per target row (16 bytes each), so every
+    // load instruction reads 4 whole rows
     const int nre = prec == FSB_PREC_BF16 ? 1 : K;
-    const uint4* ar = reinterpret_cast<const uint4*>(P.a + (size_t)q * 128);
-    uint4 a[8];
-#pragma unroll
-    for (int i = 0; i < 8; ++i) a[i] = __ldg(ar + i);
+    const int seg = lane & 7, sub = lane >> 3;
+    const uint4 a4 = __ldg(reinterpret_cast<const uint4*>(P.a + (size_t)q * 128) + seg);
     long long k1 = LLONG_MAX, d2 = NO_D;
 #pragma unroll
     for (int k = 0; k < K; ++k) {
         if (k >= nre || sc[k] < 0) continue;
-        const int j = sc[k] * TC_CHUNK + lane;
-        if (j >= P.nb) continue;
-        const long long d = na + P.nB[j] - 2ll * exact_dot(a, P.b + (size_t)j * 128);
-        const long long key = (d << 32) | (unsigned)j;
-        if (key < k1) {
-            d2 = min(d2, k1 >> 32);
-            k1 = key;
-        } else {
-            d2 = min(d2, d);
+#pragma unroll
+        for (int i = 0; i < TC_CHUNK / 4; ++i) {
+            const int j = sc[k] * TC_CHUNK + 4 * i + sub;
+            uint32_t dot = 0;
+            if (j < P.nb) {
+                const uint4 b4 = __ldg(reinterpret_cast<const uint4*>(P.b + (size_t)j * 128) + seg);
+                dot = __dp4a(a4.x, b4.x, dot);
+                dot = __dp4a(a4.y, b4.y, dot);
+                dot = __dp4a(a4.z, b4.z, dot);
+                dot = __dp4a(a4.w, b4.w, dot);
+            }
+            dot += __shfl_xor_sync(0xffffffffu, dot, 1);
+            dot += __shfl_xor_sync(0xffffffffu, dot, 2);
+            dot += __shfl_xor_sync(0xffffffffu, dot, 4);
+            if (seg == 0 && j < P.nb) {
+                const long long d = na + P.nB[j] - 2ll * (long long)dot;
+                const long long key = (d << 32) | (unsigned)j;
+                if (key < k1) {
+                    d2 = min(d2, k1 >> 32);
+                    k1 = key;
+                } else {
+                    d2 = min(d2, d);
+                }
+            }
         }
     }
     warp_top2(k1, d2);
@@ -752,16 +765,14 @@ __global__ void k_tcu_fill(unsigned long long* __restrict__ key, long long n) {
     if (i < n) key[i] = ~0ull;
 }
 
-__global__ void k_tcu_keys(const TcPair* __restrict__ pairs, int n_pairs, int n_rows, const int32_t* __restrict__ t_row,
+__global__ void k_tcu_keys(const TcPair* __restrict__ pairs, const int32_t* __restrict__ t_row,
                            const uint32_t* __restrict__ d_row, unsigned long long* __restrict__ key) {
-    const int g = blockIdx.x * blockDim.x + threadIdx.x;
-    if (g >= n_rows) return;
-    const int t = t_row[g];
-    if (t < 0) return;
-    const TcPair& P = pairs[upper_index(pairs, n_pairs, g, [](const TcPair& x) { return (long long)x.row0; })];
-    const int q = g - P.row0;
+    const TcPair& P = pairs[blockIdx.y];
+    const int q = blockIdx.x * blockDim.x + threadIdx.x;
     if (q >= P.na) return;
-    atomicMin(key + P.key0 + t, ((unsigned long long)d_row[g] << 32) | (unsigned)q);
+    const int g = P.row0 + q;
+    const int t = t_row[g];
+    if (t >= 0) atomicMin(key + P.key0 + t, ((unsigned long long)d_row[g] << 32) | (unsigned)q);
 }
 
 __global__ void k_tcu_flags(const unsigned long long* __restrict__ key, long long n, int32_t* __restrict__ flag) {
@@ -769,14 +780,13 @@ __global__ void k_tcu_flags(const unsigned long long* __restrict__ key, long lon
     if (i <= n) flag[i] = i < n && key[i] != ~0ull;
 }
 
-__global__ void k_tcu_emit(const TcPair* __restrict__ pairs, int n_pairs, long long n,
-                           const unsigned long long* __restrict__ key, const int32_t* __restrict__ pos,
-                           int32_t* __restrict__ counts) {
-    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    const int p = upper_index(pairs, n_pairs, i, [](const TcPair& x) { return x.key0; });
+__global__ void k_tcu_emit(const TcPair* __restrict__ pairs, const unsigned long long* __restrict__ key,
+                           const int32_t* __restrict__ pos, int32_t* __restrict__ counts) {
+    const int p = blockIdx.y;
     const TcPair& P = pairs[p];
-    const long long local = i - P.key0;
+    const int local = blockIdx.x * blockDim.x + threadIdx.x;
+    if (local >= P.nb) return;
+    const long long i = P.key0 + local;
     if (local == P.nb - 1) counts[p] = pos[P.key0 + P.nb] - pos[P.key0];
     const unsigned long long k = key[i];
     if (k == ~0ull) return;
@@ -893,7 +903,7 @@ int32_t run_match_bf_tc(fsb_ctx* ctx, int n_pairs, const uint8_t* const* d_a, co
     std::vector<PackSeg> segs;
     segs.reserve(2 * n_pairs);
     size_t pa = 0, pb = 0, nn = 0, rr = 0;
-    long long first = 0;
+    int max_pad = 0, max_na = 0, max_nb = 0;
     for (int p = 0; p < n_pairs; ++p) {
         TcPair& P = hp[p];
         P.pa = pack + pa;
@@ -903,12 +913,13 @@ int32_t run_match_bf_tc(fsb_ctx* ctx, int n_pairs, const uint8_t* const* d_a, co
         P.rowsc = fp8 ? rowsc + 4 * rr : nullptr;
         P.bmax = bmax + 2 * p;
         const int pad_a = P.nrb * TC_ROWS, pad_b = P.ntiles * TC_N;
+        max_pad = std::max(max_pad, std::max(pad_a, pad_b));
+        max_na = std::max(max_na, P.na);
+        max_nb = std::max(max_nb, P.nb);
         segs.push_back(PackSeg{P.a, const_cast<uint8_t*>(P.pa), const_cast<int32_t*>(P.nA), const_cast<float*>(P.rowsc),
-                               nullptr, P.na, pad_a, 0, first});
-        first += pad_a;
+                               nullptr, P.na, pad_a, 0});
         segs.push_back(PackSeg{P.b, const_cast<uint8_t*>(P.pb), const_cast<int32_t*>(P.nB), nullptr,
-                               const_cast<float*>(P.bmax), P.nb, pad_b, 1, first});
-        first += pad_b;
+                               const_cast<float*>(P.bmax), P.nb, pad_b, 1});
         pa += (size_t)pad_a * RB;
         pb += (size_t)pad_b * RB;
         nn += (size_t)P.na + P.nb;
@@ -916,10 +927,11 @@ int32_t run_match_bf_tc(fsb_ctx* ctx, int n_pairs, const uint8_t* const* d_a, co
     }
     FSB_CUDA(cudaMemcpyAsync(d_pairs, hp.data(), (size_t)n_pairs * sizeof(TcPair), cudaMemcpyHostToDevice, s));
     FSB_CUDA(cudaMemcpyAsync(d_segs, segs.data(), segs.size() * sizeof(PackSeg), cudaMemcpyHostToDevice, s));
+    const dim3 pack_grid(nblk(max_pad, 8), (unsigned)segs.size());
     if (fp8)
-        k_tc_pack<FSB_PREC_FP8><<<nblk(first, 8), 256, 0, s>>>(d_segs, (int)segs.size(), first);
+        k_tc_pack<FSB_PREC_FP8><<<pack_grid, 256, 0, s>>>(d_segs);
     else
-        k_tc_pack<FSB_PREC_BF16><<<nblk(first, 8), 256, 0, s>>>(d_segs, (int)segs.size(), first);
+        k_tc_pack<FSB_PREC_BF16><<<pack_grid, 256, 0, s>>>(d_segs);
     note_launch(1);
     FSB_CUDA(cudaGetLastError());
     Cand* part = ctx->s_tc_part.as<Cand>();
@@ -929,12 +941,13 @@ int32_t run_match_bf_tc(fsb_ctx* ctx, int n_pairs, const uint8_t* const* d_a, co
     note_launch(1);
     ctx->stage_end(ST_TC_DENSE);
     float* err_stat = stats ? reinterpret_cast<float*>(small + 2) : nullptr;
+    const dim3 fin_grid(nblk(max_na, 8), (unsigned)n_pairs);
     if (fp8)
-        k_tc_finish<TcTraits<FSB_PREC_FP8>::TOPK><<<nblk(rows, 8), 256, 0, s>>>(
-            d_pairs, n_pairs, rows, part, ratio, precision, t_row, d_row, flagged, small + 1, err_stat);
+        k_tc_finish<TcTraits<FSB_PREC_FP8>::TOPK><<<fin_grid, 256, 0, s>>>(d_pairs, part, ratio, precision, t_row,
+                                                                           d_row, flagged, small + 1, err_stat);
     else
-        k_tc_finish<TcTraits<FSB_PREC_BF16>::TOPK><<<nblk(rows, 8), 256, 0, s>>>(
-            d_pairs, n_pairs, rows, part, ratio, precision, t_row, d_row, flagged, small + 1, err_stat);
+        k_tc_finish<TcTraits<FSB_PREC_BF16>::TOPK><<<fin_grid, 256, 0, s>>>(d_pairs, part, ratio, precision, t_row,
+                                                                            d_row, flagged, small + 1, err_stat);
     note_launch(1);
     FSB_CUDA(cudaGetLastError());
     int host_small[5] = {0, 0, 0, 0, 0};
@@ -952,10 +965,10 @@ int32_t run_match_bf_tc(fsb_ctx* ctx, int n_pairs, const uint8_t* const* d_a, co
     }
     // _unique of every pair
     k_tcu_fill<<<nblk(n_keys, 256), 256, 0, s>>>(keys, n_keys);
-    k_tcu_keys<<<nblk(rows, 256), 256, 0, s>>>(d_pairs, n_pairs, rows, t_row, d_row, keys);
+    k_tcu_keys<<<dim3(nblk(max_na, 256), (unsigned)n_pairs), 256, 0, s>>>(d_pairs, t_row, d_row, keys);
     k_tcu_flags<<<nblk(n_keys + 1, 256), 256, 0, s>>>(keys, n_keys, flag);
     FSB_CUDA(cub::DeviceScan::ExclusiveSum(scan_tmp, tb_scan, flag, pos, (int)(n_keys + 1), s));
-    k_tcu_emit<<<nblk(n_keys, 256), 256, 0, s>>>(d_pairs, n_pairs, n_keys, keys, pos, counts);
+    k_tcu_emit<<<dim3(nblk(max_nb, 256), (unsigned)n_pairs), 256, 0, s>>>(d_pairs, keys, pos, counts);
     note_launch(5);
     FSB_CUDA(cudaGetLastError());
     if (stats) {

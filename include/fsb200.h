@@ -130,6 +130,14 @@ int32_t fsb_sift_features(fsb_ctx* ctx, const uint8_t* img, int32_t h, int32_t w
 int32_t fsb_sift_features_d(fsb_ctx* ctx, const uint8_t* d_img, int32_t h, int32_t w, int32_t stride,
                             const fsb_sift_params* p, int32_t nfeat, float* d_xy, float* d_resp,
                             float* d_desc, uint8_t* d_rootsift, int32_t* n_out);
+/* fsb_sift_features_d plus the selected keypoints' size (float32, pixels of the input image),
+   angle (float32, degrees) and octave (int32, 0 = the 2x upsampled octave), each nullable: the
+   keypoint attributes of gsift.detect (app/planesite/gsift.py:435-477) for the selected set,
+   which the learned match filter's features use. */
+int32_t fsb_sift_features_ex_d(fsb_ctx* ctx, const uint8_t* d_img, int32_t h, int32_t w, int32_t stride,
+                               const fsb_sift_params* p, int32_t nfeat, float* d_xy, float* d_resp,
+                               float* d_desc, uint8_t* d_rootsift, float* d_size, float* d_angle,
+                               int32_t* d_octave, int32_t* n_out);
 /* Prior prediction: projects n float32 points (d_xy, n*2) through the homography hm9 (host,
    row-major 3x3) into float64 positions d_out (n*2), adding the float32 offsets d_offset (n*2,
    nullable) - e.g. a GNSS/gimbal prior and its error. Identity hm9 converts to float64. */
@@ -140,6 +148,13 @@ int32_t fsb_match_guided_d(fsb_ctx* ctx, const double* d_pred, const uint8_t* d_
                            const double* d_bxy, const uint8_t* d_b, int32_t nb, double w_b, double h_b,
                            double radius, int32_t kc, float ratio, int64_t* d_q, int64_t* d_t,
                            int32_t* n_out);
+/* The guided matcher's candidates before its ratio test: per query the best target within the
+   radius (kc rule as fsb_match_guided; -1 when there is none) in d_t1 (na int32) and its squared
+   distance b1 and the second-best b2 (+inf for a single candidate) in d_b12 (na x 2 float32).
+   The inputs of matching._guided's ratio test (app/planesite/matching.py:137-146). */
+int32_t fsb_match_guided_cand_d(fsb_ctx* ctx, const double* d_pred, const uint8_t* d_a, int32_t na,
+                                const double* d_bxy, const uint8_t* d_b, int32_t nb, double w_b, double h_b,
+                                double radius, int32_t kc, int32_t* d_t1, float* d_b12);
 /* fsb_match_bf with every array in device memory; d_q, d_t capacity na. */
 int32_t fsb_match_bf_d(fsb_ctx* ctx, const uint8_t* d_a, int32_t na, const uint8_t* d_b, int32_t nb,
                        float ratio, int32_t precision, int64_t* d_q, int64_t* d_t, int32_t* n_out);
@@ -160,6 +175,43 @@ int32_t fsb_match_bf_batch_d(fsb_ctx* ctx, int32_t n_pairs, const uint8_t* const
    between the approximate and the exact best squared distance of a row. Any pointer may be null. */
 int32_t fsb_match_tc_stats(fsb_ctx* ctx, int64_t* rows, int64_t* fallback_rows, double* max_abs_err,
                            double* mean_abs_err);
+
+/* ---- learned match filter (no counterpart in the reference: it replaces the ratio test of
+   matching._guided, app/planesite/matching.py:142-146, by an 8-64-64-1 MLP whose labels come
+   from the plain pipeline's own RANSAC verification, matching.py:205-233) --------------------
+   Parameters: one float32 device vector of fsb_mlp_param_count() values: W1[64][8], b1[64],
+   W2[64][64], b2[64], w3[64], b3 (the first fsb_mlp_trainable_count() values, trained), then
+   the input normalisation mu[8], sigma[8]. Features (n x 8 float32) of a query's best candidate:
+   ratio sqrt(b1)/sqrt(b2) (0 for a single candidate), sqrt(b1)/512, log2(size_b/size_a), signed
+   angle difference/180, |pred_a - xy_b|/radius, response_a, response_b, octave_a; queries without
+   a candidate get zeros. */
+int32_t fsb_mlp_param_count(void);
+int32_t fsb_mlp_trainable_count(void);
+int32_t fsb_mlp_features_d(fsb_ctx* ctx, int32_t n, const int32_t* d_t1, const float* d_b12,
+                           const double* d_pred, const float* d_xy_b, const float* d_size_a,
+                           const float* d_angle_a, const float* d_resp_a, const int32_t* d_oct_a,
+                           const float* d_size_b, const float* d_angle_b, const float* d_resp_b,
+                           float radius, float* d_feat);
+/* Gradient (d_grad, trainable count) and mean binary cross-entropy (*loss, nullable) of the
+   network over n labelled samples (d_label: 0 or 1). */
+int32_t fsb_mlp_grad_d(fsb_ctx* ctx, const float* d_params, int32_t n, const float* d_feat,
+                       const float* d_label, float* d_grad, double* loss);
+/* Mini-batch Adam (beta 0.9 / 0.999) on the GPU: each epoch shuffles the samples on the device
+   (seeded) and takes floor(n / batch) steps; the epoch runs as one captured CUDA graph. d_m, d_v:
+   Adam moments (trainable count each, reset here). losses (host, nullable) receives the mean
+   loss of each of the `epochs` epochs. */
+int32_t fsb_mlp_train_d(fsb_ctx* ctx, float* d_params, float* d_m, float* d_v, int32_t n,
+                        const float* d_feat, const float* d_label, int32_t epochs, int32_t batch,
+                        float lr, uint32_t seed, double* losses);
+/* Probabilities (n float32); bf16 != 0: BF16 weights, inputs and hidden activations with FP32
+   accumulation. */
+int32_t fsb_mlp_infer_d(fsb_ctx* ctx, const float* d_params, int32_t n, const float* d_feat, int32_t bf16,
+                        float* d_prob);
+/* Accept the candidates (d_t1, d_b12 from fsb_match_guided_cand_d) whose probability exceeds
+   threshold, or - d_prob null, the fallback - those passing the ratio test of matching._guided;
+   then the one-to-one filter of _unique. Writes *n_out pairs ordered by target (capacity na). */
+int32_t fsb_mlp_filter_d(fsb_ctx* ctx, int32_t na, const int32_t* d_t1, const float* d_b12, const float* d_prob,
+                         float threshold, float ratio, int32_t nb, int64_t* d_q, int64_t* d_t, int32_t* n_out);
 
 /* Allocation-free variant of fsb_match_bf_d (FP32 distances), for callers that cannot call
    cudaMalloc: processes that reserve their whole device-memory budget up front, host frameworks
