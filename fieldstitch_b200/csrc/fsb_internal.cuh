@@ -163,6 +163,8 @@ int32_t run_pyramid(Workspace& ws, const uint8_t* d_img, int img_stride, bool ex
 int32_t upload_octave_taps(const float* taps, int stride, const int* counts);
 int32_t launch_octave_fused(const float* L0, int R, int C, float* dog, float* mag, float* ang, float* down,
                             int down_cols, cudaStream_t s);
+int32_t launch_layer_fast(int layer, const float* src, int R, int C, float* dst, float* dog, float* mag, float* ang,
+                          float* down, int down_cols, cudaStream_t s);
 
 // ---------------------------------------------------------------- detect.cu / describe.cu
 int32_t run_orient(const Workspace& ws, const Refined* ref, const uint32_t* d_nref, uint32_t n_ref_host,

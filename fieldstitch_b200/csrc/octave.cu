@@ -305,6 +305,160 @@ __global__ void __launch_bounds__(NT, 2) k_octave(Args a) {
     cp_wait_all();
 }
 
+// ------------------------------------------------------------------------------------------------
+// Per-layer tiled kernel (float32 path): L_I of one octave from L_{I-1}, 128 x 32 outputs per CTA.
+// The same pair blurs and gradient as the fused kernel (bit-identical results); the input tile
+// (16 columns and RAD(I) rows of reflect-101 halo) arrives by 16-byte cp.async, the vertical
+// pass keeps an 8-row sliding window of column pairs in registers, the horizontal pass reads the
+// row-pair interleaved vertical outputs. No ring buffers, so occupancy is 3-4 CTAs per SM.
+constexpr int LX = 128, LY = 32, LNT = 256;
+constexpr int LIN_W = LX + 32;   // input tile pitch (floats)
+constexpr int LT2_W = LX + 32;   // row-pair tile pitch (float2)
+
+struct LayerArgs {
+    const float* src;   // L_{I-1}, R x C
+    int R, C;
+    float* dst;         // L_I or null
+    float* dog;         // L_I - L_{I-1}
+    float* mag;         // gradient of L_{I-1} or null
+    float* ang;
+    float* down;        // L_{I-1}[::2, ::2] or null
+    int down_cols;
+};
+
+template <int I>
+constexpr int layer_smem() {
+    return (LY + 2 * RAD(I)) * LIN_W * 4 + (LY / 2) * LT2_W * 8;
+}
+
+template <int I>
+__global__ void __launch_bounds__(LNT) k_layer(LayerArgs a) {
+    constexpr int r = RAD(I), d = r & 1;
+    constexpr int IH = LY + 2 * r;
+    constexpr int NPAIR = (LX + 2 * r + 2 * d) / 2;
+    extern __shared__ __align__(16) float sm[];
+    float* s_in = sm;
+    float2* t2 = reinterpret_cast<float2*>(sm + IH * LIN_W);
+    const int tid = threadIdx.x;
+    const int x0 = blockIdx.x * LX, y0 = blockIdx.y * LY;
+    // input rows y0 - r .. y0 + LY + r - 1, columns x0 - 16 .. x0 + LX + 15 (reflect-101 outside)
+    if ((a.C & 3) == 0 && x0 >= 16 && x0 + LX + 16 <= a.C) {
+        for (int i = tid; i < IH * (LIN_W / 4); i += LNT) {
+            const int row = i / (LIN_W / 4), q = i - row * (LIN_W / 4);
+            const float* g = a.src + (size_t)mir(y0 - r + row, a.R) * a.C + (x0 - 16 + 4 * q);
+            cp_async16(s_in + row * LIN_W + 4 * q, g);
+        }
+    } else {
+        for (int i = tid; i < IH * LIN_W; i += LNT) {
+            const int row = i / LIN_W, col = i - row * LIN_W;
+            const float* g = a.src + (size_t)mir(y0 - r + row, a.R) * a.C + mir(x0 - 16 + col, a.C);
+            cp_async4(s_in + row * LIN_W + col, g);
+        }
+    }
+    cp_commit();
+    cp_wait_all();
+    __syncthreads();
+    // vertical pass: column pair cp (V columns 2cp, 2cp+1 = image columns x0 - r - d + 2cp ..),
+    // output rows 8g .. 8g + 7; stored row-pair interleaved at t2 index (V column + d)
+    for (int it = tid; it < NPAIR * (LY / 8); it += LNT) {
+        const int cp = it % NPAIR, g = it / NPAIR;
+        const float* base = s_in + (8 * g) * LIN_W + (16 - r - d + 2 * cp);
+        float2 x[8 + 2 * r];
+#pragma unroll
+        for (int k = 0; k < 8 + 2 * r; ++k) x[k] = *reinterpret_cast<const float2*>(base + k * LIN_W);
+#pragma unroll
+        for (int sp = 0; sp < 4; ++sp) {
+            const float2 o0 = blur_pairs<I>(x + 2 * sp), o1 = blur_pairs<I>(x + 2 * sp + 1);
+            float2* dst = t2 + (4 * g + sp) * LT2_W + 2 * cp + d;
+            dst[0] = make_float2(o0.x, o1.x);
+            dst[1] = make_float2(o0.y, o1.y);
+        }
+    }
+    __syncthreads();
+    // horizontal pass: row pair p, output columns c .. c+3 (t2 indices c + 2d .. c + 2d + 3 + 2r)
+    for (int it = tid; it < (LY / 2) * (LX / 4); it += LNT) {
+        const int p = it / (LX / 4), c = 4 * (it - p * (LX / 4));
+        const int y = y0 + 2 * p, x = x0 + c;
+        if (y >= a.R || x >= a.C) continue;
+        const float4* src = reinterpret_cast<const float4*>(t2 + p * LT2_W + c + 2 * d);
+        float2 yv[4 + 2 * r];
+#pragma unroll
+        for (int k = 0; k < 2 + r; ++k) {
+            const float4 v = src[k];
+            yv[2 * k] = make_float2(v.x, v.y);
+            yv[2 * k + 1] = make_float2(v.z, v.w);
+        }
+        float2 o[4];
+#pragma unroll
+        for (int cc = 0; cc < 4; ++cc) o[cc] = blur_pairs<I>(yv + cc);   // (row y, row y+1) at column x+cc
+        const bool vec = (a.C & 3) == 0 && x + 4 <= a.C;
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            const int yy = y + h;
+            if (yy >= a.R) break;
+            const float* ctr = s_in + (2 * p + h + r) * LIN_W + 16 + c;   // L_{I-1} at (yy, x)
+            const float4 pv = *reinterpret_cast<const float4*>(ctr);
+            const float lv[4] = {h ? o[0].y : o[0].x, h ? o[1].y : o[1].x, h ? o[2].y : o[2].x, h ? o[3].y : o[3].x};
+            const float pr[4] = {pv.x, pv.y, pv.z, pv.w};
+            float dg[4];
+#pragma unroll
+            for (int k = 0; k < 4; ++k) dg[k] = lv[k] - pr[k];
+            const size_t at = (size_t)yy * a.C + x;
+            if (vec) {
+                *reinterpret_cast<float4*>(a.dog + at) = make_float4(dg[0], dg[1], dg[2], dg[3]);
+                if (a.dst) *reinterpret_cast<float4*>(a.dst + at) = make_float4(lv[0], lv[1], lv[2], lv[3]);
+            } else {
+                for (int k = 0; k < 4 && x + k < a.C; ++k) {
+                    a.dog[at + k] = dg[k];
+                    if (a.dst) a.dst[at + k] = lv[k];
+                }
+            }
+            if (a.mag) {
+                float mg[4], an[4];
+#pragma unroll
+                for (int k = 0; k < 4; ++k) {
+                    float dx = 0.f, dy = 0.f;
+                    if (yy > 0 && yy < a.R - 1 && x + k > 0 && x + k < a.C - 1) {
+                        dx = __fsub_rn(ctr[k + 1], ctr[k - 1]);
+                        dy = __fsub_rn(ctr[k - LIN_W], ctr[k + LIN_W]);
+                    }
+                    fast_grad(dx, dy, mg[k], an[k]);
+                }
+                if (vec) {
+                    *reinterpret_cast<float4*>(a.mag + at) = make_float4(mg[0], mg[1], mg[2], mg[3]);
+                    *reinterpret_cast<float4*>(a.ang + at) = make_float4(an[0], an[1], an[2], an[3]);
+                } else {
+                    for (int k = 0; k < 4 && x + k < a.C; ++k) {
+                        a.mag[at + k] = mg[k];
+                        a.ang[at + k] = an[k];
+                    }
+                }
+            }
+            if (a.down && !(yy & 1)) {
+                float* o2 = a.down + (size_t)(yy >> 1) * a.down_cols + (x >> 1);
+                o2[0] = pr[0];
+                if (x + 2 < a.C) o2[1] = pr[2];
+            }
+        }
+    }
+}
+
+template <int I>
+int32_t launch_layer_t(const LayerArgs& a, cudaStream_t s) {
+    static bool attr[64] = {};
+    int dev = 0;
+    FSB_CUDA(cudaGetDevice(&dev));
+    if (dev < 64 && !attr[dev]) {
+        FSB_CUDA(cudaFuncSetAttribute(k_layer<I>, cudaFuncAttributeMaxDynamicSharedMemorySize, layer_smem<I>()));
+        attr[dev] = true;
+    }
+    dim3 grid((a.C + LX - 1) / LX, (a.R + LY - 1) / LY);
+    k_layer<I><<<grid, LNT, layer_smem<I>(), s>>>(a);
+    note_launch();
+    FSB_CUDA(cudaGetLastError());
+    return FSB_OK;
+}
+
 }  // namespace
 
 int32_t launch_octave_fused(const float* L0, int R, int C, float* dog, float* mag, float* ang, float* down,
@@ -339,6 +493,33 @@ int32_t launch_octave_fused(const float* L0, int R, int C, float* dog, float* ma
     note_launch();
     FSB_CUDA(cudaGetLastError());
     return FSB_OK;
+}
+
+}  // namespace fsb
+
+namespace fsb {
+
+// One layer of the float32 pyramid by the tiled per-layer kernel: L_layer from src (R x C).
+int32_t launch_layer_fast(int layer, const float* src, int R, int C, float* dst, float* dog, float* mag, float* ang,
+                          float* down, int down_cols, cudaStream_t s) {
+    LayerArgs a;
+    a.src = src;
+    a.R = R;
+    a.C = C;
+    a.dst = dst;
+    a.dog = dog;
+    a.mag = mag;
+    a.ang = ang;
+    a.down = down;
+    a.down_cols = down_cols;
+    switch (layer) {
+        case 1: return launch_layer_t<1>(a, s);
+        case 2: return launch_layer_t<2>(a, s);
+        case 3: return launch_layer_t<3>(a, s);
+        case 4: return launch_layer_t<4>(a, s);
+        case 5: return launch_layer_t<5>(a, s);
+        default: set_error("layer %d out of range", layer); return FSB_ERR_ARG;
+    }
 }
 
 }  // namespace fsb

@@ -15,6 +15,9 @@
 // from the tile already in shared memory, so none of those needs a separate pass over HBM.
 #include <cmath>
 
+#include <cstdlib>
+#include <cstring>
+
 #include "fsb_internal.cuh"
 
 namespace fsb {
@@ -202,9 +205,17 @@ void launch(bool exact, const BlurArgs& a, cudaStream_t s) {
 
 }  // namespace
 
-// octaves at least this wide go through the fused kernel (octave.cu); narrower ones have too
-// little work per row to amortise its 84-row pipeline fill and use the per-layer kernels
+// Float32 octave engine: the tiled per-layer kernels (k_layer, octave.cu) by default; the fused
+// streaming kernel (k_octave) for octaves at least kFusedMinCols wide when FSB_PYRAMID=fused.
 static const int kFusedMinCols = 2000;
+
+static bool use_fused_octaves() {
+    static const bool on = [] {
+        const char* e = std::getenv("FSB_PYRAMID");
+        return e && std::strcmp(e, "fused") == 0;
+    }();
+    return on;
+}
 
 int32_t run_pyramid(Workspace& ws, const uint8_t* d_img, int img_stride, bool exact, cudaStream_t s) {
     const Geometry& g = ws.g;
@@ -230,12 +241,24 @@ int32_t run_pyramid(Workspace& ws, const uint8_t* d_img, int img_stride, bool ex
         float* other[2];
         for (int k = 0, n = 0; k < 3; ++k)
             if (P[k] != cur) other[n++] = P[k];
-        if (!exact && g.C[o] >= kFusedMinCols) {
+        if (!exact && use_fused_octaves() && g.C[o] >= kFusedMinCols) {
             // fused octave: reads cur, writes the next base into another plane
             float* down = o + 1 < g.n_oct ? other[0] : nullptr;
             FSB_TRY(launch_octave_fused(cur, g.R[o], g.C[o], dog, mag, ang, down, o + 1 < g.n_oct ? g.C[o + 1] : 0, s));
             cur = other[0];
             continue;
+        }
+        if (!exact) {
+            const int R = g.R[o], C = g.C[o];
+            float* down = o + 1 < g.n_oct ? cur : nullptr;
+            const int dc = o + 1 < g.n_oct ? g.C[o + 1] : 0;
+            FSB_TRY(launch_layer_fast(1, cur, R, C, other[0], dog, nullptr, nullptr, nullptr, 0, s));
+            FSB_TRY(launch_layer_fast(2, other[0], R, C, other[1], dog + RC, mag, ang, nullptr, 0, s));
+            FSB_TRY(launch_layer_fast(3, other[1], R, C, other[0], dog + 2 * RC, mag + RC, ang + RC, nullptr, 0, s));
+            FSB_TRY(launch_layer_fast(4, other[0], R, C, other[1], dog + 3 * RC, mag + 2 * RC, ang + 2 * RC, down, dc,
+                                      s));
+            FSB_TRY(launch_layer_fast(5, other[1], R, C, nullptr, dog + 4 * RC, nullptr, nullptr, nullptr, 0, s));
+            continue;   // the next base is in `cur` (the dead L0 plane)
         }
         BlurArgs b{};
         b.rows = g.R[o];
