@@ -326,10 +326,12 @@ int32_t run_mlp_grad(fsb_ctx* ctx, const float* prm, int n, const float* feat, c
                      double* loss, cudaStream_t s) {
     FSB_TRY(configure_fwd_bwd());
     const int nb = (int)nblk(n, MB);
-    FSB_TRY(ctx->s_misc.ensure((size_t)nb * N_TRAIN * 4 + (size_t)n * 4 + 64));
-    float* part = ctx->s_misc.as<float>();
-    int32_t* idx = reinterpret_cast<int32_t*>(part + (size_t)nb * N_TRAIN);
-    double* dl = reinterpret_cast<double*>(idx + ((n + 1) & ~1));
+    auto al = [](size_t x) { return (x + 255) & ~size_t(255); };
+    FSB_TRY(ctx->s_misc.ensure(al((size_t)nb * N_TRAIN * 4) + al((size_t)n * 4) + al(64)));
+    uint8_t* base = ctx->s_misc.as<uint8_t>();
+    float* part = reinterpret_cast<float*>(base);
+    int32_t* idx = reinterpret_cast<int32_t*>(base + al((size_t)nb * N_TRAIN * 4));
+    double* dl = reinterpret_cast<double*>(base + al((size_t)nb * N_TRAIN * 4) + al((size_t)n * 4));
     std::vector<int32_t> iota(n);
     for (int i = 0; i < n; ++i) iota[i] = i;
     FSB_CUDA(cudaMemcpyAsync(idx, iota.data(), (size_t)n * 4, cudaMemcpyHostToDevice, s));
@@ -359,7 +361,8 @@ int32_t run_mlp_train(fsb_ctx* ctx, float* prm, float* m, float* v, int n, const
     size_t tb = 0;
     cub::DeviceRadixSort::SortPairs(nullptr, tb, (uint32_t*)nullptr, (uint32_t*)nullptr, (int32_t*)nullptr,
                                     (int32_t*)nullptr, n, 0, 32, s);
-    const size_t need = (size_t)nb * N_TRAIN * 4 + (size_t)n * 16 + tb + 1024;
+    auto al = [](size_t x) { return (x + 255) & ~size_t(255); };
+    const size_t need = al((size_t)nb * N_TRAIN * 4) + 4 * al((size_t)n * 4) + al(tb) + 2 * al(64);
     FSB_TRY(ctx->s_misc.ensure(need));
     uint8_t* cur = ctx->s_misc.as<uint8_t>();
     auto take = [&](size_t bytes) {
