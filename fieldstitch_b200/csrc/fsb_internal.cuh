@@ -165,6 +165,7 @@ int32_t launch_octave_fused(const float* L0, int R, int C, float* dog, float* ma
                             int down_cols, cudaStream_t s);
 int32_t launch_layer_fast(int layer, const float* src, int R, int C, float* dst, float* dog, float* mag, float* ang,
                           float* down, int down_cols, cudaStream_t s);
+int32_t launch_base_fast(const uint8_t* img, int stride, int ih, int iw, float* dst, cudaStream_t s);
 
 // ---------------------------------------------------------------- detect.cu / describe.cu
 int32_t run_orient(const Workspace& ws, const Refined* ref, const uint32_t* d_nref, uint32_t n_ref_host,

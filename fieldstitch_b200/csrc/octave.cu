@@ -107,21 +107,22 @@ __device__ __forceinline__ void load_rows(float* ring0, const Args& a, int x0, i
 // sum_j w_j x[r + j] over j = -r..r for two lanes at once, with symmetric pairing
 // w_0 x_0 + sum_j w_j (x_-j + x_j); two accumulation chains (odd / even j) for latency hiding.
 // The pair sums commute, so a mirrored window gives a bit-identical result.
-template <int I>
-__device__ __forceinline__ float2 blur_pairs(const float2* x) {
-    constexpr int r = RAD(I);
-    float2 a = __fmul2_rn(x[r], c_tap2[I][0]);
+template <int TS, int r>
+__device__ __forceinline__ float2 blur_pairs_t(const float2* x) {
+    float2 a = __fmul2_rn(x[r], c_tap2[TS][0]);
     float2 b = make_float2(0.f, 0.f);
 #pragma unroll
     for (int j = r; j >= 1; --j) {
         const float2 p = __fadd2_rn(x[r - j], x[r + j]);
         if (j & 1)
-            b = __ffma2_rn(p, c_tap2[I][j], b);
+            b = __ffma2_rn(p, c_tap2[TS][j], b);
         else
-            a = __ffma2_rn(p, c_tap2[I][j], a);
+            a = __ffma2_rn(p, c_tap2[TS][j], a);
     }
     return __fadd2_rn(a, b);
 }
+template <int I>
+__device__ __forceinline__ float2 blur_pairs(const float2* x) { return blur_pairs_t<I, RAD(I)>(x); }
 
 // rows yb, yb+1 (row pair rp) .. of L_I from L_{I-1} rows in `ring`; thread = (column pair, row pair)
 template <int I>
@@ -306,17 +307,25 @@ __global__ void __launch_bounds__(NT, 2) k_octave(Args a) {
 }
 
 // ------------------------------------------------------------------------------------------------
-// Per-layer tiled kernel (float32 path): L_I of one octave from L_{I-1}, 128 x 32 outputs per CTA.
-// The same pair blurs and gradient as the fused kernel (bit-identical results); the input tile
-// (16 columns and RAD(I) rows of reflect-101 halo) arrives by 16-byte cp.async, the vertical
-// pass keeps an 8-row sliding window of column pairs in registers, the horizontal pass reads the
-// row-pair interleaved vertical outputs. No ring buffers, so occupancy is 3-4 CTAs per SM.
+// Per-layer tiled kernels (float32 path), 128 x 32 outputs per CTA:
+//   k_layer<I, RAD(I), false>  L_I of one octave from L_{I-1}: the same pair blurs and gradient as
+//                              the fused kernel (bit-identical results), DoG, gradient of L_{I-1},
+//                              L_{I-1}[::2, ::2]
+//   k_layer<0, 5, true>        the octave-0 base: the 2x bilinear upsample of the uint8 image
+//                              (the reference's float32 rounding, gsift.py:90-102) computed while the
+//                              tile loads, from per-row / per-column source tables, blurred with tap
+//                              set 0
+// The input tile (16 columns and r rows of reflect-101 halo) arrives by 16-byte cp.async, the
+// vertical pass keeps an 8-row sliding window of column pairs in registers, the horizontal pass
+// reads the row-pair interleaved vertical outputs. No ring buffers: 3-4 CTAs per SM.
 constexpr int LX = 128, LY = 32, LNT = 256;
 constexpr int LIN_W = LX + 32;   // input tile pitch (floats)
 constexpr int LT2_W = LX + 32;   // row-pair tile pitch (float2)
 
 struct LayerArgs {
     const float* src;   // L_{I-1}, R x C
+    const uint8_t* img; // base: uint8 image ih x iw, row pitch img_stride
+    int img_stride, ih, iw;
     int R, C;
     float* dst;         // L_I or null
     float* dog;         // L_I - L_{I-1}
@@ -326,14 +335,14 @@ struct LayerArgs {
     int down_cols;
 };
 
-template <int I>
+template <int r>
 constexpr int layer_smem() {
-    return (LY + 2 * RAD(I)) * LIN_W * 4 + (LY / 2) * LT2_W * 8;
+    return (LY + 2 * r) * LIN_W * 4 + (LY / 2) * LT2_W * 8;
 }
 
-template <int I>
+template <int TS, int r, bool BASE>
 __global__ void __launch_bounds__(LNT) k_layer(LayerArgs a) {
-    constexpr int r = RAD(I), d = r & 1;
+    constexpr int d = r & 1;
     constexpr int IH = LY + 2 * r;
     constexpr int NPAIR = (LX + 2 * r + 2 * d) / 2;
     extern __shared__ __align__(16) float sm[];
@@ -342,7 +351,38 @@ __global__ void __launch_bounds__(LNT) k_layer(LayerArgs a) {
     const int tid = threadIdx.x;
     const int x0 = blockIdx.x * LX, y0 = blockIdx.y * LY;
     // input rows y0 - r .. y0 + LY + r - 1, columns x0 - 16 .. x0 + LX + 15 (reflect-101 outside)
-    if ((a.C & 3) == 0 && x0 >= 16 && x0 + LX + 16 <= a.C) {
+    if (BASE) {
+        // source rows / columns of every tile row / column (reflect-101 on the upsampled grid),
+        // kept in the row-pair area until the vertical pass needs it
+        int* rtab = reinterpret_cast<int*>(t2);
+        int* ctab = rtab + 2 * IH;
+        for (int i = tid; i < IH + LIN_W; i += LNT) {
+            if (i < IH) {
+                const int Y = mir(y0 - r + i, a.R), iy = Y >> 1;
+                const int ny = (Y & 1) ? min(iy + 1, a.ih - 1) : max(iy - 1, 0);
+                rtab[2 * i] = iy * a.img_stride;
+                rtab[2 * i + 1] = ny * a.img_stride;
+            } else {
+                const int c = i - IH, X = mir(x0 - 16 + c, a.C), ix = X >> 1;
+                ctab[2 * c] = ix;
+                ctab[2 * c + 1] = (X & 1) ? min(ix + 1, a.iw - 1) : max(ix - 1, 0);
+            }
+        }
+        __syncthreads();
+        const float sc = (float)(1.0 / 255.0);
+#pragma unroll 4
+        for (int i = tid; i < IH * LIN_W; i += LNT) {
+            const int row = i / LIN_W, col = i - row * LIN_W;
+            const uint8_t* r0 = a.img + rtab[2 * row];
+            const uint8_t* r1 = a.img + rtab[2 * row + 1];
+            const int ix = ctab[2 * col], nx = ctab[2 * col + 1];
+            const float p00 = __fmul_rn((float)__ldg(r0 + ix), sc), p10 = __fmul_rn((float)__ldg(r1 + ix), sc);
+            const float p01 = __fmul_rn((float)__ldg(r0 + nx), sc), p11 = __fmul_rn((float)__ldg(r1 + nx), sc);
+            const float vc = __fadd_rn(__fmul_rn(0.75f, p00), __fmul_rn(0.25f, p10));
+            const float vn = __fadd_rn(__fmul_rn(0.75f, p01), __fmul_rn(0.25f, p11));
+            s_in[row * LIN_W + col] = __fadd_rn(__fmul_rn(0.75f, vc), __fmul_rn(0.25f, vn));
+        }
+    } else if ((a.C & 3) == 0 && x0 >= 16 && x0 + LX + 16 <= a.C) {
         for (int i = tid; i < IH * (LIN_W / 4); i += LNT) {
             const int row = i / (LIN_W / 4), q = i - row * (LIN_W / 4);
             const float* g = a.src + (size_t)mir(y0 - r + row, a.R) * a.C + (x0 - 16 + 4 * q);
@@ -368,7 +408,7 @@ __global__ void __launch_bounds__(LNT) k_layer(LayerArgs a) {
         for (int k = 0; k < 8 + 2 * r; ++k) x[k] = *reinterpret_cast<const float2*>(base + k * LIN_W);
 #pragma unroll
         for (int sp = 0; sp < 4; ++sp) {
-            const float2 o0 = blur_pairs<I>(x + 2 * sp), o1 = blur_pairs<I>(x + 2 * sp + 1);
+            const float2 o0 = blur_pairs_t<TS, r>(x + 2 * sp), o1 = blur_pairs_t<TS, r>(x + 2 * sp + 1);
             float2* dst = t2 + (4 * g + sp) * LT2_W + 2 * cp + d;
             dst[0] = make_float2(o0.x, o1.x);
             dst[1] = make_float2(o0.y, o1.y);
@@ -390,15 +430,24 @@ __global__ void __launch_bounds__(LNT) k_layer(LayerArgs a) {
         }
         float2 o[4];
 #pragma unroll
-        for (int cc = 0; cc < 4; ++cc) o[cc] = blur_pairs<I>(yv + cc);   // (row y, row y+1) at column x+cc
+        for (int cc = 0; cc < 4; ++cc) o[cc] = blur_pairs_t<TS, r>(yv + cc);   // (row y, row y+1) at column x+cc
         const bool vec = (a.C & 3) == 0 && x + 4 <= a.C;
 #pragma unroll
         for (int h = 0; h < 2; ++h) {
             const int yy = y + h;
             if (yy >= a.R) break;
+            const float lv[4] = {h ? o[0].y : o[0].x, h ? o[1].y : o[1].x, h ? o[2].y : o[2].x, h ? o[3].y : o[3].x};
+            if (BASE) {
+                const size_t at = (size_t)yy * a.C + x;
+                if (vec) {
+                    *reinterpret_cast<float4*>(a.dst + at) = make_float4(lv[0], lv[1], lv[2], lv[3]);
+                } else {
+                    for (int k = 0; k < 4 && x + k < a.C; ++k) a.dst[at + k] = lv[k];
+                }
+                continue;
+            }
             const float* ctr = s_in + (2 * p + h + r) * LIN_W + 16 + c;   // L_{I-1} at (yy, x)
             const float4 pv = *reinterpret_cast<const float4*>(ctr);
-            const float lv[4] = {h ? o[0].y : o[0].x, h ? o[1].y : o[1].x, h ? o[2].y : o[2].x, h ? o[3].y : o[3].x};
             const float pr[4] = {pv.x, pv.y, pv.z, pv.w};
             float dg[4];
 #pragma unroll
@@ -443,17 +492,18 @@ __global__ void __launch_bounds__(LNT) k_layer(LayerArgs a) {
     }
 }
 
-template <int I>
+template <int TS, int r, bool BASE>
 int32_t launch_layer_t(const LayerArgs& a, cudaStream_t s) {
     static bool attr[64] = {};
     int dev = 0;
     FSB_CUDA(cudaGetDevice(&dev));
     if (dev < 64 && !attr[dev]) {
-        FSB_CUDA(cudaFuncSetAttribute(k_layer<I>, cudaFuncAttributeMaxDynamicSharedMemorySize, layer_smem<I>()));
+        FSB_CUDA(cudaFuncSetAttribute(k_layer<TS, r, BASE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      layer_smem<r>()));
         attr[dev] = true;
     }
     dim3 grid((a.C + LX - 1) / LX, (a.R + LY - 1) / LY);
-    k_layer<I><<<grid, LNT, layer_smem<I>(), s>>>(a);
+    k_layer<TS, r, BASE><<<grid, LNT, layer_smem<r>(), s>>>(a);
     note_launch();
     FSB_CUDA(cudaGetLastError());
     return FSB_OK;
@@ -502,7 +552,7 @@ namespace fsb {
 // One layer of the float32 pyramid by the tiled per-layer kernel: L_layer from src (R x C).
 int32_t launch_layer_fast(int layer, const float* src, int R, int C, float* dst, float* dog, float* mag, float* ang,
                           float* down, int down_cols, cudaStream_t s) {
-    LayerArgs a;
+    LayerArgs a{};
     a.src = src;
     a.R = R;
     a.C = C;
@@ -513,13 +563,27 @@ int32_t launch_layer_fast(int layer, const float* src, int R, int C, float* dst,
     a.down = down;
     a.down_cols = down_cols;
     switch (layer) {
-        case 1: return launch_layer_t<1>(a, s);
-        case 2: return launch_layer_t<2>(a, s);
-        case 3: return launch_layer_t<3>(a, s);
-        case 4: return launch_layer_t<4>(a, s);
-        case 5: return launch_layer_t<5>(a, s);
+        case 1: return launch_layer_t<1, 5, false>(a, s);
+        case 2: return launch_layer_t<2, 6, false>(a, s);
+        case 3: return launch_layer_t<3, 8, false>(a, s);
+        case 4: return launch_layer_t<4, 10, false>(a, s);
+        case 5: return launch_layer_t<5, 13, false>(a, s);
         default: set_error("layer %d out of range", layer); return FSB_ERR_ARG;
     }
+}
+
+
+// The float32 octave-0 base: blur (tap set 0, radius 5) of the 2x upsampled uint8 image.
+int32_t launch_base_fast(const uint8_t* img, int stride, int ih, int iw, float* dst, cudaStream_t s) {
+    LayerArgs a{};
+    a.img = img;
+    a.img_stride = stride;
+    a.ih = ih;
+    a.iw = iw;
+    a.R = 2 * ih;
+    a.C = 2 * iw;
+    a.dst = dst;
+    return launch_layer_t<0, 5, true>(a, s);
 }
 
 }  // namespace fsb

@@ -231,7 +231,10 @@ int32_t run_pyramid(Workspace& ws, const uint8_t* d_img, int img_stride, bool ex
     a.rows = g.R[0];
     a.cols = g.C[0];
     a.dst = P[0];
-    launch<0, 5, true>(exact, a, s);
+    if (exact)
+        launch<0, 5, true>(exact, a, s);
+    else
+        FSB_TRY(launch_base_fast(d_img, img_stride, g.h, g.w, P[0], s));
     float* cur = P[0];   // base of the current octave
     for (int o = 0; o < g.n_oct; ++o) {
         const long long RC = (long long)g.R[o] * g.C[o];
