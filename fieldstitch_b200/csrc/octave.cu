@@ -352,10 +352,20 @@ __global__ void __launch_bounds__(LNT) k_layer(LayerArgs a) {
     const int x0 = blockIdx.x * LX, y0 = blockIdx.y * LY;
     // input rows y0 - r .. y0 + LY + r - 1, columns x0 - 16 .. x0 + LX + 15 (reflect-101 outside)
     if (BASE) {
-        // source rows / columns of every tile row / column (reflect-101 on the upsampled grid),
-        // kept in the row-pair area until the vertical pass needs it
+        // Source rows / columns of every tile row / column (reflect-101 on the upsampled grid),
+        // then the row-interpolated values 0.75 a[iy] + 0.25 a[ny] of a window of source columns;
+        // each upsampled sample is 0.75 vc[ix] + 0.25 vc[nx] (gsift.py:90-102 rounding). Tables and
+        // window live in the row-pair area until the vertical pass needs it; a column outside the
+        // window (mirrored columns of an edge tile) is computed from global memory.
+        constexpr int VCW = 96;
         int* rtab = reinterpret_cast<int*>(t2);
         int* ctab = rtab + 2 * IH;
+        float* vcs = reinterpret_cast<float*>(ctab + 2 * LIN_W);
+        const int right = min(x0 + LX + 15, a.C - 1);
+        int lo = x0 - 16;
+        if (x0 + LX + 15 >= a.C) lo = min(lo, 2 * a.C - 2 - (x0 + LX + 15));
+        const int sx0 = max(0, (lo >> 1) - 1);
+        const int nsx = min(min(a.iw - 1, (right >> 1) + 1) - sx0 + 1, VCW);
         for (int i = tid; i < IH + LIN_W; i += LNT) {
             if (i < IH) {
                 const int Y = mir(y0 - r + i, a.R), iy = Y >> 1;
@@ -364,22 +374,38 @@ __global__ void __launch_bounds__(LNT) k_layer(LayerArgs a) {
                 rtab[2 * i + 1] = ny * a.img_stride;
             } else {
                 const int c = i - IH, X = mir(x0 - 16 + c, a.C), ix = X >> 1;
+                const int nx = (X & 1) ? min(ix + 1, a.iw - 1) : max(ix - 1, 0);
                 ctab[2 * c] = ix;
-                ctab[2 * c + 1] = (X & 1) ? min(ix + 1, a.iw - 1) : max(ix - 1, 0);
+                ctab[2 * c + 1] = nx;
             }
         }
         __syncthreads();
         const float sc = (float)(1.0 / 255.0);
+        for (int i = tid; i < IH * VCW; i += LNT) {
+            const int row = i / VCW, k = i - row * VCW;
+            if (k >= nsx) continue;
+            const float p0 = __fmul_rn((float)__ldg(a.img + rtab[2 * row] + sx0 + k), sc);
+            const float p1 = __fmul_rn((float)__ldg(a.img + rtab[2 * row + 1] + sx0 + k), sc);
+            vcs[row * VCW + k] = __fadd_rn(__fmul_rn(0.75f, p0), __fmul_rn(0.25f, p1));
+        }
+        __syncthreads();
 #pragma unroll 4
         for (int i = tid; i < IH * LIN_W; i += LNT) {
             const int row = i / LIN_W, col = i - row * LIN_W;
-            const uint8_t* r0 = a.img + rtab[2 * row];
-            const uint8_t* r1 = a.img + rtab[2 * row + 1];
             const int ix = ctab[2 * col], nx = ctab[2 * col + 1];
-            const float p00 = __fmul_rn((float)__ldg(r0 + ix), sc), p10 = __fmul_rn((float)__ldg(r1 + ix), sc);
-            const float p01 = __fmul_rn((float)__ldg(r0 + nx), sc), p11 = __fmul_rn((float)__ldg(r1 + nx), sc);
-            const float vc = __fadd_rn(__fmul_rn(0.75f, p00), __fmul_rn(0.25f, p10));
-            const float vn = __fadd_rn(__fmul_rn(0.75f, p01), __fmul_rn(0.25f, p11));
+            const int kx = ix - sx0, kn = nx - sx0;
+            float vc, vn;
+            if (kx >= 0 && kx < nsx && kn >= 0 && kn < nsx) {
+                vc = vcs[row * VCW + kx];
+                vn = vcs[row * VCW + kn];
+            } else {
+                const uint8_t* r0 = a.img + rtab[2 * row];
+                const uint8_t* r1 = a.img + rtab[2 * row + 1];
+                vc = __fadd_rn(__fmul_rn(0.75f, __fmul_rn((float)__ldg(r0 + ix), sc)),
+                               __fmul_rn(0.25f, __fmul_rn((float)__ldg(r1 + ix), sc)));
+                vn = __fadd_rn(__fmul_rn(0.75f, __fmul_rn((float)__ldg(r0 + nx), sc)),
+                               __fmul_rn(0.25f, __fmul_rn((float)__ldg(r1 + nx), sc)));
+            }
             s_in[row * LIN_W + col] = __fadd_rn(__fmul_rn(0.75f, vc), __fmul_rn(0.25f, vn));
         }
     } else if ((a.C & 3) == 0 && x0 >= 16 && x0 + LX + 16 <= a.C) {
