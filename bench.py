@@ -40,6 +40,13 @@ H_IMG, W_IMG = 1978, 2640
 RADIUS, RATIO, KC = 40.0, 0.85, 16
 
 
+def _json_num(o):
+    """numpy scalars in the JSON line"""
+    if hasattr(o, "item"):
+        return o.item()
+    raise TypeError(type(o).__name__)
+
+
 def parse():
     p = argparse.ArgumentParser()
     p.add_argument("--gpus", type=int, default=1)
@@ -53,6 +60,10 @@ def parse():
     p.add_argument("--streams", type=int, default=4, help="host threads, each with its own context/stream")
     p.add_argument("--sweep-pairs", type=int, default=256, help="dense precision sweep: pairs per batch (0: skip)")
     p.add_argument("--sweep-n", type=int, default=16384, help="dense precision sweep: descriptors per image")
+    p.add_argument("--plain-pairs", type=int, default=16,
+                   help="pairs timed through the plain sequential path (one stream, one pair at a time; 0: skip)")
+    p.add_argument("--filter-pairs", type=int, default=64,
+                   help="pairs for the learned match filter (3/4 train, 1/4 held out; 0: skip)")
     return p.parse_args()
 
 
@@ -197,7 +208,7 @@ def run_reference(args):
             "cpu_baseline": {"value": v, "unit": "pairs/s", "cores": cores, "kind": "port",
                              "sample": "1 pair per step (2 images 2640x1978 + guided match), %d steps" % args.steps},
             "e2e": {"value": v, "unit": "pairs/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
-    print(json.dumps(line), flush=True)
+    print(json.dumps(line, default=_json_num), flush=True)
     return 0
 
 
@@ -277,6 +288,76 @@ def dense_sweep(args, local):
             "flops_per_batch_algorithmic": flops, **out,
             "speedup_bf16_vs_fp32": out["fp32"]["ms_per_batch"] / out["bf16"]["ms_per_batch"],
             "speedup_fp8_vs_fp32": out["fp32"]["ms_per_batch"] / out["fp8"]["ms_per_batch"]}
+
+
+def learned_filter(args, local, pairs):
+    """The learned match filter on synthetic pairs of the workload: labels from the plain pipeline's
+    own RANSAC verification; train (GPU kernels) on the first 3/4 of the pairs, evaluate on the
+    rest against the same verification (and, for reference, against the true homography):
+    precision / recall / F1 of the ratio test vs the filter, the filter stage's throughput (BF16
+    inference), and the training time."""
+    import torch
+
+    from fieldstitch_b200 import match_filter as MF
+    from fieldstitch_b200 import synth
+    dev = torch.device("cuda", local)
+    sets = []
+    for i, (a, b, H, na, nb) in enumerate(pairs):
+        sets.append(MF.label_pair(a, b, H, na, nb, synth.prior_noise(16000, args.seed + 7 * i), radius=RADIUS,
+                                  kc=KC, ratio=RATIO, device=local))
+    ntr = max(1, (3 * len(sets)) // 4)
+    train, test = sets[:ntr], sets[ntr:]
+    feat = torch.cat([s["feat"][torch.from_numpy(s["has_cand"]).to(dev)] for s in train])
+    lab = torch.cat([s["label"][torch.from_numpy(s["has_cand"]).to(dev)] for s in train])
+    mf = MF.MatchFilter(device=local)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    losses = mf.fit(feat, lab, epochs=30, batch=8192, lr=2e-3, seed=args.seed)
+    torch.cuda.synchronize()
+    train_s = time.perf_counter() - t0
+    acc = {"plain": [0.0, 0.0], "filter": [0.0, 0.0]}   # [true positives, accepted]
+    acc_t = {"plain": [0.0, 0.0], "filter": [0.0, 0.0]}
+    pos = pos_t = 0.0
+    agree = total = 0
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ms = 0.0
+    for s in test:
+        lh, lt = s["label_host"], s["label_true"]
+        pos += lh.sum()
+        pos_t += lt.sum()
+        e0.record()
+        qm, _ = mf.matches(s["t1"], s["b12"], s["nb"], s["feat"])
+        e1.record()
+        torch.cuda.synchronize()
+        ms += e0.elapsed_time(e1)
+        qm = qm.cpu().numpy()
+        for k, q in (("plain", s["q_plain"]), ("filter", qm)):
+            acc[k][0] += lh[q].sum()
+            acc[k][1] += len(q)
+            acc_t[k][0] += lt[q].sum()
+            acc_t[k][1] += len(q)
+        p32 = mf.predict(s["feat"], bf16=False).cpu().numpy() > 0.5
+        p16 = mf.predict(s["feat"], bf16=True).cpu().numpy() > 0.5
+        agree += int((p32 == p16).sum())
+        total += len(p32)
+
+    def prf(tp_n, p):
+        tp, n = float(tp_n[0]), float(tp_n[1])
+        p = float(p)
+        prec = tp / n if n else 0.0
+        rec = tp / p if p else 0.0
+        return {"precision": prec, "recall": rec, "f1": 2 * tp / (n + p) if (n + p) else 0.0}
+
+    return {"workload": "%d synthetic pairs at %dx%d (the bench's pairs): %d train / %d held out; features of every "
+                        "query's best guided candidate (16 nearest within %g px); labels: the plain pipeline's RANSAC "
+                        "homography (cv2, 3 px) maps the candidate within 2 px" % (len(sets), W_IMG, H_IMG, len(train),
+                                                                                   len(test), RADIUS),
+            "train_correspondences": int(len(lab)), "train_epochs": 30, "train_seconds": train_s,
+            "loss_first_last": [float(losses[0]), float(losses[-1])],
+            "vs_plain_verification": {"ratio_test": prf(acc["plain"], pos), "mlp_filter": prf(acc["filter"], pos)},
+            "vs_true_homography": {"ratio_test": prf(acc_t["plain"], pos_t), "mlp_filter": prf(acc_t["filter"], pos_t)},
+            "filter_stage_pairs_per_s": len(test) / (ms / 1000.0) if ms > 0 else None,
+            "bf16_fp32_decision_agreement": agree / total if total else None}
 
 
 def run_fsb(args):
@@ -481,9 +562,32 @@ def run_fsb(args):
                "sample": "%d pairs of the same workload (OpenCV SIFT as features.sift_cpu + NumPy/cKDTree "
                          "guided match)" % n_cpu}
 
+    # ---- the plain sequential path: one context (one stream), one pair at a time
+    plain = None
+    if args.plain_pairs > 0:
+        wk = workers[0]
+        items = list(range(min(args.plain_pairs, len(pairs))))
+        wk.run(items[:1])
+        torch.cuda.synchronize()
+        p0, p1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        p0.record(wk.stream)
+        wk.run(items)
+        p1.record(wk.stream)
+        torch.cuda.synchronize()
+        ms_plain = p0.elapsed_time(p1)
+        plain = {"value": len(items) / (ms_plain / 1000.0), "unit": "pairs/s", "pairs": len(items),
+                 "path": "one context / stream, pairs one after another, host waits after every call",
+                 "batched_over_plain": value / (len(items) / (ms_plain / 1000.0))}
+
     sweep = None
     if rank == 0 and args.sweep_pairs > 0:
         sweep = dense_sweep(args, local)
+    filt = None
+    if rank == 0 and args.filter_pairs > 0:
+        fp = pairs[:args.filter_pairs]
+        if args.filter_pairs > len(pairs):
+            fp = pairs + gen_pairs(args.filter_pairs - len(pairs), args.seed + 500000)
+        filt = learned_filter(args, local, fp)
 
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": "pairs/s", "n_gpus": world, "steps": args.steps,
@@ -491,9 +595,10 @@ def run_fsb(args):
                 "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded)",
                 "config": config(args, {"host_streams": args.streams}),
                 "clocks": clk, "e2e": e2e, "gpu_launches": int(launches), "roofline": roof, "cpu_baseline": cpu,
-                "matches_per_step": matches / args.steps, "dense_precision_sweep": sweep,
+                "matches_per_step": matches / args.steps, "plain_single_stream": plain,
+                "dense_precision_sweep": sweep, "learned_filter": filt,
                 "stages_ms_per_step_summed_over_streams": {k: v[0] / args.steps for k, v in stages.items()}}
-        print(json.dumps(line), flush=True)
+        print(json.dumps(line, default=_json_num), flush=True)
     pool.shutdown()
     for wk in workers:
         wk.ctx.close()

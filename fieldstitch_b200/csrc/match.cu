@@ -235,21 +235,20 @@ __device__ __forceinline__ int exact_d2(const uint32_t* __restrict__ qa, const u
     return (qn + nB[j]) - 2 * (int)dot;
 }
 
-__global__ void __launch_bounds__(G_WARPS * 32) k_guided(const double* __restrict__ pred, const uint8_t* __restrict__ A,
-                                                         int na, const double* __restrict__ bxy,
-                                                         const uint8_t* __restrict__ B, int nb,
-                                                         const int32_t* __restrict__ nA, const int32_t* __restrict__ nB,
-                                                         GridSpec gs, const int32_t* __restrict__ start,
-                                                         const int32_t* __restrict__ items, double wb, double hb,
-                                                         double radius, int kc, float ratio,
-                                                         int32_t* __restrict__ t_row, uint32_t* __restrict__ d_row,
-                                                         int32_t* __restrict__ c_t, float* __restrict__ c_b12,
-                                                         int* __restrict__ overflow) {
-    __shared__ uint32_t s_q[G_WARPS][32];
-    __shared__ double s_cd[G_WARPS][G_CAND];
-    __shared__ int32_t s_ci[G_WARPS][G_CAND];
+// One query of the guided matcher (one warp): candidates of the prior window, exact distances,
+// top-2, ratio test; writes t_row/d_row (nullable) and the pre-ratio candidate (c_t, nullable).
+__device__ __forceinline__ void guided_query(int q, const double* __restrict__ pred, const uint8_t* __restrict__ A,
+                                             int na, const double* __restrict__ bxy,
+                                             const uint8_t* __restrict__ B, int nb,
+                                             const int32_t* __restrict__ nA, const int32_t* __restrict__ nB,
+                                             GridSpec gs, const int32_t* __restrict__ start,
+                                             const int32_t* __restrict__ items, double wb, double hb,
+                                             double radius, int kc, float ratio,
+                                             int32_t* __restrict__ t_row, uint32_t* __restrict__ d_row,
+                                             int32_t* __restrict__ c_t, float* __restrict__ c_b12,
+                                             int* __restrict__ overflow, uint32_t (*s_q)[32],
+                                             double (*s_cd)[G_CAND], int32_t (*s_ci)[G_CAND]) {
     const int wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int q = blockIdx.x * G_WARPS + wid;
     if (q >= na) return;
     const double px = pred[2 * q], py = pred[2 * q + 1];
     int32_t res_t = -1;
@@ -359,6 +358,23 @@ __global__ void __launch_bounds__(G_WARPS * 32) k_guided(const double* __restric
             c_b12[2 * q + 1] = cand_b2;
         }
     }
+}
+
+__global__ void __launch_bounds__(G_WARPS * 32) k_guided(const double* __restrict__ pred, const uint8_t* __restrict__ A,
+                                                         int na, const double* __restrict__ bxy,
+                                                         const uint8_t* __restrict__ B, int nb,
+                                                         const int32_t* __restrict__ nA, const int32_t* __restrict__ nB,
+                                                         GridSpec gs, const int32_t* __restrict__ start,
+                                                         const int32_t* __restrict__ items, double wb, double hb,
+                                                         double radius, int kc, float ratio,
+                                                         int32_t* __restrict__ t_row, uint32_t* __restrict__ d_row,
+                                                         int32_t* __restrict__ c_t, float* __restrict__ c_b12,
+                                                         int* __restrict__ overflow) {
+    __shared__ uint32_t s_q[G_WARPS][32];
+    __shared__ double s_cd[G_WARPS][G_CAND];
+    __shared__ int32_t s_ci[G_WARPS][G_CAND];
+    guided_query(blockIdx.x * G_WARPS + (threadIdx.x >> 5), pred, A, na, bxy, B, nb, nA, nB, gs, start, items, wb, hb,
+                 radius, kc, ratio, t_row, d_row, c_t, c_b12, overflow, s_q, s_cd, s_ci);
 }
 
 __global__ void k_perspective(const double* __restrict__ xy, int n, const double* __restrict__ hm,
