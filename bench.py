@@ -410,7 +410,24 @@ def run_fsb(args):
             self.dt = torch.empty(nmax, dtype=torch.int64, device=dev)
             self.n_out = ctypes.c_int32()
 
+        def extract(self, items=None):
+            """SIFT of both images and the prior projections of the pairs, into the per-pair buffers
+            that the batched guided match reads."""
+            L, c, n_out = self.L, self.ctx.handle, self.n_out
+            for i in (self.items if items is None else items):
+                ia, ib = d_img[i]
+                B = pb[i]
+                for k, (img, nf) in enumerate(((ia, pairs[i][3]), (ib, pairs[i][4]))):
+                    _lib.check(L.fsb_sift_features_d(c, P(img), h, w, w, ctypes.byref(prm), nf, P(B["xy"][k]),
+                                                     P(B["rs"][k]), None, P(B["u8"][k]), ctypes.byref(n_out)), "sift")
+                    B["n"][k] = n_out.value
+                _lib.check(L.fsb_project_d(c, P(B["xy"][0]), B["n"][0], _lib.ptr(Hs[i]), P(d_noise[i]), P(B["pred"])),
+                           "proj")
+                _lib.check(L.fsb_project_d(c, P(B["xy"][1]), B["n"][1], _lib.ptr(eye), None, P(B["bxy"])), "proj")
+            return 0
+
         def run(self, items=None):
+            """The plain per-pair sequence: SIFT A, SIFT B, projections, guided match of this pair."""
             L, c, n_out = self.L, self.ctx.handle, self.n_out
             matches = 0
             for i in (self.items if items is None else items):
@@ -429,11 +446,36 @@ def run_fsb(args):
                 matches += n_out.value
             return matches
 
+    # per-pair device buffers for the batched match
+    pb = [{"xy": [torch.empty((nmax, 2), dtype=torch.float32, device=dev) for _ in range(2)],
+           "rs": [torch.empty(nmax, dtype=torch.float32, device=dev) for _ in range(2)],
+           "u8": [torch.empty((nmax, 128), dtype=torch.uint8, device=dev) for _ in range(2)],
+           "pred": torch.empty((nmax, 2), dtype=torch.float64, device=dev),
+           "bxy": torch.empty((nmax, 2), dtype=torch.float64, device=dev),
+           "q": torch.empty(nmax, dtype=torch.int64, device=dev), "t": torch.empty(nmax, dtype=torch.int64, device=dev),
+           "n": [0, 0]} for _ in pairs]
     workers = [Worker(i, args.streams) for i in range(args.streams)]
     pool = ThreadPoolExecutor(max_workers=args.streams)
+    mctx = _lib.Context(local)   # the batched match's context (stream)
+    mstream = torch.cuda.ExternalStream(mctx.stream())
+    NPs = len(pairs)
+    Pv, Iv, Dv = ctypes.c_void_p * NPs, ctypes.c_int32 * NPs, ctypes.c_double * NPs
+    m_cnt = Iv()
+
+    def match_batch():
+        """Every pair's guided match in one call (one CUDA graph, replayed from the second step)."""
+        _lib.check(mctx.lib.fsb_match_guided_batch_d(
+            mctx.handle, NPs, Pv(*[b["pred"].data_ptr() for b in pb]), Pv(*[b["u8"][0].data_ptr() for b in pb]),
+            Iv(*[b["n"][0] for b in pb]), Pv(*[b["bxy"].data_ptr() for b in pb]),
+            Pv(*[b["u8"][1].data_ptr() for b in pb]), Iv(*[b["n"][1] for b in pb]), Dv(*([float(w)] * NPs)),
+            Dv(*([float(h)] * NPs)), RADIUS, KC, RATIO, Pv(*[b["q"].data_ptr() for b in pb]),
+            Pv(*[b["t"].data_ptr() for b in pb]), m_cnt), "guided batch")
+        return sum(m_cnt[i] for i in range(NPs))
 
     def one_step():
-        return sum(f.result() for f in [pool.submit(wk.run) for wk in workers])
+        for f in [pool.submit(wk.extract) for wk in workers]:
+            f.result()
+        return match_batch()
 
     def barrier():
         if dist is not None:
@@ -449,12 +491,13 @@ def run_fsb(args):
         e0.record(main)
         for wk in workers:
             wk.stream.wait_event(e0)
+        mstream.wait_event(e0)
         out = 0
         for _ in range(steps):
             out += fn()
-        for wk in workers:
+        for st in [wk.stream for wk in workers] + [mstream]:
             ev = torch.cuda.Event()
-            ev.record(wk.stream)
+            ev.record(st)
             main.wait_event(ev)
         e1.record(main)
         torch.cuda.synchronize()
@@ -464,20 +507,20 @@ def run_fsb(args):
         one_step()
     torch.cuda.synchronize()
     barrier()
-    for wk in workers:
-        wk.ctx.timing(True)
-        wk.ctx.stage_times()
+    for c_ in [wk.ctx for wk in workers] + [mctx]:
+        c_.timing(True)
+        c_.stage_times()
     clocks = Clocks(gpu_smi_id(torch, local))
     launches0 = _lib.launch_count()
     ms_step, matches = timed(one_step, args.steps)
     clk = clocks.stop()
     launches = _lib.launch_count() - launches0
     stages = {}
-    for wk in workers:
-        for k_, (ms_, n_) in wk.ctx.stage_times().items():
+    for c_ in [wk.ctx for wk in workers] + [mctx]:
+        for k_, (ms_, n_) in c_.stage_times().items():
             a_, b_ = stages.get(k_, (0.0, 0))
             stages[k_] = (a_ + ms_, b_ + n_)
-        wk.ctx.timing(False)
+        c_.timing(False)
     if dist is not None:
         t = torch.tensor([ms_step], device=dev)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
@@ -593,7 +636,9 @@ def run_fsb(args):
         line = {"metric": METRIC, "value": value, "unit": "pairs/s", "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
                 "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded)",
-                "config": config(args, {"host_streams": args.streams}),
+                "config": config(args, {"host_streams": args.streams,
+                                        "matching": "every pair of a step in one fsb_match_guided_batch_d call "
+                                                    "(one CUDA graph, captured once, replayed each step)"}),
                 "clocks": clk, "e2e": e2e, "gpu_launches": int(launches), "roofline": roof, "cpu_baseline": cpu,
                 "matches_per_step": matches / args.steps, "plain_single_stream": plain,
                 "dense_precision_sweep": sweep, "learned_filter": filt,
@@ -602,6 +647,7 @@ def run_fsb(args):
     pool.shutdown()
     for wk in workers:
         wk.ctx.close()
+    mctx.close()
     if dist is not None:
         barrier()
         dist.destroy_process_group()

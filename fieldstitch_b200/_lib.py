@@ -62,6 +62,8 @@ SIGNATURES = [
                                        c_vp, c_vp, c_vp]),
     ("fsb_match_guided_cand_d", c_i32, [c_vp, c_vp, c_vp, c_i32, c_vp, c_vp, c_i32, c_f64, c_f64, c_f64, c_i32,
                                         c_vp, c_vp]),
+    ("fsb_match_guided_batch_d", c_i32, [c_vp, c_i32, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_f64, c_i32,
+                                         c_f32, c_vp, c_vp, c_vp]),
     ("fsb_mlp_param_count", c_i32, []),
     ("fsb_mlp_trainable_count", c_i32, []),
     ("fsb_mlp_features_d", c_i32, [c_vp, c_i32, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp,

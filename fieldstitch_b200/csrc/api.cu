@@ -255,8 +255,10 @@ int32_t fsb_destroy(fsb_ctx* ctx) {
     ctx->pool.clear();
     DevBuf* all[] = {&ctx->s_u8a, &ctx->s_u8b, &ctx->s_f32a, &ctx->s_f32b, &ctx->s_i32, &ctx->s_i64,
                      &ctx->s_u64, &ctx->s_misc, &ctx->s_misc2, &ctx->s_host_stage, &ctx->s_cub,
-                     &ctx->s_tc_pack, &ctx->s_tc_part, &ctx->s_tc_aux, &ctx->s_count};
+                     &ctx->s_tc_pack, &ctx->s_tc_part, &ctx->s_tc_aux, &ctx->s_count, &ctx->s_gb};
     for (DevBuf* b : all) b->release();
+    if (ctx->gb_graph.exec) cudaGraphExecDestroy(ctx->gb_graph.exec);
+    if (ctx->gb_graph.graph) cudaGraphDestroy(ctx->gb_graph.graph);
     if (ctx->pinned) cudaFreeHost(ctx->pinned);
     for (auto& e : ctx->ev)
         if (e) cudaEventDestroy(e);
@@ -305,7 +307,7 @@ int64_t fsb_device_bytes(fsb_ctx* ctx) {
     for (Workspace* w : ctx->pool) t += (int64_t)w->bytes();
     const DevBuf* all[] = {&ctx->s_u8a, &ctx->s_u8b, &ctx->s_f32a, &ctx->s_f32b, &ctx->s_i32, &ctx->s_i64,
                            &ctx->s_u64, &ctx->s_misc, &ctx->s_misc2, &ctx->s_host_stage, &ctx->s_cub,
-                     &ctx->s_tc_pack, &ctx->s_tc_part, &ctx->s_tc_aux, &ctx->s_count};
+                     &ctx->s_tc_pack, &ctx->s_tc_part, &ctx->s_tc_aux, &ctx->s_count, &ctx->s_gb};
     for (const DevBuf* b : all) t += (int64_t)b->bytes;
     return t;
 }
@@ -670,6 +672,57 @@ int32_t fsb_match_guided_cand_d(fsb_ctx* ctx, const double* d_pred, const uint8_
                              nullptr, s, d_t1, d_b12));
     FSB_CUDA(cudaStreamSynchronize(s));
     ctx->stage_end(ST_MATCH);
+    return FSB_OK;
+}
+
+int32_t fsb_match_guided_batch_d(fsb_ctx* ctx, int32_t n_pairs, const double* const* d_pred, const uint8_t* const* d_a,
+                                 const int32_t* na, const double* const* d_bxy, const uint8_t* const* d_b,
+                                 const int32_t* nb, const double* w_b, const double* h_b, double radius, int32_t kc,
+                                 float ratio, int64_t* const* d_q, int64_t* const* d_t, int32_t* n_out) {
+    FSB_ARG(ctx && n_out && n_pairs >= 0, "bad arguments");
+    FSB_ARG(n_pairs == 0 || (d_pred && d_a && na && d_bxy && d_b && nb && w_b && h_b && d_q && d_t), "null array");
+    FSB_ARG(std::isfinite(radius), "non-finite radius");
+    std::vector<int> live;
+    for (int p = 0; p < n_pairs; ++p) {
+        FSB_ARG(na[p] >= 0 && nb[p] >= 0, "negative size");
+        FSB_ARG(na[p] == 0 || (d_a[p] && d_pred[p] && d_q[p] && d_t[p]), "null array");
+        FSB_ARG(nb[p] == 0 || (d_b[p] && d_bxy[p]), "null array");
+        FSB_ARG(std::isfinite(w_b[p]) && std::isfinite(h_b[p]), "non-finite frame");
+        n_out[p] = 0;
+        if (na[p] > 0 && nb[p] > 0 && radius > 0.0) live.push_back(p);
+    }
+    if (live.empty()) return FSB_OK;
+    FSB_TRY(use_device(ctx));
+    cudaStream_t s = ctx->stream;
+    const size_t L = live.size();
+    std::vector<const double*> pr(L), bx(L);
+    std::vector<const uint8_t*> pa(L), pb(L);
+    std::vector<int> ra(L), rb(L);
+    std::vector<double> wv(L), hv(L);
+    std::vector<int64_t*> pq(L), pt(L);
+    for (size_t i = 0; i < L; ++i) {
+        const int p = live[i];
+        pr[i] = d_pred[p];
+        pa[i] = d_a[p];
+        ra[i] = na[p];
+        bx[i] = d_bxy[p];
+        pb[i] = d_b[p];
+        rb[i] = nb[p];
+        wv[i] = w_b[p];
+        hv[i] = h_b[p];
+        pq[i] = d_q[p];
+        pt[i] = d_t[p];
+    }
+    FSB_TRY(ctx->s_count.ensure(L * 4 + 64));
+    int32_t* dn = ctx->s_count.as<int32_t>();
+    ctx->stage_begin(ST_MATCH);
+    FSB_TRY(run_match_guided_batch(ctx, (int)L, pr.data(), pa.data(), ra.data(), bx.data(), pb.data(), rb.data(),
+                                   wv.data(), hv.data(), radius, kc, ratio, pq.data(), pt.data(), dn, s));
+    std::vector<int> cnt(L, 0);
+    FSB_CUDA(cudaMemcpyAsync(cnt.data(), dn, L * 4, cudaMemcpyDeviceToHost, s));
+    FSB_CUDA(cudaStreamSynchronize(s));
+    ctx->stage_end(ST_MATCH);
+    for (size_t i = 0; i < L; ++i) n_out[live[i]] = cnt[i];
     return FSB_OK;
 }
 

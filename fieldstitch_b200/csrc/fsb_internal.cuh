@@ -104,6 +104,13 @@ struct TcStats {
     float mean_abs_err = 0.f;      // and its mean
 };
 
+// A captured guided-batch graph and the exact inputs it was captured for.
+struct GuidedGraph {
+    std::vector<char> key;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+};
+
 // Pyramid + detection workspace sized for one image geometry.
 struct Workspace {
     Geometry g{};
@@ -133,6 +140,8 @@ struct fsb_ctx {
     fsb::DevBuf s_cub;   // CUB temporary storage (one primitive at a time)
     fsb::DevBuf s_tc_pack, s_tc_part, s_tc_aux;   // tensor-core matcher: packed operands, candidates, tables
     fsb::DevBuf s_count;   // result counts of the API calls; never grown by the internal stages
+    fsb::DevBuf s_gb;      // guided batch scratch (addresses captured in gb_graph)
+    fsb::GuidedGraph gb_graph;
     fsb::TcStats tc_stats{};                      // of the last tensor-core dense match
     void* pinned = nullptr;
     size_t pinned_bytes = 0;
@@ -187,6 +196,10 @@ int32_t run_match_guided(fsb_ctx* ctx, const double* d_pred, const uint8_t* d_a,
                          const uint8_t* d_b, int nb, double wb, double hb, double radius, int kc, float ratio,
                          int64_t* d_q, int64_t* d_t, int* d_n, cudaStream_t s, int32_t* c_t = nullptr,
                          float* c_b12 = nullptr);
+int32_t run_match_guided_batch(fsb_ctx* ctx, int n_pairs, const double* const* d_pred, const uint8_t* const* d_a,
+                               const int* na, const double* const* d_bxy, const uint8_t* const* d_b, const int* nb,
+                               const double* wb, const double* hb, double radius, int kc, float ratio,
+                               int64_t* const* d_q, int64_t* const* d_t, int32_t* counts, cudaStream_t s);
 int32_t run_unique_rows(fsb_ctx* ctx, const int32_t* t_row, const uint32_t* d_row, int na, int nb, int64_t* d_q,
                         int64_t* d_t, int* d_n, cudaStream_t s);
 // mlp.cu

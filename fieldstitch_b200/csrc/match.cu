@@ -448,6 +448,106 @@ __global__ void k_uq_emit(const uint32_t* __restrict__ pos, const int* __restric
     to[i] = t[pos[i]];
 }
 
+
+// ------------------------------------------------------------------------------ guided batch
+// Many guided problems in one set of launches (blockIdx.y = pair): concatenated norms, one grid
+// per pair in one concatenated cell array (one prefix sum for all), one guided kernel over every
+// query of every pair, and _unique per pair over concatenated target keys.
+struct GPair {
+    const double* pred;
+    const uint8_t* a;
+    const double* bxy;
+    const uint8_t* b;
+    int na, nb;
+    double wb, hb;
+    GridSpec gs;
+    int cell0;   // first cell of this pair's grid
+    int item0;   // first target (B row) in the concatenated target arrays
+    int row0;    // first query (A row) in the concatenated query arrays
+    int64_t* q_out;
+    int64_t* t_out;
+};
+
+__global__ void k_gb_norms(const GPair* __restrict__ pairs, int which, int32_t* __restrict__ out) {
+    const GPair& P = pairs[blockIdx.y];
+    const int n = which ? P.nb : P.na;
+    const int row = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    const int lane = threadIdx.x & 31;
+    if (row >= n) return;
+    const uint8_t* d = which ? P.b : P.a;
+    const uint32_t w = reinterpret_cast<const uint32_t*>(d + (size_t)row * 128)[lane];
+    int s = (int)__dp4a(w, w, 0u);
+    for (int sh = 16; sh; sh >>= 1) s += __shfl_xor_sync(0xffffffffu, s, sh);
+    if (lane == 0) out[(which ? P.item0 : P.row0) + row] = s;
+}
+
+__global__ void k_gb_count(const GPair* __restrict__ pairs, int32_t* __restrict__ cell, int32_t* __restrict__ count) {
+    const GPair& P = pairs[blockIdx.y];
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= P.nb) return;
+    const int cx = cell_of(P.bxy[2 * j], P.gs.x0, P.gs.cs, P.gs.gw), cy = cell_of(P.bxy[2 * j + 1], P.gs.y0, P.gs.cs, P.gs.gh);
+    const int c = P.cell0 + cy * P.gs.gw + cx;
+    cell[P.item0 + j] = c;
+    atomicAdd(count + c, 1);
+}
+
+__global__ void k_gb_fill(const GPair* __restrict__ pairs, const int32_t* __restrict__ cell,
+                          const int32_t* __restrict__ start, int32_t* __restrict__ cursor, int32_t* __restrict__ items) {
+    const GPair& P = pairs[blockIdx.y];
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= P.nb) return;
+    const int c = cell[P.item0 + j];
+    items[start[c] + atomicAdd(cursor + c, 1)] = j;   // local target index
+}
+
+__global__ void __launch_bounds__(G_WARPS * 32) k_gb_guided(const GPair* __restrict__ pairs, const int32_t* __restrict__ nA,
+                                                            const int32_t* __restrict__ nB,
+                                                            const int32_t* __restrict__ start,
+                                                            const int32_t* __restrict__ items, double radius, int kc,
+                                                            float ratio, int32_t* __restrict__ t_row,
+                                                            uint32_t* __restrict__ d_row, int* __restrict__ overflow) {
+    __shared__ uint32_t s_q[G_WARPS][32];
+    __shared__ double s_cd[G_WARPS][G_CAND];
+    __shared__ int32_t s_ci[G_WARPS][G_CAND];
+    const GPair& P = pairs[blockIdx.y];
+    guided_query(blockIdx.x * G_WARPS + (threadIdx.x >> 5), P.pred, P.a, P.na, P.bxy, P.b, P.nb, nA + P.row0,
+                 nB + P.item0, P.gs, start + P.cell0, items, P.wb, P.hb, radius, kc, ratio, t_row + P.row0,
+                 d_row + P.row0, nullptr, nullptr, overflow, s_q, s_cd, s_ci);
+}
+
+__global__ void k_gb_fill_keys(unsigned long long* __restrict__ key, int n) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) key[i] = ~0ull;
+}
+
+__global__ void k_gb_keys(const GPair* __restrict__ pairs, const int32_t* __restrict__ t_row,
+                          const uint32_t* __restrict__ d_row, unsigned long long* __restrict__ key) {
+    const GPair& P = pairs[blockIdx.y];
+    const int q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= P.na) return;
+    const int t = t_row[P.row0 + q];
+    if (t >= 0) atomicMin(key + P.item0 + t, ((unsigned long long)d_row[P.row0 + q] << 32) | (unsigned)q);
+}
+
+__global__ void k_gb_flags(const unsigned long long* __restrict__ key, int n, int32_t* __restrict__ flag) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i <= n) flag[i] = i < n && key[i] != ~0ull;
+}
+
+__global__ void k_gb_emit(const GPair* __restrict__ pairs, const unsigned long long* __restrict__ key,
+                          const int32_t* __restrict__ pos, int32_t* __restrict__ counts) {
+    const GPair& P = pairs[blockIdx.y];
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= P.nb) return;
+    const int i = P.item0 + j;
+    if (j == P.nb - 1) counts[blockIdx.y] = pos[P.item0 + P.nb] - pos[P.item0];
+    const unsigned long long k = key[i];
+    if (k == ~0ull) return;
+    const int o = pos[i] - pos[P.item0];
+    P.q_out[o] = (int64_t)(k & 0xffffffffull);
+    P.t_out[o] = j;
+}
+
 }  // namespace
 
 // General one-to-one filter (matching._unique) for arbitrary int64 targets and float distances:
@@ -623,6 +723,152 @@ int32_t run_match_guided(fsb_ctx* ctx, const double* d_pred, const uint8_t* d_a,
     }
     if (!d_n) return FSB_OK;   // candidates only
     return run_unique(ctx, t_row, d_row, na, nb, d_q, d_t, d_n, s);
+}
+
+
+// Guided matching of a batch of pairs (each na, nb >= 1, radius > 0) with _unique, as one CUDA
+// graph on the context's stream: captured on the first call with a given pair table and replayed
+// while the table (pointers, sizes, frames) and the scratch addresses stay the same. counts:
+// device, one per pair.
+int32_t run_match_guided_batch(fsb_ctx* ctx, int n_pairs, const double* const* d_pred, const uint8_t* const* d_a,
+                               const int* na, const double* const* d_bxy, const uint8_t* const* d_b, const int* nb,
+                               const double* wb, const double* hb, double radius, int kc, float ratio,
+                               int64_t* const* d_q, int64_t* const* d_t, int32_t* counts, cudaStream_t s) {
+    if (n_pairs <= 0) return FSB_OK;
+    std::vector<GPair> hp(n_pairs);
+    long long cells = 0, rows = 0, items = 0;
+    int max_na = 0, max_nb = 0;
+    for (int p = 0; p < n_pairs; ++p) {
+        GPair& P = hp[p];
+        P.pred = d_pred[p];
+        P.a = d_a[p];
+        P.bxy = d_bxy[p];
+        P.b = d_b[p];
+        P.na = na[p];
+        P.nb = nb[p];
+        P.wb = wb[p];
+        P.hb = hb[p];
+        GridSpec gs;
+        gs.x0 = 0.0;
+        gs.y0 = 0.0;
+        gs.cs = radius;
+        double gwd = (wb[p] > 0 ? wb[p] : 1.0) / radius + 1.0, ghd = (hb[p] > 0 ? hb[p] : 1.0) / radius + 1.0;
+        while (gwd * ghd > 4.0e6) {
+            gs.cs *= 2.0;
+            gwd = (wb[p] > 0 ? wb[p] : 1.0) / gs.cs + 1.0;
+            ghd = (hb[p] > 0 ? hb[p] : 1.0) / gs.cs + 1.0;
+        }
+        gs.gw = (int)gwd;
+        gs.gh = (int)ghd;
+        P.gs = gs;
+        P.cell0 = (int)cells;
+        P.item0 = (int)items;
+        P.row0 = (int)rows;
+        P.q_out = d_q[p];
+        P.t_out = d_t[p];
+        cells += (long long)gs.gw * gs.gh;
+        rows += na[p];
+        items += nb[p];
+        max_na = std::max(max_na, na[p]);
+        max_nb = std::max(max_nb, nb[p]);
+    }
+    if (cells + items + rows > 0x7fffffffLL) {
+        set_error("guided batch too large (%lld cells, %lld targets, %lld queries)", cells, items, rows);
+        return FSB_ERR_ARG;
+    }
+    size_t tb1 = 0, tb2 = 0;
+    cub::DeviceScan::ExclusiveSum(nullptr, tb1, (int32_t*)nullptr, (int32_t*)nullptr, (int)(cells + 1), s);
+    cub::DeviceScan::ExclusiveSum(nullptr, tb2, (int32_t*)nullptr, (int32_t*)nullptr, (int)(items + 1), s);
+    auto al = [](size_t x) { return (x + 255) & ~size_t(255); };
+    const size_t b_pairs = al((size_t)n_pairs * sizeof(GPair)), b_rows = al((size_t)rows * 4), b_items = al((size_t)items * 4);
+    const size_t b_cells = al((size_t)(cells + 1) * 4), b_keys = al((size_t)items * 8), b_flag = al((size_t)(items + 1) * 4);
+    const size_t need = b_pairs + 3 * b_rows + 3 * b_items + 3 * b_cells + b_keys + 2 * b_flag + al(std::max(tb1, tb2)) + 512;
+    void* before = ctx->s_gb.p;
+    FSB_TRY(ctx->s_gb.ensure(need));
+    uint8_t* cur = ctx->s_gb.as<uint8_t>();
+    auto take = [&](size_t bytes) {
+        uint8_t* p = cur;
+        cur += bytes;
+        return p;
+    };
+    GPair* d_pairs = reinterpret_cast<GPair*>(take(b_pairs));
+    int32_t* nA = reinterpret_cast<int32_t*>(take(b_rows));
+    int32_t* t_row = reinterpret_cast<int32_t*>(take(b_rows));
+    uint32_t* d_row = reinterpret_cast<uint32_t*>(take(b_rows));
+    int32_t* nB = reinterpret_cast<int32_t*>(take(b_items));
+    int32_t* cell = reinterpret_cast<int32_t*>(take(b_items));
+    int32_t* gitems = reinterpret_cast<int32_t*>(take(b_items));
+    int32_t* count = reinterpret_cast<int32_t*>(take(b_cells));
+    int32_t* start = reinterpret_cast<int32_t*>(take(b_cells));
+    int32_t* cursor = reinterpret_cast<int32_t*>(take(b_cells));
+    unsigned long long* keys = reinterpret_cast<unsigned long long*>(take(b_keys));
+    int32_t* flag = reinterpret_cast<int32_t*>(take(b_flag));
+    int32_t* pos = reinterpret_cast<int32_t*>(take(b_flag));
+    void* tmp = take(al(std::max(tb1, tb2)));
+    int* overflow = reinterpret_cast<int*>(take(256));
+    // the graph is valid for exactly this table, these scratch addresses and parameters
+    GuidedGraph& G = ctx->gb_graph;
+    std::vector<char> key(sizeof(GPair) * n_pairs + 64);
+    memcpy(key.data(), hp.data(), sizeof(GPair) * n_pairs);
+    {
+        char* k = key.data() + sizeof(GPair) * n_pairs;
+        memcpy(k, &radius, 8);
+        memcpy(k + 8, &kc, 4);
+        memcpy(k + 12, &ratio, 4);
+        memcpy(k + 16, &counts, 8);
+        void* base = ctx->s_gb.p;
+        memcpy(k + 24, &base, 8);
+        const size_t nb_ = ctx->s_gb.bytes;
+        memcpy(k + 32, &nb_, 8);
+    }
+    const bool reuse = G.exec && before == ctx->s_gb.p && G.key == key;
+    if (!reuse) {
+        if (G.exec) cudaGraphExecDestroy(G.exec);
+        if (G.graph) cudaGraphDestroy(G.graph);
+        G.exec = nullptr;
+        G.graph = nullptr;
+        G.key.clear();
+        FSB_CUDA(cudaMemcpyAsync(d_pairs, hp.data(), (size_t)n_pairs * sizeof(GPair), cudaMemcpyHostToDevice, s));
+        FSB_CUDA(cudaStreamSynchronize(s));
+        FSB_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+        const unsigned py = (unsigned)n_pairs;
+        cudaMemsetAsync(count, 0, (size_t)(cells + 1) * 4, s);
+        cudaMemsetAsync(cursor, 0, (size_t)(cells + 1) * 4, s);
+        cudaMemsetAsync(overflow, 0, 4, s);
+        k_gb_norms<<<dim3(blocks(max_na, 8), py), 256, 0, s>>>(d_pairs, 0, nA);
+        k_gb_norms<<<dim3(blocks(max_nb, 8), py), 256, 0, s>>>(d_pairs, 1, nB);
+        k_gb_count<<<dim3(blocks(max_nb, 256), py), 256, 0, s>>>(d_pairs, cell, count);
+        cub::DeviceScan::ExclusiveSum(tmp, tb1, count, start, (int)(cells + 1), s);
+        k_gb_fill<<<dim3(blocks(max_nb, 256), py), 256, 0, s>>>(d_pairs, cell, start, cursor, gitems);
+        k_gb_guided<<<dim3(blocks(max_na, G_WARPS), py), G_WARPS * 32, 0, s>>>(d_pairs, nA, nB, start, gitems, radius,
+                                                                             kc, ratio, t_row, d_row, overflow);
+        k_gb_fill_keys<<<blocks(items, 256), 256, 0, s>>>(keys, (int)items);
+        k_gb_keys<<<dim3(blocks(max_na, 256), py), 256, 0, s>>>(d_pairs, t_row, d_row, keys);
+        k_gb_flags<<<blocks(items + 1, 256), 256, 0, s>>>(keys, (int)items, flag);
+        cub::DeviceScan::ExclusiveSum(tmp, tb2, flag, pos, (int)(items + 1), s);
+        k_gb_emit<<<dim3(blocks(max_nb, 256), py), 256, 0, s>>>(d_pairs, keys, pos, counts);
+        cudaError_t ce = cudaStreamEndCapture(s, &G.graph);
+        if (ce == cudaSuccess) ce = cudaGraphInstantiate(&G.exec, G.graph, 0);
+        if (ce != cudaSuccess) {
+            if (G.graph) cudaGraphDestroy(G.graph);
+            G.graph = nullptr;
+            G.exec = nullptr;
+            cudaGetLastError();
+            set_error("guided batch graph: %s", cudaGetErrorString(ce));
+            return FSB_ERR_CUDA;
+        }
+        G.key = key;
+    }
+    FSB_CUDA(cudaGraphLaunch(G.exec, s));
+    note_launch(13);
+    int h_over = 0;
+    FSB_CUDA(cudaMemcpyAsync(&h_over, overflow, sizeof(int), cudaMemcpyDeviceToHost, s));
+    FSB_CUDA(cudaStreamSynchronize(s));
+    if (h_over) {
+        set_error("more than %d B keypoints within the radius of one prediction (kc mode)", G_CAND);
+        return FSB_ERR_OVERFLOW;
+    }
+    return FSB_OK;
 }
 
 }  // namespace fsb

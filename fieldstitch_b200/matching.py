@@ -76,6 +76,42 @@ def ratio_match_bf_batch_d(a_list, b_list, ratio, precision="bf16", device=0, ou
     return [(o[0][:cnt[i]], o[1][:cnt[i]]) for i, o in enumerate(outs)]
 
 
+def guided_from_pred_batch_d(problems, radius, kc, ratio, device=0, out=None):
+    """Many ``guided_from_pred`` problems in one call on device-resident data, as one CUDA graph.
+
+    ``problems[p]`` = (pred float64 (na,2), a uint8 (na,128), b_xy float64 (nb,2), b uint8 (nb,128),
+    (w_b, h_b)), CUDA tensors on ``device``. ``out[p]`` (optional, reused across calls): a pair of
+    int64 CUDA tensors of length >= na. Returns [(q, t)] per pair, ordered by target.
+    """
+    import torch
+    n = len(problems)
+    for pred, a, bxy, b, _ in problems:
+        for x, dt, w in ((pred, torch.float64, 2), (a, torch.uint8, 128), (bxy, torch.float64, 2),
+                         (b, torch.uint8, 128)):
+            if x.dtype != dt or x.dim() != 2 or x.shape[1] != w or not x.is_contiguous() or not x.is_cuda:
+                raise ValueError("expected contiguous CUDA tensors: pred/b_xy float64 (n,2), a/b uint8 (n,128)")
+        if len(pred) != len(a) or len(bxy) != len(b):
+            raise ValueError("positions and descriptors differ in length")
+    ctx = _lib.context(device)
+    if out is None:
+        out = [(torch.empty(max(len(pr), 1), dtype=torch.int64, device=pr.device),
+                torch.empty(max(len(pr), 1), dtype=torch.int64, device=pr.device)) for pr, _, _, _, _ in problems]
+    P = ctypes.c_void_p * max(n, 1)
+    I = ctypes.c_int32 * max(n, 1)
+    D = ctypes.c_double * max(n, 1)
+    k = 0 if kc is None else int(kc)
+    cnt = I()
+    torch.cuda.current_stream(device).synchronize()
+    _lib.check(ctx.lib.fsb_match_guided_batch_d(
+        ctx.handle, n, P(*[x[0].data_ptr() for x in problems]), P(*[x[1].data_ptr() for x in problems]),
+        I(*[len(x[1]) for x in problems]), P(*[x[2].data_ptr() for x in problems]),
+        P(*[x[3].data_ptr() for x in problems]), I(*[len(x[3]) for x in problems]),
+        D(*[float(x[4][0]) for x in problems]), D(*[float(x[4][1]) for x in problems]), float(radius), k,
+        float(ratio), P(*[o[0].data_ptr() for o in out]), P(*[o[1].data_ptr() for o in out]), cnt),
+        "fsb_match_guided_batch_d")
+    return [(o[0][:cnt[i]], o[1][:cnt[i]]) for i, o in enumerate(out)]
+
+
 def tc_stats(device=0):
     """Statistics of the last tensor-core dense match on this thread's context for ``device``:
     rows, rows recomputed exactly (certificate not settled), largest / mean absolute error of the

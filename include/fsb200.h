@@ -148,6 +148,19 @@ int32_t fsb_match_guided_d(fsb_ctx* ctx, const double* d_pred, const uint8_t* d_
                            const double* d_bxy, const uint8_t* d_b, int32_t nb, double w_b, double h_b,
                            double radius, int32_t kc, float ratio, int64_t* d_q, int64_t* d_t,
                            int32_t* n_out);
+/* A batch of fsb_match_guided_d problems in one call (pointer and size arrays on the host,
+   data in device memory): pair p matches d_a[p] (na[p] queries, predicted positions d_pred[p])
+   against d_b[p] (nb[p] targets at d_bxy[p], frame w_b[p] x h_b[p]) and writes n_out[p] pairs
+   into d_q[p], d_t[p]. All pairs share one set of launches (one grid build, one guided kernel
+   over every query of every pair, one batched _unique), issued as a CUDA graph that is captured
+   on the first call and replayed while the pair table and the context's scratch are unchanged.
+   Replaces a loop over matching._guided (app/planesite/matching.py:113-152); results are
+   identical to per-pair calls. */
+int32_t fsb_match_guided_batch_d(fsb_ctx* ctx, int32_t n_pairs, const double* const* d_pred,
+                                 const uint8_t* const* d_a, const int32_t* na, const double* const* d_bxy,
+                                 const uint8_t* const* d_b, const int32_t* nb, const double* w_b,
+                                 const double* h_b, double radius, int32_t kc, float ratio,
+                                 int64_t* const* d_q, int64_t* const* d_t, int32_t* n_out);
 /* The guided matcher's candidates before its ratio test: per query the best target within the
    radius (kc rule as fsb_match_guided; -1 when there is none) in d_t1 (na int32) and its squared
    distance b1 and the second-best b2 (+inf for a single candidate) in d_b12 (na x 2 float32).
