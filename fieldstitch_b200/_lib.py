@@ -64,6 +64,7 @@ SIGNATURES = [
                                         c_vp, c_vp]),
     ("fsb_match_guided_batch_d", c_i32, [c_vp, c_i32, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_f64, c_i32,
                                          c_f32, c_vp, c_vp, c_vp]),
+    ("fsb_autotune_table", c_i32, [ctypes.c_char_p, c_i32]),
     ("fsb_mlp_param_count", c_i32, []),
     ("fsb_mlp_trainable_count", c_i32, []),
     ("fsb_mlp_features_d", c_i32, [c_vp, c_i32, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp,
@@ -181,3 +182,16 @@ def as_u8_desc(d, name="descriptors"):
     if not np.array_equal(u, d):
         raise ValueError("%s must hold uint8 values (0..255 integers)" % name)
     return np.ascontiguousarray(u)
+
+
+def autotune_table():
+    """{key: variant} of the launch-variant autotuner's choices in this process."""
+    lib = load()
+    n = int(lib.fsb_autotune_table(None, 0))
+    buf = ctypes.create_string_buffer(max(n, 1))
+    lib.fsb_autotune_table(buf, n)
+    out = {}
+    for line in buf.value.decode().splitlines():
+        k, v = line.rsplit(" ", 1)
+        out[k] = int(v)
+    return out

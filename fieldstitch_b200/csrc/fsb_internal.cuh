@@ -172,9 +172,14 @@ int32_t run_pyramid(Workspace& ws, const uint8_t* d_img, int img_stride, bool ex
 int32_t upload_octave_taps(const float* taps, int stride, const int* counts);
 int32_t launch_octave_fused(const float* L0, int R, int C, float* dog, float* mag, float* ang, float* down,
                             int down_cols, cudaStream_t s);
+int layer_tile_variants();
+int layer_tile_height(int variant);
 int32_t launch_layer_fast(int layer, const float* src, int R, int C, float* dst, float* dog, float* mag, float* ang,
-                          float* down, int down_cols, cudaStream_t s);
-int32_t launch_base_fast(const uint8_t* img, int stride, int ih, int iw, float* dst, cudaStream_t s);
+                          float* down, int down_cols, int variant, cudaStream_t s);
+int32_t launch_base_fast(const uint8_t* img, int stride, int ih, int iw, float* dst, int variant, cudaStream_t s);
+// autotune.cu: the fastest of n_variants launches of `run` for `key` (timed once per process and
+// device on `s`, then cached; FSB_AUTOTUNE=0 returns variant 0, FSB_AUTOTUNE_FILE persists choices)
+int32_t autotune(const char* key, int n_variants, int32_t (*run)(void*, int), void* arg, cudaStream_t s, int* variant);
 
 // ---------------------------------------------------------------- detect.cu / describe.cu
 int32_t run_orient(const Workspace& ws, const Refined* ref, const uint32_t* d_nref, uint32_t n_ref_host,

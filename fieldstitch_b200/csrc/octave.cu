@@ -318,7 +318,7 @@ __global__ void __launch_bounds__(NT, 2) k_octave(Args a) {
 // The input tile (16 columns and r rows of reflect-101 halo) arrives by 16-byte cp.async, the
 // vertical pass keeps an 8-row sliding window of column pairs in registers, the horizontal pass
 // reads the row-pair interleaved vertical outputs. No ring buffers: 3-4 CTAs per SM.
-constexpr int LX = 128, LY = 32, LNT = 256;
+constexpr int LX = 128, LNT = 256;   // tile width, threads; the tile height LY is a template parameter
 constexpr int LIN_W = LX + 32;   // input tile pitch (floats)
 constexpr int LT2_W = LX + 32;   // row-pair tile pitch (float2)
 
@@ -335,12 +335,12 @@ struct LayerArgs {
     int down_cols;
 };
 
-template <int r>
+template <int r, int LY>
 constexpr int layer_smem() {
     return (LY + 2 * r) * LIN_W * 4 + (LY / 2) * LT2_W * 8;
 }
 
-template <int TS, int r, bool BASE>
+template <int TS, int r, bool BASE, int LY>
 __global__ void __launch_bounds__(LNT) k_layer(LayerArgs a) {
     constexpr int d = r & 1;
     constexpr int IH = LY + 2 * r;
@@ -358,6 +358,8 @@ __global__ void __launch_bounds__(LNT) k_layer(LayerArgs a) {
         // window live in the row-pair area until the vertical pass needs it; a column outside the
         // window (mirrored columns of an edge tile) is computed from global memory.
         constexpr int VCW = 96;
+        static_assert(!BASE || (2 * IH + 2 * LIN_W) * 4 + IH * VCW * 4 <= (LY / 2) * LT2_W * 8,
+                      "base tables must fit the row-pair area");
         int* rtab = reinterpret_cast<int*>(t2);
         int* ctab = rtab + 2 * IH;
         float* vcs = reinterpret_cast<float*>(ctab + 2 * LIN_W);
@@ -518,21 +520,37 @@ __global__ void __launch_bounds__(LNT) k_layer(LayerArgs a) {
     }
 }
 
-template <int TS, int r, bool BASE>
-int32_t launch_layer_t(const LayerArgs& a, cudaStream_t s) {
+template <int TS, int r, bool BASE, int LY>
+int32_t launch_layer_ly(const LayerArgs& a, cudaStream_t s) {
     static bool attr[64] = {};
     int dev = 0;
     FSB_CUDA(cudaGetDevice(&dev));
     if (dev < 64 && !attr[dev]) {
-        FSB_CUDA(cudaFuncSetAttribute(k_layer<TS, r, BASE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                      layer_smem<r>()));
+        FSB_CUDA(cudaFuncSetAttribute(k_layer<TS, r, BASE, LY>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      layer_smem<r, LY>()));
         attr[dev] = true;
     }
     dim3 grid((a.C + LX - 1) / LX, (a.R + LY - 1) / LY);
-    k_layer<TS, r, BASE><<<grid, LNT, layer_smem<r>(), s>>>(a);
+    k_layer<TS, r, BASE, LY><<<grid, LNT, layer_smem<r, LY>(), s>>>(a);
     note_launch();
     FSB_CUDA(cudaGetLastError());
     return FSB_OK;
+}
+
+// tile heights the autotuner chooses from (index 0 is the default)
+constexpr int kTileHeights[3] = {32, 16, 64};
+
+template <int TS, int r, bool BASE>
+int32_t launch_layer_t(const LayerArgs& a, int variant, cudaStream_t s) {
+    if constexpr (BASE) {   // the base tile's source tables need a tile height of at least 32
+        return variant == 2 ? launch_layer_ly<TS, r, BASE, 64>(a, s) : launch_layer_ly<TS, r, BASE, 32>(a, s);
+    } else {
+        switch (variant) {
+            case 1: return launch_layer_ly<TS, r, BASE, 16>(a, s);
+            case 2: return launch_layer_ly<TS, r, BASE, 64>(a, s);
+            default: return launch_layer_ly<TS, r, BASE, 32>(a, s);
+        }
+    }
 }
 
 }  // namespace
@@ -575,9 +593,13 @@ int32_t launch_octave_fused(const float* L0, int R, int C, float* dog, float* ma
 
 namespace fsb {
 
-// One layer of the float32 pyramid by the tiled per-layer kernel: L_layer from src (R x C).
+int layer_tile_variants() { return 3; }
+int layer_tile_height(int variant) { return kTileHeights[variant < 0 || variant > 2 ? 0 : variant]; }
+
+// One layer of the float32 pyramid by the tiled per-layer kernel: L_layer from src (R x C), tile
+// height layer_tile_height(variant).
 int32_t launch_layer_fast(int layer, const float* src, int R, int C, float* dst, float* dog, float* mag, float* ang,
-                          float* down, int down_cols, cudaStream_t s) {
+                          float* down, int down_cols, int variant, cudaStream_t s) {
     LayerArgs a{};
     a.src = src;
     a.R = R;
@@ -589,18 +611,18 @@ int32_t launch_layer_fast(int layer, const float* src, int R, int C, float* dst,
     a.down = down;
     a.down_cols = down_cols;
     switch (layer) {
-        case 1: return launch_layer_t<1, 5, false>(a, s);
-        case 2: return launch_layer_t<2, 6, false>(a, s);
-        case 3: return launch_layer_t<3, 8, false>(a, s);
-        case 4: return launch_layer_t<4, 10, false>(a, s);
-        case 5: return launch_layer_t<5, 13, false>(a, s);
+        case 1: return launch_layer_t<1, 5, false>(a, variant, s);
+        case 2: return launch_layer_t<2, 6, false>(a, variant, s);
+        case 3: return launch_layer_t<3, 8, false>(a, variant, s);
+        case 4: return launch_layer_t<4, 10, false>(a, variant, s);
+        case 5: return launch_layer_t<5, 13, false>(a, variant, s);
         default: set_error("layer %d out of range", layer); return FSB_ERR_ARG;
     }
 }
 
 
 // The float32 octave-0 base: blur (tap set 0, radius 5) of the 2x upsampled uint8 image.
-int32_t launch_base_fast(const uint8_t* img, int stride, int ih, int iw, float* dst, cudaStream_t s) {
+int32_t launch_base_fast(const uint8_t* img, int stride, int ih, int iw, float* dst, int variant, cudaStream_t s) {
     LayerArgs a{};
     a.img = img;
     a.img_stride = stride;
@@ -609,7 +631,7 @@ int32_t launch_base_fast(const uint8_t* img, int stride, int ih, int iw, float* 
     a.R = 2 * ih;
     a.C = 2 * iw;
     a.dst = dst;
-    return launch_layer_t<0, 5, true>(a, s);
+    return launch_layer_t<0, 5, true>(a, variant, s);
 }
 
 }  // namespace fsb

@@ -15,6 +15,7 @@
 // from the tile already in shared memory, so none of those needs a separate pass over HBM.
 #include <cmath>
 
+#include <cstdio>
 #include <cstdlib>
 #include <cstring>
 
@@ -209,6 +210,40 @@ void launch(bool exact, const BlurArgs& a, cudaStream_t s) {
 // streaming kernel (k_octave) for octaves at least kFusedMinCols wide when FSB_PYRAMID=fused.
 static const int kFusedMinCols = 2000;
 
+namespace {
+struct LayerCall {
+    int layer;
+    const float* src;
+    int R, C;
+    float *dst, *dog, *mag, *ang, *down;
+    int dc;
+    cudaStream_t s;
+};
+int32_t run_layer_call(void* p, int v) {
+    const LayerCall* c = static_cast<const LayerCall*>(p);
+    return launch_layer_fast(c->layer, c->src, c->R, c->C, c->dst, c->dog, c->mag, c->ang, c->down, c->dc, v, c->s);
+}
+struct BaseCall {
+    const uint8_t* img;
+    int stride, h, w;
+    float* dst;
+    cudaStream_t s;
+};
+int32_t run_base_call(void* p, int v) {
+    const BaseCall* c = static_cast<const BaseCall*>(p);
+    return launch_base_fast(c->img, c->stride, c->h, c->w, c->dst, v == 1 ? 2 : 0, c->s);   // heights 32, 64
+}
+// one tuned per-layer launch: the tile height is chosen per (layer, octave size)
+int32_t tuned_layer(int layer, const float* src, int R, int C, float* dst, float* dog, float* mag, float* ang,
+                    float* down, int dc, cudaStream_t s) {
+    LayerCall c{layer, src, R, C, dst, dog, mag, ang, down, dc, s};
+    char key[64];
+    std::snprintf(key, sizeof(key), "k_layer%d_%dx%d", layer, R, C);
+    int v = 0;
+    return autotune(key, layer_tile_variants(), run_layer_call, &c, s, &v);
+}
+}  // namespace
+
 static bool use_fused_octaves() {
     static const bool on = [] {
         const char* e = std::getenv("FSB_PYRAMID");
@@ -231,10 +266,15 @@ int32_t run_pyramid(Workspace& ws, const uint8_t* d_img, int img_stride, bool ex
     a.rows = g.R[0];
     a.cols = g.C[0];
     a.dst = P[0];
-    if (exact)
+    if (exact) {
         launch<0, 5, true>(exact, a, s);
-    else
-        FSB_TRY(launch_base_fast(d_img, img_stride, g.h, g.w, P[0], s));
+    } else {
+        BaseCall bc{d_img, img_stride, g.h, g.w, P[0], s};
+        char key[64];
+        std::snprintf(key, sizeof(key), "k_base_%dx%d", g.h, g.w);
+        int v = 0;
+        FSB_TRY(autotune(key, 2, run_base_call, &bc, s, &v));
+    }
     float* cur = P[0];   // base of the current octave
     for (int o = 0; o < g.n_oct; ++o) {
         const long long RC = (long long)g.R[o] * g.C[o];
@@ -255,12 +295,12 @@ int32_t run_pyramid(Workspace& ws, const uint8_t* d_img, int img_stride, bool ex
             const int R = g.R[o], C = g.C[o];
             float* down = o + 1 < g.n_oct ? cur : nullptr;
             const int dc = o + 1 < g.n_oct ? g.C[o + 1] : 0;
-            FSB_TRY(launch_layer_fast(1, cur, R, C, other[0], dog, nullptr, nullptr, nullptr, 0, s));
-            FSB_TRY(launch_layer_fast(2, other[0], R, C, other[1], dog + RC, mag, ang, nullptr, 0, s));
-            FSB_TRY(launch_layer_fast(3, other[1], R, C, other[0], dog + 2 * RC, mag + RC, ang + RC, nullptr, 0, s));
-            FSB_TRY(launch_layer_fast(4, other[0], R, C, other[1], dog + 3 * RC, mag + 2 * RC, ang + 2 * RC, down, dc,
+            FSB_TRY(tuned_layer(1, cur, R, C, other[0], dog, nullptr, nullptr, nullptr, 0, s));
+            FSB_TRY(tuned_layer(2, other[0], R, C, other[1], dog + RC, mag, ang, nullptr, 0, s));
+            FSB_TRY(tuned_layer(3, other[1], R, C, other[0], dog + 2 * RC, mag + RC, ang + RC, nullptr, 0, s));
+            FSB_TRY(tuned_layer(4, other[0], R, C, other[1], dog + 3 * RC, mag + 2 * RC, ang + 2 * RC, down, dc,
                                       s));
-            FSB_TRY(launch_layer_fast(5, other[1], R, C, nullptr, dog + 4 * RC, nullptr, nullptr, nullptr, 0, s));
+            FSB_TRY(tuned_layer(5, other[1], R, C, nullptr, dog + 4 * RC, nullptr, nullptr, nullptr, 0, s));
             continue;   // the next base is in `cur` (the dead L0 plane)
         }
         BlurArgs b{};

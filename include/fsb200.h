@@ -189,6 +189,13 @@ int32_t fsb_match_bf_batch_d(fsb_ctx* ctx, int32_t n_pairs, const uint8_t* const
 int32_t fsb_match_tc_stats(fsb_ctx* ctx, int64_t* rows, int64_t* fallback_rows, double* max_abs_err,
                            double* mean_abs_err);
 
+/* Launch-variant autotuner report: the choices made so far in this process, one "key variant"
+   line each (key = device name / ordinal / kernel and size; for the per-layer pyramid kernel the
+   variant indexes the tile heights 32, 16, 64). Returns the bytes needed including the final
+   zero; writes at most len of them into buf (nullable). Set FSB_AUTOTUNE=0 to disable tuning,
+   FSB_AUTOTUNE_FILE=path to keep choices across processes. No counterpart in the reference. */
+int32_t fsb_autotune_table(char* buf, int32_t len);
+
 /* ---- learned match filter (no counterpart in the reference: it replaces the ratio test of
    matching._guided, app/planesite/matching.py:142-146, by an 8-64-64-1 MLP whose labels come
    from the plain pipeline's own RANSAC verification, matching.py:205-233) --------------------

@@ -71,3 +71,27 @@ def test_detect_fast_wide_image_matches_oracle():
     assert frac >= 0.97, frac
     back, _ = paired_fraction(got, ref)
     assert back >= 0.97, back
+
+
+def test_autotuned_tile_heights_are_bit_identical(monkeypatch):
+    """The per-layer kernel's tile heights (16, 32, 64) compute the same values: a pyramid whose
+    launches the autotuner times and picks equals the untuned one bit for bit, and the tuner
+    records one choice per (layer, octave size)."""
+    import fieldstitch_b200 as f
+    from fieldstitch_b200 import _lib, synth
+    img = synth.synth_image(700, 900, 31)
+    monkeypatch.setenv("FSB_AUTOTUNE", "0")
+    _, st0 = f.gsift.detect(img)
+    ref = st0.atlas()
+    monkeypatch.delenv("FSB_AUTOTUNE")
+    _, st1 = f.gsift.detect(img)   # first call with this geometry: every variant runs
+    got = st1.atlas()
+    _, st2 = f.gsift.detect(img)   # cached choices
+    again = st2.atlas()
+    for o in range(len(ref[0])):
+        for k in (1, 2, 3):
+            np.testing.assert_array_equal(got[k][o], ref[k][o])
+            np.testing.assert_array_equal(again[k][o], ref[k][o])
+    table = _lib.autotune_table()
+    assert any("k_layer5_1400x1800" in k for k in table), table
+    assert all(v in (0, 1, 2) for v in table.values())
