@@ -50,7 +50,9 @@ __device__ __forceinline__ void warp_append(bool flag, const T& v, T* out, uint3
 // One CTA per (octave, 4 interior rows, 256 columns): DoG layers 0..4, rows r-1 .. r+4, columns
 // c0-4 .. c0+259 are staged in shared memory with 16-byte loads (each DoG value comes from DRAM
 // about 1.5 times: the row halo), then every thread tests its column for 4 rows x layers 1..3.
-constexpr int EX_T = 256, EX_ROWS = 4, EX_W = 264;
+constexpr int EX_T = 256;            // 8 warps per block
+constexpr int EX_COLS = 30;          // output columns per warp (lanes 1..30; lanes 0 and 31 are halo)
+constexpr int EX_ROWS = 64;          // rows per block (a chunk of the octave's interior rows)
 
 struct ExTiles {
     int n_oct;
@@ -58,97 +60,89 @@ struct ExTiles {
     int first[MAXO + 1];     // first block of each octave
 };
 
+// Streaming 3x3x3 extremum test: each warp walks down a chunk of rows of 30 interior columns;
+// every DoG value is read once (coalesced), horizontal neighbours come from the adjacent lanes,
+// the 3-row vertical window of the horizontal maxima / minima stays in registers. A voxel is an
+// extremum when it equals the maximum (minimum) of its 27-neighbourhood - ties count - and is
+// beyond the threshold, as scipy's maximum_filter / minimum_filter test in the reference
+// (gsift.py:293-319). Candidates of a row are appended with one warp-aggregated atomic.
 __global__ void __launch_bounds__(EX_T) k_extrema(const float* __restrict__ DF, DetectConsts k, ExTiles tl,
                                                   uint32_t* __restrict__ cand, uint32_t* counter, uint32_t cap) {
-    __shared__ __align__(16) float tile[5][EX_ROWS + 2][EX_W];
     int o = 0;
     while (o + 1 < tl.n_oct && (int)blockIdx.x >= tl.first[o + 1]) ++o;
     const int b = blockIdx.x - tl.first[o];
     const int ry = b / tl.col_tiles[o], cx = b - ry * tl.col_tiles[o];
     const int R = k.g.R[o], C = k.g.C[o];
-    const int r0 = BORDER + ry * EX_ROWS, c0 = cx * 256;
     const long long RC = (long long)R * C;
     const float* base = DF + k.g.dog_off[o];
-    const bool vec = (C & 3) == 0 && (k.g.dog_off[o] & 3) == 0;
-    // stage layers 0..4, rows r0-1 .. r0+EX_ROWS, columns c0-4 .. c0+259
-    for (int e = threadIdx.x; e < 5 * (EX_ROWS + 2) * (EX_W / 4); e += EX_T) {
-        const int q = e % (EX_W / 4), t = e / (EX_W / 4);
-        const int rr = t % (EX_ROWS + 2), l = t / (EX_ROWS + 2);
-        const int y = r0 - 1 + rr, x = c0 - 4 + 4 * q;
-        float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
-        if (y < R) {
-            const float* p = base + l * RC + (long long)y * C;
-            if (vec && x >= 0 && x + 4 <= C) {
-                v = *reinterpret_cast<const float4*>(p + x);
-            } else {
-                if (x >= 0 && x < C) v.x = p[x];
-                if (x + 1 >= 0 && x + 1 < C) v.y = p[x + 1];
-                if (x + 2 >= 0 && x + 2 < C) v.z = p[x + 2];
-                if (x + 3 >= 0 && x + 3 < C) v.w = p[x + 3];
-            }
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    const int c = BORDER + (cx * (EX_T / 32) + wid) * EX_COLS + lane - 1;   // this lane's column
+    const int cc = min(max(c, 0), C - 1);                                    // clamped for loading
+    const bool col_ok = lane >= 1 && lane <= EX_COLS && c >= BORDER && c < C - BORDER;
+    const int y0 = BORDER + ry * EX_ROWS, y1 = min(y0 + EX_ROWS, R - BORDER);   // output rows [y0, y1)
+    float hx0[5], hx1[5], hn0[5], hn1[5], prev[3];
+    auto load_row = [&](int y, float (&hx)[5], float (&hn)[5], float (&ctr)[3]) {
+#pragma unroll
+        for (int l = 0; l < 5; ++l) {
+            const float v = __ldg(base + l * RC + (long long)y * C + cc);
+            const float vl = __shfl_up_sync(0xffffffffu, v, 1), vr = __shfl_down_sync(0xffffffffu, v, 1);
+            hx[l] = fmaxf(fmaxf(vl, v), vr);
+            hn[l] = fminf(fminf(vl, v), vr);
+            if (l >= 1 && l <= N_LAYERS) ctr[l - 1] = v;
         }
-        *reinterpret_cast<float4*>(&tile[l][rr][4 * q]) = v;
-    }
-    __syncthreads();
-    const int c = c0 + threadIdx.x, tc = threadIdx.x + 4;
-    const bool col_ok = c >= BORDER && c < C - BORDER;
-    // bit (3 s + l - 1): voxel (layer l, row r0 + s) of this column is an extremum. Separable 3x3x3
-    // maximum / minimum (columns, then rows, then layers) in registers; the voxel is an extremum
-    // when it equals the maximum (minimum) of its 27-neighbourhood - ties count - and is beyond
-    // the threshold, as scipy's maximum_filter / minimum_filter test in the reference.
-    unsigned mask = 0;
-    if (col_ok) {
-        float hmx[5][EX_ROWS + 2], hmn[5][EX_ROWS + 2];
+    };
+    float dummy[3];
+    load_row(y0 - 1, hx0, hn0, dummy);
+    load_row(y0, hx1, hn1, prev);
+    for (int y = y0; y < y1; ++y) {
+        float hx2[5], hn2[5], cur[3];
+        load_row(y + 1, hx2, hn2, cur);
+        float vmx[5], vmn[5];
 #pragma unroll
-        for (int l = 0; l < 5; ++l)
-#pragma unroll
-            for (int rr = 0; rr < EX_ROWS + 2; ++rr) {
-                const float a = tile[l][rr][tc - 1], b = tile[l][rr][tc], cc = tile[l][rr][tc + 1];
-                hmx[l][rr] = fmaxf(fmaxf(a, b), cc);
-                hmn[l][rr] = fminf(fminf(a, b), cc);
-            }
-        float vmx[5][EX_ROWS], vmn[5][EX_ROWS];
-#pragma unroll
-        for (int l = 0; l < 5; ++l)
-#pragma unroll
-            for (int s = 0; s < EX_ROWS; ++s) {
-                vmx[l][s] = fmaxf(fmaxf(hmx[l][s], hmx[l][s + 1]), hmx[l][s + 2]);
-                vmn[l][s] = fminf(fminf(hmn[l][s], hmn[l][s + 1]), hmn[l][s + 2]);
-            }
-#pragma unroll
-        for (int s = 0; s < EX_ROWS; ++s) {
-            const bool row_ok = r0 + s < R - BORDER;
+        for (int l = 0; l < 5; ++l) {
+            vmx[l] = fmaxf(fmaxf(hx0[l], hx1[l]), hx2[l]);
+            vmn[l] = fminf(fminf(hn0[l], hn1[l]), hn2[l]);
+        }
+        unsigned mask = 0;
+        if (col_ok) {
 #pragma unroll
             for (int l = 1; l <= N_LAYERS; ++l) {
-                const float v = tile[l][s + 1][tc];
-                const float mx = fmaxf(fmaxf(vmx[l - 1][s], vmx[l][s]), vmx[l + 1][s]);
-                const float mn = fminf(fminf(vmn[l - 1][s], vmn[l][s]), vmn[l + 1][s]);
-                const bool e = (v >= mx && v > k.pthr) || (v <= mn && v < -k.pthr);
-                if (row_ok && e) mask |= 1u << (3 * s + l - 1);
+                const float v = prev[l - 1];
+                const float mx = fmaxf(fmaxf(vmx[l - 1], vmx[l]), vmx[l + 1]);
+                const float mn = fminf(fminf(vmn[l - 1], vmn[l]), vmn[l + 1]);
+                if ((v >= mx && v > k.pthr) || (v <= mn && v < -k.pthr)) mask |= 1u << (l - 1);
             }
         }
-    }
-    // one warp-aggregated append of all candidates of the warp
-    const int lane = threadIdx.x & 31;
-    const int cntv = __popc(mask);
-    int incl = cntv;
+        const unsigned any = __ballot_sync(0xffffffffu, mask != 0);
+        if (any) {
+            const int cntv = __popc(mask);
+            int incl = cntv;
 #pragma unroll
-    for (int sh = 1; sh < 32; sh <<= 1) {
-        const int t = __shfl_up_sync(0xffffffffu, incl, sh);
-        if (lane >= sh) incl += t;
-    }
-    const int total = __shfl_sync(0xffffffffu, incl, 31);
-    if (total == 0) return;
-    uint32_t basepos = 0;
-    if (lane == 31) basepos = atomicAdd(counter, (uint32_t)total);
-    basepos = __shfl_sync(0xffffffffu, basepos, 31);
-    uint32_t pos = basepos + (uint32_t)(incl - cntv);
-    while (mask) {
-        const int bit = __ffs(mask) - 1;
-        mask &= mask - 1;
-        const int s = bit / 3, l = bit - 3 * s + 1;
-        if (pos < cap) cand[pos] = (uint32_t)(k.g.dog_off[o] + l * RC + (long long)(r0 + s) * C + c);
-        ++pos;
+            for (int sh = 1; sh < 32; sh <<= 1) {
+                const int t = __shfl_up_sync(0xffffffffu, incl, sh);
+                if (lane >= sh) incl += t;
+            }
+            const int total = __shfl_sync(0xffffffffu, incl, 31);
+            uint32_t basepos = 0;
+            if (lane == 31) basepos = atomicAdd(counter, (uint32_t)total);
+            basepos = __shfl_sync(0xffffffffu, basepos, 31);
+            uint32_t pos = basepos + (uint32_t)(incl - cntv);
+            while (mask) {
+                const int bit = __ffs(mask) - 1;
+                mask &= mask - 1;
+                if (pos < cap) cand[pos] = (uint32_t)(k.g.dog_off[o] + (bit + 1) * RC + (long long)y * C + c);
+                ++pos;
+            }
+        }
+#pragma unroll
+        for (int l = 0; l < 5; ++l) {
+            hx0[l] = hx1[l];
+            hx1[l] = hx2[l];
+            hn0[l] = hn1[l];
+            hn1[l] = hn2[l];
+        }
+#pragma unroll
+        for (int l = 0; l < 3; ++l) prev[l] = cur[l];
     }
 }
 
@@ -158,8 +152,9 @@ ExTiles make_tiles(const Geometry& g, int* total) {
     int acc = 0;
     for (int o = 0; o < g.n_oct; ++o) {
         t.first[o] = acc;
-        t.col_tiles[o] = (g.C[o] + 255) / 256;
-        t.row_tiles[o] = (g.R[o] - 2 * BORDER + EX_ROWS - 1) / EX_ROWS;
+        const int inner_c = g.C[o] - 2 * BORDER, inner_r = g.R[o] - 2 * BORDER;
+        t.col_tiles[o] = inner_c > 0 ? (inner_c + (EX_T / 32) * EX_COLS - 1) / ((EX_T / 32) * EX_COLS) : 0;
+        t.row_tiles[o] = inner_r > 0 ? (inner_r + EX_ROWS - 1) / EX_ROWS : 0;
         acc += t.col_tiles[o] * t.row_tiles[o];
     }
     t.first[g.n_oct] = acc;
