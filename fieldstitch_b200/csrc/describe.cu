@@ -71,17 +71,27 @@ __global__ void __launch_bounds__(OW * 32) k_orient(const float* __restrict__ MA
         const int W = 2 * rad + 1;
         const long long gb = g.grad_off[o] + (long long)(e.l - 1) * R * C;
         for (int b = 0; b < ORI_BINS; ++b) acc[b][lane] = (Acc)0;
+        // lane takes samples s = lane, lane + 32, ... of the W x W window (row-major); the window
+        // position advances by (32 / W, 32 % W) per step, one division per keypoint
+        const int dq = 32 / W, dr = 32 - dq * W;
+        int ii = lane / W - rad, jj = lane - (lane / W) * W - rad;
         for (int s = lane; s < W * W; s += 32) {
-            const int ii = s / W - rad, jj = s - (s / W) * W - rad;
             const int y = e.r + ii, x = e.c + jj;
             if (y > 0 && y < R - 1 && x > 0 && x < C - 1) {
                 const long long gi = gb + (long long)y * C + x;
                 const float d2 = (float)(ii * ii + jj * jj);
                 const float w = expf(-d2 / den);
                 const float m = MAG[gi] * w;
-                int b = (int)rintf(ANG[gi] * 0.1f);
-                b = ((b % ORI_BINS) + ORI_BINS) % ORI_BINS;
+                int b = (int)rintf(ANG[gi] * 0.1f);   // angles lie in [0, 360]: b in [0, 36]
+                if (b >= ORI_BINS) b -= ORI_BINS;
+                if (b < 0) b += ORI_BINS;
                 acc[b][lane] += (Acc)m;
+            }
+            ii += dq;
+            jj += dr;
+            if (jj > rad) {
+                jj -= W;
+                ++ii;
             }
         }
         __syncwarp();
