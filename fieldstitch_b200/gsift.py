@@ -123,3 +123,24 @@ def describe(state, kps, sel, budget=2.5e6, timings=None, rootsift=False):
     if timings is not None:
         timings["describe"] = timings.get("describe", 0.0) + time.perf_counter() - t0
     return (desc, u8) if rootsift else desc
+
+
+def cv2_octave(kps):
+    """OpenCV's packed keypoint octave for detect's keypoints: octave byte (o - 1) & 255 (o = 0 is
+    the 2x upsampled octave), layer << 8, round((X2 + 0.5) * 255) << 16 with X2 the sub-layer offset
+    of the refinement, recovered from size = 1.6 * 2^((layer + X2) / 3) * 2^o (gsift.py:462-470)."""
+    o = np.asarray(kps["octave"], np.int64)
+    layer = np.asarray(kps["layer"], np.int64)
+    scl = np.asarray(kps["size"], np.float64) / np.exp2(o.astype(np.float64))
+    x2 = 3.0 * np.log2(np.maximum(scl, 1e-30) / 1.6) - layer
+    sub = np.clip(np.rint((x2 + 0.5) * 255.0), 0, 255).astype(np.int64)
+    return (((o - 1) & 255) | (layer << 8) | (sub << 16)).astype(np.int64)
+
+
+def to_cv2_keypoints(kps):
+    """detect's keypoints as a list of cv2.KeyPoint (pt, size, angle, response, packed octave), the
+    form cv2.SIFT.detect returns, for code that consumes OpenCV keypoints."""
+    import cv2
+    packed = cv2_octave(kps)
+    return [cv2.KeyPoint(float(x), float(y), float(s), float(a), float(r), int(p))
+            for x, y, s, a, r, p in zip(kps["x"], kps["y"], kps["size"], kps["angle"], kps["response"], packed)]

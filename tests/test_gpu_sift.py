@@ -139,3 +139,23 @@ def test_large_image_against_oracle(fsb):
     frac, p = paired_fraction(ref, got, pos_tol=1e-6)
     assert frac >= 0.99, frac
     assert np.all(angle_diff(ref["angle"][p >= 0], got["angle"][p[p >= 0]]) <= 0.1)
+
+
+@pytest.mark.parametrize("case", CASES[:2])
+def test_cv2_keypoint_export_matches_opencv(fsb, golden, case):
+    """to_cv2_keypoints: for keypoints paired with OpenCV's, the packed octave (octave byte and
+    layer) is OpenCV's and the sub-layer byte is within 2; size within 0.1 %."""
+    img, _, contrast, edge, max_kp, _ = _ref(golden, case)
+    c = golden["sift_cv2"]
+    cv = {"x": c[case + "/xy"][:, 0], "y": c[case + "/xy"][:, 1], "angle": c[case + "/angle"]}
+    got, _ = fsb.gsift.detect(img, max_kp=max_kp, contrast=contrast, edge=edge)
+    _, p = paired_fraction(cv, got)
+    m = np.nonzero(p >= 0)[0]
+    assert len(m) > 20
+    ours = fsb.gsift.cv2_octave(got)[p[m]]
+    theirs = c[case + "/octave"][m].astype(np.int64)
+    assert ((ours & 0xffff) == (theirs & 0xffff)).mean() >= 0.99
+    assert (np.abs((ours >> 16) - (theirs >> 16)) <= 2).mean() >= 0.99
+    np.testing.assert_allclose(got["size"][p[m]], c[case + "/size"][m], rtol=1e-3)
+    kp = fsb.gsift.to_cv2_keypoints(got)
+    assert len(kp) == len(got["x"]) and kp[0].octave == int(fsb.gsift.cv2_octave(got)[0])
