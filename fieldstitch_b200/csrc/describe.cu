@@ -75,20 +75,36 @@ __global__ void __launch_bounds__(OW * 32) k_orient(const float* __restrict__ MA
         // position advances by (32 / W, 32 % W) per step, one division per keypoint
         const int dq = 32 / W, dr = 32 - dq * W;
         int ii = lane / W - rad, jj = lane - (lane / W) * W - rad;
-        for (int s = lane; s < W * W; s += 32) {
-            const int y = e.r + ii, x = e.c + jj;
-            if (y > 0 && y < R - 1 && x > 0 && x < C - 1) {
-                const long long gi = gb + (long long)y * C + x;
-                const float d2 = (float)(ii * ii + jj * jj);
-                const float w = expf(-d2 / den);
-                const float m = MAG[gi] * w;
-                int b = (int)rintf(ANG[gi] * 0.1f);   // angles lie in [0, 360]: b in [0, 36]
+        // two samples per step: both gathers are issued before either is accumulated (the
+        // accumulation order of the lane is unchanged)
+        for (int s = lane; s < W * W; s += 64) {
+            int ii2 = ii + dq, jj2 = jj + dr;
+            if (jj2 > rad) {
+                jj2 -= W;
+                ++ii2;
+            }
+            const int y1 = e.r + ii, x1 = e.c + jj, y2 = e.r + ii2, x2 = e.c + jj2;
+            const bool in1 = y1 > 0 && y1 < R - 1 && x1 > 0 && x1 < C - 1;
+            const bool in2 = s + 32 < W * W && y2 > 0 && y2 < R - 1 && x2 > 0 && x2 < C - 1;
+            const long long g1 = gb + (long long)y1 * C + x1, g2 = gb + (long long)y2 * C + x2;
+            const float m1 = in1 ? __ldg(MAG + g1) : 0.f, a1 = in1 ? __ldg(ANG + g1) : 0.f;
+            const float m2 = in2 ? __ldg(MAG + g2) : 0.f, a2 = in2 ? __ldg(ANG + g2) : 0.f;
+            if (in1) {
+                const float w = expf(-(float)(ii * ii + jj * jj) / den);
+                int b = (int)rintf(a1 * 0.1f);   // angles lie in [0, 360]: b in [0, 36]
                 if (b >= ORI_BINS) b -= ORI_BINS;
                 if (b < 0) b += ORI_BINS;
-                acc[b][lane] += (Acc)m;
+                acc[b][lane] += (Acc)(m1 * w);
             }
-            ii += dq;
-            jj += dr;
+            if (in2) {
+                const float w = expf(-(float)(ii2 * ii2 + jj2 * jj2) / den);
+                int b = (int)rintf(a2 * 0.1f);
+                if (b >= ORI_BINS) b -= ORI_BINS;
+                if (b < 0) b += ORI_BINS;
+                acc[b][lane] += (Acc)(m2 * w);
+            }
+            ii = ii2 + dq;
+            jj = jj2 + dr;
             if (jj > rad) {
                 jj -= W;
                 ++ii;
@@ -231,9 +247,23 @@ __global__ void __launch_bounds__(DW * 32) k_describe(const float* __restrict__ 
                 const int j0 = max(ja, jc), j1 = min(jb, jd);
                 const float* mrow = MAG + gb + (long long)y * cols;
                 const float* arow = ANG + gb + (long long)y * cols;
-                for (int jj = j0; jj <= j1; ++jj) {
+                // four pixels per step: their gradient loads are issued before any is used, the
+                // accumulation order stays pixel by pixel
+                for (int jb = j0; jb <= j1; jb += 4) {
+                float mv4[4], av4[4];
+#pragma unroll
+                for (int u = 0; u < 4; ++u) {
+                    const int x = pc + jb + u;
+                    const bool in = jb + u <= j1 && x > 0 && x < cols - 1;
+                    mv4[u] = in ? __ldg(mrow + x) : 0.f;
+                    av4[u] = in ? __ldg(arow + x) : 0.f;
+                }
+#pragma unroll
+                for (int u = 0; u < 4; ++u) {
+                    const int jj = jb + u;
                     const int x = pc + jj;
-                    if (!(x > 0 && x < cols - 1)) continue;
+                    if (!(jj <= j1 && x > 0 && x < cols - 1)) continue;
+                    const float mval = mv4[u], aval = av4[u];
                     Acc v[8];
                     int o0;
                     if (EXACT) {
@@ -244,8 +274,8 @@ __global__ void __launch_bounds__(DW * 32) k_describe(const float* __restrict__ 
                         const double fr = floor(rbin), fc = floor(cbin);
                         if ((int)fr != Rq || (int)fc != Cq) continue;
                         const double w = exp((c_rot * c_rot + r_rot * r_rot) * (-1.0 / 8.0));
-                        const double m = (double)mrow[x] * w;
-                        const double obin = ((double)arow[x] - ori) * (8.0 / 360.0);
+                        const double m = (double)mval * w;
+                        const double obin = ((double)aval - ori) * (8.0 / 360.0);
                         const double fo = floor(obin);
                         const double rb = rbin - fr, cb = cbin - fc, ob = obin - fo;
                         o0 = (int)fo;
@@ -264,8 +294,8 @@ __global__ void __launch_bounds__(DW * 32) k_describe(const float* __restrict__ 
                         const float fr = floorf(rbin), fc = floorf(cbin);
                         if ((int)fr != Rq || (int)fc != Cq) continue;
                         const float w = expf((c_rot * c_rot + r_rot * r_rot) * (-1.f / 8.f));
-                        const float m = mrow[x] * w;
-                        const float obin = (arow[x] - ori_f) * (8.f / 360.f);
+                        const float m = mval * w;
+                        const float obin = (aval - ori_f) * (8.f / 360.f);
                         const float fo = floorf(obin);
                         const float rb = rbin - fr, cb = cbin - fc, ob = obin - fo;
                         o0 = (int)fo;
@@ -286,6 +316,7 @@ __global__ void __launch_bounds__(DW * 32) k_describe(const float* __restrict__ 
                         acc[c4 * NB + o0][lane] += v[2 * c4];
                         acc[c4 * NB + o0 + 1][lane] += v[2 * c4 + 1];
                     }
+                }
                 }
             }
         }
