@@ -49,13 +49,13 @@ size_t Workspace::bytes() const {
                keys_a.bytes + keys_b.bytes + vals_a.bytes + vals_b.bytes + sort_tmp.bytes + counters.bytes +
                kx.bytes + ky.bytes + ksize.bytes + kangle.bytes + kresp.bytes + koct.bytes + klayer.bytes;
     for (const auto& b : plane) t += b.bytes;
-    return t;
+    return t + next_base.bytes;
 }
 
 void Workspace::release() {
     DevBuf* all[] = {&dog, &mag, &ang, &img, &cand, &refined, &oriented, &keys_a, &keys_b, &vals_a, &vals_b,
                      &sort_tmp, &counters, &kx, &ky, &ksize, &kangle, &kresp, &koct, &klayer,
-                     &plane[0], &plane[1], &plane[2]};
+                     &plane[0], &plane[1], &plane[2], &next_base};
     for (DevBuf* b : all) b->release();
 }
 
@@ -69,6 +69,7 @@ static int32_t prepare_workspace(Workspace& ws, int h, int w) {
     FSB_TRY(ws.mag.ensure(3 * sum * 4));
     FSB_TRY(ws.ang.ensure(3 * sum * 4));
     for (auto& b : ws.plane) FSB_TRY(b.ensure(p0 * 4));
+    if (g.n_oct > 1) FSB_TRY(ws.next_base.ensure(2 * (((size_t)g.R[1] * g.C[1] + 63) / 64 * 64) * 4));
     FSB_TRY(ws.img.ensure((size_t)h * w));
     if (ws.cap_cand < 65536) ws.cap_cand = 65536;
     if (ws.cap_cand < sum / 64) ws.cap_cand = sum / 64;

@@ -5,7 +5,8 @@
 // (kernel and size) is met on a device, autotune() runs every variant twice on the caller's
 // stream (warm-up, then timed with CUDA events) and keeps the fastest; later calls run the kept
 // variant directly. Because the variants agree bit for bit and the runs are idempotent, tuning
-// inside a real call leaves that call's outputs as they would have been.
+// inside a real call leaves that call's outputs as they would have been. A variant may itself call
+// autotune() for its own launches (the lock is never held while a variant runs).
 //   FSB_AUTOTUNE=0          always variant 0 (no timing)
 //   FSB_AUTOTUNE_FILE=path  choices are read from and appended to `path` ("key variant" lines)
 #include <cstdlib>
@@ -68,14 +69,16 @@ int32_t autotune(const char* key, int n_variants, int32_t (*run)(void*, int), vo
     *variant = 0;
     if (n_variants <= 1 || !tuning_on()) return run(arg, 0);
     const std::string k = full_key(key);
+    int cached = -1;
     {
         std::lock_guard<std::mutex> lk(g_mu);
         load_locked();
         auto it = g_best.find(k);
-        if (it != g_best.end()) {
-            *variant = it->second < n_variants ? it->second : 0;
-            return run(arg, *variant);
-        }
+        if (it != g_best.end()) cached = it->second < n_variants ? it->second : 0;
+    }
+    if (cached >= 0) {   // run outside the lock: a variant may tune its own launches
+        *variant = cached;
+        return run(arg, cached);
     }
     cudaEvent_t e0, e1;
     FSB_CUDA(cudaEventCreate(&e0));

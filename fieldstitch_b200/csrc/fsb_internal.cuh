@@ -116,6 +116,7 @@ struct Workspace {
     Geometry g{};
     DevBuf dog, mag, ang;        // atlases
     DevBuf plane[3];             // gauss-layer scratch planes (octave-0 size)
+    DevBuf next_base;            // two octave-1-sized halves: the next octave's base, alternating
     DevBuf img;                  // uploaded uint8 image
     DevBuf cand, refined, oriented;
     DevBuf keys_a, keys_b, vals_a, vals_b, sort_tmp;
@@ -177,6 +178,9 @@ int layer_tile_height(int variant);
 int32_t launch_layer_fast(int layer, const float* src, int R, int C, float* dst, float* dog, float* mag, float* ang,
                           float* down, int down_cols, int variant, cudaStream_t s);
 int32_t launch_base_fast(const uint8_t* img, int stride, int ih, int iw, float* dst, int variant, cudaStream_t s);
+int32_t launch_group_lower(const float* src, int R, int C, float* dog, float* mag, float* ang, float* l3, float* down,
+                           int down_cols, cudaStream_t s);
+int32_t launch_group_upper(const float* src, int R, int C, float* dog3, cudaStream_t s);
 // autotune.cu: the fastest of n_variants launches of `run` for `key` (timed once per process and
 // device on `s`, then cached; FSB_AUTOTUNE=0 returns variant 0, FSB_AUTOTUNE_FILE persists choices)
 int32_t autotune(const char* key, int n_variants, int32_t (*run)(void*, int), void* arg, cudaStream_t s, int* variant);

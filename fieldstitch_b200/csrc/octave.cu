@@ -65,6 +65,10 @@ struct Args {
     int down_cols;
 };
 
+// 16-byte alignment of a plane address: the atlases pack octaves back to back, so an octave's
+// planes can start off a 16-byte boundary even when its width is a multiple of 4
+__device__ __forceinline__ bool al16(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15) == 0; }
+
 __device__ __forceinline__ int mir(int p, int n) {
     if (n == 1) return 0;
     while (p < 0 || p >= n) p = p < 0 ? -p : 2 * n - 2 - p;
@@ -123,6 +127,33 @@ __device__ __forceinline__ float2 blur_pairs_t(const float2* x) {
 }
 template <int I>
 __device__ __forceinline__ float2 blur_pairs(const float2* x) { return blur_pairs_t<I, RAD(I)>(x); }
+
+// tap set TS held in registers for a whole pass (the empty asm keeps the compiler from re-reading
+// the constant bank at every packed FMA, which takes no constant operand)
+template <int TS, int r>
+__device__ __forceinline__ void load_taps(float2 (&w)[r + 1]) {
+#pragma unroll
+    for (int j = 0; j <= r; ++j) {
+        float2 t = c_tap2[TS][j];
+        asm volatile("" : "+f"(t.x), "+f"(t.y));
+        w[j] = t;
+    }
+}
+// blur_pairs_t with the taps in registers: the same operations in the same order
+template <int r>
+__device__ __forceinline__ float2 blur_pairs_w(const float2* x, const float2 (&w)[r + 1]) {
+    float2 a = __fmul2_rn(x[r], w[0]);
+    float2 b = make_float2(0.f, 0.f);
+#pragma unroll
+    for (int j = r; j >= 1; --j) {
+        const float2 p = __fadd2_rn(x[r - j], x[r + j]);
+        if (j & 1)
+            b = __ffma2_rn(p, w[j], b);
+        else
+            a = __ffma2_rn(p, w[j], a);
+    }
+    return __fadd2_rn(a, b);
+}
 
 // rows yb, yb+1 (row pair rp) .. of L_I from L_{I-1} rows in `ring`; thread = (column pair, row pair)
 template <int I>
@@ -193,6 +224,27 @@ __device__ __forceinline__ void fast_grad(float dx, float dy, float& mag, float&
     ang = a;
 }
 
+// Gradient magnitude and angle at image row yy, columns x .. x+3, from a shared plane of pitch P
+// (ctr points at (yy, x); the column left of x and right of x + 3 and the rows above and below are
+// held): dx = right - left, dy = above - below, both zero on the image border as in the reference.
+// One border test per group of four columns; the per-column test only where the group touches it.
+template <int P>
+__device__ __forceinline__ void grad4(const float* ctr, int yy, int x, int R, int C, float (&mg)[4], float (&an)[4]) {
+    const float4 cc = *reinterpret_cast<const float4*>(ctr);
+    const float4 up = *reinterpret_cast<const float4*>(ctr - P);
+    const float4 dn = *reinterpret_cast<const float4*>(ctr + P);
+    const float lf = ctr[-1], rt = ctr[4];
+    float dx[4] = {__fsub_rn(cc.y, lf), __fsub_rn(cc.z, cc.x), __fsub_rn(cc.w, cc.y), __fsub_rn(rt, cc.z)};
+    float dy[4] = {__fsub_rn(up.x, dn.x), __fsub_rn(up.y, dn.y), __fsub_rn(up.z, dn.z), __fsub_rn(up.w, dn.w)};
+    if (!(yy > 0 && yy < R - 1 && x > 0 && x + 4 < C)) {
+#pragma unroll
+        for (int k = 0; k < 4; ++k)
+            if (!(yy > 0 && yy < R - 1 && x + k > 0 && x + k < C - 1)) dx[k] = dy[k] = 0.f;
+    }
+#pragma unroll
+    for (int k = 0; k < 4; ++k) fast_grad(dx[k], dy[k], mg[k], an[k]);
+}
+
 // DoG of stage I (L_I - L_{I-1}), gradient of L_{I-1} (I = 2..4), L_3[::2, ::2] (I = 4)
 template <int I>
 __device__ __forceinline__ void epilogue(const float* prev, const float* cur, const Args& a, int x0, int yb, int ybase,
@@ -214,7 +266,7 @@ __device__ __forceinline__ void epilogue(const float* prev, const float* cur, co
     const int at = y * a.C + xg;
     const bool vec = (a.C & 3) == 0 && xg + 4 <= a.C;
     float* dg = a.dog[I - 1] + at;
-    if (vec) {
+    if (vec && al16(dg)) {
         *reinterpret_cast<float4*>(dg) = make_float4(d[0], d[1], d[2], d[3]);
     } else {
         for (int k = 0; k < 4 && xg + k < a.C; ++k) dg[k] = d[k];
@@ -235,7 +287,7 @@ __device__ __forceinline__ void epilogue(const float* prev, const float* cur, co
         }
         float* m = a.mag[I - 2] + at;
         float* n = a.ang[I - 2] + at;
-        if (vec) {
+        if (vec && al16(m) && al16(n)) {
             *reinterpret_cast<float4*>(m) = make_float4(mg[0], mg[1], mg[2], mg[3]);
             *reinterpret_cast<float4*>(n) = make_float4(an[0], an[1], an[2], an[3]);
         } else {
@@ -267,7 +319,7 @@ __global__ void __launch_bounds__(NT, 2) k_octave(Args a) {
     const int ybase = ya - 128;                             // keeps every (row - ybase) positive
     const int g0 = ya - HALO;
     const int steps = (yz - ya + 2 * HALO + S - 1) / S;
-    const bool aligned = (a.C & 3) == 0 && x0 - X0 >= 0 && x0 - X0 + WIN(0) <= a.C;
+    const bool aligned = (a.C & 3) == 0 && al16(a.L0) && x0 - X0 >= 0 && x0 - X0 + WIN(0) <= a.C;
     load_rows(ring0, a, x0, g0, ybase, aligned);
     cp_commit();
     for (int t = 0; t < steps; ++t) {
@@ -352,69 +404,117 @@ __global__ void __launch_bounds__(LNT) k_layer(LayerArgs a) {
     const int x0 = blockIdx.x * LX, y0 = blockIdx.y * LY;
     // input rows y0 - r .. y0 + LY + r - 1, columns x0 - 16 .. x0 + LX + 15 (reflect-101 outside)
     if (BASE) {
-        // Source rows / columns of every tile row / column (reflect-101 on the upsampled grid),
-        // then the row-interpolated values 0.75 a[iy] + 0.25 a[ny] of a window of source columns;
-        // each upsampled sample is 0.75 vc[ix] + 0.25 vc[nx] (gsift.py:90-102 rounding). Tables and
-        // window live in the row-pair area until the vertical pass needs it; a column outside the
-        // window (mirrored columns of an edge tile) is computed from global memory.
-        constexpr int VCW = 96;
-        static_assert(!BASE || (2 * IH + 2 * LIN_W) * 4 + IH * VCW * 4 <= (LY / 2) * LT2_W * 8,
+        // Source row / column pairs (iy, ny), (ix, nx) of every tile row / column (reflect-101 on
+        // the upsampled grid). The source block they reach is staged once as scaled floats p, the
+        // row-interpolated values vc = 0.75 p[iy] + 0.25 p[ny] are formed for every tile row over the
+        // block's columns, and each upsampled sample is 0.75 vc[ix] + 0.25 vc[nx], four columns per
+        // thread (gsift.py:90-102 rounding). Tables and vc live in the row-pair area and p in the
+        // input tile until the vertical pass needs them. A block larger than the staging window
+        // (mirror images of a tiny image) takes the per-sample global path.
+        constexpr int VCW = 96, SRW = IH / 2 + 4;
+        static_assert(!BASE || (2 * IH + 2 * LIN_W) * 4 + IH * VCW * 4 + 16 <= (LY / 2) * LT2_W * 8,
                       "base tables must fit the row-pair area");
-        int* rtab = reinterpret_cast<int*>(t2);
-        int* ctab = rtab + 2 * IH;
-        float* vcs = reinterpret_cast<float*>(ctab + 2 * LIN_W);
-        const int right = min(x0 + LX + 15, a.C - 1);
-        int lo = x0 - 16;
-        if (x0 + LX + 15 >= a.C) lo = min(lo, 2 * a.C - 2 - (x0 + LX + 15));
-        const int sx0 = max(0, (lo >> 1) - 1);
-        const int nsx = min(min(a.iw - 1, (right >> 1) + 1) - sx0 + 1, VCW);
-        for (int i = tid; i < IH + LIN_W; i += LNT) {
+        static_assert(!BASE || (SRW * VCW <= IH * LIN_W && IH % 2 == 0), "staged source block");
+        int* ry = reinterpret_cast<int*>(t2);   // iy of tile row i, then ny
+        int* rn = ry + IH;
+        int* cxs = rn + IH;                      // ix of tile column c, then nx (16-byte aligned)
+        int* cns = cxs + LIN_W;
+        float* vcs = reinterpret_cast<float*>(cns + LIN_W);
+        int* box = reinterpret_cast<int*>(vcs + IH * VCW);   // source row min / max, column min / max
+        float* ps = s_in;
+        if (tid < 4) box[tid] = (tid & 1) ? -1 : 0x7fffffff;
+        __syncthreads();
+        for (int i0 = 0; i0 < IH + LIN_W; i0 += LNT) {
+            const int i = i0 + tid;
+            int lo = 0x7fffffff, hi = -1, clo = 0x7fffffff, chi = -1;
             if (i < IH) {
                 const int Y = mir(y0 - r + i, a.R), iy = Y >> 1;
                 const int ny = (Y & 1) ? min(iy + 1, a.ih - 1) : max(iy - 1, 0);
-                rtab[2 * i] = iy * a.img_stride;
-                rtab[2 * i + 1] = ny * a.img_stride;
-            } else {
+                ry[i] = iy;
+                rn[i] = ny;
+                lo = min(iy, ny);
+                hi = max(iy, ny);
+            } else if (i < IH + LIN_W) {
                 const int c = i - IH, X = mir(x0 - 16 + c, a.C), ix = X >> 1;
                 const int nx = (X & 1) ? min(ix + 1, a.iw - 1) : max(ix - 1, 0);
-                ctab[2 * c] = ix;
-                ctab[2 * c + 1] = nx;
+                cxs[c] = ix;
+                cns[c] = nx;
+                clo = min(ix, nx);
+                chi = max(ix, nx);
+            }
+            lo = __reduce_min_sync(0xffffffffu, lo);
+            hi = __reduce_max_sync(0xffffffffu, hi);
+            clo = __reduce_min_sync(0xffffffffu, clo);
+            chi = __reduce_max_sync(0xffffffffu, chi);
+            if ((tid & 31) == 0) {
+                if (hi >= 0) {
+                    atomicMin(&box[0], lo);
+                    atomicMax(&box[1], hi);
+                }
+                if (chi >= 0) {
+                    atomicMin(&box[2], clo);
+                    atomicMax(&box[3], chi);
+                }
             }
         }
         __syncthreads();
+        const int sy0 = box[0], nsr = box[1] - box[0] + 1, sx0 = box[2], nsx = box[3] - box[2] + 1;
         const float sc = (float)(1.0 / 255.0);
-        for (int i = tid; i < IH * VCW; i += LNT) {
-            const int row = i / VCW, k = i - row * VCW;
-            if (k >= nsx) continue;
-            const float p0 = __fmul_rn((float)__ldg(a.img + rtab[2 * row] + sx0 + k), sc);
-            const float p1 = __fmul_rn((float)__ldg(a.img + rtab[2 * row + 1] + sx0 + k), sc);
-            vcs[row * VCW + k] = __fadd_rn(__fmul_rn(0.75f, p0), __fmul_rn(0.25f, p1));
-        }
-        __syncthreads();
-#pragma unroll 4
-        for (int i = tid; i < IH * LIN_W; i += LNT) {
-            const int row = i / LIN_W, col = i - row * LIN_W;
-            const int ix = ctab[2 * col], nx = ctab[2 * col + 1];
-            const int kx = ix - sx0, kn = nx - sx0;
-            float vc, vn;
-            if (kx >= 0 && kx < nsx && kn >= 0 && kn < nsx) {
-                vc = vcs[row * VCW + kx];
-                vn = vcs[row * VCW + kn];
-            } else {
-                const uint8_t* r0 = a.img + rtab[2 * row];
-                const uint8_t* r1 = a.img + rtab[2 * row + 1];
-                vc = __fadd_rn(__fmul_rn(0.75f, __fmul_rn((float)__ldg(r0 + ix), sc)),
-                               __fmul_rn(0.25f, __fmul_rn((float)__ldg(r1 + ix), sc)));
-                vn = __fadd_rn(__fmul_rn(0.75f, __fmul_rn((float)__ldg(r0 + nx), sc)),
-                               __fmul_rn(0.25f, __fmul_rn((float)__ldg(r1 + nx), sc)));
+        if (nsr <= SRW && nsx <= VCW) {
+            for (int row = tid >> 5; row < nsr; row += LNT / 32) {
+                const uint8_t* src = a.img + (size_t)(sy0 + row) * a.img_stride + sx0;
+                for (int k = tid & 31; k < nsx; k += 32) ps[row * VCW + k] = __fmul_rn((float)__ldg(src + k), sc);
             }
-            s_in[row * LIN_W + col] = __fadd_rn(__fmul_rn(0.75f, vc), __fmul_rn(0.25f, vn));
+            __syncthreads();
+            for (int i = tid; i < IH * (VCW / 4); i += LNT) {
+                const int row = i / (VCW / 4), q = 4 * (i - row * (VCW / 4));
+                if (q >= nsx) continue;
+                const float4 p0 = *reinterpret_cast<const float4*>(ps + (ry[row] - sy0) * VCW + q);
+                const float4 p1 = *reinterpret_cast<const float4*>(ps + (rn[row] - sy0) * VCW + q);
+                float4 v;
+                v.x = __fadd_rn(__fmul_rn(0.75f, p0.x), __fmul_rn(0.25f, p1.x));
+                v.y = __fadd_rn(__fmul_rn(0.75f, p0.y), __fmul_rn(0.25f, p1.y));
+                v.z = __fadd_rn(__fmul_rn(0.75f, p0.z), __fmul_rn(0.25f, p1.z));
+                v.w = __fadd_rn(__fmul_rn(0.75f, p0.w), __fmul_rn(0.25f, p1.w));
+                *reinterpret_cast<float4*>(vcs + row * VCW + q) = v;
+            }
+            __syncthreads();
+            for (int i = tid; i < IH * (LIN_W / 4); i += LNT) {
+                const int row = i / (LIN_W / 4), q = 4 * (i - row * (LIN_W / 4));
+                const int4 ix = *reinterpret_cast<const int4*>(cxs + q);
+                const int4 nx = *reinterpret_cast<const int4*>(cns + q);
+                const float* v = vcs + row * VCW - sx0;
+                float4 u;
+                u.x = __fadd_rn(__fmul_rn(0.75f, v[ix.x]), __fmul_rn(0.25f, v[nx.x]));
+                u.y = __fadd_rn(__fmul_rn(0.75f, v[ix.y]), __fmul_rn(0.25f, v[nx.y]));
+                u.z = __fadd_rn(__fmul_rn(0.75f, v[ix.z]), __fmul_rn(0.25f, v[nx.z]));
+                u.w = __fadd_rn(__fmul_rn(0.75f, v[ix.w]), __fmul_rn(0.25f, v[nx.w]));
+                *reinterpret_cast<float4*>(s_in + row * LIN_W + q) = u;
+            }
+        } else {
+            for (int i = tid; i < IH * LIN_W; i += LNT) {
+                const int row = i / LIN_W, col = i - row * LIN_W;
+                const uint8_t* r0 = a.img + (size_t)ry[row] * a.img_stride;
+                const uint8_t* r1 = a.img + (size_t)rn[row] * a.img_stride;
+                const int ix = cxs[col], nx = cns[col];
+                const float vc = __fadd_rn(__fmul_rn(0.75f, __fmul_rn((float)__ldg(r0 + ix), sc)),
+                                           __fmul_rn(0.25f, __fmul_rn((float)__ldg(r1 + ix), sc)));
+                const float vn = __fadd_rn(__fmul_rn(0.75f, __fmul_rn((float)__ldg(r0 + nx), sc)),
+                                           __fmul_rn(0.25f, __fmul_rn((float)__ldg(r1 + nx), sc)));
+                s_in[row * LIN_W + col] = __fadd_rn(__fmul_rn(0.75f, vc), __fmul_rn(0.25f, vn));
+            }
         }
-    } else if ((a.C & 3) == 0 && x0 >= 16 && x0 + LX + 16 <= a.C) {
-        for (int i = tid; i < IH * (LIN_W / 4); i += LNT) {
-            const int row = i / (LIN_W / 4), q = i - row * (LIN_W / 4);
-            const float* g = a.src + (size_t)mir(y0 - r + row, a.R) * a.C + (x0 - 16 + 4 * q);
-            cp_async16(s_in + row * LIN_W + 4 * q, g);
+    } else if ((a.C & 3) == 0 && al16(a.src) && x0 >= 16 && x0 + LX + 16 <= a.C) {
+        // eight lanes per row (the mirrored row address once per row), five 16-byte copies a lane
+        static_assert(LIN_W / 4 == 40, "five copies of eight lanes per row");
+        for (int row = tid >> 3; row < IH; row += LNT / 8) {
+            const float* g = a.src + (size_t)mir(y0 - r + row, a.R) * a.C + (x0 - 16);
+            float* d = s_in + row * LIN_W;
+#pragma unroll
+            for (int k = 0; k < 5; ++k) {
+                const int q = 4 * ((tid & 7) + 8 * k);
+                cp_async16(d + q, g + q);
+            }
         }
     } else {
         for (int i = tid; i < IH * LIN_W; i += LNT) {
@@ -428,6 +528,8 @@ __global__ void __launch_bounds__(LNT) k_layer(LayerArgs a) {
     __syncthreads();
     // vertical pass: column pair cp (V columns 2cp, 2cp+1 = image columns x0 - r - d + 2cp ..),
     // output rows 8g .. 8g + 7; stored row-pair interleaved at t2 index (V column + d)
+    float2 w[r + 1];
+    load_taps<TS, r>(w);
     for (int it = tid; it < NPAIR * (LY / 8); it += LNT) {
         const int cp = it % NPAIR, g = it / NPAIR;
         const float* base = s_in + (8 * g) * LIN_W + (16 - r - d + 2 * cp);
@@ -436,7 +538,7 @@ __global__ void __launch_bounds__(LNT) k_layer(LayerArgs a) {
         for (int k = 0; k < 8 + 2 * r; ++k) x[k] = *reinterpret_cast<const float2*>(base + k * LIN_W);
 #pragma unroll
         for (int sp = 0; sp < 4; ++sp) {
-            const float2 o0 = blur_pairs_t<TS, r>(x + 2 * sp), o1 = blur_pairs_t<TS, r>(x + 2 * sp + 1);
+            const float2 o0 = blur_pairs_w<r>(x + 2 * sp, w), o1 = blur_pairs_w<r>(x + 2 * sp + 1, w);
             float2* dst = t2 + (4 * g + sp) * LT2_W + 2 * cp + d;
             dst[0] = make_float2(o0.x, o1.x);
             dst[1] = make_float2(o0.y, o1.y);
@@ -458,7 +560,7 @@ __global__ void __launch_bounds__(LNT) k_layer(LayerArgs a) {
         }
         float2 o[4];
 #pragma unroll
-        for (int cc = 0; cc < 4; ++cc) o[cc] = blur_pairs_t<TS, r>(yv + cc);   // (row y, row y+1) at column x+cc
+        for (int cc = 0; cc < 4; ++cc) o[cc] = blur_pairs_w<r>(yv + cc, w);   // (row y, row y+1) at column x+cc
         const bool vec = (a.C & 3) == 0 && x + 4 <= a.C;
 #pragma unroll
         for (int h = 0; h < 2; ++h) {
@@ -467,10 +569,12 @@ __global__ void __launch_bounds__(LNT) k_layer(LayerArgs a) {
             const float lv[4] = {h ? o[0].y : o[0].x, h ? o[1].y : o[1].x, h ? o[2].y : o[2].x, h ? o[3].y : o[3].x};
             if (BASE) {
                 const size_t at = (size_t)yy * a.C + x;
-                if (vec) {
+                if (vec && al16(a.dst)) {
                     *reinterpret_cast<float4*>(a.dst + at) = make_float4(lv[0], lv[1], lv[2], lv[3]);
                 } else {
-                    for (int k = 0; k < 4 && x + k < a.C; ++k) a.dst[at + k] = lv[k];
+#pragma unroll
+                    for (int k = 0; k < 4; ++k)
+                        if (x + k < a.C) a.dst[at + k] = lv[k];
                 }
                 continue;
             }
@@ -481,31 +585,27 @@ __global__ void __launch_bounds__(LNT) k_layer(LayerArgs a) {
 #pragma unroll
             for (int k = 0; k < 4; ++k) dg[k] = lv[k] - pr[k];
             const size_t at = (size_t)yy * a.C + x;
-            if (vec) {
+            if (vec && al16(a.dog) && (!a.dst || al16(a.dst))) {
                 *reinterpret_cast<float4*>(a.dog + at) = make_float4(dg[0], dg[1], dg[2], dg[3]);
                 if (a.dst) *reinterpret_cast<float4*>(a.dst + at) = make_float4(lv[0], lv[1], lv[2], lv[3]);
             } else {
-                for (int k = 0; k < 4 && x + k < a.C; ++k) {
+#pragma unroll
+                for (int k = 0; k < 4; ++k) {
+                    if (x + k >= a.C) break;
                     a.dog[at + k] = dg[k];
                     if (a.dst) a.dst[at + k] = lv[k];
                 }
             }
             if (a.mag) {
                 float mg[4], an[4];
-#pragma unroll
-                for (int k = 0; k < 4; ++k) {
-                    float dx = 0.f, dy = 0.f;
-                    if (yy > 0 && yy < a.R - 1 && x + k > 0 && x + k < a.C - 1) {
-                        dx = __fsub_rn(ctr[k + 1], ctr[k - 1]);
-                        dy = __fsub_rn(ctr[k - LIN_W], ctr[k + LIN_W]);
-                    }
-                    fast_grad(dx, dy, mg[k], an[k]);
-                }
-                if (vec) {
+                grad4<LIN_W>(ctr, yy, x, a.R, a.C, mg, an);
+                if (vec && al16(a.mag) && al16(a.ang)) {
                     *reinterpret_cast<float4*>(a.mag + at) = make_float4(mg[0], mg[1], mg[2], mg[3]);
                     *reinterpret_cast<float4*>(a.ang + at) = make_float4(an[0], an[1], an[2], an[3]);
                 } else {
-                    for (int k = 0; k < 4 && x + k < a.C; ++k) {
+#pragma unroll
+                    for (int k = 0; k < 4; ++k) {
+                        if (x + k >= a.C) break;
                         a.mag[at + k] = mg[k];
                         a.ang[at + k] = an[k];
                     }
@@ -551,6 +651,307 @@ int32_t launch_layer_t(const LayerArgs& a, int variant, cudaStream_t s) {
             default: return launch_layer_ly<TS, r, BASE, 32>(a, s);
         }
     }
+}
+
+// ------------------------------------------------------------------------------------------------
+// Fused layer groups (float32 path): one persistent kernel computes consecutive layers of an
+// octave for 128 x 32 output tiles,
+//   group 0: L1, L2, L3 from L0 -> DoG 0..2, gradients of L1..L3, L3 and L3[::2, ::2]
+//   group 1: L4, L5 from L3     -> DoG 3, 4
+// Every level is held in shared memory on the tile plus the halo the levels above it need (row
+// halo GH, column halo GXH; recomputed per tile), so the intermediate layers never reach HBM:
+// per octave pixel the two launches read L0 and L3 and write the five DoG planes, six gradient
+// planes, L3 and the downsample (14.25 octave planes of traffic where five per-layer launches move
+// 20.25). Halo values outside the image equal the reflect-101 mirror of the values inside: the
+// blur of a mirror-symmetric signal is mirror-symmetric and the pair sums of blur_pairs_t commute,
+// so each level reproduces the per-layer kernels' values bit for bit. The passes are the per-layer
+// kernel's (8-row register window of column pairs; row-pair-interleaved horizontal pass), with
+// the DoG / gradient epilogue of a level run by the horizontal pass of the level above it. One
+// CTA per SM walks the tiles; the next tile's input arrives by cp.async while this one computes.
+constexpr int GX = 128, GY = 32, GNT = 512;
+
+__host__ __device__ constexpr int cmax(int a, int b) { return a > b ? a : b; }
+
+// One level of a group: the output level (row halo Ho, column halo Xo) blurred with radius r from
+// the level below (Hi, Xi). The vertical pass covers input columns VS .. VS + VW - 1 (VS even);
+// column j of its output sits at float2 index j + E of a row pair, so the horizontal pass's
+// 16-byte loads start on an even index.
+template <int Hi, int Xi, int Ho, int Xo, int r>
+struct GLevel {
+    static constexpr int HIN = Hi, XIN = Xi, HOUT = Ho, XOUT = Xo, RAD = r;
+    static constexpr int NIN = GY + 2 * Hi, MIN = GX + 2 * Xi;     // input rows, columns (= pitch)
+    static constexpr int NOUT = GY + 2 * Ho, MOUT = GX + 2 * Xo;   // output rows, columns (= pitch)
+    static constexpr int ROFF = Hi - Ho - r;                       // input row of output row 0's first tap
+    static constexpr int OFF = Xi - Xo - r;                        // input column of output column 0's first tap
+    static constexpr int E = OFF & 1;
+    static constexpr int VS = OFF - E;
+    static constexpr int VW = (MOUT + 2 * r + E + 1) & ~1;
+    static constexpr int VP = (VW + E + 1) & ~1;                   // float2 per row pair
+    static constexpr int V_FLOATS = (NOUT / 2) * VP * 2;
+    static constexpr int IN_FLOATS = NIN * MIN, OUT_FLOATS = NOUT * MOUT;
+    static_assert(ROFF >= 0 && OFF >= 0 && Xi % 4 == 0 && Xo % 4 == 0, "level geometry");
+    static_assert(VS + VW <= MIN, "vertical pass inside the input level");
+};
+
+template <int G>
+struct GSpec;
+template <>
+struct GSpec<0> {
+    using A = GLevel<20, 28, 15, 20, 5>;   // L0 -> L1
+    using B = GLevel<15, 20, 9, 12, 6>;    // L1 -> L2
+    using C = GLevel<9, 12, 1, 4, 8>;      // L2 -> L3 (halo 1: gradient of L3)
+    static constexpr int BUF0 = (cmax(A::IN_FLOATS, cmax(B::V_FLOATS, C::V_FLOATS)) + 3) & ~3;   // L0 / V2 / V3
+    static constexpr int BUF1 = (cmax(A::V_FLOATS, B::OUT_FLOATS) + 3) & ~3;                     // V1 / L2
+    static constexpr int BUF2 = (cmax(A::OUT_FLOATS, C::OUT_FLOATS) + 3) & ~3;                   // L1 / L3
+};
+template <>
+struct GSpec<1> {
+    using A = GLevel<23, 28, 13, 16, 10>;   // L3 -> L4
+    using B = GLevel<13, 16, 0, 0, 13>;     // L4 -> L5 (tile only)
+    static constexpr int BUF0 = (cmax(A::IN_FLOATS, B::V_FLOATS) + 3) & ~3;   // L3 / V5
+    static constexpr int BUF1 = (A::V_FLOATS + 3) & ~3;                       // V4
+    static constexpr int BUF2 = (A::OUT_FLOATS + 3) & ~3;                     // L4
+};
+// two input buffers (this tile's, the next tile's) and the two others
+template <int G>
+constexpr int group_smem() {
+    return (2 * GSpec<G>::BUF0 + GSpec<G>::BUF1 + GSpec<G>::BUF2) * 4;
+}
+static_assert(group_smem<0>() <= 227 * 1024 && group_smem<1>() <= 227 * 1024, "group shared memory");
+
+struct GroupArgs {
+    const float* src;   // the group's input level, R x C
+    int R, C;
+    int tiles_x, n_tiles;
+    float* dog[3];      // DoG planes of the group's layers
+    float* mag[3];      // group 0: gradients of L1, L2, L3
+    float* ang[3];
+    float* dst;         // group 0: L3
+    float* down;        // group 0: L3[::2, ::2] or null
+    int down_cols;
+};
+
+// input level of tile t (rows y0 - HIN .., columns x0 - XIN .., reflect-101 outside) by cp.async
+template <class L>
+__device__ __forceinline__ void g_load(const GroupArgs& a, int t, float* dst) {
+    const int y0 = (t / a.tiles_x) * GY, cx = (t % a.tiles_x) * GX - L::XIN;
+    if ((a.C & 3) == 0 && al16(a.src) && cx >= 0 && cx + L::MIN <= a.C) {
+        // eight lanes per row (the mirrored row address once per row)
+        for (int row = threadIdx.x >> 3; row < L::NIN; row += GNT / 8) {
+            const float* g = a.src + (size_t)mir(y0 - L::HIN + row, a.R) * a.C + cx;
+#pragma unroll
+            for (int k = 0; k < (L::MIN / 4 + 7) / 8; ++k) {
+                const int q = (threadIdx.x & 7) + 8 * k;
+                if (q < L::MIN / 4) cp_async16(dst + row * L::MIN + 4 * q, g + 4 * q);
+            }
+        }
+    } else {
+        for (int i = threadIdx.x; i < L::NIN * L::MIN; i += GNT) {
+            const int row = i / L::MIN, col = i - row * L::MIN;
+            cp_async4(dst + row * L::MIN + col, a.src + (size_t)mir(y0 - L::HIN + row, a.R) * a.C + mir(cx + col, a.C));
+        }
+    }
+}
+
+// vertical pass of level L: thread item = (column pair, 8 output rows); the last group of a level
+// whose height is not a multiple of 8 starts at row NOUT - 8 (rows it shares with the group before
+// are written twice with the same values), so every load stays inside the input level
+template <int TS, class L>
+__device__ __forceinline__ void g_vpass(const float* __restrict__ pin, float2* __restrict__ v) {
+    constexpr int r = L::RAD, NQ = L::VW / 2, NG = (L::NOUT + 7) / 8;
+    static_assert(L::NOUT >= 8 && L::NIN == L::NOUT + 2 * r + 2 * L::ROFF, "vertical pass rows");
+    float2 w[r + 1];
+    load_taps<TS, r>(w);
+    for (int it = threadIdx.x; it < NQ * NG; it += GNT) {
+        const int q = it % NQ, g = it / NQ;
+        const int y8 = min(8 * g, L::NOUT - 8);
+        const float* base = pin + (y8 + L::ROFF) * L::MIN + L::VS + 2 * q;
+        float2 x[8 + 2 * r];
+#pragma unroll
+        for (int k = 0; k < 8 + 2 * r; ++k) x[k] = *reinterpret_cast<const float2*>(base + k * L::MIN);
+        float2* d = v + (y8 / 2) * L::VP + 2 * q + L::E;
+#pragma unroll
+        for (int sp = 0; sp < 4; ++sp) {
+            const float2 o0 = blur_pairs_w<r>(x + 2 * sp, w), o1 = blur_pairs_w<r>(x + 2 * sp + 1, w);
+            d[sp * L::VP] = make_float2(o0.x, o1.x);
+            d[sp * L::VP + 1] = make_float2(o0.y, o1.y);
+        }
+    }
+}
+
+// horizontal pass of level L: thread item = (row pair, 4 columns); the level's rows go to `pout`
+// (when not null) and epi(tile row of the upper row, tile column, upper row, lower row) runs for
+// every item (it checks the tile bounds itself)
+template <int TS, class L, class Epi>
+__device__ __forceinline__ void g_hpass(const float2* __restrict__ v, float* __restrict__ pout, Epi epi) {
+    constexpr int r = L::RAD, NC = L::MOUT / 4, NP = L::NOUT / 2;
+    float2 w[r + 1];
+    load_taps<TS, r>(w);
+    for (int it = threadIdx.x; it < NP * NC; it += GNT) {
+        const int p = it / NC, c = 4 * (it - p * NC);
+        const float4* src = reinterpret_cast<const float4*>(v + p * L::VP + c + 2 * L::E);
+        float2 yv[4 + 2 * r];
+#pragma unroll
+        for (int k = 0; k < 2 + r; ++k) {
+            const float4 t = src[k];
+            yv[2 * k] = make_float2(t.x, t.y);
+            yv[2 * k + 1] = make_float2(t.z, t.w);
+        }
+        float2 o[4];
+#pragma unroll
+        for (int cc = 0; cc < 4; ++cc) o[cc] = blur_pairs_w<r>(yv + cc, w);
+        const float4 top = make_float4(o[0].x, o[1].x, o[2].x, o[3].x);
+        const float4 bot = make_float4(o[0].y, o[1].y, o[2].y, o[3].y);
+        if (pout) {
+            *reinterpret_cast<float4*>(pout + (2 * p) * L::MOUT + c) = top;
+            *reinterpret_cast<float4*>(pout + (2 * p + 1) * L::MOUT + c) = bot;
+        }
+        epi(2 * p - L::HOUT, c - L::XOUT, top, bot);
+    }
+}
+
+__device__ __forceinline__ void g_store4(float* p, float4 v, bool vec, int left) {
+    if (vec && al16(p)) {
+        *reinterpret_cast<float4*>(p) = v;
+    } else {
+        const float w[4] = {v.x, v.y, v.z, v.w};
+        for (int k = 0; k < 4 && k < left; ++k) p[k] = w[k];
+    }
+}
+
+// at image row yy, columns xx .. xx + 3: the DoG cur - prev and, with mag set, the gradient of
+// prev (prev points at prev(yy, xx) in a shared level of pitch P; the same arithmetic as k_layer)
+template <int P>
+__device__ __forceinline__ void g_dog_grad(const GroupArgs& a, int yy, int xx, const float* prev, float4 cur,
+                                           float* dog, float* mag, float* ang) {
+    const float4 pv = *reinterpret_cast<const float4*>(prev);
+    const size_t at = (size_t)yy * a.C + xx;
+    const bool vec = (a.C & 3) == 0;   // xx is a multiple of 4 below C
+    g_store4(dog + at, make_float4(cur.x - pv.x, cur.y - pv.y, cur.z - pv.z, cur.w - pv.w), vec, a.C - xx);
+    if (mag) {
+        float mg[4], an[4];
+        grad4<P>(prev, yy, xx, a.R, a.C, mg, an);
+        g_store4(mag + at, make_float4(mg[0], mg[1], mg[2], mg[3]), vec, a.C - xx);
+        g_store4(ang + at, make_float4(an[0], an[1], an[2], an[3]), vec, a.C - xx);
+    }
+}
+
+// epilogue of a level: for the tile pixels of an item, DoG (this level - prev) and the gradient of
+// prev, prev being the shared level (halo PH, PX, pitch P) below
+template <int PH, int PX, int P>
+struct GEpi {
+    const GroupArgs& a;
+    int y0, x0;
+    const float* prev;
+    float *dog, *mag, *ang;
+    __device__ __forceinline__ void operator()(int ty, int tx, float4 top, float4 bot) const {
+        if (tx < 0 || tx >= GX || x0 + tx >= a.C) return;
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            const int t = ty + h;
+            if (t < 0 || t >= GY || y0 + t >= a.R) continue;
+            g_dog_grad<P>(a, y0 + t, x0 + tx, prev + (PH + t) * P + PX + tx, h ? bot : top, dog, mag, ang);
+        }
+    }
+};
+
+template <int G>
+__global__ void __launch_bounds__(GNT, 1) k_group(GroupArgs a) {
+    using Sp = GSpec<G>;
+    using LA = typename Sp::A;
+    extern __shared__ __align__(16) float sm[];
+    float* b1 = sm + 2 * Sp::BUF0;
+    float* b2 = b1 + Sp::BUF1;
+    int t = blockIdx.x;
+    if (t >= a.n_tiles) return;
+    g_load<LA>(a, t, sm);
+    cp_commit();
+    for (int cur = 0; t < a.n_tiles; t += gridDim.x, cur ^= 1) {
+        cp_wait_all();
+        __syncthreads();   // this tile's input is in; every thread is done with the previous tile
+        const int nt = t + gridDim.x;
+        if (nt < a.n_tiles) g_load<LA>(a, nt, sm + (cur ^ 1) * Sp::BUF0);
+        cp_commit();
+        const int y0 = (t / a.tiles_x) * GY, x0 = (t % a.tiles_x) * GX;
+        float* b0 = sm + cur * Sp::BUF0;
+        if constexpr (G == 0) {
+            using LB = typename Sp::B;
+            using LC = typename Sp::C;
+            g_vpass<1, LA>(b0, reinterpret_cast<float2*>(b1));                                   // L0 -> V1
+            __syncthreads();
+            g_hpass<1, LA>(reinterpret_cast<const float2*>(b1), b2,                               // V1 -> L1
+                           GEpi<LA::HIN, LA::XIN, LA::MIN>{a, y0, x0, b0, a.dog[0], nullptr, nullptr});
+            __syncthreads();
+            g_vpass<2, LB>(b2, reinterpret_cast<float2*>(b0));                                   // L1 -> V2
+            __syncthreads();
+            g_hpass<2, LB>(reinterpret_cast<const float2*>(b0), b1,                               // V2 -> L2
+                           GEpi<LB::HIN, LB::XIN, LB::MIN>{a, y0, x0, b2, a.dog[1], a.mag[0], a.ang[0]});
+            __syncthreads();
+            g_vpass<3, LC>(b1, reinterpret_cast<float2*>(b0));                                   // L2 -> V3
+            __syncthreads();
+            g_hpass<3, LC>(reinterpret_cast<const float2*>(b0), b2,                               // V3 -> L3
+                           GEpi<LC::HIN, LC::XIN, LC::MIN>{a, y0, x0, b1, a.dog[2], a.mag[1], a.ang[1]});
+            __syncthreads();
+            // gradient of L3, L3 and L3[::2, ::2] on the tile
+            for (int it = threadIdx.x; it < GY * (GX / 4); it += GNT) {
+                const int ty = it / (GX / 4), tx = 4 * (it - ty * (GX / 4));
+                const int yy = y0 + ty, xx = x0 + tx;
+                if (yy >= a.R || xx >= a.C) continue;
+                const float* l3 = b2 + (LC::HOUT + ty) * LC::MOUT + LC::XOUT + tx;
+                const float4 v = *reinterpret_cast<const float4*>(l3);
+                float mg[4], an[4];
+                grad4<LC::MOUT>(l3, yy, xx, a.R, a.C, mg, an);
+                const size_t at = (size_t)yy * a.C + xx;
+                const bool vec = (a.C & 3) == 0;
+                g_store4(a.mag[2] + at, make_float4(mg[0], mg[1], mg[2], mg[3]), vec, a.C - xx);
+                g_store4(a.ang[2] + at, make_float4(an[0], an[1], an[2], an[3]), vec, a.C - xx);
+                g_store4(a.dst + at, v, vec, a.C - xx);
+                if (a.down && !(yy & 1)) {
+                    float* o2 = a.down + (size_t)(yy >> 1) * a.down_cols + (xx >> 1);
+                    o2[0] = v.x;
+                    if (xx + 2 < a.C) o2[1] = v.z;
+                }
+            }
+        } else {
+            using LB = typename Sp::B;
+            g_vpass<4, LA>(b0, reinterpret_cast<float2*>(b1));                                   // L3 -> V4
+            __syncthreads();
+            g_hpass<4, LA>(reinterpret_cast<const float2*>(b1), b2,                               // V4 -> L4
+                           GEpi<LA::HIN, LA::XIN, LA::MIN>{a, y0, x0, b0, a.dog[0], nullptr, nullptr});
+            __syncthreads();
+            g_vpass<5, LB>(b2, reinterpret_cast<float2*>(b0));                                   // L4 -> V5
+            __syncthreads();
+            g_hpass<5, LB>(reinterpret_cast<const float2*>(b0), nullptr,                          // V5 -> L5
+                           GEpi<LB::HIN, LB::XIN, LB::MIN>{a, y0, x0, b2, a.dog[1], nullptr, nullptr});
+        }
+    }
+    cp_wait_all();
+}
+
+int sm_count() {
+    static int n[64] = {};
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev >= 64) return 148;
+    if (!n[dev] && cudaDeviceGetAttribute(&n[dev], cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) n[dev] = 148;
+    return n[dev];
+}
+
+template <int G>
+int32_t launch_group_t(GroupArgs a, cudaStream_t s) {
+    static bool attr[64] = {};
+    int dev = 0;
+    FSB_CUDA(cudaGetDevice(&dev));
+    if (dev < 64 && !attr[dev]) {
+        FSB_CUDA(cudaFuncSetAttribute(k_group<G>, cudaFuncAttributeMaxDynamicSharedMemorySize, group_smem<G>()));
+        attr[dev] = true;
+    }
+    a.tiles_x = (a.C + GX - 1) / GX;
+    a.n_tiles = a.tiles_x * ((a.R + GY - 1) / GY);
+    const int grid = a.n_tiles < sm_count() ? a.n_tiles : sm_count();
+    k_group<G><<<grid, GNT, group_smem<G>(), s>>>(a);
+    note_launch();
+    FSB_CUDA(cudaGetLastError());
+    return FSB_OK;
 }
 
 }  // namespace
@@ -620,6 +1021,39 @@ int32_t launch_layer_fast(int layer, const float* src, int R, int C, float* dst,
     }
 }
 
+
+// Layers 1..3 of a float32 octave by the fused group kernel: from L0 (src, R x C), DoG planes
+// 0..2 at dog, dog + RC, dog + 2RC, gradients of L1..L3 at mag / ang (+ RC, + 2RC), L3 to l3 and
+// L3[::2, ::2] to down (null: last octave). down must not alias src (other tiles still read it).
+int32_t launch_group_lower(const float* src, int R, int C, float* dog, float* mag, float* ang, float* l3, float* down,
+                           int down_cols, cudaStream_t s) {
+    const long long RC = (long long)R * C;
+    GroupArgs a{};
+    a.src = src;
+    a.R = R;
+    a.C = C;
+    for (int k = 0; k < 3; ++k) {
+        a.dog[k] = dog + k * RC;
+        a.mag[k] = mag + k * RC;
+        a.ang[k] = ang + k * RC;
+    }
+    a.dst = l3;
+    a.down = down;
+    a.down_cols = down_cols;
+    return launch_group_t<0>(a, s);
+}
+
+// Layers 4, 5 of a float32 octave by the fused group kernel: from L3 (src), DoG planes 3, 4 at
+// dog3, dog3 + RC.
+int32_t launch_group_upper(const float* src, int R, int C, float* dog3, cudaStream_t s) {
+    GroupArgs a{};
+    a.src = src;
+    a.R = R;
+    a.C = C;
+    a.dog[0] = dog3;
+    a.dog[1] = dog3 + (long long)R * C;
+    return launch_group_t<1>(a, s);
+}
 
 // The float32 octave-0 base: blur (tap set 0, radius 5) of the 2x upsampled uint8 image.
 int32_t launch_base_fast(const uint8_t* img, int stride, int ih, int iw, float* dst, int variant, cudaStream_t s) {

@@ -206,8 +206,9 @@ void launch(bool exact, const BlurArgs& a, cudaStream_t s) {
 
 }  // namespace
 
-// Float32 octave engine: the tiled per-layer kernels (k_layer, octave.cu) by default; the fused
-// streaming kernel (k_octave) for octaves at least kFusedMinCols wide when FSB_PYRAMID=fused.
+// Float32 octave engines: the fused layer groups (k_group, octave.cu) by default; the tiled
+// per-layer kernels (k_layer) with FSB_PYRAMID=layer; the fused streaming kernel (k_octave) for
+// octaves at least kFusedMinCols wide with FSB_PYRAMID=fused.
 static const int kFusedMinCols = 2000;
 
 namespace {
@@ -244,13 +245,45 @@ int32_t tuned_layer(int layer, const float* src, int R, int C, float* dst, float
 }
 }  // namespace
 
-static bool use_fused_octaves() {
-    static const bool on = [] {
-        const char* e = std::getenv("FSB_PYRAMID");
-        return e && std::strcmp(e, "fused") == 0;
-    }();
-    return on;
+// FSB_PYRAMID selects the float32 octave engine (all are bit-identical): unset, the autotuner picks
+// per octave size between the per-layer kernels (variant 0, also with FSB_AUTOTUNE=0) and the
+// fused layer groups (variant 1); "layer" / "group" force one; "fused" takes the streaming
+// kernel for octaves at least kFusedMinCols wide. Read on every call.
+enum class Engine { Auto, Group, Layer, Fused };
+static Engine pyramid_engine() {
+    const char* e = std::getenv("FSB_PYRAMID");
+    if (e && std::strcmp(e, "layer") == 0) return Engine::Layer;
+    if (e && std::strcmp(e, "group") == 0) return Engine::Group;
+    if (e && std::strcmp(e, "fused") == 0) return Engine::Fused;
+    return Engine::Auto;
 }
+
+namespace {
+// One float32 octave from its base `src` (not written): DoG, gradient atlases, L3[::2, ::2] to
+// `down`; x, y are scratch planes. Both variants leave the same outputs, so the tuner may run
+// either any number of times.
+struct OctaveCall {
+    const float* src;
+    int R, C;
+    float *x, *y, *dog, *mag, *ang, *down;
+    int dc;
+    cudaStream_t s;
+};
+int32_t run_octave_call(void* p, int v) {
+    const OctaveCall* c = static_cast<const OctaveCall*>(p);
+    const long long RC = (long long)c->R * c->C;
+    if (v == 1) {
+        FSB_TRY(launch_group_lower(c->src, c->R, c->C, c->dog, c->mag, c->ang, c->x, c->down, c->dc, c->s));
+        return launch_group_upper(c->x, c->R, c->C, c->dog + 3 * RC, c->s);
+    }
+    FSB_TRY(tuned_layer(1, c->src, c->R, c->C, c->x, c->dog, nullptr, nullptr, nullptr, 0, c->s));
+    FSB_TRY(tuned_layer(2, c->x, c->R, c->C, c->y, c->dog + RC, c->mag, c->ang, nullptr, 0, c->s));
+    FSB_TRY(tuned_layer(3, c->y, c->R, c->C, c->x, c->dog + 2 * RC, c->mag + RC, c->ang + RC, nullptr, 0, c->s));
+    FSB_TRY(tuned_layer(4, c->x, c->R, c->C, c->y, c->dog + 3 * RC, c->mag + 2 * RC, c->ang + 2 * RC, c->down, c->dc,
+                        c->s));
+    return tuned_layer(5, c->y, c->R, c->C, nullptr, c->dog + 4 * RC, nullptr, nullptr, nullptr, 0, c->s);
+}
+}  // namespace
 
 int32_t run_pyramid(Workspace& ws, const uint8_t* d_img, int img_stride, bool exact, cudaStream_t s) {
     const Geometry& g = ws.g;
@@ -275,6 +308,30 @@ int32_t run_pyramid(Workspace& ws, const uint8_t* d_img, int img_stride, bool ex
         int v = 0;
         FSB_TRY(autotune(key, 2, run_base_call, &bc, s, &v));
     }
+    const Engine eng = exact ? Engine::Layer : pyramid_engine();
+    if (!exact && eng != Engine::Fused) {
+        // octave o reads its base from P[0] (o = 0) or one half of next_base and writes the next
+        // base into the other half; P[1], P[2] (and P[0] after octave 0) hold layers in flight
+        float* NB = ws.next_base.as<float>();
+        const long long half = g.n_oct > 1 ? ((long long)g.R[1] * g.C[1] + 63) / 64 * 64 : 0;
+        const float* cur = P[0];
+        for (int o = 0; o < g.n_oct; ++o) {
+            const bool last = o + 1 == g.n_oct;
+            OctaveCall c{cur, g.R[o], g.C[o], o == 0 ? P[1] : P[0], P[2], DF + g.dog_off[o], MAG + g.grad_off[o],
+                         ANG + g.grad_off[o], last ? nullptr : NB + (o & 1) * half, last ? 0 : g.C[o + 1], s};
+            if (eng == Engine::Auto) {
+                char key[64];
+                std::snprintf(key, sizeof(key), "k_octave_%dx%d", g.R[o], g.C[o]);
+                int v = 0;
+                FSB_TRY(autotune(key, 2, run_octave_call, &c, s, &v));
+            } else {
+                FSB_TRY(run_octave_call(&c, eng == Engine::Group ? 1 : 0));
+            }
+            cur = c.down;
+        }
+        FSB_CUDA(cudaGetLastError());
+        return FSB_OK;
+    }
     float* cur = P[0];   // base of the current octave
     for (int o = 0; o < g.n_oct; ++o) {
         const long long RC = (long long)g.R[o] * g.C[o];
@@ -284,7 +341,7 @@ int32_t run_pyramid(Workspace& ws, const uint8_t* d_img, int img_stride, bool ex
         float* other[2];
         for (int k = 0, n = 0; k < 3; ++k)
             if (P[k] != cur) other[n++] = P[k];
-        if (!exact && use_fused_octaves() && g.C[o] >= kFusedMinCols) {
+        if (!exact && g.C[o] >= kFusedMinCols) {
             // fused octave: reads cur, writes the next base into another plane
             float* down = o + 1 < g.n_oct ? other[0] : nullptr;
             FSB_TRY(launch_octave_fused(cur, g.R[o], g.C[o], dog, mag, ang, down, o + 1 < g.n_oct ? g.C[o + 1] : 0, s));

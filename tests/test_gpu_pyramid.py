@@ -80,6 +80,7 @@ def test_autotuned_tile_heights_are_bit_identical(monkeypatch):
     import fieldstitch_b200 as f
     from fieldstitch_b200 import _lib, synth
     img = synth.synth_image(700, 900, 31)
+    monkeypatch.setenv("FSB_PYRAMID", "layer")
     monkeypatch.setenv("FSB_AUTOTUNE", "0")
     _, st0 = f.gsift.detect(img)
     ref = st0.atlas()
@@ -95,3 +96,51 @@ def test_autotuned_tile_heights_are_bit_identical(monkeypatch):
     table = _lib.autotune_table()
     assert any("k_layer5_1400x1800" in k for k in table), table
     assert all(v in (0, 1, 2) for v in table.values())
+
+
+@pytest.mark.parametrize("hw", [(37, 53), (240, 320), (495, 661), (610, 830), (989, 1320), (1978, 2640)])
+def test_group_engine_bit_identical_to_per_layer(monkeypatch, hw):
+    """The fused layer-group kernels (L1..L3 and L4, L5 per launch, halos recomputed in shared
+    memory) give the per-layer kernels' DoG, magnitude and angle atlases bit for bit, including
+    odd and tiny octaves whose halos reflect more than once and (610 x 830) octaves whose atlas
+    planes start off a 16-byte boundary, and the same keypoints."""
+    import fieldstitch_b200 as f
+    from fieldstitch_b200 import synth
+    h, w = hw
+    img = synth.synth_image(h, w, 3 + h)
+    monkeypatch.setenv("FSB_PYRAMID", "layer")
+    k0, st0 = f.gsift.detect(img)
+    ref = st0.atlas()
+    monkeypatch.setenv("FSB_PYRAMID", "group")
+    k1, st1 = f.gsift.detect(img)
+    got = st1.atlas()
+    assert got[0] == ref[0] and len(ref[0]) >= 3
+    for o in range(len(ref[0])):
+        for k, name in ((1, "dog"), (2, "mag"), (3, "ang")):
+            np.testing.assert_array_equal(got[k][o], ref[k][o], err_msg="%s octave %d" % (name, o))
+    for key in ("x", "y", "size", "angle", "response"):
+        np.testing.assert_array_equal(k1[key], k0[key])
+
+
+def test_autotuned_octave_engines_are_bit_identical(monkeypatch):
+    """With no engine forced, the autotuner times the per-layer kernels and the fused layer groups
+    per octave size and keeps the faster; the atlases (first call, tuning; second call, cached
+    choices) equal the untuned per-layer ones bit for bit, and each octave size has a choice."""
+    import fieldstitch_b200 as f
+    from fieldstitch_b200 import _lib, synth
+    img = synth.synth_image(610, 830, 41)
+    monkeypatch.setenv("FSB_PYRAMID", "layer")
+    monkeypatch.setenv("FSB_AUTOTUNE", "0")
+    _, st0 = f.gsift.detect(img)
+    ref = st0.atlas()
+    monkeypatch.delenv("FSB_PYRAMID")
+    monkeypatch.delenv("FSB_AUTOTUNE")
+    for _ in range(2):
+        _, st = f.gsift.detect(img)
+        got = st.atlas()
+        for o in range(len(ref[0])):
+            for k in (1, 2, 3):
+                np.testing.assert_array_equal(got[k][o], ref[k][o])
+    table = _lib.autotune_table()
+    for r, c in ref[0]:
+        assert any(k.endswith("k_octave_%dx%d" % (r, c)) for k in table), (r, c, table)
