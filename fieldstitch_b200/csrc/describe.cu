@@ -4,8 +4,10 @@
 // Both histograms are accumulated without atomics, in float64, in a fixed order, so results are
 // deterministic and the float32 bins equal the reference's float64 bincount sums except in the
 // last bit of rare cases:
-//   k_orient    warp per keypoint; each lane owns a private 36-bin float64 column in shared
-//               memory; bins are then summed over lanes in lane order (gsift.py:372-432).
+//   k_orient    warp per refined extremum, visited in rank order (response descending); each
+//               lane owns a private 36-bin float64 column in shared memory; bins are then summed
+//               over lanes in lane order (gsift.py:372-432); the extremum's peaks go to its rank's
+//               slots in bin order.
 //   k_describe  warp per keypoint; lane u < 25 owns one unit square of the rotated bin grid and
 //               visits each of its samples once (row by row, the column interval solved in closed
 //               form), adding the sample's trilinear split with the reference's operation order
@@ -23,20 +25,6 @@ namespace {
 
 inline unsigned blocks(long long n, int t) { return (unsigned)((n + t - 1) / t); }
 
-template <class T>
-__device__ __forceinline__ void warp_append(bool flag, const T& v, T* out, uint32_t* counter, uint32_t cap) {
-    const unsigned m = __ballot_sync(0xffffffffu, flag);
-    if (!m) return;
-    const int lane = threadIdx.x & 31, leader = __ffs(m) - 1;
-    uint32_t base = 0;
-    if (lane == leader) base = atomicAdd(counter, (uint32_t)__popc(m));
-    base = __shfl_sync(0xffffffffu, base, leader);
-    if (flag) {
-        const uint32_t pos = base + __popc(m & ((1u << lane) - 1u));
-        if (pos < cap) out[pos] = v;
-    }
-}
-
 // keypoint scale in octave pixels: 1.6 * 2^((l + x2) / 3) (gsift.py:462)
 __device__ __forceinline__ float kp_scale(int l, float x2) {
     const float t = ((float)l + x2) / 3.f;
@@ -52,16 +40,17 @@ constexpr int OW = 4;   // warps per block
 template <class Acc>
 __global__ void __launch_bounds__(OW * 32) k_orient(const float* __restrict__ MAG, const float* __restrict__ ANG,
                                                     Geometry g, const Refined* __restrict__ ref,
-                                                    const uint32_t* n_ref, uint32_t cap_ref,
-                                                    Oriented* __restrict__ out, uint32_t* counter, uint32_t cap) {
+                                                    const uint32_t* __restrict__ order, uint32_t k0, uint32_t k1,
+                                                    Oriented* __restrict__ slots, uint32_t* __restrict__ cnt,
+                                                    uint32_t* total) {
     __shared__ Acc s_acc[OW][ORI_BINS][33];
     __shared__ float s_raw[OW][ORI_BINS];
     __shared__ float s_sm[OW][ORI_BINS];
     const int wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const uint32_t n = min(*n_ref, cap_ref);
     const uint32_t nw = gridDim.x * OW;
     Acc (*acc)[33] = s_acc[wid];
-    for (uint32_t i = blockIdx.x * OW + wid; i < n; i += nw) {
+    for (uint32_t t = k0 + blockIdx.x * OW + wid; t < k1; t += nw) {
+        const uint32_t i = order[t];
         const Refined e = ref[i];
         const int o = e.o, R = g.R[o], C = g.C[o];
         const float scl = kp_scale(e.l, e.x2);
@@ -129,6 +118,7 @@ __global__ void __launch_bounds__(OW * 32) k_orient(const float* __restrict__ MA
         for (int sh = 16; sh; sh >>= 1) hmax = fmaxf(hmax, __shfl_xor_sync(0xffffffffu, hmax, sh));
         __syncwarp();
         const float thr = 0.8f * hmax;
+        uint32_t npk = 0;   // peaks of this extremum so far, in bin order
         for (int b0 = 0; b0 < 64; b0 += 32) {
             const int b = b0 + lane;
             bool pk = false;
@@ -149,7 +139,13 @@ __global__ void __launch_bounds__(OW * 32) k_orient(const float* __restrict__ MA
                     ent.ri = i; ent.j = b; ent.angle = (float)ang;
                 }
             }
-            warp_append(pk, ent, out, counter, cap);
+            const unsigned m = __ballot_sync(0xffffffffu, pk);
+            if (pk) slots[(size_t)t * ORI_SLOTS + npk + __popc(m & ((1u << lane) - 1u))] = ent;
+            npk += __popc(m);
+        }
+        if (lane == 0) {
+            cnt[t] = npk;
+            atomicAdd(total, npk);
         }
         __syncwarp();
     }
@@ -373,16 +369,17 @@ __global__ void __launch_bounds__(DW * 32) k_describe(const float* __restrict__ 
 
 }  // namespace
 
-int32_t run_orient(const Workspace& ws, const Refined* ref, const uint32_t* d_nref, uint32_t n_ref_host,
-                   uint32_t cap_ref, Oriented* out, uint32_t* d_counter, uint32_t cap, bool exact, cudaStream_t s) {
-    const unsigned ob = blocks(n_ref_host, OW);
+int32_t run_orient(const Workspace& ws, const Refined* ref, const uint32_t* order, uint32_t k0, uint32_t k1,
+                   Oriented* slots, uint32_t* cnt, uint32_t* d_total, bool exact, cudaStream_t s) {
+    if (k1 <= k0) return FSB_OK;
+    const unsigned ob = blocks(k1 - k0, OW);
     const unsigned grid = ob < 148 * 32 ? ob : 148 * 32;
     if (exact)
-        k_orient<double><<<grid, OW * 32, 0, s>>>(ws.mag.as<float>(), ws.ang.as<float>(), ws.g, ref, d_nref, cap_ref,
-                                                  out, d_counter, cap);
+        k_orient<double><<<grid, OW * 32, 0, s>>>(ws.mag.as<float>(), ws.ang.as<float>(), ws.g, ref, order, k0, k1,
+                                                  slots, cnt, d_total);
     else
-        k_orient<float><<<grid, OW * 32, 0, s>>>(ws.mag.as<float>(), ws.ang.as<float>(), ws.g, ref, d_nref, cap_ref,
-                                                 out, d_counter, cap);
+        k_orient<float><<<grid, OW * 32, 0, s>>>(ws.mag.as<float>(), ws.ang.as<float>(), ws.g, ref, order, k0, k1,
+                                                 slots, cnt, d_total);
     note_launch();
     FSB_CUDA(cudaGetLastError());
     return FSB_OK;

@@ -254,38 +254,40 @@ __device__ __forceinline__ float kp_scale(int l, float x2) {
     return 1.6f * exp2f(t);
 }
 
-__global__ void k_sort_keys_a(const Oriented* __restrict__ ori, const Refined* __restrict__ ref, uint32_t n,
-                              unsigned long long* __restrict__ key, uint32_t* __restrict__ val) {
+// rank key of a refined extremum (31 + fbits bits): response descending (a positive finite float's
+// bits order like its value), then DoG-atlas index ascending (f < 2^fbits)
+__global__ void k_rank_keys(const Refined* __restrict__ ref, uint32_t n, int fbits,
+                            unsigned long long* __restrict__ key, uint32_t* __restrict__ val) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
-    const Oriented e = ori[i];
-    key[i] = ((unsigned long long)ref[e.ri].f << 6) | (unsigned long long)e.j;
+    const Refined r = ref[i];
+    key[i] = ((unsigned long long)(0x7fffffffu - __float_as_uint(r.resp)) << fbits) | (unsigned long long)r.f;
     val[i] = i;
 }
 
-__global__ void k_sort_keys_b(const Oriented* __restrict__ ori, const Refined* __restrict__ ref,
-                              const uint32_t* __restrict__ order, uint32_t n, uint32_t* __restrict__ key) {
-    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    key[i] = ~__float_as_uint(ref[ori[order[i]].ri].resp);
-}
-
-__global__ void k_gather(const Oriented* __restrict__ ori, const Refined* __restrict__ ref,
-                         const uint32_t* __restrict__ order, uint32_t n, float* kx, float* ky, float* ksize,
-                         float* kang, float* kresp, int32_t* koct, int32_t* klayer) {
-    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    const Oriented e = ori[order[i]];
-    const Refined r = ref[e.ri];
-    const float f = (float)(1 << r.o) * 0.5f;
-    const float scl = kp_scale(r.l, r.x2);
-    kx[i] = ((float)r.c + r.x0) * f;
-    ky[i] = ((float)r.r + r.x1) * f;
-    ksize[i] = (scl * 2.f) * f;
-    kang[i] = e.angle;
-    kresp[i] = r.resp;
-    koct[i] = r.o;
-    klayer[i] = r.l;
+// keypoints in final order: rank t's peaks (bin order) at pos[t] .. pos[t] + cnt[t] - 1, kept below
+// n_keep
+__global__ void k_gather_ranked(const Oriented* __restrict__ slots, const uint32_t* __restrict__ cnt,
+                                const uint32_t* __restrict__ pos, const Refined* __restrict__ ref, uint32_t n_rank,
+                                uint32_t n_keep, float* kx, float* ky, float* ksize, float* kang, float* kresp,
+                                int32_t* koct, int32_t* klayer) {
+    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n_rank) return;
+    const uint32_t c = cnt[t], p = pos[t];
+    for (uint32_t k = 0; k < c && p + k < n_keep; ++k) {
+        const Oriented e = slots[(size_t)t * ORI_SLOTS + k];
+        const Refined r = ref[e.ri];
+        const float f = (float)(1 << r.o) * 0.5f;
+        const float scl = kp_scale(r.l, r.x2);
+        const uint32_t i = p + k;
+        kx[i] = ((float)r.c + r.x0) * f;
+        ky[i] = ((float)r.r + r.x1) * f;
+        ksize[i] = (scl * 2.f) * f;
+        kang[i] = e.angle;
+        kresp[i] = r.resp;
+        koct[i] = r.o;
+        klayer[i] = r.l;
+    }
 }
 
 // ------------------------------------------------------------------------------------ spread
@@ -391,49 +393,57 @@ int32_t run_detect(fsb_ctx* ctx, Workspace& ws, double contrast, double edge, in
     ctx->stage_end(ST_REFINE);
     const uint32_t n_ref = h_cnt[1];
     if (n_ref == 0) { ws.n_kp = 0; return FSB_OK; }
-    uint32_t n_ori = 0;
-    ctx->stage_begin(ST_ORIENT);
-    for (int attempt = 0; attempt < 3; ++attempt) {
-        if (ws.cap_ori < (size_t)n_ref * 2 + 1024) ws.cap_ori = (size_t)n_ref * 2 + 1024;
-        FSB_TRY(ws.oriented.ensure(ws.cap_ori * sizeof(Oriented)));
-        FSB_CUDA(cudaMemsetAsync(cnt + 2, 0, sizeof(uint32_t), s));
-        FSB_TRY(run_orient(ws, ws.refined.as<Refined>(), cnt + 1, n_ref, (uint32_t)ws.cap_ref,
-                           ws.oriented.as<Oriented>(), cnt + 2, (uint32_t)ws.cap_ori, exact, s));
-        FSB_CUDA(cudaMemcpyAsync(h_cnt + 2, cnt + 2, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
-        FSB_CUDA(cudaStreamSynchronize(s));
-        n_ori = h_cnt[2];
-        if (n_ori <= ws.cap_ori) break;
-        ws.cap_ori = (size_t)n_ori + 1024;
-    }
-    ctx->stage_end(ST_ORIENT);
-    if (n_ori > ws.cap_ori) { set_error("orientation list overflow"); return FSB_ERR_OVERFLOW; }
-    if (n_ori == 0) { ws.n_kp = 0; return FSB_OK; }
+    if (max_kp <= 0) { ws.n_kp = 0; return FSB_OK; }
+    // The reference orients every refined extremum, orders the keypoints by response (stable, the
+    // keypoints listed by extremum and bin) and keeps max_kp. All peaks of an extremum share its
+    // response, so the kept keypoints are the peaks of the strongest extrema in the order
+    // (response descending, DoG index ascending), each extremum's peaks in bin order: rank the
+    // extrema once, orient them rank by rank until their peaks fill max_kp (an extremum may have
+    // none), and lay the peaks out by an exclusive scan of the per-rank counts.
     ctx->stage_begin(ST_SORT);
-    // stable two-key sort: (extremum index, bin) ascending, then response descending
-    FSB_TRY(ws.keys_a.ensure((size_t)n_ori * 8 * 2));
-    FSB_TRY(ws.vals_a.ensure((size_t)n_ori * 4 * 2));
-    FSB_TRY(ws.keys_b.ensure((size_t)n_ori * 4 * 2));
-    FSB_TRY(ws.vals_b.ensure((size_t)n_ori * 4 * 2));
-    unsigned long long* ka = ws.keys_a.as<unsigned long long>();
-    uint32_t* va = ws.vals_a.as<uint32_t>();
-    uint32_t* kb = ws.keys_b.as<uint32_t>();
-    uint32_t* vb = ws.vals_b.as<uint32_t>();
     int fbits = 1;
     while ((1ull << fbits) < (unsigned long long)g.dog_off[g.n_oct]) ++fbits;
-    const int end_a = fbits + 6;
+    const int end_bit = 31 + fbits;
+    FSB_TRY(ws.keys_a.ensure((size_t)n_ref * 8 * 2));
+    FSB_TRY(ws.vals_a.ensure((size_t)n_ref * 4 * 2));
+    FSB_TRY(ws.keys_b.ensure((size_t)n_ref * 4 * 2));
+    unsigned long long* ka = ws.keys_a.as<unsigned long long>();
+    uint32_t* va = ws.vals_a.as<uint32_t>();
+    uint32_t* rcnt = ws.keys_b.as<uint32_t>();
+    uint32_t* rpos = rcnt + n_ref;
     size_t t1 = 0, t2 = 0;
-    cub::DeviceRadixSort::SortPairs(nullptr, t1, ka, ka + n_ori, va, va + n_ori, (int)n_ori, 0, end_a, s);
-    cub::DeviceRadixSort::SortPairs(nullptr, t2, kb, kb + n_ori, vb, vb + n_ori, (int)n_ori, 0, 32, s);
+    cub::DeviceRadixSort::SortPairs(nullptr, t1, ka, ka + n_ref, va, va + n_ref, (int)n_ref, 0, end_bit, s);
+    cub::DeviceScan::ExclusiveSum(nullptr, t2, rcnt, rpos, (int)n_ref, s);
     FSB_TRY(ws.sort_tmp.ensure(t1 > t2 ? t1 : t2));
+    k_rank_keys<<<blocks(n_ref, 256), 256, 0, s>>>(ws.refined.as<Refined>(), n_ref, fbits, ka, va);
     size_t tb = ws.sort_tmp.bytes;
-    k_sort_keys_a<<<blocks(n_ori, 256), 256, 0, s>>>(ws.oriented.as<Oriented>(), ws.refined.as<Refined>(), n_ori, ka, va);
-    FSB_CUDA(cub::DeviceRadixSort::SortPairs(ws.sort_tmp.p, tb, ka, ka + n_ori, va, va + n_ori, (int)n_ori, 0, end_a, s));
-    k_sort_keys_b<<<blocks(n_ori, 256), 256, 0, s>>>(ws.oriented.as<Oriented>(), ws.refined.as<Refined>(), va + n_ori,
-                                                     n_ori, kb);
+    FSB_CUDA(cub::DeviceRadixSort::SortPairs(ws.sort_tmp.p, tb, ka, ka + n_ref, va, va + n_ref, (int)n_ref, 0,
+                                             end_bit, s));
+    note_launch(2);
+    const uint32_t* order = va + n_ref;
+    ctx->stage_end(ST_SORT);
+    ctx->stage_begin(ST_ORIENT);
+    FSB_TRY(ws.oriented.ensure((size_t)n_ref * ORI_SLOTS * sizeof(Oriented)));
+    Oriented* slots = ws.oriented.as<Oriented>();
+    FSB_CUDA(cudaMemsetAsync(cnt + 2, 0, sizeof(uint32_t), s));
+    uint32_t k1 = 0, total = 0;
+    while (true) {
+        const uint32_t k0 = k1;
+        const uint64_t want = (uint64_t)max_kp > total ? (uint64_t)max_kp - total : 1;
+        k1 = (uint32_t)((uint64_t)k0 + want < n_ref ? (uint64_t)k0 + want : n_ref);
+        FSB_TRY(run_orient(ws, ws.refined.as<Refined>(), order, k0, k1, slots, rcnt, cnt + 2, exact, s));
+        FSB_CUDA(cudaMemcpyAsync(h_cnt + 2, cnt + 2, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+        FSB_CUDA(cudaStreamSynchronize(s));
+        total = h_cnt[2];
+        if (total >= (uint32_t)max_kp || k1 >= n_ref) break;
+    }
+    ctx->stage_end(ST_ORIENT);
+    const uint32_t n_keep = total < (uint32_t)max_kp ? total : (uint32_t)max_kp;
+    if (n_keep == 0) { ws.n_kp = 0; return FSB_OK; }
+    ctx->stage_begin(ST_SORT);
     tb = ws.sort_tmp.bytes;
-    FSB_CUDA(cub::DeviceRadixSort::SortPairs(ws.sort_tmp.p, tb, kb, kb + n_ori, va + n_ori, vb, (int)n_ori, 0, 32, s));
-    const uint32_t n_keep = n_ori < (uint32_t)max_kp ? n_ori : (uint32_t)max_kp;
-    const size_t nb4 = (size_t)(n_keep ? n_keep : 1) * 4;
+    FSB_CUDA(cub::DeviceScan::ExclusiveSum(ws.sort_tmp.p, tb, rcnt, rpos, (int)k1, s));
+    const size_t nb4 = (size_t)n_keep * 4;
     FSB_TRY(ws.kx.ensure(nb4));
     FSB_TRY(ws.ky.ensure(nb4));
     FSB_TRY(ws.ksize.ensure(nb4));
@@ -441,12 +451,11 @@ int32_t run_detect(fsb_ctx* ctx, Workspace& ws, double contrast, double edge, in
     FSB_TRY(ws.kresp.ensure(nb4));
     FSB_TRY(ws.koct.ensure(nb4));
     FSB_TRY(ws.klayer.ensure(nb4));
-    if (n_keep)
-        k_gather<<<blocks(n_keep, 256), 256, 0, s>>>(ws.oriented.as<Oriented>(), ws.refined.as<Refined>(), vb, n_keep,
-                                                     ws.kx.as<float>(), ws.ky.as<float>(), ws.ksize.as<float>(),
-                                                     ws.kangle.as<float>(), ws.kresp.as<float>(), ws.koct.as<int32_t>(),
-                                                     ws.klayer.as<int32_t>());
-    note_launch(n_keep ? 3 : 2);
+    k_gather_ranked<<<blocks(k1, 256), 256, 0, s>>>(slots, rcnt, rpos, ws.refined.as<Refined>(), k1, n_keep,
+                                                    ws.kx.as<float>(), ws.ky.as<float>(), ws.ksize.as<float>(),
+                                                    ws.kangle.as<float>(), ws.kresp.as<float>(), ws.koct.as<int32_t>(),
+                                                    ws.klayer.as<int32_t>());
+    note_launch(2);
     FSB_CUDA(cudaGetLastError());
     ctx->stage_end(ST_SORT);
     ws.n_kp = (int)n_keep;

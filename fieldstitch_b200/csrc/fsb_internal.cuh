@@ -54,6 +54,7 @@ constexpr float SIGMA = 1.6f;
 constexpr int BORDER = 5;
 constexpr int MAX_INTERP = 5;
 constexpr int ORI_BINS = 36;
+constexpr int ORI_SLOTS = ORI_BINS / 2;   // peaks of one extremum: local maxima of 36 circular bins
 constexpr float ORI_RADIUS = 4.5f;
 constexpr float ORI_SIG = 1.5f;
 constexpr int ORI_R_MAX = 16;
@@ -121,7 +122,7 @@ struct Workspace {
     DevBuf cand, refined, oriented;
     DevBuf keys_a, keys_b, vals_a, vals_b, sort_tmp;
     DevBuf counters;             // [0] candidates, [1] refined, [2] oriented
-    size_t cap_cand = 0, cap_ref = 0, cap_ori = 0;
+    size_t cap_cand = 0, cap_ref = 0;
     // sorted, capped keypoints (structure of arrays)
     DevBuf kx, ky, ksize, kangle, kresp, koct, klayer;
     int n_kp = 0;
@@ -186,8 +187,8 @@ int32_t launch_group_upper(const float* src, int R, int C, float* dog3, cudaStre
 int32_t autotune(const char* key, int n_variants, int32_t (*run)(void*, int), void* arg, cudaStream_t s, int* variant);
 
 // ---------------------------------------------------------------- detect.cu / describe.cu
-int32_t run_orient(const Workspace& ws, const Refined* ref, const uint32_t* d_nref, uint32_t n_ref_host,
-                   uint32_t cap_ref, Oriented* out, uint32_t* d_counter, uint32_t cap, bool exact, cudaStream_t s);
+int32_t run_orient(const Workspace& ws, const Refined* ref, const uint32_t* order, uint32_t k0, uint32_t k1,
+                   Oriented* slots, uint32_t* cnt, uint32_t* d_total, bool exact, cudaStream_t s);
 int32_t run_detect(fsb_ctx* ctx, Workspace& ws, double contrast, double edge, int max_kp, bool exact);
 int32_t run_describe_mode(const Workspace& ws, int n, const float* d_x, const float* d_y, const float* d_size,
                           const float* d_angle, const int32_t* d_oct, const int32_t* d_layer, float* d_desc,

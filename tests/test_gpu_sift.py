@@ -159,3 +159,23 @@ def test_cv2_keypoint_export_matches_opencv(fsb, golden, case):
     np.testing.assert_allclose(got["size"][p[m]], c[case + "/size"][m], rtol=1e-3)
     kp = fsb.gsift.to_cv2_keypoints(got)
     assert len(kp) == len(got["x"]) and kp[0].octave == int(fsb.gsift.cv2_octave(got)[0])
+
+
+@pytest.mark.parametrize("exact", [False, True])
+def test_capped_detect_is_prefix_of_full_list(fsb, golden, exact):
+    """Only the strongest extrema are oriented when max_kp caps the list; the capped keypoints
+    must be exactly the first max_kp of the uncapped list (response descending, then extremum,
+    then bin), every field bit for bit, for caps below, at and above the number of keypoints."""
+    from fieldstitch_b200 import synth
+    imgs = [golden["sift_ref"]["s240x320_c04/img"]]
+    if not exact:
+        imgs.append(synth.synth_image(495, 660, 17))
+    for img in imgs:
+        full, _ = fsb.gsift.detect(img, max_kp=10 ** 7, contrast=0.015, edge=12.0, exact=exact)
+        n = len(full["x"])
+        assert n > 100
+        for cap in (1, 37, n // 3, n - 1, n, n + 5):
+            got, _ = fsb.gsift.detect(img, max_kp=cap, contrast=0.015, edge=12.0, exact=exact)
+            assert len(got["x"]) == min(cap, n)
+            for k in full:
+                np.testing.assert_array_equal(got[k], full[k][:cap], err_msg="%s cap %d" % (k, cap))
