@@ -531,7 +531,14 @@ def run_fsb(args):
     # ---- e2e through the public host API (host buffers, copies inside the timed region)
     e2e = None
     if not args.no_e2e:
-        host = [(np.ascontiguousarray(a), np.ascontiguousarray(b)) for a, b, _, _, _ in pairs]
+        # the step's input images in pinned host memory (numpy views of pinned torch tensors)
+        def pinned(x):
+            t = torch.empty(x.shape, dtype=torch.uint8, pin_memory=True)
+            t.numpy()[...] = x
+            return t
+
+        host_t = [(pinned(a), pinned(b)) for a, b, _, _, _ in pairs]
+        host = [(ta.numpy(), tb.numpy()) for ta, tb in host_t]
 
         def e2e_pair(i):
             a, b = host[i]
@@ -552,7 +559,7 @@ def run_fsb(args):
         e2e_step()
         torch.cuda.synchronize()
         barrier()
-        ksteps = max(1, args.steps // 2)
+        ksteps = max(2, args.steps)
         f0 = time.perf_counter()
         main = torch.cuda.current_stream(dev)
         g0 = torch.cuda.Event(enable_timing=True)
@@ -573,7 +580,9 @@ def run_fsb(args):
             ms_e2e = float(t.item())
         e2e = {"value": world * args.pairs / (ms_e2e / 1000.0), "unit": "pairs/s", "h2d_bytes_per_step": int(h2d),
                "d2h_bytes_per_step": int(d2h), "ms_per_step": ms_e2e, "steps": ksteps,
-               "api": "features.sift_gpu_u8 + matching.guided_from_pred, %d host threads" % args.streams}
+               "api": "features.sift_gpu_u8 + matching.guided_from_pred, %d host threads" % args.streams,
+               "host_inputs": "images in pinned host memory; keypoints / descriptors between the two calls in "
+                              "the numpy arrays the API returns"}
 
     # ---- roofline of the dominant stage (pyramid): CUDA events on the library stream, one stream
     # alone (8 images), so the per-image time is not inflated by the other streams' kernels
@@ -589,7 +598,8 @@ def run_fsb(args):
     alg = pyramid_bytes(h, w)
     achieved = alg / (per_img_ms / 1000.0) / 1e9 if per_img_ms > 0 else None
     c_ms, c_n = stages["pyramid"]
-    roof = {"bound": "hbm", "kernel": "pyramid (fused octave kernels + per-layer kernels of one image)",
+    roof = {"bound": "hbm", "kernel": "pyramid of one image (base + per octave the per-layer kernels or the fused "
+                                      "layer groups, autotuned)",
             "achieved": achieved, "peak": pk, "peak_source": pk_src, "unit": "GB/s",
             "frac": (achieved / pk) if achieved else None, "traffic": traffic_per_pyramid(),
             "algorithmic_bytes": alg, "ms_per_launch_group": per_img_ms,

@@ -47,9 +47,8 @@ __device__ __forceinline__ void warp_append(bool flag, const T& v, T* out, uint3
     }
 }
 
-// One CTA per (octave, 4 interior rows, 256 columns): DoG layers 0..4, rows r-1 .. r+4, columns
-// c0-4 .. c0+259 are staged in shared memory with 16-byte loads (each DoG value comes from DRAM
-// about 1.5 times: the row halo), then every thread tests its column for 4 rows x layers 1..3.
+// k_extrema: a block is 8 warps side by side over 240 interior columns of an EX_ROWS-row chunk of
+// one octave; each warp walks its chunk row by row (see the kernel).
 constexpr int EX_T = 256;            // 8 warps per block
 constexpr int EX_COLS = 30;          // output columns per warp (lanes 1..30; lanes 0 and 31 are halo)
 constexpr int EX_ROWS = 64;          // rows per block (a chunk of the octave's interior rows)
@@ -66,7 +65,7 @@ struct ExTiles {
 // extremum when it equals the maximum (minimum) of its 27-neighbourhood - ties count - and is
 // beyond the threshold, as scipy's maximum_filter / minimum_filter test in the reference
 // (gsift.py:293-319). Candidates of a row are appended with one warp-aggregated atomic.
-__global__ void __launch_bounds__(EX_T) k_extrema(const float* __restrict__ DF, DetectConsts k, ExTiles tl,
+__global__ void __launch_bounds__(EX_T, 5) k_extrema(const float* __restrict__ DF, DetectConsts k, ExTiles tl,
                                                   uint32_t* __restrict__ cand, uint32_t* counter, uint32_t cap) {
     int o = 0;
     while (o + 1 < tl.n_oct && (int)blockIdx.x >= tl.first[o + 1]) ++o;
@@ -80,34 +79,38 @@ __global__ void __launch_bounds__(EX_T) k_extrema(const float* __restrict__ DF, 
     const int cc = min(max(c, 0), C - 1);                                    // clamped for loading
     const bool col_ok = lane >= 1 && lane <= EX_COLS && c >= BORDER && c < C - BORDER;
     const int y0 = BORDER + ry * EX_ROWS, y1 = min(y0 + EX_ROWS, R - BORDER);   // output rows [y0, y1)
-    float hx0[5], hx1[5], hn0[5], hn1[5], prev[3];
-    auto load_row = [&](int y, float (&hx)[5], float (&hn)[5], float (&ctr)[3]) {
+    // one row of the 3-row window: horizontal max / min of the 5 layers and the centre values of
+    // layers 1..3
+    struct Row {
+        float hx[5], hn[5], c[3];
+    };
+    // layer l of row y at this lane's column: rowp + l * RC, rowp advancing by C per row
+    const float* rowp = base + (long long)(y0 - 1) * C + cc;
+    auto load_row = [&](Row& w) {
 #pragma unroll
         for (int l = 0; l < 5; ++l) {
-            const float v = __ldg(base + l * RC + (long long)y * C + cc);
+            const float v = __ldg(rowp + l * RC);
             const float vl = __shfl_up_sync(0xffffffffu, v, 1), vr = __shfl_down_sync(0xffffffffu, v, 1);
-            hx[l] = fmaxf(fmaxf(vl, v), vr);
-            hn[l] = fminf(fminf(vl, v), vr);
-            if (l >= 1 && l <= N_LAYERS) ctr[l - 1] = v;
+            w.hx[l] = fmaxf(fmaxf(vl, v), vr);
+            w.hn[l] = fminf(fminf(vl, v), vr);
+            if (l >= 1 && l <= N_LAYERS) w.c[l - 1] = v;
         }
+        rowp += C;
     };
-    float dummy[3];
-    load_row(y0 - 1, hx0, hn0, dummy);
-    load_row(y0, hx1, hn1, prev);
-    for (int y = y0; y < y1; ++y) {
-        float hx2[5], hn2[5], cur[3];
-        load_row(y + 1, hx2, hn2, cur);
+    // test row y from the window (up, mid, dn), append its extrema, then load row y + 2 into `up`
+    // (no longer needed): the three windows rotate by name, not by register moves
+    auto step = [&](Row& up, const Row& mid, const Row& dn, int y) {
         float vmx[5], vmn[5];
 #pragma unroll
         for (int l = 0; l < 5; ++l) {
-            vmx[l] = fmaxf(fmaxf(hx0[l], hx1[l]), hx2[l]);
-            vmn[l] = fminf(fminf(hn0[l], hn1[l]), hn2[l]);
+            vmx[l] = fmaxf(fmaxf(up.hx[l], mid.hx[l]), dn.hx[l]);
+            vmn[l] = fminf(fminf(up.hn[l], mid.hn[l]), dn.hn[l]);
         }
         unsigned mask = 0;
         if (col_ok) {
 #pragma unroll
             for (int l = 1; l <= N_LAYERS; ++l) {
-                const float v = prev[l - 1];
+                const float v = mid.c[l - 1];
                 const float mx = fmaxf(fmaxf(vmx[l - 1], vmx[l]), vmx[l + 1]);
                 const float mn = fminf(fminf(vmn[l - 1], vmn[l]), vmn[l + 1]);
                 if ((v >= mx && v > k.pthr) || (v <= mn && v < -k.pthr)) mask |= 1u << (l - 1);
@@ -134,15 +137,18 @@ __global__ void __launch_bounds__(EX_T) k_extrema(const float* __restrict__ DF, 
                 ++pos;
             }
         }
-#pragma unroll
-        for (int l = 0; l < 5; ++l) {
-            hx0[l] = hx1[l];
-            hx1[l] = hx2[l];
-            hn0[l] = hn1[l];
-            hn1[l] = hn2[l];
-        }
-#pragma unroll
-        for (int l = 0; l < 3; ++l) prev[l] = cur[l];
+        load_row(up);   // row y + 2 <= R - BORDER + 1 < R
+    };
+    Row w0, w1, w2;
+    load_row(w0);   // y0 - 1
+    load_row(w1);   // y0
+    load_row(w2);   // y0 + 1
+    for (int y = y0; y < y1; y += 3) {
+        step(w0, w1, w2, y);
+        if (y + 1 >= y1) break;
+        step(w1, w2, w0, y + 1);
+        if (y + 2 >= y1) break;
+        step(w2, w0, w1, y + 2);
     }
 }
 
