@@ -47,6 +47,9 @@ SIGNATURES = [
                                  c_vp, c_vp, c_vp]),
     ("fsb_unique", c_i32, [c_vp, c_vp, c_vp, c_vp, c_i32, c_vp, c_vp, c_vp]),
     ("fsb_perspective", c_i32, [c_vp, c_vp, c_i32, c_vp, c_vp]),
+    ("fsb_undistort_pixels", c_i32, [c_vp, c_vp, c_i32, c_vp, c_vp]),
+    ("fsb_predict_ground", c_i32, [c_vp, c_vp, c_i32, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, ctypes.c_double,
+                                   c_vp, c_vp]),
     ("fsb_launch_count", c_i64, []),
     ("fsb_timing", c_i32, [c_vp, c_i32]),
     ("fsb_stage_times", c_i32, [c_vp, c_vp, c_vp, c_i32]),

@@ -3,8 +3,8 @@
     python -m fieldstitch_b200.build        # or __graft_entry__.build()
 
 Each .cu under csrc/ is compiled for `-gencode arch=compute_100a,code=sm_100a` and linked into
-fieldstitch_b200/libfsb200.so. detect.cu and describe.cu are compiled with --fmad=false so their float32 arithmetic
-rounds like the reference's (one rounding per operation).
+fieldstitch_b200/libfsb200.so. detect.cu, describe.cu and geom.cu are compiled with --fmad=false so their
+arithmetic rounds like the reference's (one rounding per operation).
 """
 import os
 import shutil
@@ -19,8 +19,8 @@ INCLUDE = os.path.join(os.path.dirname(HERE), "include")
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 COMMON = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-I", INCLUDE, "--expt-relaxed-constexpr"]
-PER_FILE = {"detect.cu": ["--fmad=false"], "describe.cu": ["--fmad=false"]}
-SOURCES = ["api.cu", "pyramid.cu", "octave.cu", "detect.cu", "describe.cu", "match.cu", "tc_match.cu", "mlp.cu", "autotune.cu"]
+PER_FILE = {"detect.cu": ["--fmad=false"], "describe.cu": ["--fmad=false"], "geom.cu": ["--fmad=false"]}
+SOURCES = ["api.cu", "pyramid.cu", "octave.cu", "detect.cu", "describe.cu", "match.cu", "tc_match.cu", "mlp.cu", "autotune.cu", "geom.cu"]
 
 
 def nvcc():

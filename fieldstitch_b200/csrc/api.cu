@@ -918,6 +918,43 @@ int32_t fsb_unique(fsb_ctx* ctx, const int64_t* q, const int64_t* t, const float
     return FSB_OK;
 }
 
+int32_t fsb_undistort_pixels(fsb_ctx* ctx, const double* uv, int32_t n, const double* k8, double* out) {
+    FSB_ARG(ctx && k8, "null pointer");
+    FSB_ARG(n >= 0 && (n == 0 || (uv && out)), "bad points");
+    FSB_ARG(k8[0] != 0.0, "focal length 0");
+    if (n == 0) return FSB_OK;
+    FSB_TRY(use_device(ctx));
+    cudaStream_t s = ctx->stream;
+    FSB_TRY(ctx->s_f32a.ensure((size_t)n * 32 + 256));
+    double* du = ctx->s_f32a.as<double>();
+    double* dout = du + 2 * (size_t)n;
+    FSB_CUDA(cudaMemcpyAsync(du, uv, (size_t)n * 16, cudaMemcpyHostToDevice, s));
+    FSB_TRY(run_undistort(du, n, k8, dout, s));
+    FSB_CUDA(cudaMemcpyAsync(out, dout, (size_t)n * 16, cudaMemcpyDeviceToHost, s));
+    FSB_CUDA(cudaStreamSynchronize(s));
+    return FSB_OK;
+}
+
+int32_t fsb_predict_ground(fsb_ctx* ctx, const double* u, int32_t n, const double* kinv_i, const double* r_i,
+                           const double* c_i, const double* k_j, const double* r_j, const double* c_j, double zg,
+                           double* pred, uint8_t* ok) {
+    FSB_ARG(ctx && kinv_i && r_i && c_i && k_j && r_j && c_j, "null pointer");
+    FSB_ARG(n >= 0 && (n == 0 || (u && pred && ok)), "bad points");
+    if (n == 0) return FSB_OK;
+    FSB_TRY(use_device(ctx));
+    cudaStream_t s = ctx->stream;
+    FSB_TRY(ctx->s_f32a.ensure((size_t)n * 33 + 256));
+    double* du = ctx->s_f32a.as<double>();
+    double* dp = du + 2 * (size_t)n;
+    uint8_t* dok = reinterpret_cast<uint8_t*>(dp + 2 * (size_t)n);
+    FSB_CUDA(cudaMemcpyAsync(du, u, (size_t)n * 16, cudaMemcpyHostToDevice, s));
+    FSB_TRY(run_predict(du, n, kinv_i, r_i, c_i, k_j, r_j, c_j, zg, dp, dok, s));
+    FSB_CUDA(cudaMemcpyAsync(pred, dp, (size_t)n * 16, cudaMemcpyDeviceToHost, s));
+    FSB_CUDA(cudaMemcpyAsync(ok, dok, (size_t)n, cudaMemcpyDeviceToHost, s));
+    FSB_CUDA(cudaStreamSynchronize(s));
+    return FSB_OK;
+}
+
 int32_t fsb_perspective(fsb_ctx* ctx, const double* xy, int32_t n, const double* hm9, double* out) {
     FSB_ARG(ctx && hm9, "null pointer");
     FSB_ARG(n >= 0 && (n == 0 || (xy && out)), "bad points");

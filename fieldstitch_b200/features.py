@@ -63,3 +63,24 @@ def save_features(out_npz, xy, desc_u8, resp, w, h):
     np.savez(out_npz, xy=np.asarray(xy, np.float32), desc=np.asarray(desc_u8, np.uint8),
              resp=np.asarray(resp, np.float32), red_wh=np.array([w, h], np.int32))
     return len(xy)
+
+
+def _batch(fn, items, streams):
+    """Runs fn over items on `streams` host threads, each driving its own context (CUDA stream and
+    workspaces), so one image's host-side steps overlap the others' kernels; results in order."""
+    from concurrent.futures import ThreadPoolExecutor
+    streams = max(1, min(int(streams), len(items)))
+    if streams == 1:
+        return [fn(x) for x in items]
+    with ThreadPoolExecutor(max_workers=streams) as ex:
+        return list(ex.map(fn, items))
+
+
+def sift_gpu_batch(images, nfeats, streams=4, contrast=0.015, edge=12.0, exact=False, device=0):
+    """Batched feature extraction: sift_gpu_u8 of every image (nfeats: one cap per image or one
+    for all), spread over `streams` contexts. Returns a list of (xy, rootsift uint8, resp)."""
+    nf = list(nfeats) if np.ndim(nfeats) else [int(nfeats)] * len(images)
+    if len(nf) != len(images):
+        raise ValueError("one keypoint cap per image")
+    jobs = list(zip(images, nf))
+    return _batch(lambda j: sift_gpu_u8(j[0], j[1], contrast, edge, exact, device), jobs, streams)

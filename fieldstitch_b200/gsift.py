@@ -144,3 +144,11 @@ def to_cv2_keypoints(kps):
     packed = cv2_octave(kps)
     return [cv2.KeyPoint(float(x), float(y), float(s), float(a), float(r), int(p))
             for x, y, s, a, r, p in zip(kps["x"], kps["y"], kps["size"], kps["angle"], kps["response"], packed)]
+
+
+def detect_batch(grays, max_kp=12000, contrast=0.015, edge=12.0, exact=False, streams=4, device=0):
+    """detect() of every image, spread over `streams` contexts (one CUDA stream each). Returns a
+    list of (kps, state); each state belongs to the context that detected it and may be used by
+    describe() once the batch has returned."""
+    from .features import _batch
+    return _batch(lambda g: detect(g, True, max_kp, contrast, edge, None, exact, device), list(grays), streams)

@@ -7,13 +7,22 @@
   ``guided_from_pred`` takes predicted positions directly (the ground-plane prior of
   matching.py:155-172, or any other prior); ``kc=None`` takes every B keypoint within radius.
 * ``_unique(q, t, dd)`` - one-to-one filter on the target (matching.py:103-110).
+* ``match_pair((i, j))`` with ``init_worker`` / ``set_context`` / ``_get`` / ``load_features`` -
+  the pair worker (matching.py:17-64, 155-253): coarse exhaustive match, ground-plane prior
+  (``predict_ground``), RANSAC homography, guided match and fundamental verification; keypoint
+  undistortion (``undistort_pixels``, camera.py:5-31) and the prior run on the device.
 
 Descriptors are the feature file's uint8 RootSIFT vectors (uint8 arrays, or float arrays holding
 uint8 values as the reference does). ``na``/``nb`` must be the squared norms when given (the
 reference callers pass exactly those); the device recomputes them.
 """
 import ctypes
+import math
+import os
+import pickle
+from collections import OrderedDict
 
+import cv2
 import numpy as np
 
 from . import _lib
@@ -182,3 +191,209 @@ def _unique(q, t, dd, device=0):
     _lib.check(ctx.lib.fsb_unique(ctx.handle, _lib.ptr(q), _lib.ptr(t), _lib.ptr(dd), len(q), _lib.ptr(qo),
                                   _lib.ptr(to), ctypes.byref(n)), "fsb_unique")
     return qo[:n.value].copy(), to[:n.value].copy()
+
+
+# ------------------------------------------------------------------ camera geometry (device)
+def undistort_pixels(uv, k, device=0):
+    """camera.undistort_pixels (app/planesite/camera.py:5-31) on the device: distorted pixels
+    (n,2) -> ideal pinhole pixels with the same f, cx, cy; k = (f, cx, cy, k1, k2, p1, p2, k3).
+    float64, 25 fixed-point iterations in the reference's operation order."""
+    uv = np.ascontiguousarray(np.asarray(uv, np.float64).reshape(-1, 2))
+    k8 = np.ascontiguousarray(np.asarray(k, np.float64).reshape(8))
+    out = np.empty_like(uv)
+    if len(uv):
+        ctx = _lib.context(device)
+        _lib.check(ctx.lib.fsb_undistort_pixels(ctx.handle, _lib.ptr(uv), len(uv), _lib.ptr(k8), _lib.ptr(out)),
+                   "fsb_undistort_pixels")
+    return out
+
+
+def predict_ground(u, K_i, R_i, C_i, K_j, R_j, C_j, zg, device=0):
+    """The ground-plane prior of matching._predict (app/planesite/matching.py:155-172) on the
+    device: where undistorted pixels u (n,2) of image i land in image j when their rays meet the
+    plane z = zg. Returns (pred (n,2) float64, ok (n,) bool)."""
+    u = np.ascontiguousarray(np.asarray(u, np.float64).reshape(-1, 2))
+    mats = [np.ascontiguousarray(np.asarray(m, np.float64).reshape(-1))
+            for m in (np.linalg.inv(np.asarray(K_i, np.float64)), R_i, C_i, K_j, R_j, C_j)]
+    pred = np.empty_like(u)
+    ok = np.zeros(len(u), np.uint8)
+    if len(u):
+        ctx = _lib.context(device)
+        _lib.check(ctx.lib.fsb_predict_ground(ctx.handle, _lib.ptr(u), len(u), *[_lib.ptr(m) for m in mats],
+                                              float(zg), _lib.ptr(pred), _lib.ptr(ok)), "fsb_predict_ground")
+    return pred, ok.astype(bool)
+
+
+# ------------------------------------------------------------------ feature files
+def load_features(feat_dir, i, W, H):
+    """matching.load_features (app/planesite/matching.py:29-35): keypoints of feature file i in
+    full-resolution pixels (float64) and its uint8 RootSIFT descriptors."""
+    with np.load(os.path.join(feat_dir, "%d.npz" % i)) as d:
+        xy = d["xy"].astype(np.float64)
+        desc = d["desc"]
+        if len(xy):
+            rw, rh = d["red_wh"]
+            xy = (xy + 0.5) * np.array([W / float(rw), H / float(rh)]) - 0.5
+    return xy, desc
+
+
+def load_xy(feat_dir, i, W, H):
+    """matching.load_xy (app/planesite/matching.py:38-45): keypoint coordinates only."""
+    return load_features(feat_dir, i, W, H)[0]
+
+
+# ------------------------------------------------------------------ pair matching (worker side)
+# The worker context is the reference's pickled dict (feat_dir, W, H, K, dist, R, C, zg,
+# has_rot, prior_tol, guided_radius, min_inliers, ransac_thr and the optional n_coarse,
+# guided, guided_k, ratio, use_prior); init_worker / set_context install it per process.
+_CTX = None
+_CACHE = OrderedDict()
+_CACHE_MAX = 48
+
+
+def init_worker(ctx_file):
+    """matching.init_worker (app/planesite/matching.py:17-26): load the pickled worker context."""
+    with open(ctx_file, "rb") as f:
+        set_context(pickle.load(f))
+    try:
+        cv2.setNumThreads(1)
+    except Exception:
+        pass
+
+
+def set_context(ctx):
+    global _CTX
+    _CTX = ctx
+    _CACHE.clear()
+
+
+def _get(i, device=0):
+    """matching._get (app/planesite/matching.py:48-64): feature file i with undistorted keypoints
+    (on the device), uint8 descriptors and their squared norms, cached (least recently used)."""
+    if i in _CACHE:
+        _CACHE.move_to_end(i)
+        return _CACHE[i]
+    c = _CTX
+    xy, desc = load_features(c["feat_dir"], i, c["W"][i], c["H"][i])
+    und = xy
+    if len(xy):
+        K, dd = c["K"][i], c["dist"][i]
+        und = undistort_pixels(xy, (K[0, 0], K[0, 2], K[1, 2], dd[0], dd[1], dd[2], dd[3], dd[4]), device)
+    d = np.ascontiguousarray(desc, np.uint8)
+    df = d.astype(np.float32)
+    item = {"xy": xy, "und": und, "desc": d, "norm": (df * df).sum(1), "wh": (c["W"][i], c["H"][i])}
+    _CACHE[i] = item
+    while len(_CACHE) > _CACHE_MAX:
+        _CACHE.popitem(last=False)
+    return item
+
+
+def _predict(u, i, j, device=0):
+    """matching._predict (app/planesite/matching.py:155-172) with the worker context's cameras."""
+    c = _CTX
+    return predict_ground(u, c["K"][i], c["R"][i], c["C"][i], c["K"][j], c["R"][j], c["C"][j], c["zg"][i], device)
+
+
+def _prior_filter(q, t, ui, uj, i, j, tol, device=0):
+    """Keeps the pairs whose prior prediction of ui[q] lands within tol of uj[t]."""
+    pred, ok = _predict(ui[q], i, j, device)
+    keep = ok & (np.linalg.norm(pred - uj[t], axis=1) < tol)
+    return q[keep], t[keep]
+
+
+def _verify(c, i, j, ui, uj, q, t):
+    """matching._verify (app/planesite/matching.py:175-191): fundamental-matrix inliers (OpenCV
+    USAC_MAGSAC, plain RANSAC where MAGSAC rejects a degenerate set)."""
+    pi, pj = ui[q].astype(np.float32), uj[t].astype(np.float32)
+    F = mask = None
+    for method in (getattr(cv2, "USAC_MAGSAC", cv2.FM_RANSAC), cv2.FM_RANSAC):
+        try:
+            F, mask = cv2.findFundamentalMat(pi, pj, method, c["ransac_thr"], 0.999, 10000)
+            break
+        except cv2.error:
+            continue
+    if F is None or mask is None:
+        return None, None, 0
+    inl = mask.ravel().astype(bool)
+    return q[inl], t[inl], int(inl.sum())
+
+
+def _similarity(c, i, ui, uj, q, t):
+    """matching._similarity (app/planesite/matching.py:194-202): (rotation, scale, tx, ty) of the
+    inliers' partial affine fit, or None."""
+    try:
+        M, _ = cv2.estimateAffinePartial2D(ui[q].astype(np.float32), uj[t].astype(np.float32), method=cv2.RANSAC,
+                                           ransacReprojThreshold=0.02 * max(c["W"][i], c["H"][i]))
+    except Exception:
+        return None
+    if M is None:
+        return None
+    return (math.atan2(M[1, 0], M[0, 0]), math.hypot(M[0, 0], M[1, 0]), float(M[0, 2]), float(M[1, 2]))
+
+
+def _ratio_match(da, db, ratio, checks=None, device=0):
+    """The reference's exhaustive fallback (matching.py:74-83, a FLANN kd-forest ratio test) as the
+    exact device ratio test: the same ratio rule on the true nearest neighbours."""
+    return _ratio_match_bf(da, db, ratio, device=device)
+
+
+def _coarse_guided(c, i, j, A, B, use_prior, tol, device):
+    """Stage 1 of matching.match_pair (app/planesite/matching.py:217-233): the strongest n_coarse
+    features of each image, prior-filtered, give a RANSAC homography; guided matching around it
+    and fundamental verification. Returns (q, t, n_in) or None."""
+    ui, uj = A["und"], B["und"]
+    n1 = c.get("n_coarse", 1500)
+    if not (c.get("guided", True) and len(ui) > n1 // 2):
+        return None
+    q1, t1 = _ratio_match_bf(A["desc"][:n1], B["desc"][:n1], 0.85, device=device)
+    if use_prior and len(q1):
+        q1, t1 = _prior_filter(q1, t1, ui, uj, i, j, tol, device)
+    if len(q1) < 12:
+        return None
+    Hm, hm = cv2.findHomography(ui[q1], uj[t1], cv2.RANSAC, 0.012 * max(c["W"][i], c["H"][i]))
+    if Hm is None or hm is None or hm.sum() < 10:
+        return None
+    radius = c["guided_radius"] * max(c["W"][j], c["H"][j])
+    q, t = _guided(A, B, Hm, radius, c.get("guided_k", 24), 0.85, device)
+    if len(q) < c["min_inliers"]:
+        return None
+    q, t, n_in = _verify(c, i, j, ui, uj, q, t)
+    if q is None or n_in < max(c["min_inliers"], 40):
+        return None
+    return q, t, n_in
+
+
+def match_pair(task, device=0):
+    """matching.match_pair (app/planesite/matching.py:205-253) for task (i, j): returns
+    (i, j, q int32, t int32, similarity, n_inliers), or (i, j, None, None, None or an error tuple,
+    n) as the reference does. Descriptor matching (coarse exhaustive, guided, fallback) and the
+    camera geometry run on the device; RANSAC and the fundamental / similarity fits are OpenCV's,
+    as in the reference."""
+    i, j = task
+    c = _CTX
+    try:
+        A, B = _get(i, device), _get(j, device)
+        ui, uj = A["und"], B["und"]
+        if len(ui) < 30 or len(uj) < 30:
+            return i, j, None, None, None, 0
+        use_prior = c["has_rot"][i] and c["has_rot"][j] and c.get("use_prior", True)
+        tol = c["prior_tol"] * max(c["W"][j], c["H"][j])
+        result = _coarse_guided(c, i, j, A, B, use_prior, tol, device)
+        if result is None:
+            # exhaustive fallback (matching.py:234-246)
+            q, t = _ratio_match(A["desc"], B["desc"], c.get("ratio", 0.8), c.get("checks", 48), device)
+            if use_prior and len(q):
+                q, t = _prior_filter(q, t, ui, uj, i, j, tol, device)
+            if len(q) < 20:
+                return i, j, None, None, None, 0
+            q, t, n_in = _verify(c, i, j, ui, uj, q, t)
+            if q is None or n_in < c["min_inliers"]:
+                return i, j, None, None, None, n_in
+            result = (q, t, n_in)
+        q, t, n_in = result
+        return i, j, q.astype(np.int32), t.astype(np.int32), _similarity(c, i, ui, uj, q, t), n_in
+    except Exception as e:  # the reference reports a worker error in the similarity slot
+        import traceback
+        tb = traceback.extract_tb(e.__traceback__)[-1]
+        return i, j, None, None, ("error", "%s: %s (%s line %d)" % (type(e).__name__, e, os.path.basename(tb.filename),
+                                                                    tb.lineno)), 0

@@ -274,6 +274,18 @@ int32_t fsb_unique(fsb_ctx* ctx, const int64_t* q, const int64_t* t, const float
 /* cv2.perspectiveTransform of app/planesite/matching.py:115 on the device (float64):
    out = (H [x y 1]^T)_{xy} / (H [x y 1]^T)_z. */
 int32_t fsb_perspective(fsb_ctx* ctx, const double* xy, int32_t n, const double* hm9, double* out);
+/* camera.undistort_pixels (app/planesite/camera.py:5-31) on the device, float64: distorted pixels
+   uv (n,2) -> ideal pinhole pixels with the same f, cx, cy; k8 = f, cx, cy, k1, k2, p1, p2, k3;
+   25 fixed-point iterations in the reference's operation order (no fused multiply-add). */
+int32_t fsb_undistort_pixels(fsb_ctx* ctx, const double* uv, int32_t n, const double* k8, double* out);
+/* matching._predict (app/planesite/matching.py:155-172) on the device, float64: where the
+   undistorted pixels u (n,2) of image i land in image j under the ground-plane prior z = zg.
+   kinv_i = inverse of K_i, r_i / r_j world-to-camera rotations, c_i / c_j camera centres, k_j the
+   intrinsics of j (3x3 row-major). pred (n,2); ok[k] = 1 where the ray meets the plane in front of
+   camera i and the point lies in front of camera j. */
+int32_t fsb_predict_ground(fsb_ctx* ctx, const double* u, int32_t n, const double* kinv_i, const double* r_i,
+                           const double* c_i, const double* k_j, const double* r_j, const double* c_j, double zg,
+                           double* pred, uint8_t* ok);
 
 #ifdef __cplusplus
 }

@@ -23,3 +23,11 @@ def golden():
         with np.load(os.path.join(GOLDEN, name + ".npz")) as z:
             out[name] = {k: z[k] for k in z.files}
     return out
+
+
+@pytest.fixture(scope="session")
+def match_golden():
+    """The camera-geometry and pair-worker fixture (tests/golden/make_match_pair.py)."""
+    import numpy as np
+    with np.load(os.path.join(GOLDEN, "match_pair.npz")) as z:
+        return {k: z[k] for k in z.files}

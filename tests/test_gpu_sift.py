@@ -179,3 +179,25 @@ def test_capped_detect_is_prefix_of_full_list(fsb, golden, exact):
             assert len(got["x"]) == min(cap, n)
             for k in full:
                 np.testing.assert_array_equal(got[k], full[k][:cap], err_msg="%s cap %d" % (k, cap))
+
+
+def test_batch_entries_equal_single_calls(fsb, golden):
+    """sift_gpu_batch / detect_batch (images spread over several contexts) return exactly what the
+    single-image calls return, in input order; a batch state can be described afterwards."""
+    from fieldstitch_b200 import synth
+    imgs = [golden["sift_ref"][c + "/img"] for c in CASES] + [synth.synth_image(300, 410, 8)]
+    caps = [250, 120, 60, 400]
+    single = [fsb.features.sift_gpu_u8(im, nf) for im, nf in zip(imgs, caps)]
+    batch = fsb.features.sift_gpu_batch(imgs, caps, streams=3)
+    assert len(batch) == len(imgs)
+    for s, b in zip(single, batch):
+        for x, y in zip(s, b):
+            np.testing.assert_array_equal(x, y)
+    dets = fsb.gsift.detect_batch(imgs, max_kp=500, streams=2)
+    for im, (k, st) in zip(imgs, dets):
+        k1, _ = fsb.gsift.detect(im, max_kp=500)
+        for key in k1:
+            np.testing.assert_array_equal(k[key], k1[key])
+    k, st = dets[-1]
+    d = fsb.gsift.describe(st, k, np.arange(min(10, len(k["x"]))))
+    assert d.shape == (min(10, len(k["x"])), 128)
