@@ -918,6 +918,37 @@ int32_t fsb_unique(fsb_ctx* ctx, const int64_t* q, const int64_t* t, const float
     return FSB_OK;
 }
 
+int32_t fsb_clahe_d(fsb_ctx* ctx, const uint8_t* d_img, int32_t h, int32_t w, int32_t stride, double clip,
+                    int32_t tiles_x, int32_t tiles_y, uint8_t* d_out, int32_t out_stride) {
+    FSB_ARG(ctx && d_img && d_out, "null pointer");
+    FSB_ARG(h > 0 && w > 0 && stride >= w && out_stride >= w, "bad image size");
+    FSB_ARG(tiles_x >= 1 && tiles_y >= 1 && tiles_x * tiles_y <= 256, "tiles must be 1..256 in all");
+    FSB_TRY(use_device(ctx));
+    FSB_TRY(ctx->s_misc.ensure((size_t)tiles_x * tiles_y * 256));
+    return run_clahe(d_img, h, w, stride, clip, tiles_x, tiles_y, ctx->s_misc.as<uint8_t>(), d_out, out_stride,
+                     ctx->stream);
+}
+
+int32_t fsb_clahe(fsb_ctx* ctx, const uint8_t* img, int32_t h, int32_t w, int32_t stride, double clip,
+                  int32_t tiles_x, int32_t tiles_y, uint8_t* out, int32_t out_stride) {
+    FSB_ARG(ctx && img && out, "null pointer");
+    FSB_ARG(h > 0 && w > 0 && stride >= w && out_stride >= w, "bad image size");
+    FSB_ARG(tiles_x >= 1 && tiles_y >= 1 && tiles_x * tiles_y <= 256, "tiles must be 1..256 in all");
+    FSB_TRY(use_device(ctx));
+    cudaStream_t s = ctx->stream;
+    const size_t n = (size_t)h * w;
+    FSB_TRY(ctx->s_u8a.ensure(2 * n + 64));
+    uint8_t* din = ctx->s_u8a.as<uint8_t>();
+    uint8_t* dout = din + ((n + 63) & ~size_t(63));
+    FSB_CUDA(cudaMemcpy2DAsync(din, (size_t)w, img, (size_t)stride, (size_t)w, (size_t)h, cudaMemcpyHostToDevice, s));
+    FSB_TRY(ctx->s_misc.ensure((size_t)tiles_x * tiles_y * 256));
+    FSB_TRY(run_clahe(din, h, w, w, clip, tiles_x, tiles_y, ctx->s_misc.as<uint8_t>(), dout, w, s));
+    FSB_CUDA(cudaMemcpy2DAsync(out, (size_t)out_stride, dout, (size_t)w, (size_t)w, (size_t)h, cudaMemcpyDeviceToHost,
+                               s));
+    FSB_CUDA(cudaStreamSynchronize(s));
+    return FSB_OK;
+}
+
 int32_t fsb_undistort_pixels(fsb_ctx* ctx, const double* uv, int32_t n, const double* k8, double* out) {
     FSB_ARG(ctx && k8, "null pointer");
     FSB_ARG(n >= 0 && (n == 0 || (uv && out)), "bad points");

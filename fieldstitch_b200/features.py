@@ -84,3 +84,43 @@ def sift_gpu_batch(images, nfeats, streams=4, contrast=0.015, edge=12.0, exact=F
         raise ValueError("one keypoint cap per image")
     jobs = list(zip(images, nf))
     return _batch(lambda j: sift_gpu_u8(j[0], j[1], contrast, edge, exact, device), jobs, streams)
+
+
+def clahe(gray, clip=2.0, tiles=(8, 8), device=0):
+    """cv2.createCLAHE(clipLimit=clip, tileGridSize=tiles).apply(gray) on the device (the contrast
+    equalisation of features.prepare, app/planesite/features.py:70-71): identical uint8 output."""
+    g = _gray(gray)
+    out = np.empty(g.shape, np.uint8)
+    ctx = _lib.context(device)
+    _lib.check(ctx.lib.fsb_clahe(ctx.handle, _lib.ptr(g), g.shape[0], g.shape[1], g.strides[0], float(clip),
+                                 int(tiles[0]), int(tiles[1]), _lib.ptr(out), out.strides[0]), "fsb_clahe")
+    return out
+
+
+def prepare(buf, reduce, thumb_path, device=0):
+    """features.prepare (app/planesite/features.py:60-71): decode once (OpenCV, reduced-size JPEG
+    decoding as the reference does), write the colour thumbnail if missing, and return the grey
+    image contrast-equalised by CLAHE (clip 2.0, 8 x 8 tiles) on the device."""
+    import os
+
+    import cv2
+    flag_col = {1: cv2.IMREAD_COLOR, 2: cv2.IMREAD_REDUCED_COLOR_2, 4: cv2.IMREAD_REDUCED_COLOR_4,
+                8: cv2.IMREAD_REDUCED_COLOR_8}
+    flag_gray = {1: cv2.IMREAD_GRAYSCALE, 2: cv2.IMREAD_REDUCED_GRAYSCALE_2, 4: cv2.IMREAD_REDUCED_GRAYSCALE_4,
+                 8: cv2.IMREAD_REDUCED_GRAYSCALE_8}
+    if thumb_path and not os.path.exists(thumb_path):
+        col = cv2.imdecode(buf, flag_col[reduce] | cv2.IMREAD_IGNORE_ORIENTATION)
+        if col is None:
+            raise IOError("cannot decode image")
+        th = cv2.resize(col, ((col.shape[1] + 1) * reduce // 8, (col.shape[0] + 1) * reduce // 8),
+                        interpolation=cv2.INTER_AREA) if reduce < 8 else col
+        ok, enc = cv2.imencode(".jpg", th, [cv2.IMWRITE_JPEG_QUALITY, 88])
+        if not ok:
+            raise IOError("encode failed")
+        enc.tofile(thumb_path)
+        gray = cv2.cvtColor(col, cv2.COLOR_BGR2GRAY)
+    else:
+        gray = cv2.imdecode(buf, flag_gray[reduce] | cv2.IMREAD_IGNORE_ORIENTATION)
+        if gray is None:
+            raise IOError("cannot decode image")
+    return clahe(gray, 2.0, (8, 8), device)

@@ -274,6 +274,15 @@ int32_t fsb_unique(fsb_ctx* ctx, const int64_t* q, const int64_t* t, const float
 /* cv2.perspectiveTransform of app/planesite/matching.py:115 on the device (float64):
    out = (H [x y 1]^T)_{xy} / (H [x y 1]^T)_z. */
 int32_t fsb_perspective(fsb_ctx* ctx, const double* xy, int32_t n, const double* hm9, double* out);
+/* Contrast equalisation of features.prepare (app/planesite/features.py:60-71):
+   cv2.createCLAHE(clipLimit = clip, tileGridSize = (tiles_x, tiles_y)).apply(img) on a uint8 image,
+   identical output (OpenCV's tile extension, clipping, redistribution, LUT rounding and bilinear
+   blend); clip <= 0 disables clipping; tiles_x * tiles_y <= 256.
+   fsb_clahe takes host buffers, fsb_clahe_d device buffers (enqueued on the context's stream). */
+int32_t fsb_clahe(fsb_ctx* ctx, const uint8_t* img, int32_t h, int32_t w, int32_t stride, double clip,
+                  int32_t tiles_x, int32_t tiles_y, uint8_t* out, int32_t out_stride);
+int32_t fsb_clahe_d(fsb_ctx* ctx, const uint8_t* d_img, int32_t h, int32_t w, int32_t stride, double clip,
+                    int32_t tiles_x, int32_t tiles_y, uint8_t* d_out, int32_t out_stride);
 /* camera.undistort_pixels (app/planesite/camera.py:5-31) on the device, float64: distorted pixels
    uv (n,2) -> ideal pinhole pixels with the same f, cx, cy; k8 = f, cx, cy, k1, k2, p1, p2, k3;
    25 fixed-point iterations in the reference's operation order (no fused multiply-add). */
