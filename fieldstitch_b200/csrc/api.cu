@@ -918,6 +918,45 @@ int32_t fsb_unique(fsb_ctx* ctx, const int64_t* q, const int64_t* t, const float
     return FSB_OK;
 }
 
+int32_t fsb_build_tracks(fsb_ctx* ctx, const int64_t* u, const int64_t* v, int64_t n_edges, const int64_t* offsets,
+                         int32_t n_img, int64_t* tid, int64_t* img, int64_t* feat, int64_t* n_obs, int64_t* n_tracks) {
+    FSB_ARG(ctx && offsets && n_obs && n_tracks, "null pointer");
+    FSB_ARG(n_img >= 1 && n_edges >= 0, "bad sizes");
+    FSB_ARG(n_edges == 0 || (u && v && tid && img && feat), "null edge or output pointer");
+    for (int i = 0; i < n_img; ++i) FSB_ARG(offsets[i] >= 0 && offsets[i] <= offsets[i + 1], "offsets must ascend");
+    const long long T = offsets[n_img];
+    FSB_ARG(T < (1ll << 31) - 1, "at most 2^31 - 2 features in all");
+    for (int64_t e = 0; e < n_edges; ++e) FSB_ARG(u[e] >= 0 && u[e] < T && v[e] >= 0 && v[e] < T, "node out of range");
+    *n_obs = 0;
+    *n_tracks = 0;
+    if (n_edges == 0 || T == 0) return FSB_OK;
+    FSB_TRY(use_device(ctx));
+    cudaStream_t s = ctx->stream;
+    const size_t E = (size_t)n_edges;
+    FSB_TRY(ctx->s_i64.ensure(E * 16 + (size_t)(n_img + 1) * 8 + 64));
+    FSB_TRY(ctx->s_u64.ensure(E * 48 + 64));
+    long long* du = ctx->s_i64.as<long long>();
+    long long* dv = du + E;
+    long long* doff = dv + E;
+    long long* dtid = ctx->s_u64.as<long long>();
+    long long* dimg = dtid + 2 * E;
+    long long* dfeat = dimg + 2 * E;
+    FSB_CUDA(cudaMemcpyAsync(du, u, E * 8, cudaMemcpyHostToDevice, s));
+    FSB_CUDA(cudaMemcpyAsync(dv, v, E * 8, cudaMemcpyHostToDevice, s));
+    FSB_CUDA(cudaMemcpyAsync(doff, offsets, (size_t)(n_img + 1) * 8, cudaMemcpyHostToDevice, s));
+    int no = 0, nt = 0;
+    FSB_TRY(run_build_tracks(ctx, du, dv, n_edges, doff, n_img, (int)T, dtid, dimg, dfeat, &no, &nt, s));
+    if (no) {
+        FSB_CUDA(cudaMemcpyAsync(tid, dtid, (size_t)no * 8, cudaMemcpyDeviceToHost, s));
+        FSB_CUDA(cudaMemcpyAsync(img, dimg, (size_t)no * 8, cudaMemcpyDeviceToHost, s));
+        FSB_CUDA(cudaMemcpyAsync(feat, dfeat, (size_t)no * 8, cudaMemcpyDeviceToHost, s));
+    }
+    FSB_CUDA(cudaStreamSynchronize(s));
+    *n_obs = no;
+    *n_tracks = nt;
+    return FSB_OK;
+}
+
 int32_t fsb_clahe_d(fsb_ctx* ctx, const uint8_t* d_img, int32_t h, int32_t w, int32_t stride, double clip,
                     int32_t tiles_x, int32_t tiles_y, uint8_t* d_out, int32_t out_stride) {
     FSB_ARG(ctx && d_img && d_out, "null pointer");

@@ -231,6 +231,10 @@ int32_t run_mlp_train(fsb_ctx* ctx, float* prm, float* m, float* v, int n, const
 int32_t run_match_bf_tc(fsb_ctx* ctx, int n_pairs, const uint8_t* const* d_a, const int* na,
                         const uint8_t* const* d_b, const int* nb, float ratio, int precision, int64_t* const* q_out,
                         int64_t* const* t_out, int32_t* counts, TcStats* stats, cudaStream_t s);
+// tracks.cu
+int32_t run_build_tracks(fsb_ctx* ctx, const long long* d_u, const long long* d_v, long long ne, const long long* d_off,
+                         int n_img, int n_nodes, long long* d_tid, long long* d_img, long long* d_feat, int* n_obs,
+                         int* n_tracks, cudaStream_t s);
 // prep.cu
 int32_t run_clahe(const uint8_t* d_img, int h, int w, int stride, double clip, int tiles_x, int tiles_y,
                   uint8_t* d_lut, uint8_t* d_out, int out_stride, cudaStream_t s);

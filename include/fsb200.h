@@ -274,6 +274,14 @@ int32_t fsb_unique(fsb_ctx* ctx, const int64_t* q, const int64_t* t, const float
 /* cv2.perspectiveTransform of app/planesite/matching.py:115 on the device (float64):
    out = (H [x y 1]^T)_{xy} / (H [x y 1]^T)_z. */
 int32_t fsb_perspective(fsb_ctx* ctx, const double* xy, int32_t n, const double* hm9, double* out);
+/* recon.build_tracks (app/planesite/recon.py:14-54) on the device: feature tracks over the match
+   graph. Nodes are global feature indices (offsets[photo] + feature; offsets has n_img + 1
+   ascending entries, at most 2^31 - 2 features in all); every match is an edge u[e] - v[e]. A track
+   is a connected component of at least two matched features with no two features of the same
+   photo, numbered in the order of its smallest node; the observations (tid, img, feat; capacity
+   2 n_edges) are listed by track, then node. Same output as the reference. */
+int32_t fsb_build_tracks(fsb_ctx* ctx, const int64_t* u, const int64_t* v, int64_t n_edges, const int64_t* offsets,
+                         int32_t n_img, int64_t* tid, int64_t* img, int64_t* feat, int64_t* n_obs, int64_t* n_tracks);
 /* Contrast equalisation of features.prepare (app/planesite/features.py:60-71):
    cv2.createCLAHE(clipLimit = clip, tileGridSize = (tiles_x, tiles_y)).apply(img) on a uint8 image,
    identical output (OpenCV's tile extension, clipping, redistribution, LUT rounding and bilinear
