@@ -113,7 +113,7 @@ static int32_t detect_dev(fsb_ctx* ctx, Workspace& ws, const uint8_t* d_img, int
                           int max_kp) {
     const bool exact = (p->flags & FSB_SIFT_EXACT_BLUR) != 0;
     ctx->stage_begin(ST_PYRAMID);
-    FSB_TRY(run_pyramid(ws, d_img, stride, exact, ctx->stream));
+    FSB_TRY(run_pyramid(ws, d_img, stride, exact, ctx->stream, ctx->side, ctx->pyr_ev));
     ctx->stage_end(ST_PYRAMID);
     FSB_TRY(run_detect(ctx, ws, p->contrast, p->edge, max_kp, exact));
     return FSB_OK;
@@ -235,8 +235,14 @@ int32_t fsb_create(int32_t device, fsb_ctx** out) {
         set_error("cudaStreamCreate failed: %s", cudaGetErrorString(e));
         return FSB_ERR_CUDA;
     }
-    int32_t st = upload_taps();
+    bool ok = cudaStreamCreateWithFlags(&ctx->side, cudaStreamNonBlocking) == cudaSuccess;
+    for (auto& ev : ctx->pyr_ev) ok = ok && cudaEventCreateWithFlags(&ev, cudaEventDisableTiming) == cudaSuccess;
+    int32_t st = ok ? upload_taps() : FSB_ERR_CUDA;
     if (st != FSB_OK) {
+        if (!ok) set_error("side stream / event creation failed");
+        for (auto& ev : ctx->pyr_ev)
+            if (ev) cudaEventDestroy(ev);
+        if (ctx->side) cudaStreamDestroy(ctx->side);
         cudaStreamDestroy(ctx->stream);
         delete ctx;
         return st;
@@ -263,6 +269,10 @@ int32_t fsb_destroy(fsb_ctx* ctx) {
     if (ctx->pinned) cudaFreeHost(ctx->pinned);
     for (auto& e : ctx->ev)
         if (e) cudaEventDestroy(e);
+    if (ctx->side) cudaStreamSynchronize(ctx->side);
+    for (auto& e : ctx->pyr_ev)
+        if (e) cudaEventDestroy(e);
+    if (ctx->side) cudaStreamDestroy(ctx->side);
     cudaStreamDestroy(ctx->stream);
     delete ctx;
     return FSB_OK;

@@ -115,6 +115,20 @@ int32_t autotune(const char* key, int n_variants, int32_t (*run)(void*, int), vo
     return FSB_OK;
 }
 
+// The kept variant of `key` when it is known (or tuning is off: variant 0); false while the key
+// has not been tuned yet.
+bool autotune_cached(const char* key, int n_variants, int* variant) {
+    *variant = 0;
+    if (n_variants <= 1 || !tuning_on()) return true;
+    const std::string k = full_key(key);
+    std::lock_guard<std::mutex> lk(g_mu);
+    load_locked();
+    auto it = g_best.find(k);
+    if (it == g_best.end()) return false;
+    *variant = it->second < n_variants ? it->second : 0;
+    return true;
+}
+
 }  // namespace fsb
 
 // "key variant" lines of every choice made so far in this process (for reports); returns the

@@ -135,6 +135,8 @@ struct Workspace {
 struct fsb_ctx {
     int device = 0;
     cudaStream_t stream = nullptr;
+    cudaStream_t side = nullptr;                  // pyramid: each octave's last layers overlap the next octave
+    cudaEvent_t pyr_ev[2 * fsb::MAXO] = {};       // its fork / join events
     std::vector<fsb::Workspace*> pool;   // idle workspaces
     int live_states = 0;
     // scratch for description and matching (grown on demand)
@@ -169,7 +171,9 @@ constexpr uint32_t STATE_MAGIC = 0x51f7b200u;
 
 // ---------------------------------------------------------------- pyramid.cu
 int32_t upload_taps();
-int32_t run_pyramid(Workspace& ws, const uint8_t* d_img, int img_stride, bool exact, cudaStream_t s);
+// side / ev (2 MAXO events) may be null: then every octave runs on s alone
+int32_t run_pyramid(Workspace& ws, const uint8_t* d_img, int img_stride, bool exact, cudaStream_t s,
+                    cudaStream_t side = nullptr, cudaEvent_t* ev = nullptr);
 // octave.cu
 int32_t upload_octave_taps(const float* taps, int stride, const int* counts);
 int32_t launch_octave_fused(const float* L0, int R, int C, float* dog, float* mag, float* ang, float* down,
@@ -184,6 +188,7 @@ int32_t launch_group_lower(const float* src, int R, int C, float* dog, float* ma
 int32_t launch_group_upper(const float* src, int R, int C, float* dog3, cudaStream_t s);
 // autotune.cu: the fastest of n_variants launches of `run` for `key` (timed once per process and
 // device on `s`, then cached; FSB_AUTOTUNE=0 returns variant 0, FSB_AUTOTUNE_FILE persists choices)
+bool autotune_cached(const char* key, int n_variants, int* variant);
 int32_t autotune(const char* key, int n_variants, int32_t (*run)(void*, int), void* arg, cudaStream_t s, int* variant);
 
 // ---------------------------------------------------------------- detect.cu / describe.cu

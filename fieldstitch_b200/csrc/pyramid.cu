@@ -268,24 +268,42 @@ struct OctaveCall {
     float *x, *y, *dog, *mag, *ang, *down;
     int dc;
     cudaStream_t s;
+    // with a side stream, the octave's tail (layer 5, or the L4-L5 group) runs there after `fork`,
+    // since the next octave needs only L3's downsample; `join` marks its end
+    cudaStream_t side;
+    cudaEvent_t fork, join;
 };
 int32_t run_octave_call(void* p, int v) {
     const OctaveCall* c = static_cast<const OctaveCall*>(p);
     const long long RC = (long long)c->R * c->C;
+    cudaStream_t ts = c->s;   // stream of the tail
+    auto fork = [&]() -> int32_t {
+        if (!c->side) return FSB_OK;
+        FSB_CUDA(cudaEventRecord(c->fork, c->s));
+        FSB_CUDA(cudaStreamWaitEvent(c->side, c->fork, 0));
+        ts = c->side;
+        return FSB_OK;
+    };
     if (v == 1) {
         FSB_TRY(launch_group_lower(c->src, c->R, c->C, c->dog, c->mag, c->ang, c->x, c->down, c->dc, c->s));
-        return launch_group_upper(c->x, c->R, c->C, c->dog + 3 * RC, c->s);
+        FSB_TRY(fork());
+        FSB_TRY(launch_group_upper(c->x, c->R, c->C, c->dog + 3 * RC, ts));
+    } else {
+        FSB_TRY(tuned_layer(1, c->src, c->R, c->C, c->x, c->dog, nullptr, nullptr, nullptr, 0, c->s));
+        FSB_TRY(tuned_layer(2, c->x, c->R, c->C, c->y, c->dog + RC, c->mag, c->ang, nullptr, 0, c->s));
+        FSB_TRY(tuned_layer(3, c->y, c->R, c->C, c->x, c->dog + 2 * RC, c->mag + RC, c->ang + RC, nullptr, 0, c->s));
+        FSB_TRY(tuned_layer(4, c->x, c->R, c->C, c->y, c->dog + 3 * RC, c->mag + 2 * RC, c->ang + 2 * RC, c->down,
+                            c->dc, c->s));
+        FSB_TRY(fork());
+        FSB_TRY(tuned_layer(5, c->y, c->R, c->C, nullptr, c->dog + 4 * RC, nullptr, nullptr, nullptr, 0, ts));
     }
-    FSB_TRY(tuned_layer(1, c->src, c->R, c->C, c->x, c->dog, nullptr, nullptr, nullptr, 0, c->s));
-    FSB_TRY(tuned_layer(2, c->x, c->R, c->C, c->y, c->dog + RC, c->mag, c->ang, nullptr, 0, c->s));
-    FSB_TRY(tuned_layer(3, c->y, c->R, c->C, c->x, c->dog + 2 * RC, c->mag + RC, c->ang + RC, nullptr, 0, c->s));
-    FSB_TRY(tuned_layer(4, c->x, c->R, c->C, c->y, c->dog + 3 * RC, c->mag + 2 * RC, c->ang + 2 * RC, c->down, c->dc,
-                        c->s));
-    return tuned_layer(5, c->y, c->R, c->C, nullptr, c->dog + 4 * RC, nullptr, nullptr, nullptr, 0, c->s);
+    if (c->side) FSB_CUDA(cudaEventRecord(c->join, c->side));
+    return FSB_OK;
 }
 }  // namespace
 
-int32_t run_pyramid(Workspace& ws, const uint8_t* d_img, int img_stride, bool exact, cudaStream_t s) {
+int32_t run_pyramid(Workspace& ws, const uint8_t* d_img, int img_stride, bool exact, cudaStream_t s, cudaStream_t side,
+                    cudaEvent_t* ev) {
     const Geometry& g = ws.g;
     float* P[3] = {ws.plane[0].as<float>(), ws.plane[1].as<float>(), ws.plane[2].as<float>()};
     float* DF = ws.dog.as<float>();
@@ -311,24 +329,51 @@ int32_t run_pyramid(Workspace& ws, const uint8_t* d_img, int img_stride, bool ex
     const Engine eng = exact ? Engine::Layer : pyramid_engine();
     if (!exact && eng != Engine::Fused) {
         // octave o reads its base from P[0] (o = 0) or one half of next_base and writes the next
-        // base into the other half; P[1], P[2] (and P[0] after octave 0) hold layers in flight
+        // base into the other half; two of P[0..2] hold its layers in flight. With a side stream,
+        // an octave's tail (reading one of those planes) overlaps the next octave, which then takes
+        // the other two planes; before an octave starts, the tail two octaves back has ended, so at
+        // most one tail is in flight. While an octave size is being tuned its tail stays on s (the
+        // tuner times s only).
         float* NB = ws.next_base.as<float>();
         const long long half = g.n_oct > 1 ? ((long long)g.R[1] * g.C[1] + 63) / 64 * 64 : 0;
         const float* cur = P[0];
+        const float* tail_plane = nullptr;    // plane the latest side-stream tail reads
+        int prev_tail = -1, last_tail = -1;   // the two latest octaves whose tails ran on the side
         for (int o = 0; o < g.n_oct; ++o) {
             const bool last = o + 1 == g.n_oct;
-            OctaveCall c{cur, g.R[o], g.C[o], o == 0 ? P[1] : P[0], P[2], DF + g.dog_off[o], MAG + g.grad_off[o],
-                         ANG + g.grad_off[o], last ? nullptr : NB + (o & 1) * half, last ? 0 : g.C[o + 1], s};
-            if (eng == Engine::Auto) {
-                char key[64];
-                std::snprintf(key, sizeof(key), "k_octave_%dx%d", g.R[o], g.C[o]);
-                int v = 0;
+            // before this octave: every side tail has ended except the previous octave's (the side
+            // stream runs its tails in order, so one wait covers the earlier ones)
+            const float* busy = nullptr;
+            if (last_tail >= 0 && last_tail < o - 1) {
+                FSB_CUDA(cudaStreamWaitEvent(s, ev[2 * last_tail + 1], 0));
+            } else if (last_tail == o - 1 && last_tail >= 0) {
+                busy = tail_plane;
+                if (prev_tail >= 0) FSB_CUDA(cudaStreamWaitEvent(s, ev[2 * prev_tail + 1], 0));
+            }
+            float* pl[2];
+            for (int k = 0, n = 0; k < 3 && n < 2; ++k)
+                if (P[k] != cur && P[k] != busy) pl[n++] = P[k];
+            OctaveCall c{cur, g.R[o], g.C[o], pl[0], pl[1], DF + g.dog_off[o], MAG + g.grad_off[o],
+                         ANG + g.grad_off[o], last ? nullptr : NB + (o & 1) * half, last ? 0 : g.C[o + 1], s,
+                         nullptr, side ? ev[2 * o] : nullptr, side ? ev[2 * o + 1] : nullptr};
+            int v = eng == Engine::Group ? 1 : 0;
+            char key[64];
+            std::snprintf(key, sizeof(key), "k_octave_%dx%d", g.R[o], g.C[o]);
+            const bool known = eng != Engine::Auto || autotune_cached(key, 2, &v);
+            if (known && side) c.side = side;
+            if (eng == Engine::Auto && !known) {
                 FSB_TRY(autotune(key, 2, run_octave_call, &c, s, &v));
             } else {
-                FSB_TRY(run_octave_call(&c, eng == Engine::Group ? 1 : 0));
+                FSB_TRY(run_octave_call(&c, v));
+            }
+            if (c.side) {
+                tail_plane = v == 1 ? c.x : c.y;
+                prev_tail = last_tail;
+                last_tail = o;
             }
             cur = c.down;
         }
+        if (last_tail >= 0) FSB_CUDA(cudaStreamWaitEvent(s, ev[2 * last_tail + 1], 0));
         FSB_CUDA(cudaGetLastError());
         return FSB_OK;
     }
