@@ -101,6 +101,92 @@ static int32_t use_device(fsb_ctx* ctx) {
     return FSB_OK;
 }
 
+// Host side of the host-buffer entry points. Page-locked user memory is copied directly; pageable
+// memory goes through the context's own page-locked staging buffer (a CPU copy on the calling
+// thread), so contexts driven by several host threads do not queue behind one another in the
+// driver's shared staging of pageable copies. Within a call the staged inputs and outputs share
+// the buffer: the device-to-host copies follow the host-to-device ones on the context's stream,
+// and every host-buffer call ends synchronised.
+static bool host_pinned(const void* p) {
+    cudaPointerAttributes a;
+    if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    return a.type == cudaMemoryTypeHost;
+}
+
+static int32_t stage_ensure(fsb_ctx* ctx, size_t bytes) {
+    if (ctx->pinned_bytes >= bytes) return FSB_OK;
+    FSB_CUDA(cudaStreamSynchronize(ctx->stream));   // no copy in flight uses the old buffer
+    if (ctx->pinned) cudaFreeHost(ctx->pinned);
+    ctx->pinned = nullptr;
+    ctx->pinned_bytes = 0;
+    size_t nb = (size_t)4 << 20;
+    while (nb < bytes) nb <<= 1;
+    FSB_CUDA(cudaHostAlloc(&ctx->pinned, nb, cudaHostAllocDefault));
+    ctx->pinned_bytes = nb;
+    return FSB_OK;
+}
+
+struct HostCopy {
+    void* host;
+    void* dev;
+    size_t bytes;
+};
+
+static size_t al256(size_t x) { return (x + 255) & ~size_t(255); }
+
+// host -> device copies of k buffers, enqueued on the context's stream
+static int32_t copy_in(fsb_ctx* ctx, const HostCopy* c, int k) {
+    size_t total = 0;
+    bool direct[16];
+    for (int i = 0; i < k; ++i) {
+        direct[i] = c[i].bytes == 0 || host_pinned(c[i].host);
+        if (!direct[i]) total += al256(c[i].bytes);
+    }
+    if (total) FSB_TRY(stage_ensure(ctx, total));
+    char* st = static_cast<char*>(ctx->pinned);
+    for (int i = 0; i < k; ++i) {
+        if (c[i].bytes == 0) continue;
+        const void* src = c[i].host;
+        if (!direct[i]) {
+            std::memcpy(st, c[i].host, c[i].bytes);
+            src = st;
+            st += al256(c[i].bytes);
+        }
+        FSB_CUDA(cudaMemcpyAsync(c[i].dev, src, c[i].bytes, cudaMemcpyHostToDevice, ctx->stream));
+    }
+    return FSB_OK;
+}
+
+// device -> host copies of k buffers; returns with the data in the host buffers
+static int32_t copy_out(fsb_ctx* ctx, const HostCopy* c, int k) {
+    size_t total = 0;
+    bool direct[16];
+    for (int i = 0; i < k; ++i) {
+        direct[i] = c[i].bytes == 0 || host_pinned(c[i].host);
+        if (!direct[i]) total += al256(c[i].bytes);
+    }
+    if (total) FSB_TRY(stage_ensure(ctx, total));
+    char* st = static_cast<char*>(ctx->pinned);
+    char* at[16];
+    for (int i = 0; i < k; ++i) {
+        if (c[i].bytes == 0) continue;
+        void* dst = c[i].host;
+        if (!direct[i]) {
+            at[i] = st;
+            dst = st;
+            st += al256(c[i].bytes);
+        }
+        FSB_CUDA(cudaMemcpyAsync(dst, c[i].dev, c[i].bytes, cudaMemcpyDeviceToHost, ctx->stream));
+    }
+    FSB_CUDA(cudaStreamSynchronize(ctx->stream));
+    for (int i = 0; i < k; ++i)
+        if (c[i].bytes && !direct[i]) std::memcpy(c[i].host, at[i], c[i].bytes);
+    return FSB_OK;
+}
+
 template <class T>
 static int32_t to_dev(DevBuf& b, const T* h, size_t n, cudaStream_t s) {
     FSB_TRY(b.ensure(n * sizeof(T) + 16));
@@ -125,8 +211,16 @@ static int32_t detect_into(fsb_ctx* ctx, Workspace& ws, const uint8_t* img, int 
     cudaStream_t s = ctx->stream;
     FSB_TRY(prepare_workspace(ws, h, w));
     ctx->stage_begin(ST_UPLOAD);
-    FSB_CUDA(cudaMemcpy2DAsync(ws.img.p, (size_t)w, img, (size_t)stride, (size_t)w, (size_t)h,
-                               cudaMemcpyHostToDevice, s));
+    if (host_pinned(img)) {
+        FSB_CUDA(cudaMemcpy2DAsync(ws.img.p, (size_t)w, img, (size_t)stride, (size_t)w, (size_t)h,
+                                   cudaMemcpyHostToDevice, s));
+    } else {
+        // rows gathered into the context's page-locked buffer, one contiguous copy
+        FSB_TRY(stage_ensure(ctx, (size_t)h * w));
+        uint8_t* st = static_cast<uint8_t*>(ctx->pinned);
+        for (int r = 0; r < h; ++r) std::memcpy(st + (size_t)r * w, img + (size_t)r * stride, (size_t)w);
+        FSB_CUDA(cudaMemcpyAsync(ws.img.p, st, (size_t)h * w, cudaMemcpyHostToDevice, s));
+    }
     ctx->stage_end(ST_UPLOAD);
     return detect_dev(ctx, ws, ws.img.as<uint8_t>(), w, p, max_kp);
 }
@@ -484,13 +578,15 @@ int32_t fsb_sift_features(fsb_ctx* ctx, const uint8_t* img, int32_t h, int32_t w
     int n = 0;
     FSB_TRY(features_dev(ctx, *ws, nfeat, (p->flags & FSB_SIFT_EXACT_BLUR) != 0, dxy, drs, desc ? dd : nullptr,
                          rootsift ? ctx->s_u8a.as<uint8_t>() : nullptr, &n));
+    HostCopy out[4];
+    int k = 0;
     if (n) {
-        if (xy) FSB_CUDA(cudaMemcpyAsync(xy, dxy, (size_t)n * 8, cudaMemcpyDeviceToHost, s));
-        if (resp) FSB_CUDA(cudaMemcpyAsync(resp, drs, (size_t)n * 4, cudaMemcpyDeviceToHost, s));
-        if (desc) FSB_CUDA(cudaMemcpyAsync(desc, dd, (size_t)n * 512, cudaMemcpyDeviceToHost, s));
-        if (rootsift) FSB_CUDA(cudaMemcpyAsync(rootsift, ctx->s_u8a.p, (size_t)n * 128, cudaMemcpyDeviceToHost, s));
+        if (xy) out[k++] = {xy, dxy, (size_t)n * 8};
+        if (resp) out[k++] = {resp, drs, (size_t)n * 4};
+        if (desc) out[k++] = {desc, dd, (size_t)n * 512};
+        if (rootsift) out[k++] = {rootsift, ctx->s_u8a.p, (size_t)n * 128};
     }
-    FSB_CUDA(cudaStreamSynchronize(s));
+    FSB_TRY(copy_out(ctx, out, k));
     *n_out = n;
     return FSB_OK;
 }
@@ -870,13 +966,16 @@ int32_t fsb_match_guided(fsb_ctx* ctx, const double* pred_xy, const uint8_t* a, 
     if (na == 0 || nb == 0 || !(radius > 0.0)) return FSB_OK;
     FSB_TRY(use_device(ctx));
     cudaStream_t s = ctx->stream;
-    FSB_TRY(to_dev(ctx->s_u8a, a, (size_t)na * 128, s));
-    FSB_TRY(to_dev(ctx->s_u8b, b, (size_t)nb * 128, s));
+    FSB_TRY(ctx->s_u8a.ensure((size_t)na * 128 + 16));
+    FSB_TRY(ctx->s_u8b.ensure((size_t)nb * 128 + 16));
     FSB_TRY(ctx->s_f32a.ensure((size_t)(na + nb) * 16 + 256));
     double* dp = ctx->s_f32a.as<double>();
     double* dbx = dp + 2 * (size_t)na;
-    FSB_CUDA(cudaMemcpyAsync(dp, pred_xy, (size_t)na * 16, cudaMemcpyHostToDevice, s));
-    FSB_CUDA(cudaMemcpyAsync(dbx, b_xy, (size_t)nb * 16, cudaMemcpyHostToDevice, s));
+    const HostCopy in[4] = {{(void*)a, ctx->s_u8a.p, (size_t)na * 128},
+                            {(void*)b, ctx->s_u8b.p, (size_t)nb * 128},
+                            {(void*)pred_xy, dp, (size_t)na * 16},
+                            {(void*)b_xy, dbx, (size_t)nb * 16}};
+    FSB_TRY(copy_in(ctx, in, 4));
     FSB_TRY(ctx->s_i64.ensure((size_t)na * 16 + 64));
     int64_t* dq = ctx->s_i64.as<int64_t>();
     int64_t* dt = dq + na;
@@ -887,11 +986,8 @@ int32_t fsb_match_guided(fsb_ctx* ctx, const double* pred_xy, const uint8_t* a, 
     int n = 0;
     FSB_CUDA(cudaMemcpyAsync(&n, dn, sizeof(int), cudaMemcpyDeviceToHost, s));
     FSB_CUDA(cudaStreamSynchronize(s));
-    if (n) {
-        FSB_CUDA(cudaMemcpyAsync(q, dq, (size_t)n * 8, cudaMemcpyDeviceToHost, s));
-        FSB_CUDA(cudaMemcpyAsync(t, dt, (size_t)n * 8, cudaMemcpyDeviceToHost, s));
-        FSB_CUDA(cudaStreamSynchronize(s));
-    }
+    const HostCopy out[2] = {{q, dq, (size_t)n * 8}, {t, dt, (size_t)n * 8}};
+    FSB_TRY(copy_out(ctx, out, n ? 2 : 0));
     *n_out = n;
     return FSB_OK;
 }
