@@ -20,7 +20,7 @@ INCLUDE = os.path.join(os.path.dirname(HERE), "include")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 COMMON = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-I", INCLUDE, "--expt-relaxed-constexpr"]
 PER_FILE = {"detect.cu": ["--fmad=false"], "describe.cu": ["--fmad=false"], "geom.cu": ["--fmad=false"]}
-SOURCES = ["api.cu", "pyramid.cu", "octave.cu", "detect.cu", "describe.cu", "match.cu", "tc_match.cu", "mlp.cu", "autotune.cu", "geom.cu", "prep.cu", "tracks.cu"]
+SOURCES = ["api.cu", "pyramid.cu", "octave.cu", "detect.cu", "describe.cu", "match.cu", "tc_match.cu", "mlp.cu", "autotune.cu", "geom.cu", "prep.cu", "tracks.cu", "jpeg.cu"]
 
 
 def nvcc():
@@ -62,7 +62,7 @@ def build(verbose=False, jobs=None, extra=()):
     if failed:
         raise RuntimeError("\n".join("nvcc failed on %s:\n%s" % f for f in failed))
     if procs or not os.path.exists(LIB):
-        cmd = [nvcc(), *ARCH, "-shared", "-o", LIB, *objs, "-lcudart"]
+        cmd = [nvcc(), *ARCH, "-shared", "-o", LIB, *objs, "-lcudart", "-ldl"]
         if verbose:
             print(" ".join(cmd), flush=True)
         subprocess.check_call(cmd)

@@ -364,6 +364,7 @@ int32_t fsb_destroy(fsb_ctx* ctx) {
     for (auto& e : ctx->ev)
         if (e) cudaEventDestroy(e);
     if (ctx->side) cudaStreamSynchronize(ctx->side);
+    jpeg_release(ctx);
     for (auto& e : ctx->pyr_ev)
         if (e) cudaEventDestroy(e);
     if (ctx->side) cudaStreamDestroy(ctx->side);
@@ -1061,6 +1062,33 @@ int32_t fsb_build_tracks(fsb_ctx* ctx, const int64_t* u, const int64_t* v, int64
     *n_obs = no;
     *n_tracks = nt;
     return FSB_OK;
+}
+
+int32_t fsb_decode_gray_d(fsb_ctx* ctx, const uint8_t* data, int64_t len, int32_t reduce, uint8_t* d_out,
+                          int64_t out_cap, int32_t* h, int32_t* w) {
+    FSB_ARG(ctx && data && d_out && h && w, "null pointer");
+    FSB_ARG(len > 0 && out_cap > 0, "empty buffer");
+    FSB_ARG(reduce == 1 || reduce == 2 || reduce == 4 || reduce == 8, "reduce must be 1, 2, 4 or 8");
+    FSB_TRY(use_device(ctx));
+    return run_jpeg_gray(ctx, data, (size_t)len, reduce, d_out, (size_t)out_cap, h, w);
+}
+
+int32_t fsb_prepare_gray(fsb_ctx* ctx, const uint8_t* data, int64_t len, int32_t reduce, double clip, uint8_t* out,
+                         int64_t out_cap, int32_t* h, int32_t* w) {
+    FSB_ARG(ctx && data && out && h && w, "null pointer");
+    FSB_ARG(len > 0 && out_cap > 0, "empty buffer");
+    FSB_ARG(reduce == 1 || reduce == 2 || reduce == 4 || reduce == 8, "reduce must be 1, 2, 4 or 8");
+    FSB_TRY(use_device(ctx));
+    // decoded plane, then its equalised copy, in one scratch buffer
+    const size_t cap = (size_t)out_cap;
+    FSB_TRY(ctx->s_u8a.ensure(2 * cap + 512));
+    uint8_t* dg = ctx->s_u8a.as<uint8_t>();
+    uint8_t* de = dg + ((cap + 255) & ~size_t(255));
+    FSB_TRY(run_jpeg_gray(ctx, data, (size_t)len, reduce, dg, cap, h, w));
+    FSB_TRY(ctx->s_misc.ensure(64 * 256));
+    FSB_TRY(run_clahe(dg, *h, *w, *w, clip, 8, 8, ctx->s_misc.as<uint8_t>(), de, *w, ctx->stream));
+    const HostCopy o[1] = {{out, de, (size_t)(*h) * (*w)}};
+    return copy_out(ctx, o, 1);
 }
 
 int32_t fsb_clahe_d(fsb_ctx* ctx, const uint8_t* d_img, int32_t h, int32_t w, int32_t stride, double clip,

@@ -137,6 +137,8 @@ struct fsb_ctx {
     cudaStream_t stream = nullptr;
     cudaStream_t side = nullptr;                  // pyramid: each octave's last layers overlap the next octave
     cudaEvent_t pyr_ev[2 * fsb::MAXO] = {};       // its fork / join events
+    void* jpeg_handle = nullptr;                  // nvJPEG decoder of this context (created on first use)
+    void* jpeg_state = nullptr;
     std::vector<fsb::Workspace*> pool;   // idle workspaces
     int live_states = 0;
     // scratch for description and matching (grown on demand)
@@ -236,6 +238,10 @@ int32_t run_mlp_train(fsb_ctx* ctx, float* prm, float* m, float* v, int n, const
 int32_t run_match_bf_tc(fsb_ctx* ctx, int n_pairs, const uint8_t* const* d_a, const int* na,
                         const uint8_t* const* d_b, const int* nb, float ratio, int precision, int64_t* const* q_out,
                         int64_t* const* t_out, int32_t* counts, TcStats* stats, cudaStream_t s);
+// jpeg.cu
+int32_t run_jpeg_gray(fsb_ctx* ctx, const uint8_t* data, size_t len, int reduce, uint8_t* d_out, size_t out_cap,
+                      int* h, int* w);
+int32_t jpeg_release(fsb_ctx* ctx);
 // tracks.cu
 int32_t run_build_tracks(fsb_ctx* ctx, const long long* d_u, const long long* d_v, long long ne, const long long* d_off,
                          int n_img, int n_nodes, long long* d_tid, long long* d_img, long long* d_feat, int* n_obs,

@@ -124,3 +124,22 @@ def prepare(buf, reduce, thumb_path, device=0):
         if gray is None:
             raise IOError("cannot decode image")
     return clahe(gray, 2.0, (8, 8), device)
+
+
+def prepare_gpu(buf, reduce=1, clip=2.0, device=0):
+    """The grey half of features.prepare (app/planesite/features.py:60-71) entirely on the device:
+    nvJPEG decode of the luma plane (reduced by block means for reduce 2, 4, 8), then CLAHE (clip,
+    8 x 8 tiles). buf holds the JPEG file's bytes. Full-size decodes agree with OpenCV's grayscale
+    read to the inverse DCT's rounding; reduced ones approximately (OpenCV scales inside the DCT)."""
+    data = np.ascontiguousarray(np.frombuffer(buf, np.uint8) if not isinstance(buf, np.ndarray) else buf, np.uint8)
+    ctx = _lib.context(device)
+    h, w = ctypes.c_int32(), ctypes.c_int32()
+    cap = 1 << 22
+    while True:
+        out = np.empty(cap, np.uint8)
+        st = ctx.lib.fsb_prepare_gray(ctx.handle, _lib.ptr(data), len(data), int(reduce), float(clip), _lib.ptr(out),
+                                      cap, ctypes.byref(h), ctypes.byref(w))
+        if st == 0 or h.value * w.value <= cap:
+            _lib.check(st, "fsb_prepare_gray")
+            return out[:h.value * w.value].reshape(h.value, w.value)
+        cap = h.value * w.value

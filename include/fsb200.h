@@ -282,6 +282,17 @@ int32_t fsb_perspective(fsb_ctx* ctx, const double* xy, int32_t n, const double*
    2 n_edges) are listed by track, then node. Same output as the reference. */
 int32_t fsb_build_tracks(fsb_ctx* ctx, const int64_t* u, const int64_t* v, int64_t n_edges, const int64_t* offsets,
                          int32_t n_img, int64_t* tid, int64_t* img, int64_t* feat, int64_t* n_obs, int64_t* n_tracks);
+/* features.decode / prepare (app/planesite/features.py:18-71) on the device: the luma plane of a
+   JPEG held in host memory (data, len bytes), read at full size (reduce 1) or reduced by 2, 4, 8
+   (block means; OpenCV's reduced reads scale inside the inverse DCT, so those agree with OpenCV
+   approximately). fsb_decode_gray_d writes the plane to device memory (capacity out_cap, pitch =
+   width); fsb_prepare_gray also equalises it with CLAHE (clip, 8 x 8 tiles) and returns it in host
+   memory. *h, *w receive the output size. nvJPEG is loaded on first use (FSB_ERR_UNSUPPORTED
+   without it). */
+int32_t fsb_decode_gray_d(fsb_ctx* ctx, const uint8_t* data, int64_t len, int32_t reduce, uint8_t* d_out,
+                          int64_t out_cap, int32_t* h, int32_t* w);
+int32_t fsb_prepare_gray(fsb_ctx* ctx, const uint8_t* data, int64_t len, int32_t reduce, double clip, uint8_t* out,
+                         int64_t out_cap, int32_t* h, int32_t* w);
 /* Contrast equalisation of features.prepare (app/planesite/features.py:60-71):
    cv2.createCLAHE(clipLimit = clip, tileGridSize = (tiles_x, tiles_y)).apply(img) on a uint8 image,
    identical output (OpenCV's tile extension, clipping, redistribution, LUT rounding and bilinear
