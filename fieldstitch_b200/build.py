@@ -20,7 +20,7 @@ INCLUDE = os.path.join(os.path.dirname(HERE), "include")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 COMMON = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-I", INCLUDE, "--expt-relaxed-constexpr"]
 PER_FILE = {"detect.cu": ["--fmad=false"], "describe.cu": ["--fmad=false"], "geom.cu": ["--fmad=false"]}
-SOURCES = ["api.cu", "pyramid.cu", "octave.cu", "detect.cu", "describe.cu", "match.cu", "tc_match.cu", "mlp.cu", "autotune.cu", "geom.cu", "prep.cu", "tracks.cu", "jpeg.cu"]
+SOURCES = ["api.cu", "pyramid.cu", "octave.cu", "detect.cu", "describe.cu", "match.cu", "tc_match.cu", "mlp.cu", "autotune.cu", "geom.cu", "prep.cu", "tracks.cu", "jpeg.cu", "ransac.cu"]
 
 
 def nvcc():

@@ -238,6 +238,9 @@ int32_t run_mlp_train(fsb_ctx* ctx, float* prm, float* m, float* v, int n, const
 int32_t run_match_bf_tc(fsb_ctx* ctx, int n_pairs, const uint8_t* const* d_a, const int* na,
                         const uint8_t* const* d_b, const int* nb, float ratio, int precision, int64_t* const* q_out,
                         int64_t* const* t_out, int32_t* counts, TcStats* stats, cudaStream_t s);
+// ransac.cu
+int32_t run_ransac_h(const long long* d_off, int n_pairs, const double2* d_src, const double2* d_dst, double thr,
+                     int iters, unsigned long long seed, double* d_H, uint8_t* d_mask, int* d_ninl, cudaStream_t s);
 // jpeg.cu
 int32_t run_jpeg_gray(fsb_ctx* ctx, const uint8_t* data, size_t len, int reduce, uint8_t* d_out, size_t out_cap,
                       int* h, int* w);

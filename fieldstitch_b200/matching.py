@@ -224,6 +224,40 @@ def predict_ground(u, K_i, R_i, C_i, K_j, R_j, C_j, zg, device=0):
     return pred, ok.astype(bool)
 
 
+# ------------------------------------------------------------------ geometric verification
+def find_homography_batch(problems, thr, iters=1024, seed=0, device=0):
+    """RANSAC homographies of many pairs in one launch (cv2.findHomography(src, dst, cv2.RANSAC,
+    thr) as matching.match_pair calls it, app/planesite/matching.py:226). problems: list of (src
+    (n,2), dst (n,2)). Returns a list of (H (3,3) float64 or None, mask (n,1) uint8) per pair, in the
+    shape OpenCV returns; None where a pair has fewer than 4 correspondences or no usable sample."""
+    src = [np.asarray(s, np.float64).reshape(-1, 2) for s, _ in problems]
+    dst = [np.asarray(d, np.float64).reshape(-1, 2) for _, d in problems]
+    if any(len(a) != len(b) for a, b in zip(src, dst)):
+        raise ValueError("src and dst differ in length")
+    off = np.ascontiguousarray(np.r_[0, np.cumsum([len(a) for a in src])].astype(np.int64))
+    S = np.ascontiguousarray(np.concatenate(src) if src else np.zeros((0, 2)))
+    D = np.ascontiguousarray(np.concatenate(dst) if dst else np.zeros((0, 2)))
+    P = len(problems)
+    H = np.zeros((max(P, 1), 9))
+    mask = np.zeros(max(len(S), 1), np.uint8)
+    n_in = np.zeros(max(P, 1), np.int32)
+    if P:
+        ctx = _lib.context(device)
+        _lib.check(ctx.lib.fsb_find_homography_batch(ctx.handle, P, _lib.ptr(off), _lib.ptr(S), _lib.ptr(D),
+                                                     float(thr), int(iters), int(seed) & (2 ** 64 - 1), _lib.ptr(H),
+                                                     _lib.ptr(mask), _lib.ptr(n_in)), "fsb_find_homography_batch")
+    out = []
+    for p in range(P):
+        m = mask[off[p]:off[p + 1]].reshape(-1, 1).copy()
+        out.append((None if not H[p].any() else H[p].reshape(3, 3).copy(), m))
+    return out
+
+
+def find_homography(src, dst, thr, iters=1024, seed=0, device=0):
+    """One pair of find_homography_batch: (H or None, mask)."""
+    return find_homography_batch([(src, dst)], thr, iters, seed, device)[0]
+
+
 # ------------------------------------------------------------------ feature files
 def load_features(feat_dir, i, W, H):
     """matching.load_features (app/planesite/matching.py:29-35): keypoints of feature file i in
@@ -350,7 +384,11 @@ def _coarse_guided(c, i, j, A, B, use_prior, tol, device):
         q1, t1 = _prior_filter(q1, t1, ui, uj, i, j, tol, device)
     if len(q1) < 12:
         return None
-    Hm, hm = cv2.findHomography(ui[q1], uj[t1], cv2.RANSAC, 0.012 * max(c["W"][i], c["H"][i]))
+    thr = 0.012 * max(c["W"][i], c["H"][i])
+    if c.get("ransac", "opencv") == "device":   # the device RANSAC (statistically equal, not identical)
+        Hm, hm = find_homography(ui[q1], uj[t1], thr, device=device)
+    else:
+        Hm, hm = cv2.findHomography(ui[q1], uj[t1], cv2.RANSAC, thr)
     if Hm is None or hm is None or hm.sum() < 10:
         return None
     radius = c["guided_radius"] * max(c["W"][j], c["H"][j])

@@ -282,6 +282,17 @@ int32_t fsb_perspective(fsb_ctx* ctx, const double* xy, int32_t n, const double*
    2 n_edges) are listed by track, then node. Same output as the reference. */
 int32_t fsb_build_tracks(fsb_ctx* ctx, const int64_t* u, const int64_t* v, int64_t n_edges, const int64_t* offsets,
                          int32_t n_img, int64_t* tid, int64_t* img, int64_t* feat, int64_t* n_obs, int64_t* n_tracks);
+/* The stage-1 homography of matching.match_pair (app/planesite/matching.py:226,
+   cv2.findHomography(src, dst, cv2.RANSAC, thr)) for n_pairs pairs in one launch: pair p's
+   correspondences are src / dst rows offsets[p] .. offsets[p+1] - 1 (float64 (x, y)); `iters`
+   hypotheses per pair from 4-point samples (seeded, deterministic); inliers: squared reprojection
+   error <= thr^2; the homography (9 per pair, row-major, h33 = 1; zeros when a pair has fewer than
+   4 correspondences or no usable sample) is refined by least squares over the best hypothesis's
+   inliers; mask (one byte per correspondence) and n_inliers as OpenCV returns them. Random samples
+   differ from OpenCV's: results agree statistically. */
+int32_t fsb_find_homography_batch(fsb_ctx* ctx, int32_t n_pairs, const int64_t* offsets, const double* src,
+                                  const double* dst, double thr, int32_t iters, uint64_t seed, double* H, uint8_t* mask,
+                                  int32_t* n_inliers);
 /* features.decode / prepare (app/planesite/features.py:18-71) on the device: the luma plane of a
    JPEG held in host memory (data, len bytes), read at full size (reduce 1) or reduced by 2, 4, 8
    (block means; OpenCV's reduced reads scale inside the inverse DCT, so those agree with OpenCV
