@@ -24,8 +24,12 @@ void set_error(const char* fmt, ...) {
 
 int32_t DevBuf::ensure(size_t n) {
     if (n <= bytes && p) return FSB_OK;
-    release();
+    // geometric growth: buffers sized by data (keypoint and match counts) settle after a few calls;
+    // each regrowth frees, and cudaFree waits for the whole device (every stream of every context)
     size_t want = n < 256 ? 256 : n;
+    if (p && want < bytes + bytes / 2) want = bytes + bytes / 2;
+    if (want > ((size_t)1 << 20)) want = (want + ((size_t)1 << 20) - 1) & ~(((size_t)1 << 20) - 1);
+    release();
     cudaError_t e = cudaMalloc(&p, want);
     if (e != cudaSuccess) {
         p = nullptr;
