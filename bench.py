@@ -606,6 +606,8 @@ def run_fsb(args):
             "algorithmic_bytes": alg, "ms_per_launch_group": per_img_ms,
             "measured": "CUDA events on the library stream, one stream alone, %d images" % pyr_n,
             "ms_per_launch_group_in_timed_region": c_ms / max(c_n, 1)}
+    n_iso = max(pyr_n, 1)
+    iso_stages = {k: v[0] / n_iso for k, v in iso_st.items() if v[1] > 0}
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
@@ -653,7 +655,8 @@ def run_fsb(args):
                 "clocks": clk, "e2e": e2e, "gpu_launches": int(launches), "roofline": roof, "cpu_baseline": cpu,
                 "matches_per_step": matches / args.steps, "plain_single_stream": plain,
                 "dense_precision_sweep": sweep, "learned_filter": filt,
-                "stages_ms_per_step_summed_over_streams": {k: v[0] / args.steps for k, v in stages.items()}}
+                "stages_ms_per_step_summed_over_streams": {k: v[0] / args.steps for k, v in stages.items()},
+                "stages_ms_per_image_one_stream": iso_stages}
         print(json.dumps(line, default=_json_num), flush=True)
     pool.shutdown()
     for wk in workers:

@@ -286,22 +286,62 @@ static std::atomic<long long> g_launches{0};
 
 void fsb::note_launch(int n) { fsb::g_launches.fetch_add(n, std::memory_order_relaxed); }
 
+namespace {
+cudaEvent_t take_event(std::vector<cudaEvent_t>& free_list) {
+    cudaEvent_t e = nullptr;
+    if (!free_list.empty()) {
+        e = free_list.back();
+        free_list.pop_back();
+    } else if (cudaEventCreate(&e) != cudaSuccess) {
+        e = nullptr;
+    }
+    return e;
+}
+}  // namespace
+
 void fsb_ctx::stage_begin(int st) {
     if (!timing) return;
-    cudaEventRecord(ev[2 * st], stream);
-    ev_open[st] = true;
+    if (ev_open[st]) ev_free.push_back(ev_open[st]);
+    ev_open[st] = take_event(ev_free);
+    if (ev_open[st]) cudaEventRecord(ev_open[st], stream);
 }
 
 void fsb_ctx::stage_end(int st) {
     if (!timing || !ev_open[st]) return;
-    cudaEventRecord(ev[2 * st + 1], stream);
-    cudaEventSynchronize(ev[2 * st + 1]);
-    float ms = 0.f;
-    if (cudaEventElapsedTime(&ms, ev[2 * st], ev[2 * st + 1]) == cudaSuccess) {
-        stage_ms[st] += ms;
-        stage_n[st] += 1;
+    cudaEvent_t e1 = take_event(ev_free);
+    if (!e1) return;
+    cudaEventRecord(e1, stream);
+    ev_pending.push_back({st, ev_open[st], e1});
+    ev_open[st] = nullptr;
+    // the oldest pairs finished long ago in a busy pipeline: reading them back does not wait
+    if (ev_pending.size() >= 512) stage_resolve(64);
+}
+
+void fsb_ctx::stage_resolve(size_t keep) {
+    if (ev_pending.size() <= keep) return;
+    const size_t n = ev_pending.size() - keep;
+    for (size_t i = 0; i < n; ++i) {
+        const StageMark& m = ev_pending[i];
+        float ms = 0.f;
+        if (cudaEventSynchronize(m.e1) == cudaSuccess && cudaEventElapsedTime(&ms, m.e0, m.e1) == cudaSuccess) {
+            stage_ms[m.st] += ms;
+            stage_n[m.st] += 1;
+        }
+        ev_free.push_back(m.e0);
+        ev_free.push_back(m.e1);
     }
-    ev_open[st] = false;
+    ev_pending.erase(ev_pending.begin(), ev_pending.begin() + (std::ptrdiff_t)n);
+}
+
+void fsb_ctx::stage_release() {
+    stage_resolve(0);
+    for (cudaEvent_t& e : ev_open)
+        if (e) {
+            ev_free.push_back(e);
+            e = nullptr;
+        }
+    for (cudaEvent_t e : ev_free) cudaEventDestroy(e);
+    ev_free.clear();
 }
 
 using namespace fsb;
@@ -365,8 +405,7 @@ int32_t fsb_destroy(fsb_ctx* ctx) {
     if (ctx->gb_graph.exec) cudaGraphExecDestroy(ctx->gb_graph.exec);
     if (ctx->gb_graph.graph) cudaGraphDestroy(ctx->gb_graph.graph);
     if (ctx->pinned) cudaFreeHost(ctx->pinned);
-    for (auto& e : ctx->ev)
-        if (e) cudaEventDestroy(e);
+    ctx->stage_release();
     if (ctx->side) cudaStreamSynchronize(ctx->side);
     jpeg_release(ctx);
     for (auto& e : ctx->pyr_ev)
@@ -909,14 +948,21 @@ int64_t fsb_launch_count(void) { return fsb::g_launches.load(); }
 int32_t fsb_timing(fsb_ctx* ctx, int32_t on) {
     FSB_ARG(ctx, "ctx is null");
     FSB_TRY(use_device(ctx));
-    if (on && !ctx->ev[0])
-        for (auto& e : ctx->ev) FSB_CUDA(cudaEventCreate(&e));
+    // events for the stage marks are created here, not inside the timed pipeline
+    if (on)
+        while (ctx->ev_free.size() < 1024) {
+            cudaEvent_t e = nullptr;
+            FSB_CUDA(cudaEventCreate(&e));
+            ctx->ev_free.push_back(e);
+        }
     ctx->timing = on != 0;
     return FSB_OK;
 }
 
 int32_t fsb_stage_times(fsb_ctx* ctx, double* ms, int64_t* calls, int32_t n) {
     FSB_ARG(ctx && n >= 0, "bad arguments");
+    FSB_TRY(use_device(ctx));
+    ctx->stage_resolve(0);
     for (int i = 0; i < n && i < ST_COUNT; ++i) {
         if (ms) ms[i] = ctx->stage_ms[i];
         if (calls) calls[i] = ctx->stage_n[i];

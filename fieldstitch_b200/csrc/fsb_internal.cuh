@@ -151,14 +151,19 @@ struct fsb_ctx {
     fsb::TcStats tc_stats{};                      // of the last tensor-core dense match
     void* pinned = nullptr;
     size_t pinned_bytes = 0;
-    // stage timers: events recorded at stage boundaries while timing is on
+    // stage timers: event pairs recorded at stage boundaries while timing is on, read back lazily
+    // (when many are pending, and when the times are queried), so timing adds no host wait
+    struct StageMark { int st; cudaEvent_t e0, e1; };
     bool timing = false;
-    cudaEvent_t ev[2 * fsb::ST_COUNT] = {};
-    bool ev_open[fsb::ST_COUNT] = {};
+    std::vector<cudaEvent_t> ev_free;
+    std::vector<StageMark> ev_pending;
+    cudaEvent_t ev_open[fsb::ST_COUNT] = {};
     double stage_ms[fsb::ST_COUNT] = {};
     long long stage_n[fsb::ST_COUNT] = {};
     void stage_begin(int st);
-    void stage_end(int st);    // synchronises on the end event and accumulates
+    void stage_end(int st);
+    void stage_resolve(size_t keep);   // accumulates all but the newest `keep` pending pairs
+    void stage_release();
 };
 
 struct fsb_state {

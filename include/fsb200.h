@@ -67,7 +67,8 @@ int64_t fsb_device_bytes(fsb_ctx* ctx);
 int64_t fsb_launch_count(void);
 /* Per-stage device timing, the counterpart of gsift.detect(timings=dict)
    (app/planesite/gsift.py:441-446): while on, CUDA events bracket each stage on the context
-   stream. fsb_stage_times copies the accumulated milliseconds and call counts of the FSB_STAGE_*
+   stream; they are read back lazily, so timing adds no host wait to the pipeline (the reference
+   synchronises at each stage instead). fsb_stage_times waits for the pending ones, copies the accumulated milliseconds and call counts of the FSB_STAGE_*
    stages (n entries each, nullable) and resets them. */
 int32_t fsb_timing(fsb_ctx* ctx, int32_t on);
 int32_t fsb_stage_times(fsb_ctx* ctx, double* ms, int64_t* calls, int32_t n);

@@ -201,3 +201,27 @@ def test_batch_entries_equal_single_calls(fsb, golden):
     k, st = dets[-1]
     d = fsb.gsift.describe(st, k, np.arange(min(10, len(k["x"]))))
     assert d.shape == (min(10, len(k["x"])), 128)
+
+
+def test_stage_timers_accumulate_without_changing_results(fsb, golden):
+    """Stage timing (gsift.detect(timings=...)): every stage the sequence runs is counted once per
+    image with a positive time, the times reset when read, and results equal an untimed run."""
+    from fieldstitch_b200 import _lib
+    img, _, _, _, _, nfeat = _ref(golden, CASES[1])
+    ctx = _lib.context(0)
+    base = fsb.features.sift_gpu_u8(img, nfeat)
+    ctx.timing(True)
+    ctx.stage_times()
+    try:
+        runs = [fsb.features.sift_gpu_u8(img, nfeat) for _ in range(3)]
+        st = ctx.stage_times()
+        again = ctx.stage_times()
+    finally:
+        ctx.timing(False)
+    for r in runs:
+        for a, b in zip(r, base):
+            np.testing.assert_array_equal(a, b)
+    for name in ("pyramid", "extrema", "refine", "orientation", "describe"):
+        ms, n = st[name]
+        assert n == 3 and ms > 0.0, (name, st[name])
+    assert all(v == (0.0, 0) for v in again.values()), again
