@@ -1143,6 +1143,36 @@ int32_t fsb_find_homography_batch(fsb_ctx* ctx, int32_t n_pairs, const int64_t* 
     return copy_out(ctx, out, 3);
 }
 
+int32_t fsb_spread(fsb_ctx* ctx, const float* x, const float* y, const float* resp, int32_t n, int32_t W, int32_t H,
+                   int32_t nfeat, int32_t order, int32_t* sel, int32_t* n_out) {
+    FSB_ARG(ctx && n_out, "null pointer");
+    FSB_ARG(n >= 0 && nfeat >= 0, "negative size");
+    FSB_ARG(W > 0 && H > 0, "image size must be positive");
+    FSB_ARG(order == FSB_SPREAD_SELECTION || order == FSB_SPREAD_RESPONSE, "order must be 0 or 1");
+    FSB_ARG(n == 0 || (x && y && resp && sel), "null keypoint or output array");
+    *n_out = 0;
+    for (int32_t i = 1; i < n; ++i)
+        FSB_ARG(resp[i] <= resp[i - 1], "keypoints must be in response-descending order (as detect returns them)");
+    if (n == 0 || nfeat == 0) return FSB_OK;
+    FSB_TRY(use_device(ctx));
+    const size_t N = (size_t)n;
+    FSB_TRY(ctx->s_f32b.ensure(al256(N * 4) * 3));
+    FSB_TRY(ctx->s_i32.ensure(N * 4 + 256));
+    float* dx = ctx->s_f32b.as<float>();
+    float* dy = dx + al256(N * 4) / 4;
+    float* dr = dy + al256(N * 4) / 4;
+    int32_t* ds = ctx->s_i32.as<int32_t>();
+    const HostCopy in[3] = {{(void*)x, dx, N * 4}, {(void*)y, dy, N * 4}, {(void*)resp, dr, N * 4}};
+    FSB_TRY(copy_in(ctx, in, 3));
+    int n_sel = 0;
+    FSB_TRY(spread_dev(ctx, dx, dy, dr, n, (float)W, (float)H, nfeat, order == FSB_SPREAD_SELECTION, ds, &n_sel,
+                       ctx->stream));
+    const HostCopy out[1] = {{sel, ds, (size_t)n_sel * 4}};
+    FSB_TRY(copy_out(ctx, out, 1));
+    *n_out = n_sel;
+    return FSB_OK;
+}
+
 int32_t fsb_decode_gray_d(fsb_ctx* ctx, const uint8_t* data, int64_t len, int32_t reduce, uint8_t* d_out,
                           int64_t out_cap, int32_t* h, int32_t* w) {
     FSB_ARG(ctx && data && d_out && h && w, "null pointer");

@@ -297,45 +297,156 @@ __global__ void k_gather_ranked(const Oriented* __restrict__ slots, const uint32
 }
 
 // ------------------------------------------------------------------------------------ spread
-__global__ void k_cells(const float* __restrict__ x, const float* __restrict__ y, int n, float W, float H,
-                        uint32_t* __restrict__ cell, uint32_t* __restrict__ iota) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    int cx = (int)(x[i] / W * 12.f), cy = (int)(y[i] / H * 9.f);
-    cx = min(max(cx, 0), 11);
-    cy = min(max(cy, 0), 8);
-    cell[i] = (uint32_t)(cy * 12 + cx);
-    iota[i] = (uint32_t)i;
+// Grid-spread selection of features.py:38-57 on keypoints already in response-descending order
+// (the detector's output order; ties in detection order), restated without sorts:
+//   * cell = clip(int(x / W * 12), 0, 11) + 12 * clip(int(y / H * 9), 0, 8) in float32;
+//   * the reference orders by (cell, response descending, index), which on this input is
+//     (cell, index): an element's rank in its cell is the number of earlier elements of that cell;
+//   * "group 0" = rank < cap = ceil(nfeat / 108); their selection position is the cell's start
+//     (exclusive scan of min(count, cap) over cells) + rank; the others ("the rest", in index
+//     order = response order) follow from position n1 = the group-0 total; positions >= nfeat are
+//     dropped (sel[:n]);
+//   * the stable response sort of features.py:126 orders the selection by (response descending,
+//     selection position): index order, except inside a run of equal responses, where the
+//     selection positions decide.
+// The input is split into chunks of `ch` elements, one warp each: k_sp_hist counts cells per
+// chunk, k_sp_pos ranks inside the chunk (warp multi-split by __match_any_sync, chunk prefixes from
+// the histograms) and writes each element's selection position (or -1), k_sp_place scatters
+// the selected indices to their final slots.
+constexpr int SP_GX = 12, SP_GY = 9, SP_CELLS = SP_GX * SP_GY;
+
+__device__ __forceinline__ int sp_cell(float x, float y, float W, float H) {
+    int cx = (int)(x / W * (float)SP_GX), cy = (int)(y / H * (float)SP_GY);
+    cx = min(max(cx, 0), SP_GX - 1);
+    cy = min(max(cy, 0), SP_GY - 1);
+    return cy * SP_GX + cx;
 }
 
-// positions sorted by cell (ties by index): flag the first `cap` of each cell
-__global__ void k_cell_rank(const uint32_t* __restrict__ cell_sorted, int n, int cap, uint8_t* __restrict__ flag) {
-    const int p = blockIdx.x * blockDim.x + threadIdx.x;
-    if (p >= n) return;
-    // rank = p - first position with the same cell (binary search, cells are sorted)
-    const uint32_t c = cell_sorted[p];
-    int lo = 0, hi = p;
-    while (lo < hi) {
-        const int mid = (lo + hi) >> 1;
-        if (cell_sorted[mid] < c) lo = mid + 1; else hi = mid;
+__device__ __forceinline__ int warp_sum(int v) {
+#pragma unroll
+    for (int sh = 16; sh; sh >>= 1) v += __shfl_xor_sync(0xffffffffu, v, sh);
+    return v;
+}
+
+__global__ void __launch_bounds__(32) k_sp_hist(const float* __restrict__ x, const float* __restrict__ y, int n,
+                                                float W, float H, int ch, int* __restrict__ hist) {
+    __shared__ int h[SP_CELLS];
+    const int lane = threadIdx.x;
+    for (int c = lane; c < SP_CELLS; c += 32) h[c] = 0;
+    __syncwarp();
+    const int i0 = blockIdx.x * ch, i1 = min(i0 + ch, n);
+    for (int i = i0 + lane; i < i1; i += 32) atomicAdd(&h[sp_cell(x[i], y[i], W, H)], 1);
+    __syncwarp();
+    for (int c = lane; c < SP_CELLS; c += 32) hist[blockIdx.x * SP_CELLS + c] = h[c];
+}
+
+__global__ void __launch_bounds__(32) k_sp_pos(const float* __restrict__ x, const float* __restrict__ y, int n,
+                                               float W, float H, int ch, int nch, const int* __restrict__ hist,
+                                               int cap, int nfeat, int* __restrict__ pos,
+                                               int* __restrict__ chunk_sel) {
+    __shared__ int run[SP_CELLS];      // elements of the cell before the current step (all chunks)
+    __shared__ int start0[SP_CELLS];   // first selection position of the cell's group-0 elements
+    const int lane = threadIdx.x, k = blockIdx.x;
+    // lane owns cells 4 lane .. 4 lane + 3 (lanes 27..31 none)
+    int pre[4], tot[4], g0_pre = 0, g0_tot = 0;
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+        const int c = 4 * lane + q;
+        pre[q] = tot[q] = 0;
+        if (c < SP_CELLS)
+            for (int kk = 0; kk < nch; ++kk) {
+                const int v = hist[kk * SP_CELLS + c];
+                if (kk < k) pre[q] += v;
+                tot[q] += v;
+            }
+        g0_pre += min(pre[q], cap);
+        g0_tot += min(tot[q], cap);
     }
-    flag[p] = (p - lo) < cap ? 1 : 0;
+    int incl = g0_tot;
+#pragma unroll
+    for (int sh = 1; sh < 32; sh <<= 1) {
+        const int t = __shfl_up_sync(0xffffffffu, incl, sh);
+        if (lane >= sh) incl += t;
+    }
+    int st = incl - g0_tot;
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+        const int c = 4 * lane + q;
+        if (c < SP_CELLS) {
+            start0[c] = st;
+            run[c] = pre[q];
+        }
+        st += min(tot[q], cap);
+    }
+    const int n1 = __shfl_sync(0xffffffffu, incl, 31);
+    // elements of earlier chunks outside group 0: every earlier element minus the group-0 ones,
+    // which are the first min(pre, cap) of each cell
+    int g1_before = k * ch - warp_sum(g0_pre);
+    __syncwarp();
+    const int i0 = k * ch, i1 = min(i0 + ch, n);
+    int chosen = 0;
+    for (int base = i0; base < i1; base += 32) {
+        const int i = base + lane;
+        const bool v = i < i1;
+        const int c = v ? sp_cell(x[i], y[i], W, H) : SP_CELLS + lane;   // idle lanes: a key of their own
+        const unsigned peers = __match_any_sync(0xffffffffu, c);
+        const unsigned lt = (1u << lane) - 1u;
+        const int rl = __popc(peers & lt);
+        const int rank = v ? run[c] + rl : 0;
+        __syncwarp();
+        if (v && rl == 0) run[c] += __popc(peers);   // the lowest lane of the cell's peers advances it
+        __syncwarp();
+        const bool g0 = v && rank < cap;
+        const unsigned g1m = __ballot_sync(0xffffffffu, v && !g0);
+        int p = -1;
+        if (g0) p = start0[c] + rank;
+        else if (v) p = n1 + g1_before + __popc(g1m & lt);
+        g1_before += __popc(g1m);
+        const bool take = v && p < nfeat;
+        if (v) pos[i] = take ? p : -1;
+        chosen += __popc(__ballot_sync(0xffffffffu, take));
+    }
+    if (lane == 0) chunk_sel[k] = chosen;
 }
 
-__global__ void k_mark(const uint32_t* __restrict__ sel, int n_sel, uint8_t* __restrict__ chosen) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < n_sel) chosen[sel[i]] = 1;
+// final slot of each selected element: selected elements before it, corrected inside its run of
+// equal responses (elements of the run after it with a smaller selection position come first,
+// elements before it with a larger one come after). by_position: slot = selection position
+// (the order _spread returns) instead.
+__global__ void __launch_bounds__(32) k_sp_place(const float* __restrict__ resp, int n, int ch,
+                                                 const int* __restrict__ pos, const int* __restrict__ chunk_sel,
+                                                 bool by_position, int32_t* __restrict__ sel) {
+    const int lane = threadIdx.x, k = blockIdx.x;
+    int before = 0;
+    for (int kk = lane; kk < k; kk += 32) before += chunk_sel[kk];
+    before = warp_sum(before);
+    const int i0 = k * ch, i1 = min(i0 + ch, n);
+    for (int base = i0; base < i1; base += 32) {
+        const int i = base + lane;
+        const int p = i < i1 ? pos[i] : -1;
+        const unsigned cm = __ballot_sync(0xffffffffu, p >= 0);
+        if (p >= 0) {
+            int f = before + __popc(cm & ((1u << lane) - 1u));
+            if (by_position) {
+                f = p;
+            } else {
+                const float r = resp[i];
+                for (int j = i - 1; j >= 0 && resp[j] == r; --j)
+                    if (pos[j] > p) --f;
+                for (int j = i + 1; j < n && resp[j] == r; ++j) {
+                    const int pj = pos[j];
+                    if (pj >= 0 && pj < p) ++f;
+                }
+            }
+            sel[f] = i;
+        }
+        before += __popc(cm);
+    }
 }
 
-__global__ void k_not(const uint8_t* __restrict__ a, uint8_t* __restrict__ b, int n) {
+__global__ void k_iota(int32_t* __restrict__ out, int n) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < n) b[i] = a[i] ? 0 : 1;
-}
-
-__global__ void k_resp_keys(const uint32_t* __restrict__ sel, int n, const float* __restrict__ resp,
-                            uint32_t* __restrict__ key) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < n) key[i] = ~__float_as_uint(resp[sel[i]]);
+    if (i < n) out[i] = i;
 }
 
 inline unsigned blocks(long long n, int t) { return (unsigned)((n + t - 1) / t); }
@@ -468,70 +579,41 @@ int32_t run_detect(fsb_ctx* ctx, Workspace& ws, double contrast, double edge, in
     return FSB_OK;
 }
 
-// grid-spread selection of nfeat keypoints out of the detected (response-sorted) ones,
-// features.py:38-57 followed by the stable response sort of features.py:126. Writes the selected
-// keypoint indices to d_sel and their count to *n_sel.
-int32_t run_spread(const Workspace& ws, int nfeat, int32_t* d_sel_out, int* n_sel, fsb_ctx* ctx, cudaStream_t s) {
-    const int n = ws.n_kp;
-    uint32_t* sel = reinterpret_cast<uint32_t*>(d_sel_out);
+// grid-spread selection of nfeat keypoints out of n response-sorted ones (features.py:38-57),
+// then (by_position false) the stable response sort of features.py:126: d_sel receives
+// min(n, nfeat) keypoint indices. Three launches, no host wait.
+int32_t spread_dev(fsb_ctx* ctx, const float* d_x, const float* d_y, const float* d_resp, int n, float W, float H,
+                   int nfeat, bool by_position, int32_t* d_sel, int* n_sel, cudaStream_t s) {
+    *n_sel = 0;
+    if (n <= 0 || nfeat <= 0) return FSB_OK;
     if (n <= nfeat) {
-        // every keypoint, already in stable response order
-        std::vector<uint32_t> idx(n);
-        for (int i = 0; i < n; ++i) idx[i] = (uint32_t)i;
-        if (n) FSB_CUDA(cudaMemcpyAsync(sel, idx.data(), n * 4, cudaMemcpyHostToDevice, s));
-        FSB_CUDA(cudaStreamSynchronize(s));
+        // every keypoint, already in stable response order (and _spread returns range(n))
+        k_iota<<<blocks(n, 256), 256, 0, s>>>(d_sel, n);
+        note_launch();
+        FSB_CUDA(cudaGetLastError());
         *n_sel = n;
         return FSB_OK;
     }
-    const size_t N = (size_t)n;
-    FSB_TRY(ctx->s_misc.ensure(N * 4 * 7 + N * 2 + 64));
-    uint32_t* cell = ctx->s_misc.as<uint32_t>();
-    uint32_t* iota = cell + N;
-    uint32_t* cell_s = iota + N;
-    uint32_t* idx_s = cell_s + N;
-    uint32_t* rest = idx_s + N;
-    uint32_t* keyb = rest + N;
-    uint8_t* flag = reinterpret_cast<uint8_t*>(keyb + 2 * N);
-    uint8_t* chosen = flag + N;
-    FSB_TRY(ctx->s_i32.ensure(64));
-    int* d_cnt = ctx->s_i32.as<int>();
-    k_cells<<<blocks(n, 256), 256, 0, s>>>(ws.kx.as<float>(), ws.ky.as<float>(), n, (float)ws.g.w, (float)ws.g.h, cell, iota);
-    size_t t1 = 0, t2 = 0, t3 = 0;
-    cub::DeviceRadixSort::SortPairs(nullptr, t1, cell, cell_s, iota, idx_s, n, 0, 7, s);
-    cub::DeviceSelect::Flagged(nullptr, t2, idx_s, flag, sel, d_cnt, n, s);
-    cub::DeviceRadixSort::SortPairs(nullptr, t3, keyb, keyb, sel, sel, nfeat, 0, 32, s);
-    size_t tmax = t1 > t2 ? t1 : t2;
-    tmax = tmax > t3 ? tmax : t3;
-    FSB_TRY(ctx->s_misc2.ensure(tmax + N * 8 + 256));
-    void* tmp = ctx->s_misc2.p;
-    uint32_t* sel2 = reinterpret_cast<uint32_t*>(static_cast<char*>(tmp) + ((tmax + 255) / 256) * 256);
-    size_t tb = tmax;
-    FSB_CUDA(cub::DeviceRadixSort::SortPairs(tmp, tb, cell, cell_s, iota, idx_s, n, 0, 7, s));
-    const int cap = (nfeat + 107) / 108;
-    k_cell_rank<<<blocks(n, 256), 256, 0, s>>>(cell_s, n, cap, flag);
-    tb = tmax;
-    FSB_CUDA(cub::DeviceSelect::Flagged(tmp, tb, idx_s, flag, sel2, d_cnt, n, s));
-    int n1 = 0;
-    FSB_CUDA(cudaMemcpyAsync(&n1, d_cnt, sizeof(int), cudaMemcpyDeviceToHost, s));
-    FSB_CUDA(cudaStreamSynchronize(s));
-    if (n1 > nfeat) n1 = nfeat;
-    if (n1 < nfeat) {
-        FSB_CUDA(cudaMemsetAsync(chosen, 0, N, s));
-        if (n1 > 0) k_mark<<<blocks(n1, 256), 256, 0, s>>>(sel2, n1, chosen);
-        k_not<<<blocks(n, 256), 256, 0, s>>>(chosen, flag, n);
-        tb = tmax;
-        FSB_CUDA(cub::DeviceSelect::Flagged(tmp, tb, iota, flag, rest, d_cnt + 2, n, s));
-        // rest is in index order == response order (ties by index)
-        FSB_CUDA(cudaMemcpyAsync(sel2 + n1, rest, (size_t)(nfeat - n1) * 4, cudaMemcpyDeviceToDevice, s));
-    }
-    // stable sort of the selection by response, descending (features.py:126)
-    k_resp_keys<<<blocks(nfeat, 256), 256, 0, s>>>(sel2, nfeat, ws.kresp.as<float>(), keyb);
-    note_launch(n1 < nfeat ? 5 : 3);
-    tb = tmax;
-    FSB_CUDA(cub::DeviceRadixSort::SortPairs(tmp, tb, keyb, keyb + N, sel2, sel, nfeat, 0, 32, s));
+    // at most 64 chunks of a multiple of 1024 elements
+    const int ch = 1024 * (int)((n + 65535) / 65536);
+    const int nch = (n + ch - 1) / ch;
+    FSB_TRY(ctx->s_misc.ensure((size_t)nch * (SP_CELLS + 1) * 4 + (size_t)n * 4 + 512));
+    int* hist = ctx->s_misc.as<int>();
+    int* chunk_sel = hist + (size_t)nch * SP_CELLS;
+    int* pos = chunk_sel + nch;
+    const int cap = (nfeat + SP_CELLS - 1) / SP_CELLS;
+    k_sp_hist<<<nch, 32, 0, s>>>(d_x, d_y, n, W, H, ch, hist);
+    k_sp_pos<<<nch, 32, 0, s>>>(d_x, d_y, n, W, H, ch, nch, hist, cap, nfeat, pos, chunk_sel);
+    k_sp_place<<<nch, 32, 0, s>>>(d_resp, n, ch, pos, chunk_sel, by_position, d_sel);
+    note_launch(3);
     FSB_CUDA(cudaGetLastError());
     *n_sel = nfeat;
     return FSB_OK;
+}
+
+int32_t run_spread(const Workspace& ws, int nfeat, int32_t* d_sel_out, int* n_sel, fsb_ctx* ctx, cudaStream_t s) {
+    return spread_dev(ctx, ws.kx.as<float>(), ws.ky.as<float>(), ws.kresp.as<float>(), ws.n_kp, (float)ws.g.w,
+                      (float)ws.g.h, nfeat, false, d_sel_out, n_sel, s);
 }
 
 }  // namespace fsb

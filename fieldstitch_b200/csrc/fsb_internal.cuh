@@ -209,6 +209,8 @@ int32_t run_describe(const Workspace& ws, int n, const float* d_x, const float* 
                      const float* d_angle, const int32_t* d_oct, const int32_t* d_layer, float* d_desc,
                      uint8_t* d_u8, cudaStream_t s);
 int32_t run_spread(const Workspace& ws, int nfeat, int32_t* d_sel, int* n_sel, fsb_ctx* ctx, cudaStream_t s);
+int32_t spread_dev(fsb_ctx* ctx, const float* d_x, const float* d_y, const float* d_resp, int n, float W, float H,
+                   int nfeat, bool by_position, int32_t* d_sel, int* n_sel, cudaStream_t s);
 
 // ---------------------------------------------------------------- match.cu
 int32_t run_match_bf(fsb_ctx* ctx, const uint8_t* d_a, int na, const uint8_t* d_b, int nb, float ratio,

@@ -32,6 +32,36 @@ def _extract(g2, nfeat, contrast, edge, exact, want_desc, want_u8, device):
     return xy[:n], (desc[:n] if desc is not None else None), resp[:n], (u8[:n] if u8 is not None else None)
 
 
+def spread_arrays(x, y, resp, W, H, n, response_order=False, device=0):
+    """features._spread (app/planesite/features.py:38-57) on the device over keypoint arrays in
+    response-descending order (detect's order): int64 indices of min(len, n) keypoints spread over
+    a 12 x 9 grid, in _spread's order, or (response_order=True) after the stable response sort of
+    features.py:126. Ties among equal responses go by index."""
+    xs = np.ascontiguousarray(x, np.float32)
+    ys = np.ascontiguousarray(y, np.float32)
+    rs = np.ascontiguousarray(resp, np.float32)
+    if not (len(xs) == len(ys) == len(rs)):
+        raise ValueError("x, y and resp differ in length")
+    ctx = _lib.context(device)
+    out = np.empty(max(min(len(xs), int(n)), 1), np.int32)
+    k = ctypes.c_int32()
+    _lib.check(ctx.lib.fsb_spread(ctx.handle, _lib.ptr(xs), _lib.ptr(ys), _lib.ptr(rs), len(xs), int(W), int(H),
+                                  int(n), 1 if response_order else 0, _lib.ptr(out), ctypes.byref(k)), "fsb_spread")
+    return out[:k.value].astype(np.int64)
+
+
+def _spread(kps, W, H, n, gx=12, gy=9):
+    """features._spread with the reference's signature: kps are objects with .pt and .response
+    (cv2.KeyPoint or the reference's _KP), in response-descending order; returns a list of ints."""
+    if (gx, gy) != (12, 9):
+        raise ValueError("the device selection uses the reference's 12 x 9 grid")
+    if len(kps) <= n:
+        return list(range(len(kps)))
+    xy = np.array([k.pt for k in kps], np.float32).reshape(-1, 2)
+    r = np.array([k.response for k in kps], np.float32)
+    return spread_arrays(xy[:, 0], xy[:, 1], r, W, H, n).tolist()
+
+
 def sift_gpu(g2, nfeat, gpu=True, contrast=0.015, edge=12.0, exact=False, device=0):
     """features.sift_gpu (app/planesite/features.py:115-129): (xy, desc, resp, t_desc); returns
     zeros and None when fewer than 10 keypoints are found."""

@@ -112,6 +112,17 @@ int32_t fsb_state_free(fsb_state* st);
 int32_t fsb_state_geometry(fsb_state* st, int32_t* n_oct, int32_t* rows, int32_t* cols);
 int32_t fsb_state_atlas(fsb_state* st, int32_t which, float* out, int64_t n_floats);
 
+/* features._spread (app/planesite/features.py:38-57) on the device: n keypoints (x, y, response;
+   host arrays, responses non-increasing as detect returns them, else FSB_ERR_ARG) of a W x H
+   image; keeps min(n, nfeat) spread over a 12 x 9 grid (per cell the strongest first, at most
+   ceil(nfeat / 108) per cell, then the strongest of the rest, ties by index). order
+   FSB_SPREAD_SELECTION returns the indices in _spread's order, FSB_SPREAD_RESPONSE after the
+   stable response sort that follows it (features.py:126). sel holds min(n, nfeat) int32. */
+#define FSB_SPREAD_SELECTION 0
+#define FSB_SPREAD_RESPONSE 1
+int32_t fsb_spread(fsb_ctx* ctx, const float* x, const float* y, const float* resp, int32_t n, int32_t W, int32_t H,
+                   int32_t nfeat, int32_t order, int32_t* sel, int32_t* n_out);
+
 /* features.sift_gpu (app/planesite/features.py:115-129) in one device pass: detect with
    max_kp = int(2.2 nfeat) (p->max_kp is ignored), grid-spread selection of nfeat keypoints
    (features.py:38-57, ties by index), stable sort by response, describe, RootSIFT. Outputs hold
