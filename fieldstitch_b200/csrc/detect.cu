@@ -309,11 +309,14 @@ __global__ void k_gather_ranked(const Oriented* __restrict__ slots, const uint32
 //   * the stable response sort of features.py:126 orders the selection by (response descending,
 //     selection position): index order, except inside a run of equal responses, where the
 //     selection positions decide.
-// The input is split into chunks of `ch` elements, one warp each: k_sp_hist counts cells per
-// chunk, k_sp_pos ranks inside the chunk (warp multi-split by __match_any_sync, chunk prefixes from
-// the histograms) and writes each element's selection position (or -1), k_sp_place scatters
-// the selected indices to their final slots.
+// The input is split into chunks of `ch` elements (a multiple of 1024; at most 64 chunks), one
+// 1024-thread block each, one element per thread per step: k_sp_hist counts cells per chunk;
+// k_sp_pos ranks elements in their cells (per-warp multi-split by __match_any_sync, warps in
+// order through per-cell prefix sums, chunks in order through the histograms) and writes each
+// element's selection position (or -1) and the number selected per 32-element group; k_sp_place
+// (a warp per group) puts each selected index in its final slot.
 constexpr int SP_GX = 12, SP_GY = 9, SP_CELLS = SP_GX * SP_GY;
+constexpr int SP_T = 1024, SP_NW = SP_T / 32;
 
 __device__ __forceinline__ int sp_cell(float x, float y, float W, float H) {
     int cx = (int)(x / W * (float)SP_GX), cy = (int)(y / H * (float)SP_GY);
@@ -328,120 +331,160 @@ __device__ __forceinline__ int warp_sum(int v) {
     return v;
 }
 
-__global__ void __launch_bounds__(32) k_sp_hist(const float* __restrict__ x, const float* __restrict__ y, int n,
-                                                float W, float H, int ch, int* __restrict__ hist) {
+__global__ void __launch_bounds__(SP_T) k_sp_hist(const float* __restrict__ x, const float* __restrict__ y, int n,
+                                                  float W, float H, int ch, int* __restrict__ hist) {
     __shared__ int h[SP_CELLS];
-    const int lane = threadIdx.x;
-    for (int c = lane; c < SP_CELLS; c += 32) h[c] = 0;
-    __syncwarp();
+    const int tid = threadIdx.x;
+    if (tid < SP_CELLS) h[tid] = 0;
+    __syncthreads();
     const int i0 = blockIdx.x * ch, i1 = min(i0 + ch, n);
-    for (int i = i0 + lane; i < i1; i += 32) atomicAdd(&h[sp_cell(x[i], y[i], W, H)], 1);
-    __syncwarp();
-    for (int c = lane; c < SP_CELLS; c += 32) hist[blockIdx.x * SP_CELLS + c] = h[c];
+    for (int i = i0 + tid; i < i1; i += SP_T) atomicAdd(&h[sp_cell(x[i], y[i], W, H)], 1);
+    __syncthreads();
+    if (tid < SP_CELLS) hist[blockIdx.x * SP_CELLS + tid] = h[tid];
 }
 
-__global__ void __launch_bounds__(32) k_sp_pos(const float* __restrict__ x, const float* __restrict__ y, int n,
-                                               float W, float H, int ch, int nch, const int* __restrict__ hist,
-                                               int cap, int nfeat, int* __restrict__ pos,
-                                               int* __restrict__ chunk_sel) {
-    __shared__ int run[SP_CELLS];      // elements of the cell before the current step (all chunks)
-    __shared__ int start0[SP_CELLS];   // first selection position of the cell's group-0 elements
-    const int lane = threadIdx.x, k = blockIdx.x;
-    // lane owns cells 4 lane .. 4 lane + 3 (lanes 27..31 none)
-    int pre[4], tot[4], g0_pre = 0, g0_tot = 0;
+__global__ void __launch_bounds__(SP_T) k_sp_pos(const float* __restrict__ x, const float* __restrict__ y, int n,
+                                                 float W, float H, int ch, int nch, const int* __restrict__ hist,
+                                                 int cap, int nfeat, int* __restrict__ pos, int* __restrict__ grp_sel,
+                                                 int* __restrict__ chunk_sel) {
+    __shared__ int run[SP_CELLS];          // elements of the cell before the current step (all chunks)
+    __shared__ int start0[SP_CELLS];       // first selection position of the cell's group-0 elements
+    __shared__ int wc[SP_NW][SP_CELLS];    // per warp and cell: count, then the warp's base
+    __shared__ int wg1[SP_NW];             // per warp: elements outside group 0, then their base
+    __shared__ int s_n1, s_g1, s_sel;
+    const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5, k = blockIdx.x;
+    const unsigned lt = (1u << lane) - 1u;
+    if (w == 0) {
+        // lane owns cells 4 lane .. 4 lane + 3 (lanes 27..31 none)
+        int pre[4], tot[4], g0_pre = 0, g0_tot = 0;
 #pragma unroll
-    for (int q = 0; q < 4; ++q) {
-        const int c = 4 * lane + q;
-        pre[q] = tot[q] = 0;
-        if (c < SP_CELLS)
-            for (int kk = 0; kk < nch; ++kk) {
-                const int v = hist[kk * SP_CELLS + c];
-                if (kk < k) pre[q] += v;
-                tot[q] += v;
-            }
-        g0_pre += min(pre[q], cap);
-        g0_tot += min(tot[q], cap);
-    }
-    int incl = g0_tot;
-#pragma unroll
-    for (int sh = 1; sh < 32; sh <<= 1) {
-        const int t = __shfl_up_sync(0xffffffffu, incl, sh);
-        if (lane >= sh) incl += t;
-    }
-    int st = incl - g0_tot;
-#pragma unroll
-    for (int q = 0; q < 4; ++q) {
-        const int c = 4 * lane + q;
-        if (c < SP_CELLS) {
-            start0[c] = st;
-            run[c] = pre[q];
+        for (int q = 0; q < 4; ++q) {
+            const int c = 4 * lane + q;
+            pre[q] = tot[q] = 0;
+            if (c < SP_CELLS)
+                for (int kk = 0; kk < nch; ++kk) {
+                    const int v = hist[kk * SP_CELLS + c];
+                    if (kk < k) pre[q] += v;
+                    tot[q] += v;
+                }
+            g0_pre += min(pre[q], cap);
+            g0_tot += min(tot[q], cap);
         }
-        st += min(tot[q], cap);
+        int incl = g0_tot;
+#pragma unroll
+        for (int sh = 1; sh < 32; sh <<= 1) {
+            const int t = __shfl_up_sync(0xffffffffu, incl, sh);
+            if (lane >= sh) incl += t;
+        }
+        int st = incl - g0_tot;
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            const int c = 4 * lane + q;
+            if (c < SP_CELLS) {
+                start0[c] = st;
+                run[c] = pre[q];
+            }
+            st += min(tot[q], cap);
+        }
+        g0_pre = warp_sum(g0_pre);
+        if (lane == 31) s_n1 = incl;
+        // elements of earlier chunks outside group 0: every earlier element minus the group-0
+        // ones, which are the first min(pre, cap) of each cell
+        if (lane == 0) {
+            s_g1 = k * ch - g0_pre;
+            s_sel = 0;
+        }
     }
-    const int n1 = __shfl_sync(0xffffffffu, incl, 31);
-    // elements of earlier chunks outside group 0: every earlier element minus the group-0 ones,
-    // which are the first min(pre, cap) of each cell
-    int g1_before = k * ch - warp_sum(g0_pre);
-    __syncwarp();
+    __syncthreads();
+    const int n1 = s_n1;
     const int i0 = k * ch, i1 = min(i0 + ch, n);
-    int chosen = 0;
-    for (int base = i0; base < i1; base += 32) {
-        const int i = base + lane;
+    for (int base = i0; base < i1; base += SP_T) {
+        const int i = base + tid;
         const bool v = i < i1;
         const int c = v ? sp_cell(x[i], y[i], W, H) : SP_CELLS + lane;   // idle lanes: a key of their own
         const unsigned peers = __match_any_sync(0xffffffffu, c);
-        const unsigned lt = (1u << lane) - 1u;
         const int rl = __popc(peers & lt);
-        const int rank = v ? run[c] + rl : 0;
+        for (int q = lane; q < SP_CELLS; q += 32) wc[w][q] = 0;
         __syncwarp();
-        if (v && rl == 0) run[c] += __popc(peers);   // the lowest lane of the cell's peers advances it
-        __syncwarp();
+        if (v && rl == 0) wc[w][c] = __popc(peers);
+        __syncthreads();
+        if (tid < SP_CELLS) {
+            int acc = run[tid];
+            for (int ww = 0; ww < SP_NW; ++ww) {
+                const int t = wc[ww][tid];
+                wc[ww][tid] = acc;
+                acc += t;
+            }
+            run[tid] = acc;
+        }
+        __syncthreads();
+        const int rank = v ? wc[w][c] + rl : 0;
         const bool g0 = v && rank < cap;
         const unsigned g1m = __ballot_sync(0xffffffffu, v && !g0);
+        if (lane == 0) wg1[w] = __popc(g1m);
+        __syncthreads();
+        if (w == 0) {
+            const int cnt = wg1[lane];
+            int incl = cnt;
+#pragma unroll
+            for (int sh = 1; sh < 32; sh <<= 1) {
+                const int t = __shfl_up_sync(0xffffffffu, incl, sh);
+                if (lane >= sh) incl += t;
+            }
+            const int g1b = s_g1;
+            wg1[lane] = g1b + incl - cnt;
+            __syncwarp();
+            if (lane == 31) s_g1 = g1b + incl;
+        }
+        __syncthreads();
         int p = -1;
         if (g0) p = start0[c] + rank;
-        else if (v) p = n1 + g1_before + __popc(g1m & lt);
-        g1_before += __popc(g1m);
+        else if (v) p = n1 + wg1[w] + __popc(g1m & lt);
         const bool take = v && p < nfeat;
         if (v) pos[i] = take ? p : -1;
-        chosen += __popc(__ballot_sync(0xffffffffu, take));
+        const unsigned tm = __ballot_sync(0xffffffffu, take);
+        if (lane == 0 && base + 32 * w < i1) {
+            grp_sel[(base + 32 * w) >> 5] = __popc(tm);
+            atomicAdd(&s_sel, __popc(tm));
+        }
     }
-    if (lane == 0) chunk_sel[k] = chosen;
+    __syncthreads();
+    if (tid == 0) chunk_sel[k] = s_sel;
 }
 
-// final slot of each selected element: selected elements before it, corrected inside its run of
-// equal responses (elements of the run after it with a smaller selection position come first,
-// elements before it with a larger one come after). by_position: slot = selection position
-// (the order _spread returns) instead.
-__global__ void __launch_bounds__(32) k_sp_place(const float* __restrict__ resp, int n, int ch,
-                                                 const int* __restrict__ pos, const int* __restrict__ chunk_sel,
-                                                 bool by_position, int32_t* __restrict__ sel) {
-    const int lane = threadIdx.x, k = blockIdx.x;
+// final slot of each selected element: selected elements before it (earlier chunks, earlier
+// groups of its chunk, earlier lanes), corrected inside its run of equal responses (elements of
+// the run after it with a smaller selection position come first, elements before it with a
+// larger one come after). by_position: slot = selection position (the order _spread returns).
+__global__ void __launch_bounds__(256) k_sp_place(const float* __restrict__ resp, int n, int ch,
+                                                  const int* __restrict__ pos, const int* __restrict__ grp_sel,
+                                                  const int* __restrict__ chunk_sel, bool by_position,
+                                                  int32_t* __restrict__ sel) {
+    const int lane = threadIdx.x & 31;
+    const int g = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;   // 32-element group
+    if (g * 32 >= n) return;
+    const int k = (g * 32) / ch;
     int before = 0;
     for (int kk = lane; kk < k; kk += 32) before += chunk_sel[kk];
+    for (int gg = (k * ch >> 5) + lane; gg < g; gg += 32) before += grp_sel[gg];
     before = warp_sum(before);
-    const int i0 = k * ch, i1 = min(i0 + ch, n);
-    for (int base = i0; base < i1; base += 32) {
-        const int i = base + lane;
-        const int p = i < i1 ? pos[i] : -1;
-        const unsigned cm = __ballot_sync(0xffffffffu, p >= 0);
-        if (p >= 0) {
-            int f = before + __popc(cm & ((1u << lane) - 1u));
-            if (by_position) {
-                f = p;
-            } else {
-                const float r = resp[i];
-                for (int j = i - 1; j >= 0 && resp[j] == r; --j)
-                    if (pos[j] > p) --f;
-                for (int j = i + 1; j < n && resp[j] == r; ++j) {
-                    const int pj = pos[j];
-                    if (pj >= 0 && pj < p) ++f;
-                }
-            }
-            sel[f] = i;
+    const int i = g * 32 + lane;
+    const int p = i < n ? pos[i] : -1;
+    const unsigned cm = __ballot_sync(0xffffffffu, p >= 0);
+    if (p < 0) return;
+    int f = before + __popc(cm & ((1u << lane) - 1u));
+    if (by_position) {
+        f = p;
+    } else {
+        const float r = resp[i];
+        for (int j = i - 1; j >= 0 && resp[j] == r; --j)
+            if (pos[j] > p) --f;
+        for (int j = i + 1; j < n && resp[j] == r; ++j) {
+            const int pj = pos[j];
+            if (pj >= 0 && pj < p) ++f;
         }
-        before += __popc(cm);
     }
+    sel[f] = i;
 }
 
 __global__ void k_iota(int32_t* __restrict__ out, int n) {
@@ -597,14 +640,17 @@ int32_t spread_dev(fsb_ctx* ctx, const float* d_x, const float* d_y, const float
     // at most 64 chunks of a multiple of 1024 elements
     const int ch = 1024 * (int)((n + 65535) / 65536);
     const int nch = (n + ch - 1) / ch;
-    FSB_TRY(ctx->s_misc.ensure((size_t)nch * (SP_CELLS + 1) * 4 + (size_t)n * 4 + 512));
+    const int ngrp = (n + 31) / 32;
+    FSB_TRY(ctx->s_misc.ensure(((size_t)nch * (SP_CELLS + 1) + (size_t)ngrp + (size_t)n) * 4 + 512));
     int* hist = ctx->s_misc.as<int>();
     int* chunk_sel = hist + (size_t)nch * SP_CELLS;
-    int* pos = chunk_sel + nch;
+    int* grp_sel = chunk_sel + nch;
+    int* pos = grp_sel + ngrp;
     const int cap = (nfeat + SP_CELLS - 1) / SP_CELLS;
-    k_sp_hist<<<nch, 32, 0, s>>>(d_x, d_y, n, W, H, ch, hist);
-    k_sp_pos<<<nch, 32, 0, s>>>(d_x, d_y, n, W, H, ch, nch, hist, cap, nfeat, pos, chunk_sel);
-    k_sp_place<<<nch, 32, 0, s>>>(d_resp, n, ch, pos, chunk_sel, by_position, d_sel);
+    k_sp_hist<<<nch, SP_T, 0, s>>>(d_x, d_y, n, W, H, ch, hist);
+    k_sp_pos<<<nch, SP_T, 0, s>>>(d_x, d_y, n, W, H, ch, nch, hist, cap, nfeat, pos, grp_sel, chunk_sel);
+    k_sp_place<<<blocks((long long)ngrp * 32, 256), 256, 0, s>>>(d_resp, n, ch, pos, grp_sel, chunk_sel,
+                                                                   by_position, d_sel);
     note_launch(3);
     FSB_CUDA(cudaGetLastError());
     *n_sel = nfeat;
