@@ -7,7 +7,8 @@
 //   k_extrema   3x3x3 extrema of DoG layers 1..3 (gsift.py:293-319), warp-aggregated append
 //   k_refine    sub-pixel fit, contrast and edge tests (gsift.py:322-369), thread per candidate
 //   orientation peaks come from describe.cu (run_orient)
-//   sort        stable radix sorts: (extremum index, bin) then response descending (gsift.py:471)
+//   sort        rank of the refined extrema: stable radix sort by response, DoG index inside ties
+//               (gsift.py:471)
 //   k_gather    keypoint fields in input-image pixels (gsift.py:462-474)
 //   spread      grid-spread selection of features.py:38-57
 #include <cub/cub.cuh>
@@ -260,15 +261,36 @@ __device__ __forceinline__ float kp_scale(int l, float x2) {
     return 1.6f * exp2f(t);
 }
 
-// rank key of a refined extremum (31 + fbits bits): response descending (a positive finite float's
-// bits order like its value), then DoG-atlas index ascending (f < 2^fbits)
-__global__ void k_rank_keys(const Refined* __restrict__ ref, uint32_t n, int fbits,
-                            unsigned long long* __restrict__ key, uint32_t* __restrict__ val) {
+// rank key of a refined extremum: response descending (a positive finite float's bits order like
+// its value); the DoG-atlas index breaks ties afterwards (k_rank_ties)
+__global__ void k_rank_keys(const Refined* __restrict__ ref, uint32_t n, uint32_t* __restrict__ key,
+                            uint32_t* __restrict__ val) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
-    const Refined r = ref[i];
-    key[i] = ((unsigned long long)(0x7fffffffu - __float_as_uint(r.resp)) << fbits) | (unsigned long long)r.f;
+    key[i] = 0x7fffffffu - __float_as_uint(ref[i].resp);
     val[i] = i;
+}
+
+// ranks from the (stable) response sort: inside a run of equal responses the extrema are ordered
+// by DoG-atlas index (their order in the refined list is the atomic append order), so an element
+// goes to the run's start + the number of run members with a smaller index
+__global__ void k_rank_ties(const uint32_t* __restrict__ key, const uint32_t* __restrict__ val,
+                            const Refined* __restrict__ ref, uint32_t n, uint32_t* __restrict__ order) {
+    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n) return;
+    const uint32_t k = key[t], v = val[t];
+    uint32_t a = t, b = t + 1;
+    while (a > 0 && key[a - 1] == k) --a;
+    while (b < n && key[b] == k) ++b;
+    if (b - a == 1) {
+        order[t] = v;
+        return;
+    }
+    const uint32_t f = ref[v].f;
+    uint32_t r = a;
+    for (uint32_t u = a; u < b; ++u)
+        if (ref[val[u]].f < f) ++r;
+    order[r] = v;
 }
 
 // keypoints in final order: rank t's peaks (bin order) at pos[t] .. pos[t] + cnt[t] - 1, kept below
@@ -561,26 +583,26 @@ int32_t run_detect(fsb_ctx* ctx, Workspace& ws, double contrast, double edge, in
     // extrema once, orient them rank by rank until their peaks fill max_kp (an extremum may have
     // none), and lay the peaks out by an exclusive scan of the per-rank counts.
     ctx->stage_begin(ST_SORT);
-    int fbits = 1;
-    while ((1ull << fbits) < (unsigned long long)g.dog_off[g.n_oct]) ++fbits;
-    const int end_bit = 31 + fbits;
-    FSB_TRY(ws.keys_a.ensure((size_t)n_ref * 8 * 2));
+    // a stable 31-bit sort by response, then the index order inside runs of equal responses:
+    // (response descending, DoG index ascending) with half the radix passes of one 63-bit key
+    FSB_TRY(ws.keys_a.ensure((size_t)n_ref * 4 * 2));
     FSB_TRY(ws.vals_a.ensure((size_t)n_ref * 4 * 2));
     FSB_TRY(ws.keys_b.ensure((size_t)n_ref * 4 * 2));
-    unsigned long long* ka = ws.keys_a.as<unsigned long long>();
+    uint32_t* ka = ws.keys_a.as<uint32_t>();
     uint32_t* va = ws.vals_a.as<uint32_t>();
     uint32_t* rcnt = ws.keys_b.as<uint32_t>();
     uint32_t* rpos = rcnt + n_ref;
     size_t t1 = 0, t2 = 0;
-    cub::DeviceRadixSort::SortPairs(nullptr, t1, ka, ka + n_ref, va, va + n_ref, (int)n_ref, 0, end_bit, s);
+    cub::DeviceRadixSort::SortPairs(nullptr, t1, ka, ka + n_ref, va, va + n_ref, (int)n_ref, 0, 31, s);
     cub::DeviceScan::ExclusiveSum(nullptr, t2, rcnt, rpos, (int)n_ref, s);
     FSB_TRY(ws.sort_tmp.ensure(t1 > t2 ? t1 : t2));
-    k_rank_keys<<<blocks(n_ref, 256), 256, 0, s>>>(ws.refined.as<Refined>(), n_ref, fbits, ka, va);
+    k_rank_keys<<<blocks(n_ref, 256), 256, 0, s>>>(ws.refined.as<Refined>(), n_ref, ka, va);
     size_t tb = ws.sort_tmp.bytes;
-    FSB_CUDA(cub::DeviceRadixSort::SortPairs(ws.sort_tmp.p, tb, ka, ka + n_ref, va, va + n_ref, (int)n_ref, 0,
-                                             end_bit, s));
-    note_launch(2);
-    const uint32_t* order = va + n_ref;
+    FSB_CUDA(cub::DeviceRadixSort::SortPairs(ws.sort_tmp.p, tb, ka, ka + n_ref, va, va + n_ref, (int)n_ref, 0, 31,
+                                             s));
+    uint32_t* order = va;   // the unsorted values are dead
+    k_rank_ties<<<blocks(n_ref, 256), 256, 0, s>>>(ka + n_ref, va + n_ref, ws.refined.as<Refined>(), n_ref, order);
+    note_launch(3);
     ctx->stage_end(ST_SORT);
     ctx->stage_begin(ST_ORIENT);
     FSB_TRY(ws.oriented.ensure((size_t)n_ref * ORI_SLOTS * sizeof(Oriented)));

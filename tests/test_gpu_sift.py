@@ -225,3 +225,37 @@ def test_stage_timers_accumulate_without_changing_results(fsb, golden):
         ms, n = st[name]
         assert n == 3 and ms > 0.0, (name, st[name])
     assert all(v == (0.0, 0) for v in again.values()), again
+
+
+def _tiled(tile, ny, nx):
+    return np.ascontiguousarray(np.tile(tile, (ny, nx)))
+
+
+def test_equal_responses_rank_by_dog_index(fsb):
+    """A tiled image repeats every extremum at several places with bit-equal responses; the device
+    ranks such ties by DoG-atlas index like the reference (extrema in atlas order, stable sort by
+    response): in exact mode each run of equal responses lists its positions in the oracle's
+    order, and repeated runs give identical lists whatever order the extrema were found in."""
+    from fieldstitch_b200 import synth
+    from oracle import gsift_ref
+    img = _tiled(synth.synth_image(64, 64, 17), 4, 4)
+    ref, _ = gsift_ref.detect(img, max_kp=100000)
+    runs = [fsb.gsift.detect(img, max_kp=100000, exact=True)[0] for _ in range(3)]
+    for r in runs[1:]:
+        for key in ("x", "y", "response", "angle"):
+            np.testing.assert_array_equal(r[key], runs[0][key])
+    got = runs[0]
+
+    def groups(k):
+        out = {}
+        for x, y, v in zip(k["x"], k["y"], k["response"]):
+            seq = out.setdefault(float(v), [])
+            if not seq or seq[-1] != (float(x), float(y)):
+                seq.append((float(x), float(y)))
+        return {v: s for v, s in out.items() if len(s) > 1}
+
+    gg, gr = groups(got), groups(ref)
+    common = [v for v in gg if v in gr and set(gg[v]) == set(gr[v])]
+    assert len(common) >= 10, (len(gg), len(gr), len(common))
+    for v in common:
+        assert gg[v] == gr[v], v
