@@ -8,7 +8,7 @@ octave); it is trained on the GPU (libfsb200's own forward/backward/Adam kernels
 per epoch) on labels that the plain pipeline produces by its own verification: a candidate is an
 inlier when the RANSAC homography fitted to the plain pipeline's matches maps it within 2 px.
 The plain ratio test stays the fallback (``MatchFilter.matches`` without a trained network) and
-the judge of the filter's precision and recall (``score``).
+the yardstick of the filter's precision and recall (``score``).
 
 Device data are torch CUDA tensors (torch is used only for device memory here).
 """

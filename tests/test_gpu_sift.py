@@ -1,5 +1,5 @@
 """Parity of the CUDA SIFT path (through the C ABI) with the oracle, the reference fixtures and
-OpenCV. Tolerances are the north-star ones: position <= 0.01 px, angle <= 0.1 deg, descriptor
+OpenCV. Tolerances are the parity targets: position <= 0.01 px, angle <= 0.1 deg, descriptor
 bytes within +-1."""
 import numpy as np
 import pytest
