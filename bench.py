@@ -80,6 +80,27 @@ def config(args, extra=None):
     return c
 
 
+def rank_seed(seed, rank):
+    """Seed of a rank's pairs: the ranks are replicas, each extracting and matching its own pairs
+    (disjoint seeds for fewer than 100000 pairs per rank); no data-path collective."""
+    return seed + 100000 * rank
+
+
+def max_over_ranks(ms, dist, device):
+    """The slowest rank's time (a step of the whole job ends when every rank has finished)."""
+    if dist is None:
+        return ms
+    import torch
+    t = torch.tensor([float(ms)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def job_rate(world, pairs_per_rank, ms):
+    """Whole-job pairs/s: every rank's pairs over the slowest rank's time."""
+    return world * pairs_per_rank / (ms / 1000.0)
+
+
 def gen_pairs(n, seed):
     import multiprocessing as mp
     jobs = [(H_IMG, W_IMG, seed + i) for i in range(n)]
@@ -401,7 +422,7 @@ def run_fsb(args):
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
-    pairs = gen_pairs(args.pairs, args.seed + 100000 * rank)   # before any CUDA work
+    pairs = gen_pairs(args.pairs, rank_seed(args.seed, rank))   # before any CUDA work
     torch.cuda.set_device(local)
     dist = None
     if world > 1:
@@ -554,11 +575,9 @@ def run_fsb(args):
             stages[k_] = (a_ + ms_, b_ + n_)
         c_.timing(False)
     if dist is not None:
-        t = torch.tensor([ms_step], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms_step = float(t.item())
+        ms_step = max_over_ranks(ms_step, dist, dev)
         barrier()
-    value = world * args.pairs / (ms_step / 1000.0)
+    value = job_rate(world, args.pairs, ms_step)
 
     # ---- e2e through the public host API (host buffers, copies inside the timed region)
     e2e = None
@@ -607,11 +626,8 @@ def run_fsb(args):
         g1.record(main)
         torch.cuda.synchronize()
         ms_e2e = max(g0.elapsed_time(g1), (time.perf_counter() - f0) * 1000.0) / ksteps
-        if dist is not None:
-            t = torch.tensor([ms_e2e], device=dev)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            ms_e2e = float(t.item())
-        e2e = {"value": world * args.pairs / (ms_e2e / 1000.0), "unit": "pairs/s", "h2d_bytes_per_step": int(h2d),
+        ms_e2e = max_over_ranks(ms_e2e, dist, dev)
+        e2e = {"value": job_rate(world, args.pairs, ms_e2e), "unit": "pairs/s", "h2d_bytes_per_step": int(h2d),
                "d2h_bytes_per_step": int(d2h), "ms_per_step": ms_e2e, "steps": ksteps,
                "api": "features.sift_gpu_u8 + matching.guided_from_pred, %d host threads" % args.streams,
                "host_inputs": "images in pinned host memory; keypoints / descriptors between the two calls in "
