@@ -87,20 +87,34 @@ __global__ void __launch_bounds__(EX_T, 5) k_extrema(const float* __restrict__ D
     };
     // layer l of row y at this lane's column: rowp + l * RC, rowp advancing by C per row
     const float* rowp = base + (long long)(y0 - 1) * C + cc;
-    auto load_row = [&](Row& w) {
+    auto issue_row = [&](float (&raw)[5]) {
+#pragma unroll
+        for (int l = 0; l < 5; ++l) raw[l] = __ldg(rowp + l * RC);
+        rowp += C;
+    };
+    auto finish_row = [&](Row& w, const float (&raw)[5]) {
 #pragma unroll
         for (int l = 0; l < 5; ++l) {
-            const float v = __ldg(rowp + l * RC);
+            const float v = raw[l];
             const float vl = __shfl_up_sync(0xffffffffu, v, 1), vr = __shfl_down_sync(0xffffffffu, v, 1);
             w.hx[l] = fmaxf(fmaxf(vl, v), vr);
             w.hn[l] = fminf(fminf(vl, v), vr);
             if (l >= 1 && l <= N_LAYERS) w.c[l - 1] = v;
         }
-        rowp += C;
     };
-    // test row y from the window (up, mid, dn), append its extrema, then load row y + 2 into `up`
-    // (no longer needed): the three windows rotate by name, not by register moves
+    auto load_row = [&](Row& w) {
+        float raw[5];
+        issue_row(raw);
+        finish_row(w, raw);
+    };
+    // test row y from the window (up, mid, dn), append its extrema, then finish row y + 2 into `up`
+    // (no longer needed): the three windows rotate by name, not by register moves. Row y + 2's
+    // loads are issued before the test, so they are in flight while it runs (a few registers
+    // spill at 5 blocks per SM; the kernel is bound by load latency, and this took it from 0.220
+    // to 0.193 ms per 2640 x 1978 image)
     auto step = [&](Row& up, const Row& mid, const Row& dn, int y) {
+        float raw[5];
+        issue_row(raw);   // row y + 2 <= R - BORDER + 1 < R, in flight while row y is tested
         float vmx[5], vmn[5];
 #pragma unroll
         for (int l = 0; l < 5; ++l) {
@@ -138,7 +152,7 @@ __global__ void __launch_bounds__(EX_T, 5) k_extrema(const float* __restrict__ D
                 ++pos;
             }
         }
-        load_row(up);   // row y + 2 <= R - BORDER + 1 < R
+        finish_row(up, raw);
     };
     Row w0, w1, w2;
     load_row(w0);   // y0 - 1
