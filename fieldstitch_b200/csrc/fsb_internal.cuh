@@ -4,6 +4,7 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <atomic>
 #include <cstdarg>
 #include <cstdio>
 #include <string>
@@ -46,6 +47,19 @@ enum Stage { ST_UPLOAD = 0, ST_PYRAMID, ST_EXTREMA, ST_REFINE, ST_ORIENT, ST_SOR
             return FSB_ERR_ARG;                             \
         }                                                   \
     } while (0)
+
+// Raises a kernel's dynamic shared-memory limit to `bytes` on the current device once per device
+// (`done` holds the largest value set, per device; two threads meeting a device first may both set
+// it, which is harmless). carveout >= 0 also sets the preferred shared-memory carveout.
+inline int32_t smem_attr(const void* func, int bytes, std::atomic<int> (&done)[64], int carveout = -1) {
+    int dev = 0;
+    FSB_CUDA(cudaGetDevice(&dev));
+    if (dev >= 0 && dev < 64 && done[dev].load(std::memory_order_acquire) >= bytes) return FSB_OK;
+    FSB_CUDA(cudaFuncSetAttribute(func, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+    if (carveout >= 0) FSB_CUDA(cudaFuncSetAttribute(func, cudaFuncAttributePreferredSharedMemoryCarveout, carveout));
+    if (dev >= 0 && dev < 64) done[dev].store(bytes, std::memory_order_release);
+    return FSB_OK;
+}
 
 // ------------------------------------------------------------------------ SIFT constants
 // app/planesite/gsift.py:13-25, 224

@@ -276,14 +276,8 @@ __global__ void k_mlp_accept(int n, const int32_t* __restrict__ t1, const float*
 size_t fwd_bwd_smem() { return sizeof(float) * (size_t)(OFF_B3 + MB * NF + 4 * MB * HP + MB); }
 
 int32_t configure_fwd_bwd() {
-    static bool done[64] = {};
-    int dev = 0;
-    FSB_CUDA(cudaGetDevice(&dev));
-    if (dev < 64 && !done[dev]) {
-        FSB_CUDA(cudaFuncSetAttribute(k_mlp_fwd_bwd, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fwd_bwd_smem()));
-        done[dev] = true;
-    }
-    return FSB_OK;
+    static std::atomic<int> done[64];
+    return smem_attr((const void*)k_mlp_fwd_bwd, (int)fwd_bwd_smem(), done);
 }
 
 }  // namespace

@@ -622,14 +622,8 @@ __global__ void __launch_bounds__(LNT) k_layer(LayerArgs a) {
 
 template <int TS, int r, bool BASE, int LY>
 int32_t launch_layer_ly(const LayerArgs& a, cudaStream_t s) {
-    static bool attr[64] = {};
-    int dev = 0;
-    FSB_CUDA(cudaGetDevice(&dev));
-    if (dev < 64 && !attr[dev]) {
-        FSB_CUDA(cudaFuncSetAttribute(k_layer<TS, r, BASE, LY>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                      layer_smem<r, LY>()));
-        attr[dev] = true;
-    }
+    static std::atomic<int> attr[64];
+    FSB_TRY(smem_attr((const void*)k_layer<TS, r, BASE, LY>, layer_smem<r, LY>(), attr));
     dim3 grid((a.C + LX - 1) / LX, (a.R + LY - 1) / LY);
     k_layer<TS, r, BASE, LY><<<grid, LNT, layer_smem<r, LY>(), s>>>(a);
     note_launch();
@@ -938,13 +932,8 @@ int sm_count() {
 
 template <int G>
 int32_t launch_group_t(GroupArgs a, cudaStream_t s) {
-    static bool attr[64] = {};
-    int dev = 0;
-    FSB_CUDA(cudaGetDevice(&dev));
-    if (dev < 64 && !attr[dev]) {
-        FSB_CUDA(cudaFuncSetAttribute(k_group<G>, cudaFuncAttributeMaxDynamicSharedMemorySize, group_smem<G>()));
-        attr[dev] = true;
-    }
+    static std::atomic<int> attr[64];
+    FSB_TRY(smem_attr((const void*)k_group<G>, group_smem<G>(), attr));
     a.tiles_x = (a.C + GX - 1) / GX;
     a.n_tiles = a.tiles_x * ((a.R + GY - 1) / GY);
     const int grid = a.n_tiles < sm_count() ? a.n_tiles : sm_count();
@@ -958,12 +947,8 @@ int32_t launch_group_t(GroupArgs a, cudaStream_t s) {
 
 int32_t launch_octave_fused(const float* L0, int R, int C, float* dog, float* mag, float* ang, float* down,
                             int down_cols, cudaStream_t s) {
-    static bool attr = false;
-    if (!attr) {
-        FSB_CUDA(cudaFuncSetAttribute(k_octave, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES));
-        FSB_CUDA(cudaFuncSetAttribute(k_octave, cudaFuncAttributePreferredSharedMemoryCarveout, 100));
-        attr = true;
-    }
+    static std::atomic<int> attr[64];
+    FSB_TRY(smem_attr((const void*)k_octave, SMEM_BYTES, attr, 100));
     Args a;
     a.L0 = L0;
     a.R = R;

@@ -132,13 +132,8 @@ int32_t run_clahe(const uint8_t* d_img, int h, int w, int stride, double clip, i
     const dim3 grid((w + 63) / 64, (h + 15) / 16);
     const int smem = tiles_x * tiles_y * 256;
     if (smem > 48 * 1024) {
-        static bool attr[64] = {};
-        int dev = 0;
-        FSB_CUDA(cudaGetDevice(&dev));
-        if (dev >= 64 || !attr[dev]) {
-            FSB_CUDA(cudaFuncSetAttribute(k_clahe_apply, cudaFuncAttributeMaxDynamicSharedMemorySize, 64 * 1024));
-            if (dev < 64) attr[dev] = true;
-        }
+        static std::atomic<int> attr[64];
+        FSB_TRY(smem_attr((const void*)k_clahe_apply, 64 * 1024, attr));
     }
     k_clahe_apply<<<grid, 256, smem, s>>>(d_img, h, w, stride, d_lut, tiles_x, tiles_y, inv_tw, inv_th, d_out,
                                           out_stride);

@@ -798,13 +798,8 @@ __global__ void k_tcu_emit(const TcPair* __restrict__ pairs, const unsigned long
 template <int PREC>
 int32_t tc_launch_dense(const TcPair* d_pairs, int n_pairs, int n_items, Cand* part, int* err, int grid,
                         cudaStream_t s) {
-    static bool configured[64] = {};
-    int dev = 0;
-    FSB_CUDA(cudaGetDevice(&dev));
-    if (dev < 64 && !configured[dev]) {
-        FSB_CUDA(cudaFuncSetAttribute(k_tc_dense<PREC>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_bytes<PREC>()));
-        configured[dev] = true;
-    }
+    static std::atomic<int> configured[64];
+    FSB_TRY(smem_attr((const void*)k_tc_dense<PREC>, (int)smem_bytes<PREC>(), configured));
     k_tc_dense<PREC><<<grid, TC_THREADS, smem_bytes<PREC>(), s>>>(d_pairs, n_pairs, n_items, part, err);
     FSB_CUDA(cudaGetLastError());
     return FSB_OK;
