@@ -78,3 +78,17 @@ def test_sift_gpu_selection_is_spread_of_detect(golden):
             sel = sel[np.argsort(-kps["response"][sel], kind="stable")]
             np.testing.assert_array_equal(xy, np.c_[kps["x"][sel], kps["y"][sel]].astype(np.float32))
             np.testing.assert_array_equal(resp, kps["response"][sel])
+
+
+def test_spread_matches_reference_fixtures():
+    """The device selection against the reference's own _spread outputs (tests/golden/spread.npz),
+    in _spread's order and after the stable response sort."""
+    import os
+    from fieldstitch_b200 import features
+    with np.load(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "spread.npz")) as z:
+        for k in range(int(z["n_cases"])):
+            x, y, r = z["c%d/x" % k], z["c%d/y" % k], z["c%d/resp" % k]
+            W, H, n = (int(v) for v in z["c%d/wh_n" % k])
+            np.testing.assert_array_equal(features.spread_arrays(x, y, r, W, H, n), z["c%d/sel" % k])
+            np.testing.assert_array_equal(features.spread_arrays(x, y, r, W, H, n, response_order=True),
+                                          z["c%d/sorted" % k])
