@@ -1147,6 +1147,7 @@ int32_t fsb_spread(fsb_ctx* ctx, const float* x, const float* y, const float* re
                    int32_t nfeat, int32_t order, int32_t* sel, int32_t* n_out) {
     FSB_ARG(ctx && n_out, "null pointer");
     FSB_ARG(n >= 0 && nfeat >= 0, "negative size");
+    FSB_ARG(n <= (1 << 30), "at most 2^30 keypoints");
     FSB_ARG(W > 0 && H > 0, "image size must be positive");
     FSB_ARG(order == FSB_SPREAD_SELECTION || order == FSB_SPREAD_RESPONSE, "order must be 0 or 1");
     FSB_ARG(n == 0 || (x && y && resp && sel), "null keypoint or output array");

@@ -674,7 +674,7 @@ int32_t spread_dev(fsb_ctx* ctx, const float* d_x, const float* d_y, const float
         return FSB_OK;
     }
     // at most 64 chunks of a multiple of 1024 elements
-    const int ch = 1024 * (int)((n + 65535) / 65536);
+    const int ch = (int)(1024 * (((long long)n + 65535) / 65536));
     const int nch = (n + ch - 1) / ch;
     const int ngrp = (n + 31) / 32;
     FSB_TRY(ctx->s_misc.ensure(((size_t)nch * (SP_CELLS + 1) + (size_t)ngrp + (size_t)n) * 4 + 512));
