@@ -78,3 +78,24 @@ def test_host_validation():
     assert _lib.as_u8_desc(np.full((2, 128), 7.0, np.float32)).dtype == np.uint8
     q, t = matching._ratio_match_bf(np.zeros((1, 128), np.float32), np.zeros((5, 128), np.float32), 0.8)
     assert len(q) == len(t) == 0
+
+
+def test_spread_arguments_checked_before_the_device():
+    """fsb_spread rejects unsorted responses, a bad order code and negative sizes with a status
+    before touching the context (a bogus non-null context pointer is never dereferenced)."""
+    lib = _lib.load()
+    x = np.arange(5, dtype=np.float32)
+    r_up = np.arange(5, dtype=np.float32)          # ascending: not detect's order
+    r_dn = r_up[::-1].copy()
+    sel = np.zeros(5, np.int32)
+    n = ctypes.c_int32(-1)
+    bogus = ctypes.c_void_p(1)
+    P = _lib.ptr
+    assert lib.fsb_spread(bogus, P(x), P(x), P(r_up), 5, 100, 100, 3, 0, P(sel), ctypes.byref(n)) == 1
+    assert b"response-descending" in lib.fsb_last_error()
+    assert lib.fsb_spread(bogus, P(x), P(x), P(r_dn), 5, 100, 100, 3, 7, P(sel), ctypes.byref(n)) == 1
+    assert lib.fsb_spread(bogus, P(x), P(x), P(r_dn), -1, 100, 100, 3, 0, P(sel), ctypes.byref(n)) == 1
+    assert lib.fsb_spread(bogus, P(x), P(x), P(r_dn), 5, 0, 100, 3, 0, P(sel), ctypes.byref(n)) == 1
+    from fieldstitch_b200 import features
+    with pytest.raises(ValueError):
+        features._spread([], 100, 100, 10, gx=8)
