@@ -121,6 +121,29 @@ def guided_from_pred_batch_d(problems, radius, kc, ratio, device=0, out=None):
     return [(o[0][:cnt[i]], o[1][:cnt[i]]) for i, o in enumerate(out)]
 
 
+def match_guided_batch(problems, radius, kc=None, ratio=0.85, device=0):
+    """Batched guided matching on host arrays: ``problems[p]`` = (pred (na,2), a_desc (na,128),
+    b_xy (nb,2), b_desc (nb,128), (w_b, h_b)) as ``guided_from_pred`` takes them (descriptors uint8
+    or their float32 values). The data go to the device once and every pair runs in one
+    ``guided_from_pred_batch_d`` call; returns [(q, t)] int64 numpy arrays per pair, each equal to
+    ``guided_from_pred`` on that pair."""
+    import torch
+    dev = torch.device("cuda", device)
+    staged = []
+    for pred, a_desc, b_xy, b_desc, wh in problems:
+        a = _lib.as_u8_desc(a_desc, "A desc")
+        b = _lib.as_u8_desc(b_desc, "B desc")
+        pr = np.ascontiguousarray(np.asarray(pred, np.float64).reshape(-1, 2))
+        bx = np.ascontiguousarray(np.asarray(b_xy, np.float64).reshape(-1, 2))
+        staged.append((torch.from_numpy(pr).to(dev), torch.from_numpy(np.ascontiguousarray(a)).to(dev),
+                       torch.from_numpy(bx).to(dev), torch.from_numpy(np.ascontiguousarray(b)).to(dev),
+                       (float(wh[0]), float(wh[1]))))
+    if kc is not None and int(kc) < 1:
+        raise ValueError("kc must be >= 1 or None")
+    res = guided_from_pred_batch_d(staged, radius, kc, ratio, device=device)
+    return [(q.cpu().numpy().astype(np.int64), t.cpu().numpy().astype(np.int64)) for q, t in res]
+
+
 def tc_stats(device=0):
     """Statistics of the last tensor-core dense match on this thread's context for ``device``:
     rows, rows recomputed exactly (certificate not settled), largest / mean absolute error of the

@@ -60,3 +60,22 @@ def test_batch_equals_per_pair(kc):
     _check(m, probs, m.guided_from_pred_batch_d(dev, 40.0, kc, 0.85, out=out), kc)
     # a different table (one pair fewer): a new capture
     _check(m, probs[1:], m.guided_from_pred_batch_d(dev[1:], 40.0, kc, 0.85, out=out[1:]), kc)
+
+
+@pytest.mark.parametrize("kc", [16, None])
+def test_host_batch_entry_equals_per_pair(kc):
+    """matching.match_guided_batch (host arrays in and out) returns each pair's guided_from_pred
+    result, with float32 RootSIFT-valued descriptors accepted like the per-pair call."""
+    import fieldstitch_b200 as F
+    m = F.matching
+    sizes = [(900, 700), (0, 30), (50, 0), (3000, 2500)]
+    probs = [_problem(na, nb, 40 + i) for i, (na, nb) in enumerate(sizes)]
+    got = m.match_guided_batch([(p, a.astype(np.float32), bxy, b, (W, H)) for p, a, bxy, b in probs], 40.0, kc,
+                               0.85)
+    for (pred, a, bxy, b), (q, t) in zip(probs, got):
+        if len(a) == 0 or len(b) == 0:
+            assert len(q) == 0
+            continue
+        q2, t2 = m.guided_from_pred(pred, a, bxy, b, (W, H), 40.0, kc, 0.85)
+        np.testing.assert_array_equal(q, q2)
+        np.testing.assert_array_equal(t, t2)
