@@ -209,25 +209,65 @@ def cpu_pair(pair, pidx, seed, cores):
     return len(q), time.perf_counter() - t0
 
 
+def _pool_task(job):
+    """One pair on one process of the CPU pool (one thread per process, as one worker of the
+    reference's process pool)."""
+    pair, pidx, seed = job
+    return cpu_pair(pair, pidx, seed, 1)
+
+
+def _pool_warm(_):
+    import cv2  # noqa: F401
+    import scipy.spatial  # noqa: F401
+
+    from oracle import features_ref, matching_ref  # noqa: F401
+    return os.getpid()
+
+
+class CpuPool:
+    """The reference's CPU path run the way its pipeline runs pair work: a process pool of one
+    worker per host core, one pair per task (app/planesite/pipeline.py:535-536,
+    pool.imap(match_pair, pairs)); here each task extracts both images and matches them."""
+
+    def __init__(self, workers):
+        import multiprocessing as mp
+        self.workers = workers
+        self.pool = mp.get_context("spawn").Pool(workers)
+        self.pool.map(_pool_warm, range(4 * workers), chunksize=1)   # imports done before timing
+
+    def step(self, pairs, seed):
+        """Wall-clock seconds for every pair of `pairs` through the pool."""
+        t0 = time.perf_counter()
+        self.pool.map(_pool_task, [(p, i, seed) for i, p in enumerate(pairs)], chunksize=1)
+        return time.perf_counter() - t0
+
+    def close(self):
+        self.pool.close()
+        self.pool.join()
+
+
 def run_reference(args):
+    """The reference's CPU implementation of the path (oracle port) with every host core: one step
+    = one pool pass over `cores` pairs of the workload (the same pairs every step)."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return 0
     cores = os.cpu_count() or 1
-    pairs = gen_pairs(args.warmup + args.steps, args.seed)
-    for i in range(args.warmup):
-        cpu_pair(pairs[i], i, args.seed, cores)
-    times = []
-    for i in range(args.warmup, args.warmup + args.steps):
-        times.append(cpu_pair(pairs[i], i, args.seed, cores)[1])
-    per_pair = sum(times) / len(times)
-    v = 1.0 / per_pair
+    pairs = gen_pairs(cores, args.seed)
+    pool = CpuPool(cores)
+    for _ in range(args.warmup):
+        pool.step(pairs, args.seed)
+    times = [pool.step(pairs, args.seed) for _ in range(args.steps)]
+    pool.close()
+    per_step = sum(times) / len(times)
+    v = len(pairs) / per_step
     line = {"metric": METRIC, "value": v, "unit": "pairs/s", "n_gpus": args.gpus, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": per_pair * 1000.0, "higher_is_better": True, "scaling": "weak",
+            "warmup": args.warmup, "ms_per_step": per_step * 1000.0, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded)",
-            "config": config(args, {"pairs_per_step_per_gpu": 1}), "impl": "reference",
+            "config": config(args, {"pairs_per_step_per_gpu": len(pairs)}), "impl": "reference",
             "cpu_baseline": {"value": v, "unit": "pairs/s", "cores": cores, "kind": "port",
-                             "sample": "1 pair per step (2 images 2640x1978 + guided match), %d steps" % args.steps},
+                             "sample": "%d pairs per step (2 images 2640x1978 + guided match each) over a pool of "
+                                       "%d processes, one thread each, %d steps" % (len(pairs), cores, args.steps)},
             "e2e": {"value": v, "unit": "pairs/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line, default=_json_num), flush=True)
     return 0
@@ -423,6 +463,7 @@ def run_fsb(args):
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
     pairs = gen_pairs(args.pairs, rank_seed(args.seed, rank))   # before any CUDA work
+    cpu_pool = CpuPool(os.cpu_count() or 1) if rank == 0 and world == 1 and not args.no_cpu else None
     torch.cuda.set_device(local)
     dist = None
     if world > 1:
@@ -579,6 +620,34 @@ def run_fsb(args):
         barrier()
     value = job_rate(world, args.pairs, ms_step)
 
+    # ---- parity of the timed steps' output (outside the timed region): the last step's batched
+    # guided matches of two pairs against the oracle's guided matcher (NumPy / cKDTree, the
+    # reference's _guided restated) run on the GPU's own keypoints, descriptors and predictions
+    parity = {"pairs": [], "parity_checked": False}
+    try:
+        from oracle import matching_ref
+        torch.cuda.synchronize()
+        ok = True
+        for i in range(min(2, len(pairs))):
+            B = pb[i]
+            na_, nb_ = B["n"]
+            pred = B["pred"][:na_].cpu().numpy()
+            ua = B["u8"][0][:na_].cpu().numpy()
+            bxy = B["bxy"][:nb_].cpu().numpy()
+            ub = B["u8"][1][:nb_].cpu().numpy()
+            q_ref, t_ref = matching_ref.guided_from_pred(pred, ua, bxy, ub, (w, h), RADIUS, KC, RATIO)
+            n_ = m_cnt[i]
+            q_g, t_g = B["q"][:n_].cpu().numpy(), B["t"][:n_].cpu().numpy()
+            same = bool(np.array_equal(q_g, q_ref) and np.array_equal(t_g, t_ref))
+            ok = ok and same
+            parity["pairs"].append({"pair": i, "keypoints": [int(na_), int(nb_)], "matches_gpu": int(n_),
+                                    "matches_oracle": int(len(q_ref)), "identical": same})
+        parity["parity_checked"] = ok
+        parity["what"] = ("the batched guided matches of pairs 0 and 1 of the last timed step equal the oracle's "
+                          "guided matcher on the same keypoints, descriptors and predictions")
+    except Exception as e:  # reported in the line, never hidden
+        parity["error"] = ("%s: %s" % (type(e).__name__, e))[:200]
+
     # ---- e2e through the public host API (host buffers, copies inside the timed region)
     e2e = None
     if not args.no_e2e:
@@ -662,9 +731,16 @@ def run_fsb(args):
         cores = os.cpu_count() or 1
         n_cpu = 2
         ts = [cpu_pair(pairs[i], i, args.seed, cores)[1] for i in range(n_cpu)]
-        cpu = {"value": n_cpu / sum(ts), "unit": "pairs/s", "cores": cores, "kind": "port",
-               "sample": "%d pairs of the same workload (OpenCV SIFT as features.sift_cpu + NumPy/cKDTree "
-                         "guided match)" % n_cpu}
+        pool_pairs = pairs[:min(len(pairs), cores)]
+        pool_s = cpu_pool.step(pool_pairs, args.seed) if cpu_pool is not None else None
+        cpu = {"value": len(pool_pairs) / pool_s if pool_s else n_cpu / sum(ts), "unit": "pairs/s", "cores": cores,
+               "kind": "port",
+               "sample": "%d pairs of the same workload (OpenCV SIFT as features.sift_cpu + NumPy/cKDTree guided "
+                         "match) over a pool of %d processes, one thread each, one pair per task (as the "
+                         "reference's pipeline pool runs pairs)" % (len(pool_pairs), cores),
+               "serial": {"value": n_cpu / sum(ts), "unit": "pairs/s", "threads": cores,
+                          "sample": "%d pairs one after another in one process, OpenCV on %d threads" % (n_cpu, cores)}}
+        cpu_pool.close()
 
     # ---- the plain sequential path: one context (one stream), one pair at a time
     plain = None
@@ -701,6 +777,7 @@ def run_fsb(args):
                                         "matching": "every pair of a step in one fsb_match_guided_batch_d call "
                                                     "(one CUDA graph, captured once, replayed each step)"}),
                 "clocks": clk, "e2e": e2e, "gpu_launches": int(launches), "roofline": roof, "cpu_baseline": cpu,
+                "parity_checked": parity["parity_checked"], "parity": parity,
                 "matches_per_step": matches / args.steps, "plain_single_stream": plain,
                 "dense_precision_sweep": sweep, "learned_filter": filt,
                 "stages_ms_per_step_summed_over_streams": {k: v[0] / args.steps for k, v in stages.items()},

@@ -886,8 +886,9 @@ int32_t run_match_guided_batch(fsb_ctx* ctx, int n_pairs, const double* const* d
 //
 // The array lives in every GPU that loads this library until the process exits. Host code may
 // not use its name as an address (on the host it is only a stand-in symbol), so its device
-// address is looked up once per device with cudaGetSymbolAddress, with that device current, by
-// the first call made on the device; that first call should come before any stream capture.
+// address is looked up with cudaGetSymbolAddress, with that device current, by the first call made
+// on the device (and again by the first call in another context of that device, e.g. after a
+// cudaDeviceReset); that first call should come before any stream capture.
 // Every call shares the array and it keeps the last call's contents: the per-target key table is
 // re-filled at the start of each call, everything else is fully overwritten. Calls whose work
 // overlaps on the GPU (different streams, or host threads using the same device) race on the
@@ -906,8 +907,29 @@ static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratch
 
 std::mutex g_noalloc_mu;
 void* g_noalloc_addr[256] = {};
+void* g_noalloc_ctx[256] = {};   // the CUDA context the cached address belongs to
 
-// device address of g_noalloc_scratch on the current device (looked up on first use)
+// The current CUDA context (driver-level handle), through the runtime's driver entry point so the
+// library needs no link against libcuda; null if it cannot be queried.
+void* current_context() {
+    typedef int (*CtxGetCurrent)(void**);
+    static CtxGetCurrent fn = [] {
+        void* f = nullptr;
+        cudaDriverEntryPointQueryResult q{};
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f, cudaEnableDefault, &q) != cudaSuccess ||
+            q != cudaDriverEntryPointSuccess)
+            f = nullptr;
+        return reinterpret_cast<CtxGetCurrent>(f);
+    }();
+    void* c = nullptr;
+    if (fn == nullptr || fn(&c) != 0) return nullptr;
+    return c;
+}
+
+// Device address of g_noalloc_scratch in the current device's current context. It is looked up
+// on the first call in a context and cached with that context's handle; a different context on
+// the same device (the module loaded again after cudaDeviceReset, or a driver-API context other
+// than the primary one) looks it up again.
 int32_t noalloc_scratch(void** out) {
     int dev = 0;
     FSB_CUDA(cudaGetDevice(&dev));
@@ -915,8 +937,9 @@ int32_t noalloc_scratch(void** out) {
         set_error("device ordinal %d out of range", dev);
         return FSB_ERR_ARG;
     }
+    void* ctx = current_context();
     std::lock_guard<std::mutex> lk(g_noalloc_mu);
-    if (!g_noalloc_addr[dev]) {
+    if (!g_noalloc_addr[dev] || ctx == nullptr || ctx != g_noalloc_ctx[dev]) {
         void* p = nullptr;
         const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
         if (e != cudaSuccess || p == nullptr) {
@@ -924,6 +947,7 @@ int32_t noalloc_scratch(void** out) {
             return FSB_ERR_CUDA;
         }
         g_noalloc_addr[dev] = p;
+        g_noalloc_ctx[dev] = ctx;
     }
     *out = g_noalloc_addr[dev];
     return FSB_OK;

@@ -6,7 +6,11 @@ Same signatures and outputs: ``detect`` returns (dict of host arrays x, y, size,
 descriptors with L2 norm 512 (unrounded, OpenCV scaling). The state owns the device-resident
 gradient atlas and is released when it is garbage-collected (or by ``state.close()``).
 
-There is no CPU path: ``gpu=False`` raises. ``exact=True`` selects float64 blur accumulation
+There is no CPU path: ``gpu=False`` raises. This is the one deliberate signature difference: the
+reference's ``detect(gray, gpu=False, ...)`` defaults to its NumPy path, this module's ``gpu``
+defaults to True, so a caller relying on the default gets the GPU (the reference's own GPU worker,
+features.sift_gpu, passes gpu=True explicitly, features.py:119; only its start-up self-test calls
+the CPU default, as the comparison side). ``exact=True`` selects float64 blur accumulation
 (bit-identical pyramid to the reference's NumPy/SciPy path) and float64 descriptor sample math.
 """
 import ctypes

@@ -255,7 +255,9 @@ int32_t fsb_mlp_filter_d(fsb_ctx* ctx, int32_t na, const int32_t* d_t1, const fl
    int32, the number of pairs, ordered by target) are device pointers; the work is queued on
    `stream` (a cudaStream_t; null = the legacy default stream) and the call does not wait for it.
    The first call on a device looks up the array's device address (cudaGetSymbolAddress) with
-   that device current; make that first call before any stream capture. Calls share the array:
+   that device current, and so does the first call in any other CUDA context of that device (after
+   a cudaDeviceReset, or in a driver-API context other than the primary one); make that first call
+   before any stream capture. Calls share the array:
    calls whose work can overlap on the GPU race and must be serialised by the caller. */
 int32_t fsb_match_bf_noalloc(const uint8_t* d_a, int32_t na, const uint8_t* d_b, int32_t nb, float ratio,
                              int64_t* d_q, int64_t* d_t, int32_t* d_n, void* stream);

@@ -2,7 +2,7 @@
 
 Run in the build container, where the reference source tree is available:
 
-    python tests/golden/make_golden.py /root/reference/app
+    python tests/golden/make_golden.py <path to the reference's app directory>
 
 It imports PlaneSite's own modules (planesite.gsift / features / matching) and runs their CPU
 code paths on small seeded inputs, plus OpenCV SIFT (the reference's CPU extractor), and writes
@@ -124,4 +124,6 @@ def main(ref_app):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference/app")
+    if len(sys.argv) != 2:
+        sys.exit("usage: make_golden.py <path to the reference's app directory>")
+    main(sys.argv[1])

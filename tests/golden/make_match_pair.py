@@ -2,7 +2,7 @@
 
 Run in the build container, where the reference source tree is available:
 
-    python tests/golden/make_match_pair.py /root/reference/app
+    python tests/golden/make_match_pair.py <path to the reference's app directory>
 
 It imports PlaneSite's camera.undistort_pixels, matching._predict and matching.match_pair and runs
 them on a seeded synthetic two-view scene: a nadir camera pair over flat ground (the second view
@@ -113,4 +113,6 @@ def main(app_dir):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference/app")
+    if len(sys.argv) != 2:
+        sys.exit("usage: make_match_pair.py <path to the reference's app directory>")
+    main(sys.argv[1])

@@ -1,7 +1,7 @@
 """Golden grid-spread fixtures: the reference's features._spread (and the stable response sort that
 follows it in features.py:126) on seeded keypoint lists in detect's order (responses descending).
 
-    python tests/golden/make_spread.py /root/reference/app
+    python tests/golden/make_spread.py <path to the reference's app directory>
 
 Cases: uniform, clustered (few cells) and border-crossing positions; distinct responses and
 heavily tied ones (a handful of values), n below, near and far above the cap. Writes spread.npz
@@ -53,4 +53,6 @@ def main(app_dir):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference/app")
+    if len(sys.argv) != 2:
+        sys.exit("usage: make_spread.py <path to the reference's app directory>")
+    main(sys.argv[1])

@@ -1,6 +1,6 @@
 """Golden track fixtures: the reference's recon.build_tracks on seeded synthetic match graphs.
 
-    python tests/golden/make_tracks.py /root/reference/app
+    python tests/golden/make_tracks.py <path to the reference's app directory>
 
 Graphs: photos with random feature counts (some zero), pairs of random verified matches plus
 chains of true tracks across several photos, some joined so that a component holds two features
@@ -65,4 +65,6 @@ def main(app_dir):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference/app")
+    if len(sys.argv) != 2:
+        sys.exit("usage: make_tracks.py <path to the reference's app directory>")
+    main(sys.argv[1])

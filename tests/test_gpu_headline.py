@@ -1,0 +1,133 @@
+"""Parity at the benchmark's own configuration: 2640 x 1978 images (octave 0 is 5280 x 3956, nine
+octaves), contrast 0.015, edge 12, the worker's keypoint caps at both ends of the benchmark's range
+(nfeat 16000 and 2000, detect's max_kp = 2.2 nfeat), the float32 path the benchmark times (and
+the float64-blur mode for a bit-level check).
+
+The fixture (tests/golden/make_headline.py) holds the reference's own CPU outputs on two of the
+benchmark's seeded images (gsift.detect, features.sift_gpu + features._save) and OpenCV SIFT's
+keypoints with the same parameters. Tolerances are the parity targets: position <= 0.01 px,
+angle <= 0.1 deg, RootSIFT bytes within +-1. The measured fractions are printed (pytest -s).
+"""
+import hashlib
+import os
+
+import numpy as np
+import pytest
+
+from sift_compare import paired_fraction
+
+pytestmark = pytest.mark.gpu
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+CASES = ["h1000_n16000", "h1001_n2000"]
+H, W = 1978, 2640
+
+
+@pytest.fixture(scope="module")
+def fsb():
+    import fieldstitch_b200 as f
+    f.context(0)
+    return f
+
+
+@pytest.fixture(scope="module")
+def head():
+    with np.load(os.path.join(HERE, "golden", "headline.npz")) as z:
+        return {k: z[k] for k in z.files}
+
+
+_IMAGES = {}
+
+
+def _case(head, case):
+    from fieldstitch_b200 import synth
+    seed, nfeat, max_kp, contrast, edge = head[case + "/params"]
+    if case not in _IMAGES:
+        img = synth.synth_image(H, W, int(seed))
+        dig = np.frombuffer(hashlib.sha256(img.tobytes()).digest()[:8], np.uint64)[0]
+        assert dig == head[case + "/digest"], "regenerated image differs from the fixture's"
+        _IMAGES[case] = img
+    ref = {k: head[case + "/kp_" + k] for k in ("x", "y", "size", "angle", "response", "octave", "layer")}
+    return _IMAGES[case], ref, int(nfeat), int(max_kp), float(contrast), float(edge)
+
+
+@pytest.mark.parametrize("case", CASES)
+def test_headline_detect_fast_matches_reference(fsb, head, case):
+    """float32 path: >= 97 % of the reference's keypoints within 0.01 px / 0.1 deg, both ways, and
+    the same number of keypoints (the cap)."""
+    img, ref, _, max_kp, contrast, edge = _case(head, case)
+    got, _ = fsb.gsift.detect(img, max_kp=max_kp, contrast=contrast, edge=edge)
+    assert len(got["x"]) == len(ref["x"]), (len(got["x"]), len(ref["x"]))
+    frac, p = paired_fraction(ref, got)
+    back, _ = paired_fraction(got, ref)
+    m = p >= 0
+    dsz = np.abs(got["size"][p[m]] / ref["size"][m] - 1).max()
+    drs = np.abs(got["response"][p[m]] / ref["response"][m] - 1).max()
+    print("\n[headline %s] float32 path vs reference: %d keypoints, paired %.4f (reference->gpu), %.4f "
+          "(gpu->reference); max relative size / response difference on pairs %.2e / %.2e"
+          % (case, len(ref["x"]), frac, back, dsz, drs))
+    assert frac >= 0.97 and back >= 0.97, (frac, back)
+    assert dsz < 1e-4 and drs < 1e-3
+
+
+@pytest.mark.parametrize("case", CASES)
+def test_headline_detect_exact_matches_reference(fsb, head, case):
+    """float64-blur mode: >= 99 % of keypoints with bit-identical x, y and response."""
+    img, ref, _, max_kp, contrast, edge = _case(head, case)
+    got, _ = fsb.gsift.detect(img, max_kp=max_kp, contrast=contrast, edge=edge, exact=True)
+    frac, p = paired_fraction(ref, got, pos_tol=0.0, ang_tol=0.1)
+    m = p >= 0
+    same_resp = (got["response"][p[m]] == ref["response"][m]).mean()
+    print("\n[headline %s] float64-blur mode vs reference: bit-identical positions %.4f, identical responses "
+          "on those %.4f" % (case, frac, same_resp))
+    assert frac >= 0.99, frac
+    assert same_resp >= 0.99, same_resp
+
+
+@pytest.mark.parametrize("case", CASES)
+def test_headline_detect_agrees_with_opencv_as_the_reference_does(fsb, head, case):
+    """OpenCV SIFT with the same parameters: the share of OpenCV's keypoints that the float32 path
+    reproduces (0.01 px, 0.1 deg) is at least the share the reference's own CPU path reproduces,
+    less 1 %; the share is computed here from the fixture."""
+    img, ref, _, max_kp, contrast, edge = _case(head, case)
+    cv = {"x": head[case + "/cv_xy"][:, 0], "y": head[case + "/cv_xy"][:, 1], "angle": head[case + "/cv_angle"]}
+    got, _ = fsb.gsift.detect(img, max_kp=max_kp, contrast=contrast, edge=edge)
+    f_ref, _ = paired_fraction(cv, ref)
+    f_got, _ = paired_fraction(cv, got)
+    print("\n[headline %s] OpenCV keypoints reproduced: reference CPU path %.4f, float32 GPU path %.4f"
+          % (case, f_ref, f_got))
+    assert f_got >= f_ref - 0.01, (f_got, f_ref)
+
+
+@pytest.mark.parametrize("case", CASES)
+def test_headline_sift_gpu_matches_reference_worker(fsb, head, case):
+    """features.sift_gpu sequence (detect, grid spread, describe, RootSIFT): the selected keypoints
+    agree with the reference worker's within 0.01 px for >= 97 % both ways, and the RootSIFT bytes
+    of paired rows (the fixture keeps the strongest 4000) are within +-1 for >= 99.9 % of bytes."""
+    img, _, nfeat, _, _, _ = _case(head, case)
+    want_xy, want_u8 = head[case + "/sg_xy"], head[case + "/sg_u8"]
+    xy, u8, resp = fsb.features.sift_gpu_u8(img, nfeat)
+    assert len(xy) == len(want_xy)
+    from scipy.spatial import cKDTree
+    tree = cKDTree(xy.astype(np.float64))
+    cand = tree.query_ball_point(want_xy.astype(np.float64), r=0.01)
+    hit = np.array([len(c) > 0 for c in cand])
+    back = np.array([len(c) > 0 for c in cKDTree(want_xy.astype(np.float64)).query_ball_point(
+        xy.astype(np.float64), r=0.01)])
+    ok = tot = 0
+    worst = 0
+    for i in range(len(want_u8)):
+        if not cand[i]:
+            continue
+        # keypoints at one position with several orientations: the closest descriptor is the pair
+        d = np.abs(u8[cand[i]].astype(np.int32) - want_u8[i].astype(np.int32))
+        j = int(np.argmin(d.sum(1)))
+        ok += int((d[j] <= 1).sum())
+        tot += d.shape[1]
+        worst = max(worst, int(d[j].max()))
+    byte_frac = ok / max(tot, 1)
+    print("\n[headline %s] worker output vs reference: %d keypoints, selected positions paired %.4f / %.4f, "
+          "RootSIFT bytes within +-1 %.5f (worst %d) over %d rows"
+          % (case, len(xy), hit.mean(), back.mean(), byte_frac, worst, tot // 128))
+    assert hit.mean() >= 0.97 and back.mean() >= 0.97, (hit.mean(), back.mean())
+    assert byte_frac >= 0.999, byte_frac

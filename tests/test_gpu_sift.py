@@ -54,14 +54,17 @@ def test_detect_fast_matches_reference(fsb, golden, case):
 
 @pytest.mark.parametrize("case", CASES[:2])
 def test_detect_agrees_with_opencv(fsb, golden, case):
-    """OpenCV SIFT (the reference CPU extractor) on the same image: >= 90 % of OpenCV's keypoints
-    have a GPU keypoint within 0.01 px and 0.1 deg (the reference's own CPU path reaches ~98 %)."""
-    img, _, contrast, edge, max_kp, _ = _ref(golden, case)
+    """OpenCV SIFT (the reference CPU extractor) on the same image: the share of OpenCV's keypoints
+    with a GPU keypoint within 0.01 px and 0.1 deg is at least the share the reference's own CPU
+    path reaches on the same image (computed here from the fixture), less 1 %."""
+    img, ref, contrast, edge, max_kp, _ = _ref(golden, case)
     c = golden["sift_cv2"]
     cv = {"x": c[case + "/xy"][:, 0], "y": c[case + "/xy"][:, 1], "angle": c[case + "/angle"]}
     got, _ = fsb.gsift.detect(img, max_kp=max_kp, contrast=contrast, edge=edge)
     frac, p = paired_fraction(cv, got)
-    assert frac >= 0.90, frac
+    f_ref, _ = paired_fraction(cv, ref)
+    print("\n[%s] OpenCV keypoints reproduced: reference CPU path %.4f, float32 GPU path %.4f" % (case, f_ref, frac))
+    assert frac >= f_ref - 0.01, (frac, f_ref)
     # descriptors of paired keypoints: OpenCV rounds to integers; compare bytes
     m = np.nonzero(p >= 0)[0]
     _, st = fsb.gsift.detect(img, max_kp=max_kp, contrast=contrast, edge=edge)

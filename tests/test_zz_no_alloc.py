@@ -50,11 +50,30 @@ def test_no_alloc_matches_allocating_entry_point_twice():
         np.testing.assert_array_equal(t, t_ref)
 
 
-def test_no_alloc_rejects_sizes_beyond_its_limit():
+def test_no_alloc_at_its_largest_layout():
+    """16384 x 16384 fills the per-target key table and the top-2 table to their fixed capacity;
+    16384 x 130 runs the most column splits the table allows for a full A side."""
+    import torch
+
+    import fieldstitch_b200 as F
+    from fieldstitch_b200 import _lib, synth
+    lib = _lib.load()
+    dev = torch.device("cuda", 0)
+    for na, nb, seed, ratio in [(16384, 16384, 13, 0.8), (16384, 130, 14, 0.8)]:
+        a, b, _ = synth.synth_descriptors(na, nb, seed)
+        q_ref, t_ref = F.matching._ratio_match_bf(a, b, ratio)
+        q, t = _call(lib, torch, a, b, ratio, dev)
+        assert len(q_ref) > 0
+        np.testing.assert_array_equal(q, q_ref)
+        np.testing.assert_array_equal(t, t_ref)
+
+
+@pytest.mark.parametrize("na,nb", [(16385, 10), (10, 16385)])
+def test_no_alloc_rejects_sizes_beyond_its_limit(na, nb):
     from fieldstitch_b200 import _lib
     lib = _lib.load()
     # the size check comes before any pointer is used, so placeholder addresses are never touched
-    st = lib.fsb_match_bf_noalloc(ctypes.c_void_p(16), 16385, ctypes.c_void_p(16), 10, ctypes.c_float(0.8),
+    st = lib.fsb_match_bf_noalloc(ctypes.c_void_p(16), na, ctypes.c_void_p(16), nb, ctypes.c_float(0.8),
                                   ctypes.c_void_p(16), ctypes.c_void_p(16), ctypes.c_void_p(16), None)
     assert st == 1
     assert b"16384-row limit" in lib.fsb_last_error()
