@@ -64,6 +64,9 @@ def parse():
                    help="pairs timed through the plain sequential path (one stream, one pair at a time; 0: skip)")
     p.add_argument("--filter-pairs", type=int, default=64,
                    help="pairs for the learned match filter (3/4 train, 1/4 held out; 0: skip)")
+    p.add_argument("--flight-lines", type=int, default=20,
+                   help="synthetic flight: lines x frames per line (20: 400 frames; 0: skip)")
+    p.add_argument("--flight-train", type=int, default=200, help="synthetic flight: pairs that train the filter")
     return p.parse_args()
 
 
@@ -453,6 +456,242 @@ def learned_filter(args, local, pairs):
             "bf16_fp32_decision_agreement": agree / total if total else None}
 
 
+def synthetic_flight(args, local):
+    """Config 5: a seeded 20000 x 16000 procedural terrain, frames of 2640 x 1978 cropped from it along a
+    lawnmower grid (80 % forward / 70 % side overlap, +-3 deg yaw, +-2 % scale; return lines flown at
+    180 deg), the reference pipeline's GNSS neighbour pairs (16 nearest within 0.95 x the long
+    footprint side, plus the next two frames), prior = true homography + N(0, 15 px).
+
+    Batched path: every frame extracted once (sift_gpu sequence, nfeat 7000, the "accurate" preset)
+    on args.streams contexts, the prior projections, then every pair's guided match in one
+    fsb_match_guided_batch_d call (a CUDA graph). Plain path: one context, frames then pairs one
+    after another (host waits after every call). Both from frames resident in HBM; device events and
+    the host clock, the larger. The learned filter is trained on the first pairs' candidates (labels:
+    the plain pipeline's RANSAC) and replaces the ratio test on every pair."""
+    import ctypes
+    from concurrent.futures import ThreadPoolExecutor
+
+    import torch
+
+    from fieldstitch_b200 import _lib, synth
+    from fieldstitch_b200 import match_filter as MF
+    dev = torch.device("cuda", local)
+    h, w = H_IMG, W_IMG
+    t0 = time.perf_counter()
+    terrain = synth.flight_terrain(args.seed + 5, device=local)
+    poses = synth.lawnmower(args.seed + 6, lines=args.flight_lines, per_line=args.flight_lines)
+    frames = synth.render_frames(terrain, poses, seed=args.seed + 7)
+    del terrain
+    torch.cuda.empty_cache()
+    pairs = synth.gnss_pairs(poses, sigma=15.0, seed=args.seed + 8)
+    torch.cuda.synchronize()
+    gen_s = time.perf_counter() - t0
+    n, P, nf = len(poses), len(pairs), 7000
+    prm = _lib.SiftParams(0.015, 12.0, 0, 0)
+
+    def Pt(t):
+        return ctypes.c_void_p(t.data_ptr())
+
+    xy = torch.empty((n, nf, 2), dtype=torch.float32, device=dev)
+    rs = torch.empty((n, nf), dtype=torch.float32, device=dev)
+    u8 = torch.empty((n, nf, 128), dtype=torch.uint8, device=dev)
+    sz = torch.empty((n, nf), dtype=torch.float32, device=dev)
+    an = torch.empty((n, nf), dtype=torch.float32, device=dev)
+    oc = torch.empty((n, nf), dtype=torch.int32, device=dev)
+    bxy = torch.empty((n, nf, 2), dtype=torch.float64, device=dev)
+    pred = torch.empty((P, nf, 2), dtype=torch.float64, device=dev)
+    g = torch.Generator(device=dev).manual_seed(args.seed + 9)
+    noise = (15.0 * torch.randn((P, nf, 2), generator=g, device=dev)).to(torch.float32)
+    q_b = torch.empty((P, nf), dtype=torch.int64, device=dev)
+    t_b = torch.empty((P, nf), dtype=torch.int64, device=dev)
+    Hs = [np.ascontiguousarray(synth.frame_homography(poses[i], poses[j]).reshape(9)) for i, j in pairs]
+    eye = np.eye(3).reshape(9).copy()
+    nk = [0] * n
+    by_first = [[] for _ in range(n)]
+    for p, (i, _) in enumerate(pairs):
+        by_first[i].append(p)
+    S = args.streams
+    ctxs = [_lib.Context(local) for _ in range(S)]
+    mctx = _lib.Context(local)
+    pool = ThreadPoolExecutor(max_workers=S)
+
+    def extract_frames(k):
+        c = ctxs[k]
+        L, cnt = c.lib, ctypes.c_int32()
+        for i in range(k, n, S):
+            _lib.check(L.fsb_sift_features_ex_d(c.handle, Pt(frames[i]), h, w, w, ctypes.byref(prm), nf, Pt(xy[i]),
+                                                Pt(rs[i]), None, Pt(u8[i]), Pt(sz[i]), Pt(an[i]), Pt(oc[i]),
+                                                ctypes.byref(cnt)), "sift")
+            nk[i] = cnt.value
+            _lib.check(L.fsb_project_d(c.handle, Pt(xy[i]), nk[i], _lib.ptr(eye), None, Pt(bxy[i])), "proj")
+            for p in by_first[i]:
+                _lib.check(L.fsb_project_d(c.handle, Pt(xy[i]), nk[i], _lib.ptr(Hs[p]), Pt(noise[p]), Pt(pred[p])),
+                           "proj")
+
+    Pv, Iv, Dv = ctypes.c_void_p * P, ctypes.c_int32 * P, ctypes.c_double * P
+    counts = Iv()
+
+    def match_all():
+        _lib.check(mctx.lib.fsb_match_guided_batch_d(
+            mctx.handle, P, Pv(*[pred[p].data_ptr() for p in range(P)]), Pv(*[u8[i].data_ptr() for i, _ in pairs]),
+            Iv(*[nk[i] for i, _ in pairs]), Pv(*[bxy[j].data_ptr() for _, j in pairs]),
+            Pv(*[u8[j].data_ptr() for _, j in pairs]), Iv(*[nk[j] for _, j in pairs]), Dv(*([float(w)] * P)),
+            Dv(*([float(h)] * P)), RADIUS, KC, RATIO, Pv(*[q_b[p].data_ptr() for p in range(P)]),
+            Pv(*[t_b[p].data_ptr() for p in range(P)]), counts), "guided batch")
+
+    def batched():
+        for f in [pool.submit(extract_frames, k) for k in range(S)]:
+            f.result()
+        match_all()
+
+    def clocked(fn, streams):
+        """(ms, result): device events bracketing every stream, and the host clock; the larger."""
+        main = torch.cuda.current_stream(dev)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        w0 = time.perf_counter()
+        e0.record(main)
+        for st in streams:
+            st.wait_event(e0)
+        out = fn()
+        for st in streams:
+            ev = torch.cuda.Event()
+            ev.record(st)
+            main.wait_event(ev)
+        e1.record(main)
+        torch.cuda.synchronize()
+        return max(e0.elapsed_time(e1), (time.perf_counter() - w0) * 1000.0), out
+
+    streams = [torch.cuda.ExternalStream(c.stream()) for c in ctxs + [mctx]]
+    batched()   # warm-up: workspaces, autotuning of the frame geometry, the match graph's capture
+    torch.cuda.synchronize()
+    ms_batched, _ = clocked(batched, streams)
+    got = [(q_b[p, :counts[p]].clone(), t_b[p, :counts[p]].clone()) for p in range(P)]
+
+    # ---- plain path: one context, one call at a time
+    pc = ctxs[0]
+    L, cnt = pc.lib, ctypes.c_int32()
+    q_p = torch.empty(nf, dtype=torch.int64, device=dev)
+    t_p = torch.empty(nf, dtype=torch.int64, device=dev)
+    same = [True]
+
+    def plain():
+        for i in range(n):
+            _lib.check(L.fsb_sift_features_ex_d(pc.handle, Pt(frames[i]), h, w, w, ctypes.byref(prm), nf, Pt(xy[i]),
+                                                Pt(rs[i]), None, Pt(u8[i]), Pt(sz[i]), Pt(an[i]), Pt(oc[i]),
+                                                ctypes.byref(cnt)), "sift")
+            nk[i] = cnt.value
+            _lib.check(L.fsb_project_d(pc.handle, Pt(xy[i]), nk[i], _lib.ptr(eye), None, Pt(bxy[i])), "proj")
+        for p, (i, j) in enumerate(pairs):
+            _lib.check(L.fsb_project_d(pc.handle, Pt(xy[i]), nk[i], _lib.ptr(Hs[p]), Pt(noise[p]), Pt(pred[p])),
+                       "proj")
+            _lib.check(L.fsb_match_guided_d(pc.handle, Pt(pred[p]), Pt(u8[i]), nk[i], Pt(bxy[j]), Pt(u8[j]), nk[j],
+                                            float(w), float(h), RADIUS, KC, RATIO, Pt(q_p), Pt(t_p),
+                                            ctypes.byref(cnt)), "guided")
+            m = cnt.value
+            same[0] = same[0] and m == len(got[p][0]) and torch.equal(q_p[:m], got[p][0]) and \
+                torch.equal(t_p[:m], got[p][1])
+
+    ms_plain, _ = clocked(plain, [torch.cuda.ExternalStream(pc.stream())])
+
+    # ---- correctness of the batched matches against the true homographies
+    n_match = n_good = pairs_ok = 0
+    xy_h = xy.cpu().numpy()
+    for p, (i, j) in enumerate(pairs):
+        q, t = got[p][0].cpu().numpy(), got[p][1].cpu().numpy()
+        if len(q) == 0:
+            continue
+        proj = synth.apply_homography(Hs[p].reshape(3, 3), xy_h[i][q])
+        good = np.linalg.norm(proj - xy_h[j][t], axis=1) < 3.0
+        n_match += len(q)
+        n_good += int(good.sum())
+        pairs_ok += int(good.sum() >= 20)
+
+    # ---- learned filter: trained on the first pairs' candidates, applied to every pair
+    def frame_dict(i):
+        k = nk[i]
+        return {"xy": xy[i, :k], "resp": rs[i, :k], "u8": u8[i, :k], "size": sz[i, :k], "angle": an[i, :k],
+                "octave": oc[i, :k]}
+
+    n_train = min(args.flight_train, P)
+    feats, labs = [], []
+    for p in range(n_train):
+        i, j = pairs[p]
+        A, B = frame_dict(i), frame_dict(j)
+        pr = pred[p, :nk[i]]
+        t1, b12 = MF.candidates(pr, A, B, (w, h), RADIUS, KC, local)
+        ft = MF.features(t1, b12, pr, A, B, RADIUS, local)
+        q, t = MF.accept(t1, b12, nk[j], None, ratio=RATIO, device=local)
+        t1h = t1.cpu().numpy()
+        lab, _ = MF.ransac_labels(xy_h[i][:nk[i]].astype(np.float64), xy_h[j][:nk[j]].astype(np.float64),
+                                  q.cpu().numpy(), t.cpu().numpy(), t1h)
+        ok = torch.from_numpy(t1h >= 0).to(dev)
+        feats.append(ft[ok])
+        labs.append(torch.from_numpy(lab).to(dev)[ok])
+    mf = MF.MatchFilter(device=local)
+    mf.fit(torch.cat(feats), torch.cat(labs), epochs=30, batch=8192, lr=2e-3, seed=args.seed)
+    torch.cuda.synchronize()
+
+    acc = {"ratio_test": [0, 0], "mlp_filter": [0, 0]}
+    pos = 0
+
+    def filter_all(evaluate):
+        nonlocal pos
+        for p, (i, j) in enumerate(pairs):
+            A, B = frame_dict(i), frame_dict(j)
+            pr = pred[p, :nk[i]]
+            t1, b12 = MF.candidates(pr, A, B, (w, h), RADIUS, KC, local)
+            ft = MF.features(t1, b12, pr, A, B, RADIUS, local)
+            qf, tf = mf.matches(t1, b12, nk[j], ft)
+            if evaluate and p >= n_train:
+                t1h = t1.cpu().numpy()
+                okc = t1h >= 0
+                truth = np.zeros(nk[i], bool)
+                if okc.any():
+                    proj = synth.apply_homography(Hs[p].reshape(3, 3), xy_h[i][:nk[i]][okc])
+                    truth[okc] = np.linalg.norm(proj - xy_h[j][t1h[okc]], axis=1) < 3.0
+                pos += int(truth.sum())
+                qr = got[p][0].cpu().numpy()
+                for key, qq in (("ratio_test", qr), ("mlp_filter", qf.cpu().numpy())):
+                    acc[key][0] += int(truth[qq].sum())
+                    acc[key][1] += len(qq)
+
+    filter_all(True)
+    ms_filter, _ = clocked(lambda: filter_all(False), [torch.cuda.ExternalStream(_lib.context(local).stream())])
+
+    def prf(k):
+        tp, m = acc[k]
+        return {"precision": tp / m if m else 0.0, "recall": tp / pos if pos else 0.0,
+                "f1": 2 * tp / (m + pos) if (m + pos) else 0.0}
+
+    pool.shutdown()
+    for c in ctxs + [mctx]:
+        c.close()
+    del frames
+    torch.cuda.empty_cache()
+    return {"workload": "synthetic flight: %d frames %dx%d cropped from a seeded 20000x16000 terrain on a %dx%d "
+                        "lawnmower grid (80%%/70%% overlap, +-3 deg yaw, +-2%% scale), %d GNSS neighbour pairs "
+                        "(pipeline.py:452-476 rule, 16 neighbours), nfeat 7000, prior = true homography + "
+                        "N(0, 15 px), the %d nearest within %g px, ratio %g"
+                        % (n, w, h, args.flight_lines, args.flight_lines, P, KC, RADIUS, RATIO),
+            "frames": n, "pairs": P, "generate_s": gen_s,
+            "batched": {"ms": ms_batched, "pairs_per_s": P / (ms_batched / 1000.0), "streams": S,
+                        "path": "frames extracted once on %d contexts + projections + one guided-batch graph" % S},
+            "plain_fp32": {"ms": ms_plain, "pairs_per_s": P / (ms_plain / 1000.0),
+                           "path": "one context, frames then pairs one call at a time"},
+            "batched_over_plain": ms_plain / ms_batched,
+            "identical_matches_batched_vs_plain": bool(same[0]),
+            "matches": {"total": n_match, "within_3px_of_truth": n_good,
+                        "pairs_with_20_correct": pairs_ok, "precision_vs_truth": n_good / n_match if n_match else 0.0},
+            "learned_filter": {"train_pairs": n_train, "held_out_pairs": P - n_train,
+                               "vs_true_homography": {"ratio_test": prf("ratio_test"), "mlp_filter": prf("mlp_filter")},
+                               "filter_path_ms": ms_filter,
+                               "e2e_with_filter_pairs_per_s": P / ((ms_batched + ms_filter) / 1000.0),
+                               "path": "per pair: guided candidates, features, BF16 inference, accept (one stream)"},
+            "precision": "distances are exact integers (uint8 RootSIFT): FP32, BF16 and FP8 give the same matches; "
+                         "the extraction is float32"}
+
+
 def run_fsb(args):
     import ctypes
     from concurrent.futures import ThreadPoolExecutor
@@ -762,6 +1001,9 @@ def run_fsb(args):
     sweep = None
     if rank == 0 and args.sweep_pairs > 0:
         sweep = dense_sweep(args, local)
+    flight = None
+    if rank == 0 and args.flight_lines > 0:
+        flight = synthetic_flight(args, local)
     filt = None
     if rank == 0 and args.filter_pairs > 0:
         fp = pairs[:args.filter_pairs]
@@ -779,7 +1021,7 @@ def run_fsb(args):
                 "clocks": clk, "e2e": e2e, "gpu_launches": int(launches), "roofline": roof, "cpu_baseline": cpu,
                 "parity_checked": parity["parity_checked"], "parity": parity,
                 "matches_per_step": matches / args.steps, "plain_single_stream": plain,
-                "dense_precision_sweep": sweep, "learned_filter": filt,
+                "dense_precision_sweep": sweep, "learned_filter": filt, "synthetic_flight": flight,
                 "stages_ms_per_step_summed_over_streams": {k: v[0] / args.steps for k, v in stages.items()},
                 "stages_ms_per_image_one_stream": iso_stages}
         print(json.dumps(line, default=_json_num), flush=True)

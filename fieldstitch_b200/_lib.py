@@ -51,6 +51,8 @@ SIGNATURES = [
     ("fsb_build_tracks", c_i32, [c_vp, c_vp, c_vp, c_i64, c_vp, c_i32, c_vp, c_vp, c_vp, c_vp, c_vp]),
     ("fsb_find_homography_batch", c_i32, [c_vp, c_i32, c_vp, c_vp, c_vp, ctypes.c_double, c_i32, ctypes.c_uint64,
                                           c_vp, c_vp, c_vp]),
+    ("fsb_find_fundamental_batch", c_i32, [c_vp, c_i32, c_vp, c_vp, c_vp, ctypes.c_double, c_i32, ctypes.c_uint64,
+                                           c_vp, c_vp, c_vp]),
     ("fsb_spread", c_i32, [c_vp, c_vp, c_vp, c_vp, c_i32, c_i32, c_i32, c_i32, c_i32, c_vp, c_vp]),
     ("fsb_decode_gray_d", c_i32, [c_vp, c_vp, c_i64, c_i32, c_vp, c_i64, c_vp, c_vp]),
     ("fsb_prepare_gray", c_i32, [c_vp, c_vp, c_i64, c_i32, ctypes.c_double, c_vp, c_i64, c_vp, c_vp]),

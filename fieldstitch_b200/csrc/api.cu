@@ -1143,6 +1143,35 @@ int32_t fsb_find_homography_batch(fsb_ctx* ctx, int32_t n_pairs, const int64_t* 
     return copy_out(ctx, out, 3);
 }
 
+int32_t fsb_find_fundamental_batch(fsb_ctx* ctx, int32_t n_pairs, const int64_t* offsets, const double* src,
+                                   const double* dst, double thr, int32_t iters, uint64_t seed, double* F, uint8_t* mask,
+                                   int32_t* n_inliers) {
+    FSB_ARG(ctx && offsets && F && n_inliers, "null pointer");
+    FSB_ARG(n_pairs >= 0 && iters >= 1 && iters <= (1 << 20) && thr > 0.0, "bad arguments");
+    FSB_ARG(offsets[0] == 0, "offsets must start at 0");
+    for (int p = 0; p < n_pairs; ++p) FSB_ARG(offsets[p + 1] >= offsets[p], "offsets must ascend");
+    if (n_pairs == 0) return FSB_OK;
+    const size_t N = (size_t)offsets[n_pairs];
+    FSB_ARG(N == 0 || (src && dst && mask), "null point or mask array");
+    FSB_TRY(use_device(ctx));
+    FSB_TRY(ctx->s_f32a.ensure(N * 32 + 256));
+    FSB_TRY(ctx->s_i64.ensure((size_t)(n_pairs + 1) * 8 + 256));
+    FSB_TRY(ctx->s_f32b.ensure((size_t)n_pairs * 76 + N + 512));
+    double* dsrc = ctx->s_f32a.as<double>();
+    double* ddst = dsrc + 2 * N;
+    long long* doff = ctx->s_i64.as<long long>();
+    double* dF = ctx->s_f32b.as<double>();
+    int* dn = reinterpret_cast<int*>(dF + 9 * (size_t)n_pairs);
+    uint8_t* dm = reinterpret_cast<uint8_t*>(dn + n_pairs);
+    const HostCopy in[3] = {{(void*)src, dsrc, N * 16}, {(void*)dst, ddst, N * 16},
+                            {(void*)offsets, doff, (size_t)(n_pairs + 1) * 8}};
+    FSB_TRY(copy_in(ctx, in, 3));
+    FSB_TRY(run_ransac_f(doff, n_pairs, reinterpret_cast<const double2*>(dsrc), reinterpret_cast<const double2*>(ddst),
+                         thr, iters, seed, dF, dm, dn, ctx->stream));
+    const HostCopy out[3] = {{F, dF, (size_t)n_pairs * 72}, {n_inliers, dn, (size_t)n_pairs * 4}, {mask, dm, N}};
+    return copy_out(ctx, out, 3);
+}
+
 int32_t fsb_spread(fsb_ctx* ctx, const float* x, const float* y, const float* resp, int32_t n, int32_t W, int32_t H,
                    int32_t nfeat, int32_t order, int32_t* sel, int32_t* n_out) {
     FSB_ARG(ctx && n_out, "null pointer");

@@ -566,8 +566,14 @@ int32_t run_detect(fsb_ctx* ctx, Workspace& ws, double contrast, double edge, in
             note_launch();
         }
         FSB_CUDA(cudaGetLastError());
-        FSB_CUDA(cudaMemcpyAsync(h_cnt, cnt, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+        uint32_t h_head[PYR_ERR_WORD + 1];
+        FSB_CUDA(cudaMemcpyAsync(h_head, cnt, sizeof(h_head), cudaMemcpyDeviceToHost, s));
         FSB_CUDA(cudaStreamSynchronize(s));
+        if (h_head[PYR_ERR_WORD]) {
+            set_error("pyramid: a TMA row copy did not complete in time (strip engine)");
+            return FSB_ERR_TIMEOUT;
+        }
+        h_cnt[0] = h_head[0];
         if (h_cnt[0] <= ws.cap_cand) break;
         ws.cap_cand = (size_t)h_cnt[0] + (h_cnt[0] >> 3) + 1024;
         FSB_TRY(ws.cand.ensure(ws.cap_cand * sizeof(uint32_t)));

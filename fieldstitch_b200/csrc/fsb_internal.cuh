@@ -207,6 +207,10 @@ int32_t launch_base_fast(const uint8_t* img, int stride, int ih, int iw, float* 
 int32_t launch_group_lower(const float* src, int R, int C, float* dog, float* mag, float* ang, float* l3, float* down,
                            int down_cols, cudaStream_t s);
 int32_t launch_group_upper(const float* src, int R, int C, float* dog3, cudaStream_t s);
+// strip engine: the whole float32 octave in one launch (err: device word set when a TMA wait gives up)
+int32_t launch_octave_strip(const float* L0, int R, int C, float* dog, float* mag, float* ang, float* down,
+                            int down_cols, int* err, cudaStream_t s);
+constexpr int PYR_ERR_WORD = 8;   // index of the pyramid's error word in Workspace::counters
 // autotune.cu: the fastest of n_variants launches of `run` for `key` (timed once per process and
 // device on `s`, then cached; FSB_AUTOTUNE=0 returns variant 0, FSB_AUTOTUNE_FILE persists choices)
 bool autotune_cached(const char* key, int n_variants, int* variant);
@@ -262,6 +266,8 @@ int32_t run_match_bf_tc(fsb_ctx* ctx, int n_pairs, const uint8_t* const* d_a, co
 // ransac.cu
 int32_t run_ransac_h(const long long* d_off, int n_pairs, const double2* d_src, const double2* d_dst, double thr,
                      int iters, unsigned long long seed, double* d_H, uint8_t* d_mask, int* d_ninl, cudaStream_t s);
+int32_t run_ransac_f(const long long* d_off, int n_pairs, const double2* d_src, const double2* d_dst, double thr,
+                     int iters, unsigned long long seed, double* d_F, uint8_t* d_mask, int* d_ninl, cudaStream_t s);
 // jpeg.cu
 int32_t run_jpeg_gray(fsb_ctx* ctx, const uint8_t* data, size_t len, int reduce, uint8_t* d_out, size_t out_cap,
                       int* h, int* w);

@@ -18,6 +18,10 @@
 // gradient of L_{i-1} (layers 1..3) and L_3[::2, ::2] (the next octave's base), with 16-byte
 // stores where the row pitch allows. HBM traffic per octave pixel: L0 read once (plus the column
 // halo) and 44 B written; no intermediate layer ever leaves the SM.
+#include <cuda.h>
+
+#include <cstring>
+
 #include "fsb_internal.cuh"
 
 namespace fsb {
@@ -943,7 +947,476 @@ int32_t launch_group_t(GroupArgs a, cudaStream_t s) {
     return FSB_OK;
 }
 
+// ------------------------------------------------------------------------------------------------
+// Strip engine (float32 path): one launch per octave. A CTA owns a 128-column strip and a range of
+// output rows and streams down it eight rows per step; all five layers of the octave are held in
+// shared-memory row rings, so per octave pixel HBM sees one read of L0 (plus the strip's column
+// halo) and the 44 bytes of DoG and gradient output, nothing else.
+//
+//   level i (L0 .. L4) ring: TN(i) rows of TWID(i) columns starting TH(i) columns left of the
+//       strip; slot of image row y = (y - RB) mod TN(i). Ring 0 holds the 2 r_1 + 8 rows stage 1
+//       reads plus the next eight rows arriving by TMA (one 2-D tensor copy per row, the row index
+//       reflected at the image's top and bottom; columns outside the image are filled in from
+//       global memory with the reflected column after the copy lands).
+//   stage i (1 .. 5), at step t, produces rows Y_i = Y_1 - TLAG(i) .. + 7 of L_i, Y_1 = V0 + 8t + 3:
+//       phase A  vertical pass of L_{i-1} into the row-pair interleaved buffer (thread = column
+//                pair, all eight rows: 2 r + 8 loads); with it the gradient of L_{i-1} at rows
+//                Y_i .. (i = 2..4, plus L3[::2, ::2] for i = 4) and the DoG L_{i-1} - L_{i-2} at
+//                rows Y_{i-1} .. (i = 2..5), both on the strip's own columns;
+//       phase B  horizontal pass (thread = row pair x four columns) into ring i; stage 5 writes the
+//                DoG L5 - L4 from registers instead.
+// The passes are the per-layer kernels' (the same packed pair blurs in the same order), so the
+// outputs are bit-identical to theirs: L0 is mirrored once and every level computed on the
+// extended domain is the mirror image of its interior (pair sums commute). A stage runs only while
+// its rows are needed by the output range (the range widened by the later layers' radii).
+constexpr int TW = 128, TSTEP = 8, TNT = 256;
+__host__ __device__ constexpr int TH(int i) { return i == 0 ? 44 : i == 1 ? 38 : i == 2 ? 32 : i == 3 ? 24 : i == 4 ? 14 : 0; }
+__host__ __device__ constexpr int TWID(int i) { return i == 0 ? 216 : i == 1 ? 204 : i == 2 ? 192 : i == 3 ? 176 : i == 4 ? 156 : 128; }
+__host__ __device__ constexpr int TPITCH(int i) { return i == 0 ? 224 : TWID(i); }
+__host__ __device__ constexpr int TN(int i) { return i == 0 ? 2 * 5 + 2 * TSTEP : 2 * RAD(i + 1) + TSTEP; }
+// rows (and columns) of L_i needed beyond the output range
+__host__ __device__ constexpr int TE(int i) { return i == 0 ? 42 : i == 1 ? 37 : i == 2 ? 31 : i == 3 ? 23 : i == 4 ? 13 : 0; }
+__host__ __device__ constexpr int TLAG(int i) { return i == 1 ? 0 : i == 2 ? 6 : i == 3 ? 14 : i == 4 ? 24 : 37; }
+// vertical pass of stage i: columns x0 - TH(i-1) .. (ring i-1 column j = V column j), TVW(i) of them,
+// stored at float2 index j + TSD(i) % 2 so that the horizontal pass reads from an even index
+__host__ __device__ constexpr int TVW(int i) { return TWID(i - 1); }
+__host__ __device__ constexpr int TSD(int i) { return TH(i - 1) - TH(i) - RAD(i); }
+constexpr int TVP = 218;   // float2 per row pair of the vertical-pass buffer
+__host__ __device__ constexpr int toff(int i) { return i == 0 ? 0 : toff(i - 1) + TN(i - 1) * TPITCH(i - 1); }
+constexpr int TVB_OFF = toff(5);
+constexpr int TBAR_OFF = TVB_OFF + 4 * TVP * 2;
+constexpr int TSMEM = TBAR_OFF * 4 + 32;
+constexpr int TROW_BYTES = TWID(0) * 4;   // one TMA row copy
+static_assert(TSD(1) >= 0 && TSD(2) >= 0 && TSD(3) >= 0 && TSD(4) >= 0 && TSD(5) >= 0, "strip halos");
+static_assert(TVW(1) + TSD(1) % 2 <= TVP && TVW(5) + TSD(5) % 2 <= TVP, "vertical buffer width");
+static_assert((toff(1) * 4) % 128 == 0 && (TPITCH(0) * 4) % 128 == 0, "TMA destinations 128-byte aligned");
+static_assert(TSMEM <= 113 * 1024, "two CTAs per SM");
+constexpr long long TSTRIP_TIMEOUT = 2000000000ll;   // cycles (about a second) for one TMA row block
+
+struct StripArgs {
+    const float* L0;   // octave base, R x C, row pitch C
+    int R, C, rows;    // rows: output rows per CTA
+    float* dog[5];
+    float* mag[3];
+    float* ang[3];
+    float* down;       // L3[::2, ::2] (pitch down_cols) or null
+    int down_cols;
+    int* err;          // set to 1 when a TMA wait gives up
+};
+
+__device__ __forceinline__ uint32_t s_addr(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ bool s_mbar_test(uint64_t* b, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(s_addr(b)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+
+// Waits (bounded) for one row block; every thread waits, then the CTA agrees on the outcome.
+__device__ __forceinline__ bool s_mbar_wait(uint64_t* b, uint32_t parity) {
+    bool ok = s_mbar_test(b, parity);
+    if (!ok) {
+        const long long t0 = clock64();
+        while (!(ok = s_mbar_test(b, parity)) && clock64() - t0 < TSTRIP_TIMEOUT) {
+        }
+    }
+    return ok;
+}
+
+// rows y .. y + 7 of L0 into ring 0: TMA (one thread issues eight row copies on `bar`) or, when
+// tma is false, cp.async with reflected rows and columns
+__device__ __forceinline__ void s_load_block(const CUtensorMap* tm, const StripArgs& a, float* ring0, uint64_t* bar,
+                                             int x0, int y, int RB, bool tma) {
+    if (tma) {
+        if (threadIdx.x == 0) {
+            asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(s_addr(bar)),
+                         "r"(TSTEP * TROW_BYTES)
+                         : "memory");
+#pragma unroll 1
+            for (int k = 0; k < TSTEP; ++k) {
+                const int row = y + k;
+                float* dst = ring0 + ((row - RB) % TN(0)) * TPITCH(0);
+                asm volatile(
+                    "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];" ::"r"(
+                        s_addr(dst)),
+                    "l"(reinterpret_cast<uint64_t>(tm)), "r"(x0 - TH(0)), "r"(mir(row, a.R)), "r"(s_addr(bar))
+                    : "memory");
+            }
+        }
+    } else {
+        const int c = threadIdx.x;
+        if (c < TWID(0)) {
+            int xs = x0 - TH(0) + c;
+            if (xs < 0 || xs >= a.C) xs = mir(xs, a.C);
+#pragma unroll 1
+            for (int k = 0; k < TSTEP; ++k) {
+                const int row = y + k;
+                cp_async4(ring0 + ((row - RB) % TN(0)) * TPITCH(0) + c, a.L0 + (size_t)mir(row, a.R) * a.C + xs);
+            }
+        }
+        cp_commit();
+    }
+}
+
+// After a TMA block landed: the columns outside the image (zero-filled) get their reflected values
+__device__ __forceinline__ void s_fix_edges(const StripArgs& a, float* ring0, int x0, int y, int RB) {
+    const int lo = TH(0) - x0;                 // ring columns [0, lo) are left of the image
+    const int hi = a.C - (x0 - TH(0));         // ring columns [hi, TWID(0)) are right of it
+    if (lo <= 0 && hi >= TWID(0)) return;
+    for (int i = threadIdx.x; i < TSTEP * TWID(0); i += TNT) {
+        const int k = i / TWID(0), c = i - k * TWID(0);
+        if (c >= lo && c < hi) continue;
+        const int row = y + k;
+        ring0[((row - RB) % TN(0)) * TPITCH(0) + c] = __ldg(a.L0 + (size_t)mir(row, a.R) * a.C + mir(x0 - TH(0) + c, a.C));
+    }
+}
+
+// Gradient of the float32 path for two pixels at once: fast_grad's operations in fast_grad's order,
+// the multiplications and additions packed in pairs (identical roundings).
+__device__ __forceinline__ void fast_grad2(float2 dx, float2 dy, float2& mag, float2& ang) {
+    const float2 d2 = __fadd2_rn(__fmul2_rn(dx, dx), __fmul2_rn(dy, dy));
+    const float2 rs = make_float2(d2.x > 0.f ? rsqrtf(d2.x) : 0.f, d2.y > 0.f ? rsqrtf(d2.y) : 0.f);
+    const float2 m = __fmul2_rn(d2, rs);
+    mag = make_float2(d2.x > 0.f ? m.x : 0.f, d2.y > 0.f ? m.y : 0.f);
+    const float ax0 = fabsf(dx.x), ay0 = fabsf(dy.x), ax1 = fabsf(dx.y), ay1 = fabsf(dy.y);
+    const float mx0 = fmaxf(ax0, ay0), mn0 = fminf(ax0, ay0), mx1 = fmaxf(ax1, ay1), mn1 = fminf(ax1, ay1);
+    const float2 t = make_float2(mx0 > 0.f ? __fdividef(mn0, mx0) : 0.f, mx1 > 0.f ? __fdividef(mn1, mx1) : 0.f);
+    const float2 z = __fmul2_rn(t, t);
+    float2 p = make_float2(-2.323089093e-01f, -2.323089093e-01f);
+    p = __ffma2_rn(p, z, make_float2(1.252652928e+00f, 1.252652928e+00f));
+    p = __ffma2_rn(p, z, make_float2(-3.203537344e+00f, -3.203537344e+00f));
+    p = __ffma2_rn(p, z, make_float2(5.524570187e+00f, 5.524570187e+00f));
+    p = __ffma2_rn(p, z, make_float2(-7.969057098e+00f, -7.969057098e+00f));
+    p = __ffma2_rn(p, z, make_float2(1.142854019e+01f, 1.142854019e+01f));
+    p = __ffma2_rn(p, z, make_float2(-1.909660354e+01f, -1.909660354e+01f));
+    p = __ffma2_rn(p, z, make_float2(5.729574144e+01f, 5.729574144e+01f));
+    float2 v = __fmul2_rn(p, t);
+    float2 f = __fadd2_rn(make_float2(90.f, 90.f), make_float2(-v.x, -v.y));
+    v = make_float2(ay0 > ax0 ? f.x : v.x, ay1 > ax1 ? f.y : v.y);
+    f = __fadd2_rn(make_float2(180.f, 180.f), make_float2(-v.x, -v.y));
+    v = make_float2(dx.x < 0.f ? f.x : v.x, dx.y < 0.f ? f.y : v.y);
+    f = __fadd2_rn(make_float2(360.f, 360.f), make_float2(-v.x, -v.y));
+    ang = make_float2(dy.x < 0.f ? f.x : v.x, dy.y < 0.f ? f.y : v.y);
+}
+
+__device__ __forceinline__ void s_store4(float* p, float4 v, bool vec, int left) {
+    if (vec) {
+        *reinterpret_cast<float4*>(p) = v;
+    } else {
+        const float w[4] = {v.x, v.y, v.z, v.w};
+        for (int k = 0; k < 4 && k < left; ++k) p[k] = w[k];
+    }
+}
+
+template <int I>
+__device__ __forceinline__ int s_slot(int row, int RB) { return (row - RB) % TN(I); }
+
+struct StripCta {
+    int x0, ya, yz, RB;
+    bool vec;   // 16-byte stores of the output planes (C multiple of 4, planes aligned)
+};
+
+// vertical pass of stage I, column pair q: all eight rows Y .. Y + 7
+template <int I>
+__device__ __forceinline__ void s_vitem(const float* __restrict__ ring, float2* __restrict__ vb, int q, int s0,
+                                        const float2 (&w)[RAD(I) + 1]) {
+    constexpr int r = RAD(I), N = TN(I - 1), P = TPITCH(I - 1), dd = TSD(I) & 1;
+    const float* base = ring + 2 * q;
+    float2 x[2 * r + TSTEP];
+    int s = s0;
+#pragma unroll
+    for (int k = 0; k < 2 * r + TSTEP; ++k) {
+        x[k] = *reinterpret_cast<const float2*>(base + s * P);
+        s = s + 1 == N ? 0 : s + 1;
+    }
+    float2* d = vb + 2 * q + dd;
+#pragma unroll
+    for (int sp = 0; sp < TSTEP / 2; ++sp) {
+        const float2 o0 = blur_pairs_w<r>(x + 2 * sp, w), o1 = blur_pairs_w<r>(x + 2 * sp + 1, w);
+        d[sp * TVP] = make_float2(o0.x, o1.x);
+        d[sp * TVP + 1] = make_float2(o0.y, o1.y);
+    }
+}
+
+// gradient of L_I (I = 1..3) at image row y, strip columns 4g .. 4g + 3, from ring I; for I = 3
+// also L3[::2, ::2]
+template <int I>
+__device__ __forceinline__ void s_grad_item(const float* __restrict__ ring, const StripArgs& a, const StripCta& k,
+                                            int y, int g) {
+    constexpr int P = TPITCH(I);
+    const int x = k.x0 + 4 * g;
+    if (x >= a.C) return;
+    const float* ct = ring + s_slot<I>(y, k.RB) * P + TH(I) + 4 * g;
+    const float* up = ring + s_slot<I>(y - 1, k.RB) * P + TH(I) + 4 * g;
+    const float* dn = ring + s_slot<I>(y + 1, k.RB) * P + TH(I) + 4 * g;
+    const float2 c0 = *reinterpret_cast<const float2*>(ct), c1 = *reinterpret_cast<const float2*>(ct + 2);
+    const float2 u0 = *reinterpret_cast<const float2*>(up), u1 = *reinterpret_cast<const float2*>(up + 2);
+    const float2 d0 = *reinterpret_cast<const float2*>(dn), d1 = *reinterpret_cast<const float2*>(dn + 2);
+    const float lf = ct[-1], rt = ct[4];
+    float2 dxa = make_float2(__fsub_rn(c0.y, lf), __fsub_rn(c1.x, c0.x));
+    float2 dxb = make_float2(__fsub_rn(c1.y, c0.y), __fsub_rn(rt, c1.x));
+    float2 dya = make_float2(__fsub_rn(u0.x, d0.x), __fsub_rn(u0.y, d0.y));
+    float2 dyb = make_float2(__fsub_rn(u1.x, d1.x), __fsub_rn(u1.y, d1.y));
+    if (!(y > 0 && y < a.R - 1 && x > 0 && x + 4 < a.C)) {
+        float dxv[4] = {dxa.x, dxa.y, dxb.x, dxb.y}, dyv[4] = {dya.x, dya.y, dyb.x, dyb.y};
+#pragma unroll
+        for (int j = 0; j < 4; ++j)
+            if (!(y > 0 && y < a.R - 1 && x + j > 0 && x + j < a.C - 1)) dxv[j] = dyv[j] = 0.f;
+        dxa = make_float2(dxv[0], dxv[1]);
+        dxb = make_float2(dxv[2], dxv[3]);
+        dya = make_float2(dyv[0], dyv[1]);
+        dyb = make_float2(dyv[2], dyv[3]);
+    }
+    float2 ma, mb, na, nb;
+    fast_grad2(dxa, dya, ma, na);
+    fast_grad2(dxb, dyb, mb, nb);
+    const size_t at = (size_t)y * a.C + x;
+    s_store4(a.mag[I - 1] + at, make_float4(ma.x, ma.y, mb.x, mb.y), k.vec, a.C - x);
+    s_store4(a.ang[I - 1] + at, make_float4(na.x, na.y, nb.x, nb.y), k.vec, a.C - x);
+    if (I == 3 && a.down && !(y & 1)) {
+        float* o = a.down + (size_t)(y >> 1) * a.down_cols + (x >> 1);
+        o[0] = c0.x;
+        if (x + 2 < a.C) o[1] = c1.x;
+    }
+}
+
+// DoG L_I - L_{I-1} (I = 1..4) at image row y, strip columns 4g .. 4g + 3
+template <int I>
+__device__ __forceinline__ void s_dog_item(const float* __restrict__ ri, const float* __restrict__ rp, const StripArgs& a,
+                                           const StripCta& k, int y, int g) {
+    const int x = k.x0 + 4 * g;
+    if (x >= a.C) return;
+    const float* c = ri + s_slot<I>(y, k.RB) * TPITCH(I) + TH(I) + 4 * g;
+    const float* p = rp + s_slot<I - 1>(y, k.RB) * TPITCH(I - 1) + TH(I - 1) + 4 * g;
+    const float2 c0 = *reinterpret_cast<const float2*>(c), c1 = *reinterpret_cast<const float2*>(c + 2);
+    const float2 p0 = *reinterpret_cast<const float2*>(p), p1 = *reinterpret_cast<const float2*>(p + 2);
+    const float2 d0 = __fadd2_rn(c0, make_float2(-p0.x, -p0.y)), d1 = __fadd2_rn(c1, make_float2(-p1.x, -p1.y));
+    s_store4(a.dog[I - 1] + (size_t)y * a.C + x, make_float4(d0.x, d0.y, d1.x, d1.y), k.vec, a.C - x);
+}
+
+// Phase A of stage I: vertical pass (rows Y .. Y + 7 of V_I), gradient of L_{I-1} at rows Y .., DoG
+// L_{I-1} - L_{I-2} at rows Y + RAD(I) .. (the rows stage I-1 produced in this step)
+template <int I>
+__device__ __forceinline__ void s_phase_a(float* const* ring, float2* vb, const StripArgs& a, const StripCta& k, int Y,
+                                          bool act) {
+    constexpr int r = RAD(I);
+    constexpr int NV = TVW(I) / 2, NVP = (NV + 31) & ~31;
+    const int ylo = max(k.ya, 0), yhi = min(k.yz, a.R);
+    const bool g_on = I >= 2 && I <= 4 && Y + TSTEP > ylo && Y < yhi;
+    const int Yd = Y + r;   // rows of the DoG L_{I-1} - L_{I-2}
+    const bool d_on = I >= 2 && Yd + TSTEP > ylo && Yd < yhi;
+    const int nv = act ? NVP : 0;
+    const int ng = g_on ? TSTEP * (TW / 4) : 0;
+    const int nd = d_on ? TSTEP * (TW / 4) : 0;
+    float2 w[r + 1];
+    load_taps<I, r>(w);
+    const int s0 = s_slot<I - 1>(Y - r, k.RB);
+    for (int it = threadIdx.x; it < nv + ng + nd; it += TNT) {
+        if (it < nv) {
+            if (it < NV) s_vitem<I>(ring[I - 1], vb, it, s0, w);
+        } else if (it < nv + ng) {
+            if constexpr (I >= 2 && I <= 4) {
+                const int j = it - nv, y = Y + j / (TW / 4);
+                if (y >= ylo && y < yhi) s_grad_item<I - 1>(ring[I - 1], a, k, y, j % (TW / 4));
+            }
+        } else {
+            if constexpr (I >= 2) {
+                const int j = it - nv - ng, y = Yd + j / (TW / 4);
+                if (y >= ylo && y < yhi) s_dog_item<I - 1>(ring[I - 1], ring[I - 2], a, k, y, j % (TW / 4));
+            }
+        }
+    }
+}
+
+// Phase B of stage I: horizontal pass, thread = (row pair p, columns 4c .. 4c + 3 of ring I); stage 5
+// writes the DoG L5 - L4 of the strip's columns instead of a ring
+template <int I>
+__device__ __forceinline__ void s_phase_b(float* const* ring, const float2* vb, const StripArgs& a, const StripCta& k,
+                                          int Y) {
+    constexpr int r = RAD(I), NC = TWID(I) / 4, off = TSD(I) + (TSD(I) & 1);
+    float2 w[r + 1];
+    load_taps<I, r>(w);
+    const int it = threadIdx.x;
+    if (it >= 4 * NC) return;
+    const int p = it / NC, c = 4 * (it - p * NC);
+    const float4* src = reinterpret_cast<const float4*>(vb + p * TVP + c + off);
+    float2 yv[4 + 2 * r];
+#pragma unroll
+    for (int j = 0; j < 2 + r; ++j) {
+        const float4 v = src[j];
+        yv[2 * j] = make_float2(v.x, v.y);
+        yv[2 * j + 1] = make_float2(v.z, v.w);
+    }
+    float2 o[4];
+#pragma unroll
+    for (int cc = 0; cc < 4; ++cc) o[cc] = blur_pairs_w<r>(yv + cc, w);
+    const float4 top = make_float4(o[0].x, o[1].x, o[2].x, o[3].x);
+    const float4 bot = make_float4(o[0].y, o[1].y, o[2].y, o[3].y);
+    const int y = Y + 2 * p;
+    if constexpr (I < 5) {
+        float* ri = ring[I];
+        *reinterpret_cast<float4*>(ri + s_slot<I>(y, k.RB) * TPITCH(I) + c) = top;
+        *reinterpret_cast<float4*>(ri + s_slot<I>(y + 1, k.RB) * TPITCH(I) + c) = bot;
+    } else {
+        const int x = k.x0 + c;
+        if (x >= a.C) return;
+        const int ylo = max(k.ya, 0), yhi = min(k.yz, a.R);
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            const int yy = y + h;
+            if (yy < ylo || yy >= yhi) continue;
+            const float* pr = ring[4] + s_slot<4>(yy, k.RB) * TPITCH(4) + TH(4) + c;
+            const float2 p0 = *reinterpret_cast<const float2*>(pr), p1 = *reinterpret_cast<const float2*>(pr + 2);
+            const float4 l = h ? bot : top;
+            const float2 d0 = __fadd2_rn(make_float2(l.x, l.y), make_float2(-p0.x, -p0.y));
+            const float2 d1 = __fadd2_rn(make_float2(l.z, l.w), make_float2(-p1.x, -p1.y));
+            s_store4(a.dog[4] + (size_t)yy * a.C + x, make_float4(d0.x, d0.y, d1.x, d1.y), k.vec, a.C - x);
+        }
+    }
+}
+
+template <int I>
+__device__ __forceinline__ void s_stage(float* const* ring, float2* vb, const StripArgs& a, const StripCta& k, int Y1) {
+    const int Y = Y1 - TLAG(I);
+    const bool act = Y + TSTEP > k.ya - TE(I) && Y < k.yz + TE(I);
+    s_phase_a<I>(ring, vb, a, k, Y, act);
+    __syncthreads();
+    if (act) s_phase_b<I>(ring, vb, a, k, Y);
+    __syncthreads();
+}
+
+__global__ void __launch_bounds__(TNT, 2) k_strip(const __grid_constant__ CUtensorMap tmap, StripArgs a, int use_tma) {
+    extern __shared__ __align__(1024) float sm_strip[];
+    float* sm = sm_strip;
+    float* ring[5] = {sm + toff(0), sm + toff(1), sm + toff(2), sm + toff(3), sm + toff(4)};
+    float2* vb = reinterpret_cast<float2*>(sm + TVB_OFF);
+    uint64_t* bar = reinterpret_cast<uint64_t*>(sm + TBAR_OFF);
+    if (use_tma && (s_addr(sm) & 127) != 0) {   // TMA destinations must be 128-byte aligned
+        if (threadIdx.x == 0) atomicExch(a.err, 2);
+        return;
+    }
+    StripCta k;
+    k.x0 = blockIdx.x * TW;
+    k.ya = blockIdx.y * a.rows;
+    k.yz = min(a.R, k.ya + a.rows);
+    const int V0 = k.ya - TE(0);   // first L0 row held
+    k.RB = V0 - 64;                // every row read is above RB
+    k.vec = (a.C & 3) == 0;
+    for (int i = 0; i < 5; ++i) k.vec = k.vec && al16(a.dog[i]);
+    for (int i = 0; i < 3; ++i) k.vec = k.vec && al16(a.mag[i]) && al16(a.ang[i]);
+    const bool tma = use_tma != 0;
+    const int T = (k.yz - k.ya + TE(0) + TLAG(5) - 3 + TSTEP - 1) / TSTEP;   // steps
+    if (tma && threadIdx.x == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(s_addr(bar)) : "memory");
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(s_addr(bar + 1)) : "memory");
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
+    s_load_block(&tmap, a, ring[0], bar, k.x0, V0, k.RB, tma);
+    s_load_block(&tmap, a, ring[0], bar + 1, k.x0, V0 + TSTEP, k.RB, tma);
+    for (int t = 0; t < T; ++t) {
+        // blocks t and t + 1 (rows V0 + 8t .. V0 + 8t + 15) must be in ring 0
+        if (tma) {
+            bool ok = true;
+            for (int b = (t == 0 ? 0 : t + 1); b <= t + 1; ++b) {
+                ok = ok && s_mbar_wait(bar + (b & 1), (b >> 1) & 1);
+                if (ok) s_fix_edges(a, ring[0], k.x0, V0 + TSTEP * b, k.RB);
+            }
+            if (__syncthreads_or(!ok)) {
+                if (threadIdx.x == 0) atomicExch(a.err, 1);
+                return;
+            }
+        } else {
+            cp_wait_all();
+            __syncthreads();
+        }
+        // the rows of block t + 2 take the slots of rows no stage reads in this step
+        if (t + 2 <= T) {
+            if (tma && threadIdx.x == 0) asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+            s_load_block(&tmap, a, ring[0], bar + (t & 1), k.x0, V0 + TSTEP * (t + 2), k.RB, tma);
+        }
+        const int Y1 = V0 + TSTEP * t + 3;
+        s_stage<1>(ring, vb, a, k, Y1);
+        s_stage<2>(ring, vb, a, k, Y1);
+        s_stage<3>(ring, vb, a, k, Y1);
+        s_stage<4>(ring, vb, a, k, Y1);
+        s_stage<5>(ring, vb, a, k, Y1);
+    }
+    // every issued TMA block (0 .. T) was waited for inside the loop
+    if (!tma) cp_wait_all();
+}
+
+// cuTensorMapEncodeTiled through the runtime's driver entry point (no link against libcuda)
+typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                  const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                  CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+EncodeTiledFn encode_tiled() {
+    static EncodeTiledFn fn = [] {
+        void* f = nullptr;
+        cudaDriverEntryPointQueryResult q{};
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &f, cudaEnableDefault, &q) != cudaSuccess ||
+            q != cudaDriverEntryPointSuccess)
+            f = nullptr;
+        return reinterpret_cast<EncodeTiledFn>(f);
+    }();
+    return fn;
+}
+
 }  // namespace
+
+// One float32 octave by the strip engine (one launch): from the base L0 (R x C, pitch C), the five
+// DoG planes at dog + k RC, gradients of L1..L3 at mag / ang + k RC, L3[::2, ::2] to down (pitch
+// down_cols; null for the last octave). err (device) is set when a TMA wait gives up.
+int32_t launch_octave_strip(const float* L0, int R, int C, float* dog, float* mag, float* ang, float* down,
+                            int down_cols, int* err, cudaStream_t s) {
+    static std::atomic<int> attr[64];
+    FSB_TRY(smem_attr((const void*)k_strip, TSMEM, attr));
+    StripArgs a{};
+    a.L0 = L0;
+    a.R = R;
+    a.C = C;
+    const long long RC = (long long)R * C;
+    for (int i = 0; i < 5; ++i) a.dog[i] = dog + i * RC;
+    for (int i = 0; i < 3; ++i) {
+        a.mag[i] = mag + i * RC;
+        a.ang[i] = ang + i * RC;
+    }
+    a.down = down;
+    a.down_cols = down_cols;
+    a.err = err;
+    // TMA row copies need a 16-byte row pitch and base; the box is the 216-column L0 window
+    CUtensorMap tm;
+    std::memset(&tm, 0, sizeof(tm));
+    int use_tma = 0;
+    EncodeTiledFn enc = encode_tiled();
+    if (enc && (C & 3) == 0 && C >= TWID(0) && (reinterpret_cast<uintptr_t>(L0) & 15) == 0) {
+        const cuuint64_t dims[2] = {(cuuint64_t)C, (cuuint64_t)R};
+        const cuuint64_t strides[1] = {(cuuint64_t)C * 4};
+        const cuuint32_t box[2] = {(cuuint32_t)TWID(0), 1};
+        const cuuint32_t es[2] = {1, 1};
+        use_tma = enc(&tm, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, const_cast<float*>(L0), dims, strides, box, es,
+                      CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                      CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+    }
+    // about two CTAs per SM: strips x row chunks, chunk heights a multiple of the step
+    const int strips = (C + TW - 1) / TW;
+    int chunks = (2 * sm_count() + strips / 2) / strips;
+    if (chunks < 1) chunks = 1;
+    int rows = (R + chunks - 1) / chunks;
+    rows = (rows + TSTEP - 1) / TSTEP * TSTEP;
+    a.rows = rows;
+    dim3 grid(strips, (R + rows - 1) / rows);
+    k_strip<<<grid, TNT, TSMEM, s>>>(tm, a, use_tma);
+    note_launch();
+    FSB_CUDA(cudaGetLastError());
+    return FSB_OK;
+}
 
 int32_t launch_octave_fused(const float* L0, int R, int C, float* dog, float* mag, float* ang, float* down,
                             int down_cols, cudaStream_t s) {

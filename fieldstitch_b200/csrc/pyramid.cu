@@ -249,11 +249,12 @@ int32_t tuned_layer(int layer, const float* src, int R, int C, float* dst, float
 // per octave size between the per-layer kernels (variant 0, also with FSB_AUTOTUNE=0) and the
 // fused layer groups (variant 1); "layer" / "group" force one; "fused" takes the streaming
 // kernel for octaves at least kFusedMinCols wide. Read on every call.
-enum class Engine { Auto, Group, Layer, Fused };
+enum class Engine { Auto, Group, Layer, Fused, Strip };
 static Engine pyramid_engine() {
     const char* e = std::getenv("FSB_PYRAMID");
     if (e && std::strcmp(e, "layer") == 0) return Engine::Layer;
     if (e && std::strcmp(e, "group") == 0) return Engine::Group;
+    if (e && std::strcmp(e, "strip") == 0) return Engine::Strip;
     if (e && std::strcmp(e, "fused") == 0) return Engine::Fused;
     return Engine::Auto;
 }
@@ -272,6 +273,7 @@ struct OctaveCall {
     // since the next octave needs only L3's downsample; `join` marks its end
     cudaStream_t side;
     cudaEvent_t fork, join;
+    int* err;   // error word of the strip engine's bounded waits
 };
 int32_t run_octave_call(void* p, int v) {
     const OctaveCall* c = static_cast<const OctaveCall*>(p);
@@ -284,6 +286,12 @@ int32_t run_octave_call(void* p, int v) {
         ts = c->side;
         return FSB_OK;
     };
+    if (v == 2) {
+        // the whole octave in one launch: no tail to move to the side stream
+        FSB_TRY(launch_octave_strip(c->src, c->R, c->C, c->dog, c->mag, c->ang, c->down, c->dc, c->err, c->s));
+        if (c->side) FSB_CUDA(cudaEventRecord(c->join, c->s));
+        return FSB_OK;
+    }
     if (v == 1) {
         FSB_TRY(launch_group_lower(c->src, c->R, c->C, c->dog, c->mag, c->ang, c->x, c->down, c->dc, c->s));
         FSB_TRY(fork());
@@ -306,6 +314,8 @@ int32_t run_pyramid(Workspace& ws, const uint8_t* d_img, int img_stride, bool ex
                     cudaEvent_t* ev) {
     const Geometry& g = ws.g;
     float* P[3] = {ws.plane[0].as<float>(), ws.plane[1].as<float>(), ws.plane[2].as<float>()};
+    int* err = ws.counters.as<int>() + PYR_ERR_WORD;
+    FSB_CUDA(cudaMemsetAsync(err, 0, sizeof(int), s));
     float* DF = ws.dog.as<float>();
     float* MAG = ws.mag.as<float>();
     float* ANG = ws.ang.as<float>();
@@ -355,14 +365,14 @@ int32_t run_pyramid(Workspace& ws, const uint8_t* d_img, int img_stride, bool ex
                 if (P[k] != cur && P[k] != busy) pl[n++] = P[k];
             OctaveCall c{cur, g.R[o], g.C[o], pl[0], pl[1], DF + g.dog_off[o], MAG + g.grad_off[o],
                          ANG + g.grad_off[o], last ? nullptr : NB + (o & 1) * half, last ? 0 : g.C[o + 1], s,
-                         nullptr, side ? ev[2 * o] : nullptr, side ? ev[2 * o + 1] : nullptr};
-            int v = eng == Engine::Group ? 1 : 0;
+                         nullptr, side ? ev[2 * o] : nullptr, side ? ev[2 * o + 1] : nullptr, err};
+            int v = eng == Engine::Group ? 1 : eng == Engine::Strip ? 2 : 0;
             char key[64];
-            std::snprintf(key, sizeof(key), "k_octave_%dx%d", g.R[o], g.C[o]);
-            const bool known = eng != Engine::Auto || autotune_cached(key, 2, &v);
-            if (known && side) c.side = side;
+            std::snprintf(key, sizeof(key), "k_octave3_%dx%d", g.R[o], g.C[o]);
+            const bool known = eng != Engine::Auto || autotune_cached(key, 3, &v);
+            if (known && side && v != 2) c.side = side;
             if (eng == Engine::Auto && !known) {
-                FSB_TRY(autotune(key, 2, run_octave_call, &c, s, &v));
+                FSB_TRY(autotune(key, 3, run_octave_call, &c, s, &v));
             } else {
                 FSB_TRY(run_octave_call(&c, v));
             }

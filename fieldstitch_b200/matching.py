@@ -276,6 +276,41 @@ def find_homography_batch(problems, thr, iters=1024, seed=0, device=0):
     return out
 
 
+def find_fundamental_batch(problems, thr, iters=2048, seed=0, device=0):
+    """Fundamental matrices of many pairs in one launch (matching._verify's
+    cv2.findFundamentalMat(pi, pj, USAC_MAGSAC, thr, 0.999, 10000), app/planesite/matching.py:175-191,
+    batched): seven-point samples, inliers by both point-to-epipolar-line distances <= thr, eight-point
+    least-squares refinement. problems: list of (pi (n,2), pj (n,2)). Returns a list of (F (3,3)
+    float64 or None, mask (n,1) uint8) per pair, as OpenCV returns them; None where a pair has fewer
+    than 8 correspondences or no candidate with 8 inliers."""
+    src = [np.asarray(s, np.float64).reshape(-1, 2) for s, _ in problems]
+    dst = [np.asarray(d, np.float64).reshape(-1, 2) for _, d in problems]
+    if any(len(a) != len(b) for a, b in zip(src, dst)):
+        raise ValueError("src and dst differ in length")
+    off = np.ascontiguousarray(np.r_[0, np.cumsum([len(a) for a in src])].astype(np.int64))
+    S = np.ascontiguousarray(np.concatenate(src) if src else np.zeros((0, 2)))
+    D = np.ascontiguousarray(np.concatenate(dst) if dst else np.zeros((0, 2)))
+    P = len(problems)
+    F = np.zeros((max(P, 1), 9))
+    mask = np.zeros(max(len(S), 1), np.uint8)
+    n_in = np.zeros(max(P, 1), np.int32)
+    if P:
+        ctx = _lib.context(device)
+        _lib.check(ctx.lib.fsb_find_fundamental_batch(ctx.handle, P, _lib.ptr(off), _lib.ptr(S), _lib.ptr(D),
+                                                      float(thr), int(iters), int(seed) & (2 ** 64 - 1), _lib.ptr(F),
+                                                      _lib.ptr(mask), _lib.ptr(n_in)), "fsb_find_fundamental_batch")
+    out = []
+    for p in range(P):
+        m = mask[off[p]:off[p + 1]].reshape(-1, 1).copy()
+        out.append((None if not F[p].any() else F[p].reshape(3, 3).copy(), m))
+    return out
+
+
+def find_fundamental(pi, pj, thr, iters=2048, seed=0, device=0):
+    """One pair of find_fundamental_batch: (F or None, mask)."""
+    return find_fundamental_batch([(pi, pj)], thr, iters, seed, device)[0]
+
+
 def find_homography(src, dst, thr, iters=1024, seed=0, device=0):
     """One pair of find_homography_batch: (H or None, mask)."""
     return find_homography_batch([(src, dst)], thr, iters, seed, device)[0]
@@ -358,11 +393,18 @@ def _prior_filter(q, t, ui, uj, i, j, tol, device=0):
     return q[keep], t[keep]
 
 
-def _verify(c, i, j, ui, uj, q, t):
+def _verify(c, i, j, ui, uj, q, t, device=0):
     """matching._verify (app/planesite/matching.py:175-191): fundamental-matrix inliers (OpenCV
-    USAC_MAGSAC, plain RANSAC where MAGSAC rejects a degenerate set)."""
+    USAC_MAGSAC, plain RANSAC where MAGSAC rejects a degenerate set); with the context's
+    ransac="device", the device's batched fundamental RANSAC (statistically equal, not identical)."""
     pi, pj = ui[q].astype(np.float32), uj[t].astype(np.float32)
     F = mask = None
+    if c.get("ransac", "opencv") == "device":
+        F, mask = find_fundamental(pi.astype(np.float64), pj.astype(np.float64), c["ransac_thr"], device=device)
+        if F is None or mask is None:
+            return None, None, 0
+        inl = mask.ravel().astype(bool)
+        return q[inl], t[inl], int(inl.sum())
     for method in (getattr(cv2, "USAC_MAGSAC", cv2.FM_RANSAC), cv2.FM_RANSAC):
         try:
             F, mask = cv2.findFundamentalMat(pi, pj, method, c["ransac_thr"], 0.999, 10000)
@@ -418,7 +460,7 @@ def _coarse_guided(c, i, j, A, B, use_prior, tol, device):
     q, t = _guided(A, B, Hm, radius, c.get("guided_k", 24), 0.85, device)
     if len(q) < c["min_inliers"]:
         return None
-    q, t, n_in = _verify(c, i, j, ui, uj, q, t)
+    q, t, n_in = _verify(c, i, j, ui, uj, q, t, device)
     if q is None or n_in < max(c["min_inliers"], 40):
         return None
     return q, t, n_in
@@ -429,7 +471,8 @@ def match_pair(task, device=0):
     (i, j, q int32, t int32, similarity, n_inliers), or (i, j, None, None, None or an error tuple,
     n) as the reference does. Descriptor matching (coarse exhaustive, guided, fallback) and the
     camera geometry run on the device; RANSAC and the fundamental / similarity fits are OpenCV's,
-    as in the reference."""
+    as in the reference, unless the context sets ransac="device" (the stage-1 homography and the
+    fundamental verification then run on the device)."""
     i, j = task
     c = _CTX
     try:
@@ -447,7 +490,7 @@ def match_pair(task, device=0):
                 q, t = _prior_filter(q, t, ui, uj, i, j, tol, device)
             if len(q) < 20:
                 return i, j, None, None, None, 0
-            q, t, n_in = _verify(c, i, j, ui, uj, q, t)
+            q, t, n_in = _verify(c, i, j, ui, uj, q, t, device)
             if q is None or n_in < c["min_inliers"]:
                 return i, j, None, None, None, n_in
             result = (q, t, n_in)

@@ -162,3 +162,128 @@ def synth_descriptors_device(na, nb, seed, device=0, true_frac=0.3, noise=4):
         truth = torch.full((nb,), -1, dtype=torch.int64, device=dev)
         truth[rows_b] = rows_a
     return a.contiguous(), b.contiguous(), truth
+
+
+# --------------------------------------------------------------------------- synthetic flight
+# One seeded procedural terrain texture, nadir frames cropped from it along a lawnmower grid, the
+# true frame-to-frame homographies and the GNSS neighbour pair list of the reference's pipeline.
+
+def flight_terrain(seed, h=16000, w=20000, device=0):
+    """uint8 (h, w) CUDA tensor: the terrain texture of the synthetic flight, drawn on the GPU with
+    torch: Gaussian blobs at three scales (impulses convolved in the frequency domain, sigma 4, 14
+    and 40 px) plus 1/f band-limited noise, rescaled so that the 0.5 and 99.5 percentiles map to 0
+    and 255."""
+    import torch
+    dev = torch.device("cuda", device)
+    g = torch.Generator(device=dev).manual_seed(int(seed))
+    fy = torch.fft.fftfreq(h, device=dev)[:, None]
+    fx = torch.fft.rfftfreq(w, device=dev)[None, :]
+    f2 = fx * fx + fy * fy
+    # 1/f noise in the band [1/1024, 0.45] cycles per pixel
+    spec = torch.fft.rfft2(torch.randn((h, w), generator=g, device=dev))
+    f = torch.sqrt(f2)
+    spec *= torch.where((f >= 1.0 / 1024) & (f <= 0.45), 1.0 / torch.clamp(f, min=1.0 / 1024), torch.zeros_like(f))
+    noise = torch.fft.irfft2(spec, s=(h, w))
+    del spec
+    noise /= noise.std().clamp_min(1e-6)
+    # blobs: about one per 13 000 px at each scale, signed amplitudes
+    blobs = torch.zeros((h, w), device=dev)
+    for sigma in (4.0, 14.0, 40.0):
+        n = int(h * w / 13000)
+        imp = torch.zeros((h, w), device=dev)
+        ys = torch.randint(0, h, (n,), generator=g, device=dev)
+        xs = torch.randint(0, w, (n,), generator=g, device=dev)
+        amp = torch.rand((n,), generator=g, device=dev) * 2.0 - 1.0
+        imp.index_put_((ys, xs), amp, accumulate=True)
+        sp = torch.fft.rfft2(imp)
+        sp *= torch.exp(-2.0 * (torch.pi ** 2) * sigma * sigma * f2) * (2.0 * torch.pi * sigma * sigma)
+        blobs += torch.fft.irfft2(sp, s=(h, w))
+        del imp, sp
+    img = blobs / blobs.std().clamp_min(1e-6) + 0.6 * noise
+    del blobs, noise
+    lo, hi = torch.quantile(img[::8, ::8].reshape(-1)[:16_000_000], torch.tensor([0.005, 0.995], device=dev))
+    img = (img - lo) * (255.0 / float(max(hi - lo, 1e-6)))
+    return torch.clamp(torch.round(img), 0, 255).to(torch.uint8)
+
+
+def lawnmower(seed, lines=20, per_line=20, W=2640, H=1978, forward=0.8, side=0.7, margin=200.0,
+              yaw_deg=3.0, scale_jitter=0.02):
+    """Frame poses of a serpentine lawnmower flight over the terrain: (n, 4) float64 rows (cx, cy,
+    yaw in radians, scale) in terrain pixels, flight lines along the terrain's y axis (the frames'
+    short side along track) with the given forward / side overlap, the return lines flown with
+    the heading turned by 180 deg, each frame with uniform +-yaw_deg yaw and +-scale_jitter scale."""
+    rng = np.random.default_rng(seed)
+    step_y, step_x = (1.0 - forward) * H, (1.0 - side) * W
+    out = []
+    for l in range(lines):
+        ks = range(per_line) if l % 2 == 0 else range(per_line - 1, -1, -1)
+        for k in ks:
+            cx = margin + W / 2.0 + step_x * l
+            cy = margin + H / 2.0 + step_y * k
+            yaw = math.radians(rng.uniform(-yaw_deg, yaw_deg)) + (0.0 if l % 2 == 0 else math.pi)
+            out.append((cx, cy, yaw, 1.0 + rng.uniform(-scale_jitter, scale_jitter)))
+    return np.array(out, np.float64)
+
+
+def frame_to_terrain(pose, W=2640, H=1978):
+    """3x3 map of frame pixels to terrain pixels for pose (cx, cy, yaw, scale)."""
+    cx, cy, yaw, s = pose
+    c, si = math.cos(yaw) * s, math.sin(yaw) * s
+    return np.array([[c, -si, cx - c * (W - 1) / 2.0 + si * (H - 1) / 2.0],
+                     [si, c, cy - si * (W - 1) / 2.0 - c * (H - 1) / 2.0],
+                     [0.0, 0.0, 1.0]])
+
+
+def frame_homography(pose_i, pose_j, W=2640, H=1978):
+    """The true homography of frame i pixels to frame j pixels."""
+    return np.linalg.inv(frame_to_terrain(pose_j, W, H)) @ frame_to_terrain(pose_i, W, H)
+
+
+def render_frames(terrain, poses, W=2640, H=1978, noise_sigma=2.0, seed=0):
+    """(n, H, W) uint8 CUDA tensor: each frame the terrain resampled (bilinear) at its pose, plus
+    Gaussian noise, rounded and clipped."""
+    import torch
+    dev = terrain.device
+    th, tw = terrain.shape
+    src = terrain.to(torch.float32)[None, None]
+    g = torch.Generator(device=dev).manual_seed(int(seed) + 17)
+    v, u = torch.meshgrid(torch.arange(H, device=dev, dtype=torch.float64),
+                          torch.arange(W, device=dev, dtype=torch.float64), indexing="ij")
+    out = torch.empty((len(poses), H, W), dtype=torch.uint8, device=dev)
+    for k, pose in enumerate(poses):
+        M = torch.tensor(frame_to_terrain(pose, W, H), device=dev)
+        x = M[0, 0] * u + M[0, 1] * v + M[0, 2]
+        y = M[1, 0] * u + M[1, 1] * v + M[1, 2]
+        # align_corners=True: -1 and 1 are the centres of the first and last terrain pixels
+        grid = torch.stack((x / (tw - 1) * 2 - 1, y / (th - 1) * 2 - 1), -1).to(torch.float32)[None]
+        fr = torch.nn.functional.grid_sample(src, grid, mode="bilinear", padding_mode="border", align_corners=True)[0, 0]
+        fr += noise_sigma * torch.randn(fr.shape, generator=g, device=dev)
+        out[k] = torch.clamp(torch.round(fr), 0, 255).to(torch.uint8)
+    return out
+
+
+def gnss_pairs(centers, W=2640, H=1978, neighbors=16, sigma=0.0, seed=0):
+    """Candidate pairs of the reference's pipeline (app/planesite/pipeline.py:452-476) from frame
+    positions (GNSS, here the frame centres plus N(0, sigma) noise, in terrain pixels at unit
+    scale): the `neighbors` nearest frames within 2 x 0.95 x half the long footprint side, plus the
+    next two frames in flight order when within twice that half side. Sorted (i < j) list."""
+    from scipy.spatial import cKDTree
+    xy = np.asarray(centers, np.float64)[:, :2]
+    if sigma > 0:
+        xy = xy + np.random.default_rng(seed).normal(0.0, sigma, xy.shape)
+    n = len(xy)
+    tree = cKDTree(xy)
+    k = min(n - 1, neighbors)
+    dists, nbrs = tree.query(xy, k=k + 1)
+    half_long = max(W, H) / 2.0
+    pairs = set()
+    for i in range(n):
+        for d, j in zip(dists[i][1:], nbrs[i][1:]):
+            if j < n and d < 2 * half_long * 0.95:
+                pairs.add((min(i, int(j)), max(i, int(j))))
+    for i in range(n - 1):
+        for off in (1, 2):
+            j = i + off
+            if j < n and np.hypot(*(xy[i] - xy[j])) < 2 * half_long:
+                pairs.add((i, j))
+    return sorted(pairs)

@@ -307,6 +307,19 @@ int32_t fsb_build_tracks(fsb_ctx* ctx, const int64_t* u, const int64_t* v, int64
 int32_t fsb_find_homography_batch(fsb_ctx* ctx, int32_t n_pairs, const int64_t* offsets, const double* src,
                                   const double* dst, double thr, int32_t iters, uint64_t seed, double* H, uint8_t* mask,
                                   int32_t* n_inliers);
+/* The fundamental-matrix verification of matching.match_pair (matching._verify,
+   app/planesite/matching.py:175-191, cv2.findFundamentalMat(pi, pj, USAC_MAGSAC, thr, 0.999,
+   10000)) for n_pairs pairs in one launch: pair p's correspondences are src (image i) / dst
+   (image j) rows offsets[p] .. offsets[p+1] - 1 (float64 (x, y)); `iters` seven-point samples per
+   pair (seeded, deterministic); inliers: both squared distances to the epipolar lines <= thr^2;
+   the best candidate refined by eight-point least squares over its inliers. F (9 per pair,
+   row-major, x_j^T F x_i = 0, F33 = 1 or unit norm; zeros when a pair has fewer than 8
+   correspondences or no candidate with 8 inliers), mask (one byte per correspondence) and
+   n_inliers. Random samples and the consensus rule differ from MAGSAC's: results agree
+   statistically. */
+int32_t fsb_find_fundamental_batch(fsb_ctx* ctx, int32_t n_pairs, const int64_t* offsets, const double* src,
+                                   const double* dst, double thr, int32_t iters, uint64_t seed, double* F,
+                                   uint8_t* mask, int32_t* n_inliers);
 /* features.decode / prepare (app/planesite/features.py:18-71) on the device: the luma plane of a
    JPEG held in host memory (data, len bytes), read at full size (reduce 1) or reduced by 2, 4, 8
    (block means; OpenCV's reduced reads scale inside the inverse DCT, so those agree with OpenCV

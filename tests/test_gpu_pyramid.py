@@ -98,12 +98,16 @@ def test_autotuned_tile_heights_are_bit_identical(monkeypatch):
     assert all(v in (0, 1, 2) for v in table.values())
 
 
-@pytest.mark.parametrize("hw", [(37, 53), (240, 320), (495, 661), (610, 830), (989, 1320), (1978, 2640)])
-def test_group_engine_bit_identical_to_per_layer(monkeypatch, hw):
+@pytest.mark.parametrize("engine", ["group", "strip"])
+@pytest.mark.parametrize("hw", [(37, 53), (240, 320), (495, 661), (610, 830), (989, 1320), (1978, 2640),
+                                (1001, 1111)])
+def test_octave_engine_bit_identical_to_per_layer(monkeypatch, hw, engine):
     """The fused layer-group kernels (L1..L3 and L4, L5 per launch, halos recomputed in shared
-    memory) give the per-layer kernels' DoG, magnitude and angle atlases bit for bit, including
-    odd and tiny octaves whose halos reflect more than once and (610 x 830) octaves whose atlas
-    planes start off a 16-byte boundary, and the same keypoints."""
+    memory) and the strip engine (the whole octave in one launch, layers in shared-memory row
+    rings, L0 rows by TMA where the row pitch allows) give the per-layer kernels' DoG, magnitude
+    and angle atlases bit for bit, including odd and tiny octaves whose halos reflect more than
+    once, (610 x 830) octaves whose atlas planes start off a 16-byte boundary and (1001 x 1111)
+    octave widths that are not a multiple of four, and the same keypoints."""
     import fieldstitch_b200 as f
     from fieldstitch_b200 import synth
     h, w = hw
@@ -111,7 +115,7 @@ def test_group_engine_bit_identical_to_per_layer(monkeypatch, hw):
     monkeypatch.setenv("FSB_PYRAMID", "layer")
     k0, st0 = f.gsift.detect(img)
     ref = st0.atlas()
-    monkeypatch.setenv("FSB_PYRAMID", "group")
+    monkeypatch.setenv("FSB_PYRAMID", engine)
     k1, st1 = f.gsift.detect(img)
     got = st1.atlas()
     assert got[0] == ref[0] and len(ref[0]) >= 3
@@ -123,8 +127,8 @@ def test_group_engine_bit_identical_to_per_layer(monkeypatch, hw):
 
 
 def test_autotuned_octave_engines_are_bit_identical(monkeypatch):
-    """With no engine forced, the autotuner times the per-layer kernels and the fused layer groups
-    per octave size and keeps the faster; the atlases (first call, tuning; second call, cached
+    """With no engine forced, the autotuner times the per-layer kernels, the fused layer groups and
+    the strip engine per octave size and keeps the fastest; the atlases (first call, tuning; second call, cached
     choices) equal the untuned per-layer ones bit for bit, and each octave size has a choice."""
     import fieldstitch_b200 as f
     from fieldstitch_b200 import _lib, synth
@@ -143,4 +147,4 @@ def test_autotuned_octave_engines_are_bit_identical(monkeypatch):
                 np.testing.assert_array_equal(got[k][o], ref[k][o])
     table = _lib.autotune_table()
     for r, c in ref[0]:
-        assert any(k.endswith("k_octave_%dx%d" % (r, c)) for k in table), (r, c, table)
+        assert any(k.endswith("k_octave3_%dx%d" % (r, c)) for k in table), (r, c, table)
