@@ -58,6 +58,10 @@ def parse():
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-cpu", action="store_true")
     p.add_argument("--streams", type=int, default=6, help="host threads, each with its own context/stream")
+    p.add_argument("--extract", default="graph", choices=["graph", "threads"],
+                   help="graph: every image of a step in one sync-free batch (one CUDA graph); threads: "
+                        "fsb_sift_features_d per image on --streams host threads")
+    p.add_argument("--chains", type=int, default=8, help="images in flight inside the extraction graph")
     p.add_argument("--sweep-pairs", type=int, default=256, help="dense precision sweep: pairs per batch (0: skip)")
     p.add_argument("--sweep-n", type=int, default=16384, help="dense precision sweep: descriptors per image")
     p.add_argument("--plain-pairs", type=int, default=16,
@@ -805,9 +809,38 @@ def run_fsb(args):
             Pv(*[b["t"].data_ptr() for b in pb]), m_cnt), "guided batch")
         return sum(m_cnt[i] for i in range(NPs))
 
+    # the step's extraction as one sync-free batch: every image in one fsb_sift_features_batch_d call
+    # (one CUDA graph, args.chains images in flight), then every pair's prior projections queued
+    # with one call on the match context
+    ectx = _lib.Context(local)
+    estream = torch.cuda.ExternalStream(ectx.stream())
+    NI = 2 * NPs
+    Pi, Ii = ctypes.c_void_p * NI, ctypes.c_int32 * NI
+    e_imgs = Pi(*[d_img[i][k].data_ptr() for i in range(NPs) for k in range(2)])
+    e_nf = Ii(*[pairs[i][3 + k] for i in range(NPs) for k in range(2)])
+    e_xy = Pi(*[pb[i]["xy"][k].data_ptr() for i in range(NPs) for k in range(2)])
+    e_rs = Pi(*[pb[i]["rs"][k].data_ptr() for i in range(NPs) for k in range(2)])
+    e_u8 = Pi(*[pb[i]["u8"][k].data_ptr() for i in range(NPs) for k in range(2)])
+    e_dcnt = torch.empty(NI, dtype=torch.int32, device=dev)
+    e_hcnt = Ii()
+    p_hm = np.ascontiguousarray(np.concatenate([np.concatenate([Hs[i], eye]) for i in range(NPs)]))
+    p_off = Pi(*[v for i in range(NPs) for v in (d_noise[i].data_ptr(), None)])
+    p_out = Pi(*[v for i in range(NPs) for v in (pb[i]["pred"].data_ptr(), pb[i]["bxy"].data_ptr())])
+
+    def extract_graph():
+        _lib.check(ectx.lib.fsb_sift_features_batch_d(ectx.handle, NI, e_imgs, h, w, w, ctypes.byref(prm), e_nf, e_xy,
+                                                      e_rs, e_u8, ctypes.c_void_p(e_dcnt.data_ptr()), e_hcnt,
+                                                      args.chains), "sift batch")
+        for i in range(NPs):
+            pb[i]["n"] = [e_hcnt[2 * i], e_hcnt[2 * i + 1]]
+        _lib.check(mctx.lib.fsb_project_batch_d(mctx.handle, NI, e_xy, e_hcnt, _lib.ptr(p_hm), p_off, p_out), "proj")
+
     def one_step():
-        for f in [pool.submit(wk.extract) for wk in workers]:
-            f.result()
+        if args.extract == "graph":
+            extract_graph()
+        else:
+            for f in [pool.submit(wk.extract) for wk in workers]:
+                f.result()
         return match_batch()
 
     def barrier():
@@ -825,10 +858,11 @@ def run_fsb(args):
         for wk in workers:
             wk.stream.wait_event(e0)
         mstream.wait_event(e0)
+        estream.wait_event(e0)
         out = 0
         for _ in range(steps):
             out += fn()
-        for st in [wk.stream for wk in workers] + [mstream]:
+        for st in [wk.stream for wk in workers] + [mstream, estream]:
             ev = torch.cuda.Event()
             ev.record(st)
             main.wait_event(ev)
@@ -840,7 +874,7 @@ def run_fsb(args):
         one_step()
     torch.cuda.synchronize()
     barrier()
-    for c_ in [wk.ctx for wk in workers] + [mctx]:
+    for c_ in [wk.ctx for wk in workers] + [mctx, ectx]:
         c_.timing(True)
         c_.stage_times()
     clocks = Clocks(gpu_smi_id(torch, local))
@@ -849,7 +883,7 @@ def run_fsb(args):
     clk = clocks.stop()
     launches = _lib.launch_count() - launches0
     stages = {}
-    for c_ in [wk.ctx for wk in workers] + [mctx]:
+    for c_ in [wk.ctx for wk in workers] + [mctx, ectx]:
         for k_, (ms_, n_) in c_.stage_times().items():
             a_, b_ = stages.get(k_, (0.0, 0))
             stages[k_] = (a_ + ms_, b_ + n_)
@@ -912,9 +946,28 @@ def run_fsb(args):
             d2h = (len(xa) + len(xb)) * (8 + 4 + 128) + 16 * len(q) + 16
             return h2d, d2h
 
-        def e2e_step():
+        def e2e_step_threads():
             res = list(pool.map(e2e_pair, range(len(pairs))))
             return sum(r[0] for r in res), sum(r[1] for r in res)
+
+        def e2e_step_batch():
+            """features.sift_gpu_u8_batch (every image of the step: one upload, one graph, one download)
+            then matching.match_guided_batch (every pair: one upload, one graph call, one download)."""
+            imgs = [im for a, b in host for im in (a, b)]
+            nfs = [pairs[i][3 + k] for i in range(len(pairs)) for k in range(2)]
+            feats = F.features.sift_gpu_u8_batch(imgs, nfs, chains=args.chains, device=local)
+            probs, h2d, d2h = [], sum(im.nbytes for im in imgs), 0
+            for i in range(len(pairs)):
+                (xa, ua, ra), (xb, ub, rb) = feats[2 * i], feats[2 * i + 1]
+                pr = synth.apply_homography(pairs[i][2], xa) + noise[i][:len(xa)]
+                probs.append((pr, ua, xb.astype(np.float64), ub, (w, h)))
+                d2h += (len(xa) + len(xb)) * (8 + 4 + 128)
+                h2d += pr.nbytes + ua.nbytes + 16 * len(xb) + ub.nbytes
+            res = F.matching.match_guided_batch(probs, RADIUS, KC, RATIO, device=local)
+            d2h += sum(16 * len(q) for q, _ in res)
+            return h2d, d2h
+
+        e2e_step = e2e_step_batch if args.extract == "graph" else e2e_step_threads
 
         e2e_step()
         torch.cuda.synchronize()
@@ -937,7 +990,9 @@ def run_fsb(args):
         ms_e2e = max_over_ranks(ms_e2e, dist, dev)
         e2e = {"value": job_rate(world, args.pairs, ms_e2e), "unit": "pairs/s", "h2d_bytes_per_step": int(h2d),
                "d2h_bytes_per_step": int(d2h), "ms_per_step": ms_e2e, "steps": ksteps,
-               "api": "features.sift_gpu_u8 + matching.guided_from_pred, %d host threads" % args.streams,
+               "api": ("features.sift_gpu_u8_batch (one graph for every image) + matching.match_guided_batch "
+                       "(one graph for every pair)" if args.extract == "graph" else
+                       "features.sift_gpu_u8 + matching.guided_from_pred, %d host threads" % args.streams),
                "host_inputs": "images in pinned host memory; keypoints / descriptors between the two calls in "
                               "the numpy arrays the API returns"}
 
@@ -1015,7 +1070,11 @@ def run_fsb(args):
         line = {"metric": METRIC, "value": value, "unit": "pairs/s", "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
                 "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded)",
-                "config": config(args, {"host_streams": args.streams,
+                "config": config(args, {"host_streams": args.streams, "extraction": (
+                                            "every image of a step in one fsb_sift_features_batch_d call (one CUDA "
+                                            "graph, %d images in flight, no host wait inside)" % args.chains
+                                            if args.extract == "graph" else
+                                            "fsb_sift_features_d per image on %d host threads" % args.streams),
                                         "matching": "every pair of a step in one fsb_match_guided_batch_d call "
                                                     "(one CUDA graph, captured once, replayed each step)"}),
                 "clocks": clk, "e2e": e2e, "gpu_launches": int(launches), "roofline": roof, "cpu_baseline": cpu,
@@ -1029,6 +1088,7 @@ def run_fsb(args):
     for wk in workers:
         wk.ctx.close()
     mctx.close()
+    ectx.close()
     if dist is not None:
         barrier()
         dist.destroy_process_group()

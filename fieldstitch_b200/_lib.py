@@ -51,6 +51,8 @@ SIGNATURES = [
     ("fsb_build_tracks", c_i32, [c_vp, c_vp, c_vp, c_i64, c_vp, c_i32, c_vp, c_vp, c_vp, c_vp, c_vp]),
     ("fsb_find_homography_batch", c_i32, [c_vp, c_i32, c_vp, c_vp, c_vp, ctypes.c_double, c_i32, ctypes.c_uint64,
                                           c_vp, c_vp, c_vp]),
+    ("fsb_sift_features_batch_d", c_i32, [c_vp, c_i32, c_vp, c_i32, c_i32, c_i32, c_vp, c_vp, c_vp, c_vp, c_vp,
+                                          c_vp, c_vp, c_i32]),
     ("fsb_find_fundamental_batch", c_i32, [c_vp, c_i32, c_vp, c_vp, c_vp, ctypes.c_double, c_i32, ctypes.c_uint64,
                                            c_vp, c_vp, c_vp]),
     ("fsb_spread", c_i32, [c_vp, c_vp, c_vp, c_vp, c_i32, c_i32, c_i32, c_i32, c_i32, c_vp, c_vp]),
@@ -65,6 +67,7 @@ SIGNATURES = [
     ("fsb_stage_times", c_i32, [c_vp, c_vp, c_vp, c_i32]),
     ("fsb_sift_features_d", c_i32, [c_vp, c_vp, c_i32, c_i32, c_i32, c_vp, c_i32, c_vp, c_vp, c_vp, c_vp, c_vp]),
     ("fsb_project_d", c_i32, [c_vp, c_vp, c_i32, c_vp, c_vp, c_vp]),
+    ("fsb_project_batch_d", c_i32, [c_vp, c_i32, c_vp, c_vp, c_vp, c_vp, c_vp]),
     ("fsb_match_guided_d", c_i32, [c_vp, c_vp, c_vp, c_i32, c_vp, c_vp, c_i32, c_f64, c_f64, c_f64, c_i32, c_f32,
                                    c_vp, c_vp, c_vp]),
     ("fsb_match_bf_d", c_i32, [c_vp, c_vp, c_i32, c_vp, c_i32, c_f32, c_i32, c_vp, c_vp, c_vp]),

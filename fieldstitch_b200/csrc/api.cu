@@ -51,7 +51,8 @@ void DevBuf::release() {
 size_t Workspace::bytes() const {
     size_t t = dog.bytes + mag.bytes + ang.bytes + img.bytes + cand.bytes + refined.bytes + oriented.bytes +
                keys_a.bytes + keys_b.bytes + vals_a.bytes + vals_b.bytes + sort_tmp.bytes + counters.bytes +
-               kx.bytes + ky.bytes + ksize.bytes + kangle.bytes + kresp.bytes + koct.bytes + klayer.bytes;
+               kx.bytes + ky.bytes + ksize.bytes + kangle.bytes + kresp.bytes + koct.bytes + klayer.bytes +
+               spread.bytes + take.bytes;
     for (const auto& b : plane) t += b.bytes;
     return t + next_base.bytes;
 }
@@ -59,7 +60,7 @@ size_t Workspace::bytes() const {
 void Workspace::release() {
     DevBuf* all[] = {&dog, &mag, &ang, &img, &cand, &refined, &oriented, &keys_a, &keys_b, &vals_a, &vals_b,
                      &sort_tmp, &counters, &kx, &ky, &ksize, &kangle, &kresp, &koct, &klayer,
-                     &plane[0], &plane[1], &plane[2], &next_base};
+                     &plane[0], &plane[1], &plane[2], &next_base, &spread, &take};
     for (DevBuf* b : all) b->release();
 }
 
@@ -230,10 +231,13 @@ static int32_t detect_into(fsb_ctx* ctx, Workspace& ws, const uint8_t* img, int 
 }
 
 // selected keypoints -> describe inputs (tx..tly) and optional interleaved xy / response outputs
-__global__ void k_take(const int32_t* __restrict__ sel, int n, const float* x, const float* y, const float* sz,
-                       const float* an, const float* rs, const int32_t* oc, const int32_t* ly, float* ox, float* oy,
-                       float* osz, float* oan, float* ors, int32_t* ooc, int32_t* oly, float* oxy, float* oresp) {
+// d_n (nullable): the selection count on the device, n a capacity
+__global__ void k_take(const int32_t* __restrict__ sel, int n, const int* __restrict__ d_n, const float* x,
+                       const float* y, const float* sz, const float* an, const float* rs, const int32_t* oc,
+                       const int32_t* ly, float* ox, float* oy, float* osz, float* oan, float* ors, int32_t* ooc,
+                       int32_t* oly, float* oxy, float* oresp) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (d_n) n = min(*d_n, n);
     if (i >= n) return;
     const int k = sel[i];
     ox[i] = x[k]; oy[i] = y[k]; osz[i] = sz[k]; oan[i] = an[k]; ors[i] = rs[k]; ooc[i] = oc[k]; oly[i] = ly[k];
@@ -263,7 +267,7 @@ static int32_t features_dev(fsb_ctx* ctx, Workspace& ws, int nfeat, bool exact, 
     float* trs = tan_ + n_sel;
     int32_t* toc = reinterpret_cast<int32_t*>(trs + n_sel);
     int32_t* tly = toc + n_sel;
-    k_take<<<(n_sel + 255) / 256, 256, 0, s>>>(sel, n_sel, ws.kx.as<float>(), ws.ky.as<float>(),
+    k_take<<<(n_sel + 255) / 256, 256, 0, s>>>(sel, n_sel, nullptr, ws.kx.as<float>(), ws.ky.as<float>(),
                                                ws.ksize.as<float>(), ws.kangle.as<float>(), ws.kresp.as<float>(),
                                                ws.koct.as<int32_t>(), ws.klayer.as<int32_t>(), tx, ty, tsz, tan_,
                                                trs, toc, tly, d_xy, d_resp);
@@ -346,6 +350,78 @@ void fsb_ctx::stage_release() {
 
 using namespace fsb;
 
+// ---- sync-free batched extraction: one CUDA graph per batch
+namespace fsb {
+namespace {
+// per image after its chain ran: the feature count and the flags (ASYNC_*, 8 = pyramid timeout)
+__global__ void k_batch_status(const uint32_t* cnt, int32_t* count, uint32_t* status) {
+    if (threadIdx.x != 0) return;
+    *count = (int32_t)cnt[6];
+    *status = cnt[7] | (cnt[PYR_ERR_WORD] ? 8u : 0u);
+}
+
+struct BatchCall {
+    int n_img;
+    const uint8_t* const* imgs;
+    int h, w, stride;
+    const fsb_sift_params* p;
+    const int32_t* nfeats;
+    float* const* xy;
+    float* const* resp;
+    uint8_t* const* u8;
+    int32_t* d_counts;
+};
+
+// the stream work of the batch (captured): image i on chain i mod chains
+int32_t batch_body(fsb_ctx* ctx, const BatchCall& b) {
+    auto& x = ctx->xb;
+    const int chains = (int)x.streams.size();
+    const bool exact = (b.p->flags & FSB_SIFT_EXACT_BLUR) != 0;
+    FSB_CUDA(cudaEventRecord(x.fork, ctx->stream));
+    for (int c = 0; c < chains; ++c) FSB_CUDA(cudaStreamWaitEvent(x.streams[c], x.fork, 0));
+    uint32_t* status = x.status.as<uint32_t>();
+    for (int i = 0; i < b.n_img; ++i) {
+        const int c = i % chains;
+        cudaStream_t s = x.streams[c];
+        Workspace& ws = *x.ws[c];
+        const int nfeat = b.nfeats[i];
+        FSB_TRY(run_pyramid(ws, b.imgs[i], b.stride, exact, s, nullptr, nullptr));
+        FSB_TRY(run_detect_async(ws, b.p->contrast, b.p->edge, x.caps, (int)((double)nfeat * 2.2), exact, s));
+        const int nf = x.caps.nfeat;
+        float* tx = ws.take.as<float>();
+        float* ty = tx + nf;
+        float* tsz = ty + nf;
+        float* tan_ = tsz + nf;
+        float* trs = tan_ + nf;
+        int32_t* toc = reinterpret_cast<int32_t*>(trs + nf);
+        int32_t* tly = toc + nf;
+        int32_t* sel = tly + nf;
+        FSB_TRY(spread_async(ws, x.caps, nfeat, sel, s));
+        const int* d_nsel = reinterpret_cast<const int*>(ws.counters.as<uint32_t>() + 6);
+        k_take<<<(nf + 255) / 256, 256, 0, s>>>(sel, nf, d_nsel, ws.kx.as<float>(), ws.ky.as<float>(),
+                                               ws.ksize.as<float>(), ws.kangle.as<float>(), ws.kresp.as<float>(),
+                                               ws.koct.as<int32_t>(), ws.klayer.as<int32_t>(), tx, ty, tsz, tan_, trs,
+                                               toc, tly, b.xy[i], b.resp ? b.resp[i] : nullptr);
+        FSB_TRY(run_describe_dev(ws, nf, d_nsel, tx, ty, tsz, tan_, toc, tly, nullptr, b.u8[i], exact, s));
+        k_batch_status<<<1, 32, 0, s>>>(ws.counters.as<uint32_t>(), b.d_counts + i, status + i);
+        note_launch(2);
+        FSB_CUDA(cudaGetLastError());
+    }
+    for (int c = 0; c < chains; ++c) {
+        FSB_CUDA(cudaEventRecord(x.join[c], x.streams[c]));
+        FSB_CUDA(cudaStreamWaitEvent(ctx->stream, x.join[c], 0));
+    }
+    return FSB_OK;
+}
+
+template <class T>
+void key_put(std::vector<char>& k, const T& v) {
+    const char* p = reinterpret_cast<const char*>(&v);
+    k.insert(k.end(), p, p + sizeof(T));
+}
+}  // namespace
+}  // namespace fsb
+
 extern "C" {
 
 int32_t fsb_version(void) { return 100; }
@@ -404,6 +480,20 @@ int32_t fsb_destroy(fsb_ctx* ctx) {
     for (DevBuf* b : all) b->release();
     if (ctx->gb_graph.exec) cudaGraphExecDestroy(ctx->gb_graph.exec);
     if (ctx->gb_graph.graph) cudaGraphDestroy(ctx->gb_graph.graph);
+    {
+        auto& x = ctx->xb;
+        for (cudaStream_t cs : x.streams) cudaStreamSynchronize(cs);
+        if (x.graph.exec) cudaGraphExecDestroy(x.graph.exec);
+        if (x.graph.graph) cudaGraphDestroy(x.graph.graph);
+        for (Workspace* w : x.ws) {
+            w->release();
+            delete w;
+        }
+        for (cudaStream_t cs : x.streams) cudaStreamDestroy(cs);
+        for (cudaEvent_t e : x.join) cudaEventDestroy(e);
+        if (x.fork) cudaEventDestroy(x.fork);
+        x.status.release();
+    }
     if (ctx->pinned) cudaFreeHost(ctx->pinned);
     ctx->stage_release();
     if (ctx->side) cudaStreamSynchronize(ctx->side);
@@ -686,6 +776,181 @@ int32_t fsb_sift_features_ex_d(fsb_ctx* ctx, const uint8_t* d_img, int32_t h, in
     return FSB_OK;
 }
 
+
+int32_t fsb_sift_features_batch_d(fsb_ctx* ctx, int32_t n_img, const uint8_t* const* d_imgs, int32_t h, int32_t w,
+                                  int32_t stride, const fsb_sift_params* p, const int32_t* nfeats, float* const* d_xy,
+                                  float* const* d_resp, uint8_t* const* d_rootsift, int32_t* d_counts,
+                                  int32_t* h_counts, int32_t chains) {
+    FSB_ARG(ctx && p, "null pointer");
+    FSB_ARG(n_img >= 0, "n_img < 0");
+    if (n_img == 0) return FSB_OK;
+    FSB_ARG(d_imgs && nfeats && d_xy && d_rootsift && d_counts, "null array");
+    FSB_ARG(h > 0 && w > 0 && stride >= w, "bad image size or stride");
+    FSB_ARG(h <= 32768 && w <= 32768, "image larger than 32768 pixels on a side");
+    FSB_ARG(chains >= 1 && chains <= 32, "chains must be 1..32");
+    int nf_max = 0;
+    for (int i = 0; i < n_img; ++i) {
+        FSB_ARG(nfeats[i] >= 0 && nfeats[i] <= (1 << 24), "nfeat out of range");
+        FSB_ARG(d_imgs[i] && d_xy[i] && d_rootsift[i], "null image or output pointer");
+        nf_max = nfeats[i] > nf_max ? nfeats[i] : nf_max;
+    }
+    FSB_TRY(use_device(ctx));
+    auto& x = ctx->xb;
+    cudaStream_t s = ctx->stream;
+    const bool timing = ctx->timing;
+    ctx->timing = false;   // stage events are not captured
+    struct Restore {
+        fsb_ctx* c;
+        bool t;
+        ~Restore() { c->timing = t; }
+    } restore{ctx, timing};
+    // first batch of a geometry: image 0 by the host-driven path (autotunes the pyramid for the
+    // geometry, and its refined-extremum count sizes the sort capacity)
+    if (x.h != h || x.w != w || x.warm_ref == 0) {
+        Workspace* ws = acquire(ctx);
+        struct Guard {
+            fsb_ctx* c;
+            Workspace* w;
+            ~Guard() { give_back(c, w); }
+        } guard{ctx, ws};
+        FSB_TRY(prepare_workspace(*ws, h, w));
+        FSB_TRY(detect_dev(ctx, *ws, d_imgs[0], stride, p, (int)((double)nfeats[0] * 2.2)));
+        int n0 = 0;
+        FSB_TRY(features_dev(ctx, *ws, nfeats[0], (p->flags & FSB_SIFT_EXACT_BLUR) != 0, d_xy[0],
+                             d_resp ? d_resp[0] : nullptr, nullptr, d_rootsift[0], &n0));
+        FSB_CUDA(cudaStreamSynchronize(s));
+        x.h = h;
+        x.w = w;
+        x.warm_ref = (int)std::min<size_t>(ws->cap_ref, (size_t)1 << 30);
+    }
+    // chains: streams, events, workspaces sized for the geometry and the capacities
+    while ((int)x.streams.size() < chains) {
+        cudaStream_t cs;
+        cudaEvent_t ev;
+        FSB_CUDA(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
+        FSB_CUDA(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+        x.streams.push_back(cs);
+        x.join.push_back(ev);
+        x.ws.push_back(new Workspace());
+    }
+    if (!x.fork) FSB_CUDA(cudaEventCreateWithFlags(&x.fork, cudaEventDisableTiming));
+    AsyncCaps caps{};
+    Workspace probe;
+    probe.g = make_geometry(h, w);
+    probe.cap_ref = (size_t)x.warm_ref + (size_t)x.warm_ref / 2;
+    FSB_TRY(async_caps(probe, (int)((double)nf_max * 2.2), nf_max, &caps));
+    const bool regrow = caps.kp > x.caps.kp || caps.nfeat > x.caps.nfeat || caps.ref > x.caps.ref ||
+                        caps.cand != x.caps.cand;
+    if (regrow || (int)x.ws.size() != (int)x.streams.size()) {
+        caps.kp = std::max(caps.kp, x.caps.kp);
+        caps.nfeat = std::max(caps.nfeat, x.caps.nfeat);
+        caps.ref = std::max(caps.ref, x.caps.ref);
+        caps.rank = (uint32_t)(2 * caps.kp + 32);
+        x.caps = caps;
+    }
+    // the streams the capture uses are the first `chains`; the others idle
+    std::vector<cudaStream_t> all_streams = x.streams;
+    std::vector<cudaEvent_t> all_join = x.join;
+    std::vector<Workspace*> all_ws = x.ws;
+    x.streams.resize(chains);
+    x.join.resize(chains);
+    x.ws.resize(chains);
+    struct Back {
+        fsb_ctx::ExtractBatch& x;
+        std::vector<cudaStream_t> s;
+        std::vector<cudaEvent_t> j;
+        std::vector<Workspace*> w;
+        ~Back() { x.streams = s; x.join = j; x.ws = w; }
+    } back{x, all_streams, all_join, all_ws};
+    for (Workspace* ws : x.ws) {
+        if (ws->g.h != h || ws->g.w != w) FSB_TRY(prepare_workspace(*ws, h, w));
+        FSB_TRY(prepare_async(*ws, x.caps, s));
+    }
+    FSB_TRY(x.status.ensure((size_t)n_img * 4 + 64));
+    // the captured graph is replayed while every argument and buffer address is unchanged
+    std::vector<char> key;
+    key_put(key, n_img);
+    key_put(key, h);
+    key_put(key, w);
+    key_put(key, stride);
+    key_put(key, chains);
+    key_put(key, *p);
+    key_put(key, x.caps);
+    key_put(key, d_counts);
+    key_put(key, x.status.p);
+    for (int i = 0; i < n_img; ++i) {
+        key_put(key, d_imgs[i]);
+        key_put(key, nfeats[i]);
+        key_put(key, d_xy[i]);
+        key_put(key, d_resp ? d_resp[i] : nullptr);
+        key_put(key, d_rootsift[i]);
+    }
+    for (Workspace* ws : x.ws) {
+        const void* ptrs[] = {ws->dog.p, ws->mag.p, ws->ang.p, ws->plane[0].p, ws->plane[1].p, ws->plane[2].p,
+                              ws->next_base.p, ws->cand.p, ws->refined.p, ws->oriented.p, ws->keys_a.p, ws->keys_b.p,
+                              ws->vals_a.p, ws->sort_tmp.p, ws->counters.p, ws->kx.p, ws->ky.p, ws->ksize.p,
+                              ws->kangle.p, ws->kresp.p, ws->koct.p, ws->klayer.p, ws->spread.p, ws->take.p};
+        for (const void* q : ptrs) key_put(key, q);
+        key_put(key, ws->sort_tmp.bytes);
+    }
+    if (!x.graph.exec || key != x.graph.key) {
+        if (x.graph.exec) cudaGraphExecDestroy(x.graph.exec);
+        if (x.graph.graph) cudaGraphDestroy(x.graph.graph);
+        x.graph.exec = nullptr;
+        x.graph.graph = nullptr;
+        BatchCall bc{n_img, d_imgs, h, w, stride, p, nfeats, d_xy, d_resp, d_rootsift, d_counts};
+        FSB_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+        const int32_t st = batch_body(ctx, bc);
+        cudaGraph_t g = nullptr;
+        const cudaError_t e = cudaStreamEndCapture(s, &g);
+        if (st != FSB_OK) {
+            if (g) cudaGraphDestroy(g);
+            return st;
+        }
+        if (e != cudaSuccess) {
+            if (g) cudaGraphDestroy(g);
+            set_error("capture of the extraction batch failed: %s", cudaGetErrorString(e));
+            return FSB_ERR_CUDA;
+        }
+        x.graph.graph = g;
+        FSB_CUDA(cudaGraphInstantiate(&x.graph.exec, g, 0));
+        x.graph.key = key;
+    }
+    FSB_CUDA(cudaGraphLaunch(x.graph.exec, s));
+    // one wait per batch: the flags say which images (if any) exceeded a capacity
+    FSB_TRY(stage_ensure(ctx, (size_t)n_img * 8 + 64));
+    uint32_t* h_status = static_cast<uint32_t*>(ctx->pinned);
+    int32_t* h_cnt = reinterpret_cast<int32_t*>(h_status + n_img);
+    FSB_CUDA(cudaMemcpyAsync(h_status, x.status.p, (size_t)n_img * 4, cudaMemcpyDeviceToHost, s));
+    FSB_CUDA(cudaMemcpyAsync(h_cnt, d_counts, (size_t)n_img * 4, cudaMemcpyDeviceToHost, s));
+    FSB_CUDA(cudaStreamSynchronize(s));
+    for (int i = 0; i < n_img; ++i) {
+        if (h_status[i] & 8u) {
+            set_error("pyramid: a TMA row copy did not complete in time (strip engine), image %d", i);
+            return FSB_ERR_TIMEOUT;
+        }
+        if (h_status[i] == 0) continue;
+        // a capacity was exceeded: this image again by the host-driven path
+        Workspace* ws = acquire(ctx);
+        struct Guard {
+            fsb_ctx* c;
+            Workspace* w;
+            ~Guard() { give_back(c, w); }
+        } guard{ctx, ws};
+        FSB_TRY(prepare_workspace(*ws, h, w));
+        FSB_TRY(detect_dev(ctx, *ws, d_imgs[i], stride, p, (int)((double)nfeats[i] * 2.2)));
+        int n = 0;
+        FSB_TRY(features_dev(ctx, *ws, nfeats[i], (p->flags & FSB_SIFT_EXACT_BLUR) != 0, d_xy[i],
+                             d_resp ? d_resp[i] : nullptr, nullptr, d_rootsift[i], &n));
+        h_cnt[i] = n;
+        FSB_CUDA(cudaMemcpyAsync(d_counts + i, &h_cnt[i], 4, cudaMemcpyHostToDevice, s));
+        FSB_CUDA(cudaStreamSynchronize(s));
+        x.redone += 1;
+    }
+    if (h_counts) std::memcpy(h_counts, h_cnt, (size_t)n_img * 4);
+    return FSB_OK;
+}
+
 int32_t fsb_project_d(fsb_ctx* ctx, const float* d_xy, int32_t n, const double* hm9, const float* d_offset,
                       double* d_out) {
     FSB_ARG(ctx && hm9, "null pointer");
@@ -694,6 +959,20 @@ int32_t fsb_project_d(fsb_ctx* ctx, const float* d_xy, int32_t n, const double* 
     FSB_TRY(use_device(ctx));
     FSB_TRY(run_project(d_xy, n, hm9, d_offset, d_out, ctx->stream));
     FSB_CUDA(cudaStreamSynchronize(ctx->stream));
+    return FSB_OK;
+}
+
+int32_t fsb_project_batch_d(fsb_ctx* ctx, int32_t n_sets, const float* const* d_xy, const int32_t* n,
+                            const double* hm9, const float* const* d_offset, double* const* d_out) {
+    FSB_ARG(ctx && (n_sets == 0 || (d_xy && n && hm9 && d_out)), "null pointer");
+    FSB_ARG(n_sets >= 0, "n_sets < 0");
+    for (int k = 0; k < n_sets; ++k) FSB_ARG(n[k] >= 0 && (n[k] == 0 || (d_xy[k] && d_out[k])), "bad points");
+    if (n_sets == 0) return FSB_OK;
+    FSB_TRY(use_device(ctx));
+    for (int k = 0; k < n_sets; ++k)
+        if (n[k] > 0)
+            FSB_TRY(run_project(d_xy[k], n[k], hm9 + 9 * (size_t)k, d_offset ? d_offset[k] : nullptr, d_out[k],
+                                ctx->stream));
     return FSB_OK;
 }
 

@@ -41,8 +41,13 @@ template <class Acc>
 __global__ void __launch_bounds__(OW * 32) k_orient(const float* __restrict__ MAG, const float* __restrict__ ANG,
                                                     Geometry g, const Refined* __restrict__ ref,
                                                     const uint32_t* __restrict__ order, uint32_t k0, uint32_t k1,
+                                                    const uint32_t* __restrict__ d_range,
                                                     Oriented* __restrict__ slots, uint32_t* __restrict__ cnt,
                                                     uint32_t* total) {
+    if (d_range) {   // the rank range on the device ([k0, k1) of this pass)
+        k0 = d_range[0];
+        k1 = d_range[1];
+    }
     __shared__ Acc s_acc[OW][ORI_BINS][33];
     __shared__ float s_raw[OW][ORI_BINS];
     __shared__ float s_sm[OW][ORI_BINS];
@@ -190,7 +195,8 @@ __device__ __forceinline__ void j_range(float a, float b, float lo, float hi, in
 // (R' + dr, C' + dc) it touches. Cell (R, C) then sums its four contributors in a fixed order.
 template <bool EXACT>
 __global__ void __launch_bounds__(DW * 32) k_describe(const float* __restrict__ MAG, const float* __restrict__ ANG,
-                                                      Geometry g, int n, const float* __restrict__ kx,
+                                                      Geometry g, int n, const int* __restrict__ d_n,
+                                                      const float* __restrict__ kx,
                                                       const float* __restrict__ ky, const float* __restrict__ ks,
                                                       const float* __restrict__ ka, const int32_t* __restrict__ ko,
                                                       const int32_t* __restrict__ kl, float* __restrict__ desc,
@@ -202,6 +208,7 @@ __global__ void __launch_bounds__(DW * 32) k_describe(const float* __restrict__ 
     const int wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
     Acc (*acc)[32] = s_acc[wid];
     const int Rq = lane / 5 - 1, Cq = lane % 5 - 1;
+    if (d_n) n = min(*d_n, n);   // the count on the device, n a capacity
     for (int k = blockIdx.x * DW + wid; k < n; k += gridDim.x * DW) {
         for (int b = 0; b < 4 * NB; ++b) acc[b][lane] = (Acc)0;
         // keypoint geometry in float64 as the reference's host code computes it (gsift.py:490-501)
@@ -376,10 +383,10 @@ int32_t run_orient(const Workspace& ws, const Refined* ref, const uint32_t* orde
     const unsigned grid = ob < 148 * 32 ? ob : 148 * 32;
     if (exact)
         k_orient<double><<<grid, OW * 32, 0, s>>>(ws.mag.as<float>(), ws.ang.as<float>(), ws.g, ref, order, k0, k1,
-                                                  slots, cnt, d_total);
+                                                  nullptr, slots, cnt, d_total);
     else
         k_orient<float><<<grid, OW * 32, 0, s>>>(ws.mag.as<float>(), ws.ang.as<float>(), ws.g, ref, order, k0, k1,
-                                                 slots, cnt, d_total);
+                                                 nullptr, slots, cnt, d_total);
     note_launch();
     FSB_CUDA(cudaGetLastError());
     return FSB_OK;
@@ -392,11 +399,49 @@ int32_t run_describe_mode(const Workspace& ws, int n, const float* d_x, const fl
     const unsigned nb = blocks(n, DW);
     const unsigned grid = nb < 148u * 32u ? nb : 148u * 32u;
     if (exact)
-        k_describe<true><<<grid, DW * 32, 0, s>>>(ws.mag.as<float>(), ws.ang.as<float>(), ws.g, n, d_x, d_y, d_size,
+        k_describe<true><<<grid, DW * 32, 0, s>>>(ws.mag.as<float>(), ws.ang.as<float>(), ws.g, n, nullptr, d_x, d_y,
+                                                  d_size,
                                                   d_angle, d_oct, d_layer, d_desc, d_u8);
     else
-        k_describe<false><<<grid, DW * 32, 0, s>>>(ws.mag.as<float>(), ws.ang.as<float>(), ws.g, n, d_x, d_y, d_size,
+        k_describe<false><<<grid, DW * 32, 0, s>>>(ws.mag.as<float>(), ws.ang.as<float>(), ws.g, n, nullptr, d_x, d_y,
+                                                   d_size,
                                                    d_angle, d_oct, d_layer, d_desc, d_u8);
+    note_launch();
+    FSB_CUDA(cudaGetLastError());
+    return FSB_OK;
+}
+
+// Orientation of ranks [d_range[0], d_range[1]) read on the device; grid sized for max_ranks ranks.
+int32_t run_orient_dev(const Workspace& ws, const Refined* ref, const uint32_t* order, uint32_t max_ranks,
+                       const uint32_t* d_range, Oriented* slots, uint32_t* cnt, uint32_t* d_total, bool exact,
+                       cudaStream_t s) {
+    if (max_ranks == 0) return FSB_OK;
+    const unsigned ob = blocks(max_ranks, OW);
+    const unsigned grid = ob < 148 * 32 ? ob : 148 * 32;
+    if (exact)
+        k_orient<double><<<grid, OW * 32, 0, s>>>(ws.mag.as<float>(), ws.ang.as<float>(), ws.g, ref, order, 0, 0,
+                                                  d_range, slots, cnt, d_total);
+    else
+        k_orient<float><<<grid, OW * 32, 0, s>>>(ws.mag.as<float>(), ws.ang.as<float>(), ws.g, ref, order, 0, 0,
+                                                 d_range, slots, cnt, d_total);
+    note_launch();
+    FSB_CUDA(cudaGetLastError());
+    return FSB_OK;
+}
+
+// Descriptors of *d_n keypoints (read on the device; at most cap), grid sized for cap.
+int32_t run_describe_dev(const Workspace& ws, int cap, const int* d_n, const float* d_x, const float* d_y,
+                         const float* d_size, const float* d_angle, const int32_t* d_oct, const int32_t* d_layer,
+                         float* d_desc, uint8_t* d_u8, bool exact, cudaStream_t s) {
+    if (cap <= 0) return FSB_OK;
+    const unsigned nb = blocks(cap, DW);
+    const unsigned grid = nb < 148u * 32u ? nb : 148u * 32u;
+    if (exact)
+        k_describe<true><<<grid, DW * 32, 0, s>>>(ws.mag.as<float>(), ws.ang.as<float>(), ws.g, cap, d_n, d_x, d_y,
+                                                  d_size, d_angle, d_oct, d_layer, d_desc, d_u8);
+    else
+        k_describe<false><<<grid, DW * 32, 0, s>>>(ws.mag.as<float>(), ws.ang.as<float>(), ws.g, cap, d_n, d_x, d_y,
+                                                   d_size, d_angle, d_oct, d_layer, d_desc, d_u8);
     note_launch();
     FSB_CUDA(cudaGetLastError());
     return FSB_OK;

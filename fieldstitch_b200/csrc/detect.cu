@@ -277,11 +277,14 @@ __device__ __forceinline__ float kp_scale(int l, float x2) {
 
 // rank key of a refined extremum: response descending (a positive finite float's bits order like
 // its value); the DoG-atlas index breaks ties afterwards (k_rank_ties)
-__global__ void k_rank_keys(const Refined* __restrict__ ref, uint32_t n, uint32_t* __restrict__ key,
-                            uint32_t* __restrict__ val) {
+// d_n (nullable): the refined count on the device; entries from it up to n get the largest key, so
+// a stable sort of n entries puts them last (n is then a capacity)
+__global__ void k_rank_keys(const Refined* __restrict__ ref, uint32_t n, const uint32_t* __restrict__ d_n,
+                            uint32_t* __restrict__ key, uint32_t* __restrict__ val) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
-    key[i] = 0x7fffffffu - __float_as_uint(ref[i].resp);
+    const uint32_t m = d_n ? min(*d_n, n) : n;
+    key[i] = i < m ? 0x7fffffffu - __float_as_uint(ref[i].resp) : 0x7fffffffu;
     val[i] = i;
 }
 
@@ -289,8 +292,10 @@ __global__ void k_rank_keys(const Refined* __restrict__ ref, uint32_t n, uint32_
 // by DoG-atlas index (their order in the refined list is the atomic append order), so an element
 // goes to the run's start + the number of run members with a smaller index
 __global__ void k_rank_ties(const uint32_t* __restrict__ key, const uint32_t* __restrict__ val,
-                            const Refined* __restrict__ ref, uint32_t n, uint32_t* __restrict__ order) {
+                            const Refined* __restrict__ ref, uint32_t n, const uint32_t* __restrict__ d_n,
+                            uint32_t* __restrict__ order) {
     const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (d_n) n = min(*d_n, n);
     if (t >= n) return;
     const uint32_t k = key[t], v = val[t];
     uint32_t a = t, b = t + 1;
@@ -309,11 +314,17 @@ __global__ void k_rank_ties(const uint32_t* __restrict__ key, const uint32_t* __
 
 // keypoints in final order: rank t's peaks (bin order) at pos[t] .. pos[t] + cnt[t] - 1, kept below
 // n_keep
+// d_rk (nullable): on the device, [0] the ranks oriented, [1] the keypoints kept (n_rank is then a
+// capacity and n_keep unused)
 __global__ void k_gather_ranked(const Oriented* __restrict__ slots, const uint32_t* __restrict__ cnt,
                                 const uint32_t* __restrict__ pos, const Refined* __restrict__ ref, uint32_t n_rank,
-                                uint32_t n_keep, float* kx, float* ky, float* ksize, float* kang, float* kresp,
-                                int32_t* koct, int32_t* klayer) {
+                                uint32_t n_keep, const uint32_t* __restrict__ d_rk, float* kx, float* ky, float* ksize,
+                                float* kang, float* kresp, int32_t* koct, int32_t* klayer) {
     const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (d_rk) {
+        n_rank = min(d_rk[0], n_rank);
+        n_keep = d_rk[1];
+    }
     if (t >= n_rank) return;
     const uint32_t c = cnt[t], p = pos[t];
     for (uint32_t k = 0; k < c && p + k < n_keep; ++k) {
@@ -368,9 +379,11 @@ __device__ __forceinline__ int warp_sum(int v) {
 }
 
 __global__ void __launch_bounds__(SP_T) k_sp_hist(const float* __restrict__ x, const float* __restrict__ y, int n,
-                                                  float W, float H, int ch, int* __restrict__ hist) {
+                                                  const int* __restrict__ d_n, float W, float H, int ch,
+                                                  int* __restrict__ hist) {
     __shared__ int h[SP_CELLS];
     const int tid = threadIdx.x;
+    if (d_n) n = min(*d_n, n);
     if (tid < SP_CELLS) h[tid] = 0;
     __syncthreads();
     const int i0 = blockIdx.x * ch, i1 = min(i0 + ch, n);
@@ -380,9 +393,11 @@ __global__ void __launch_bounds__(SP_T) k_sp_hist(const float* __restrict__ x, c
 }
 
 __global__ void __launch_bounds__(SP_T) k_sp_pos(const float* __restrict__ x, const float* __restrict__ y, int n,
-                                                 float W, float H, int ch, int nch, const int* __restrict__ hist,
-                                                 int cap, int nfeat, int* __restrict__ pos, int* __restrict__ grp_sel,
+                                                 const int* __restrict__ d_n, float W, float H, int ch, int nch,
+                                                 const int* __restrict__ hist, int cap, int nfeat,
+                                                 int* __restrict__ pos, int* __restrict__ grp_sel,
                                                  int* __restrict__ chunk_sel) {
+    if (d_n) n = min(*d_n, n);
     __shared__ int run[SP_CELLS];          // elements of the cell before the current step (all chunks)
     __shared__ int start0[SP_CELLS];       // first selection position of the cell's group-0 elements
     __shared__ int wc[SP_NW][SP_CELLS];    // per warp and cell: count, then the warp's base
@@ -492,12 +507,22 @@ __global__ void __launch_bounds__(SP_T) k_sp_pos(const float* __restrict__ x, co
 // groups of its chunk, earlier lanes), corrected inside its run of equal responses (elements of
 // the run after it with a smaller selection position come first, elements before it with a
 // larger one come after). by_position: slot = selection position (the order _spread returns).
-__global__ void __launch_bounds__(256) k_sp_place(const float* __restrict__ resp, int n, int ch,
-                                                  const int* __restrict__ pos, const int* __restrict__ grp_sel,
-                                                  const int* __restrict__ chunk_sel, bool by_position,
-                                                  int32_t* __restrict__ sel) {
+// d_n (nullable): the keypoint count on the device, n a capacity; at most nfeat keypoints are
+// all selected, in their own order (features.py:39-40 returns range(n)), as k_iota does
+__global__ void __launch_bounds__(256) k_sp_place(const float* __restrict__ resp, int n, const int* __restrict__ d_n,
+                                                  int nfeat, int ch, const int* __restrict__ pos,
+                                                  const int* __restrict__ grp_sel, const int* __restrict__ chunk_sel,
+                                                  bool by_position, int32_t* __restrict__ sel) {
     const int lane = threadIdx.x & 31;
     const int g = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;   // 32-element group
+    if (d_n) {
+        n = min(*d_n, n);
+        if (n <= nfeat) {
+            const int i = g * 32 + lane;
+            if (i < n) sel[i] = i;
+            return;
+        }
+    }
     if (g * 32 >= n) return;
     const int k = (g * 32) / ch;
     int before = 0;
@@ -616,12 +641,13 @@ int32_t run_detect(fsb_ctx* ctx, Workspace& ws, double contrast, double edge, in
     cub::DeviceRadixSort::SortPairs(nullptr, t1, ka, ka + n_ref, va, va + n_ref, (int)n_ref, 0, 31, s);
     cub::DeviceScan::ExclusiveSum(nullptr, t2, rcnt, rpos, (int)n_ref, s);
     FSB_TRY(ws.sort_tmp.ensure(t1 > t2 ? t1 : t2));
-    k_rank_keys<<<blocks(n_ref, 256), 256, 0, s>>>(ws.refined.as<Refined>(), n_ref, ka, va);
+    k_rank_keys<<<blocks(n_ref, 256), 256, 0, s>>>(ws.refined.as<Refined>(), n_ref, nullptr, ka, va);
     size_t tb = ws.sort_tmp.bytes;
     FSB_CUDA(cub::DeviceRadixSort::SortPairs(ws.sort_tmp.p, tb, ka, ka + n_ref, va, va + n_ref, (int)n_ref, 0, 31,
                                              s));
     uint32_t* order = va;   // the unsorted values are dead
-    k_rank_ties<<<blocks(n_ref, 256), 256, 0, s>>>(ka + n_ref, va + n_ref, ws.refined.as<Refined>(), n_ref, order);
+    k_rank_ties<<<blocks(n_ref, 256), 256, 0, s>>>(ka + n_ref, va + n_ref, ws.refined.as<Refined>(), n_ref, nullptr,
+                                                   order);
     note_launch(3);
     ctx->stage_end(ST_SORT);
     ctx->stage_begin(ST_ORIENT);
@@ -653,7 +679,7 @@ int32_t run_detect(fsb_ctx* ctx, Workspace& ws, double contrast, double edge, in
     FSB_TRY(ws.kresp.ensure(nb4));
     FSB_TRY(ws.koct.ensure(nb4));
     FSB_TRY(ws.klayer.ensure(nb4));
-    k_gather_ranked<<<blocks(k1, 256), 256, 0, s>>>(slots, rcnt, rpos, ws.refined.as<Refined>(), k1, n_keep,
+    k_gather_ranked<<<blocks(k1, 256), 256, 0, s>>>(slots, rcnt, rpos, ws.refined.as<Refined>(), k1, n_keep, nullptr,
                                                     ws.kx.as<float>(), ws.ky.as<float>(), ws.ksize.as<float>(),
                                                     ws.kangle.as<float>(), ws.kresp.as<float>(), ws.koct.as<int32_t>(),
                                                     ws.klayer.as<int32_t>());
@@ -689,10 +715,10 @@ int32_t spread_dev(fsb_ctx* ctx, const float* d_x, const float* d_y, const float
     int* grp_sel = chunk_sel + nch;
     int* pos = grp_sel + ngrp;
     const int cap = (nfeat + SP_CELLS - 1) / SP_CELLS;
-    k_sp_hist<<<nch, SP_T, 0, s>>>(d_x, d_y, n, W, H, ch, hist);
-    k_sp_pos<<<nch, SP_T, 0, s>>>(d_x, d_y, n, W, H, ch, nch, hist, cap, nfeat, pos, grp_sel, chunk_sel);
-    k_sp_place<<<blocks((long long)ngrp * 32, 256), 256, 0, s>>>(d_resp, n, ch, pos, grp_sel, chunk_sel,
-                                                                   by_position, d_sel);
+    k_sp_hist<<<nch, SP_T, 0, s>>>(d_x, d_y, n, nullptr, W, H, ch, hist);
+    k_sp_pos<<<nch, SP_T, 0, s>>>(d_x, d_y, n, nullptr, W, H, ch, nch, hist, cap, nfeat, pos, grp_sel, chunk_sel);
+    k_sp_place<<<blocks((long long)ngrp * 32, 256), 256, 0, s>>>(d_resp, n, nullptr, nfeat, ch, pos, grp_sel,
+                                                                   chunk_sel, by_position, d_sel);
     note_launch(3);
     FSB_CUDA(cudaGetLastError());
     *n_sel = nfeat;
@@ -702,6 +728,169 @@ int32_t spread_dev(fsb_ctx* ctx, const float* d_x, const float* d_y, const float
 int32_t run_spread(const Workspace& ws, int nfeat, int32_t* d_sel_out, int* n_sel, fsb_ctx* ctx, cudaStream_t s) {
     return spread_dev(ctx, ws.kx.as<float>(), ws.ky.as<float>(), ws.kresp.as<float>(), ws.n_kp, (float)ws.g.w,
                       (float)ws.g.h, nfeat, false, d_sel_out, n_sel, s);
+}
+
+}  // namespace fsb
+
+// -------------------------------------------------------------------------------------------------
+// Detection with every count on the device (no host wait; stream-capturable): the same stages and
+// the same outputs as run_detect, each launch sized by a capacity fixed beforehand and reading its
+// count from ws.counters. Status words (uint32) of ws.counters: [0] candidates, [1] refined,
+// [2] orientation peaks, [3] / [4] the current orientation pass's rank range, [5] keypoints kept,
+// [6] features selected, [7] flags (ASYNC_*). A flagged image must be redone by the host-driven path.
+namespace fsb {
+namespace {
+
+// orientation pass `pass`: the next rank range, as run_detect's loop forms it (empty once the cap
+// is met or every refined extremum is oriented)
+__global__ void k_orient_range(uint32_t* cnt, int pass, uint32_t max_kp, uint32_t cap_ref, uint32_t cap_rank) {
+    if (threadIdx.x != 0) return;
+    const uint32_t n_ref = min(cnt[1], cap_ref), total = cnt[2], k1 = pass == 0 ? 0u : cnt[4];
+    if (pass > 0 && (total >= max_kp || k1 >= n_ref)) {
+        cnt[3] = k1;
+        return;
+    }
+    const uint32_t want = max_kp > total ? max_kp - total : 1u;
+    const unsigned long long e = (unsigned long long)k1 + want;
+    uint32_t nk = (uint32_t)min(e, (unsigned long long)n_ref);
+    nk = min(nk, cap_rank);
+    cnt[3] = k1;
+    cnt[4] = nk;
+}
+
+// after the passes: keypoints kept and the overflow / incomplete flags
+__global__ void k_detect_finish(uint32_t* cnt, uint32_t max_kp, uint32_t cap_cand, uint32_t cap_ref) {
+    if (threadIdx.x != 0) return;
+    const uint32_t n_ref = min(cnt[1], cap_ref), total = cnt[2], k1 = cnt[4];
+    uint32_t flags = cnt[7];
+    if (cnt[0] > cap_cand) flags |= ASYNC_CAND_OVERFLOW;
+    if (cnt[1] > cap_ref) flags |= ASYNC_REF_OVERFLOW;
+    if (total < max_kp && k1 < n_ref) flags |= ASYNC_ORIENT_INCOMPLETE;
+    cnt[7] = flags;
+    cnt[5] = cnt[0] == 0 || n_ref == 0 ? 0u : min(total, max_kp);
+}
+
+// features selected: none below 10 keypoints (features.py:121-122), else min(n, nfeat)
+__global__ void k_select_count(uint32_t* cnt, int nfeat) {
+    if (threadIdx.x != 0) return;
+    const uint32_t n = cnt[5];
+    cnt[6] = n < 10u ? 0u : min(n, (uint32_t)nfeat);
+}
+
+}  // namespace
+
+int32_t async_caps(const Workspace& ws, int max_kp, int nfeat, AsyncCaps* c) {
+    const Geometry& g = ws.g;
+    long long vox = 0;
+    for (int o = 0; o < g.n_oct; ++o)
+        vox += (long long)N_LAYERS * max(0, g.R[o] - 2 * BORDER) * max(0, g.C[o] - 2 * BORDER);
+    c->cand = (uint32_t)std::min<long long>(std::max<long long>(vox, 1), 1ll << 22);
+    c->ref = (uint32_t)std::min<long long>(std::max<long long>((long long)ws.cap_ref, 1ll << 16), c->cand);
+    c->ref = (c->ref + 1023) / 1024 * 1024;
+    c->kp = std::max(max_kp, 1);
+    c->rank = (uint32_t)(2 * c->kp + 32);
+    c->nfeat = std::max(nfeat, 1);
+    return FSB_OK;
+}
+
+int32_t prepare_async(Workspace& ws, const AsyncCaps& c, cudaStream_t s) {
+    if (ws.cap_cand < c.cand) {
+        ws.cap_cand = c.cand;
+        FSB_TRY(ws.cand.ensure((size_t)c.cand * sizeof(uint32_t)));
+    }
+    FSB_TRY(ws.refined.ensure((size_t)c.ref * sizeof(Refined)));
+    FSB_TRY(ws.keys_a.ensure((size_t)c.ref * 4 * 2));
+    FSB_TRY(ws.vals_a.ensure((size_t)c.ref * 4 * 2));
+    FSB_TRY(ws.keys_b.ensure((size_t)c.rank * 4 * 2));
+    FSB_TRY(ws.oriented.ensure((size_t)c.rank * ORI_SLOTS * sizeof(Oriented)));
+    size_t t1 = 0, t2 = 0;
+    uint32_t* k = ws.keys_a.as<uint32_t>();
+    FSB_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, t1, k, k + c.ref, k, k + c.ref, (int)c.ref, 0, 31, s));
+    FSB_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, t2, k, k, (int)c.rank, s));
+    FSB_TRY(ws.sort_tmp.ensure(t1 > t2 ? t1 : t2));
+    const size_t kb = (size_t)c.kp * 4;
+    FSB_TRY(ws.kx.ensure(kb));
+    FSB_TRY(ws.ky.ensure(kb));
+    FSB_TRY(ws.ksize.ensure(kb));
+    FSB_TRY(ws.kangle.ensure(kb));
+    FSB_TRY(ws.kresp.ensure(kb));
+    FSB_TRY(ws.koct.ensure(kb));
+    FSB_TRY(ws.klayer.ensure(kb));
+    // spread scratch: chunk histograms, positions, group and chunk counts, the selection
+    const int ch = (int)(1024 * (((long long)c.kp + 65535) / 65536));
+    const int nch = (c.kp + ch - 1) / ch, ngrp = (c.kp + 31) / 32;
+    FSB_TRY(ws.spread.ensure(((size_t)nch * (SP_CELLS + 1) + (size_t)ngrp + 2 * (size_t)c.kp) * 4 + 512));
+    // the selected keypoints' fields for description (7 arrays of nfeat) and the selection (kp)
+    FSB_TRY(ws.take.ensure(((size_t)c.nfeat * 7 + (size_t)c.kp) * 4 + 512));
+    return FSB_OK;
+}
+
+int32_t run_detect_async(Workspace& ws, double contrast, double edge, const AsyncCaps& c, int max_kp, bool exact,
+                         cudaStream_t s) {
+    const uint32_t mk = (uint32_t)std::max(1, std::min(max_kp, c.kp));
+    const Geometry& g = ws.g;
+    const DetectConsts k = make_consts(g, contrast, edge);
+    uint32_t* cnt = ws.counters.as<uint32_t>();
+    const float* DF = ws.dog.as<float>();
+    FSB_CUDA(cudaMemsetAsync(cnt, 0, 8 * sizeof(uint32_t), s));
+    int nblk = 0;
+    const ExTiles tl = make_tiles(g, &nblk);
+    if (nblk > 0) k_extrema<<<nblk, EX_T, 0, s>>>(DF, k, tl, ws.cand.as<uint32_t>(), cnt, c.cand);
+    const unsigned gr = std::min(blocks(c.cand, 128), 148u * 16u);
+    k_refine<<<gr, 128, 0, s>>>(DF, k, ws.cand.as<uint32_t>(), cnt, c.cand, ws.refined.as<Refined>(), cnt + 1, c.ref);
+    uint32_t* ka = ws.keys_a.as<uint32_t>();
+    uint32_t* va = ws.vals_a.as<uint32_t>();
+    k_rank_keys<<<blocks(c.ref, 256), 256, 0, s>>>(ws.refined.as<Refined>(), c.ref, cnt + 1, ka, va);
+    size_t tb = ws.sort_tmp.bytes;
+    FSB_CUDA(cub::DeviceRadixSort::SortPairs(ws.sort_tmp.p, tb, ka, ka + c.ref, va, va + c.ref, (int)c.ref, 0, 31,
+                                             s));
+    uint32_t* order = va;
+    k_rank_ties<<<blocks(c.ref, 256), 256, 0, s>>>(ka + c.ref, va + c.ref, ws.refined.as<Refined>(), c.ref, cnt + 1,
+                                                   order);
+    uint32_t* rcnt = ws.keys_b.as<uint32_t>();
+    uint32_t* rpos = rcnt + c.rank;
+    FSB_CUDA(cudaMemsetAsync(rcnt, 0, (size_t)c.rank * 4, s));
+    Oriented* slots = ws.oriented.as<Oriented>();
+    for (int pass = 0; pass < ASYNC_ORIENT_PASSES; ++pass) {
+        k_orient_range<<<1, 32, 0, s>>>(cnt, pass, mk, c.ref, c.rank);
+        FSB_TRY(run_orient_dev(ws, ws.refined.as<Refined>(), order, (uint32_t)c.kp, cnt + 3, slots, rcnt, cnt + 2,
+                               exact, s));
+    }
+    k_detect_finish<<<1, 32, 0, s>>>(cnt, mk, c.cand, c.ref);
+    tb = ws.sort_tmp.bytes;
+    FSB_CUDA(cub::DeviceScan::ExclusiveSum(ws.sort_tmp.p, tb, rcnt, rpos, (int)c.rank, s));
+    k_gather_ranked<<<blocks(c.rank, 256), 256, 0, s>>>(slots, rcnt, rpos, ws.refined.as<Refined>(), c.rank, 0, cnt + 4,
+                                                        ws.kx.as<float>(), ws.ky.as<float>(), ws.ksize.as<float>(),
+                                                        ws.kangle.as<float>(), ws.kresp.as<float>(),
+                                                        ws.koct.as<int32_t>(), ws.klayer.as<int32_t>());
+    note_launch(6 + 2 * ASYNC_ORIENT_PASSES);
+    FSB_CUDA(cudaGetLastError());
+    return FSB_OK;
+}
+
+int32_t spread_async(Workspace& ws, const AsyncCaps& c, int nfeat, int32_t* d_sel, cudaStream_t s) {
+    uint32_t* cnt = ws.counters.as<uint32_t>();
+    k_select_count<<<1, 32, 0, s>>>(cnt, nfeat);
+    if (nfeat <= 0) return FSB_OK;
+    const int* d_n = reinterpret_cast<const int*>(cnt + 5);
+    const int n = c.kp;
+    const int ch = (int)(1024 * (((long long)n + 65535) / 65536));
+    const int nch = (n + ch - 1) / ch;
+    const int ngrp = (n + 31) / 32;
+    int* hist = ws.spread.as<int>();
+    int* chunk_sel = hist + (size_t)nch * SP_CELLS;
+    int* grp_sel = chunk_sel + nch;
+    int* pos = grp_sel + ngrp;
+    const int cap = (nfeat + SP_CELLS - 1) / SP_CELLS;
+    const float W = (float)ws.g.w, H = (float)ws.g.h;
+    k_sp_hist<<<nch, SP_T, 0, s>>>(ws.kx.as<float>(), ws.ky.as<float>(), n, d_n, W, H, ch, hist);
+    k_sp_pos<<<nch, SP_T, 0, s>>>(ws.kx.as<float>(), ws.ky.as<float>(), n, d_n, W, H, ch, nch, hist, cap, nfeat, pos,
+                                  grp_sel, chunk_sel);
+    k_sp_place<<<blocks((long long)ngrp * 32, 256), 256, 0, s>>>(ws.kresp.as<float>(), n, d_n, nfeat, ch, pos, grp_sel,
+                                                                   chunk_sel, false, d_sel);
+    note_launch(4);
+    FSB_CUDA(cudaGetLastError());
+    return FSB_OK;
 }
 
 }  // namespace fsb

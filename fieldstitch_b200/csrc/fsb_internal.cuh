@@ -111,6 +111,13 @@ struct DevBuf {
     template <class T> T* as() const { return reinterpret_cast<T*>(p); }
 };
 
+// Capacities of the sync-free extraction (fixed per geometry and keypoint cap; an image that exceeds
+// one is flagged and redone by the host-driven path).
+struct AsyncCaps {
+    uint32_t cand, ref, rank;   // extrema candidates, refined extrema (sorted), ranks oriented
+    int kp, nfeat;              // keypoint cap (largest max_kp of the batch), features selected
+};
+
 // Outcome of one tensor-core dense match (all pairs of the call).
 struct TcStats {
     long long rows = 0;            // query rows
@@ -135,6 +142,7 @@ struct Workspace {
     DevBuf img;                  // uploaded uint8 image
     DevBuf cand, refined, oriented;
     DevBuf keys_a, keys_b, vals_a, vals_b, sort_tmp;
+    DevBuf spread, take;         // sync-free extraction: spread scratch, selected keypoint fields
     DevBuf counters;             // [0] candidates, [1] refined, [2] oriented
     size_t cap_cand = 0, cap_ref = 0;
     // sorted, capped keypoints (structure of arrays)
@@ -163,6 +171,19 @@ struct fsb_ctx {
     fsb::DevBuf s_gb;      // guided batch scratch (addresses captured in gb_graph)
     fsb::GuidedGraph gb_graph;
     fsb::TcStats tc_stats{};                      // of the last tensor-core dense match
+    // sync-free batched extraction (fsb_sift_features_batch_d): chains of images, each with its own
+    // stream and workspace, captured as one CUDA graph and replayed while the call is unchanged
+    struct ExtractBatch {
+        std::vector<cudaStream_t> streams;
+        std::vector<fsb::Workspace*> ws;
+        std::vector<cudaEvent_t> join;
+        cudaEvent_t fork = nullptr;
+        fsb::GuidedGraph graph;
+        fsb::DevBuf status;
+        fsb::AsyncCaps caps{};
+        int h = 0, w = 0, warm_ref = 0;
+        long long redone = 0;   // images redone by the host-driven path
+    } xb;
     void* pinned = nullptr;
     size_t pinned_bytes = 0;
     // stage timers: event pairs recorded at stage boundaries while timing is on, read back lazily
@@ -227,6 +248,22 @@ int32_t run_describe(const Workspace& ws, int n, const float* d_x, const float* 
                      const float* d_angle, const int32_t* d_oct, const int32_t* d_layer, float* d_desc,
                      uint8_t* d_u8, cudaStream_t s);
 int32_t run_spread(const Workspace& ws, int nfeat, int32_t* d_sel, int* n_sel, fsb_ctx* ctx, cudaStream_t s);
+// Sync-free extraction (every count on the device; stream-capturable). Capacities are fixed per
+// geometry and keypoint cap; an image that exceeds one is flagged in counters[7] (ASYNC_*).
+constexpr uint32_t ASYNC_CAND_OVERFLOW = 1, ASYNC_REF_OVERFLOW = 2, ASYNC_ORIENT_INCOMPLETE = 4;
+constexpr int ASYNC_ORIENT_PASSES = 3;
+int32_t async_caps(const Workspace& ws, int max_kp, int nfeat, AsyncCaps* c);
+int32_t prepare_async(Workspace& ws, const AsyncCaps& c, cudaStream_t s);
+// max_kp (<= c.kp) is this image's keypoint cap
+int32_t run_detect_async(Workspace& ws, double contrast, double edge, const AsyncCaps& c, int max_kp, bool exact,
+                         cudaStream_t s);
+int32_t spread_async(Workspace& ws, const AsyncCaps& c, int nfeat, int32_t* d_sel, cudaStream_t s);
+int32_t run_orient_dev(const Workspace& ws, const Refined* ref, const uint32_t* order, uint32_t max_ranks,
+                       const uint32_t* d_range, Oriented* slots, uint32_t* cnt, uint32_t* d_total, bool exact,
+                       cudaStream_t s);
+int32_t run_describe_dev(const Workspace& ws, int cap, const int* d_n, const float* d_x, const float* d_y,
+                         const float* d_size, const float* d_angle, const int32_t* d_oct, const int32_t* d_layer,
+                         float* d_desc, uint8_t* d_u8, bool exact, cudaStream_t s);
 int32_t spread_dev(fsb_ctx* ctx, const float* d_x, const float* d_y, const float* d_resp, int n, float W, float H,
                    int nfeat, bool by_position, int32_t* d_sel, int* n_sel, cudaStream_t s);
 

@@ -277,15 +277,16 @@ int32_t run_ransac_h(const long long* d_off, int n_pairs, const double2* d_src, 
 //     system reduced by Gaussian elimination with partial pivoting to its two-dimensional null
 //     space F1, F2 (samples of lower rank are rejected), det(a F1 + (1 - a) F2) = 0 solved as a
 //     cubic: one to three candidates per sample;
-//   * a correspondence is an inlier when both squared distances to its epipolar lines (of x2 to
-//     F x1 and of x1 to F^T x2, in pixels) are at most thr^2; the candidate with the most inliers
-//     wins (ties: lower hypothesis, then lower root index: schedule-independent);
+//   * a correspondence is an inlier when its Sampson distance (the first-order geometric error of
+//     x2^T F x1 = 0, in pixels) is at most thr, the rule OpenCV's USAC_MAGSAC applies to the mask
+//     it returns; the candidate with the most inliers wins (ties: lower hypothesis, then lower root
+//     index: schedule-independent);
 //   * local optimisation: the normalised eight-point least squares over the winner's inliers (the
 //     smallest eigenvector of A^T A by cyclic Jacobi), rank 2 enforced by removing the smallest
 //     singular direction, kept while it does not lose inliers (two rounds);
 //   * F in pixels scaled to F33 = 1 (unit norm when F33 is near zero), the mask of its inliers.
-// MAGSAC++ scores hypotheses by marginalising over the noise scale; the threshold test here is
-// the plain consensus rule, so the masks agree statistically, not bit for bit.
+// MAGSAC++ scores hypotheses by marginalising over the noise scale; the score here is the plain
+// inlier count, and random samples differ, so the masks agree statistically, not bit for bit.
 namespace fsb {
 namespace {
 
@@ -424,15 +425,15 @@ __device__ void denorm_f(const double* f, const Norm& n1, const Norm& n2, double
         for (int j = 0; j < 3; ++j) out[3 * i + j] = T2t[3 * i] * A[j] + T2t[3 * i + 1] * A[3 + j] + T2t[3 * i + 2] * A[6 + j];
 }
 
-// both squared point-to-epipolar-line distances (pixels) of correspondence (x1, x2) at most thr2
+// squared Sampson distance (pixels) of correspondence (x1, x2) at most thr2:
+// (x2^T F x1)^2 <= thr2 ((F x1)_1^2 + (F x1)_2^2 + (F^T x2)_1^2 + (F^T x2)_2^2)
 __device__ __forceinline__ bool f_inlier(const double* F, double2 a, double2 b, double thr2) {
     const double l0 = F[0] * a.x + F[1] * a.y + F[2], l1 = F[3] * a.x + F[4] * a.y + F[5];
     const double l2 = F[6] * a.x + F[7] * a.y + F[8];
     const double m0 = F[0] * b.x + F[3] * b.y + F[6], m1 = F[1] * b.x + F[4] * b.y + F[7];
     const double e = b.x * l0 + b.y * l1 + l2;
-    const double e2 = e * e;
-    const double n1 = l0 * l0 + l1 * l1, n2 = m0 * m0 + m1 * m1;
-    return e2 <= thr2 * n1 && e2 <= thr2 * n2 && n1 > 0 && n2 > 0;
+    const double den = l0 * l0 + l1 * l1 + m0 * m0 + m1 * m1;
+    return den > 0 && e * e <= thr2 * den;
 }
 
 constexpr int FT = 256;

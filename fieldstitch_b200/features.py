@@ -116,6 +116,72 @@ def sift_gpu_batch(images, nfeats, streams=4, contrast=0.015, edge=12.0, exact=F
     return _batch(lambda j: sift_gpu_u8(j[0], j[1], contrast, edge, exact, device), jobs, streams)
 
 
+def sift_gpu_batch_d(images, nfeats, out_xy, out_u8, out_resp=None, chains=8, contrast=0.015, edge=12.0,
+                     exact=False, device=0):
+    """Batched feature extraction on device data with no host wait inside the batch
+    (fsb_sift_features_batch_d: one CUDA graph, `chains` images in flight). images: same-size
+    uint8 CUDA tensors; nfeats: one cap per image; out_xy[i] (>= nfeat, 2) float32, out_u8[i]
+    (>= nfeat, 128) uint8 and optionally out_resp[i] CUDA tensors. Returns the feature counts (host
+    list); equal to sift_gpu_u8 / fsb_sift_features_d image by image."""
+    import ctypes
+
+    import torch
+    n = len(images)
+    if n == 0:
+        return []
+    nf = list(nfeats) if np.ndim(nfeats) else [int(nfeats)] * n
+    h, w = images[0].shape
+    if any(tuple(im.shape) != (h, w) for im in images):
+        raise ValueError("the images of a batch share one size")
+    ctx = _lib.context(device)
+    Pv, Iv = ctypes.c_void_p * n, ctypes.c_int32 * n
+    counts = torch.empty(n, dtype=torch.int32, device=images[0].device)
+    h_counts = Iv()
+    prm = _lib.SiftParams(float(contrast), float(edge), 0, _lib.SIFT_EXACT_BLUR if exact else 0)
+    torch.cuda.current_stream(images[0].device).synchronize()
+    _lib.check(ctx.lib.fsb_sift_features_batch_d(
+        ctx.handle, n, Pv(*[im.data_ptr() for im in images]), h, w, images[0].stride(0), ctypes.byref(prm),
+        Iv(*[int(v) for v in nf]), Pv(*[t.data_ptr() for t in out_xy]),
+        Pv(*[t.data_ptr() for t in out_resp]) if out_resp is not None else None, Pv(*[t.data_ptr() for t in out_u8]),
+        ctypes.c_void_p(counts.data_ptr()), h_counts, int(chains)), "fsb_sift_features_batch_d")
+    return [h_counts[i] for i in range(n)]
+
+
+_BATCH_BUFS = {}
+
+
+def sift_gpu_u8_batch(images, nfeats, chains=8, contrast=0.015, edge=12.0, exact=False, device=0):
+    """sift_gpu_u8 of many same-size host images as one sync-free batch: the images go to the
+    device (asynchronously when they are in page-locked memory), one CUDA graph extracts them all
+    (fsb_sift_features_batch_d) and the results come back. Returns [(xy float32 (n,2), RootSIFT
+    uint8 (n,128), resp float32 (n,))], equal to sift_gpu_u8 image by image. The device buffers are
+    kept between calls of the same shape, so a repeated batch replays its graph."""
+    import torch
+    n = len(images)
+    if n == 0:
+        return []
+    nf = list(nfeats) if np.ndim(nfeats) else [int(nfeats)] * n
+    h, w = np.asarray(images[0]).shape
+    dev = torch.device("cuda", device)
+    nmax = max(1, max(int(v) for v in nf))
+    key = (n, h, w, nmax, device)
+    if key not in _BATCH_BUFS:
+        _BATCH_BUFS.clear()
+        _BATCH_BUFS[key] = {"img": torch.empty((n, h, w), dtype=torch.uint8, device=dev),
+                            "xy": torch.empty((n, nmax, 2), dtype=torch.float32, device=dev),
+                            "u8": torch.empty((n, nmax, 128), dtype=torch.uint8, device=dev),
+                            "rs": torch.empty((n, nmax), dtype=torch.float32, device=dev)}
+    b = _BATCH_BUFS[key]
+    for i, im in enumerate(images):
+        t = torch.from_numpy(np.ascontiguousarray(im, np.uint8))
+        b["img"][i].copy_(t, non_blocking=t.is_pinned())
+    counts = sift_gpu_batch_d([b["img"][i] for i in range(n)], nf, [b["xy"][i] for i in range(n)],
+                              [b["u8"][i] for i in range(n)], [b["rs"][i] for i in range(n)], chains, contrast,
+                              edge, exact, device)
+    return [(b["xy"][i, :c].cpu().numpy(), b["u8"][i, :c].cpu().numpy(), b["rs"][i, :c].cpu().numpy())
+            for i, c in enumerate(counts)]
+
+
 def clahe(gray, clip=2.0, tiles=(8, 8), device=0):
     """cv2.createCLAHE(clipLimit=clip, tileGridSize=tiles).apply(gray) on the device (the contrast
     equalisation of features.prepare, app/planesite/features.py:70-71): identical uint8 output."""

@@ -279,7 +279,7 @@ def find_homography_batch(problems, thr, iters=1024, seed=0, device=0):
 def find_fundamental_batch(problems, thr, iters=2048, seed=0, device=0):
     """Fundamental matrices of many pairs in one launch (matching._verify's
     cv2.findFundamentalMat(pi, pj, USAC_MAGSAC, thr, 0.999, 10000), app/planesite/matching.py:175-191,
-    batched): seven-point samples, inliers by both point-to-epipolar-line distances <= thr, eight-point
+    batched): seven-point samples, inliers by Sampson distance <= thr (OpenCV's MAGSAC mask rule), eight-point
     least-squares refinement. problems: list of (pi (n,2), pj (n,2)). Returns a list of (F (3,3)
     float64 or None, mask (n,1) uint8) per pair, as OpenCV returns them; None where a pair has fewer
     than 8 correspondences or no candidate with 8 inliers."""

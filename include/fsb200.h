@@ -150,11 +150,32 @@ int32_t fsb_sift_features_ex_d(fsb_ctx* ctx, const uint8_t* d_img, int32_t h, in
                                const fsb_sift_params* p, int32_t nfeat, float* d_xy, float* d_resp,
                                float* d_desc, uint8_t* d_rootsift, float* d_size, float* d_angle,
                                int32_t* d_octave, int32_t* n_out);
+/* fsb_sift_features_d over a batch of n_img same-size images in device memory (the per-photo
+   feature step of the reference's GPU worker, app/planesite/features.py:115-129 and 343-378, for a
+   batch), with no host wait inside the batch: every count stays on the device and each launch is
+   sized by a capacity fixed for the geometry, so the whole batch is one CUDA graph - `chains`
+   images in flight, each chain with its own stream and workspace - captured on the first call and
+   replayed while the arguments and buffers are unchanged. Image i: d_imgs[i] (h x w, row pitch
+   stride), nfeats[i] features; outputs d_xy[i] (nfeat*2 float32), d_resp[i] (nfeat float32,
+   nullable array), d_rootsift[i] (nfeat*128 uint8); d_counts (device, n_img int32) receives the
+   feature counts, h_counts (host, nullable) too. The first call for a geometry runs image 0 by
+   the host-driven path first (autotuning, capacities). The call waits once, at the end; an image
+   that exceeded a capacity is redone by the host-driven path, so the outputs always equal
+   fsb_sift_features_d's. */
+int32_t fsb_sift_features_batch_d(fsb_ctx* ctx, int32_t n_img, const uint8_t* const* d_imgs, int32_t h, int32_t w,
+                                  int32_t stride, const fsb_sift_params* p, const int32_t* nfeats, float* const* d_xy,
+                                  float* const* d_resp, uint8_t* const* d_rootsift, int32_t* d_counts,
+                                  int32_t* h_counts, int32_t chains);
 /* Prior prediction: projects n float32 points (d_xy, n*2) through the homography hm9 (host,
    row-major 3x3) into float64 positions d_out (n*2), adding the float32 offsets d_offset (n*2,
    nullable) - e.g. a GNSS/gimbal prior and its error. Identity hm9 converts to float64. */
 int32_t fsb_project_d(fsb_ctx* ctx, const float* d_xy, int32_t n, const double* hm9,
                       const float* d_offset, double* d_out);
+/* fsb_project_d for n_sets point sets (set k: d_xy[k], n[k] points, homography hm9 + 9k, offsets
+   d_offset[k] or none when d_offset is null, output d_out[k]), queued on the context's stream with
+   no host wait (later work on the same context sees the results). */
+int32_t fsb_project_batch_d(fsb_ctx* ctx, int32_t n_sets, const float* const* d_xy, const int32_t* n,
+                            const double* hm9, const float* const* d_offset, double* const* d_out);
 /* fsb_match_guided with every array in device memory; d_q, d_t capacity na. */
 int32_t fsb_match_guided_d(fsb_ctx* ctx, const double* d_pred, const uint8_t* d_a, int32_t na,
                            const double* d_bxy, const uint8_t* d_b, int32_t nb, double w_b, double h_b,
@@ -311,7 +332,7 @@ int32_t fsb_find_homography_batch(fsb_ctx* ctx, int32_t n_pairs, const int64_t* 
    app/planesite/matching.py:175-191, cv2.findFundamentalMat(pi, pj, USAC_MAGSAC, thr, 0.999,
    10000)) for n_pairs pairs in one launch: pair p's correspondences are src (image i) / dst
    (image j) rows offsets[p] .. offsets[p+1] - 1 (float64 (x, y)); `iters` seven-point samples per
-   pair (seeded, deterministic); inliers: both squared distances to the epipolar lines <= thr^2;
+   pair (seeded, deterministic); inliers: Sampson distance <= thr (OpenCV's USAC_MAGSAC mask rule);
    the best candidate refined by eight-point least squares over its inliers. F (9 per pair,
    row-major, x_j^T F x_i = 0, F33 = 1 or unit norm; zeros when a pair has fewer than 8
    correspondences or no candidate with 8 inliers), mask (one byte per correspondence) and

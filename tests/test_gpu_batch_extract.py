@@ -1,0 +1,58 @@
+"""The sync-free batched extraction (fsb_sift_features_batch_d: every count on the device, the batch
+captured as one CUDA graph with several images in flight) returns exactly what the host-driven
+per-image path (fsb_sift_features_d, features.sift_gpu's sequence) returns: the same feature
+counts, coordinates, responses and RootSIFT bytes, on the first call (capture) and on replays,
+for uneven keypoint caps including caps above the keypoint count and a flat image."""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def _per_image(F, img, nfeat):
+    xy, u8, resp = F.features.sift_gpu_u8(img, nfeat)
+    return xy, u8, resp
+
+
+@pytest.mark.parametrize("hw,chains", [((989, 1320), 3), ((495, 660), 8)])
+def test_batch_extraction_equals_per_image(hw, chains):
+    import torch
+
+    import fieldstitch_b200 as F
+    from fieldstitch_b200 import synth
+    h, w = hw
+    dev = torch.device("cuda", 0)
+    imgs = [synth.synth_image(h, w, 300 + k) for k in range(7)]
+    imgs[5] = np.full((h, w), 90, np.uint8)          # no keypoints
+    nfeats = [3000, 500, 12000, 800, 20000, 1000, 64]
+    d_imgs = [torch.from_numpy(im).to(dev) for im in imgs]
+    nmax = max(nfeats)
+    xy = [torch.zeros((nmax, 2), dtype=torch.float32, device=dev) for _ in imgs]
+    u8 = [torch.zeros((nmax, 128), dtype=torch.uint8, device=dev) for _ in imgs]
+    rs = [torch.zeros(nmax, dtype=torch.float32, device=dev) for _ in imgs]
+    want = [_per_image(F, im, nf) for im, nf in zip(imgs, nfeats)]
+    for rep in range(3):   # capture, then replays
+        for t in xy + u8 + rs:
+            t.zero_()
+        counts = F.features.sift_gpu_batch_d(d_imgs, nfeats, xy, u8, rs, chains=chains)
+        for k, (wxy, wu8, wrs) in enumerate(want):
+            n = len(wxy)
+            assert counts[k] == n, (rep, k, counts[k], n)
+            np.testing.assert_array_equal(xy[k][:n].cpu().numpy(), wxy)
+            np.testing.assert_array_equal(u8[k][:n].cpu().numpy(), wu8)
+            np.testing.assert_array_equal(rs[k][:n].cpu().numpy(), wrs)
+    assert counts[5] == 0 and counts[2] > 0
+
+
+def test_batch_extraction_rejects_bad_arguments():
+    import ctypes
+
+    from fieldstitch_b200 import _lib
+    ctx = _lib.context(0)
+    prm = _lib.SiftParams(0.015, 12.0, 0, 0)
+    P1, I1 = ctypes.c_void_p * 1, ctypes.c_int32 * 1
+    st = ctx.lib.fsb_sift_features_batch_d(ctx.handle, 1, P1(16), 100, 100, 100, ctypes.byref(prm), I1(10), P1(16),
+                                           None, P1(16), ctypes.c_void_p(16), None, 0)
+    assert st == 1 and b"chains" in ctx.lib.fsb_last_error()
+    assert ctx.lib.fsb_sift_features_batch_d(ctx.handle, 0, None, 0, 0, 0, ctypes.byref(prm), None, None, None,
+                                             None, None, None, 4) == 0

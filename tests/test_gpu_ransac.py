@@ -72,7 +72,7 @@ def test_match_pair_with_device_ransac(match_golden, tmp_path):
     assert len(ref & got) >= 0.95 * len(ref) and abs(n_in - int(g["guided/n_in"])) <= 0.05 * int(g["guided/n_in"])
 
 
-def _two_view(seed, n, outliers, noise=0.5):
+def _two_view(seed, n, outliers, noise=0.25):
     """A seeded two-view scene with relief (points 0-30 m above ground, cameras at 100 m, 20 m
     apart, a few degrees of relative rotation), pixel correspondences with noise and outliers."""
     rng = np.random.default_rng(seed)
