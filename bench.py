@@ -908,16 +908,21 @@ def run_fsb(args):
             ua = B["u8"][0][:na_].cpu().numpy()
             bxy = B["bxy"][:nb_].cpu().numpy()
             ub = B["u8"][1][:nb_].cpu().numpy()
-            q_ref, t_ref = matching_ref.guided_from_pred(pred, ua, bxy, ub, (w, h), RADIUS, KC, RATIO)
             n_ = m_cnt[i]
             q_g, t_g = B["q"][:n_].cpu().numpy(), B["t"][:n_].cpu().numpy()
+            q_ref, t_ref = matching_ref.guided_from_pred(pred, ua, bxy, ub, (w, h), RADIUS, KC, RATIO, ties="index")
             same = bool(np.array_equal(q_g, q_ref) and np.array_equal(t_g, t_ref))
+            q_kd, t_kd = matching_ref.guided_from_pred(pred, ua, bxy, ub, (w, h), RADIUS, KC, RATIO)
+            shared = len(set(zip(q_g.tolist(), t_g.tolist())) & set(zip(q_kd.tolist(), t_kd.tolist())))
             ok = ok and same
             parity["pairs"].append({"pair": i, "keypoints": [int(na_), int(nb_)], "matches_gpu": int(n_),
-                                    "matches_oracle": int(len(q_ref)), "identical": same})
+                                    "matches_oracle": int(len(q_ref)), "identical": same,
+                                    "matches_oracle_kdtree_ties": int(len(q_kd)), "shared_with_kdtree_ties": shared})
         parity["parity_checked"] = ok
         parity["what"] = ("the batched guided matches of pairs 0 and 1 of the last timed step equal the oracle's "
-                          "guided matcher on the same keypoints, descriptors and predictions")
+                          "guided matcher on the same keypoints, descriptors and predictions, equal-distance "
+                          "candidates at the kc-th place taken by index as the device does (with cKDTree's own "
+                          "order among them the shared count is reported beside)")
     except Exception as e:  # reported in the line, never hidden
         parity["error"] = ("%s: %s" % (type(e).__name__, e))[:200]
 

@@ -1077,34 +1077,6 @@ __device__ __forceinline__ void s_fix_edges(const StripArgs& a, float* ring0, in
     }
 }
 
-// Gradient of the float32 path for two pixels at once: fast_grad's operations in fast_grad's order,
-// the multiplications and additions packed in pairs (identical roundings).
-__device__ __forceinline__ void fast_grad2(float2 dx, float2 dy, float2& mag, float2& ang) {
-    const float2 d2 = __fadd2_rn(__fmul2_rn(dx, dx), __fmul2_rn(dy, dy));
-    const float2 rs = make_float2(d2.x > 0.f ? rsqrtf(d2.x) : 0.f, d2.y > 0.f ? rsqrtf(d2.y) : 0.f);
-    const float2 m = __fmul2_rn(d2, rs);
-    mag = make_float2(d2.x > 0.f ? m.x : 0.f, d2.y > 0.f ? m.y : 0.f);
-    const float ax0 = fabsf(dx.x), ay0 = fabsf(dy.x), ax1 = fabsf(dx.y), ay1 = fabsf(dy.y);
-    const float mx0 = fmaxf(ax0, ay0), mn0 = fminf(ax0, ay0), mx1 = fmaxf(ax1, ay1), mn1 = fminf(ax1, ay1);
-    const float2 t = make_float2(mx0 > 0.f ? __fdividef(mn0, mx0) : 0.f, mx1 > 0.f ? __fdividef(mn1, mx1) : 0.f);
-    const float2 z = __fmul2_rn(t, t);
-    float2 p = make_float2(-2.323089093e-01f, -2.323089093e-01f);
-    p = __ffma2_rn(p, z, make_float2(1.252652928e+00f, 1.252652928e+00f));
-    p = __ffma2_rn(p, z, make_float2(-3.203537344e+00f, -3.203537344e+00f));
-    p = __ffma2_rn(p, z, make_float2(5.524570187e+00f, 5.524570187e+00f));
-    p = __ffma2_rn(p, z, make_float2(-7.969057098e+00f, -7.969057098e+00f));
-    p = __ffma2_rn(p, z, make_float2(1.142854019e+01f, 1.142854019e+01f));
-    p = __ffma2_rn(p, z, make_float2(-1.909660354e+01f, -1.909660354e+01f));
-    p = __ffma2_rn(p, z, make_float2(5.729574144e+01f, 5.729574144e+01f));
-    float2 v = __fmul2_rn(p, t);
-    float2 f = __fadd2_rn(make_float2(90.f, 90.f), make_float2(-v.x, -v.y));
-    v = make_float2(ay0 > ax0 ? f.x : v.x, ay1 > ax1 ? f.y : v.y);
-    f = __fadd2_rn(make_float2(180.f, 180.f), make_float2(-v.x, -v.y));
-    v = make_float2(dx.x < 0.f ? f.x : v.x, dx.y < 0.f ? f.y : v.y);
-    f = __fadd2_rn(make_float2(360.f, 360.f), make_float2(-v.x, -v.y));
-    ang = make_float2(dy.x < 0.f ? f.x : v.x, dy.y < 0.f ? f.y : v.y);
-}
-
 __device__ __forceinline__ void s_store4(float* p, float4 v, bool vec, int left) {
     if (vec) {
         *reinterpret_cast<float4*>(p) = v;
@@ -1173,12 +1145,15 @@ __device__ __forceinline__ void s_grad_item(const float* __restrict__ ring, cons
         dya = make_float2(dyv[0], dyv[1]);
         dyb = make_float2(dyv[2], dyv[3]);
     }
-    float2 ma, mb, na, nb;
-    fast_grad2(dxa, dya, ma, na);
-    fast_grad2(dxb, dyb, mb, nb);
+    // the scalar gradient of the other engines (same code, same roundings)
+    float mg[4], an[4];
+    fast_grad(dxa.x, dya.x, mg[0], an[0]);
+    fast_grad(dxa.y, dya.y, mg[1], an[1]);
+    fast_grad(dxb.x, dyb.x, mg[2], an[2]);
+    fast_grad(dxb.y, dyb.y, mg[3], an[3]);
     const size_t at = (size_t)y * a.C + x;
-    s_store4(a.mag[I - 1] + at, make_float4(ma.x, ma.y, mb.x, mb.y), k.vec, a.C - x);
-    s_store4(a.ang[I - 1] + at, make_float4(na.x, na.y, nb.x, nb.y), k.vec, a.C - x);
+    s_store4(a.mag[I - 1] + at, make_float4(mg[0], mg[1], mg[2], mg[3]), k.vec, a.C - x);
+    s_store4(a.ang[I - 1] + at, make_float4(an[0], an[1], an[2], an[3]), k.vec, a.C - x);
     if (I == 3 && a.down && !(y & 1)) {
         float* o = a.down + (size_t)(y >> 1) * a.down_cols + (x >> 1);
         o[0] = c0.x;

@@ -178,8 +178,14 @@ def sift_gpu_u8_batch(images, nfeats, chains=8, contrast=0.015, edge=12.0, exact
     counts = sift_gpu_batch_d([b["img"][i] for i in range(n)], nf, [b["xy"][i] for i in range(n)],
                               [b["u8"][i] for i in range(n)], [b["rs"][i] for i in range(n)], chains, contrast,
                               edge, exact, device)
-    return [(b["xy"][i, :c].cpu().numpy(), b["u8"][i, :c].cpu().numpy(), b["rs"][i, :c].cpu().numpy())
-            for i, c in enumerate(counts)]
+    # the valid rows of every image gathered on the device, one copy per kind back to the host
+    if sum(counts) == 0:
+        return [(np.zeros((0, 2), np.float32), np.zeros((0, 128), np.uint8), np.zeros(0, np.float32)) for _ in counts]
+    xy = torch.cat([b["xy"][i, :c] for i, c in enumerate(counts)]).cpu().numpy()
+    u8 = torch.cat([b["u8"][i, :c] for i, c in enumerate(counts)]).cpu().numpy()
+    rs = torch.cat([b["rs"][i, :c] for i, c in enumerate(counts)]).cpu().numpy()
+    cut = np.cumsum(counts)[:-1]
+    return list(zip(np.split(xy, cut), np.split(u8, cut), np.split(rs, cut)))
 
 
 def clahe(gray, clip=2.0, tiles=(8, 8), device=0):

@@ -121,27 +121,66 @@ def guided_from_pred_batch_d(problems, radius, kc, ratio, device=0, out=None):
     return [(o[0][:cnt[i]], o[1][:cnt[i]]) for i, o in enumerate(out)]
 
 
+_STAGE = {}
+
+
 def match_guided_batch(problems, radius, kc=None, ratio=0.85, device=0):
     """Batched guided matching on host arrays: ``problems[p]`` = (pred (na,2), a_desc (na,128),
     b_xy (nb,2), b_desc (nb,128), (w_b, h_b)) as ``guided_from_pred`` takes them (descriptors uint8
-    or their float32 values). The data go to the device once and every pair runs in one
-    ``guided_from_pred_batch_d`` call; returns [(q, t)] int64 numpy arrays per pair, each equal to
-    ``guided_from_pred`` on that pair."""
+    or their float32 values). The data go to the device in one copy per kind into buffers kept
+    between calls with the same sizes (so a repeated batch replays its graph), every pair runs in
+    one ``guided_from_pred_batch_d`` call and the results come back in one copy; returns [(q, t)]
+    int64 numpy arrays per pair, each equal to ``guided_from_pred`` on that pair."""
     import torch
-    dev = torch.device("cuda", device)
-    staged = []
-    for pred, a_desc, b_xy, b_desc, wh in problems:
-        a = _lib.as_u8_desc(a_desc, "A desc")
-        b = _lib.as_u8_desc(b_desc, "B desc")
-        pr = np.ascontiguousarray(np.asarray(pred, np.float64).reshape(-1, 2))
-        bx = np.ascontiguousarray(np.asarray(b_xy, np.float64).reshape(-1, 2))
-        staged.append((torch.from_numpy(pr).to(dev), torch.from_numpy(np.ascontiguousarray(a)).to(dev),
-                       torch.from_numpy(bx).to(dev), torch.from_numpy(np.ascontiguousarray(b)).to(dev),
-                       (float(wh[0]), float(wh[1]))))
     if kc is not None and int(kc) < 1:
         raise ValueError("kc must be >= 1 or None")
-    res = guided_from_pred_batch_d(staged, radius, kc, ratio, device=device)
-    return [(q.cpu().numpy().astype(np.int64), t.cpu().numpy().astype(np.int64)) for q, t in res]
+    dev = torch.device("cuda", device)
+    n = len(problems)
+    if n == 0:
+        return []
+    preds, As, bxys, Bs, whs = [], [], [], [], []
+    for pred, a_desc, b_xy, b_desc, wh in problems:
+        As.append(np.ascontiguousarray(_lib.as_u8_desc(a_desc, "A desc")))
+        Bs.append(np.ascontiguousarray(_lib.as_u8_desc(b_desc, "B desc")))
+        preds.append(np.asarray(pred, np.float64).reshape(-1, 2))
+        bxys.append(np.asarray(b_xy, np.float64).reshape(-1, 2))
+        whs.append((float(wh[0]), float(wh[1])))
+        if len(preds[-1]) != len(As[-1]) or len(bxys[-1]) != len(Bs[-1]):
+            raise ValueError("positions and descriptors differ in length")
+    na = [len(a) for a in As]
+    nb = [len(b) for b in Bs]
+    key = (device, tuple(na), tuple(nb))
+    if key not in _STAGE:
+        _STAGE.clear()
+        A, Bn = max(sum(na), 1), max(sum(nb), 1)
+        _STAGE[key] = {"pred": torch.empty((A, 2), dtype=torch.float64, device=dev),
+                       "a": torch.empty((A, 128), dtype=torch.uint8, device=dev),
+                       "bxy": torch.empty((Bn, 2), dtype=torch.float64, device=dev),
+                       "b": torch.empty((Bn, 128), dtype=torch.uint8, device=dev),
+                       "q": torch.empty(A + n, dtype=torch.int64, device=dev),
+                       "t": torch.empty(A + n, dtype=torch.int64, device=dev)}
+    st = _STAGE[key]
+    oa = np.r_[0, np.cumsum(na)].astype(np.int64)
+    ob = np.r_[0, np.cumsum(nb)].astype(np.int64)
+    st["pred"][:oa[-1]].copy_(torch.from_numpy(np.concatenate(preds) if oa[-1] else np.zeros((0, 2))))
+    st["a"][:oa[-1]].copy_(torch.from_numpy(np.concatenate(As) if oa[-1] else np.zeros((0, 128), np.uint8)))
+    st["bxy"][:ob[-1]].copy_(torch.from_numpy(np.concatenate(bxys) if ob[-1] else np.zeros((0, 2))))
+    st["b"][:ob[-1]].copy_(torch.from_numpy(np.concatenate(Bs) if ob[-1] else np.zeros((0, 128), np.uint8)))
+    staged, out = [], []
+    for p in range(n):
+        staged.append((st["pred"][oa[p]:oa[p + 1]], st["a"][oa[p]:oa[p + 1]], st["bxy"][ob[p]:ob[p + 1]],
+                       st["b"][ob[p]:ob[p + 1]], whs[p]))
+        # output slots: na[p] + 1 entries per pair (at least one, so that every pointer is distinct)
+        out.append((st["q"][oa[p] + p:oa[p + 1] + p + 1], st["t"][oa[p] + p:oa[p + 1] + p + 1]))
+    res = guided_from_pred_batch_d(staged, radius, kc, ratio, device=device, out=out)
+    lens = [len(q) for q, _ in res]
+    if sum(lens) == 0:
+        e = np.zeros(0, np.int64)
+        return [(e, e) for _ in range(n)]
+    qa = torch.cat([q for q, _ in res]).cpu().numpy()
+    ta = torch.cat([t for _, t in res]).cpu().numpy()
+    cut = np.cumsum(lens)[:-1]
+    return list(zip(np.split(qa, cut), np.split(ta, cut)))
 
 
 def tc_stats(device=0):

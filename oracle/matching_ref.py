@@ -50,11 +50,15 @@ def perspective(xy, Hm):
     return cv2.perspectiveTransform(np.asarray(xy, np.float64).reshape(-1, 1, 2), np.asarray(Hm, np.float64)).reshape(-1, 2)
 
 
-def guided_from_pred(pred, a_desc, b_und, b_desc, wh_b, radius, kc, ratio, a_norm=None, b_norm=None):
+def guided_from_pred(pred, a_desc, b_und, b_desc, wh_b, radius, kc, ratio, a_norm=None, b_norm=None,
+                     ties="tree"):
     """Guided matching given predicted positions of A's keypoints in B (matching.py:116-152):
     keep predictions inside B +- radius; candidates = the kc nearest B keypoints strictly within
     radius (cKDTree); float32 distances; top-2 ratio test; one-to-one filter.
-    ``kc=None`` takes every B keypoint within radius."""
+    ``kc=None`` takes every B keypoint within radius. ``ties``: "tree" keeps cKDTree's own order
+    among B keypoints at equal distance (the reference's call); "index" keeps the smaller index
+    (SIFT lists several orientations of one position, so equal distances at the kc-th candidate
+    are common on real keypoints; cKDTree's order among them is implementation-defined)."""
     from scipy.spatial import cKDTree
     a_desc = np.asarray(a_desc, np.float32)
     b_desc = np.asarray(b_desc, np.float32)
@@ -68,8 +72,16 @@ def guided_from_pred(pred, a_desc, b_und, b_desc, wh_b, radius, kc, ratio, a_nor
         return np.zeros(0, np.int64), np.zeros(0, np.int64)
     tree = cKDTree(b_und)
     k = nb if kc is None else min(kc, nb)
-    dist, idx = tree.query(pred[inside], k=k, distance_upper_bound=radius)
-    if k == 1:
+    if ties == "index" and kc is not None and k < nb:
+        kq = min(nb, k + 32)
+        dist, idx = tree.query(pred[inside], k=kq, distance_upper_bound=radius)
+        if kq == 1:
+            dist, idx = dist[:, None], idx[:, None]
+        order = np.lexsort((np.where(idx < nb, idx, nb), dist))[:, :k]
+        idx = np.take_along_axis(idx, order, axis=1)
+    else:
+        dist, idx = tree.query(pred[inside], k=k, distance_upper_bound=radius)
+    if idx.ndim == 1:
         idx = idx[:, None]
     valid = idx < nb
     has = valid.any(1)

@@ -56,3 +56,19 @@ def test_batch_extraction_rejects_bad_arguments():
     assert st == 1 and b"chains" in ctx.lib.fsb_last_error()
     assert ctx.lib.fsb_sift_features_batch_d(ctx.handle, 0, None, 0, 0, 0, ctypes.byref(prm), None, None, None,
                                              None, None, None, 4) == 0
+
+
+def test_host_batch_api_equals_per_image():
+    """features.sift_gpu_u8_batch (host arrays in and out: one upload, one graph, one download per
+    kind) returns sift_gpu_u8's output image by image, on two calls in a row."""
+    import fieldstitch_b200 as F
+    from fieldstitch_b200 import synth
+    imgs = [synth.synth_image(600, 800, 500 + k) for k in range(5)]
+    nfeats = [2000, 300, 5000, 50, 1200]
+    want = [_per_image(F, im, nf) for im, nf in zip(imgs, nfeats)]
+    for _ in range(2):
+        got = F.features.sift_gpu_u8_batch(imgs, nfeats, chains=2)
+        for (gxy, gu8, grs), (wxy, wu8, wrs) in zip(got, want):
+            np.testing.assert_array_equal(gxy, wxy)
+            np.testing.assert_array_equal(gu8, wu8)
+            np.testing.assert_array_equal(grs, wrs)
