@@ -70,7 +70,8 @@ def parse():
                    help="pairs for the learned match filter (3/4 train, 1/4 held out; 0: skip)")
     p.add_argument("--flight-lines", type=int, default=20,
                    help="synthetic flight: lines x frames per line (20: 400 frames; 0: skip)")
-    p.add_argument("--flight-train", type=int, default=200, help="synthetic flight: pairs that train the filter")
+    p.add_argument("--flight-train", type=int, default=500,
+                   help="synthetic flight: pairs whose candidates train the learned filter (the rest are held out)")
     return p.parse_args()
 
 
@@ -633,8 +634,12 @@ def synthetic_flight(args, local):
         feats.append(ft[ok])
         labs.append(torch.from_numpy(lab).to(dev)[ok])
     mf = MF.MatchFilter(device=local)
-    mf.fit(torch.cat(feats), torch.cat(labs), epochs=30, batch=8192, lr=2e-3, seed=args.seed)
+    train_feat, train_lab = torch.cat(feats), torch.cat(labs)
     torch.cuda.synchronize()
+    t_fit = time.perf_counter()
+    mf.fit(train_feat, train_lab, epochs=30, batch=8192, lr=2e-3, seed=args.seed)
+    torch.cuda.synchronize()
+    fit_s = time.perf_counter() - t_fit
 
     acc = {"ratio_test": [0, 0], "mlp_filter": [0, 0]}
     pos = 0
@@ -688,6 +693,8 @@ def synthetic_flight(args, local):
             "matches": {"total": n_match, "within_3px_of_truth": n_good,
                         "pairs_with_20_correct": pairs_ok, "precision_vs_truth": n_good / n_match if n_match else 0.0},
             "learned_filter": {"train_pairs": n_train, "held_out_pairs": P - n_train,
+                               "train_correspondences": int(len(train_lab)), "train_seconds": fit_s,
+                               "labels": "the plain pipeline's RANSAC homography (cv2, 3 px) of the ratio-test matches",
                                "vs_true_homography": {"ratio_test": prf("ratio_test"), "mlp_filter": prf("mlp_filter")},
                                "filter_path_ms": ms_filter,
                                "e2e_with_filter_pairs_per_s": P / ((ms_batched + ms_filter) / 1000.0),
@@ -955,21 +962,20 @@ def run_fsb(args):
             res = list(pool.map(e2e_pair, range(len(pairs))))
             return sum(r[0] for r in res), sum(r[1] for r in res)
 
+        e_imgs = [im for a, b in host for im in (a, b)]
+        e_nfs = [pairs[i][3 + k] for i in range(len(pairs)) for k in range(2)]
+        e_pairs = [(2 * i, 2 * i + 1) for i in range(len(pairs))]
+        e_priors = [pairs[i][2] for i in range(len(pairs))]
+        e_off = [noise[i].astype(np.float32) for i in range(len(pairs))]
+
         def e2e_step_batch():
-            """features.sift_gpu_u8_batch (every image of the step: one upload, one graph, one download)
-            then matching.match_guided_batch (every pair: one upload, one graph call, one download)."""
-            imgs = [im for a, b in host for im in (a, b)]
-            nfs = [pairs[i][3 + k] for i in range(len(pairs)) for k in range(2)]
-            feats = F.features.sift_gpu_u8_batch(imgs, nfs, chains=args.chains, device=local)
-            probs, h2d, d2h = [], sum(im.nbytes for im in imgs), 0
-            for i in range(len(pairs)):
-                (xa, ua, ra), (xb, ub, rb) = feats[2 * i], feats[2 * i + 1]
-                pr = synth.apply_homography(pairs[i][2], xa) + noise[i][:len(xa)]
-                probs.append((pr, ua, xb.astype(np.float64), ub, (w, h)))
-                d2h += (len(xa) + len(xb)) * (8 + 4 + 128)
-                h2d += pr.nbytes + ua.nbytes + 16 * len(xb) + ub.nbytes
-            res = F.matching.match_guided_batch(probs, RADIUS, KC, RATIO, device=local)
-            d2h += sum(16 * len(q) for q, _ in res)
+            """frontend.extract_and_match: the step's host images to the device, one graph extracting
+            every image, the priors projected on the device, one graph matching every pair, the match
+            lists back to the host."""
+            res = F.frontend.extract_and_match(e_imgs, e_nfs, e_pairs, e_priors, RADIUS, KC, RATIO, offsets=e_off,
+                                               chains=args.chains, device=local)
+            h2d = sum(im.nbytes for im in e_imgs) + 16 * len(e_pairs) * max(e_nfs) + 72 * len(e_pairs)
+            d2h = sum(16 * len(q) for q, _ in res) + 4 * len(e_imgs)
             return h2d, d2h
 
         e2e_step = e2e_step_batch if args.extract == "graph" else e2e_step_threads
@@ -995,11 +1001,14 @@ def run_fsb(args):
         ms_e2e = max_over_ranks(ms_e2e, dist, dev)
         e2e = {"value": job_rate(world, args.pairs, ms_e2e), "unit": "pairs/s", "h2d_bytes_per_step": int(h2d),
                "d2h_bytes_per_step": int(d2h), "ms_per_step": ms_e2e, "steps": ksteps,
-               "api": ("features.sift_gpu_u8_batch (one graph for every image) + matching.match_guided_batch "
-                       "(one graph for every pair)" if args.extract == "graph" else
+               "api": ("frontend.extract_and_match: host images in, one graph for every image, priors projected "
+                       "on the device, one graph for every pair, match lists out" if args.extract == "graph" else
                        "features.sift_gpu_u8 + matching.guided_from_pred, %d host threads" % args.streams),
-               "host_inputs": "images in pinned host memory; keypoints / descriptors between the two calls in "
-                              "the numpy arrays the API returns"}
+               "host_inputs": ("images in pinned host memory, the prior homographies and their errors in host "
+                               "memory; the features stay on the device between extraction and matching"
+                               if args.extract == "graph" else
+                               "images in pinned host memory; keypoints / descriptors between the two calls in "
+                               "the numpy arrays the API returns")}
 
     # ---- roofline of the dominant stage (pyramid): CUDA events on the library stream, one stream
     # alone (8 images), so the per-image time is not inflated by the other streams' kernels

@@ -200,32 +200,47 @@ __device__ __forceinline__ void hpass(const float2* t2, float* out, int yb, int 
     *reinterpret_cast<float2*>(out + s1 * P + 2 * g) = make_float2(o[0].y, o[1].y);
 }
 
-// Gradient magnitude and direction (degrees in [0, 360)) for the default (float32) pyramid:
-// magnitude through the reciprocal square root (within a few ulps of sqrt), direction by octant
-// reduction to t = min/max in [0, 1] and an odd polynomial for atan(t) in degrees. The
-// coefficients were fitted here by iteratively reweighted least squares on Chebyshev nodes
-// (max error 2.2e-6 deg; 7.4e-6 deg with float32 evaluation), so the angle stays well inside the
+// Gradient magnitude and direction (degrees in [0, 360)) of four pixels for the default (float32)
+// pyramid: magnitude through the reciprocal square root (within a few ulps of sqrt), direction by
+// octant reduction to t = min/max in [0, 1] and an odd polynomial for atan(t) in degrees. The
+// coefficients were fitted here by iteratively reweighted least squares on Chebyshev nodes (max
+// error 2.2e-6 deg; 7.4e-6 deg with float32 evaluation), so the angle stays well inside the
 // reference's 0.1 deg keypoint tolerance. atan2(0, 0) = 0 as in the reference (border pixels).
-__device__ __forceinline__ void fast_grad(float dx, float dy, float& mag, float& ang) {
-    const float d2 = __fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dy, dy));
-    mag = d2 > 0.f ? d2 * rsqrtf(d2) : 0.f;
-    const float ax = fabsf(dx), ay = fabsf(dy);
-    const float mx = fmaxf(ax, ay), mn = fminf(ax, ay);
-    const float t = mx > 0.f ? __fdividef(mn, mx) : 0.f;
-    const float z = t * t;
-    float p = -2.323089093e-01f;
-    p = fmaf(p, z, 1.252652928e+00f);
-    p = fmaf(p, z, -3.203537344e+00f);
-    p = fmaf(p, z, 5.524570187e+00f);
-    p = fmaf(p, z, -7.969057098e+00f);
-    p = fmaf(p, z, 1.142854019e+01f);
-    p = fmaf(p, z, -1.909660354e+01f);
-    p = fmaf(p, z, 5.729574144e+01f);
-    float a = p * t;                       // atan(min/max) in degrees, [0, 45]
-    if (ay > ax) a = 90.f - a;
-    if (dx < 0.f) a = 180.f - a;
-    if (dy < 0.f) a = 360.f - a;           // atan2 < 0 maps to a + 360 (may round to 360, as there)
-    ang = a;
+// Pixels go through in pairs with packed FP32x2 arithmetic; every multiply and add is explicitly
+// rounded (nothing is contracted into a fused multiply-add), so each engine that calls this
+// function computes the same bits.
+__device__ __forceinline__ void fast_grad4(const float (&dx)[4], const float (&dy)[4], float (&mag)[4],
+                                           float (&ang)[4]) {
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+        const float2 X = make_float2(dx[2 * h], dx[2 * h + 1]), Y = make_float2(dy[2 * h], dy[2 * h + 1]);
+        const float2 d2 = __fadd2_rn(__fmul2_rn(X, X), __fmul2_rn(Y, Y));
+        const float2 rs = make_float2(d2.x > 0.f ? rsqrtf(d2.x) : 0.f, d2.y > 0.f ? rsqrtf(d2.y) : 0.f);
+        const float2 m = __fmul2_rn(d2, rs);
+        const float ax0 = fabsf(X.x), ay0 = fabsf(Y.x), ax1 = fabsf(X.y), ay1 = fabsf(Y.y);
+        const float mx0 = fmaxf(ax0, ay0), mn0 = fminf(ax0, ay0), mx1 = fmaxf(ax1, ay1), mn1 = fminf(ax1, ay1);
+        const float2 t = make_float2(mx0 > 0.f ? __fdividef(mn0, mx0) : 0.f, mx1 > 0.f ? __fdividef(mn1, mx1) : 0.f);
+        const float2 z = __fmul2_rn(t, t);
+        float2 p = make_float2(-2.323089093e-01f, -2.323089093e-01f);
+        p = __ffma2_rn(p, z, make_float2(1.252652928e+00f, 1.252652928e+00f));
+        p = __ffma2_rn(p, z, make_float2(-3.203537344e+00f, -3.203537344e+00f));
+        p = __ffma2_rn(p, z, make_float2(5.524570187e+00f, 5.524570187e+00f));
+        p = __ffma2_rn(p, z, make_float2(-7.969057098e+00f, -7.969057098e+00f));
+        p = __ffma2_rn(p, z, make_float2(1.142854019e+01f, 1.142854019e+01f));
+        p = __ffma2_rn(p, z, make_float2(-1.909660354e+01f, -1.909660354e+01f));
+        p = __ffma2_rn(p, z, make_float2(5.729574144e+01f, 5.729574144e+01f));
+        float2 a = __fmul2_rn(p, t);   // atan(min/max) in degrees, [0, 45]
+        float2 f = __fadd2_rn(make_float2(90.f, 90.f), make_float2(-a.x, -a.y));
+        a = make_float2(ay0 > ax0 ? f.x : a.x, ay1 > ax1 ? f.y : a.y);
+        f = __fadd2_rn(make_float2(180.f, 180.f), make_float2(-a.x, -a.y));
+        a = make_float2(X.x < 0.f ? f.x : a.x, X.y < 0.f ? f.y : a.y);
+        f = __fadd2_rn(make_float2(360.f, 360.f), make_float2(-a.x, -a.y));   // atan2 < 0 maps to a + 360
+        a = make_float2(Y.x < 0.f ? f.x : a.x, Y.y < 0.f ? f.y : a.y);
+        mag[2 * h] = m.x;
+        mag[2 * h + 1] = m.y;
+        ang[2 * h] = a.x;
+        ang[2 * h + 1] = a.y;
+    }
 }
 
 // Gradient magnitude and angle at image row yy, columns x .. x+3, from a shared plane of pitch P
@@ -245,8 +260,7 @@ __device__ __forceinline__ void grad4(const float* ctr, int yy, int x, int R, in
         for (int k = 0; k < 4; ++k)
             if (!(yy > 0 && yy < R - 1 && x + k > 0 && x + k < C - 1)) dx[k] = dy[k] = 0.f;
     }
-#pragma unroll
-    for (int k = 0; k < 4; ++k) fast_grad(dx[k], dy[k], mg[k], an[k]);
+    fast_grad4(dx, dy, mg, an);
 }
 
 // DoG of stage I (L_I - L_{I-1}), gradient of L_{I-1} (I = 2..4), L_3[::2, ::2] (I = 4)
@@ -278,17 +292,17 @@ __device__ __forceinline__ void epilogue(const float* prev, const float* cur, co
     if (I >= 2 && I <= 4) {
         const float* up = prev + wrap<PR>(ps + PR - 1) * PP + 4 * q + hp;
         const float* dn = prev + wrap<PR>(ps + 1) * PP + 4 * q + hp;
-        float mg[4], an[4];
+        float mg[4], an[4], dx[4], dy[4];
 #pragma unroll
         for (int k = 0; k < 4; ++k) {
             const int x = xg + k;
-            float dx = 0.f, dy = 0.f;
+            dx[k] = dy[k] = 0.f;
             if (y > 0 && y < a.R - 1 && x > 0 && x < a.C - 1) {
-                dx = __fsub_rn(pr[k + 1], pr[k - 1]);
-                dy = __fsub_rn(up[k], dn[k]);
+                dx[k] = __fsub_rn(pr[k + 1], pr[k - 1]);
+                dy[k] = __fsub_rn(up[k], dn[k]);
             }
-            fast_grad(dx, dy, mg[k], an[k]);
         }
+        fast_grad4(dx, dy, mg, an);
         float* m = a.mag[I - 2] + at;
         float* n = a.ang[I - 2] + at;
         if (vec && al16(m) && al16(n)) {
@@ -1145,12 +1159,10 @@ __device__ __forceinline__ void s_grad_item(const float* __restrict__ ring, cons
         dya = make_float2(dyv[0], dyv[1]);
         dyb = make_float2(dyv[2], dyv[3]);
     }
-    // the scalar gradient of the other engines (same code, same roundings)
+    // the gradient of the other engines (same function, same roundings)
+    const float dxv[4] = {dxa.x, dxa.y, dxb.x, dxb.y}, dyv[4] = {dya.x, dya.y, dyb.x, dyb.y};
     float mg[4], an[4];
-    fast_grad(dxa.x, dya.x, mg[0], an[0]);
-    fast_grad(dxa.y, dya.y, mg[1], an[1]);
-    fast_grad(dxb.x, dyb.x, mg[2], an[2]);
-    fast_grad(dxb.y, dyb.y, mg[3], an[3]);
+    fast_grad4(dxv, dyv, mg, an);
     const size_t at = (size_t)y * a.C + x;
     s_store4(a.mag[I - 1] + at, make_float4(mg[0], mg[1], mg[2], mg[3]), k.vec, a.C - x);
     s_store4(a.ang[I - 1] + at, make_float4(an[0], an[1], an[2], an[3]), k.vec, a.C - x);

@@ -72,3 +72,34 @@ def test_host_batch_api_equals_per_image():
             np.testing.assert_array_equal(gxy, wxy)
             np.testing.assert_array_equal(gu8, wu8)
             np.testing.assert_array_equal(grs, wrs)
+
+
+def test_extract_and_match_equals_per_pair_calls():
+    """frontend.extract_and_match (features kept on the device between the two graphs) returns the
+    matches of the per-image / per-pair host calls (sift_gpu_u8, guided_from_pred), on two calls."""
+    import fieldstitch_b200 as F
+    from fieldstitch_b200 import synth
+    h, w = 700, 900
+    pairs_src = [synth.synth_pair(h, w, 700 + k) for k in range(3)]
+    imgs = [im for a, b, _ in pairs_src for im in (a, b)]
+    nfeats = [3000, 2500, 800, 4000, 1500, 1500]
+    pairs = [(0, 1), (2, 3), (4, 5), (1, 0)]
+    priors = [pairs_src[0][2], pairs_src[1][2], pairs_src[2][2], np.linalg.inv(pairs_src[0][2])]
+    offs = [synth.prior_noise(5000, 40 + p) for p in range(len(pairs))]
+    feats = [F.features.sift_gpu_u8(im, nf) for im, nf in zip(imgs, nfeats)]
+    want = []
+    for (i, j), H, o in zip(pairs, priors, offs):
+        xa = feats[i][0]
+        pred = synth.apply_homography(H, xa) + o[:len(xa)].astype(np.float64)
+        want.append(F.matching.guided_from_pred(pred, feats[i][1], feats[j][0].astype(np.float64), feats[j][1],
+                                                (w, h), 40.0, 16, 0.85))
+    for _ in range(2):
+        got, fe = F.frontend.extract_and_match(imgs, nfeats, pairs, priors, 40.0, 16, 0.85, offsets=offs,
+                                               chains=3, return_features=True)
+        for (gq, gt), (wq, wt) in zip(got, want):
+            assert len(wq) > 0
+            np.testing.assert_array_equal(gq, wq)
+            np.testing.assert_array_equal(gt, wt)
+        for (gxy, gu8, grs), (wxy, wu8, wrs) in zip(fe, feats):
+            np.testing.assert_array_equal(gxy, wxy)
+            np.testing.assert_array_equal(gu8, wu8)
