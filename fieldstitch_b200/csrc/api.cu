@@ -357,7 +357,7 @@ namespace {
 __global__ void k_batch_status(const uint32_t* cnt, int32_t* count, uint32_t* status) {
     if (threadIdx.x != 0) return;
     *count = (int32_t)cnt[6];
-    *status = cnt[7] | (cnt[PYR_ERR_WORD] || cnt[EX_ERR_WORD] ? 8u : 0u);
+    *status = cnt[7] | (cnt[PYR_ERR_WORD] ? 8u : 0u);
 }
 
 struct BatchCall {
@@ -926,7 +926,7 @@ int32_t fsb_sift_features_batch_d(fsb_ctx* ctx, int32_t n_img, const uint8_t* co
     FSB_CUDA(cudaStreamSynchronize(s));
     for (int i = 0; i < n_img; ++i) {
         if (h_status[i] & 8u) {
-            set_error("a TMA row copy (pyramid or extrema) did not complete in time, image %d", i);
+            set_error("pyramid: a TMA row copy did not complete in time (strip engine), image %d", i);
             return FSB_ERR_TIMEOUT;
         }
         if (h_status[i] == 0) continue;

@@ -12,11 +12,8 @@
 //   k_gather    keypoint fields in input-image pixels (gsift.py:462-474)
 //   spread      grid-spread selection of features.py:38-57
 #include <cub/cub.cuh>
-#include <cuda.h>
 
 #include <cmath>
-#include <cstdlib>
-#include <cstring>
 
 #include "fsb_internal.cuh"
 
@@ -184,244 +181,6 @@ ExTiles make_tiles(const Geometry& g, int* total) {
     t.first[g.n_oct] = acc;
     *total = acc;
     return t;
-}
-
-// k_extrema_tma: the same test and append as k_extrema, fed from shared memory. A block (8 warps
-// side by side, 240 output columns, EX_ROWS rows of one octave) streams its rows of all five DoG
-// layers through an EXT_NS-row ring: one 3-D TMA copy per row (256 columns x 5 layers, the
-// octave's DoG block as a tensor of C x R x 5 floats), EXT_NS copies in flight, each slot
-// refilled once every warp has read it. Octaves whose rows or layer planes are not 16-byte
-// aligned (or narrower than the box) keep k_extrema.
-constexpr int EXT_NS = 8, EXT_W = 256;
-constexpr int EXT_SLOT = 5 * EXT_W;   // floats per ring row
-constexpr int EXT_SMEM = EXT_NS * EXT_SLOT * 4 + EXT_NS * 8;
-constexpr long long EXT_TIMEOUT = 2000000000ll;   // cycles for one row (about a second)
-
-struct ExMaps {
-    CUtensorMap m[MAXO];
-};
-
-__device__ __forceinline__ uint32_t ex_saddr(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
-
-__device__ __forceinline__ bool ex_wait(uint64_t* b, uint32_t parity) {
-    auto test = [&]() {
-        uint32_t ok;
-        asm volatile(
-            "{\n\t.reg .pred p;\n\t"
-            "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
-            "selp.u32 %0, 1, 0, p;\n\t}"
-            : "=r"(ok)
-            : "r"(ex_saddr(b)), "r"(parity)
-            : "memory");
-        return ok != 0;
-    };
-    if (test()) return true;
-    const long long t0 = clock64();
-    while (clock64() - t0 < EXT_TIMEOUT)
-        if (test()) return true;
-    return false;
-}
-
-__global__ void __launch_bounds__(EX_T, 4) k_extrema_tma(const __grid_constant__ ExMaps maps, DetectConsts k,
-                                                         ExTiles tl, uint32_t* __restrict__ cand, uint32_t* counter,
-                                                         uint32_t cap, int* err) {
-    extern __shared__ __align__(1024) float sm_ex[];
-    uint64_t* full = reinterpret_cast<uint64_t*>(sm_ex + EXT_NS * EXT_SLOT);
-    int o = 0;
-    while (o + 1 < tl.n_oct && (int)blockIdx.x >= tl.first[o + 1]) ++o;
-    const int b = blockIdx.x - tl.first[o];
-    const int ry = b / tl.col_tiles[o], cx = b - ry * tl.col_tiles[o];
-    const int R = k.g.R[o], C = k.g.C[o];
-    const long long RC = (long long)R * C;
-    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-    const int cb = BORDER + cx * (EX_T / 32) * EX_COLS - 1;   // the block's first (halo) column
-    const int cs = cb & ~3;                                    // the copy's first column (16-byte aligned)
-    const int c = cb + wid * EX_COLS + lane;                   // this lane's column
-    const int sidx = (cb - cs) + wid * EX_COLS + lane;         // its index in a ring row (< 245)
-    const bool col_ok = lane >= 1 && lane <= EX_COLS && c >= BORDER && c < C - BORDER;
-    const int y0 = BORDER + ry * EX_ROWS, y1 = min(y0 + EX_ROWS, R - BORDER);   // output rows [y0, y1)
-    const int nrows = y1 - y0 + 2;                                               // rows y0 - 1 .. y1
-    const CUtensorMap* tm = &maps.m[o];
-    if ((ex_saddr(sm_ex) & 127) != 0) {   // TMA destinations must be 128-byte aligned (uniform test)
-        if (threadIdx.x == 0) atomicExch(err, 2);
-        return;
-    }
-    if (threadIdx.x == 0) {
-        for (int s = 0; s < EXT_NS; ++s)
-            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(ex_saddr(full + s)) : "memory");
-        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-    }
-    __syncthreads();
-    auto issue = [&](int r) {   // row y0 - 1 + r into slot r mod EXT_NS (one thread)
-        const int s = r % EXT_NS;
-        asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(ex_saddr(full + s)),
-                     "r"(EXT_SLOT * 4)
-                     : "memory");
-        asm volatile(
-            "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], "
-            "[%5];" ::"r"(ex_saddr(sm_ex + s * EXT_SLOT)),
-            "l"(reinterpret_cast<uint64_t>(tm)), "r"(cs), "r"(y0 - 1 + r), "r"(0), "r"(ex_saddr(full + s))
-            : "memory");
-    };
-    if (threadIdx.x == 0)
-        for (int r = 0; r < nrows && r < EXT_NS; ++r) issue(r);
-    struct Row {
-        float hx[5], hn[5], c[3];
-    };
-    int rn = 0;   // rows read so far
-    // next row of the window from the ring; false (every thread) when a copy did not land in time
-    auto read_row = [&](Row& w) -> bool {
-        const int s = rn % EXT_NS;
-        const bool ok = ex_wait(full + s, (uint32_t)(rn / EXT_NS) & 1u);
-        float raw[5];
-        const float* p = sm_ex + s * EXT_SLOT + sidx;
-#pragma unroll
-        for (int l = 0; l < 5; ++l) raw[l] = p[l * EXT_W];
-        if (__syncthreads_or(!ok)) return false;   // every warp is done with slot s
-        if (threadIdx.x == 0 && rn + EXT_NS < nrows) {
-            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-            issue(rn + EXT_NS);
-        }
-        ++rn;
-#pragma unroll
-        for (int l = 0; l < 5; ++l) {
-            const float v = raw[l];
-            const float vl = __shfl_up_sync(0xffffffffu, v, 1), vr = __shfl_down_sync(0xffffffffu, v, 1);
-            w.hx[l] = fmaxf(fmaxf(vl, v), vr);
-            w.hn[l] = fminf(fminf(vl, v), vr);
-            if (l >= 1 && l <= N_LAYERS) w.c[l - 1] = v;
-        }
-        return true;
-    };
-    // test row y from the window (up, mid, dn) and append its extrema (as k_extrema)
-    auto test = [&](const Row& up, const Row& mid, const Row& dn, int y) {
-        float vmx[5], vmn[5];
-#pragma unroll
-        for (int l = 0; l < 5; ++l) {
-            vmx[l] = fmaxf(fmaxf(up.hx[l], mid.hx[l]), dn.hx[l]);
-            vmn[l] = fminf(fminf(up.hn[l], mid.hn[l]), dn.hn[l]);
-        }
-        unsigned mask = 0;
-        if (col_ok) {
-#pragma unroll
-            for (int l = 1; l <= N_LAYERS; ++l) {
-                const float v = mid.c[l - 1];
-                const float mx = fmaxf(fmaxf(vmx[l - 1], vmx[l]), vmx[l + 1]);
-                const float mn = fminf(fminf(vmn[l - 1], vmn[l]), vmn[l + 1]);
-                if ((v >= mx && v > k.pthr) || (v <= mn && v < -k.pthr)) mask |= 1u << (l - 1);
-            }
-        }
-        const unsigned any = __ballot_sync(0xffffffffu, mask != 0);
-        if (any) {
-            const int cntv = __popc(mask);
-            int incl = cntv;
-#pragma unroll
-            for (int sh = 1; sh < 32; sh <<= 1) {
-                const int t = __shfl_up_sync(0xffffffffu, incl, sh);
-                if (lane >= sh) incl += t;
-            }
-            const int total = __shfl_sync(0xffffffffu, incl, 31);
-            uint32_t basepos = 0;
-            if (lane == 31) basepos = atomicAdd(counter, (uint32_t)total);
-            basepos = __shfl_sync(0xffffffffu, basepos, 31);
-            uint32_t pos = basepos + (uint32_t)(incl - cntv);
-            while (mask) {
-                const int bit = __ffs(mask) - 1;
-                mask &= mask - 1;
-                if (pos < cap) cand[pos] = (uint32_t)(k.g.dog_off[o] + (bit + 1) * RC + (long long)y * C + c);
-                ++pos;
-            }
-        }
-    };
-    Row w0, w1, w2;
-    bool ok = read_row(w0) && read_row(w1) && read_row(w2);   // rows y0 - 1, y0, y0 + 1
-    for (int y = y0; ok && y < y1; y += 3) {
-        test(w0, w1, w2, y);
-        if (y + 1 >= y1 || !(ok = read_row(w0))) break;   // row y + 2
-        test(w1, w2, w0, y + 1);
-        if (y + 2 >= y1 || !(ok = read_row(w1))) break;   // row y + 3
-        test(w2, w0, w1, y + 2);
-        if (y + 3 >= y1 || !(ok = read_row(w2))) break;   // row y + 4
-    }
-    if (!ok && threadIdx.x == 0) atomicExch(err, 1);
-}
-
-typedef CUresult (*ExEncodeFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
-                               const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
-                               CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
-ExEncodeFn ex_encode() {
-    static ExEncodeFn fn = [] {
-        void* f = nullptr;
-        cudaDriverEntryPointQueryResult q{};
-        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &f, cudaEnableDefault, &q) != cudaSuccess ||
-            q != cudaDriverEntryPointSuccess)
-            f = nullptr;
-        return reinterpret_cast<ExEncodeFn>(f);
-    }();
-    return fn;
-}
-
-// The extremum candidates of every octave: octaves whose DoG rows and layer planes are 16-byte
-// aligned (and at least a box wide) by k_extrema_tma, the others by k_extrema; both append to
-// counter (cap entries). FSB_EXTREMA=plain keeps k_extrema for every octave. err: the status word
-// set when a TMA wait gives up.
-int32_t launch_extrema(const float* DF, const Geometry& g, const DetectConsts& k, uint32_t* cand, uint32_t* counter,
-                       uint32_t cap, int* err, cudaStream_t s) {
-    int nblk = 0;
-    const ExTiles all = make_tiles(g, &nblk);
-    if (nblk == 0) return FSB_OK;
-    const char* env = std::getenv("FSB_EXTREMA");
-    const bool plain = env && std::strcmp(env, "plain") == 0;
-    ExEncodeFn enc = plain ? nullptr : ex_encode();
-    ExMaps maps;
-    std::memset(&maps, 0, sizeof(maps));
-    bool use[MAXO] = {};
-    int n_use = 0;
-    for (int o = 0; o < g.n_oct && enc; ++o) {
-        const long long R = g.R[o], C = g.C[o];
-        const uintptr_t base = reinterpret_cast<uintptr_t>(DF + g.dog_off[o]);
-        if ((C & 3) || ((R * C) & 3) || (base & 15) || C < EXT_W || all.col_tiles[o] == 0 || all.row_tiles[o] == 0)
-            continue;
-        const cuuint64_t dims[3] = {(cuuint64_t)C, (cuuint64_t)R, 5};
-        const cuuint64_t strides[2] = {(cuuint64_t)C * 4, (cuuint64_t)(R * C) * 4};
-        const cuuint32_t box[3] = {(cuuint32_t)EXT_W, 1, 5};
-        const cuuint32_t es[3] = {1, 1, 1};
-        if (enc(&maps.m[o], CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, reinterpret_cast<void*>(base), dims, strides, box, es,
-                CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
-                CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS) {
-            use[o] = true;
-            ++n_use;
-        }
-    }
-    // two tile sets over the same geometry: the TMA octaves and the others
-    ExTiles ta = all, tb = all;
-    int na = 0, nb = 0;
-    for (int o = 0; o < g.n_oct; ++o) {
-        ta.first[o] = na;
-        tb.first[o] = nb;
-        const int n = all.col_tiles[o] * all.row_tiles[o];
-        if (use[o]) {
-            na += n;
-            tb.col_tiles[o] = tb.row_tiles[o] = 0;
-        } else {
-            nb += n;
-            ta.col_tiles[o] = ta.row_tiles[o] = 0;
-        }
-    }
-    ta.first[g.n_oct] = na;
-    tb.first[g.n_oct] = nb;
-    if (na > 0) {
-        static std::atomic<int> attr[64];
-        FSB_TRY(smem_attr((const void*)k_extrema_tma, EXT_SMEM, attr));
-        k_extrema_tma<<<na, EX_T, EXT_SMEM, s>>>(maps, k, ta, cand, counter, cap, err);
-        note_launch();
-    }
-    if (nb > 0) {
-        k_extrema<<<nb, EX_T, 0, s>>>(DF, k, tb, cand, counter, cap);
-        note_launch();
-    }
-    FSB_CUDA(cudaGetLastError());
-    return FSB_OK;
 }
 
 struct Fit {
@@ -825,20 +584,21 @@ int32_t run_detect(fsb_ctx* ctx, Workspace& ws, double contrast, double edge, in
     ctx->stage_begin(ST_EXTREMA);
     for (int attempt = 0; attempt < 3; ++attempt) {
         FSB_CUDA(cudaMemsetAsync(cnt, 0, 3 * sizeof(uint32_t), s));
-        FSB_CUDA(cudaMemsetAsync(cnt + EX_ERR_WORD, 0, sizeof(uint32_t), s));
-        FSB_TRY(launch_extrema(DF, g, k, ws.cand.as<uint32_t>(), cnt, (uint32_t)ws.cap_cand,
-                               reinterpret_cast<int*>(cnt + EX_ERR_WORD), s));
-        uint32_t h_head[EX_ERR_WORD + 1];
+        int nblk = 0;
+        const ExTiles tl = make_tiles(g, &nblk);
+        if (nblk > 0) {
+            k_extrema<<<nblk, EX_T, 0, s>>>(DF, k, tl, ws.cand.as<uint32_t>(), cnt, (uint32_t)ws.cap_cand);
+            note_launch();
+        }
+        FSB_CUDA(cudaGetLastError());
+        uint32_t h_head[PYR_ERR_WORD + 1];
         FSB_CUDA(cudaMemcpyAsync(h_head, cnt, sizeof(h_head), cudaMemcpyDeviceToHost, s));
         FSB_CUDA(cudaStreamSynchronize(s));
         if (h_head[PYR_ERR_WORD]) {
             set_error("pyramid: a TMA row copy did not complete in time (strip engine)");
             return FSB_ERR_TIMEOUT;
         }
-        if (h_head[EX_ERR_WORD]) {
-            set_error("extrema: a TMA row copy did not complete in time (status %u)", h_head[EX_ERR_WORD]);
-            return FSB_ERR_TIMEOUT;
-        }
+
         h_cnt[0] = h_head[0];
         if (h_cnt[0] <= ws.cap_cand) break;
         ws.cap_cand = (size_t)h_cnt[0] + (h_cnt[0] >> 3) + 1024;
@@ -1074,9 +834,9 @@ int32_t run_detect_async(Workspace& ws, double contrast, double edge, const Asyn
     uint32_t* cnt = ws.counters.as<uint32_t>();
     const float* DF = ws.dog.as<float>();
     FSB_CUDA(cudaMemsetAsync(cnt, 0, 8 * sizeof(uint32_t), s));
-    FSB_CUDA(cudaMemsetAsync(cnt + EX_ERR_WORD, 0, sizeof(uint32_t), s));
-    FSB_TRY(launch_extrema(DF, g, k, ws.cand.as<uint32_t>(), cnt, c.cand, reinterpret_cast<int*>(cnt + EX_ERR_WORD),
-                           s));
+    int nblk = 0;
+    const ExTiles tl = make_tiles(g, &nblk);
+    if (nblk > 0) k_extrema<<<nblk, EX_T, 0, s>>>(DF, k, tl, ws.cand.as<uint32_t>(), cnt, c.cand);
     const unsigned gr = std::min(blocks(c.cand, 128), 148u * 16u);
     k_refine<<<gr, 128, 0, s>>>(DF, k, ws.cand.as<uint32_t>(), cnt, c.cand, ws.refined.as<Refined>(), cnt + 1, c.ref);
     uint32_t* ka = ws.keys_a.as<uint32_t>();

@@ -232,7 +232,6 @@ int32_t launch_group_upper(const float* src, int R, int C, float* dog3, cudaStre
 int32_t launch_octave_strip(const float* L0, int R, int C, float* dog, float* mag, float* ang, float* down,
                             int down_cols, int* err, cudaStream_t s);
 constexpr int PYR_ERR_WORD = 8;   // index of the pyramid's error word in Workspace::counters
-constexpr int EX_ERR_WORD = 9;    // index of the extrema kernel's error word (set by a TMA wait that gave up)
 // autotune.cu: the fastest of n_variants launches of `run` for `key` (timed once per process and
 // device on `s`, then cached; FSB_AUTOTUNE=0 returns variant 0, FSB_AUTOTUNE_FILE persists choices)
 bool autotune_cached(const char* key, int n_variants, int* variant);

@@ -148,22 +148,3 @@ def test_autotuned_octave_engines_are_bit_identical(monkeypatch):
     table = _lib.autotune_table()
     for r, c in ref[0]:
         assert any(k.endswith("k_octave3_%dx%d" % (r, c)) for k in table), (r, c, table)
-
-
-@pytest.mark.parametrize("hw", [(240, 320), (989, 1320), (1978, 2640), (1001, 1111), (610, 830)])
-def test_extrema_tma_equals_plain(monkeypatch, hw):
-    """The TMA-fed extremum kernel (rows of the five DoG layers streamed through a shared-memory ring)
-    finds the plain kernel's candidates: the same keypoints, bit for bit, in the same order, on
-    octaves it takes and octaves it leaves to the plain kernel (widths not a multiple of four,
-    planes off a 16-byte boundary)."""
-    import fieldstitch_b200 as f
-    from fieldstitch_b200 import synth
-    h, w = hw
-    img = synth.synth_image(h, w, 17 + w)
-    monkeypatch.setenv("FSB_EXTREMA", "plain")
-    k0, _ = f.gsift.detect(img, max_kp=100000)
-    monkeypatch.delenv("FSB_EXTREMA")
-    k1, _ = f.gsift.detect(img, max_kp=100000)
-    assert len(k0["x"]) > 0
-    for key in ("x", "y", "size", "angle", "response", "octave", "layer"):
-        np.testing.assert_array_equal(k1[key], k0[key])
