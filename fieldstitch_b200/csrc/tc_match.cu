@@ -21,7 +21,7 @@
 //                shared-memory ring with bulk asynchronous copies (no tensor map, no multicast);
 //                warp 1 issues the MMAs (M=128, N=128) for the two 128-row halves of a 256-row
 //                query block into double-buffered FP32 accumulators (4 x 128 of the 512 TMEM
-//                columns); warps 2-9 read the accumulators with tcgen05.ld (32 columns at a time)
+//                columns); warps 2-9 read the accumulators with tcgen05.ld (a 128-column row per wait)
 //                and keep, per query row, the two largest 32-column maxima and their chunks.
 //   k_tc_finish  per query row: the two best chunks over all column splits and the exact integer
 //                distances (dp4a) of their columns (BF16: the best chunk only; the second chunk's
@@ -507,20 +507,20 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
                 if (!ok) break;
                 tc_fence_after();
                 const uint32_t base = tmem + ((uint32_t)(lq * 32) << 16) + (uint32_t)(ac * 256 + h * 128);
-#pragma unroll 1
+                // the whole 128-column row at once (four loads, one wait), then the accumulator is free
+                uint32_t r[TC_N / TC_CHUNK][32];
+#pragma unroll
+                for (int ch = 0; ch < TC_N / TC_CHUNK; ++ch) tmem_ld32(base + ch * TC_CHUNK, r[ch]);
+                tmem_wait_ld();
+                tc_fence_before();
+                __syncwarp();
+                if (lane == 0) mbar_arrive(acc_empty + ac);
+#pragma unroll
                 for (int ch = 0; ch < TC_N / TC_CHUNK; ++ch) {
-                    uint32_t r[32];
-                    tmem_ld32(base + ch * TC_CHUNK, r);
-                    tmem_wait_ld();
-                    if (ch == TC_N / TC_CHUNK - 1) {
-                        tc_fence_before();
-                        __syncwarp();
-                        if (lane == 0) mbar_arrive(acc_empty + ac);
-                    }
                     const int j0 = t * TC_N + ch * TC_CHUNK;
                     float v[32];
 #pragma unroll
-                    for (int i = 0; i < 32; ++i) v[i] = __uint_as_float(r[i]);
+                    for (int i = 0; i < 32; ++i) v[i] = __uint_as_float(r[ch][i]);
                     if (j0 + TC_CHUNK > P.nb) {
 #pragma unroll
                         for (int i = 0; i < 32; ++i)
@@ -588,123 +588,221 @@ __device__ __forceinline__ void warp_top2(long long& k1, long long& d2) {
 
 constexpr long long NO_D = LLONG_MAX >> 32;   // "no distance" (above every uint8 distance)
 
-template <int K>
-__global__ void k_tc_finish(const TcPair* __restrict__ pairs, const Cand* __restrict__ part,
-                            float ratio, int prec, int32_t* __restrict__ t_row, uint32_t* __restrict__ d_row,
-                            int32_t* __restrict__ flagged, int* __restrict__ n_flagged, float* __restrict__ err_stat) {
-    const TcPair& P = pairs[blockIdx.y];
-    const int q = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
-    const int lane = threadIdx.x & 31;
-    if (q >= P.na) return;
-    const int g = P.row0 + q;
-    const int ne = P.splits * K;   // <= 32
-    Cand e = lane < ne ? part[P.part0 + (size_t)q * ne + lane] : Cand{-INFINITY, -1};
-    // the K best chunks over all splits (value descending, chunk ascending)
-    float sv[K];
-    int sc[K];
+constexpr int FIN_PASSES = 2;   // a warp finishes 4 rows per pass
+
+// Per-lane error statistics of the certificate (kept by the lane that finishes a row, summed per
+// block, then one global update per block: a global atomic per row on one address serialises the
+// whole kernel).
+struct ErrAcc {
+    float mx = 0.f, sum = 0.f;
+    int n = 0;
+};
+
+// Top-2 merge of (key1 = d << 32 | j, d2) over the 8 lanes of a row group (xor 1, 2, 4).
+__device__ __forceinline__ void group_top2(long long& k1, long long& d2) {
 #pragma unroll
-    for (int k = 0; k < K; ++k) {
-        float bv = e.v;
-        int bc = e.j < 0 ? INT_MAX : e.j;
-        for (int sh = 16; sh; sh >>= 1) {
-            const float ov = __shfl_xor_sync(0xffffffffu, bv, sh);
-            const int oc = __shfl_xor_sync(0xffffffffu, bc, sh);
-            if (ov > bv || (ov == bv && oc < bc)) {
-                bv = ov;
-                bc = oc;
+    for (int sh = 1; sh < 8; sh <<= 1) {
+        const long long ok1 = __shfl_xor_sync(0xffffffffu, k1, sh);
+        const long long od2 = __shfl_xor_sync(0xffffffffu, d2, sh);
+        const long long hi = max(k1, ok1);
+        d2 = min(min(d2, od2), hi >> 32);
+        k1 = min(k1, ok1);
+    }
+}
+
+// A warp finishes 4 query rows at a time, 8 lanes per row: lane = 8 * grp + seg, seg the 16-byte
+// segment of the 128-byte rows that the lane multiplies. Per row:
+//   1. the K best chunks over the column splits (value descending, chunk ascending; one split's
+//      records are already in that order);
+//   2. the exact distances of the re-ranked chunks' 32 columns each: 32 independent 16-byte loads
+//      and dp4a per lane, then a transposed butterfly over seg (16 + 8 + 4 shuffles) leaves lane
+//      seg the whole dots of columns 4 seg .. 4 seg + 3; top-2 over the row's lanes;
+//   3. (lane seg 0) the certificate and the float32 ratio test of the reference: BF16, the best
+//      chunk's tensor-core maximum must equal the exact best (the values are exact) and the next
+//      chunk's maximum is the exact best outside it; E4M3, the rounding bound must settle the
+//      decision. Unsettled rows go to k_tc_exact_rows.
+template <int K>
+__global__ void __launch_bounds__(256) k_tc_finish(const TcPair* __restrict__ pairs, const Cand* __restrict__ part,
+                                                   float ratio, int prec, int32_t* __restrict__ t_row,
+                                                   uint32_t* __restrict__ d_row, int32_t* __restrict__ flagged,
+                                                   int* __restrict__ n_flagged, float* __restrict__ err_stat) {
+    __shared__ float s_mx, s_sum;
+    __shared__ int s_n;
+    if (threadIdx.x == 0) {
+        s_mx = 0.f;
+        s_sum = 0.f;
+        s_n = 0;
+    }
+    __syncthreads();
+    const TcPair& P = pairs[blockIdx.y];
+    const int lane = threadIdx.x & 31, seg = lane & 7, grp = lane >> 3;
+    const int nre = prec == FSB_PREC_BF16 ? 1 : K;
+    const bool h4 = seg & 4, h2 = seg & 2, h1 = seg & 1;
+    ErrAcc acc;
+    const int wq = (blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5)) * (4 * FIN_PASSES);
+    for (int pass = 0; pass < FIN_PASSES; ++pass) {
+        const int q0 = wq + 4 * pass;
+        if (q0 >= P.na) break;   // warp-uniform
+        const int qr = q0 + grp;
+        const bool live = qr < P.na;
+        const int q = live ? qr : P.na - 1;   // dead groups repeat a live row and write nothing
+        // 1. the K best chunks
+        float sv[K];
+        int sc[K];
+        if (P.splits == 1) {
+#pragma unroll
+            for (int k = 0; k < K; ++k) {
+                const Cand c = part[P.part0 + (size_t)q * K + k];
+                sv[k] = c.v;
+                sc[k] = c.j;
+            }
+        } else {
+            const int ne = P.splits * K;   // <= 32: at most 4 records per lane
+            Cand e[4];
+#pragma unroll
+            for (int t = 0; t < 4; ++t) {
+                const int idx = seg + 8 * t;
+                e[t] = idx < ne ? part[P.part0 + (size_t)q * ne + idx] : Cand{-INFINITY, -1};
+                if (e[t].j < 0) e[t] = Cand{-INFINITY, INT_MAX};
+            }
+#pragma unroll
+            for (int k = 0; k < K; ++k) {
+                float bv = e[0].v;
+                int bc = e[0].j;
+#pragma unroll
+                for (int t = 1; t < 4; ++t)
+                    if (e[t].v > bv || (e[t].v == bv && e[t].j < bc)) {
+                        bv = e[t].v;
+                        bc = e[t].j;
+                    }
+#pragma unroll
+                for (int sh = 1; sh < 8; sh <<= 1) {
+                    const float ov = __shfl_xor_sync(0xffffffffu, bv, sh);
+                    const int oc = __shfl_xor_sync(0xffffffffu, bc, sh);
+                    if (ov > bv || (ov == bv && oc < bc)) {
+                        bv = ov;
+                        bc = oc;
+                    }
+                }
+                sv[k] = bv;
+                sc[k] = bc == INT_MAX ? -1 : bc;
+#pragma unroll
+                for (int t = 0; t < 4; ++t)
+                    if (e[t].j == bc && bc != INT_MAX) e[t] = Cand{-INFINITY, INT_MAX};
             }
         }
-        sv[k] = bv;
-        sc[k] = bc == INT_MAX ? -1 : bc;
-        if (e.j == bc && e.j >= 0) e = Cand{-INFINITY, -1};
-    }
-    const long long na = P.nA[q];
-    double inv_s = 1.0, eps = 0.0;
-    if (prec == FSB_PREC_FP8) {
-        const float4 rs = reinterpret_cast<const float4*>(P.rowsc)[q];
-        const double bl = P.bmax[0], be = P.bmax[1];
-        inv_s = rs.y;
-        eps = (double)rs.z * be + (double)rs.w * bl + (double)rs.w * be + (double)rs.z * bl * (1.0 / 512.0) + 4.0;
-    }
-    // exact distances of the re-ranked chunks: 8 lanes per target row (16 bytes each), so every
-    // load instruction reads 4 whole rows
-    const int nre = prec == FSB_PREC_BF16 ? 1 : K;
-    const int seg = lane & 7, sub = lane >> 3;
-    const uint4 a4 = __ldg(reinterpret_cast<const uint4*>(P.a + (size_t)q * 128) + seg);
-    long long k1 = LLONG_MAX, d2 = NO_D;
+        const long long na = P.nA[q];
+        double inv_s = 1.0, eps = 0.0;
+        if (prec == FSB_PREC_FP8) {
+            const float4 rs = reinterpret_cast<const float4*>(P.rowsc)[q];
+            const double bl = P.bmax[0], be = P.bmax[1];
+            inv_s = rs.y;
+            eps = (double)rs.z * be + (double)rs.w * bl + (double)rs.w * be + (double)rs.z * bl * (1.0 / 512.0) +
+                  4.0;
+        }
+        // 2. exact distances of the re-ranked chunks
+        const uint4 a4 = __ldg(reinterpret_cast<const uint4*>(P.a + (size_t)q * 128) + seg);
+        long long k1 = LLONG_MAX, d2 = NO_D;
 #pragma unroll
-    for (int k = 0; k < K; ++k) {
-        if (k >= nre || sc[k] < 0) continue;
+        for (int k = 0; k < K; ++k) {
+            if (k >= nre) break;   // warp-uniform
+            const int jc = sc[k] < 0 ? P.nb : sc[k] * TC_CHUNK;   // an empty chunk: no valid column
+            uint32_t p[32];
 #pragma unroll
-        for (int i = 0; i < TC_CHUNK / 4; ++i) {
-            const int j = sc[k] * TC_CHUNK + 4 * i + sub;
-            uint32_t dot = 0;
-            if (j < P.nb) {
-                const uint4 b4 = __ldg(reinterpret_cast<const uint4*>(P.b + (size_t)j * 128) + seg);
-                dot = __dp4a(a4.x, b4.x, dot);
-                dot = __dp4a(a4.y, b4.y, dot);
-                dot = __dp4a(a4.z, b4.z, dot);
-                dot = __dp4a(a4.w, b4.w, dot);
+            for (int i = 0; i < 32; ++i) {
+                const int j = jc + i;
+                uint32_t dot = 0;
+                if (j < P.nb) {
+                    const uint4 b4 = __ldg(reinterpret_cast<const uint4*>(P.b + (size_t)j * 128) + seg);
+                    dot = __dp4a(a4.x, b4.x, dot);
+                    dot = __dp4a(a4.y, b4.y, dot);
+                    dot = __dp4a(a4.z, b4.z, dot);
+                    dot = __dp4a(a4.w, b4.w, dot);
+                }
+                p[i] = dot;
             }
-            dot += __shfl_xor_sync(0xffffffffu, dot, 1);
-            dot += __shfl_xor_sync(0xffffffffu, dot, 2);
-            dot += __shfl_xor_sync(0xffffffffu, dot, 4);
-            if (seg == 0 && j < P.nb) {
-                const long long d = na + P.nB[j] - 2ll * (long long)dot;
-                const long long key = (d << 32) | (unsigned)j;
-                if (key < k1) {
-                    d2 = min(d2, k1 >> 32);
-                    k1 = key;
-                } else {
-                    d2 = min(d2, d);
+#pragma unroll
+            for (int t = 0; t < 16; ++t)
+                p[t] = (h4 ? p[t + 16] : p[t]) + __shfl_xor_sync(0xffffffffu, h4 ? p[t] : p[t + 16], 4);
+#pragma unroll
+            for (int t = 0; t < 8; ++t)
+                p[t] = (h2 ? p[t + 8] : p[t]) + __shfl_xor_sync(0xffffffffu, h2 ? p[t] : p[t + 8], 2);
+#pragma unroll
+            for (int t = 0; t < 4; ++t)
+                p[t] = (h1 ? p[t + 4] : p[t]) + __shfl_xor_sync(0xffffffffu, h1 ? p[t] : p[t + 4], 1);
+#pragma unroll
+            for (int t = 0; t < 4; ++t) {
+                const int j = jc + 4 * seg + t;
+                if (j < P.nb) {
+                    const long long d = na + __ldg(P.nB + j) - 2ll * (long long)p[t];
+                    const long long key = (d << 32) | (unsigned)j;
+                    if (key < k1) {
+                        d2 = min(d2, k1 >> 32);
+                        k1 = key;
+                    } else {
+                        d2 = min(d2, d);
+                    }
                 }
             }
         }
-    }
-    warp_top2(k1, d2);
-    if (lane != 0) return;
-    const bool has1 = k1 != LLONG_MAX;
-    const long long e1 = has1 ? (k1 >> 32) : NO_D;
-    const int j1 = (int)(k1 & 0xffffffffll);
-    long long e2 = d2;
-    bool mismatch = false;
-    float err = 0.f;
-    if (has1) {
-        const double approx = (double)na - 2.0 * (double)sv[0] * inv_s;   // the best chunk's maximum
-        err = (float)fabs(approx - (double)e1);
-        if (prec == FSB_PREC_BF16) {
-            mismatch = err != 0.f;
-            // BF16 values are exact: the best column outside the first chunk is the second chunk's maximum
-            if (sv[1] > -INFINITY) e2 = min(e2, na - (long long)(2.0 * (double)sv[1]));
+        group_top2(k1, d2);
+        if (seg != 0 || !live) continue;
+        // 3. certificate and ratio test
+        const int g = P.row0 + q;
+        const bool has1 = k1 != LLONG_MAX;
+        const long long e1 = has1 ? (k1 >> 32) : NO_D;
+        const int j1 = (int)(k1 & 0xffffffffll);
+        long long e2 = d2;
+        bool mismatch = false;
+        float err = 0.f;
+        if (has1) {
+            const double approx = (double)na - 2.0 * (double)sv[0] * inv_s;   // the best chunk's maximum
+            err = (float)fabs(approx - (double)e1);
+            if (prec == FSB_PREC_BF16) {
+                mismatch = err != 0.f;
+                // BF16 values are exact: the best column outside the first chunk is the second chunk's maximum
+                if (sv[1] > -INFINITY) e2 = min(e2, na - (long long)(2.0 * (double)sv[1]));
+            }
+        }
+        // lower bound on the exact distance of every column outside the re-ranked chunks
+        double L = INFINITY;
+        const float vb = sv[nre < K ? nre : K - 1];
+        if (vb > -INFINITY) {
+            L = ceil((double)na - 2.0 * ((double)vb * inv_s + eps));
+            if (L < 0.0) L = 0.0;
+        }
+        const float fL = L > 16777216.0 ? 16777216.f : (float)L;
+        const float f1 = e1 > (1ll << 24) ? 16777216.f : (float)e1;
+        const float f2 = e2 > (1ll << 24) ? 16777216.f : (float)e2;
+        const bool accept = has1 && (double)e1 < L && ratio_ok(f1, fminf(f2, fL), ratio);
+        const bool reject = !has1 || !ratio_ok(fminf(f1, fL), f2, ratio);
+        if (has1) {
+            acc.mx = fmaxf(acc.mx, err);
+            acc.sum += err;
+            ++acc.n;
+        }
+        if (!mismatch && accept) {
+            t_row[g] = j1;
+            d_row[g] = (uint32_t)e1;
+        } else if (!mismatch && reject) {
+            t_row[g] = -1;
+            d_row[g] = has1 ? (uint32_t)e1 : 0u;
+        } else {
+            t_row[g] = -1;
+            d_row[g] = 0u;
+            flagged[atomicAdd(n_flagged, 1)] = g;
         }
     }
-    // lower bound on the exact distance of every column outside the re-ranked chunks
-    double L = INFINITY;
-    const float vb = sv[nre < K ? nre : K - 1];
-    if (vb > -INFINITY) {
-        L = ceil((double)na - 2.0 * ((double)vb * inv_s + eps));
-        if (L < 0.0) L = 0.0;
+    if (acc.n) {   // err >= 0: its bits order like the values
+        atomicMax(reinterpret_cast<int*>(&s_mx), __float_as_int(acc.mx));
+        atomicAdd(&s_sum, acc.sum);
+        atomicAdd(&s_n, acc.n);
     }
-    const float fL = L > 16777216.0 ? 16777216.f : (float)L;
-    const float f1 = e1 > (1ll << 24) ? 16777216.f : (float)e1;
-    const float f2 = e2 > (1ll << 24) ? 16777216.f : (float)e2;
-    const bool accept = has1 && (double)e1 < L && ratio_ok(f1, fminf(f2, fL), ratio);
-    const bool reject = !has1 || !ratio_ok(fminf(f1, fL), f2, ratio);
-    if (err_stat && has1) {
-        atomicMax(reinterpret_cast<int*>(err_stat), __float_as_int(err));
-        atomicAdd(err_stat + 1, err);
-        atomicAdd(reinterpret_cast<int*>(err_stat) + 2, 1);
-    }
-    if (!mismatch && accept) {
-        t_row[g] = j1;
-        d_row[g] = (uint32_t)e1;
-    } else if (!mismatch && reject) {
-        t_row[g] = -1;
-        d_row[g] = has1 ? (uint32_t)e1 : 0u;
-    } else {
-        t_row[g] = -1;
-        d_row[g] = 0u;
-        flagged[atomicAdd(n_flagged, 1)] = g;
+    __syncthreads();
+    if (threadIdx.x == 0 && err_stat && s_n) {
+        atomicMax(reinterpret_cast<int*>(err_stat), __float_as_int(s_mx));
+        atomicAdd(err_stat + 1, s_sum);
+        atomicAdd(reinterpret_cast<int*>(err_stat) + 2, s_n);
     }
 }
 
@@ -936,7 +1034,7 @@ int32_t run_match_bf_tc(fsb_ctx* ctx, int n_pairs, const uint8_t* const* d_a, co
     note_launch(1);
     ctx->stage_end(ST_TC_DENSE);
     float* err_stat = stats ? reinterpret_cast<float*>(small + 2) : nullptr;
-    const dim3 fin_grid(nblk(max_na, 8), (unsigned)n_pairs);
+    const dim3 fin_grid(nblk(max_na, 8 * 4 * FIN_PASSES), (unsigned)n_pairs);
     if (fp8)
         k_tc_finish<TcTraits<FSB_PREC_FP8>::TOPK><<<fin_grid, 256, 0, s>>>(d_pairs, part, ratio, precision, t_row,
                                                                            d_row, flagged, small + 1, err_stat);
