@@ -389,8 +389,10 @@ __global__ void __launch_bounds__(NT, 2) k_octave(Args a) {
 // vertical pass keeps an 8-row sliding window of column pairs in registers, the horizontal pass
 // reads the row-pair interleaved vertical outputs. No ring buffers: 3-4 CTAs per SM.
 constexpr int LX = 128, LNT = 256;   // tile width, threads; the tile height LY is a template parameter
-constexpr int LIN_W = LX + 32;   // input tile pitch (floats)
-constexpr int LT2_W = LX + 32;   // row-pair tile pitch (float2)
+constexpr int LIN_C = LX + 32;   // input tile columns (16 of halo on each side)
+constexpr int LIN_W = LX + 40;   // input tile pitch (floats): rows 2 apart differ by 64 bytes mod 128
+constexpr int LT2_W = LX + 34;   // row-pair tile pitch (float2): 16 bytes past a multiple of 128, so
+                                 // row pairs p and p + 1 start in opposite 16-byte bank groups
 
 struct LayerArgs {
     const float* src;   // L_{I-1}, R x C
@@ -430,19 +432,19 @@ __global__ void __launch_bounds__(LNT) k_layer(LayerArgs a) {
         // input tile until the vertical pass needs them. A block larger than the staging window
         // (mirror images of a tiny image) takes the per-sample global path.
         constexpr int VCW = 96, SRW = IH / 2 + 4;
-        static_assert(!BASE || (2 * IH + 2 * LIN_W) * 4 + IH * VCW * 4 + 16 <= (LY / 2) * LT2_W * 8,
+        static_assert(!BASE || (2 * IH + 2 * LIN_C) * 4 + IH * VCW * 4 + 16 <= (LY / 2) * LT2_W * 8,
                       "base tables must fit the row-pair area");
         static_assert(!BASE || (SRW * VCW <= IH * LIN_W && IH % 2 == 0), "staged source block");
         int* ry = reinterpret_cast<int*>(t2);   // iy of tile row i, then ny
         int* rn = ry + IH;
         int* cxs = rn + IH;                      // ix of tile column c, then nx (16-byte aligned)
-        int* cns = cxs + LIN_W;
-        float* vcs = reinterpret_cast<float*>(cns + LIN_W);
+        int* cns = cxs + LIN_C;
+        float* vcs = reinterpret_cast<float*>(cns + LIN_C);
         int* box = reinterpret_cast<int*>(vcs + IH * VCW);   // source row min / max, column min / max
         float* ps = s_in;
         if (tid < 4) box[tid] = (tid & 1) ? -1 : 0x7fffffff;
         __syncthreads();
-        for (int i0 = 0; i0 < IH + LIN_W; i0 += LNT) {
+        for (int i0 = 0; i0 < IH + LIN_C; i0 += LNT) {
             const int i = i0 + tid;
             int lo = 0x7fffffff, hi = -1, clo = 0x7fffffff, chi = -1;
             if (i < IH) {
@@ -452,7 +454,7 @@ __global__ void __launch_bounds__(LNT) k_layer(LayerArgs a) {
                 rn[i] = ny;
                 lo = min(iy, ny);
                 hi = max(iy, ny);
-            } else if (i < IH + LIN_W) {
+            } else if (i < IH + LIN_C) {
                 const int c = i - IH, X = mir(x0 - 16 + c, a.C), ix = X >> 1;
                 const int nx = (X & 1) ? min(ix + 1, a.iw - 1) : max(ix - 1, 0);
                 cxs[c] = ix;
@@ -497,8 +499,8 @@ __global__ void __launch_bounds__(LNT) k_layer(LayerArgs a) {
                 *reinterpret_cast<float4*>(vcs + row * VCW + q) = v;
             }
             __syncthreads();
-            for (int i = tid; i < IH * (LIN_W / 4); i += LNT) {
-                const int row = i / (LIN_W / 4), q = 4 * (i - row * (LIN_W / 4));
+            for (int i = tid; i < IH * (LIN_C / 4); i += LNT) {
+                const int row = i / (LIN_C / 4), q = 4 * (i - row * (LIN_C / 4));
                 const int4 ix = *reinterpret_cast<const int4*>(cxs + q);
                 const int4 nx = *reinterpret_cast<const int4*>(cns + q);
                 const float* v = vcs + row * VCW - sx0;
@@ -510,8 +512,8 @@ __global__ void __launch_bounds__(LNT) k_layer(LayerArgs a) {
                 *reinterpret_cast<float4*>(s_in + row * LIN_W + q) = u;
             }
         } else {
-            for (int i = tid; i < IH * LIN_W; i += LNT) {
-                const int row = i / LIN_W, col = i - row * LIN_W;
+            for (int i = tid; i < IH * LIN_C; i += LNT) {
+                const int row = i / LIN_C, col = i - row * LIN_C;
                 const uint8_t* r0 = a.img + (size_t)ry[row] * a.img_stride;
                 const uint8_t* r1 = a.img + (size_t)rn[row] * a.img_stride;
                 const int ix = cxs[col], nx = cns[col];
@@ -524,7 +526,7 @@ __global__ void __launch_bounds__(LNT) k_layer(LayerArgs a) {
         }
     } else if ((a.C & 3) == 0 && al16(a.src) && x0 >= 16 && x0 + LX + 16 <= a.C) {
         // eight lanes per row (the mirrored row address once per row), five 16-byte copies a lane
-        static_assert(LIN_W / 4 == 40, "five copies of eight lanes per row");
+        static_assert(LIN_C / 4 == 40, "five copies of eight lanes per row");
         for (int row = tid >> 3; row < IH; row += LNT / 8) {
             const float* g = a.src + (size_t)mir(y0 - r + row, a.R) * a.C + (x0 - 16);
             float* d = s_in + row * LIN_W;
@@ -535,8 +537,8 @@ __global__ void __launch_bounds__(LNT) k_layer(LayerArgs a) {
             }
         }
     } else {
-        for (int i = tid; i < IH * LIN_W; i += LNT) {
-            const int row = i / LIN_W, col = i - row * LIN_W;
+        for (int i = tid; i < IH * LIN_C; i += LNT) {
+            const int row = i / LIN_C, col = i - row * LIN_C;
             const float* g = a.src + (size_t)mir(y0 - r + row, a.R) * a.C + mir(x0 - 16 + col, a.C);
             cp_async4(s_in + row * LIN_W + col, g);
         }
@@ -563,9 +565,15 @@ __global__ void __launch_bounds__(LNT) k_layer(LayerArgs a) {
         }
     }
     __syncthreads();
-    // horizontal pass: row pair p, output columns c .. c+3 (t2 indices c + 2d .. c + 2d + 3 + 2r)
+    // horizontal pass: row pair p, output columns c .. c+3 (t2 indices c + 2d .. c + 2d + 3 + 2r).
+    // A warp covers row pairs p, p + 1 x 64 columns. 16-byte loads are served 8 lanes at a time:
+    // in each group of 8 lanes, four read row pair p and four row pair p + 1 (columns 4 apart, a
+    // 32-byte stride: one bank parity per row pair, opposite parities by the pitch), so the 8
+    // lanes cover all 32 banks once
+    static_assert(LX == 128 && (LY / 2) % 2 == 0 && LNT % 32 == 0, "horizontal pass mapping");
     for (int it = tid; it < (LY / 2) * (LX / 4); it += LNT) {
-        const int p = it / (LX / 4), c = 4 * (it - p * (LX / 4));
+        const int wi = it >> 5, l = it & 31;
+        const int p = 2 * (wi >> 1) + ((l >> 2) & 1), c = 64 * (wi & 1) + 4 * ((l & 3) + 4 * (l >> 3));
         const int y = y0 + 2 * p, x = x0 + c;
         if (y >= a.R || x >= a.C) continue;
         const float4* src = reinterpret_cast<const float4*>(t2 + p * LT2_W + c + 2 * d);
