@@ -60,14 +60,23 @@ struct ExTiles {
     int first[MAXO + 1];     // first block of each octave
 };
 
+constexpr int EX_DEPTH = 6;          // rows in flight per lane (the shared-memory ring's slots)
+
+__device__ __forceinline__ void ex_cp_async4(float* dst, const float* src) {
+    const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(d), "l"(src) : "memory");
+}
+
 // Streaming 3x3x3 extremum test: each warp walks down a chunk of rows of 30 interior columns;
-// every DoG value is read once (coalesced), horizontal neighbours come from the adjacent lanes,
+// every DoG value is read once (coalesced, EX_DEPTH rows ahead through a shared-memory ring),
+// horizontal neighbours come from the adjacent lanes,
 // the 3-row vertical window of the horizontal maxima / minima stays in registers. A voxel is an
 // extremum when it equals the maximum (minimum) of its 27-neighbourhood - ties count - and is
 // beyond the threshold, as scipy's maximum_filter / minimum_filter test in the reference
 // (gsift.py:293-319). Candidates of a row are appended with one warp-aggregated atomic.
-__global__ void __launch_bounds__(EX_T, 5) k_extrema(const float* __restrict__ DF, DetectConsts k, ExTiles tl,
+__global__ void __launch_bounds__(EX_T, 4) k_extrema(const float* __restrict__ DF, DetectConsts k, ExTiles tl,
                                                   uint32_t* __restrict__ cand, uint32_t* counter, uint32_t cap) {
+    __shared__ float ex_ring[EX_DEPTH * 5 * EX_T];
     int o = 0;
     while (o + 1 < tl.n_oct && (int)blockIdx.x >= tl.first[o + 1]) ++o;
     const int b = blockIdx.x - tl.first[o];
@@ -85,12 +94,32 @@ __global__ void __launch_bounds__(EX_T, 5) k_extrema(const float* __restrict__ D
     struct Row {
         float hx[5], hn[5], c[3];
     };
-    // layer l of row y at this lane's column: rowp + l * RC, rowp advancing by C per row
-    const float* rowp = base + (long long)(y0 - 1) * C + cc;
-    auto issue_row = [&](float (&raw)[5]) {
+    // Row r's five layer values at this lane's column arrive by 4-byte cp.async into the lane's own
+    // ring slot ((r - (y0 - 1)) % EX_DEPTH), EX_DEPTH rows ahead of the row being finished; only the
+    // lane that copied a value reads it, so a lane waits on its own copy groups and no barrier is
+    // needed. One commit group per row (empty past the last needed row) keeps the count uniform.
+    float* ring = ex_ring + threadIdx.x;   // element (slot, l) at ring[(slot * 5 + l) * EX_T]
+    const float* colp = base + cc;
+    const int last_row = min(y1 + 1, R - 1);
+    int next_row = y0 - 1, next_slot = 0, take_slot = 0;
+    auto issue_next = [&]() {
+        if (next_row <= last_row) {
+            const float* src = colp + (long long)next_row * C;
 #pragma unroll
-        for (int l = 0; l < 5; ++l) raw[l] = __ldg(rowp + l * RC);
-        rowp += C;
+            for (int l = 0; l < 5; ++l) ex_cp_async4(ring + (next_slot * 5 + l) * EX_T, src + l * RC);
+        }
+        asm volatile("cp.async.commit_group;\n" ::: "memory");
+        ++next_row;
+        next_slot = next_slot + 1 == EX_DEPTH ? 0 : next_slot + 1;
+    };
+    // the oldest row in flight, once landed (EX_DEPTH groups outstanding -> wait for all but the
+    // newest EX_DEPTH - 1), then its slot gets the next row
+    auto take_row = [&](float (&raw)[5]) {
+        asm volatile("cp.async.wait_group %0;\n" ::"n"(EX_DEPTH - 1) : "memory");
+#pragma unroll
+        for (int l = 0; l < 5; ++l) raw[l] = ring[(take_slot * 5 + l) * EX_T];
+        take_slot = take_slot + 1 == EX_DEPTH ? 0 : take_slot + 1;
+        issue_next();
     };
     auto finish_row = [&](Row& w, const float (&raw)[5]) {
 #pragma unroll
@@ -104,17 +133,12 @@ __global__ void __launch_bounds__(EX_T, 5) k_extrema(const float* __restrict__ D
     };
     auto load_row = [&](Row& w) {
         float raw[5];
-        issue_row(raw);
+        take_row(raw);
         finish_row(w, raw);
     };
     // test row y from the window (up, mid, dn), append its extrema, then finish row y + 2 into `up`
-    // (no longer needed): the three windows rotate by name, not by register moves. Row y + 2's
-    // loads are issued before the test, so they are in flight while it runs (a few registers
-    // spill at 5 blocks per SM; the kernel is bound by load latency, and this took it from 0.220
-    // to 0.193 ms per 2640 x 1978 image)
+    // (no longer needed): the three windows rotate by name, not by register moves
     auto step = [&](Row& up, const Row& mid, const Row& dn, int y) {
-        float raw[5];
-        issue_row(raw);   // row y + 2 <= R - BORDER + 1 < R, in flight while row y is tested
         float vmx[5], vmn[5];
 #pragma unroll
         for (int l = 0; l < 5; ++l) {
@@ -152,8 +176,9 @@ __global__ void __launch_bounds__(EX_T, 5) k_extrema(const float* __restrict__ D
                 ++pos;
             }
         }
-        finish_row(up, raw);
+        load_row(up);   // row y + 2
     };
+    for (int i = 0; i < EX_DEPTH; ++i) issue_next();   // rows y0 - 1 .. y0 + EX_DEPTH - 2
     Row w0, w1, w2;
     load_row(w0);   // y0 - 1
     load_row(w1);   // y0
@@ -165,6 +190,7 @@ __global__ void __launch_bounds__(EX_T, 5) k_extrema(const float* __restrict__ D
         if (y + 2 >= y1) break;
         step(w2, w0, w1, y + 2);
     }
+    asm volatile("cp.async.wait_group 0;\n" ::: "memory");   // no copy outlives the block
 }
 
 ExTiles make_tiles(const Geometry& g, int* total) {
