@@ -60,7 +60,7 @@ struct ExTiles {
     int first[MAXO + 1];     // first block of each octave
 };
 
-constexpr int EX_DEPTH = 6;          // rows in flight per lane (the shared-memory ring's slots)
+constexpr int EX_DEPTH = 9;          // rows in flight per lane (the shared-memory ring's slots)
 
 __device__ __forceinline__ void ex_cp_async4(float* dst, const float* src) {
     const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
