@@ -363,6 +363,7 @@ __global__ void k_batch_status(const uint32_t* cnt, int32_t* count, uint32_t* st
 struct BatchCall {
     int n_img;
     const uint8_t* const* imgs;
+    const uint8_t* const* h_imgs;   // page-locked host images uploaded by the graph, or null
     int h, w, stride;
     const fsb_sift_params* p;
     const int32_t* nfeats;
@@ -379,12 +380,34 @@ int32_t batch_body(fsb_ctx* ctx, const BatchCall& b) {
     const bool exact = (b.p->flags & FSB_SIFT_EXACT_BLUR) != 0;
     FSB_CUDA(cudaEventRecord(x.fork, ctx->stream));
     for (int c = 0; c < chains; ++c) FSB_CUDA(cudaStreamWaitEvent(x.streams[c], x.fork, 0));
+    if (b.h_imgs) {
+        // the uploads on their own stream, in image order: image i's chain waits for image i only,
+        // so later uploads overlap the extraction of earlier images
+        x.copy_nodes.assign(b.n_img, nullptr);
+        FSB_CUDA(cudaStreamWaitEvent(x.upload, x.fork, 0));
+        const size_t bytes = (size_t)b.h * b.stride;
+        for (int i = 0; i < b.n_img; ++i) {
+            FSB_CUDA(cudaMemcpyAsync(const_cast<uint8_t*>(b.imgs[i]), b.h_imgs[i], bytes, cudaMemcpyHostToDevice,
+                                     x.upload));
+            cudaStreamCaptureStatus cs;
+            const cudaGraphNode_t* deps = nullptr;
+            size_t nd = 0;
+            FSB_CUDA(cudaStreamGetCaptureInfo(x.upload, &cs, nullptr, nullptr, &deps, &nd));
+            if (cs != cudaStreamCaptureStatusActive || nd != 1) {
+                set_error("capture of the image uploads: unexpected capture state");
+                return FSB_ERR_CUDA;
+            }
+            x.copy_nodes[i] = deps[0];
+            FSB_CUDA(cudaEventRecord(x.uploaded[i], x.upload));
+        }
+    }
     uint32_t* status = x.status.as<uint32_t>();
     for (int i = 0; i < b.n_img; ++i) {
         const int c = i % chains;
         cudaStream_t s = x.streams[c];
         Workspace& ws = *x.ws[c];
         const int nfeat = b.nfeats[i];
+        if (b.h_imgs) FSB_CUDA(cudaStreamWaitEvent(s, x.uploaded[i], 0));
         FSB_TRY(run_pyramid(ws, b.imgs[i], b.stride, exact, s, nullptr, nullptr));
         FSB_TRY(run_detect_async(ws, b.p->contrast, b.p->edge, x.caps, (int)((double)nfeat * 2.2), exact, s));
         const int nf = x.caps.nfeat;
@@ -410,6 +433,10 @@ int32_t batch_body(fsb_ctx* ctx, const BatchCall& b) {
     for (int c = 0; c < chains; ++c) {
         FSB_CUDA(cudaEventRecord(x.join[c], x.streams[c]));
         FSB_CUDA(cudaStreamWaitEvent(ctx->stream, x.join[c], 0));
+    }
+    if (b.h_imgs) {   // the upload stream rejoins too (its last node precedes every chain anyway)
+        FSB_CUDA(cudaEventRecord(x.uploaded[b.n_img - 1], x.upload));
+        FSB_CUDA(cudaStreamWaitEvent(ctx->stream, x.uploaded[b.n_img - 1], 0));
     }
     return FSB_OK;
 }
@@ -694,7 +721,6 @@ int32_t fsb_sift_features(fsb_ctx* ctx, const uint8_t* img, int32_t h, int32_t w
     FSB_ARG(nfeat >= 0, "nfeat < 0");
     *n_out = 0;
     FSB_TRY(use_device(ctx));
-    cudaStream_t s = ctx->stream;
     Workspace* ws = acquire(ctx);
     struct Guard {
         fsb_ctx* c;
@@ -777,10 +803,15 @@ int32_t fsb_sift_features_ex_d(fsb_ctx* ctx, const uint8_t* d_img, int32_t h, in
 }
 
 
-int32_t fsb_sift_features_batch_d(fsb_ctx* ctx, int32_t n_img, const uint8_t* const* d_imgs, int32_t h, int32_t w,
-                                  int32_t stride, const fsb_sift_params* p, const int32_t* nfeats, float* const* d_xy,
-                                  float* const* d_resp, uint8_t* const* d_rootsift, int32_t* d_counts,
-                                  int32_t* h_counts, int32_t chains) {
+}  // extern "C"
+
+namespace fsb {
+namespace {
+// fsb_sift_features_batch_d and, with h_imgs, fsb_sift_features_batch_hd
+int32_t sift_features_batch(fsb_ctx* ctx, int32_t n_img, const uint8_t* const* h_imgs, const uint8_t* const* d_imgs,
+                            int32_t h, int32_t w, int32_t stride, const fsb_sift_params* p, const int32_t* nfeats,
+                            float* const* d_xy, float* const* d_resp, uint8_t* const* d_rootsift, int32_t* d_counts,
+                            int32_t* h_counts, int32_t chains) {
     FSB_ARG(ctx && p, "null pointer");
     FSB_ARG(n_img >= 0, "n_img < 0");
     if (n_img == 0) return FSB_OK;
@@ -795,6 +826,14 @@ int32_t fsb_sift_features_batch_d(fsb_ctx* ctx, int32_t n_img, const uint8_t* co
         nf_max = nfeats[i] > nf_max ? nfeats[i] : nf_max;
     }
     FSB_TRY(use_device(ctx));
+    if (h_imgs) {
+        for (int i = 0; i < n_img; ++i) {
+            FSB_ARG(h_imgs[i], "null host image");
+            cudaPointerAttributes at{};
+            FSB_CUDA(cudaPointerGetAttributes(&at, h_imgs[i]));
+            FSB_ARG(at.type == cudaMemoryTypeHost, "host images must be page-locked (cudaHostAlloc / registered)");
+        }
+    }
     auto& x = ctx->xb;
     cudaStream_t s = ctx->stream;
     const bool timing = ctx->timing;
@@ -814,6 +853,9 @@ int32_t fsb_sift_features_batch_d(fsb_ctx* ctx, int32_t n_img, const uint8_t* co
             ~Guard() { give_back(c, w); }
         } guard{ctx, ws};
         FSB_TRY(prepare_workspace(*ws, h, w));
+        if (h_imgs)
+            FSB_CUDA(cudaMemcpyAsync(const_cast<uint8_t*>(d_imgs[0]), h_imgs[0], (size_t)h * stride,
+                                     cudaMemcpyHostToDevice, s));
         FSB_TRY(detect_dev(ctx, *ws, d_imgs[0], stride, p, (int)((double)nfeats[0] * 2.2)));
         int n0 = 0;
         FSB_TRY(features_dev(ctx, *ws, nfeats[0], (p->flags & FSB_SIFT_EXACT_BLUR) != 0, d_xy[0],
@@ -834,6 +876,14 @@ int32_t fsb_sift_features_batch_d(fsb_ctx* ctx, int32_t n_img, const uint8_t* co
         x.ws.push_back(new Workspace());
     }
     if (!x.fork) FSB_CUDA(cudaEventCreateWithFlags(&x.fork, cudaEventDisableTiming));
+    if (h_imgs) {
+        if (!x.upload) FSB_CUDA(cudaStreamCreateWithFlags(&x.upload, cudaStreamNonBlocking));
+        while ((int)x.uploaded.size() < n_img) {
+            cudaEvent_t ev;
+            FSB_CUDA(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+            x.uploaded.push_back(ev);
+        }
+    }
     AsyncCaps caps{};
     Workspace probe;
     probe.g = make_geometry(h, w);
@@ -870,6 +920,7 @@ int32_t fsb_sift_features_batch_d(fsb_ctx* ctx, int32_t n_img, const uint8_t* co
     // the captured graph is replayed while every argument and buffer address is unchanged
     std::vector<char> key;
     key_put(key, n_img);
+    key_put(key, h_imgs != nullptr);   // the uploads' sources are set per launch, not keyed
     key_put(key, h);
     key_put(key, w);
     key_put(key, stride);
@@ -898,7 +949,7 @@ int32_t fsb_sift_features_batch_d(fsb_ctx* ctx, int32_t n_img, const uint8_t* co
         if (x.graph.graph) cudaGraphDestroy(x.graph.graph);
         x.graph.exec = nullptr;
         x.graph.graph = nullptr;
-        BatchCall bc{n_img, d_imgs, h, w, stride, p, nfeats, d_xy, d_resp, d_rootsift, d_counts};
+        BatchCall bc{n_img, d_imgs, h_imgs, h, w, stride, p, nfeats, d_xy, d_resp, d_rootsift, d_counts};
         FSB_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
         const int32_t st = batch_body(ctx, bc);
         cudaGraph_t g = nullptr;
@@ -915,6 +966,11 @@ int32_t fsb_sift_features_batch_d(fsb_ctx* ctx, int32_t n_img, const uint8_t* co
         x.graph.graph = g;
         FSB_CUDA(cudaGraphInstantiate(&x.graph.exec, g, 0));
         x.graph.key = key;
+    }
+    if (h_imgs) {
+        for (int i = 0; i < n_img; ++i)
+            FSB_CUDA(cudaGraphExecMemcpyNodeSetParams1D(x.graph.exec, x.copy_nodes[i], const_cast<uint8_t*>(d_imgs[i]),
+                                                        h_imgs[i], (size_t)h * stride, cudaMemcpyHostToDevice));
     }
     FSB_CUDA(cudaGraphLaunch(x.graph.exec, s));
     // one wait per batch: the flags say which images (if any) exceeded a capacity
@@ -949,6 +1005,28 @@ int32_t fsb_sift_features_batch_d(fsb_ctx* ctx, int32_t n_img, const uint8_t* co
     }
     if (h_counts) std::memcpy(h_counts, h_cnt, (size_t)n_img * 4);
     return FSB_OK;
+}
+}  // namespace
+}  // namespace fsb
+
+extern "C" {
+
+int32_t fsb_sift_features_batch_d(fsb_ctx* ctx, int32_t n_img, const uint8_t* const* d_imgs, int32_t h, int32_t w,
+                                  int32_t stride, const fsb_sift_params* p, const int32_t* nfeats, float* const* d_xy,
+                                  float* const* d_resp, uint8_t* const* d_rootsift, int32_t* d_counts,
+                                  int32_t* h_counts, int32_t chains) {
+    return fsb::sift_features_batch(ctx, n_img, nullptr, d_imgs, h, w, stride, p, nfeats, d_xy, d_resp, d_rootsift,
+                                    d_counts, h_counts, chains);
+}
+
+int32_t fsb_sift_features_batch_hd(fsb_ctx* ctx, int32_t n_img, const uint8_t* const* h_imgs,
+                                   uint8_t* const* d_imgs, int32_t h, int32_t w, int32_t stride,
+                                   const fsb_sift_params* p, const int32_t* nfeats, float* const* d_xy,
+                                   float* const* d_resp, uint8_t* const* d_rootsift, int32_t* d_counts,
+                                   int32_t* h_counts, int32_t chains) {
+    FSB_ARG(n_img <= 0 || h_imgs, "null host image array");
+    return fsb::sift_features_batch(ctx, n_img, h_imgs, d_imgs, h, w, stride, p, nfeats, d_xy, d_resp, d_rootsift,
+                                    d_counts, h_counts, chains);
 }
 
 int32_t fsb_project_d(fsb_ctx* ctx, const float* d_xy, int32_t n, const double* hm9, const float* d_offset,

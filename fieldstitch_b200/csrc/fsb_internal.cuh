@@ -178,6 +178,9 @@ struct fsb_ctx {
         std::vector<fsb::Workspace*> ws;
         std::vector<cudaEvent_t> join;
         cudaEvent_t fork = nullptr;
+        cudaStream_t upload = nullptr;            // host-image batches: the uploads, in image order
+        std::vector<cudaEvent_t> uploaded;        // image i on the device (captured edges)
+        std::vector<cudaGraphNode_t> copy_nodes;  // the upload of image i in the captured graph
         fsb::GuidedGraph graph;
         fsb::DevBuf status;
         fsb::AsyncCaps caps{};

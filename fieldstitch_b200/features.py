@@ -117,12 +117,15 @@ def sift_gpu_batch(images, nfeats, streams=4, contrast=0.015, edge=12.0, exact=F
 
 
 def sift_gpu_batch_d(images, nfeats, out_xy, out_u8, out_resp=None, chains=8, contrast=0.015, edge=12.0,
-                     exact=False, device=0):
+                     exact=False, device=0, host_images=None):
     """Batched feature extraction on device data with no host wait inside the batch
     (fsb_sift_features_batch_d: one CUDA graph, `chains` images in flight). images: same-size
     uint8 CUDA tensors; nfeats: one cap per image; out_xy[i] (>= nfeat, 2) float32, out_u8[i]
-    (>= nfeat, 128) uint8 and optionally out_resp[i] CUDA tensors. Returns the feature counts (host
-    list); equal to sift_gpu_u8 / fsb_sift_features_d image by image."""
+    (>= nfeat, 128) uint8 and optionally out_resp[i] CUDA tensors. With host_images (page-locked
+    host arrays or CPU tensors, one per image, rows as long as the device images'), the graph
+    uploads host_images[i] into images[i] itself, overlapping the uploads with the extraction
+    (fsb_sift_features_batch_hd). Returns the feature counts (host list); equal to sift_gpu_u8 /
+    fsb_sift_features_d image by image."""
     import ctypes
 
     import torch
@@ -133,27 +136,53 @@ def sift_gpu_batch_d(images, nfeats, out_xy, out_u8, out_resp=None, chains=8, co
     h, w = images[0].shape
     if any(tuple(im.shape) != (h, w) for im in images):
         raise ValueError("the images of a batch share one size")
+    stride = images[0].stride(0)
     ctx = _lib.context(device)
     Pv, Iv = ctypes.c_void_p * n, ctypes.c_int32 * n
     counts = torch.empty(n, dtype=torch.int32, device=images[0].device)
     h_counts = Iv()
     prm = _lib.SiftParams(float(contrast), float(edge), 0, _lib.SIFT_EXACT_BLUR if exact else 0)
+    outs = (Iv(*[int(v) for v in nf]), Pv(*[t.data_ptr() for t in out_xy]),
+            Pv(*[t.data_ptr() for t in out_resp]) if out_resp is not None else None,
+            Pv(*[t.data_ptr() for t in out_u8]), ctypes.c_void_p(counts.data_ptr()), h_counts, int(chains))
     torch.cuda.current_stream(images[0].device).synchronize()
-    _lib.check(ctx.lib.fsb_sift_features_batch_d(
-        ctx.handle, n, Pv(*[im.data_ptr() for im in images]), h, w, images[0].stride(0), ctypes.byref(prm),
-        Iv(*[int(v) for v in nf]), Pv(*[t.data_ptr() for t in out_xy]),
-        Pv(*[t.data_ptr() for t in out_resp]) if out_resp is not None else None, Pv(*[t.data_ptr() for t in out_u8]),
-        ctypes.c_void_p(counts.data_ptr()), h_counts, int(chains)), "fsb_sift_features_batch_d")
+    if host_images is None:
+        _lib.check(ctx.lib.fsb_sift_features_batch_d(ctx.handle, n, Pv(*[im.data_ptr() for im in images]), h, w,
+                                                     stride, ctypes.byref(prm), *outs), "fsb_sift_features_batch_d")
+    else:
+        hp = []
+        for im in host_images:
+            if isinstance(im, torch.Tensor):
+                ok = im.dtype == torch.uint8 and tuple(im.shape) == (h, w) and im.stride(0) == stride
+                hp.append(im.data_ptr())
+            else:
+                ok = im.dtype == np.uint8 and im.shape == (h, w) and im.strides == (stride, 1)
+                hp.append(im.ctypes.data)
+            if not ok:
+                raise ValueError("host images: uint8 (%d, %d) with %d-byte rows" % (h, w, stride))
+        _lib.check(ctx.lib.fsb_sift_features_batch_hd(ctx.handle, n, Pv(*hp), Pv(*[im.data_ptr() for im in images]),
+                                                      h, w, stride, ctypes.byref(prm), *outs),
+                   "fsb_sift_features_batch_hd")
     return [h_counts[i] for i in range(n)]
+
+
+def _all_pinned(images):
+    """True when every image is a host array in page-locked memory (the graph can upload it)."""
+    import torch
+    for im in images:
+        a = np.asarray(im)
+        if a.dtype != np.uint8 or not a.flags["C_CONTIGUOUS"] or not torch.from_numpy(a).is_pinned():
+            return False
+    return True
 
 
 _BATCH_BUFS = {}
 
 
 def sift_gpu_u8_batch(images, nfeats, chains=8, contrast=0.015, edge=12.0, exact=False, device=0):
-    """sift_gpu_u8 of many same-size host images as one sync-free batch: the images go to the
-    device (asynchronously when they are in page-locked memory), one CUDA graph extracts them all
-    (fsb_sift_features_batch_d) and the results come back. Returns [(xy float32 (n,2), RootSIFT
+    """sift_gpu_u8 of many same-size host images as one sync-free batch: one CUDA graph extracts
+    them all (fsb_sift_features_batch_d; images in page-locked memory are uploaded by the graph
+    itself, overlapping the extraction: fsb_sift_features_batch_hd) and the results come back. Returns [(xy float32 (n,2), RootSIFT
     uint8 (n,128), resp float32 (n,))], equal to sift_gpu_u8 image by image. The device buffers are
     kept between calls of the same shape, so a repeated batch replays its graph."""
     import torch
@@ -172,12 +201,15 @@ def sift_gpu_u8_batch(images, nfeats, chains=8, contrast=0.015, edge=12.0, exact
                             "u8": torch.empty((n, nmax, 128), dtype=torch.uint8, device=dev),
                             "rs": torch.empty((n, nmax), dtype=torch.float32, device=dev)}
     b = _BATCH_BUFS[key]
-    for i, im in enumerate(images):
-        t = torch.from_numpy(np.ascontiguousarray(im, np.uint8))
-        b["img"][i].copy_(t, non_blocking=t.is_pinned())
+    host = None
+    if _all_pinned(images):   # the graph uploads them, overlapping the extraction
+        host = [np.asarray(im) for im in images]
+    else:
+        for i, im in enumerate(images):
+            b["img"][i].copy_(torch.from_numpy(np.ascontiguousarray(im, np.uint8)))
     counts = sift_gpu_batch_d([b["img"][i] for i in range(n)], nf, [b["xy"][i] for i in range(n)],
                               [b["u8"][i] for i in range(n)], [b["rs"][i] for i in range(n)], chains, contrast,
-                              edge, exact, device)
+                              edge, exact, device, host_images=host)
     # the valid rows of every image gathered on the device, one copy per kind back to the host
     if sum(counts) == 0:
         return [(np.zeros((0, 2), np.float32), np.zeros((0, 128), np.uint8), np.zeros(0, np.float32)) for _ in counts]

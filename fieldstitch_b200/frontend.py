@@ -4,11 +4,12 @@ every pair, with the features kept in device memory between the two stages.
 In the reference, the feature workers write one npz file per photo (features._save,
 app/planesite/features.py:74-86) and the pair workers read them back (matching._get,
 app/planesite/matching.py:48-64) before guided matching (matching._guided, matching.py:113-152).
-``extract_and_match`` does the same work for a batch: the images go to the device (one copy
-each, asynchronous from page-locked memory), one CUDA graph extracts them all
-(features.sift_gpu_batch_d), every pair's prior prediction is projected on the device, one CUDA
-graph matches every pair (matching.guided_from_pred_batch_d), and the match lists come back in one
-copy. The features come back too when asked for (one copy per kind).
+``extract_and_match`` does the same work for a batch: one CUDA graph extracts every image
+(features.sift_gpu_batch_d; images in page-locked memory are uploaded by that graph, each
+image's extraction starting once its own upload is done), every pair's prior prediction is
+projected on the device, one CUDA graph matches every pair (matching.guided_from_pred_batch_d),
+and the match lists come back in one copy. The features come back too when asked for (one copy
+per kind).
 """
 import ctypes
 
@@ -41,7 +42,8 @@ def extract_and_match(images, nfeats, pairs, priors, radius, kc=16, ratio=0.85, 
                       return_features=False, contrast=0.015, edge=12.0, device=0):
     """Features of every image and guided matches of every pair.
 
-    images: same-size uint8 host arrays (page-locked ones are copied asynchronously); nfeats: one
+    images: same-size uint8 host arrays (page-locked ones are uploaded inside the extraction
+    graph, overlapping the extraction of the images before them); nfeats: one
     keypoint cap per image (features.sift_gpu's nfeat); pairs: list of (i, j) image indices;
     priors: one 3x3 homography per pair mapping image i pixels to image j pixels (the GNSS /
     gimbal prior of matching._predict in homography form); offsets: optional per-pair float32
@@ -57,9 +59,12 @@ def extract_and_match(images, nfeats, pairs, priors, radius, kc=16, ratio=0.85, 
     nf = list(nfeats) if np.ndim(nfeats) else [int(nfeats)] * n_img
     nmax = max(1, max(int(v) for v in nf))
     b = _buffers(n_img, h, w, nmax, max(P, 1), device)
-    for i, im in enumerate(images):
-        t = torch.from_numpy(np.ascontiguousarray(im, np.uint8))
-        b["img"][i].copy_(t, non_blocking=t.is_pinned())
+    host = None
+    if features._all_pinned(images):   # uploaded by the extraction graph, overlapping the extraction
+        host = [np.asarray(im) for im in images]
+    else:
+        for i, im in enumerate(images):
+            b["img"][i].copy_(torch.from_numpy(np.ascontiguousarray(im, np.uint8)))
     if offsets is not None:
         off = np.zeros((max(P, 1), nmax, 2), np.float32)
         for p, o in enumerate(offsets):
@@ -68,7 +73,7 @@ def extract_and_match(images, nfeats, pairs, priors, radius, kc=16, ratio=0.85, 
         b["off"].copy_(torch.from_numpy(off))
     counts = features.sift_gpu_batch_d([b["img"][i] for i in range(n_img)], nf, [b["xy"][i] for i in range(n_img)],
                                        [b["u8"][i] for i in range(n_img)], [b["rs"][i] for i in range(n_img)], chains,
-                                       contrast, edge, False, device)
+                                       contrast, edge, False, device, host_images=host)
     if P:
         # image j's keypoints as float64 positions, every pair's prediction, on the device
         ctx = _lib.context(device)

@@ -166,6 +166,18 @@ int32_t fsb_sift_features_batch_d(fsb_ctx* ctx, int32_t n_img, const uint8_t* co
                                   int32_t stride, const fsb_sift_params* p, const int32_t* nfeats, float* const* d_xy,
                                   float* const* d_resp, uint8_t* const* d_rootsift, int32_t* d_counts,
                                   int32_t* h_counts, int32_t chains);
+/* fsb_sift_features_batch_d from host images: h_imgs[i] (page-locked host memory, h rows of
+   `stride` bytes) is uploaded into d_imgs[i] by the same graph, on a copy stream in image order,
+   and image i's extraction waits for its own upload only, so the uploads of later images overlap
+   the extraction of earlier ones. The graph is keyed like fsb_sift_features_batch_d's (device
+   buffers, not host addresses): a later call with other host buffers replays it with the uploads
+   re-pointed. Pageable host memory is rejected (FSB_ERR_ARG). The end-to-end form of the
+   reference's per-photo worker loop (app/planesite/features.py:115-129 over a spawn queue). */
+int32_t fsb_sift_features_batch_hd(fsb_ctx* ctx, int32_t n_img, const uint8_t* const* h_imgs,
+                                   uint8_t* const* d_imgs, int32_t h, int32_t w, int32_t stride,
+                                   const fsb_sift_params* p, const int32_t* nfeats, float* const* d_xy,
+                                   float* const* d_resp, uint8_t* const* d_rootsift, int32_t* d_counts,
+                                   int32_t* h_counts, int32_t chains);
 /* Prior prediction: projects n float32 points (d_xy, n*2) through the homography hm9 (host,
    row-major 3x3) into float64 positions d_out (n*2), adding the float32 offsets d_offset (n*2,
    nullable) - e.g. a GNSS/gimbal prior and its error. Identity hm9 converts to float64. */

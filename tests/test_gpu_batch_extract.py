@@ -103,3 +103,73 @@ def test_extract_and_match_equals_per_pair_calls():
         for (gxy, gu8, grs), (wxy, wu8, wrs) in zip(fe, feats):
             np.testing.assert_array_equal(gxy, wxy)
             np.testing.assert_array_equal(gu8, wu8)
+
+
+def _pinned(a):
+    import torch
+    t = torch.empty(a.shape, dtype=torch.uint8, pin_memory=True)
+    t.numpy()[...] = a
+    return t
+
+
+def test_graph_uploads_from_page_locked_images():
+    """fsb_sift_features_batch_hd (the uploads captured in the extraction graph, each image's chain
+    waiting for its own upload): the per-image results, on the capture and on replays whose host
+    buffers are other page-locked arrays (the uploads re-pointed, the graph kept), with the batch
+    larger than the chains so later uploads overlap earlier extractions."""
+    import fieldstitch_b200 as F
+    from fieldstitch_b200 import synth
+    imgs = [synth.synth_image(600, 800, 900 + k) for k in range(7)]
+    nfeats = [2000, 300, 5000, 50, 1200, 800, 2500]
+    want = [_per_image(F, im, nf) for im, nf in zip(imgs, nfeats)]
+    assert F.features._all_pinned([_pinned(imgs[0]).numpy()])
+    for rep in range(3):
+        hold = [_pinned(im) for im in imgs]   # new page-locked buffers every call
+        got = F.features.sift_gpu_u8_batch([t.numpy() for t in hold], nfeats, chains=3)
+        for k, ((gxy, gu8, grs), (wxy, wu8, wrs)) in enumerate(zip(got, want)):
+            np.testing.assert_array_equal(gxy, wxy, err_msg="call %d image %d" % (rep, k))
+            np.testing.assert_array_equal(gu8, wu8)
+            np.testing.assert_array_equal(grs, wrs)
+
+
+def test_graph_uploads_reject_pageable_memory():
+    import ctypes
+
+    import torch
+
+    from fieldstitch_b200 import _lib
+    ctx = _lib.context(0)
+    prm = _lib.SiftParams(0.015, 12.0, 0, 0)
+    img = np.zeros((64, 64), np.uint8)   # pageable
+    d = torch.zeros((64, 64), dtype=torch.uint8, device="cuda:0")
+    xy = torch.zeros((10, 2), dtype=torch.float32, device="cuda:0")
+    u8 = torch.zeros((10, 128), dtype=torch.uint8, device="cuda:0")
+    cnt = torch.zeros(1, dtype=torch.int32, device="cuda:0")
+    P1, I1 = ctypes.c_void_p * 1, ctypes.c_int32 * 1
+    st = ctx.lib.fsb_sift_features_batch_hd(ctx.handle, 1, P1(img.ctypes.data), P1(d.data_ptr()), 64, 64, 64,
+                                            ctypes.byref(prm), I1(10), P1(xy.data_ptr()), None, P1(u8.data_ptr()),
+                                            ctypes.c_void_p(cnt.data_ptr()), None, 2)
+    assert st == 1 and b"page-locked" in ctx.lib.fsb_last_error()
+
+
+def test_extract_and_match_from_page_locked_images():
+    """frontend.extract_and_match with page-locked images (the uploads inside the extraction graph)
+    returns the matches of the pageable-input path."""
+    import fieldstitch_b200 as F
+    from fieldstitch_b200 import synth
+    h, w = 700, 900
+    src = [synth.synth_pair(h, w, 800 + k) for k in range(3)]
+    imgs = [im for a, b, _ in src for im in (a, b)]
+    nfeats = [3000, 2500, 800, 4000, 1500, 1500]
+    pairs = [(0, 1), (2, 3), (4, 5)]
+    priors = [s[2] for s in src]
+    offs = [synth.prior_noise(5000, 60 + p) for p in range(len(pairs))]
+    want = F.frontend.extract_and_match(imgs, nfeats, pairs, priors, 40.0, 16, 0.85, offsets=offs, chains=2)
+    for _ in range(2):
+        hold = [_pinned(im) for im in imgs]
+        got = F.frontend.extract_and_match([t.numpy() for t in hold], nfeats, pairs, priors, 40.0, 16, 0.85,
+                                           offsets=offs, chains=2)
+        for (gq, gt), (wq, wt) in zip(got, want):
+            assert len(wq) > 0
+            np.testing.assert_array_equal(gq, wq)
+            np.testing.assert_array_equal(gt, wt)
