@@ -61,7 +61,7 @@ def parse():
     p.add_argument("--extract", default="graph", choices=["graph", "threads"],
                    help="graph: every image of a step in one sync-free batch (one CUDA graph); threads: "
                         "fsb_sift_features_d per image on --streams host threads")
-    p.add_argument("--chains", type=int, default=8, help="images in flight inside the extraction graph")
+    p.add_argument("--chains", type=int, default=16, help="images in flight inside the extraction graph")
     p.add_argument("--sweep-pairs", type=int, default=256, help="dense precision sweep: pairs per batch (0: skip)")
     p.add_argument("--sweep-n", type=int, default=16384, help="dense precision sweep: descriptors per image")
     p.add_argument("--plain-pairs", type=int, default=16,

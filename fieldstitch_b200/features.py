@@ -116,7 +116,7 @@ def sift_gpu_batch(images, nfeats, streams=4, contrast=0.015, edge=12.0, exact=F
     return _batch(lambda j: sift_gpu_u8(j[0], j[1], contrast, edge, exact, device), jobs, streams)
 
 
-def sift_gpu_batch_d(images, nfeats, out_xy, out_u8, out_resp=None, chains=8, contrast=0.015, edge=12.0,
+def sift_gpu_batch_d(images, nfeats, out_xy, out_u8, out_resp=None, chains=16, contrast=0.015, edge=12.0,
                      exact=False, device=0, host_images=None):
     """Batched feature extraction on device data with no host wait inside the batch
     (fsb_sift_features_batch_d: one CUDA graph, `chains` images in flight). images: same-size
@@ -179,7 +179,7 @@ def _all_pinned(images):
 _BATCH_BUFS = {}
 
 
-def sift_gpu_u8_batch(images, nfeats, chains=8, contrast=0.015, edge=12.0, exact=False, device=0):
+def sift_gpu_u8_batch(images, nfeats, chains=16, contrast=0.015, edge=12.0, exact=False, device=0):
     """sift_gpu_u8 of many same-size host images as one sync-free batch: one CUDA graph extracts
     them all (fsb_sift_features_batch_d; images in page-locked memory are uploaded by the graph
     itself, overlapping the extraction: fsb_sift_features_batch_hd) and the results come back. Returns [(xy float32 (n,2), RootSIFT

@@ -38,7 +38,7 @@ def _buffers(n_img, h, w, nmax, n_pairs, device):
     return _BUFS[key]
 
 
-def extract_and_match(images, nfeats, pairs, priors, radius, kc=16, ratio=0.85, offsets=None, chains=8,
+def extract_and_match(images, nfeats, pairs, priors, radius, kc=16, ratio=0.85, offsets=None, chains=16,
                       return_features=False, contrast=0.015, edge=12.0, device=0):
     """Features of every image and guided matches of every pair.
 
