@@ -14,8 +14,10 @@ extraction of both images + the match.
 value  : pairs/s with the images resident in HBM (device-pointer C ABI, fsb_*_d).
 e2e    : the same pairs through the public host API (features.sift_gpu_u8 + matching
          guided_from_pred) with host buffers, copies included.
-roofline: the pyramid (dominant stage) from CUDA events on the library stream over the timed
-         steps; algorithmic bytes per image = H*W + 44 * (sum of octave pixels).
+roofline: the pyramid (dominant stage): the step's images through the pyramid stage alone as one
+         graph with the extraction graph's images in flight (fsb_pyramid_batch_d), CUDA events on its
+         stream; beside it the same for one image at a time on one stream; algorithmic bytes per
+         image = H*W + 44 * (sum of octave pixels).
 --impl reference: the reference's CPU implementation of the path (OpenCV SIFT as
          features.sift_cpu calls it + the NumPy/cKDTree guided matcher), oracle port, on the host
          cores; one pair per step.
@@ -962,7 +964,7 @@ def run_fsb(args):
             res = list(pool.map(e2e_pair, range(len(pairs))))
             return sum(r[0] for r in res), sum(r[1] for r in res)
 
-        e_imgs = [im for a, b in host for im in (a, b)]
+        x_imgs = [im for a, b in host for im in (a, b)]
         e_nfs = [pairs[i][3 + k] for i in range(len(pairs)) for k in range(2)]
         e_pairs = [(2 * i, 2 * i + 1) for i in range(len(pairs))]
         e_priors = [pairs[i][2] for i in range(len(pairs))]
@@ -972,10 +974,10 @@ def run_fsb(args):
             """frontend.extract_and_match: the step's host images to the device, one graph extracting
             every image, the priors projected on the device, one graph matching every pair, the match
             lists back to the host."""
-            res = F.frontend.extract_and_match(e_imgs, e_nfs, e_pairs, e_priors, RADIUS, KC, RATIO, offsets=e_off,
+            res = F.frontend.extract_and_match(x_imgs, e_nfs, e_pairs, e_priors, RADIUS, KC, RATIO, offsets=e_off,
                                                chains=args.chains, device=local)
-            h2d = sum(im.nbytes for im in e_imgs) + 16 * len(e_pairs) * max(e_nfs) + 72 * len(e_pairs)
-            d2h = sum(16 * len(q) for q, _ in res) + 4 * len(e_imgs)
+            h2d = sum(im.nbytes for im in x_imgs) + 16 * len(e_pairs) * max(e_nfs) + 72 * len(e_pairs)
+            d2h = sum(16 * len(q) for q, _ in res) + 4 * len(x_imgs)
             return h2d, d2h
 
         e2e_step = e2e_step_batch if args.extract == "graph" else e2e_step_threads
@@ -1010,8 +1012,25 @@ def run_fsb(args):
                                "images in pinned host memory; keypoints / descriptors between the two calls in "
                                "the numpy arrays the API returns")}
 
-    # ---- roofline of the dominant stage (pyramid): CUDA events on the library stream, one stream
-    # alone (8 images), so the per-image time is not inflated by the other streams' kernels
+    # ---- roofline of the dominant stage (pyramid), in the configuration the extraction graph runs
+    # it: the pyramids of the step's images alone as one graph (fsb_pyramid_batch_d, args.chains
+    # images in flight), CUDA events on the extraction context's stream around 3 replays
+    def pyr_batch():
+        _lib.check(ectx.lib.fsb_pyramid_batch_d(ectx.handle, NI, e_imgs, h, w, w, 0, args.chains), "pyramid batch")
+
+    pyr_batch()
+    pyr_batch()
+    torch.cuda.synchronize()
+    pb0, pb1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    pyr_reps = 3
+    pb0.record(estream)
+    for _ in range(pyr_reps):
+        pyr_batch()
+    pb1.record(estream)
+    torch.cuda.synchronize()
+    pyr_batch_ms = pb0.elapsed_time(pb1) / (pyr_reps * NI)
+    # and one image at a time on one stream (the latency of one image's launch chain; octaves 3-8
+    # are launch-latency bound there)
     iso = workers[0]
     iso.ctx.timing(True)
     iso.ctx.stage_times()
@@ -1022,15 +1041,20 @@ def run_fsb(args):
     pyr_ms, pyr_n = iso_st["pyramid"]
     per_img_ms = pyr_ms / max(pyr_n, 1)
     alg = pyramid_bytes(h, w)
-    achieved = alg / (per_img_ms / 1000.0) / 1e9 if per_img_ms > 0 else None
-    c_ms, c_n = stages["pyramid"]
+    achieved = alg / (pyr_batch_ms / 1000.0) / 1e9 if pyr_batch_ms > 0 else None
+    ach_one = alg / (per_img_ms / 1000.0) / 1e9 if per_img_ms > 0 else None
     roof = {"bound": "hbm", "kernel": "pyramid of one image (base + per octave the per-layer kernels or the fused "
                                       "layer groups, autotuned)",
             "achieved": achieved, "peak": pk, "peak_source": pk_src, "unit": "GB/s",
             "frac": (achieved / pk) if achieved else None, "traffic": traffic_per_pyramid(),
-            "algorithmic_bytes": alg, "ms_per_launch_group": per_img_ms,
-            "measured": "CUDA events on the library stream, one stream alone, %d images" % pyr_n,
-            "ms_per_launch_group_in_timed_region": c_ms / max(c_n, 1)}
+            "algorithmic_bytes": alg, "ms_per_launch_group": pyr_batch_ms,
+            "measured": ("CUDA events on the extraction stream around %d replays of the pyramid stage of the step's "
+                         "%d images as one graph (fsb_pyramid_batch_d, %d in flight: the configuration of the "
+                         "extraction graph); time per image" % (pyr_reps, NI, args.chains)),
+            "one_stream": {"achieved": ach_one, "frac": (ach_one / pk) if ach_one else None,
+                           "ms_per_launch_group": per_img_ms,
+                           "measured": "CUDA events on the library stream, one image at a time on one stream, "
+                                       "%d images (includes the launch-chain latency of octaves 3-8)" % pyr_n}}
     n_iso = max(pyr_n, 1)
     iso_stages = {k: v[0] / n_iso for k, v in iso_st.items() if v[1] > 0}
 

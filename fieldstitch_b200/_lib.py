@@ -55,6 +55,7 @@ SIGNATURES = [
                                           c_vp, c_vp, c_i32]),
     ("fsb_sift_features_batch_hd", c_i32, [c_vp, c_i32, c_vp, c_vp, c_i32, c_i32, c_i32, c_vp, c_vp, c_vp, c_vp,
                                            c_vp, c_vp, c_vp, c_i32]),
+    ("fsb_pyramid_batch_d", c_i32, [c_vp, c_i32, c_vp, c_i32, c_i32, c_i32, c_i32, c_i32]),
     ("fsb_find_fundamental_batch", c_i32, [c_vp, c_i32, c_vp, c_vp, c_vp, ctypes.c_double, c_i32, ctypes.c_uint64,
                                            c_vp, c_vp, c_vp]),
     ("fsb_spread", c_i32, [c_vp, c_vp, c_vp, c_vp, c_i32, c_i32, c_i32, c_i32, c_i32, c_vp, c_vp]),

@@ -510,8 +510,11 @@ int32_t fsb_destroy(fsb_ctx* ctx) {
     {
         auto& x = ctx->xb;
         for (cudaStream_t cs : x.streams) cudaStreamSynchronize(cs);
+        if (x.upload) cudaStreamSynchronize(x.upload);
         if (x.graph.exec) cudaGraphExecDestroy(x.graph.exec);
         if (x.graph.graph) cudaGraphDestroy(x.graph.graph);
+        if (x.pyr_graph.exec) cudaGraphExecDestroy(x.pyr_graph.exec);
+        if (x.pyr_graph.graph) cudaGraphDestroy(x.pyr_graph.graph);
         for (Workspace* w : x.ws) {
             w->release();
             delete w;
@@ -519,6 +522,8 @@ int32_t fsb_destroy(fsb_ctx* ctx) {
         for (cudaStream_t cs : x.streams) cudaStreamDestroy(cs);
         for (cudaEvent_t e : x.join) cudaEventDestroy(e);
         if (x.fork) cudaEventDestroy(x.fork);
+        for (cudaEvent_t e : x.uploaded) cudaEventDestroy(e);
+        if (x.upload) cudaStreamDestroy(x.upload);
         x.status.release();
     }
     if (ctx->pinned) cudaFreeHost(ctx->pinned);
@@ -982,7 +987,7 @@ int32_t sift_features_batch(fsb_ctx* ctx, int32_t n_img, const uint8_t* const* h
     FSB_CUDA(cudaStreamSynchronize(s));
     for (int i = 0; i < n_img; ++i) {
         if (h_status[i] & 8u) {
-            set_error("pyramid: a TMA row copy did not complete in time (strip engine), image %d", i);
+            set_error("pyramid: a TMA copy of the pyramid did not complete in time, image %d", i);
             return FSB_ERR_TIMEOUT;
         }
         if (h_status[i] == 0) continue;
@@ -1027,6 +1032,119 @@ int32_t fsb_sift_features_batch_hd(fsb_ctx* ctx, int32_t n_img, const uint8_t* c
     FSB_ARG(n_img <= 0 || h_imgs, "null host image array");
     return fsb::sift_features_batch(ctx, n_img, h_imgs, d_imgs, h, w, stride, p, nfeats, d_xy, d_resp, d_rootsift,
                                     d_counts, h_counts, chains);
+}
+
+int32_t fsb_pyramid_batch_d(fsb_ctx* ctx, int32_t n_img, const uint8_t* const* d_imgs, int32_t h, int32_t w,
+                            int32_t stride, int32_t flags, int32_t chains) {
+    FSB_ARG(ctx, "null context");
+    FSB_ARG(n_img >= 0, "n_img < 0");
+    if (n_img == 0) return FSB_OK;
+    FSB_ARG(d_imgs, "null image array");
+    FSB_ARG(h > 0 && w > 0 && stride >= w, "bad image size or stride");
+    FSB_ARG(h <= 32768 && w <= 32768, "image larger than 32768 pixels on a side");
+    FSB_ARG(chains >= 1 && chains <= 32, "chains must be 1..32");
+    for (int i = 0; i < n_img; ++i) FSB_ARG(d_imgs[i], "null image pointer");
+    FSB_TRY(use_device(ctx));
+    const bool exact = (flags & FSB_SIFT_EXACT_BLUR) != 0;
+    auto& x = ctx->xb;
+    cudaStream_t s = ctx->stream;
+    while ((int)x.streams.size() < chains) {
+        cudaStream_t cs;
+        cudaEvent_t ev;
+        FSB_CUDA(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
+        FSB_CUDA(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+        x.streams.push_back(cs);
+        x.join.push_back(ev);
+        x.ws.push_back(new Workspace());
+    }
+    if (!x.fork) FSB_CUDA(cudaEventCreateWithFlags(&x.fork, cudaEventDisableTiming));
+    for (int c = 0; c < chains; ++c)
+        if (x.ws[c]->g.h != h || x.ws[c]->g.w != w) FSB_TRY(prepare_workspace(*x.ws[c], h, w));
+    const bool timing = ctx->timing;
+    ctx->timing = false;
+    struct Restore {
+        fsb_ctx* c;
+        bool t;
+        ~Restore() { c->timing = t; }
+    } restore{ctx, timing};
+    // a geometry's first pyramid runs outside any capture: the autotuner times its variants then
+    if (x.pyr_h != h || x.pyr_w != w) {
+        FSB_TRY(run_pyramid(*x.ws[0], d_imgs[0], stride, exact, s, nullptr, nullptr));
+        FSB_CUDA(cudaStreamSynchronize(s));
+        x.pyr_h = h;
+        x.pyr_w = w;
+    }
+    std::vector<char> key;
+    key_put(key, n_img);
+    key_put(key, h);
+    key_put(key, w);
+    key_put(key, stride);
+    key_put(key, chains);
+    key_put(key, exact);
+    for (int i = 0; i < n_img; ++i) key_put(key, d_imgs[i]);
+    for (int c = 0; c < chains; ++c) {
+        const Workspace* ws = x.ws[c];
+        const void* ptrs[] = {ws->dog.p, ws->mag.p, ws->ang.p, ws->plane[0].p, ws->plane[1].p, ws->plane[2].p,
+                              ws->next_base.p, ws->counters.p};
+        for (const void* q : ptrs) key_put(key, q);
+    }
+    if (!x.pyr_graph.exec || key != x.pyr_graph.key) {
+        if (x.pyr_graph.exec) cudaGraphExecDestroy(x.pyr_graph.exec);
+        if (x.pyr_graph.graph) cudaGraphDestroy(x.pyr_graph.graph);
+        x.pyr_graph.exec = nullptr;
+        x.pyr_graph.graph = nullptr;
+        FSB_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+        int32_t st = FSB_OK;
+        [&]() {
+            auto chk = [&](cudaError_t e) {
+                if (e != cudaSuccess && st == FSB_OK) {
+                    set_error("capture of the pyramid batch: %s", cudaGetErrorString(e));
+                    st = FSB_ERR_CUDA;
+                }
+                return st == FSB_OK;
+            };
+            if (!chk(cudaEventRecord(x.fork, s))) return;
+            for (int c = 0; c < chains; ++c)
+                if (!chk(cudaStreamWaitEvent(x.streams[c], x.fork, 0))) return;
+            for (int i = 0; i < n_img; ++i) {
+                const int c = i % chains;
+                st = run_pyramid(*x.ws[c], d_imgs[i], stride, exact, x.streams[c], nullptr, nullptr);
+                if (st != FSB_OK) return;
+            }
+            for (int c = 0; c < chains; ++c) {
+                if (!chk(cudaEventRecord(x.join[c], x.streams[c]))) return;
+                if (!chk(cudaStreamWaitEvent(s, x.join[c], 0))) return;
+            }
+        }();
+        cudaGraph_t g = nullptr;
+        const cudaError_t e = cudaStreamEndCapture(s, &g);
+        if (st != FSB_OK || e != cudaSuccess) {
+            if (g) cudaGraphDestroy(g);
+            if (st == FSB_OK) {
+                set_error("capture of the pyramid batch failed: %s", cudaGetErrorString(e));
+                st = FSB_ERR_CUDA;
+            }
+            return st;
+        }
+        x.pyr_graph.graph = g;
+        FSB_CUDA(cudaGraphInstantiate(&x.pyr_graph.exec, g, 0));
+        x.pyr_graph.key = key;
+    }
+    FSB_CUDA(cudaGraphLaunch(x.pyr_graph.exec, s));
+    // the error words of the chains' bounded waits (strip engine)
+    const int used = chains < n_img ? chains : n_img;
+    FSB_TRY(stage_ensure(ctx, (size_t)used * 4 + 64));
+    int32_t* h_err = static_cast<int32_t*>(ctx->pinned);
+    for (int c = 0; c < used; ++c)
+        FSB_CUDA(cudaMemcpyAsync(h_err + c, x.ws[c]->counters.as<int32_t>() + PYR_ERR_WORD, 4, cudaMemcpyDeviceToHost,
+                                 s));
+    FSB_CUDA(cudaStreamSynchronize(s));
+    for (int c = 0; c < used; ++c)
+        if (h_err[c]) {
+            set_error("pyramid: a TMA copy of the pyramid did not complete in time, chain %d", c);
+            return FSB_ERR_TIMEOUT;
+        }
+    return FSB_OK;
 }
 
 int32_t fsb_project_d(fsb_ctx* ctx, const float* d_xy, int32_t n, const double* hm9, const float* d_offset,

@@ -621,7 +621,7 @@ int32_t run_detect(fsb_ctx* ctx, Workspace& ws, double contrast, double edge, in
         FSB_CUDA(cudaMemcpyAsync(h_head, cnt, sizeof(h_head), cudaMemcpyDeviceToHost, s));
         FSB_CUDA(cudaStreamSynchronize(s));
         if (h_head[PYR_ERR_WORD]) {
-            set_error("pyramid: a TMA row copy did not complete in time (strip engine)");
+            set_error("pyramid: a TMA copy of the pyramid did not complete in time");
             return FSB_ERR_TIMEOUT;
         }
 

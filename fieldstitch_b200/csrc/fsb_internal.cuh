@@ -182,6 +182,8 @@ struct fsb_ctx {
         std::vector<cudaEvent_t> uploaded;        // image i on the device (captured edges)
         std::vector<cudaGraphNode_t> copy_nodes;  // the upload of image i in the captured graph
         fsb::GuidedGraph graph;
+        fsb::GuidedGraph pyr_graph;   // fsb_pyramid_batch_d
+        int pyr_h = 0, pyr_w = 0;     // geometry whose pyramid ran once outside a capture (autotuned)
         fsb::DevBuf status;
         fsb::AsyncCaps caps{};
         int h = 0, w = 0, warm_ref = 0;
@@ -226,7 +228,7 @@ int32_t launch_octave_fused(const float* L0, int R, int C, float* dog, float* ma
 int layer_tile_variants();
 int layer_tile_height(int variant);
 int32_t launch_layer_fast(int layer, const float* src, int R, int C, float* dst, float* dog, float* mag, float* ang,
-                          float* down, int down_cols, int variant, cudaStream_t s);
+                          float* down, int down_cols, int variant, int* err, cudaStream_t s);
 int32_t launch_base_fast(const uint8_t* img, int stride, int ih, int iw, float* dst, int variant, cudaStream_t s);
 int32_t launch_group_lower(const float* src, int R, int C, float* dog, float* mag, float* ang, float* l3, float* down,
                            int down_cols, cudaStream_t s);

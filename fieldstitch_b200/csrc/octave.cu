@@ -376,6 +376,51 @@ __global__ void __launch_bounds__(NT, 2) k_octave(Args a) {
     cp_wait_all();
 }
 
+// cuTensorMapEncodeTiled through the runtime's driver entry point (no link against libcuda)
+typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                  const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                  CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+EncodeTiledFn encode_tiled() {
+    static EncodeTiledFn fn = [] {
+        void* f = nullptr;
+        cudaDriverEntryPointQueryResult q{};
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &f, cudaEnableDefault, &q) != cudaSuccess ||
+            q != cudaDriverEntryPointSuccess)
+            f = nullptr;
+        return reinterpret_cast<EncodeTiledFn>(f);
+    }();
+    return fn;
+}
+
+
+// bounded waits on a shared-memory mbarrier (TMA completion)
+constexpr long long TSTRIP_TIMEOUT = 2000000000ll;   // cycles (about a second) for one TMA copy
+
+__device__ __forceinline__ uint32_t s_addr(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ bool s_mbar_test(uint64_t* b, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(s_addr(b)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+
+// Waits (bounded) for one row block; every thread waits, then the CTA agrees on the outcome.
+__device__ __forceinline__ bool s_mbar_wait(uint64_t* b, uint32_t parity) {
+    bool ok = s_mbar_test(b, parity);
+    if (!ok) {
+        const long long t0 = clock64();
+        while (!(ok = s_mbar_test(b, parity)) && clock64() - t0 < TSTRIP_TIMEOUT) {
+        }
+    }
+    return ok;
+}
+
 // ------------------------------------------------------------------------------------------------
 // Per-layer tiled kernels (float32 path), 128 x 32 outputs per CTA:
 //   k_layer<I, RAD(I), false>  L_I of one octave from L_{I-1}: the same pair blurs and gradient as
@@ -405,19 +450,26 @@ struct LayerArgs {
     float* ang;
     float* down;        // L_{I-1}[::2, ::2] or null
     int down_cols;
+    int* err;           // set to 1 when the tile's TMA copy does not complete in time
 };
 
+// shared memory: the input tile (LIN_W floats per row), the row-pair tile, the TMA mbarrier
+template <int r, int LY>
+constexpr int layer_bar_off() {
+    return (LY + 2 * r) * LIN_W * 4 + (LY / 2) * LT2_W * 8;
+}
 template <int r, int LY>
 constexpr int layer_smem() {
-    return (LY + 2 * r) * LIN_W * 4 + (LY / 2) * LT2_W * 8;
+    return layer_bar_off<r, LY>() + 16;
 }
 
 template <int TS, int r, bool BASE, int LY>
-__global__ void __launch_bounds__(LNT) k_layer(LayerArgs a) {
+__global__ void __launch_bounds__(LNT) k_layer(const __grid_constant__ CUtensorMap tm, LayerArgs a, int use_tma) {
     constexpr int d = r & 1;
     constexpr int IH = LY + 2 * r;
     constexpr int NPAIR = (LX + 2 * r + 2 * d) / 2;
-    extern __shared__ __align__(16) float sm[];
+    static_assert(layer_bar_off<r, LY>() % 16 == 0, "mbarrier alignment");
+    extern __shared__ __align__(128) float sm[];
     float* s_in = sm;
     float2* t2 = reinterpret_cast<float2*>(sm + IH * LIN_W);
     const int tid = threadIdx.x;
@@ -524,6 +576,34 @@ __global__ void __launch_bounds__(LNT) k_layer(LayerArgs a) {
                 s_in[row * LIN_W + col] = __fadd_rn(__fmul_rn(0.75f, vc), __fmul_rn(0.25f, vn));
             }
         }
+    } else if (use_tma && (s_addr(s_in) & 127) == 0 && y0 >= r && y0 + LY + r <= a.R && x0 >= 16 &&
+               x0 + LX + 16 <= a.C) {
+        // an interior tile (no reflected row or column): one 2-D tensor copy of LIN_W x IH floats
+        // (columns x0 - 16 .., rows y0 - r ..; the copy's last 8 columns are not read and may lie
+        // outside the plane, where the copy fills zeros), completion on an mbarrier
+        uint64_t* bar = reinterpret_cast<uint64_t*>(reinterpret_cast<char*>(sm) + layer_bar_off<r, LY>());
+        if (tid == 0) {
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(s_addr(bar)) : "memory");
+            asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        }
+        __syncthreads();
+        if (tid == 0) {
+            asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(s_addr(bar)),
+                         "r"(IH * LIN_W * 4)
+                         : "memory");
+            asm volatile(
+                "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], "
+                "[%4];" ::"r"(s_addr(s_in)),
+                "l"(reinterpret_cast<uint64_t>(&tm)), "r"(x0 - 16), "r"(y0 - r), "r"(s_addr(bar))
+                : "memory");
+        }
+        if (__syncthreads_or(!s_mbar_wait(bar, 0))) {
+            // the copy did not land in time: flag it, give it one more bounded wait (so that no copy
+            // into this CTA's shared memory is left in flight when possible) and leave the tile
+            if (tid == 0) atomicExch(a.err, 1);
+            s_mbar_wait(bar, 0);
+            return;
+        }
     } else if ((a.C & 3) == 0 && al16(a.src) && x0 >= 16 && x0 + LX + 16 <= a.C) {
         // eight lanes per row (the mirrored row address once per row), five 16-byte copies a lane
         static_assert(LIN_C / 4 == 40, "five copies of eight lanes per row");
@@ -571,6 +651,66 @@ __global__ void __launch_bounds__(LNT) k_layer(LayerArgs a) {
     // 32-byte stride: one bank parity per row pair, opposite parities by the pitch), so the 8
     // lanes cover all 32 banks once
     static_assert(LX == 128 && (LY / 2) % 2 == 0 && LNT % 32 == 0, "horizontal pass mapping");
+    // Fast path for tiles whose outputs and gradient neighbourhoods lie inside the plane, with
+    // 16-byte aligned planes and rows (uniform per CTA): no per-row bounds, border or alignment
+    // tests and 32-bit offsets. Same arithmetic as the general path below, so the same bits.
+    bool fast = (a.C & 3) == 0 && (long long)a.R * a.C < (1ll << 31) && x0 + LX <= a.C && y0 + LY <= a.R &&
+                (!a.dst || al16(a.dst));
+    if (!BASE)
+        fast = fast && al16(a.dog) && (!a.mag || (al16(a.mag) && al16(a.ang))) && y0 >= 1 && y0 + LY <= a.R - 1 &&
+               x0 >= 1 && x0 + LX < a.C;
+    if (fast) {
+        for (int it = tid; it < (LY / 2) * (LX / 4); it += LNT) {
+            const int wi = it >> 5, l = it & 31;
+            const int p = 2 * (wi >> 1) + ((l >> 2) & 1), c = 64 * (wi & 1) + 4 * ((l & 3) + 4 * (l >> 3));
+            const int y = y0 + 2 * p, x = x0 + c;
+            const float4* src = reinterpret_cast<const float4*>(t2 + p * LT2_W + c + 2 * d);
+            float2 yv[4 + 2 * r];
+#pragma unroll
+            for (int k = 0; k < 2 + r; ++k) {
+                const float4 v = src[k];
+                yv[2 * k] = make_float2(v.x, v.y);
+                yv[2 * k + 1] = make_float2(v.z, v.w);
+            }
+            float2 o[4];
+#pragma unroll
+            for (int cc = 0; cc < 4; ++cc) o[cc] = blur_pairs_w<r>(yv + cc, w);
+            const int at0 = y * a.C + x;
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                const int at = at0 + h * a.C;
+                const float4 lv = h ? make_float4(o[0].y, o[1].y, o[2].y, o[3].y)
+                                    : make_float4(o[0].x, o[1].x, o[2].x, o[3].x);
+                if (BASE) {
+                    *reinterpret_cast<float4*>(a.dst + at) = lv;
+                    continue;
+                }
+                const float* ctr = s_in + (2 * p + h + r) * LIN_W + 16 + c;   // L_{I-1} at (y + h, x)
+                const float4 pv = *reinterpret_cast<const float4*>(ctr);
+                *reinterpret_cast<float4*>(a.dog + at) = make_float4(lv.x - pv.x, lv.y - pv.y, lv.z - pv.z, lv.w - pv.w);
+                if (a.dst) *reinterpret_cast<float4*>(a.dst + at) = lv;
+                if (a.mag) {
+                    const float4 up = *reinterpret_cast<const float4*>(ctr - LIN_W);
+                    const float4 dn = *reinterpret_cast<const float4*>(ctr + LIN_W);
+                    const float lf = ctr[-1], rt = ctr[4];
+                    const float dx[4] = {__fsub_rn(pv.y, lf), __fsub_rn(pv.z, pv.x), __fsub_rn(pv.w, pv.y),
+                                         __fsub_rn(rt, pv.z)};
+                    const float dy[4] = {__fsub_rn(up.x, dn.x), __fsub_rn(up.y, dn.y), __fsub_rn(up.z, dn.z),
+                                         __fsub_rn(up.w, dn.w)};
+                    float mg[4], an[4];
+                    fast_grad4(dx, dy, mg, an);
+                    *reinterpret_cast<float4*>(a.mag + at) = make_float4(mg[0], mg[1], mg[2], mg[3]);
+                    *reinterpret_cast<float4*>(a.ang + at) = make_float4(an[0], an[1], an[2], an[3]);
+                }
+                if (a.down && h == 0) {   // y is even: y0 and 2p are
+                    float* o2 = a.down + (y >> 1) * a.down_cols + (x >> 1);
+                    o2[0] = pv.x;
+                    o2[1] = pv.z;
+                }
+            }
+        }
+        return;
+    }
     for (int it = tid; it < (LY / 2) * (LX / 4); it += LNT) {
         const int wi = it >> 5, l = it & 31;
         const int p = 2 * (wi >> 1) + ((l >> 2) & 1), c = 64 * (wi & 1) + 4 * ((l & 3) + 4 * (l >> 3));
@@ -646,12 +786,31 @@ __global__ void __launch_bounds__(LNT) k_layer(LayerArgs a) {
     }
 }
 
+// Tensor map of a layer's source plane for the tile copies (box LIN_W x rows): needs 16-byte
+// aligned rows and base and the box inside the plane's extent; 0 when not possible (the tiles then
+// load by cp.async)
+int layer_tensor_map(CUtensorMap* tm, const float* src, int R, int C, int rows) {
+    EncodeTiledFn enc = encode_tiled();
+    if (!enc || (C & 3) != 0 || C < LIN_W || R < rows || (reinterpret_cast<uintptr_t>(src) & 15) != 0) return 0;
+    const cuuint64_t dims[2] = {(cuuint64_t)C, (cuuint64_t)R};
+    const cuuint64_t strides[1] = {(cuuint64_t)C * 4};
+    const cuuint32_t box[2] = {(cuuint32_t)LIN_W, (cuuint32_t)rows};
+    const cuuint32_t es[2] = {1, 1};
+    return enc(tm, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, const_cast<float*>(src), dims, strides, box, es,
+               CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+               CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
 template <int TS, int r, bool BASE, int LY>
 int32_t launch_layer_ly(const LayerArgs& a, cudaStream_t s) {
     static std::atomic<int> attr[64];
     FSB_TRY(smem_attr((const void*)k_layer<TS, r, BASE, LY>, layer_smem<r, LY>(), attr));
+    static_assert(LY + 2 * r <= 256, "tensor copy box height");
+    CUtensorMap tm;
+    std::memset(&tm, 0, sizeof(tm));
+    const int use_tma = !BASE && a.err ? layer_tensor_map(&tm, a.src, a.R, a.C, LY + 2 * r) : 0;
     dim3 grid((a.C + LX - 1) / LX, (a.R + LY - 1) / LY);
-    k_layer<TS, r, BASE, LY><<<grid, LNT, layer_smem<r, LY>(), s>>>(a);
+    k_layer<TS, r, BASE, LY><<<grid, LNT, layer_smem<r, LY>(), s>>>(tm, a, use_tma);
     note_launch();
     FSB_CUDA(cudaGetLastError());
     return FSB_OK;
@@ -1013,7 +1172,6 @@ static_assert(TSD(1) >= 0 && TSD(2) >= 0 && TSD(3) >= 0 && TSD(4) >= 0 && TSD(5)
 static_assert(TVW(1) + TSD(1) % 2 <= TVP && TVW(5) + TSD(5) % 2 <= TVP, "vertical buffer width");
 static_assert((toff(1) * 4) % 128 == 0 && (TPITCH(0) * 4) % 128 == 0, "TMA destinations 128-byte aligned");
 static_assert(TSMEM <= 113 * 1024, "two CTAs per SM");
-constexpr long long TSTRIP_TIMEOUT = 2000000000ll;   // cycles (about a second) for one TMA row block
 
 struct StripArgs {
     const float* L0;   // octave base, R x C, row pitch C
@@ -1025,31 +1183,6 @@ struct StripArgs {
     int down_cols;
     int* err;          // set to 1 when a TMA wait gives up
 };
-
-__device__ __forceinline__ uint32_t s_addr(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
-
-__device__ __forceinline__ bool s_mbar_test(uint64_t* b, uint32_t parity) {
-    uint32_t ok;
-    asm volatile(
-        "{\n\t.reg .pred p;\n\t"
-        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
-        "selp.u32 %0, 1, 0, p;\n\t}"
-        : "=r"(ok)
-        : "r"(s_addr(b)), "r"(parity)
-        : "memory");
-    return ok != 0;
-}
-
-// Waits (bounded) for one row block; every thread waits, then the CTA agrees on the outcome.
-__device__ __forceinline__ bool s_mbar_wait(uint64_t* b, uint32_t parity) {
-    bool ok = s_mbar_test(b, parity);
-    if (!ok) {
-        const long long t0 = clock64();
-        while (!(ok = s_mbar_test(b, parity)) && clock64() - t0 < TSTRIP_TIMEOUT) {
-        }
-    }
-    return ok;
-}
 
 // rows y .. y + 7 of L0 into ring 0: TMA (one thread issues eight row copies on `bar`) or, when
 // tma is false, cp.async with reflected rows and columns
@@ -1324,7 +1457,10 @@ __global__ void __launch_bounds__(TNT, 2) k_strip(const __grid_constant__ CUtens
                 if (ok) s_fix_edges(a, ring[0], k.x0, V0 + TSTEP * b, k.RB);
             }
             if (__syncthreads_or(!ok)) {
+                // flag it and give the copies still in flight (blocks t, t + 1) one more bounded wait
+                // each before leaving
                 if (threadIdx.x == 0) atomicExch(a.err, 1);
+                for (int b = t; b <= t + 1; ++b) s_mbar_wait(bar + (b & 1), (b >> 1) & 1);
                 return;
             }
         } else {
@@ -1345,22 +1481,6 @@ __global__ void __launch_bounds__(TNT, 2) k_strip(const __grid_constant__ CUtens
     }
     // every issued TMA block (0 .. T) was waited for inside the loop
     if (!tma) cp_wait_all();
-}
-
-// cuTensorMapEncodeTiled through the runtime's driver entry point (no link against libcuda)
-typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
-                                  const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
-                                  CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
-EncodeTiledFn encode_tiled() {
-    static EncodeTiledFn fn = [] {
-        void* f = nullptr;
-        cudaDriverEntryPointQueryResult q{};
-        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &f, cudaEnableDefault, &q) != cudaSuccess ||
-            q != cudaDriverEntryPointSuccess)
-            f = nullptr;
-        return reinterpret_cast<EncodeTiledFn>(f);
-    }();
-    return fn;
 }
 
 }  // namespace
@@ -1453,8 +1573,9 @@ int layer_tile_height(int variant) { return kTileHeights[variant < 0 || variant 
 // One layer of the float32 pyramid by the tiled per-layer kernel: L_layer from src (R x C), tile
 // height layer_tile_height(variant).
 int32_t launch_layer_fast(int layer, const float* src, int R, int C, float* dst, float* dog, float* mag, float* ang,
-                          float* down, int down_cols, int variant, cudaStream_t s) {
+                          float* down, int down_cols, int variant, int* err, cudaStream_t s) {
     LayerArgs a{};
+    a.err = err;
     a.src = src;
     a.R = R;
     a.C = C;

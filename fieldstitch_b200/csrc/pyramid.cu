@@ -218,11 +218,13 @@ struct LayerCall {
     int R, C;
     float *dst, *dog, *mag, *ang, *down;
     int dc;
+    int* err;   // error word of the tile copies' bounded waits
     cudaStream_t s;
 };
 int32_t run_layer_call(void* p, int v) {
     const LayerCall* c = static_cast<const LayerCall*>(p);
-    return launch_layer_fast(c->layer, c->src, c->R, c->C, c->dst, c->dog, c->mag, c->ang, c->down, c->dc, v, c->s);
+    return launch_layer_fast(c->layer, c->src, c->R, c->C, c->dst, c->dog, c->mag, c->ang, c->down, c->dc, v, c->err,
+                             c->s);
 }
 struct BaseCall {
     const uint8_t* img;
@@ -236,8 +238,8 @@ int32_t run_base_call(void* p, int v) {
 }
 // one tuned per-layer launch: the tile height is chosen per (layer, octave size)
 int32_t tuned_layer(int layer, const float* src, int R, int C, float* dst, float* dog, float* mag, float* ang,
-                    float* down, int dc, cudaStream_t s) {
-    LayerCall c{layer, src, R, C, dst, dog, mag, ang, down, dc, s};
+                    float* down, int dc, int* err, cudaStream_t s) {
+    LayerCall c{layer, src, R, C, dst, dog, mag, ang, down, dc, err, s};
     char key[64];
     std::snprintf(key, sizeof(key), "k_layer%d_%dx%d", layer, R, C);
     int v = 0;
@@ -297,13 +299,14 @@ int32_t run_octave_call(void* p, int v) {
         FSB_TRY(fork());
         FSB_TRY(launch_group_upper(c->x, c->R, c->C, c->dog + 3 * RC, ts));
     } else {
-        FSB_TRY(tuned_layer(1, c->src, c->R, c->C, c->x, c->dog, nullptr, nullptr, nullptr, 0, c->s));
-        FSB_TRY(tuned_layer(2, c->x, c->R, c->C, c->y, c->dog + RC, c->mag, c->ang, nullptr, 0, c->s));
-        FSB_TRY(tuned_layer(3, c->y, c->R, c->C, c->x, c->dog + 2 * RC, c->mag + RC, c->ang + RC, nullptr, 0, c->s));
+        FSB_TRY(tuned_layer(1, c->src, c->R, c->C, c->x, c->dog, nullptr, nullptr, nullptr, 0, c->err, c->s));
+        FSB_TRY(tuned_layer(2, c->x, c->R, c->C, c->y, c->dog + RC, c->mag, c->ang, nullptr, 0, c->err, c->s));
+        FSB_TRY(tuned_layer(3, c->y, c->R, c->C, c->x, c->dog + 2 * RC, c->mag + RC, c->ang + RC, nullptr, 0, c->err,
+                            c->s));
         FSB_TRY(tuned_layer(4, c->x, c->R, c->C, c->y, c->dog + 3 * RC, c->mag + 2 * RC, c->ang + 2 * RC, c->down,
-                            c->dc, c->s));
+                            c->dc, c->err, c->s));
         FSB_TRY(fork());
-        FSB_TRY(tuned_layer(5, c->y, c->R, c->C, nullptr, c->dog + 4 * RC, nullptr, nullptr, nullptr, 0, ts));
+        FSB_TRY(tuned_layer(5, c->y, c->R, c->C, nullptr, c->dog + 4 * RC, nullptr, nullptr, nullptr, 0, c->err, ts));
     }
     if (c->side) FSB_CUDA(cudaEventRecord(c->join, c->side));
     return FSB_OK;
@@ -407,12 +410,12 @@ int32_t run_pyramid(Workspace& ws, const uint8_t* d_img, int img_stride, bool ex
             const int R = g.R[o], C = g.C[o];
             float* down = o + 1 < g.n_oct ? cur : nullptr;
             const int dc = o + 1 < g.n_oct ? g.C[o + 1] : 0;
-            FSB_TRY(tuned_layer(1, cur, R, C, other[0], dog, nullptr, nullptr, nullptr, 0, s));
-            FSB_TRY(tuned_layer(2, other[0], R, C, other[1], dog + RC, mag, ang, nullptr, 0, s));
-            FSB_TRY(tuned_layer(3, other[1], R, C, other[0], dog + 2 * RC, mag + RC, ang + RC, nullptr, 0, s));
+            FSB_TRY(tuned_layer(1, cur, R, C, other[0], dog, nullptr, nullptr, nullptr, 0, err, s));
+            FSB_TRY(tuned_layer(2, other[0], R, C, other[1], dog + RC, mag, ang, nullptr, 0, err, s));
+            FSB_TRY(tuned_layer(3, other[1], R, C, other[0], dog + 2 * RC, mag + RC, ang + RC, nullptr, 0, err, s));
             FSB_TRY(tuned_layer(4, other[0], R, C, other[1], dog + 3 * RC, mag + 2 * RC, ang + 2 * RC, down, dc,
-                                      s));
-            FSB_TRY(tuned_layer(5, other[1], R, C, nullptr, dog + 4 * RC, nullptr, nullptr, nullptr, 0, s));
+                                err, s));
+            FSB_TRY(tuned_layer(5, other[1], R, C, nullptr, dog + 4 * RC, nullptr, nullptr, nullptr, 0, err, s));
             continue;   // the next base is in `cur` (the dead L0 plane)
         }
         BlurArgs b{};

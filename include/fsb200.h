@@ -178,6 +178,16 @@ int32_t fsb_sift_features_batch_hd(fsb_ctx* ctx, int32_t n_img, const uint8_t* c
                                    const fsb_sift_params* p, const int32_t* nfeats, float* const* d_xy,
                                    float* const* d_resp, uint8_t* const* d_rootsift, int32_t* d_counts,
                                    int32_t* h_counts, int32_t chains);
+/* The Gaussian / DoG pyramid stage alone (gsift.py `_pyramid`, app/planesite/gsift.py:158-179, and
+   the gradient atlases of `_Atlas`, :227-267) for n_img device images of one size, on `chains`
+   streams (image i on chain i mod chains) captured as one CUDA graph and replayed while the image
+   pointers are unchanged; the same chains and workspaces as fsb_sift_features_batch_d. The
+   atlases stay in the chain workspaces (each chain holds the last image it processed), so this is
+   the stage that fsb_sift_features_batch_d runs first, exposed to time the pyramid in the batch
+   configuration. A geometry's first call runs one pyramid outside the capture (autotuning).
+   flags: FSB_SIFT_EXACT_BLUR or 0. Waits for the batch. */
+int32_t fsb_pyramid_batch_d(fsb_ctx* ctx, int32_t n_img, const uint8_t* const* d_imgs, int32_t h, int32_t w,
+                            int32_t stride, int32_t flags, int32_t chains);
 /* Prior prediction: projects n float32 points (d_xy, n*2) through the homography hm9 (host,
    row-major 3x3) into float64 positions d_out (n*2), adding the float32 offsets d_offset (n*2,
    nullable) - e.g. a GNSS/gimbal prior and its error. Identity hm9 converts to float64. */

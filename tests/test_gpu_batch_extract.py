@@ -173,3 +173,40 @@ def test_extract_and_match_from_page_locked_images():
             assert len(wq) > 0
             np.testing.assert_array_equal(gq, wq)
             np.testing.assert_array_equal(gt, wt)
+
+
+def test_pyramid_batch_runs_and_leaves_extraction_unchanged():
+    """fsb_pyramid_batch_d (the pyramid stage of a batch alone, one graph, several chains) runs on
+    its capture and replays, rejects bad arguments, and a batched extraction on the same context
+    afterwards still equals the per-image path."""
+    import ctypes
+
+    import torch
+
+    import fieldstitch_b200 as F
+    from fieldstitch_b200 import _lib, synth
+    h, w = 495, 660
+    dev = torch.device("cuda", 0)
+    imgs = [synth.synth_image(h, w, 700 + k) for k in range(5)]
+    d_imgs = [torch.from_numpy(im).to(dev) for im in imgs]
+    ctx = _lib.context(0)
+    Pv = ctypes.c_void_p * len(imgs)
+    arr = Pv(*[t.data_ptr() for t in d_imgs])
+    for _ in range(3):
+        _lib.check(ctx.lib.fsb_pyramid_batch_d(ctx.handle, len(imgs), arr, h, w, w, 0, 3), "pyramid batch")
+    assert ctx.lib.fsb_pyramid_batch_d(ctx.handle, len(imgs), arr, h, w, w, 0, 0) == 1
+    assert b"chains" in ctx.lib.fsb_last_error()
+    assert ctx.lib.fsb_pyramid_batch_d(ctx.handle, 1, Pv(None), h, w, w, 0, 2) == 1
+    assert ctx.lib.fsb_pyramid_batch_d(ctx.handle, 0, None, 0, 0, 0, 0, 2) == 0
+    nfeats = [1500, 400, 3000, 800, 50]
+    nmax = max(nfeats)
+    xy = [torch.zeros((nmax, 2), dtype=torch.float32, device=dev) for _ in imgs]
+    u8 = [torch.zeros((nmax, 128), dtype=torch.uint8, device=dev) for _ in imgs]
+    rs = [torch.zeros(nmax, dtype=torch.float32, device=dev) for _ in imgs]
+    counts = F.features.sift_gpu_batch_d(d_imgs, nfeats, xy, u8, rs, chains=3)
+    for k, (im, nf) in enumerate(zip(imgs, nfeats)):
+        wxy, wu8, wrs = _per_image(F, im, nf)
+        n = len(wxy)
+        assert counts[k] == n
+        np.testing.assert_array_equal(xy[k][:n].cpu().numpy(), wxy)
+        np.testing.assert_array_equal(u8[k][:n].cpu().numpy(), wu8)
