@@ -289,6 +289,7 @@ static std::atomic<long long> g_launches{0};
 }  // namespace fsb
 
 void fsb::note_launch(int n) { fsb::g_launches.fetch_add(n, std::memory_order_relaxed); }
+long long fsb::launch_mark() { return fsb::g_launches.load(std::memory_order_relaxed); }
 
 namespace {
 cudaEvent_t take_event(std::vector<cudaEvent_t>& free_list) {
@@ -955,8 +956,11 @@ int32_t sift_features_batch(fsb_ctx* ctx, int32_t n_img, const uint8_t* const* h
         x.graph.exec = nullptr;
         x.graph.graph = nullptr;
         BatchCall bc{n_img, d_imgs, h_imgs, h, w, stride, p, nfeats, d_xy, d_resp, d_rootsift, d_counts};
+        const long long m0 = launch_mark();
         FSB_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
         const int32_t st = batch_body(ctx, bc);
+        x.graph.n_kernels = (int)(launch_mark() - m0);
+        note_launch(-x.graph.n_kernels);   // the kernels run (and count) at each replay
         cudaGraph_t g = nullptr;
         const cudaError_t e = cudaStreamEndCapture(s, &g);
         if (st != FSB_OK) {
@@ -978,6 +982,7 @@ int32_t sift_features_batch(fsb_ctx* ctx, int32_t n_img, const uint8_t* const* h
                                                         h_imgs[i], (size_t)h * stride, cudaMemcpyHostToDevice));
     }
     FSB_CUDA(cudaGraphLaunch(x.graph.exec, s));
+    note_launch(x.graph.n_kernels);
     // one wait per batch: the flags say which images (if any) exceeded a capacity
     FSB_TRY(stage_ensure(ctx, (size_t)n_img * 8 + 64));
     uint32_t* h_status = static_cast<uint32_t*>(ctx->pinned);
@@ -1093,6 +1098,7 @@ int32_t fsb_pyramid_batch_d(fsb_ctx* ctx, int32_t n_img, const uint8_t* const* d
         if (x.pyr_graph.graph) cudaGraphDestroy(x.pyr_graph.graph);
         x.pyr_graph.exec = nullptr;
         x.pyr_graph.graph = nullptr;
+        const long long m0 = launch_mark();
         FSB_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
         int32_t st = FSB_OK;
         [&]() {
@@ -1118,6 +1124,8 @@ int32_t fsb_pyramid_batch_d(fsb_ctx* ctx, int32_t n_img, const uint8_t* const* d
         }();
         cudaGraph_t g = nullptr;
         const cudaError_t e = cudaStreamEndCapture(s, &g);
+        x.pyr_graph.n_kernels = (int)(launch_mark() - m0);
+        note_launch(-x.pyr_graph.n_kernels);
         if (st != FSB_OK || e != cudaSuccess) {
             if (g) cudaGraphDestroy(g);
             if (st == FSB_OK) {
@@ -1131,6 +1139,7 @@ int32_t fsb_pyramid_batch_d(fsb_ctx* ctx, int32_t n_img, const uint8_t* const* d
         x.pyr_graph.key = key;
     }
     FSB_CUDA(cudaGraphLaunch(x.pyr_graph.exec, s));
+    note_launch(x.pyr_graph.n_kernels);
     // the error words of the chains' bounded waits (strip engine)
     const int used = chains < n_img ? chains : n_img;
     FSB_TRY(stage_ensure(ctx, (size_t)used * 4 + 64));

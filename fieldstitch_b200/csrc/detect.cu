@@ -62,6 +62,19 @@ struct ExTiles {
 
 constexpr int EX_DEPTH = 9;          // rows in flight per lane (the shared-memory ring's slots)
 
+// three-input maximum / minimum (one instruction on sm_100); exact, so the same values as two
+// two-input ones
+__device__ __forceinline__ float max3f(float a, float b, float c) {
+    float d;
+    asm("max.f32 %0, %1, %2, %3;" : "=f"(d) : "f"(a), "f"(b), "f"(c));
+    return d;
+}
+__device__ __forceinline__ float min3f(float a, float b, float c) {
+    float d;
+    asm("min.f32 %0, %1, %2, %3;" : "=f"(d) : "f"(a), "f"(b), "f"(c));
+    return d;
+}
+
 __device__ __forceinline__ void ex_cp_async4(float* dst, const float* src) {
     const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
     asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(d), "l"(src) : "memory");
@@ -126,8 +139,8 @@ __global__ void __launch_bounds__(EX_T, 4) k_extrema(const float* __restrict__ D
         for (int l = 0; l < 5; ++l) {
             const float v = raw[l];
             const float vl = __shfl_up_sync(0xffffffffu, v, 1), vr = __shfl_down_sync(0xffffffffu, v, 1);
-            w.hx[l] = fmaxf(fmaxf(vl, v), vr);
-            w.hn[l] = fminf(fminf(vl, v), vr);
+            w.hx[l] = max3f(vl, v, vr);
+            w.hn[l] = min3f(vl, v, vr);
             if (l >= 1 && l <= N_LAYERS) w.c[l - 1] = v;
         }
     };
@@ -142,16 +155,16 @@ __global__ void __launch_bounds__(EX_T, 4) k_extrema(const float* __restrict__ D
         float vmx[5], vmn[5];
 #pragma unroll
         for (int l = 0; l < 5; ++l) {
-            vmx[l] = fmaxf(fmaxf(up.hx[l], mid.hx[l]), dn.hx[l]);
-            vmn[l] = fminf(fminf(up.hn[l], mid.hn[l]), dn.hn[l]);
+            vmx[l] = max3f(up.hx[l], mid.hx[l], dn.hx[l]);
+            vmn[l] = min3f(up.hn[l], mid.hn[l], dn.hn[l]);
         }
         unsigned mask = 0;
         if (col_ok) {
 #pragma unroll
             for (int l = 1; l <= N_LAYERS; ++l) {
                 const float v = mid.c[l - 1];
-                const float mx = fmaxf(fmaxf(vmx[l - 1], vmx[l]), vmx[l + 1]);
-                const float mn = fminf(fminf(vmn[l - 1], vmn[l]), vmn[l + 1]);
+                const float mx = max3f(vmx[l - 1], vmx[l], vmx[l + 1]);
+                const float mn = min3f(vmn[l - 1], vmn[l], vmn[l + 1]);
                 if ((v >= mx && v > k.pthr) || (v <= mn && v < -k.pthr)) mask |= 1u << (l - 1);
             }
         }
@@ -207,6 +220,19 @@ ExTiles make_tiles(const Geometry& g, int* total) {
     t.first[g.n_oct] = acc;
     *total = acc;
     return t;
+}
+
+// The extremum candidates of every octave in one launch, appended to `cand` through `cnt[0]`.
+int32_t launch_extrema(const Geometry& g, const float* DF, const DetectConsts& k, uint32_t* cand, uint32_t* cnt,
+                       uint32_t cap, cudaStream_t s) {
+    int n = 0;
+    const ExTiles t = make_tiles(g, &n);
+    if (n > 0) {
+        k_extrema<<<n, EX_T, 0, s>>>(DF, k, t, cand, cnt, cap);
+        note_launch();
+    }
+    FSB_CUDA(cudaGetLastError());
+    return FSB_OK;
 }
 
 struct Fit {
@@ -610,13 +636,7 @@ int32_t run_detect(fsb_ctx* ctx, Workspace& ws, double contrast, double edge, in
     ctx->stage_begin(ST_EXTREMA);
     for (int attempt = 0; attempt < 3; ++attempt) {
         FSB_CUDA(cudaMemsetAsync(cnt, 0, 3 * sizeof(uint32_t), s));
-        int nblk = 0;
-        const ExTiles tl = make_tiles(g, &nblk);
-        if (nblk > 0) {
-            k_extrema<<<nblk, EX_T, 0, s>>>(DF, k, tl, ws.cand.as<uint32_t>(), cnt, (uint32_t)ws.cap_cand);
-            note_launch();
-        }
-        FSB_CUDA(cudaGetLastError());
+        FSB_TRY(launch_extrema(g, DF, k, ws.cand.as<uint32_t>(), cnt, (uint32_t)ws.cap_cand, s));
         uint32_t h_head[PYR_ERR_WORD + 1];
         FSB_CUDA(cudaMemcpyAsync(h_head, cnt, sizeof(h_head), cudaMemcpyDeviceToHost, s));
         FSB_CUDA(cudaStreamSynchronize(s));
@@ -860,9 +880,7 @@ int32_t run_detect_async(Workspace& ws, double contrast, double edge, const Asyn
     uint32_t* cnt = ws.counters.as<uint32_t>();
     const float* DF = ws.dog.as<float>();
     FSB_CUDA(cudaMemsetAsync(cnt, 0, 8 * sizeof(uint32_t), s));
-    int nblk = 0;
-    const ExTiles tl = make_tiles(g, &nblk);
-    if (nblk > 0) k_extrema<<<nblk, EX_T, 0, s>>>(DF, k, tl, ws.cand.as<uint32_t>(), cnt, c.cand);
+    FSB_TRY(launch_extrema(g, DF, k, ws.cand.as<uint32_t>(), cnt, c.cand, s));
     const unsigned gr = std::min(blocks(c.cand, 128), 148u * 16u);
     k_refine<<<gr, 128, 0, s>>>(DF, k, ws.cand.as<uint32_t>(), cnt, c.cand, ws.refined.as<Refined>(), cnt + 1, c.ref);
     uint32_t* ka = ws.keys_a.as<uint32_t>();
@@ -890,7 +908,7 @@ int32_t run_detect_async(Workspace& ws, double contrast, double edge, const Asyn
                                                         ws.kx.as<float>(), ws.ky.as<float>(), ws.ksize.as<float>(),
                                                         ws.kangle.as<float>(), ws.kresp.as<float>(),
                                                         ws.koct.as<int32_t>(), ws.klayer.as<int32_t>());
-    note_launch(6 + 2 * ASYNC_ORIENT_PASSES);
+    note_launch(5 + ASYNC_ORIENT_PASSES);   // k_extrema* and k_orient count themselves
     FSB_CUDA(cudaGetLastError());
     return FSB_OK;
 }

@@ -19,6 +19,7 @@ void set_error(const char* fmt, ...);
 
 // Count of kernel launches issued by this library (observability; read by fsb_launch_count).
 void note_launch(int n = 1);
+long long launch_mark();   // the running count of note_launch
 
 // Per-stage device timers (CUDA events on the context stream), enabled by fsb_timing().
 enum Stage { ST_UPLOAD = 0, ST_PYRAMID, ST_EXTREMA, ST_REFINE, ST_ORIENT, ST_SORT, ST_SPREAD, ST_DESCRIBE,
@@ -131,6 +132,7 @@ struct GuidedGraph {
     std::vector<char> key;
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
+    int n_kernels = 0;   // this library's kernels in the graph (counted per replay, not at capture)
 };
 
 // Pyramid + detection workspace sized for one image geometry.
