@@ -1032,6 +1032,8 @@ def run_fsb(args):
     # and one image at a time on one stream (the latency of one image's launch chain; octaves 3-8
     # are launch-latency bound there)
     iso = workers[0]
+    iso.run(items=[0])   # the context's first pair sizes its buffers; not timed
+    torch.cuda.synchronize()
     iso.ctx.timing(True)
     iso.ctx.stage_times()
     iso.run(items=list(range(min(4, len(pairs)))))
