@@ -463,148 +463,13 @@ constexpr int layer_smem() {
     return layer_bar_off<r, LY>() + 16;
 }
 
-template <int TS, int r, bool BASE, int LY>
-__global__ void __launch_bounds__(LNT) k_layer(const __grid_constant__ CUtensorMap tm, LayerArgs a, int use_tma) {
-    constexpr int d = r & 1;
+// The input tile (rows y0 - r .., columns x0 - 16 .., reflect-101 outside the plane) by
+// per-thread cp.async (the caller commits and waits)
+template <int r, int LY>
+__device__ __forceinline__ void layer_load_cp(const LayerArgs& a, float* __restrict__ s_in, int x0, int y0) {
     constexpr int IH = LY + 2 * r;
-    constexpr int NPAIR = (LX + 2 * r + 2 * d) / 2;
-    static_assert(layer_bar_off<r, LY>() % 16 == 0, "mbarrier alignment");
-    extern __shared__ __align__(128) float sm[];
-    float* s_in = sm;
-    float2* t2 = reinterpret_cast<float2*>(sm + IH * LIN_W);
     const int tid = threadIdx.x;
-    const int x0 = blockIdx.x * LX, y0 = blockIdx.y * LY;
-    // input rows y0 - r .. y0 + LY + r - 1, columns x0 - 16 .. x0 + LX + 15 (reflect-101 outside)
-    if (BASE) {
-        // Source row / column pairs (iy, ny), (ix, nx) of every tile row / column (reflect-101 on
-        // the upsampled grid). The source block they reach is staged once as scaled floats p, the
-        // row-interpolated values vc = 0.75 p[iy] + 0.25 p[ny] are formed for every tile row over the
-        // block's columns, and each upsampled sample is 0.75 vc[ix] + 0.25 vc[nx], four columns per
-        // thread (gsift.py:90-102 rounding). Tables and vc live in the row-pair area and p in the
-        // input tile until the vertical pass needs them. A block larger than the staging window
-        // (mirror images of a tiny image) takes the per-sample global path.
-        constexpr int VCW = 96, SRW = IH / 2 + 4;
-        static_assert(!BASE || (2 * IH + 2 * LIN_C) * 4 + IH * VCW * 4 + 16 <= (LY / 2) * LT2_W * 8,
-                      "base tables must fit the row-pair area");
-        static_assert(!BASE || (SRW * VCW <= IH * LIN_W && IH % 2 == 0), "staged source block");
-        int* ry = reinterpret_cast<int*>(t2);   // iy of tile row i, then ny
-        int* rn = ry + IH;
-        int* cxs = rn + IH;                      // ix of tile column c, then nx (16-byte aligned)
-        int* cns = cxs + LIN_C;
-        float* vcs = reinterpret_cast<float*>(cns + LIN_C);
-        int* box = reinterpret_cast<int*>(vcs + IH * VCW);   // source row min / max, column min / max
-        float* ps = s_in;
-        if (tid < 4) box[tid] = (tid & 1) ? -1 : 0x7fffffff;
-        __syncthreads();
-        for (int i0 = 0; i0 < IH + LIN_C; i0 += LNT) {
-            const int i = i0 + tid;
-            int lo = 0x7fffffff, hi = -1, clo = 0x7fffffff, chi = -1;
-            if (i < IH) {
-                const int Y = mir(y0 - r + i, a.R), iy = Y >> 1;
-                const int ny = (Y & 1) ? min(iy + 1, a.ih - 1) : max(iy - 1, 0);
-                ry[i] = iy;
-                rn[i] = ny;
-                lo = min(iy, ny);
-                hi = max(iy, ny);
-            } else if (i < IH + LIN_C) {
-                const int c = i - IH, X = mir(x0 - 16 + c, a.C), ix = X >> 1;
-                const int nx = (X & 1) ? min(ix + 1, a.iw - 1) : max(ix - 1, 0);
-                cxs[c] = ix;
-                cns[c] = nx;
-                clo = min(ix, nx);
-                chi = max(ix, nx);
-            }
-            lo = __reduce_min_sync(0xffffffffu, lo);
-            hi = __reduce_max_sync(0xffffffffu, hi);
-            clo = __reduce_min_sync(0xffffffffu, clo);
-            chi = __reduce_max_sync(0xffffffffu, chi);
-            if ((tid & 31) == 0) {
-                if (hi >= 0) {
-                    atomicMin(&box[0], lo);
-                    atomicMax(&box[1], hi);
-                }
-                if (chi >= 0) {
-                    atomicMin(&box[2], clo);
-                    atomicMax(&box[3], chi);
-                }
-            }
-        }
-        __syncthreads();
-        const int sy0 = box[0], nsr = box[1] - box[0] + 1, sx0 = box[2], nsx = box[3] - box[2] + 1;
-        const float sc = (float)(1.0 / 255.0);
-        if (nsr <= SRW && nsx <= VCW) {
-            for (int row = tid >> 5; row < nsr; row += LNT / 32) {
-                const uint8_t* src = a.img + (size_t)(sy0 + row) * a.img_stride + sx0;
-                for (int k = tid & 31; k < nsx; k += 32) ps[row * VCW + k] = __fmul_rn((float)__ldg(src + k), sc);
-            }
-            __syncthreads();
-            for (int i = tid; i < IH * (VCW / 4); i += LNT) {
-                const int row = i / (VCW / 4), q = 4 * (i - row * (VCW / 4));
-                if (q >= nsx) continue;
-                const float4 p0 = *reinterpret_cast<const float4*>(ps + (ry[row] - sy0) * VCW + q);
-                const float4 p1 = *reinterpret_cast<const float4*>(ps + (rn[row] - sy0) * VCW + q);
-                float4 v;
-                v.x = __fadd_rn(__fmul_rn(0.75f, p0.x), __fmul_rn(0.25f, p1.x));
-                v.y = __fadd_rn(__fmul_rn(0.75f, p0.y), __fmul_rn(0.25f, p1.y));
-                v.z = __fadd_rn(__fmul_rn(0.75f, p0.z), __fmul_rn(0.25f, p1.z));
-                v.w = __fadd_rn(__fmul_rn(0.75f, p0.w), __fmul_rn(0.25f, p1.w));
-                *reinterpret_cast<float4*>(vcs + row * VCW + q) = v;
-            }
-            __syncthreads();
-            for (int i = tid; i < IH * (LIN_C / 4); i += LNT) {
-                const int row = i / (LIN_C / 4), q = 4 * (i - row * (LIN_C / 4));
-                const int4 ix = *reinterpret_cast<const int4*>(cxs + q);
-                const int4 nx = *reinterpret_cast<const int4*>(cns + q);
-                const float* v = vcs + row * VCW - sx0;
-                float4 u;
-                u.x = __fadd_rn(__fmul_rn(0.75f, v[ix.x]), __fmul_rn(0.25f, v[nx.x]));
-                u.y = __fadd_rn(__fmul_rn(0.75f, v[ix.y]), __fmul_rn(0.25f, v[nx.y]));
-                u.z = __fadd_rn(__fmul_rn(0.75f, v[ix.z]), __fmul_rn(0.25f, v[nx.z]));
-                u.w = __fadd_rn(__fmul_rn(0.75f, v[ix.w]), __fmul_rn(0.25f, v[nx.w]));
-                *reinterpret_cast<float4*>(s_in + row * LIN_W + q) = u;
-            }
-        } else {
-            for (int i = tid; i < IH * LIN_C; i += LNT) {
-                const int row = i / LIN_C, col = i - row * LIN_C;
-                const uint8_t* r0 = a.img + (size_t)ry[row] * a.img_stride;
-                const uint8_t* r1 = a.img + (size_t)rn[row] * a.img_stride;
-                const int ix = cxs[col], nx = cns[col];
-                const float vc = __fadd_rn(__fmul_rn(0.75f, __fmul_rn((float)__ldg(r0 + ix), sc)),
-                                           __fmul_rn(0.25f, __fmul_rn((float)__ldg(r1 + ix), sc)));
-                const float vn = __fadd_rn(__fmul_rn(0.75f, __fmul_rn((float)__ldg(r0 + nx), sc)),
-                                           __fmul_rn(0.25f, __fmul_rn((float)__ldg(r1 + nx), sc)));
-                s_in[row * LIN_W + col] = __fadd_rn(__fmul_rn(0.75f, vc), __fmul_rn(0.25f, vn));
-            }
-        }
-    } else if (use_tma && (s_addr(s_in) & 127) == 0 && y0 >= r && y0 + LY + r <= a.R && x0 >= 16 &&
-               x0 + LX + 16 <= a.C) {
-        // an interior tile (no reflected row or column): one 2-D tensor copy of LIN_W x IH floats
-        // (columns x0 - 16 .., rows y0 - r ..; the copy's last 8 columns are not read and may lie
-        // outside the plane, where the copy fills zeros), completion on an mbarrier
-        uint64_t* bar = reinterpret_cast<uint64_t*>(reinterpret_cast<char*>(sm) + layer_bar_off<r, LY>());
-        if (tid == 0) {
-            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(s_addr(bar)) : "memory");
-            asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-        }
-        __syncthreads();
-        if (tid == 0) {
-            asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(s_addr(bar)),
-                         "r"(IH * LIN_W * 4)
-                         : "memory");
-            asm volatile(
-                "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], "
-                "[%4];" ::"r"(s_addr(s_in)),
-                "l"(reinterpret_cast<uint64_t>(&tm)), "r"(x0 - 16), "r"(y0 - r), "r"(s_addr(bar))
-                : "memory");
-        }
-        if (__syncthreads_or(!s_mbar_wait(bar, 0))) {
-            // the copy did not land in time: flag it, give it one more bounded wait (so that no copy
-            // into this CTA's shared memory is left in flight when possible) and leave the tile
-            if (tid == 0) atomicExch(a.err, 1);
-            s_mbar_wait(bar, 0);
-            return;
-        }
-    } else if ((a.C & 3) == 0 && al16(a.src) && x0 >= 16 && x0 + LX + 16 <= a.C) {
+    if ((a.C & 3) == 0 && al16(a.src) && x0 >= 16 && x0 + LX + 16 <= a.C) {
         // eight lanes per row (the mirrored row address once per row), five 16-byte copies a lane
         static_assert(LIN_C / 4 == 40, "five copies of eight lanes per row");
         for (int row = tid >> 3; row < IH; row += LNT / 8) {
@@ -623,9 +488,36 @@ __global__ void __launch_bounds__(LNT) k_layer(const __grid_constant__ CUtensorM
             cp_async4(s_in + row * LIN_W + col, g);
         }
     }
-    cp_commit();
-    cp_wait_all();
-    __syncthreads();
+}
+
+// Whether a tile's input lies inside the plane (no reflected row or column): such tiles arrive by
+// one 2-D tensor copy of LIN_W x (LY + 2r) floats (the copy's last 8 columns are not read and may
+// lie outside the plane, where the copy fills zeros)
+template <int r, int LY>
+__device__ __forceinline__ bool layer_tile_inside(const LayerArgs& a, int x0, int y0) {
+    return y0 >= r && y0 + LY + r <= a.R && x0 >= 16 && x0 + LX + 16 <= a.C;
+}
+// thread 0: the tile's tensor copy into s_in, completion (bytes) on bar
+template <int r, int LY>
+__device__ __forceinline__ void layer_tma_issue(const CUtensorMap* tm, float* s_in, uint64_t* bar, int x0, int y0) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(s_addr(bar)),
+                 "r"((LY + 2 * r) * LIN_W * 4)
+                 : "memory");
+    asm volatile(
+        "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], "
+        "[%4];" ::"r"(s_addr(s_in)),
+        "l"(reinterpret_cast<uint64_t>(tm)), "r"(x0 - 16), "r"(y0 - r), "r"(s_addr(bar))
+        : "memory");
+}
+
+// The passes of one tile once its input (s_in) is in shared memory: vertical pass into the
+// row-pair tile t2, then the horizontal pass and the epilogue (L_I, DoG, gradient, downsample).
+template <int TS, int r, bool BASE, int LY>
+__device__ __forceinline__ void layer_compute(const LayerArgs& a, const float* __restrict__ s_in,
+                                              float2* __restrict__ t2, int x0, int y0) {
+    constexpr int d = r & 1;
+    constexpr int NPAIR = (LX + 2 * r + 2 * d) / 2;
+    const int tid = threadIdx.x;
     // vertical pass: column pair cp (V columns 2cp, 2cp+1 = image columns x0 - r - d + 2cp ..),
     // output rows 8g .. 8g + 7; stored row-pair interleaved at t2 index (V column + d)
     float2 w[r + 1];
@@ -784,6 +676,146 @@ __global__ void __launch_bounds__(LNT) k_layer(const __grid_constant__ CUtensorM
             }
         }
     }
+}
+
+
+template <int TS, int r, bool BASE, int LY>
+__global__ void __launch_bounds__(LNT, r <= 10 ? 4 : 3) k_layer(const __grid_constant__ CUtensorMap tm, LayerArgs a,
+                                                                int use_tma) {
+    constexpr int d = r & 1;
+    constexpr int IH = LY + 2 * r;
+    constexpr int NPAIR = (LX + 2 * r + 2 * d) / 2;
+    static_assert(layer_bar_off<r, LY>() % 16 == 0, "mbarrier alignment");
+    extern __shared__ __align__(128) float sm[];
+    float* s_in = sm;
+    float2* t2 = reinterpret_cast<float2*>(sm + IH * LIN_W);
+    const int tid = threadIdx.x;
+    const int x0 = blockIdx.x * LX, y0 = blockIdx.y * LY;
+    // input rows y0 - r .. y0 + LY + r - 1, columns x0 - 16 .. x0 + LX + 15 (reflect-101 outside)
+    if (BASE) {
+        // Source row / column pairs (iy, ny), (ix, nx) of every tile row / column (reflect-101 on
+        // the upsampled grid). The source block they reach is staged once as scaled floats p, the
+        // row-interpolated values vc = 0.75 p[iy] + 0.25 p[ny] are formed for every tile row over the
+        // block's columns, and each upsampled sample is 0.75 vc[ix] + 0.25 vc[nx], four columns per
+        // thread (gsift.py:90-102 rounding). Tables and vc live in the row-pair area and p in the
+        // input tile until the vertical pass needs them. A block larger than the staging window
+        // (mirror images of a tiny image) takes the per-sample global path.
+        constexpr int VCW = 96, SRW = IH / 2 + 4;
+        static_assert(!BASE || (2 * IH + 2 * LIN_C) * 4 + IH * VCW * 4 + 16 <= (LY / 2) * LT2_W * 8,
+                      "base tables must fit the row-pair area");
+        static_assert(!BASE || (SRW * VCW <= IH * LIN_W && IH % 2 == 0), "staged source block");
+        int* ry = reinterpret_cast<int*>(t2);   // iy of tile row i, then ny
+        int* rn = ry + IH;
+        int* cxs = rn + IH;                      // ix of tile column c, then nx (16-byte aligned)
+        int* cns = cxs + LIN_C;
+        float* vcs = reinterpret_cast<float*>(cns + LIN_C);
+        int* box = reinterpret_cast<int*>(vcs + IH * VCW);   // source row min / max, column min / max
+        float* ps = s_in;
+        if (tid < 4) box[tid] = (tid & 1) ? -1 : 0x7fffffff;
+        __syncthreads();
+        for (int i0 = 0; i0 < IH + LIN_C; i0 += LNT) {
+            const int i = i0 + tid;
+            int lo = 0x7fffffff, hi = -1, clo = 0x7fffffff, chi = -1;
+            if (i < IH) {
+                const int Y = mir(y0 - r + i, a.R), iy = Y >> 1;
+                const int ny = (Y & 1) ? min(iy + 1, a.ih - 1) : max(iy - 1, 0);
+                ry[i] = iy;
+                rn[i] = ny;
+                lo = min(iy, ny);
+                hi = max(iy, ny);
+            } else if (i < IH + LIN_C) {
+                const int c = i - IH, X = mir(x0 - 16 + c, a.C), ix = X >> 1;
+                const int nx = (X & 1) ? min(ix + 1, a.iw - 1) : max(ix - 1, 0);
+                cxs[c] = ix;
+                cns[c] = nx;
+                clo = min(ix, nx);
+                chi = max(ix, nx);
+            }
+            lo = __reduce_min_sync(0xffffffffu, lo);
+            hi = __reduce_max_sync(0xffffffffu, hi);
+            clo = __reduce_min_sync(0xffffffffu, clo);
+            chi = __reduce_max_sync(0xffffffffu, chi);
+            if ((tid & 31) == 0) {
+                if (hi >= 0) {
+                    atomicMin(&box[0], lo);
+                    atomicMax(&box[1], hi);
+                }
+                if (chi >= 0) {
+                    atomicMin(&box[2], clo);
+                    atomicMax(&box[3], chi);
+                }
+            }
+        }
+        __syncthreads();
+        const int sy0 = box[0], nsr = box[1] - box[0] + 1, sx0 = box[2], nsx = box[3] - box[2] + 1;
+        const float sc = (float)(1.0 / 255.0);
+        if (nsr <= SRW && nsx <= VCW) {
+            for (int row = tid >> 5; row < nsr; row += LNT / 32) {
+                const uint8_t* src = a.img + (size_t)(sy0 + row) * a.img_stride + sx0;
+                for (int k = tid & 31; k < nsx; k += 32) ps[row * VCW + k] = __fmul_rn((float)__ldg(src + k), sc);
+            }
+            __syncthreads();
+            for (int i = tid; i < IH * (VCW / 4); i += LNT) {
+                const int row = i / (VCW / 4), q = 4 * (i - row * (VCW / 4));
+                if (q >= nsx) continue;
+                const float4 p0 = *reinterpret_cast<const float4*>(ps + (ry[row] - sy0) * VCW + q);
+                const float4 p1 = *reinterpret_cast<const float4*>(ps + (rn[row] - sy0) * VCW + q);
+                float4 v;
+                v.x = __fadd_rn(__fmul_rn(0.75f, p0.x), __fmul_rn(0.25f, p1.x));
+                v.y = __fadd_rn(__fmul_rn(0.75f, p0.y), __fmul_rn(0.25f, p1.y));
+                v.z = __fadd_rn(__fmul_rn(0.75f, p0.z), __fmul_rn(0.25f, p1.z));
+                v.w = __fadd_rn(__fmul_rn(0.75f, p0.w), __fmul_rn(0.25f, p1.w));
+                *reinterpret_cast<float4*>(vcs + row * VCW + q) = v;
+            }
+            __syncthreads();
+            for (int i = tid; i < IH * (LIN_C / 4); i += LNT) {
+                const int row = i / (LIN_C / 4), q = 4 * (i - row * (LIN_C / 4));
+                const int4 ix = *reinterpret_cast<const int4*>(cxs + q);
+                const int4 nx = *reinterpret_cast<const int4*>(cns + q);
+                const float* v = vcs + row * VCW - sx0;
+                float4 u;
+                u.x = __fadd_rn(__fmul_rn(0.75f, v[ix.x]), __fmul_rn(0.25f, v[nx.x]));
+                u.y = __fadd_rn(__fmul_rn(0.75f, v[ix.y]), __fmul_rn(0.25f, v[nx.y]));
+                u.z = __fadd_rn(__fmul_rn(0.75f, v[ix.z]), __fmul_rn(0.25f, v[nx.z]));
+                u.w = __fadd_rn(__fmul_rn(0.75f, v[ix.w]), __fmul_rn(0.25f, v[nx.w]));
+                *reinterpret_cast<float4*>(s_in + row * LIN_W + q) = u;
+            }
+        } else {
+            for (int i = tid; i < IH * LIN_C; i += LNT) {
+                const int row = i / LIN_C, col = i - row * LIN_C;
+                const uint8_t* r0 = a.img + (size_t)ry[row] * a.img_stride;
+                const uint8_t* r1 = a.img + (size_t)rn[row] * a.img_stride;
+                const int ix = cxs[col], nx = cns[col];
+                const float vc = __fadd_rn(__fmul_rn(0.75f, __fmul_rn((float)__ldg(r0 + ix), sc)),
+                                           __fmul_rn(0.25f, __fmul_rn((float)__ldg(r1 + ix), sc)));
+                const float vn = __fadd_rn(__fmul_rn(0.75f, __fmul_rn((float)__ldg(r0 + nx), sc)),
+                                           __fmul_rn(0.25f, __fmul_rn((float)__ldg(r1 + nx), sc)));
+                s_in[row * LIN_W + col] = __fadd_rn(__fmul_rn(0.75f, vc), __fmul_rn(0.25f, vn));
+            }
+        }
+    } else if (use_tma && (s_addr(s_in) & 127) == 0 && layer_tile_inside<r, LY>(a, x0, y0)) {
+        // an interior tile: one tensor copy, completion on an mbarrier
+        uint64_t* bar = reinterpret_cast<uint64_t*>(reinterpret_cast<char*>(sm) + layer_bar_off<r, LY>());
+        if (tid == 0) {
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(s_addr(bar)) : "memory");
+            asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        }
+        __syncthreads();
+        if (tid == 0) layer_tma_issue<r, LY>(&tm, s_in, bar, x0, y0);
+        if (__syncthreads_or(!s_mbar_wait(bar, 0))) {
+            // the copy did not land in time: flag it, give it one more bounded wait (so that no copy
+            // into this CTA's shared memory is left in flight when possible) and leave the tile
+            if (tid == 0) atomicExch(a.err, 1);
+            s_mbar_wait(bar, 0);
+            return;
+        }
+    } else {
+        layer_load_cp<r, LY>(a, s_in, x0, y0);
+    }
+    cp_commit();
+    cp_wait_all();
+    __syncthreads();
+    layer_compute<TS, r, BASE, LY>(a, s_in, t2, x0, y0);
 }
 
 // Tensor map of a layer's source plane for the tile copies (box LIN_W x rows): needs 16-byte

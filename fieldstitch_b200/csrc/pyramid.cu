@@ -236,10 +236,16 @@ int32_t run_base_call(void* p, int v) {
     const BaseCall* c = static_cast<const BaseCall*>(p);
     return launch_base_fast(c->img, c->stride, c->h, c->w, c->dst, v == 1 ? 2 : 0, c->s);   // heights 32, 64
 }
-// one tuned per-layer launch: the tile height is chosen per (layer, octave size)
+// one tuned per-layer launch: the tile height is chosen per (layer, octave size);
+// FSB_LAYER_VARIANT=k (read on every call) runs variant k everywhere instead, so each variant can
+// be checked against the others
 int32_t tuned_layer(int layer, const float* src, int R, int C, float* dst, float* dog, float* mag, float* ang,
                     float* down, int dc, int* err, cudaStream_t s) {
     LayerCall c{layer, src, R, C, dst, dog, mag, ang, down, dc, err, s};
+    if (const char* fv = std::getenv("FSB_LAYER_VARIANT")) {
+        const int v = std::atoi(fv);
+        if (v >= 0 && v < layer_tile_variants()) return run_layer_call(&c, v);
+    }
     char key[64];
     std::snprintf(key, sizeof(key), "k_layer%d_%dx%d", layer, R, C);
     int v = 0;

@@ -148,3 +148,29 @@ def test_autotuned_octave_engines_are_bit_identical(monkeypatch):
     table = _lib.autotune_table()
     for r, c in ref[0]:
         assert any(k.endswith("k_octave3_%dx%d" % (r, c)) for k in table), (r, c, table)
+
+
+@pytest.mark.parametrize("variant", [1, 2])
+@pytest.mark.parametrize("hw", [(37, 53), (240, 320), (610, 830), (1001, 1111), (1978, 2640)])
+def test_layer_tile_height_variants_bit_identical(monkeypatch, hw, variant):
+    """Each tile height of the per-layer kernel, forced for every layer (16 and 64 rows against
+    32), gives the same DoG, magnitude and angle atlases bit for bit - interior tiles by tensor
+    copy, border tiles by cp.async with reflected rows and columns - on tiny octaves, planes off a
+    16-byte boundary and widths that are not a multiple of four, and the same keypoints."""
+    import fieldstitch_b200 as f
+    from fieldstitch_b200 import synth
+    h, w = hw
+    img = synth.synth_image(h, w, 11 + w)
+    monkeypatch.setenv("FSB_PYRAMID", "layer")
+    monkeypatch.setenv("FSB_LAYER_VARIANT", "0")
+    k0, st0 = f.gsift.detect(img)
+    ref = st0.atlas()
+    monkeypatch.setenv("FSB_LAYER_VARIANT", str(variant))
+    k1, st1 = f.gsift.detect(img)
+    got = st1.atlas()
+    assert got[0] == ref[0]
+    for o in range(len(ref[0])):
+        for k, name in ((1, "dog"), (2, "mag"), (3, "ang")):
+            np.testing.assert_array_equal(got[k][o], ref[k][o], err_msg="%s octave %d" % (name, o))
+    for key in ("x", "y", "size", "angle", "response"):
+        np.testing.assert_array_equal(k1[key], k0[key])
