@@ -99,3 +99,24 @@ def test_spread_arguments_checked_before_the_device():
     from fieldstitch_b200 import features
     with pytest.raises(ValueError):
         features._spread([], 100, 100, 10, gx=8)
+
+
+def test_pyramid_batch_arguments_checked_before_the_device():
+    """fsb_pyramid_batch_d rejects a null context, negative counts, bad sizes, a chain count outside
+    1..32 and null image pointers with a status before touching the device (a bogus non-null
+    context pointer is never dereferenced); an empty batch is a no-op."""
+    lib = _lib.load()
+    bogus = ctypes.c_void_p(1)
+    P2 = ctypes.c_void_p * 2
+    imgs = P2(16, 32)
+    assert lib.fsb_pyramid_batch_d(None, 2, imgs, 100, 100, 100, 0, 2) == 1
+    assert lib.fsb_pyramid_batch_d(bogus, -1, imgs, 100, 100, 100, 0, 2) == 1
+    assert lib.fsb_pyramid_batch_d(bogus, 0, None, 0, 0, 0, 0, 2) == 0
+    assert lib.fsb_pyramid_batch_d(bogus, 2, None, 100, 100, 100, 0, 2) == 1
+    assert lib.fsb_pyramid_batch_d(bogus, 2, imgs, 100, 100, 50, 0, 2) == 1
+    assert lib.fsb_pyramid_batch_d(bogus, 2, imgs, 40000, 100, 100, 0, 2) == 1
+    assert lib.fsb_pyramid_batch_d(bogus, 2, imgs, 100, 100, 100, 0, 0) == 1
+    assert b"chains" in lib.fsb_last_error()
+    assert lib.fsb_pyramid_batch_d(bogus, 2, imgs, 100, 100, 100, 0, 33) == 1
+    assert lib.fsb_pyramid_batch_d(bogus, 2, P2(16, None), 100, 100, 100, 0, 2) == 1
+    assert b"null image" in lib.fsb_last_error()
