@@ -201,25 +201,39 @@ __device__ __forceinline__ void hpass(const float2* t2, float* out, int yb, int 
 }
 
 // Gradient magnitude and direction (degrees in [0, 360)) of four pixels for the default (float32)
-// pyramid: magnitude through the reciprocal square root (within a few ulps of sqrt), direction by
-// octant reduction to t = min/max in [0, 1] and an odd polynomial for atan(t) in degrees. The
+// pyramid: magnitude by the approximate square root (within a few ulps of sqrt), direction by
+// octant reduction to t = min/max in [0, 1] (approximate reciprocal) and an odd polynomial for
+// atan(t) in degrees. The
 // coefficients were fitted here by iteratively reweighted least squares on Chebyshev nodes (max
 // error 2.2e-6 deg; 7.4e-6 deg with float32 evaluation), so the angle stays well inside the
 // reference's 0.1 deg keypoint tolerance. atan2(0, 0) = 0 as in the reference (border pixels).
 // Pixels go through in pairs with packed FP32x2 arithmetic; every multiply and add is explicitly
 // rounded (nothing is contracted into a fused multiply-add), so each engine that calls this
 // function computes the same bits.
+// the hardware's approximate square root and reciprocal (a few ulps; sqrt of 0 is 0)
+__device__ __forceinline__ float sqrt_approx(float x) {
+    float y;
+    asm("sqrt.approx.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+__device__ __forceinline__ float rcp_approx(float x) {
+    float y;
+    asm("rcp.approx.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+
 __device__ __forceinline__ void fast_grad4(const float (&dx)[4], const float (&dy)[4], float (&mag)[4],
                                            float (&ang)[4]) {
 #pragma unroll
     for (int h = 0; h < 2; ++h) {
         const float2 X = make_float2(dx[2 * h], dx[2 * h + 1]), Y = make_float2(dy[2 * h], dy[2 * h + 1]);
         const float2 d2 = __fadd2_rn(__fmul2_rn(X, X), __fmul2_rn(Y, Y));
-        const float2 rs = make_float2(d2.x > 0.f ? rsqrtf(d2.x) : 0.f, d2.y > 0.f ? rsqrtf(d2.y) : 0.f);
-        const float2 m = __fmul2_rn(d2, rs);
+        const float2 m = make_float2(sqrt_approx(d2.x), sqrt_approx(d2.y));
         const float ax0 = fabsf(X.x), ay0 = fabsf(Y.x), ax1 = fabsf(X.y), ay1 = fabsf(Y.y);
         const float mx0 = fmaxf(ax0, ay0), mn0 = fminf(ax0, ay0), mx1 = fmaxf(ax1, ay1), mn1 = fminf(ax1, ay1);
-        const float2 t = make_float2(mx0 > 0.f ? __fdividef(mn0, mx0) : 0.f, mx1 > 0.f ? __fdividef(mn1, mx1) : 0.f);
+        // min / max with the maximum kept above zero: 0 / tiny = 0 where both components vanish
+        const float2 t = __fmul2_rn(make_float2(mn0, mn1),
+                                    make_float2(rcp_approx(fmaxf(mx0, 1e-30f)), rcp_approx(fmaxf(mx1, 1e-30f))));
         const float2 z = __fmul2_rn(t, t);
         float2 p = make_float2(-2.323089093e-01f, -2.323089093e-01f);
         p = __ffma2_rn(p, z, make_float2(1.252652928e+00f, 1.252652928e+00f));
