@@ -782,6 +782,24 @@ __global__ void __launch_bounds__(LNT, r <= 10 ? 4 : 3) k_layer(const __grid_con
                 *reinterpret_cast<float4*>(vcs + row * VCW + q) = v;
             }
             __syncthreads();
+            // Tiles whose columns reflect at no image or source edge: column X = x0 - 16 + q + k
+            // samples source columns X / 2 and X / 2 -+ 1 in a fixed pattern, so four outputs take
+            // four consecutive row-interpolated values (the same products and sums as the tables)
+            if (x0 >= 18 && x0 + LX + 15 <= a.C - 3 && sx0 == (x0 - 16) / 2 - 1) {
+                for (int i = tid; i < IH * (LIN_C / 4); i += LNT) {
+                    const int row = i / (LIN_C / 4), m = i - row * (LIN_C / 4);
+                    const float* vr = vcs + row * VCW + 2 * m;   // source columns X / 2 - 1 .. + 2
+                    const float2 lo = *reinterpret_cast<const float2*>(vr);
+                    const float2 hi = *reinterpret_cast<const float2*>(vr + 2);
+                    const float a1 = __fmul_rn(0.75f, lo.y), a2 = __fmul_rn(0.75f, hi.x);
+                    float4 u;
+                    u.x = __fadd_rn(a1, __fmul_rn(0.25f, lo.x));
+                    u.y = __fadd_rn(a1, __fmul_rn(0.25f, hi.x));
+                    u.z = __fadd_rn(a2, __fmul_rn(0.25f, lo.y));
+                    u.w = __fadd_rn(a2, __fmul_rn(0.25f, hi.y));
+                    *reinterpret_cast<float4*>(s_in + row * LIN_W + 4 * m) = u;
+                }
+            } else {
             for (int i = tid; i < IH * (LIN_C / 4); i += LNT) {
                 const int row = i / (LIN_C / 4), q = 4 * (i - row * (LIN_C / 4));
                 const int4 ix = *reinterpret_cast<const int4*>(cxs + q);
@@ -793,6 +811,7 @@ __global__ void __launch_bounds__(LNT, r <= 10 ? 4 : 3) k_layer(const __grid_con
                 u.z = __fadd_rn(__fmul_rn(0.75f, v[ix.z]), __fmul_rn(0.25f, v[nx.z]));
                 u.w = __fadd_rn(__fmul_rn(0.75f, v[ix.w]), __fmul_rn(0.25f, v[nx.w]));
                 *reinterpret_cast<float4*>(s_in + row * LIN_W + q) = u;
+            }
             }
         } else {
             for (int i = tid; i < IH * LIN_C; i += LNT) {
