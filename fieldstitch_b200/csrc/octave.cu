@@ -999,16 +999,20 @@ __device__ __forceinline__ void g_load(const GroupArgs& a, int t, float* dst) {
 
 // vertical pass of level L: thread item = (column pair, 8 output rows); the last group of a level
 // whose height is not a multiple of 8 starts at row NOUT - 8 (rows it shares with the group before
-// are written twice with the same values), so every load stays inside the input level
+// are written twice with the same values), so every load stays inside the input level. Only the
+// level's rows below kmax and the columns its horizontal pass reads for output columns below jmax
+// are computed (a tile that reaches past the image needs its level only to the halo beyond it).
 template <int TS, class L>
-__device__ __forceinline__ void g_vpass(const float* __restrict__ pin, float2* __restrict__ v) {
+__device__ __forceinline__ void g_vpass(const float* __restrict__ pin, float2* __restrict__ v, int kmax, int jmax) {
     constexpr int r = L::RAD, NQ = L::VW / 2, NG = (L::NOUT + 7) / 8;
     static_assert(L::NOUT >= 8 && L::NIN == L::NOUT + 2 * r + 2 * L::ROFF, "vertical pass rows");
     float2 w[r + 1];
     load_taps<TS, r>(w);
+    const int qmax = jmax + 2 * r + L::E + 4;   // 2q below it: every column the needed items read
     for (int it = threadIdx.x; it < NQ * NG; it += GNT) {
         const int q = it % NQ, g = it / NQ;
         const int y8 = min(8 * g, L::NOUT - 8);
+        if (y8 >= kmax || 2 * q >= qmax) continue;
         const float* base = pin + (y8 + L::ROFF) * L::MIN + L::VS + 2 * q;
         float2 x[8 + 2 * r];
 #pragma unroll
@@ -1025,14 +1029,17 @@ __device__ __forceinline__ void g_vpass(const float* __restrict__ pin, float2* _
 
 // horizontal pass of level L: thread item = (row pair, 4 columns); the level's rows go to `pout`
 // (when not null) and epi(tile row of the upper row, tile column, upper row, lower row) runs for
-// every item (it checks the tile bounds itself)
+// every item (it checks the tile bounds itself); items at rows from kmax or columns from jmax on
+// are not needed and skipped
 template <int TS, class L, class Epi>
-__device__ __forceinline__ void g_hpass(const float2* __restrict__ v, float* __restrict__ pout, Epi epi) {
+__device__ __forceinline__ void g_hpass(const float2* __restrict__ v, float* __restrict__ pout, Epi epi, int kmax,
+                                        int jmax) {
     constexpr int r = L::RAD, NC = L::MOUT / 4, NP = L::NOUT / 2;
     float2 w[r + 1];
     load_taps<TS, r>(w);
     for (int it = threadIdx.x; it < NP * NC; it += GNT) {
         const int p = it / NC, c = 4 * (it - p * NC);
+        if (2 * p >= kmax || c >= jmax) continue;
         const float4* src = reinterpret_cast<const float4*>(v + p * L::VP + c + 2 * L::E);
         float2 yv[4 + 2 * r];
 #pragma unroll
@@ -1117,24 +1124,28 @@ __global__ void __launch_bounds__(GNT, 1) k_group(GroupArgs a) {
         if (nt < a.n_tiles) g_load<LA>(a, nt, sm + (cur ^ 1) * Sp::BUF0);
         cp_commit();
         const int y0 = (t / a.tiles_x) * GY, x0 = (t % a.tiles_x) * GX;
+        const int vy = min(GY, a.R - y0), vx = min(GX, a.C - x0);   // the tile's pixels inside the image
         float* b0 = sm + cur * Sp::BUF0;
         if constexpr (G == 0) {
             using LB = typename Sp::B;
             using LC = typename Sp::C;
-            g_vpass<1, LA>(b0, reinterpret_cast<float2*>(b1));                                   // L0 -> V1
+            g_vpass<1, LA>(b0, reinterpret_cast<float2*>(b1), vy + 2 * LA::HOUT, vx + 2 * LA::XOUT);  // L0 -> V1
             __syncthreads();
             g_hpass<1, LA>(reinterpret_cast<const float2*>(b1), b2,                               // V1 -> L1
-                           GEpi<LA::HIN, LA::XIN, LA::MIN>{a, y0, x0, b0, a.dog[0], nullptr, nullptr});
+                           GEpi<LA::HIN, LA::XIN, LA::MIN>{a, y0, x0, b0, a.dog[0], nullptr, nullptr},
+                           vy + 2 * LA::HOUT, vx + 2 * LA::XOUT);
             __syncthreads();
-            g_vpass<2, LB>(b2, reinterpret_cast<float2*>(b0));                                   // L1 -> V2
+            g_vpass<2, LB>(b2, reinterpret_cast<float2*>(b0), vy + 2 * LB::HOUT, vx + 2 * LB::XOUT);  // L1 -> V2
             __syncthreads();
             g_hpass<2, LB>(reinterpret_cast<const float2*>(b0), b1,                               // V2 -> L2
-                           GEpi<LB::HIN, LB::XIN, LB::MIN>{a, y0, x0, b2, a.dog[1], a.mag[0], a.ang[0]});
+                           GEpi<LB::HIN, LB::XIN, LB::MIN>{a, y0, x0, b2, a.dog[1], a.mag[0], a.ang[0]},
+                           vy + 2 * LB::HOUT, vx + 2 * LB::XOUT);
             __syncthreads();
-            g_vpass<3, LC>(b1, reinterpret_cast<float2*>(b0));                                   // L2 -> V3
+            g_vpass<3, LC>(b1, reinterpret_cast<float2*>(b0), vy + 2 * LC::HOUT, vx + 2 * LC::XOUT);  // L2 -> V3
             __syncthreads();
             g_hpass<3, LC>(reinterpret_cast<const float2*>(b0), b2,                               // V3 -> L3
-                           GEpi<LC::HIN, LC::XIN, LC::MIN>{a, y0, x0, b1, a.dog[2], a.mag[1], a.ang[1]});
+                           GEpi<LC::HIN, LC::XIN, LC::MIN>{a, y0, x0, b1, a.dog[2], a.mag[1], a.ang[1]},
+                           vy + 2 * LC::HOUT, vx + 2 * LC::XOUT);
             __syncthreads();
             // gradient of L3, L3 and L3[::2, ::2] on the tile
             for (int it = threadIdx.x; it < GY * (GX / 4); it += GNT) {
@@ -1158,15 +1169,17 @@ __global__ void __launch_bounds__(GNT, 1) k_group(GroupArgs a) {
             }
         } else {
             using LB = typename Sp::B;
-            g_vpass<4, LA>(b0, reinterpret_cast<float2*>(b1));                                   // L3 -> V4
+            g_vpass<4, LA>(b0, reinterpret_cast<float2*>(b1), vy + 2 * LA::HOUT, vx + 2 * LA::XOUT);  // L3 -> V4
             __syncthreads();
             g_hpass<4, LA>(reinterpret_cast<const float2*>(b1), b2,                               // V4 -> L4
-                           GEpi<LA::HIN, LA::XIN, LA::MIN>{a, y0, x0, b0, a.dog[0], nullptr, nullptr});
+                           GEpi<LA::HIN, LA::XIN, LA::MIN>{a, y0, x0, b0, a.dog[0], nullptr, nullptr},
+                           vy + 2 * LA::HOUT, vx + 2 * LA::XOUT);
             __syncthreads();
-            g_vpass<5, LB>(b2, reinterpret_cast<float2*>(b0));                                   // L4 -> V5
+            g_vpass<5, LB>(b2, reinterpret_cast<float2*>(b0), vy + 2 * LB::HOUT, vx + 2 * LB::XOUT);  // L4 -> V5
             __syncthreads();
             g_hpass<5, LB>(reinterpret_cast<const float2*>(b0), nullptr,                          // V5 -> L5
-                           GEpi<LB::HIN, LB::XIN, LB::MIN>{a, y0, x0, b2, a.dog[1], nullptr, nullptr});
+                           GEpi<LB::HIN, LB::XIN, LB::MIN>{a, y0, x0, b2, a.dog[1], nullptr, nullptr},
+                           vy + 2 * LB::HOUT, vx + 2 * LB::XOUT);
         }
     }
     cp_wait_all();
